@@ -1,0 +1,109 @@
+"""Generates the golden fixtures under tests/golden/<case>/.
+
+Each case is a seeded synthetic PLINK data set (eqtl_b200.synth) plus the
+outputs of the reference eqtl program itself, built from the reference's own
+sources by `make -C oracle` (oracle/_ref/eqtl). Run from the repository root:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+The fixtures are small (n=120 samples, 800 SNPs, 40 genes) so they commit
+cheaply; larger parity cases are generated on the fly by the GPU tests.
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from eqtl_b200 import synth  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "eqtl")
+
+# name -> (generator params, list of runs (tag, argv tail))
+CASES = {
+    "small": dict(
+        geno=dict(seed=101, n=120, m=800, n_chrom=3, chrom_len=5_000_000, family=(4, 5, 100),
+                  miss_rate=0.01, maf_lo=0.02),
+        genes=dict(seed=102, n_genes=40, body=1000),
+        pheno=dict(kind="lm", seed=103, n_cov=2),
+        runs=[
+            ("all", ["--model", "lm,lmm", "--mode", "all", "-w", "500000", "--pval-cis", "1e-2",
+                     "--pval-trans", "1e-2", "-t", "2"]),
+            ("gw", ["--model", "lm,lmm", "--mode", "gw", "--pval-trans", "1e-2", "-t", "1"]),
+            ("perm", ["--model", "lm,lmm", "--mode", "all", "-w", "500000", "--pval-cis", "1e-2",
+                      "--pval-trans", "1e-3", "--perm", "30", "--seed", "7", "--perm-trans-thr", "1e-2",
+                      "--perm-trans-top", "5", "-t", "2"]),
+            ("filter", ["--model", "lm", "--mode", "all", "-w", "500000", "--miss-hand", "filter",
+                        "--maf", "0.1", "--pval-cis", "1e-2", "--pval-trans", "1e-2", "-t", "1"]),
+            ("int", ["--model", "lm,lmm", "--mode", "trans", "--pheno-norm", "int", "--pval-trans",
+                     "1e-2", "-t", "1"]),
+            ("grm", ["--make-grm"]),
+        ]),
+    "nogff": dict(
+        geno=dict(seed=201, n=96, m=600, n_chrom=2, chrom_len=3_000_000, family=None,
+                  miss_rate=0.02, maf_lo=0.01),
+        genes=dict(seed=202, n_genes=24, body=1),
+        pheno=dict(kind="lmm", seed=203, n_cov=0),
+        runs=[
+            ("gw", ["--model", "lm,lmm", "--pval-trans", "5e-2", "--max-miss", "0.05", "-t", "1"]),
+            ("grm", ["--make-grm", "--max-miss", "0.05"]),
+        ]),
+}
+
+
+def build_case(name: str, spec: dict) -> None:
+    d = os.path.join(HERE, name)
+    if os.path.isdir(d):
+        shutil.rmtree(d)
+    os.makedirs(d)
+    g = synth.make_genotypes(**spec["geno"])
+    synth.write_plink(os.path.join(d, "geno"), g)
+    gs = spec["genes"]
+    chroms = sorted(set(g.chrom), key=g.chrom.index)
+    ids, gc, st, en, sd, tss = synth.make_genes(gs["seed"], gs["n_genes"], chroms,
+                                                spec["geno"]["chrom_len"], body=gs["body"])
+    ph = spec["pheno"]
+    if ph["kind"] == "lm":
+        Y, C = synth.make_pheno_lm(ph["seed"], g, gs["n_genes"], ph["n_cov"], cis_effects=True,
+                                   gene_tss=tss, gene_chrom=gc, window=500_000, n_trans=10)
+    else:
+        Y, C, _ = synth.make_pheno_lmm(ph["seed"], g, gs["n_genes"], ph["n_cov"], n_trans=10)
+    synth.write_pheno(os.path.join(d, "pheno.tsv"), g.samples, ids, Y)
+    have_cov = C.shape[1] > 0
+    if have_cov:
+        synth.write_covar(os.path.join(d, "covar.tsv"), g.samples, C)
+    have_gff = name != "nogff"
+    if have_gff:
+        synth.write_gff(os.path.join(d, "genes.gff"), ids, gc, st, en, sd)
+    manifest = {"runs": {}}
+    for tag, argv in spec["runs"]:
+        cmd = [REF, "-b", "geno"]
+        if "--make-grm" not in argv:
+            cmd += ["-e", "pheno.tsv"]
+            if have_gff:
+                cmd += ["-g", "genes.gff"]
+            if have_cov:
+                cmd += ["-c", "covar.tsv"]
+        cmd += argv + ["-o", f"ref_{tag}"]
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise SystemExit(f"{name}/{tag} failed: {r.stderr}")
+        manifest["runs"][tag] = {"argv": cmd[1:]}
+    for f in os.listdir(d):
+        if ".tmp." in f:
+            os.remove(os.path.join(d, f))
+    with open(os.path.join(d, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    if not os.path.exists(REF):
+        raise SystemExit("build the reference first: make -C oracle")
+    for name, spec in CASES.items():
+        build_case(name, spec)
+        print("built", name)
