@@ -1,0 +1,186 @@
+"""ctypes binding of libeqtl_cuda (include/eqtl_b200.h).
+
+This is the Python view of the C ABI used by the tests and the benchmark.
+It loads the in-tree eqtl_b200/lib/libeqtl_cuda.so and raises if it is
+missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libeqtl_cuda.so")
+
+EQTL_OK = 0
+ERRORS = {-1: "EQTL_E_ARG", -2: "EQTL_E_CUDA", -3: "EQTL_E_NOMEM", -4: "EQTL_E_STATE", -5: "EQTL_E_DEVICE",
+          -6: "EQTL_E_UNSUPPORTED", -7: "EQTL_E_OVERFLOW", -8: "EQTL_E_INTERNAL"}
+MISS_FILTER, MISS_IMPUTE = 0, 1
+PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
+
+# every symbol include/eqtl_b200.h declares
+EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
+           "eqtl_geno_dosage", "eqtl_scan_trans_lm"]
+
+
+class GeneResult(C.Structure):
+    _fields_ = [("n_tested", C.c_int32), ("acat_used", C.c_int32), ("acat_tan_sum", C.c_double),
+                ("best_snp", C.c_int64), ("best_p", C.c_double), ("best_beta", C.c_double),
+                ("best_se", C.c_double), ("best_t", C.c_double), ("best_r2", C.c_double)]
+
+
+class Pair(C.Structure):
+    _fields_ = [("snp", C.c_int64), ("gene", C.c_int32), ("reserved", C.c_int32), ("beta", C.c_double),
+                ("se", C.c_double), ("t", C.c_double), ("p", C.c_double), ("r2", C.c_double)]
+
+
+class ScanParams(C.Structure):
+    _fields_ = [("n", C.c_int32), ("n_genes", C.c_int32), ("p", C.c_int32), ("exclude_cis", C.c_int32),
+                ("pthr", C.c_double), ("perm_thr", C.c_double),
+                ("gene_chrom", C.POINTER(C.c_int32)), ("gene_lo", C.POINTER(C.c_int64)),
+                ("gene_hi", C.POINTER(C.c_int64)), ("snp_chrom", C.POINTER(C.c_int32)),
+                ("snp_pos", C.POINTER(C.c_int64))]
+
+
+GENE_DTYPE = np.dtype([("n_tested", np.int32), ("acat_used", np.int32), ("acat_tan_sum", np.float64),
+                       ("best_snp", np.int64), ("best_p", np.float64), ("best_beta", np.float64),
+                       ("best_se", np.float64), ("best_t", np.float64), ("best_r2", np.float64)])
+PAIR_DTYPE = np.dtype([("snp", np.int64), ("gene", np.int32), ("reserved", np.int32), ("beta", np.float64),
+                       ("se", np.float64), ("t", np.float64), ("p", np.float64), ("r2", np.float64)])
+assert GENE_DTYPE.itemsize == C.sizeof(GeneResult) and PAIR_DTYPE.itemsize == C.sizeof(Pair)
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built: run `python -m eqtl_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        vp, i32, i64, dp = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        lib.eqtl_open.argtypes = [C.c_int, C.POINTER(vp)]
+        lib.eqtl_close.argtypes = [vp]
+        lib.eqtl_close.restype = None
+        lib.eqtl_last_error.argtypes = [vp]
+        lib.eqtl_last_error.restype = C.c_char_p
+        lib.eqtl_set_precision.argtypes = [vp, C.c_int]
+        lib.eqtl_geno_load_bed.argtypes = [vp, vp, i64, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp,
+                                           C.POINTER(i64)]
+        lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
+        lib.eqtl_scan_trans_lm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, i64, C.POINTER(i64), vp,
+                                           i64, C.POINTER(i64)]
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class EqtlError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Context:
+    """One device context (eqtl_open / eqtl_close)."""
+
+    def __init__(self, device: int = 0, precision: int = PREC_SPLIT_F16):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.eqtl_open(device, C.byref(h))
+        if rc != EQTL_OK:
+            raise EqtlError(rc, "eqtl_open failed")
+        self.h = h
+        if precision != PREC_SPLIT_F16:
+            self._check(self.lib.eqtl_set_precision(self.h, precision))
+        self.n_kept = 0
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eqtl_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != EQTL_OK:
+            raise EqtlError(rc, self.lib.eqtl_last_error(self.h).decode())
+
+    # -- genotypes
+    def load_bed(self, rows: np.ndarray, n_file: int, sample_col, miss_hand: int = MISS_IMPUTE,
+                 max_miss: float = 0.8, maf_min: float = 0.0):
+        rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        col = np.ascontiguousarray(sample_col, dtype=np.int32)
+        m = rows.shape[0]
+        keep = np.zeros(m, np.uint8)
+        af = np.zeros(m, np.float64)
+        nm = np.zeros(m, np.int32)
+        nk = C.c_int64()
+        self._check(self.lib.eqtl_geno_load_bed(self.h, _ptr(rows), m, rows.shape[1] if m else (n_file + 3) // 4,
+                                                n_file, _ptr(col), col.size, miss_hand, max_miss, maf_min,
+                                                _ptr(keep), _ptr(af), _ptr(nm), C.byref(nk)))
+        self.n_kept = nk.value
+        self.n = col.size
+        return keep.astype(bool), af, nm
+
+    def dosage(self, lo: int, hi: int) -> np.ndarray:
+        out = np.zeros((hi - lo, self.n), np.float64)
+        self._check(self.lib.eqtl_geno_dosage(self.h, lo, hi, _ptr(out)))
+        return out
+
+    # -- scans
+    @staticmethod
+    def _params(n, G, p, pthr, perm_thr, windows):
+        prm = ScanParams()
+        prm.n, prm.n_genes, prm.p = n, G, p
+        prm.pthr, prm.perm_thr = pthr, perm_thr
+        keep = []
+        if windows is not None:
+            gchrom, glo, ghi, schrom, spos, exclude = windows
+            arrs = [np.ascontiguousarray(gchrom, np.int32), np.ascontiguousarray(glo, np.int64),
+                    np.ascontiguousarray(ghi, np.int64), np.ascontiguousarray(schrom, np.int32),
+                    np.ascontiguousarray(spos, np.int64)]
+            keep = arrs
+            prm.gene_chrom = arrs[0].ctypes.data_as(C.POINTER(C.c_int32))
+            prm.gene_lo = arrs[1].ctypes.data_as(C.POINTER(C.c_int64))
+            prm.gene_hi = arrs[2].ctypes.data_as(C.POINTER(C.c_int64))
+            prm.snp_chrom = arrs[3].ctypes.data_as(C.POINTER(C.c_int32))
+            prm.snp_pos = arrs[4].ctypes.data_as(C.POINTER(C.c_int64))
+            prm.exclude_cis = 1 if exclude else 0
+        return prm, keep
+
+    def _scan(self, fn, Y, X, pthr, perm_thr, windows, extra=()):
+        Y = np.asfortranarray(Y, dtype=np.float64)   # [n, G] column-major
+        X = np.asfortranarray(X, dtype=np.float64)   # [n, p]
+        n, G = Y.shape
+        prm, keep = self._params(n, G, X.shape[1], pthr, perm_thr, windows)
+        genes = np.zeros(G, GENE_DTYPE)
+        cap = 1 << 16
+        while True:
+            pairs = np.zeros(cap, PAIR_DTYPE)
+            cands = np.zeros(cap, PAIR_DTYPE)
+            npair, ncand = C.c_int64(), C.c_int64()
+            rc = fn(self.h, C.byref(prm), _ptr(Y), _ptr(X), *extra, _ptr(genes), _ptr(pairs), cap, C.byref(npair),
+                    _ptr(cands), cap, C.byref(ncand))
+            if rc == -7 and max(npair.value, ncand.value) > cap:
+                cap = max(npair.value, ncand.value)
+                continue
+            self._check(rc)
+            return genes, pairs[: npair.value], cands[: ncand.value]
+
+    def scan_trans_lm(self, Y, X, pthr, perm_thr=0.0, windows=None):
+        """eqtl_scan_trans_lm: Y [n, G] (gene columns), X [n, p] with intercept."""
+        return self._scan(self.lib.eqtl_scan_trans_lm, Y, X, pthr, perm_thr, windows)

@@ -1,0 +1,455 @@
+// C ABI of libeqtl_cuda and the host-side helpers shared by the scans.
+//
+// Every exported function catches all C++ exceptions, stores the message
+// in ctx->last_error and returns a negative EQTL_E_* code; nothing throws
+// across the ABI (the reference's die()/exception path, src/util.cpp:15-19,
+// becomes a status code the caller turns into its own "[E] ..." exit).
+#include <cublas_v2.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+
+#include "internal.hpp"
+#include "scan_host.hpp"
+#include "tstat.hpp"
+
+namespace eqtl {
+
+// ------------------------------------------------------------ tensor maps
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  EQTL_CHECK(fn != nullptr, EQTL_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+  return fn;
+}
+
+// 2-D map over a row-major [rows, k_pad] 16-bit matrix, box = 64 x box_rows,
+// 128-byte swizzle (the layout smem_desc_sw128 describes). Rows past `rows`
+// read as zeros.
+void make_map_2d(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k_pad, uint32_t box_rows, bool bf16) {
+  EQTL_CHECK(base != nullptr && rows > 0, EQTL_E_INTERNAL, "make_map_2d: empty operand");
+  EQTL_CHECK(k_pad % 64 == 0, EQTL_E_INTERNAL, "make_map_2d: k_pad must be a multiple of 64");
+  EQTL_CHECK((reinterpret_cast<uintptr_t>(base) & 15) == 0, EQTL_E_INTERNAL, "make_map_2d: base not 16B aligned");
+  const cuuint64_t dims[2] = {k_pad, rows};
+  const cuuint64_t strides[1] = {k_pad * 2};
+  const cuuint32_t box[2] = {64, box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                           const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  EQTL_CHECK(r == CUDA_SUCCESS, EQTL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(r) + ")");
+}
+
+int sm_count(eqtl_ctx* ctx) { return ctx->sm_count; }
+
+void check_tile_status(eqtl_ctx* ctx, const char* what) {
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  uint32_t st = 0;
+  EQTL_CUDA(cudaMemcpy(&st, ctx->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    static const char* names[] = {"ok",          "operand stage timeout", "ring slot timeout",
+                                  "accumulator commit timeout", "accumulator drain timeout",
+                                  "unwind timeout", "bad shape"};
+    throw Error(EQTL_E_DEVICE, std::string(what) + ": device wait expired (" +
+                                   (st < 7 ? names[st] : "unknown") + ")");
+  }
+}
+
+// --------------------------------------------------------- covariate math
+std::vector<double> xtx_inverse(const double* X, int n, int p) {
+  std::vector<double> A(static_cast<size_t>(p) * p, 0.0);
+  for (int a = 0; a < p; ++a)
+    for (int b = 0; b <= a; ++b) {
+      double s = 0;
+      for (int i = 0; i < n; ++i) s += X[static_cast<size_t>(a) * n + i] * X[static_cast<size_t>(b) * n + i];
+      A[a * p + b] = A[b * p + a] = s;
+    }
+  // Cholesky A = L L', then inverse column by column
+  std::vector<double> L(A);
+  for (int j = 0; j < p; ++j) {
+    double d = L[j * p + j];
+    for (int k = 0; k < j; ++k) d -= L[j * p + k] * L[j * p + k];
+    EQTL_CHECK(d > 0, EQTL_E_ARG, "covariate matrix X'X is singular");
+    L[j * p + j] = std::sqrt(d);
+    for (int i = j + 1; i < p; ++i) {
+      double s = L[i * p + j];
+      for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
+      L[i * p + j] = s / L[j * p + j];
+    }
+  }
+  std::vector<double> inv(static_cast<size_t>(p) * p, 0.0), y(p), x(p);
+  for (int c = 0; c < p; ++c) {
+    for (int i = 0; i < p; ++i) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) s -= L[i * p + k] * y[k];
+      y[i] = s / L[i * p + i];
+    }
+    for (int i = p - 1; i >= 0; --i) {
+      double s = y[i];
+      for (int k = i + 1; k < p; ++k) s -= L[k * p + i] * x[k];
+      x[i] = s / L[i * p + i];
+    }
+    for (int i = 0; i < p; ++i) inv[i * p + c] = x[i];
+  }
+  return inv;
+}
+
+static cublasHandle_t blas(eqtl_ctx* ctx) {
+  if (!ctx->cublas) {
+    cublasHandle_t h;
+    EQTL_CHECK(cublasCreate(&h) == CUBLAS_STATUS_SUCCESS, EQTL_E_CUDA, "cublasCreate failed");
+    cublasSetStream(h, ctx->stream);
+    ctx->cublas = h;
+  }
+  return static_cast<cublasHandle_t>(ctx->cublas);
+}
+
+#define EQTL_BLAS(call) EQTL_CHECK((call) == CUBLAS_STATUS_SUCCESS, EQTL_E_CUDA, #call " failed")
+
+void residualize_genes(eqtl_ctx* ctx, const double* dX, const double* dXtXinv, int n, int p, int G, double* dY,
+                       double* dXtY) {
+  cublasHandle_t h = blas(ctx);
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  // XtY = X' Y  [p, G]
+  EQTL_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, p, G, n, &one, dX, n, dY, n, &zero, dXtY, p));
+  // C = XtXinv XtY (XtXinv symmetric; row-major == column-major)
+  DevBuf<double> C;
+  C.alloc(static_cast<size_t>(p) * G);
+  EQTL_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, G, p, &one, dXtXinv, p, dXtY, p, &zero, C.p, p));
+  // Y <- Y - X C
+  EQTL_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, G, p, &mone, dX, n, C.p, p, &one, dY, n));
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+namespace {
+__global__ void col_sumsq_kernel(const double* Y, int n, int G, double* out) {
+  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (g >= G) return;
+  double s = 0;
+  for (int i = lane; i < n; i += 32) {
+    const double v = Y[static_cast<int64_t>(g) * n + i];
+    s += v * v;
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[g] = s;
+}
+}  // namespace
+
+void gene_yty(eqtl_ctx* ctx, const double* dY, int n, int G, std::vector<double>& yty) {
+  DevBuf<double> d;
+  d.alloc(G);
+  col_sumsq_kernel<<<(G + 7) / 8, 256, 0, ctx->stream>>>(dY, n, G, d.p);
+  EQTL_CUDA(cudaGetLastError());
+  yty.resize(G);
+  d.download(yty.data(), G, ctx->stream);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (gtg < 1e-12 || df <= 0) return;
+  q.beta = gty / gtg;
+  const double rss = yty - q.beta * gty;
+  const double s2 = std::max(rss / df, 0.0);
+  q.se = std::sqrt(s2 / gtg);
+  q.t = q.se > 0 ? q.beta / q.se : 0.0;
+  q.p = t_two_sided_p(q.t, df);
+  q.r2 = yty > 0 ? 1.0 - rss / yty : 0.0;
+}
+
+void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
+                 std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands) {
+  pairs.clear();
+  cands.clear();
+  const int G = prm->n_genes;
+  std::vector<const eqtl_pair*> best(G, nullptr);
+  for (const eqtl_pair& q : refined) {
+    if (q.p <= prm->pthr) pairs.push_back(q);
+    if (prm->perm_thr > 0 && std::isfinite(q.p) && q.p < prm->perm_thr) cands.push_back(q);
+    const eqtl_pair*& b = best[q.gene];
+    if (!b || q.p < b->p || (q.p == b->p && q.snp < b->snp)) b = &q;
+  }
+  for (int g = 0; g < G; ++g) {
+    eqtl_gene_result& r = genes[g];
+    if (r.n_tested > 0 && best[g]) {
+      r.best_snp = best[g]->snp;
+      r.best_p = best[g]->p;
+      r.best_beta = best[g]->beta;
+      r.best_se = best[g]->se;
+      r.best_t = best[g]->t;
+      r.best_r2 = best[g]->r2;
+    } else {
+      r.best_snp = -1;
+      r.best_p = 2.0;
+      r.best_beta = r.best_se = r.best_t = r.best_r2 = 0.0;
+    }
+  }
+  std::sort(pairs.begin(), pairs.end(), [](const eqtl_pair& a, const eqtl_pair& b) {
+    return a.snp != b.snp ? a.snp < b.snp : a.gene < b.gene;
+  });
+  std::sort(cands.begin(), cands.end(), [](const eqtl_pair& a, const eqtl_pair& b) {
+    if (a.gene != b.gene) return a.gene < b.gene;
+    if (a.p != b.p) return a.p < b.p;
+    return a.snp < b.snp;
+  });
+}
+
+void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
+                       const std::vector<int2>& deferred) {
+  if (deferred.empty()) return;
+  std::map<std::pair<int, int64_t>, double> pv;
+  for (const eqtl_pair& q : refined) pv[{q.gene, q.snp}] = q.p;
+  const long double kPiL = 3.14159265358979323846L;
+  for (const int2& d : deferred) {
+    auto it = pv.find({d.x, static_cast<int64_t>(d.y)});
+    EQTL_CHECK(it != pv.end(), EQTL_E_INTERNAL, "deferred ACAT pair was not refined");
+    double p = it->second;
+    if (!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12) continue;  // AcatAcc::add guards
+    if (p <= 0.0) p = 1e-300;
+    genes[d.x].acat_tan_sum += static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+  }
+}
+
+void upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, ScanWindows& w) {
+  if (!prm->gene_chrom || !prm->gene_lo || !prm->gene_hi || !prm->snp_chrom || !prm->snp_pos) return;
+  w.gc.upload(prm->gene_chrom, prm->n_genes, ctx->stream);
+  w.glo.upload(prm->gene_lo, prm->n_genes, ctx->stream);
+  w.ghi.upload(prm->gene_hi, prm->n_genes, ctx->stream);
+  w.sc.upload(prm->snp_chrom, m, ctx->stream);
+  w.sp.upload(prm->snp_pos, m, ctx->stream);
+}
+
+DeviceTTable::DeviceTTable(eqtl_ctx* ctx, double df) {
+  EQTL_CHECK(df > 0, EQTL_E_ARG, "residual degrees of freedom must be positive");
+  static std::mutex mu;
+  static std::map<double, TTableHost> cache;
+  TTableHost T;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(df);
+    if (it == cache.end()) it = cache.emplace(df, build_ttable(df)).first;
+    T = it->second;
+  }
+  h.upload(T.h.data(), T.h.size(), ctx->stream);
+  L.upload(T.L.data(), T.L.size(), ctx->stream);
+  t.h = h.p;
+  t.L = L.p;
+  t.t0 = static_cast<float>(T.t0);
+  t.du_inv = static_cast<float>(T.na / (T.t0 * T.t0));
+  t.s0 = static_cast<float>(T.s0);
+  t.ds_inv = static_cast<float>(T.nb / (T.s_end - T.s0));
+  t.s_end = static_cast<float>(T.s_end);
+  t.inv_df = static_cast<float>(1.0 / df);
+  t.na = T.na;
+  t.nb = T.nb;
+}
+
+namespace {
+__global__ void fill_u64(unsigned long long* p, int n, unsigned long long v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+}  // namespace
+
+ScanOutputs::ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint) : ctx(c), G(genes) {
+  acat.alloc(G);
+  used.alloc(G);
+  tested.alloc(G);
+  best.alloc(G);
+  count.alloc(1);
+  cap = static_cast<unsigned int>(std::min<int64_t>(std::max<int64_t>(cap_hint, 1 << 16), 1 << 26));
+  cand.alloc(cap);
+  (void)m;
+}
+
+void ScanOutputs::reset() {
+  acat.zero(ctx->stream);
+  used.zero(ctx->stream);
+  tested.zero(ctx->stream);
+  count.zero(ctx->stream);
+  fill_u64<<<(G + 255) / 256, 256, 0, ctx->stream>>>(best.p, G, ~0ull);
+  EQTL_CUDA(cudaGetLastError());
+}
+
+void ScanOutputs::run(const std::function<void(dev::GeneOut)>& launch) {
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    reset();
+    dev::GeneOut o{acat.p, used.p, tested.p, best.p, cand.p, count.p, cap};
+    launch(o);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+    count.download(&n_cand, 1, ctx->stream);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (n_cand <= cap) return;
+    EQTL_CHECK(n_cand <= (1u << 28), EQTL_E_OVERFLOW,
+               "scan produced " + std::to_string(n_cand) + " candidate pairs; lower the p threshold");
+    cap = n_cand + n_cand / 8;
+    cand.alloc(cap);
+  }
+  throw Error(EQTL_E_INTERNAL, "candidate buffer did not converge");
+}
+
+void ScanOutputs::collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred) {
+  std::vector<double> a(G);
+  std::vector<int> u(G), t(G);
+  std::vector<unsigned long long> b(G);
+  acat.download(a.data(), G, ctx->stream);
+  used.download(u.data(), G, ctx->stream);
+  tested.download(t.data(), G, ctx->stream);
+  best.download(b.data(), G, ctx->stream);
+  std::vector<int2> c(n_cand);
+  cand.download(c.data(), n_cand, ctx->stream);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  todo.clear();
+  deferred.clear();
+  for (const int2& q : c) {
+    const uint32_t s = static_cast<uint32_t>(q.y);
+    const int2 clean = make_int2(q.x, static_cast<int>(s & ~dev::kCandDeferred));
+    todo.push_back(clean);
+    if (s & dev::kCandDeferred) deferred.push_back(clean);
+  }
+  for (int g = 0; g < G; ++g) {
+    genes[g].n_tested = t[g];
+    genes[g].acat_used = u[g];
+    genes[g].acat_tan_sum = a[g];
+    genes[g].best_snp = -1;
+    if (t[g] > 0 && b[g] != ~0ull) todo.push_back(make_int2(g, static_cast<int>(b[g] & 0xFFFFFFFFull)));
+  }
+  std::sort(todo.begin(), todo.end(), [](int2 x, int2 y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
+  todo.erase(std::unique(todo.begin(), todo.end(), [](int2 x, int2 y) { return x.x == y.x && x.y == y.y; }),
+             todo.end());
+}
+
+}  // namespace eqtl
+
+// ===================================================================== ABI
+using eqtl::Error;
+
+template <class F>
+static int guarded(eqtl_ctx* ctx, F&& f) {
+  if (!ctx) return EQTL_E_ARG;
+  try {
+    EQTL_CUDA(cudaSetDevice(ctx->device));
+    f();
+    ctx->last_error.clear();
+    return EQTL_OK;
+  } catch (const Error& e) {
+    ctx->last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    ctx->last_error = "host allocation failed";
+    return EQTL_E_NOMEM;
+  } catch (const std::exception& e) {
+    ctx->last_error = e.what();
+    return EQTL_E_INTERNAL;
+  }
+}
+
+extern "C" {
+
+int eqtl_open(int device, eqtl_ctx** out) {
+  if (!out) return EQTL_E_ARG;
+  *out = nullptr;
+  auto* ctx = new (std::nothrow) eqtl_ctx;
+  if (!ctx) return EQTL_E_NOMEM;
+  ctx->device = device;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) {
+    delete ctx;
+    return EQTL_E_CUDA;
+  }
+  int rc = guarded(ctx, [&] {
+    cudaDeviceProp prop;
+    EQTL_CUDA(cudaGetDeviceProperties(&prop, device));
+    EQTL_CHECK(prop.major == 10 && prop.minor == 0, EQTL_E_UNSUPPORTED,
+               std::string("libeqtl_cuda is built for sm_100a (B200); device is ") + prop.name);
+    ctx->sm_count = prop.multiProcessorCount;
+    EQTL_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    EQTL_CUDA(cudaMalloc(&ctx->d_status, sizeof(uint32_t)));
+    EQTL_CUDA(cudaMemset(ctx->d_status, 0, sizeof(uint32_t)));
+  });
+  if (rc != EQTL_OK) {
+    eqtl_close(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return EQTL_OK;
+}
+
+void eqtl_close(eqtl_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* eqtl_last_error(const eqtl_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int eqtl_set_precision(eqtl_ctx* ctx, int precision) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(precision == EQTL_PREC_SPLIT_F16 || precision == EQTL_PREC_SPLIT_BF16 ||
+                   precision == EQTL_PREC_FP32_SIMT,
+               EQTL_E_ARG, "unknown precision");
+    EQTL_CHECK(ctx->geno.m_all == 0, EQTL_E_STATE, "set the precision before loading genotypes");
+    ctx->precision = precision;
+  });
+}
+
+int eqtl_geno_load_bed(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int32_t n_file,
+                       const int32_t* sample_col, int32_t n, int32_t miss_hand, double max_miss, double maf_min,
+                       uint8_t* keep_out, double* af_out, int32_t* n_miss_out, int64_t* n_kept_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK((rows || m == 0) && sample_col, EQTL_E_ARG, "null input");
+    eqtl::geno_load(ctx, rows, m, bytes_per_snp, n_file, sample_col, n, miss_hand, max_miss, maf_min);
+    const eqtl::Geno& g = ctx->geno;
+    if (keep_out) {
+      std::fill(keep_out, keep_out + m, 0);
+      for (int64_t s : g.kept_h) keep_out[s] = 1;
+    }
+    if (af_out) std::copy(g.af_h.begin(), g.af_h.end(), af_out);
+    if (n_miss_out) std::copy(g.n_miss_h.begin(), g.n_miss_h.end(), n_miss_out);
+    if (n_kept_out) *n_kept_out = g.m;
+  });
+}
+
+int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(out || hi == lo, EQTL_E_ARG, "null output");
+    eqtl::geno_dosage(ctx, lo, hi, out);
+  });
+}
+
+int eqtl_scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                       eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap, int64_t* n_pairs,
+                       eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(prm && Y && X && genes, EQTL_E_ARG, "null input");
+    EQTL_CHECK(ctx->precision != EQTL_PREC_FP32_SIMT, EQTL_E_UNSUPPORTED,
+               "the FP32 CUDA-core comparator is available for the LMM scan only");
+    std::vector<eqtl_pair> pv, cv;
+    eqtl::scan_trans_lm(ctx, prm, Y, X, genes, pv, cv);
+    if (n_pairs) *n_pairs = static_cast<int64_t>(pv.size());
+    if (n_cands) *n_cands = static_cast<int64_t>(cv.size());
+    EQTL_CHECK(static_cast<int64_t>(pv.size()) <= pair_cap && static_cast<int64_t>(cv.size()) <= cand_cap,
+               EQTL_E_OVERFLOW, "result buffer too small");
+    if (!pv.empty()) std::copy(pv.begin(), pv.end(), pairs);
+    if (!cv.empty()) std::copy(cv.begin(), cv.end(), cands);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+// K1: PLINK .bed decode on the device.
+//
+// Restates PlinkBed::decode_row (src/plink_bed.cpp:263-320): 2-bit code of
+// sample i at byte col/4, bits 2*(col%4); 00 -> 2 A1 alleles, 10 -> 1,
+// 11 -> 0, 01 -> missing (LUT :221-224). Per SNP: missing count, A1 sum,
+// mean-imputation value mu = sum / n_ok, allele frequency af = mu / 2 and
+// the filters (max missing fraction, --miss-hand filter, af in
+// (1e-12, 1-1e-12), MAF gate) in the same FP64 expressions, so keep flags
+// and af are bit-identical. Kept SNPs are then expanded once into the
+// centred FP16 hi/lo operand every tensor-core contraction reads:
+//     gc[s, i] = (dosage[s, i] - mu_s) * 64,   missing -> 0,
+// (centring leaves every statistic unchanged because the covariates always
+// contain an intercept; it removes the mean from the split).
+#include <cuda_bf16.h>
+
+#include "internal.hpp"
+
+namespace eqtl {
+namespace {
+
+__device__ __forceinline__ int bed_code(const uint8_t* row, int col) {
+  const uint32_t b = __ldg(row + (col >> 2));
+  const uint32_t pair = (b >> ((col & 3) * 2)) & 3u;
+  // LUT {2, -1, 1, 0} packed as bytes
+  return static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
+}
+
+__global__ void bed_stats_kernel(const uint8_t* __restrict__ bed, int64_t m, int64_t bps,
+                                 const int32_t* __restrict__ col, int n, int miss_hand, double max_miss,
+                                 double maf_min, int32_t* n_miss, int32_t* s1, int32_t* s2, uint8_t* pass,
+                                 double* af, double* mu) {
+  const int lane = threadIdx.x & 31;
+  const int64_t snp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (snp >= m) return;
+  const uint8_t* row = bed + snp * bps;
+  int nm = 0, a = 0, b = 0;
+  for (int i = lane; i < n; i += 32) {
+    const int c = bed_code(row, __ldg(col + i));
+    if (c < 0) {
+      ++nm;
+    } else {
+      a += c;
+      b += c * c;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    nm += __shfl_xor_sync(0xffffffffu, nm, o);
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane) return;
+  const int n_ok = n - nm;
+  bool keep = n_ok > 0;
+  const double sum = static_cast<double>(a);
+  double m_imp = 0.0, f = 0.0;
+  if (n_ok > 0) {
+    m_imp = sum / n_ok;
+    f = (sum / static_cast<double>(n_ok)) / 2.0;
+  }
+  const double miss_frac = static_cast<double>(nm) / static_cast<double>(n);
+  if (miss_frac > max_miss + 1e-15) keep = false;
+  if (miss_hand == EQTL_MISS_FILTER && nm > 0) keep = false;
+  if (f < 0) f = 0;
+  if (f > 1) f = 1;
+  if (f < 1e-12 || f > 1.0 - 1e-12) keep = false;
+  if (maf_min > 0.0 && (f < maf_min || f > 1.0 - maf_min)) keep = false;
+  n_miss[snp] = nm;
+  s1[snp] = a;
+  s2[snp] = b;
+  pass[snp] = keep ? 1 : 0;
+  af[snp] = f;
+  mu[snp] = m_imp;
+}
+
+template <class T>
+__device__ __forceinline__ T to16(double v);
+template <>
+__device__ __forceinline__ __half to16<__half>(double v) {
+  return __double2half(v);
+}
+template <>
+__device__ __forceinline__ __nv_bfloat16 to16<__nv_bfloat16>(double v) {
+  return __double2bfloat16(v);
+}
+__device__ __forceinline__ double from16(__half h) { return static_cast<double>(__half2float(h)); }
+__device__ __forceinline__ double from16(__nv_bfloat16 h) { return static_cast<double>(__bfloat162float(h)); }
+
+template <class T>
+__global__ void bed_expand_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                  int n, int k_pad, const int64_t* __restrict__ kept, int64_t m_kept,
+                                  const double* __restrict__ mu, float scale, T* hi, T* lo) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k_pad) return;
+  const int c_col = k < n ? __ldg(col + k) : 0;
+  for (int64_t r = blockIdx.y; r < m_kept; r += gridDim.y) {
+    const int64_t s = __ldg(kept + r);
+    double v = 0.0;
+    if (k < n) {
+      const int c = bed_code(bed + s * bps, c_col);
+      v = c < 0 ? 0.0 : (static_cast<double>(c) - __ldg(mu + s));
+    }
+    v *= static_cast<double>(scale);
+    const T h = to16<T>(v);
+    const T l = to16<T>(v - from16(h));
+    hi[r * k_pad + k] = h;
+    lo[r * k_pad + k] = l;
+  }
+}
+
+__global__ void bed_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                  int n, const int64_t* __restrict__ kept, int64_t lo, int64_t hi,
+                                  const double* __restrict__ mu, double* out) {
+  const int64_t total = (hi - lo) * n;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n;
+    const int i = static_cast<int>(e - r * n);
+    const int64_t s = kept[lo + r];
+    const int c = bed_code(bed + s * bps, col[i]);
+    out[e] = c < 0 ? mu[s] : static_cast<double>(c);
+  }
+}
+
+}  // namespace
+
+void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
+               const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min) {
+  EQTL_CHECK(m >= 0 && n > 0 && n_file > 0, EQTL_E_ARG, "geno_load: bad sizes");
+  EQTL_CHECK(bytes_per_snp == (n_file + 3) / 4, EQTL_E_ARG, "geno_load: bytes_per_snp != ceil(n_file/4)");
+  for (int i = 0; i < n; ++i)
+    EQTL_CHECK(sample_col[i] >= 0 && sample_col[i] < n_file, EQTL_E_ARG, "geno_load: sample_col out of range");
+  EQTL_CHECK(miss_hand == EQTL_MISS_FILTER || miss_hand == EQTL_MISS_IMPUTE, EQTL_E_ARG, "geno_load: miss_hand");
+  Geno& g = ctx->geno;
+  cudaStream_t st = ctx->stream;
+  g.m_all = m;
+  g.n = n;
+  g.n_file = n_file;
+  g.bytes_per_snp = bytes_per_snp;
+  g.k_pad = ((n + 63) / 64) * 64;
+  g.bed.upload(rows, static_cast<size_t>(m * bytes_per_snp), st);
+  g.col.upload(sample_col, n, st);
+  g.n_miss.alloc(m);
+  g.s1.alloc(m);
+  g.s2.alloc(m);
+  g.pass.alloc(m);
+  g.af.alloc(m);
+  g.mu.alloc(m);
+  if (m > 0) {
+    const int per_block = 8;
+    bed_stats_kernel<<<static_cast<unsigned>((m + per_block - 1) / per_block), 32 * per_block, 0, st>>>(
+        g.bed.p, m, bytes_per_snp, g.col.p, n, miss_hand, max_miss, maf_min, g.n_miss.p, g.s1.p, g.s2.p, g.pass.p,
+        g.af.p, g.mu.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  std::vector<uint8_t> pass(m);
+  g.mu_h.resize(m);
+  g.af_h.resize(m);
+  g.n_miss_h.resize(m);
+  g.pass.download(pass.data(), m, st);
+  g.mu.download(g.mu_h.data(), m, st);
+  g.af.download(g.af_h.data(), m, st);
+  g.n_miss.download(g.n_miss_h.data(), m, st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  g.kept_h.clear();
+  for (int64_t s = 0; s < m; ++s)
+    if (pass[s]) g.kept_h.push_back(s);
+  g.m = static_cast<int64_t>(g.kept_h.size());
+  g.kept.upload(g.kept_h.data(), g.kept_h.size(), st);
+  const size_t elems = static_cast<size_t>(g.m) * g.k_pad;
+  g.gc_hi.alloc(elems);
+  g.gc_lo.alloc(elems);
+  if (g.m > 0) {
+    dim3 grid((g.k_pad + 255) / 256, static_cast<unsigned>(g.m < 65535 ? g.m : 65535));
+    if (ctx->precision == EQTL_PREC_SPLIT_BF16) {
+      bed_expand_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+          g.bed.p, bytes_per_snp, g.col.p, n, g.k_pad, g.kept.p, g.m, g.mu.p, kGcScale,
+          reinterpret_cast<__nv_bfloat16*>(g.gc_hi.p), reinterpret_cast<__nv_bfloat16*>(g.gc_lo.p));
+    } else {
+      bed_expand_kernel<__half><<<grid, 256, 0, st>>>(g.bed.p, bytes_per_snp, g.col.p, n, g.k_pad, g.kept.p,
+                                                       g.m, g.mu.p, kGcScale, g.gc_hi.p, g.gc_lo.p);
+    }
+    EQTL_CUDA(cudaGetLastError());
+  }
+  EQTL_CUDA(cudaStreamSynchronize(st));
+}
+
+void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {
+  Geno& g = ctx->geno;
+  EQTL_CHECK(lo >= 0 && hi <= g.m && lo <= hi, EQTL_E_ARG, "geno_dosage: range outside kept SNPs");
+  if (hi == lo) return;
+  DevBuf<double> d;
+  d.alloc(static_cast<size_t>(hi - lo) * g.n);
+  bed_dosage_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, lo, hi,
+                                                   g.mu.p, d.p);
+  EQTL_CUDA(cudaGetLastError());
+  d.download(out_host, d.n, ctx->stream);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace eqtl

@@ -1,0 +1,145 @@
+// Internal host-side declarations of libeqtl_cuda: the context object behind
+// the C ABI, device buffer ownership, and the launchers each .cu file
+// provides. Nothing here crosses the ABI.
+#pragma once
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/eqtl_b200.h"
+
+namespace eqtl {
+
+// Thrown inside the library, converted to a status code at the ABI boundary.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define EQTL_CUDA(call)                                                                          \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      throw ::eqtl::Error(EQTL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+#define EQTL_CHECK(cond, code, msg)                         \
+  do {                                                      \
+    if (!(cond)) throw ::eqtl::Error((code), (msg));        \
+  } while (0)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error(EQTL_E_NOMEM, "device allocation of " + std::to_string(count * sizeof(T)) +
+                                    " bytes failed: " + cudaGetErrorString(e));
+    }
+    n = count;
+  }
+  void zero(cudaStream_t s) {
+    if (p) EQTL_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) EQTL_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void download(T* h, size_t count, cudaStream_t s) const {
+    if (count) EQTL_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+};
+
+// Decoded genotypes resident on the device (one .bed load).
+struct Geno {
+  int64_t m_all = 0;      // SNP rows uploaded
+  int64_t m = 0;          // SNPs kept by decode (rows of every SNP-side operand)
+  int n = 0;              // analysis samples
+  int n_file = 0;         // .fam samples
+  int64_t bytes_per_snp = 0;
+  int k_pad = 0;          // n rounded up to a multiple of 64
+  DevBuf<uint8_t> bed;    // [m_all, bytes_per_snp]
+  DevBuf<int32_t> col;    // [n] .fam column per analysis sample
+  DevBuf<int32_t> n_miss; // [m_all]
+  DevBuf<int32_t> s1;     // [m_all] sum of non-missing A1 counts
+  DevBuf<int32_t> s2;     // [m_all] sum of squares
+  DevBuf<uint8_t> pass;   // [m_all]
+  DevBuf<double> af;      // [m_all]
+  DevBuf<double> mu;      // [m_all] imputation mean
+  DevBuf<int64_t> kept;   // [m] row index of kept SNP
+  DevBuf<__half> gc_hi, gc_lo;  // [m, k_pad] (dosage - mean) * kGcScale, hi/lo FP16
+  std::vector<int64_t> kept_h;
+  std::vector<double> mu_h, af_h;
+  std::vector<int32_t> n_miss_h;
+};
+
+// Rotated genotypes for the LMM scans: Gt = Q^T (g - mean), Gt^2, hi/lo.
+struct Rotated {
+  int64_t m = 0;
+  int k_pad = 0;
+  DevBuf<__half> gt_hi, gt_lo, gt2_hi, gt2_lo;
+};
+
+struct LmmBasisDev {
+  int n = 0;
+  DevBuf<double> Q;        // [n, n] column-major (column j = eigenvector j)
+  DevBuf<double> lambda;   // [n]
+  std::vector<double> Q_h, lambda_h;
+};
+
+}  // namespace eqtl
+
+struct eqtl_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t* d_status = nullptr;  // device status word of the last tile launch
+  void* cublas = nullptr;        // cublasHandle_t
+  std::string last_error;
+  eqtl::Geno geno;
+  eqtl::Rotated rot;
+  eqtl::LmmBasisDev basis;
+  bool have_basis = false;
+  int precision = EQTL_PREC_SPLIT_F16;
+};
+
+namespace eqtl {
+
+// scale applied to centred dosages before the FP16 split (exact power of two)
+constexpr float kGcScale = 64.0f;
+
+// -- geno.cu
+void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
+               const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min);
+
+void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
+
+// -- scan drivers
+void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                   eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands);
+
+// -- status check after a tile launch (capi.cu)
+void check_tile_status(eqtl_ctx* ctx, const char* what);
+
+}  // namespace eqtl

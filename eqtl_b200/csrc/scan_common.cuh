@@ -1,0 +1,89 @@
+// Pieces shared by the scan epilogues: per-gene / per-SNP window logic
+// (include/eqtl/scan_common.hpp:58-69), the per-gene reduction state
+// (n_tested, ACAT tan sum, best key) and candidate compaction.
+#pragma once
+#include "tdist.cuh"
+#include "tile_gemm.cuh"
+
+namespace eqtl {
+namespace dev {
+
+enum WinMode : int { kWinNone = 0, kWinExclude = 1, kWinInclude = 2 };
+
+// high bit of a candidate's SNP field: its ACAT term is added on the host
+constexpr uint32_t kCandDeferred = 0x80000000u;
+
+struct GeneOut {
+  double* acat_sum;            // [G] sum of tan((1/2 - p) pi)
+  int* acat_used;              // [G]
+  int* n_tested;               // [G]
+  unsigned long long* best;    // [G] best_key (min)
+  int2* cand;                  // (gene, kept snp | kCandDeferred) with |t| >= t_cand or a deferred ACAT term
+  unsigned int* cand_count;
+  unsigned int cand_cap;
+};
+
+struct Windows {
+  int mode;
+  const int32_t* gene_chrom;
+  const int64_t* gene_lo;
+  const int64_t* gene_hi;
+  const int32_t* snp_chrom;
+  const int64_t* snp_pos;
+};
+
+// Per-thread (= per gene row) running state inside one tile.
+struct GeneAcc {
+  double acat = 0.0;
+  int used = 0;
+  int tested = 0;
+  unsigned long long best = ~0ull;
+  int chrom = -1;
+  int64_t lo = 0, hi = -1;
+
+  __device__ __forceinline__ void reset() {
+    acat = 0.0;
+    used = 0;
+    tested = 0;
+    best = ~0ull;
+  }
+  __device__ __forceinline__ void load_window(const Windows& w, int g) {
+    if (w.mode != kWinNone) {
+      chrom = w.gene_chrom[g];
+      lo = w.gene_lo[g];
+      hi = w.gene_hi[g];
+    }
+  }
+  // true if the (gene, snp) pair is part of this scope
+  __device__ __forceinline__ bool in_scope(const Windows& w, int64_t s) const {
+    if (w.mode == kWinNone) return true;
+    const bool inwin = chrom >= 0 && __ldg(w.snp_chrom + s) == chrom && __ldg(w.snp_pos + s) >= lo &&
+                       __ldg(w.snp_pos + s) <= hi;
+    return w.mode == kWinExclude ? !inwin : inwin;
+  }
+  __device__ __forceinline__ void add(const TailOut& o, int64_t s) {
+    ++tested;
+    if (o.use_acat) {
+      acat += o.term;  // 0 for deferred terms
+      ++used;
+    }
+    const unsigned long long k = best_key(o.neglog10p, static_cast<uint32_t>(s));
+    best = k < best ? k : best;
+  }
+  __device__ __forceinline__ void flush(const GeneOut& out, int g) const {
+    if (tested == 0) return;
+    atomicAdd(out.acat_sum + g, acat);
+    atomicAdd(out.acat_used + g, used);
+    atomicAdd(out.n_tested + g, tested);
+    atomicMin(out.best + g, best);
+  }
+};
+
+__device__ __forceinline__ void emit_candidate(const GeneOut& out, int g, int64_t s, bool deferred) {
+  const unsigned int idx = atomicAdd(out.cand_count, 1u);
+  if (idx < out.cand_cap)
+    out.cand[idx] = make_int2(g, static_cast<int>(static_cast<uint32_t>(s) | (deferred ? kCandDeferred : 0u)));
+}
+
+}  // namespace dev
+}  // namespace eqtl

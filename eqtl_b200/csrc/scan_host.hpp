@@ -1,0 +1,157 @@
+// Host-side plumbing shared by the scan drivers: tensor-map setup and tile
+// launches, per-gene output buffers (with candidate-overflow retry), window
+// tables, the device t table, and the FP64 finishing arithmetic applied to
+// refined pairs. Included only by .cu files.
+#pragma once
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "internal.hpp"
+#include "scan_common.cuh"
+#include "tile_gemm.cuh"
+#include "tstat.hpp"
+
+namespace eqtl {
+
+// -- covariate algebra (host FP64)
+std::vector<double> xtx_inverse(const double* X, int n, int p);  // (X'X)^-1, row-major p x p
+// Y[n, G] <- Y - X (XtXinv X'Y), on the device (cuBLAS DGEMM). XtY: scratch [p, G].
+void residualize_genes(eqtl_ctx* ctx, const double* dX, const double* dXtXinv, int n, int p, int G, double* dY,
+                       double* dXtY);
+void gene_yty(eqtl_ctx* ctx, const double* dY, int n, int G, std::vector<double>& yty);
+
+// FP64 hit_from_gty / test_lm arithmetic (src/scan_trans_lm.cpp:21-36).
+void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q);
+
+// Splits refined pairs into the pair list (p <= pthr, sorted by snp then
+// gene) and stage-2 candidates (p < perm_thr, sorted by gene, p, snp), and
+// sets each gene's best from the refined pairs (smallest p, lowest snp).
+void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
+                 std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands);
+
+struct ScanWindows {
+  DevBuf<int32_t> gc, sc;
+  DevBuf<int64_t> glo, ghi, sp;
+  dev::Windows view(int mode) const {
+    dev::Windows w;
+    w.mode = (gc.p && sc.p) ? mode : dev::kWinNone;
+    w.gene_chrom = gc.p;
+    w.gene_lo = glo.p;
+    w.gene_hi = ghi.p;
+    w.snp_chrom = sc.p;
+    w.snp_pos = sp.p;
+    return w;
+  }
+};
+void upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, ScanWindows& w);
+
+struct DeviceTTable {
+  DevBuf<float> h, L;
+  dev::TTable t{};
+  DeviceTTable(eqtl_ctx* ctx, double df);
+  dev::TTable view() const { return t; }
+};
+
+// Per-gene outputs of one scan launch + candidate buffer.
+struct ScanOutputs {
+  eqtl_ctx* ctx;
+  int G;
+  DevBuf<double> acat;
+  DevBuf<int> used, tested;
+  DevBuf<unsigned long long> best;
+  DevBuf<int2> cand;
+  DevBuf<unsigned int> count;
+  unsigned int cap;
+  unsigned int n_cand = 0;
+  ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint);
+  void reset();
+  // runs `launch` until every candidate fitted in the buffer
+  void run(const std::function<void(dev::GeneOut)>& launch);
+  // downloads per-gene sums into genes[] and returns the (gene, snp) pairs to
+  // refine: all candidates plus each gene's best SNP
+  void collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred);
+};
+
+// Adds, for every deferred (gene, snp) pair, the reference's long-double ACAT
+// term tan((0.5L - p) pi_L) computed from the refined FP64 p
+// (src/stats_extra.cpp:16-22; p <= 0 -> 1e-300).
+void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
+                       const std::vector<int2>& deferred);
+
+void make_map_2d(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k_pad, uint32_t box_rows, bool bf16);
+int sm_count(eqtl_ctx* ctx);
+
+// Launches the persistent tile kernel for NACC accumulators. a_*[j] are the
+// gene-side hi/lo operands of accumulator j ([rows_a, k_pad]); b_*[0..1] the
+// SNP-side pairs ([rows_b, k_pad]); bsel[j] picks the pair, prod[j] the
+// products. tiles: optional explicit tile list (device pointer) + count.
+template <int NT, int NACC, class EpiParams>
+void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
+                   const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
+                   int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
+                   int n_tile_list = 0);
+
+}  // namespace eqtl
+
+// ----------------------------------------------------------------- template
+namespace eqtl {
+
+template <class EpiParams>
+struct EpiOf;
+
+template <int NT, int NACC, class EpiParams>
+void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
+                   const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
+                   int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
+                   int n_tile_list) {
+  using Epi = typename EpiOf<EpiParams>::type;
+  using C = dev::TileCfg<NT, NACC>;
+  dev::TileMaps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  for (int j = 0; j < NACC; ++j) {
+    make_map_2d(&maps.a[2 * j], a_hi[j], rows_a, k_pad, dev::kTileM, bf16);
+    make_map_2d(&maps.a[2 * j + 1], a_lo[j], rows_a, k_pad, dev::kTileM, bf16);
+  }
+  int npairs = 0;
+  for (int j = 0; j < NACC; ++j) npairs = std::max(npairs, bsel[j] + 1);
+  for (int b = 0; b < npairs; ++b) {
+    make_map_2d(&maps.b[2 * b], b_hi[b], rows_b, k_pad, NT, bf16);
+    make_map_2d(&maps.b[2 * b + 1], b_lo[b], rows_b, k_pad, NT, bf16);
+  }
+  for (int b = npairs; b < 2; ++b) {
+    maps.b[2 * b] = maps.b[0];
+    maps.b[2 * b + 1] = maps.b[1];
+  }
+  dev::TileShape sh{};
+  sh.rows_a = static_cast<int>(rows_a);
+  sh.rows_b = static_cast<int>(rows_b);
+  sh.kchunks = k_pad / dev::kChunkK;
+  sh.n_acc = NACC;
+  for (int j = 0; j < dev::kMaxAcc; ++j) {
+    sh.bsel[j] = j < NACC ? bsel[j] : 0;
+    sh.prod[j] = j < NACC ? prod[j] : 0;
+  }
+  sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
+  sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
+  sh.tile_list = tile_list;
+  sh.n_tiles = tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b;
+  sh.status = ctx->d_status;
+  if (sh.n_tiles == 0) return;
+  EQTL_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
+  const int grid = std::min(sh.n_tiles, sm_count(ctx));
+  if (bf16) {
+    auto kern = dev::tile_kernel<NT, NACC, 1u, Epi>;
+    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
+    kern<<<grid, 192, C::SMEM_BYTES, ctx->stream>>>(maps, sh, ep);
+  } else {
+    auto kern = dev::tile_kernel<NT, NACC, 0u, Epi>;
+    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
+    kern<<<grid, 192, C::SMEM_BYTES, ctx->stream>>>(maps, sh, ep);
+  }
+  EQTL_CUDA(cudaGetLastError());
+  check_tile_status(ctx, "tile kernel");
+}
+
+}  // namespace eqtl

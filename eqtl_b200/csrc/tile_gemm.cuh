@@ -1,0 +1,284 @@
+// Persistent, warp-specialised tcgen05 tile kernel shared by every scan
+// contraction. It computes, for a tile of 128 gene-side rows (M) and NT
+// SNP-side rows (N), up to NACC FP32 accumulators
+//
+//     acc[j][g, s] = sum_k  A_j[g, k] * B_{bsel[j]}[s, k]
+//
+// where every operand is held as an FP16 (or BF16) hi/lo pair and the
+// product is formed as hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32
+// rounding). Both operands are K-major in global memory (row = gene or SNP,
+// K = sample index, zero-padded to a multiple of 64).
+//
+// Roles (192 threads):
+//   warp 0      TMA producer: one elected lane streams 64-wide K chunks of
+//               (A_hi, A_lo, B_hi, B_lo) into a STAGES-deep smem ring.
+//   warp 1      TMEM owner + MMA issuer: one elected lane issues
+//               tcgen05.mma (M=128, N=NT, K=16) into TMEM accumulators and
+//               releases ring slots with tcgen05.commit.
+//   warps 2..5  epilogue: each thread owns one accumulator row (TMEM lane),
+//               reads 16-column chunks with tcgen05.ld and hands them to the
+//               scan-specific Epi functor, which never writes the M x N
+//               matrix to HBM.
+// When NACC*NT <= 256 the accumulators are double-buffered so the epilogue of
+// tile i overlaps the MMAs of tile i+1.
+#pragma once
+#include "sm100.cuh"
+
+namespace eqtl {
+namespace dev {
+
+constexpr int kMaxAcc = 4;
+constexpr int kTileM = 128;
+constexpr int kChunkK = 64;  // 16-bit elements per K chunk (one 128-byte swizzle row)
+
+struct alignas(64) TileMaps {
+  CUtensorMap a[2 * kMaxAcc];  // gene-side operand of accumulator j: [2j] hi, [2j+1] lo
+  CUtensorMap b[4];            // SNP-side operand pairs: [0] hi, [1] lo, [2] hi, [3] lo
+};
+
+struct TileShape {
+  int rows_a;             // valid gene-side rows
+  int rows_b;             // valid SNP-side rows
+  int kchunks;            // K / 64
+  int n_acc;              // == NACC
+  int bsel[kMaxAcc];      // SNP-side pair used by accumulator j (0 or 1)
+  int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi
+  int tiles_a;            // ceil(rows_a / 128)
+  int tiles_b;            // ceil(rows_b / NT)
+  int n_tiles;            // tile work items (tiles_a * tiles_b unless a tile list is given)
+  const int2* tile_list;  // optional explicit (tile_a, tile_b) list (banded scans); null = dense
+  uint32_t* status;       // device status word (DevStatus)
+};
+
+template <int NT, int NACC>
+struct TileCfg {
+  static constexpr int A_BYTES = kTileM * kChunkK * 2;
+  static constexpr int B_BYTES = NT * kChunkK * 2;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int STAGES = (196608 / STAGE_BYTES) < 2 ? 2 : (196608 / STAGE_BYTES > 6 ? 6 : 196608 / STAGE_BYTES);
+  static constexpr int NBUF = (2 * NACC * NT <= 512) ? 2 : 1;
+  static constexpr uint32_t COLS_USED = NBUF * NACC * NT;
+  static constexpr uint32_t TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
+                                        : COLS_USED <= 256 ? 256 : 512;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+  static_assert(NACC >= 1 && NACC <= kMaxAcc, "NACC");
+  static_assert(NT % 16 == 0 && NT >= 16 && NT <= 256, "NT");
+  static_assert(NACC * NT <= 512, "TMEM");
+  static_assert(STAGES * STAGE_BYTES + 1024 + 256 <= 232448, "smem");
+};
+
+__device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta, int& tb) {
+  if (sh.tile_list) {
+    const int2 c = sh.tile_list[t];
+    ta = c.x;
+    tb = c.y;
+  } else {
+    tb = t / sh.tiles_a;
+    ta = t - tb * sh.tiles_a;
+  }
+}
+
+template <int NT, int NACC, uint32_t AB_FMT, class Epi>
+__global__ void __launch_bounds__(192, 1)
+    tile_kernel(const __grid_constant__ TileMaps maps, const TileShape sh,
+                const __grid_constant__ typename Epi::Params ep) {
+  using C = TileCfg<NT, NACC>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t* empty = full + C::STAGES;
+  uint64_t* accf = empty + C::STAGES;  // [2]
+  uint64_t* acce = accf + 2;           // [2]
+  uint64_t* drain = acce + 2;          // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  volatile uint32_t* abort_flag = tmem_slot + 1;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C::STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 128);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0u;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    for (int j = 0; j < 2 * NACC; ++j) tma_prefetch_map(&maps.a[j]);
+    for (int j = 0; j < 4; ++j) tma_prefetch_map(&maps.b[j]);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, C::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  uint32_t* status = sh.status;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (elect_one()) {
+      int stage = 0;
+      uint32_t phase = 0;
+      uint32_t issued_phase[6] = {0, 0, 0, 0, 0, 0};
+      bool issued[6] = {false, false, false, false, false, false};
+      bool ok = true;
+      for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
+        int ta, tb;
+        tile_coords(sh, t, ta, tb);
+        const int ra = ta * kTileM, rb = tb * NT;
+        for (int j = 0; j < NACC && ok; ++j) {
+          const int bp = sh.bsel[j];
+          for (int kc = 0; kc < sh.kchunks; ++kc) {
+            if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
+              ok = false;
+              break;
+            }
+            uint8_t* sb = smem + stage * C::STAGE_BYTES;
+            mbar_arrive_expect_tx(&full[stage], C::STAGE_BYTES);
+            tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
+            tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
+            tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[2 * bp], &full[stage], kc * kChunkK, rb);
+            tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
+            issued[stage] = true;
+            issued_phase[stage] = phase;
+            if (++stage == C::STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        }
+      }
+      // Drain: every load issued into a ring slot must land before the CTA
+      // may exit (bounded; normally already complete).
+      for (int s = 0; s < C::STAGES; ++s) {
+        if (!issued[s]) continue;
+        const long long t0 = clock64();
+        while (!mbar_test(&full[s], issued_phase[s])) {
+          if (clock64() - t0 > kWaitCycles) {
+            set_status(status, kDevTimeoutDrain);
+            break;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issuer
+    if (elect_one()) {
+      constexpr uint32_t idesc = idesc_f16(kTileM, NT, AB_FMT);
+      int stage = 0;
+      uint32_t phase = 0;
+      int buf = 0;
+      uint32_t accphase = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
+        if (!mbar_wait(&acce[buf], accphase ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) break;
+        tc_fence_after();
+        const uint32_t dbase = tmem_base + static_cast<uint32_t>(buf * NACC * NT);
+        for (int j = 0; j < NACC && ok; ++j) {
+          const uint32_t d = dbase + static_cast<uint32_t>(j * NT);
+          const int pm = sh.prod[j];
+          for (int kc = 0; kc < sh.kchunks; ++kc) {
+            if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
+            const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
+            const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
+#pragma unroll
+            for (int k = 0; k < kChunkK / 16; ++k) {
+              const uint32_t off = static_cast<uint32_t>(k * 32);
+              uint32_t accum = (kc > 0 || k > 0) ? 1u : 0u;
+              if (pm & 1) {
+                umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                accum = 1u;
+              }
+              if (pm & 2) {
+                umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
+                accum = 1u;
+              }
+              if (pm & 4) {
+                umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+              }
+            }
+            umma_commit(&empty[stage]);
+            if (++stage == C::STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+        }
+        if (!ok) break;
+        umma_commit(&accf[buf]);
+        if (C::NBUF == 2) {
+          buf ^= 1;
+          if (buf == 0) accphase ^= 1u;
+        } else {
+          accphase ^= 1u;
+        }
+      }
+      // Drain: all issued MMAs complete before TMEM is released (bounded).
+      umma_commit(drain);
+      const long long t0 = clock64();
+      while (!mbar_test(drain, 0u)) {
+        if (clock64() - t0 > kWaitCycles) {
+          set_status(status, kDevTimeoutDrain);
+          break;
+        }
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+    const int row = quarter * 32 + lane;
+    Epi epi(ep, sh);
+    int buf = 0;
+    uint32_t accphase = 0;
+    for (int t = blockIdx.x; t < sh.n_tiles; t += gridDim.x) {
+      int ta, tb;
+      tile_coords(sh, t, ta, tb);
+      if (!mbar_wait(&accf[buf], accphase, status, abort_flag, kDevTimeoutAccFull)) break;
+      tc_fence_after();
+      const uint32_t tbase =
+          tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buf * NACC * NT);
+      epi.begin_tile(ta * kTileM + row, tb * NT);
+#pragma unroll 1
+      for (int c = 0; c < NT; c += 16) {
+        float v[NACC][16];
+#pragma unroll
+        for (int j = 0; j < NACC; ++j) tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v[j]);
+        tmem_wait_ld();
+        epi.template chunk<NACC>(c, v);
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+      epi.end_tile();
+      if (C::NBUF == 2) {
+        buf ^= 1;
+        if (buf == 0) accphase ^= 1u;
+      } else {
+        accphase ^= 1u;
+      }
+    }
+    epi.finish();
+  }
+
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, C::TMEM_COLS);
+  }
+}
+
+}  // namespace dev
+}  // namespace eqtl
