@@ -1,0 +1,366 @@
+#!/usr/bin/env python3
+"""Benchmark of the trans/gw LMM association scan on B200.
+
+Workload (seeded synthetic data with the benchmark shapes; no data set ships
+with the reference): n = 2,000 samples (50 families of 10 siblings + 1,500
+unrelated, founders' alleles at MAF ~ U(0.01, 0.5), 1% missing calls),
+m = 500,000 SNPs, 10,000 genes with per-gene heritability h2 ~ U(0, 0.8) drawn
+from the genotype covariance, intercept-only covariates; `--mode gw` (every
+SNP against every gene). The metric counts tests = finite (SNP, gene) tests
+(GeneSummary.n_tested), i.e. 5e9 per step.
+
+One step = one pass of the path over the workload:
+  value  genotypes decoded and the GRM eigenbasis resident in HBM: spectral
+         rotation of all SNPs, per-gene REML prep, the tensor-core scan with
+         its fused epilogue and the FP64 refinement of candidate pairs
+         (the phenotype matrix is uploaded inside the step);
+  e2e    the same job through the C ABI from HOST buffers: .bed bytes and
+         phenotypes copied in, decode, GRM, eigendecomposition, rotation,
+         REML, scan, refinement, results copied out.
+Inputs are larger than L2 (the rotated genotypes alone are 8 GB), so no L2
+flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "trans-LMM SNP-gene tests/s, split-BF16 vs plain FP32 on 1 B200 at |Δlog10p|≤1e-3"
+UNIT = "tests/s"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+def workload(args, seed_offset=0):
+    from eqtl_b200 import synth
+    t0 = time.time()
+    rows, sub, _ = synth.make_bed_rows_chunked(20261208 + seed_offset, args.n, args.m, family=args.family,
+                                               maf_lo=0.01, maf_hi=0.5, miss_rate=0.01,
+                                               keep_codes_every=max(1, args.m // 2000))
+    Y, _ = synth.polygenic_pheno(20261209 + seed_offset, sub, args.genes)
+    X = np.ones((args.n, 1))
+    return rows, Y, X, time.time() - t0
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def event_pair(ctx):
+    import torch
+    s = torch.cuda.ExternalStream(ctx.stream_ptr(), device=torch.device("cuda", ctx.device))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return s, a, b
+
+
+def run_value_step(ctx, Y, X):
+    ctx.rotate()
+    genes, pairs, cands, delta = ctx.scan_trans_lmm(Y, X, pthr=1e-5)
+    return int(genes["n_tested"].sum()), len(pairs)
+
+
+def run_e2e_step(ctx, rows, n, Y, X):
+    ctx.load_bed(rows, n, np.arange(n, dtype=np.int32))
+    ctx.lmm_basis()
+    genes, pairs, cands, delta = ctx.scan_trans_lmm(Y, X, pthr=1e-5)
+    return int(genes["n_tested"].sum()), genes, pairs
+
+
+# ----------------------------------------------------------- reference arm
+def reference_sample(args, rows, Y, tmp):
+    """Writes a bounded sample of the workload (all n samples, the first
+    `ref_snps` SNPs, the first `ref_genes` genes) as PLINK + TSV files."""
+    from eqtl_b200 import synth
+    ms, gs = min(args.ref_snps, args.m), min(args.ref_genes, args.genes)
+    pre = os.path.join(tmp, "sample")
+    with open(pre + ".fam", "w") as f:
+        for i in range(args.n):
+            f.write(f"S{i + 1:05d} S{i + 1:05d} 0 0 0 -9\n")
+    with open(pre + ".bim", "w") as f:
+        for s in range(ms):
+            f.write(f"1\trs{s + 1}\t0\t{100 * (s + 1)}\tA\tG\n")
+    with open(pre + ".bed", "wb") as f:
+        f.write(bytes([0x6C, 0x1B, 0x01]))
+        f.write(np.ascontiguousarray(rows[:ms]).tobytes())
+    synth.write_pheno(os.path.join(tmp, "pheno.tsv"), [f"S{i + 1:05d}" for i in range(args.n)],
+                      [f"G{g + 1:05d}" for g in range(gs)], Y[:, :gs])
+    return pre, ms, gs
+
+
+def run_reference(exe, pre, tmp, threads):
+    out = os.path.join(tmp, "out")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, "-b", pre, "-e", os.path.join(tmp, "pheno.tsv"), "--model", "lmm", "--mode", "gw",
+                        "--pval-trans", "1e-5", "-t", str(threads), "-o", out], capture_output=True, text=True)
+    dt = time.perf_counter() - t0
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    tested = 0
+    with open(out + ".lmm.gw.region.tsv") as f:
+        next(f)
+        for ln in f:
+            tested += int(ln.split("\t")[3])
+    return tested, dt
+
+
+def reference_arm(args):
+    exe = os.path.join(ROOT, "oracle", "_ref", "eqtl")
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference"}
+    if not os.path.exists(exe):
+        print(json.dumps({**base, "unavailable": "oracle/_ref/eqtl not built (make -C oracle needs the reference "
+                                                   "sources)"}))
+        return
+    threads = os.cpu_count() or 1
+    rows, Y, X, _ = workload(args)
+    tmp = tempfile.mkdtemp(prefix="eqtl_ref_")
+    try:
+        pre, ms, gs = reference_sample(args, rows, Y, tmp)
+        for _ in range(args.warmup if args.warmup < 2 else 1):
+            run_reference(exe, pre, tmp, threads)
+        times, tested = [], 0
+        for _ in range(args.steps):
+            tested, dt = run_reference(exe, pre, tmp, threads)
+            times.append(dt)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    ms_step = 1e3 * statistics.mean(times)
+    value = tested / (ms_step / 1e3)
+    sample = (f"reference eqtl (built from its sources) --model lmm --mode gw -t {threads} on n={args.n}, "
+              f"{ms} SNPs x {gs} genes of the workload ({tested} tests per run, GRM + eigen + REML included)")
+    print(json.dumps({**base, "value": value, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "f64", "data": "synthetic",
+                      "config": config(args),
+                      "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def config(args):
+    return {"workload": "trans/gw LMM scan (--model lmm --mode gw)", "n_samples": args.n, "n_snps": args.m,
+            "n_genes": args.genes, "covariates": "intercept", "family_structure": list(args.family),
+            "pthr": 1e-5, "l2": "inputs larger than L2 (8 GB rotated genotypes)",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+# ------------------------------------------------------------------ B200 arm
+def b200_arm(args, rank, world, local_rank):
+    import torch
+    from eqtl_b200 import capi
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        import datetime
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    rows, Y, X, gen_s = workload(args)
+    n = args.n
+    pk, pk_kind = peaks()
+
+    ctx = capi.Context(local_rank)
+    h2d = rows.nbytes + Y.nbytes + X.nbytes
+    # ---- e2e: full job from host buffers through the C ABI
+    e2e_ms = []
+    tests = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tests, genes, pairs = run_e2e_step(ctx, rows, n, Y, X)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    d2h = genes.nbytes + pairs.nbytes
+    setup = {k: ctx.stage_ms(k) for k in ("decode", "grm", "eigen")}
+
+    # ---- value: resident genotypes + basis
+    for _ in range(args.warmup):
+        run_value_step(ctx, Y, X)
+    stream, ev0, ev1 = event_pair(ctx)
+    launches0 = ctx.launch_count()
+    scan_ms, stage = [], {k: [] for k in ("rotate", "prep", "scan", "refine")}
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            tests, _ = run_value_step(ctx, Y, X)
+            for k in stage:
+                stage[k].append(ctx.stage_ms(k))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms_total, max(e2e_ms) if e2e_ms else 0.0], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms_total, e2e_max = float(t[0]), float(t[1])
+    else:
+        e2e_max = max(e2e_ms) if e2e_ms else 0.0
+    ms_step = ms_total / args.steps
+    value = tests * world / (ms_step / 1e3)
+    e2e_value = tests * world / (statistics.mean(e2e_ms) / 1e3) if e2e_ms else None
+
+    # ---- roofline of the dominant kernel (the scan tile kernel)
+    scan_ms = statistics.mean(stage["scan"])
+    p_cov = X.shape[1]
+    flops = tests * 2.0 * n * (p_cov + 2)
+    achieved = flops / (scan_ms / 1e3) / 1e12
+    peak = pk.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": scan_traffic(tests), "kernel": "tile_kernel<128,3> (trans-LMM scan)",
+            "algorithmic_flops_per_test": 2 * n * (p_cov + 2),
+            "peak_source": f"{pk_kind} bf16 dense sustained (kernel runs >100 ms under the power cap)",
+            "issued_flops_per_test": 3 * 2 * n * (p_cov + 2)}
+
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f16x2 split (FP32 accumulate), FP64 REML/refine", "data": "synthetic",
+           "config": config(args),
+           "stage_ms": {k: statistics.mean(v) for k, v in stage.items()}, "setup_ms": setup,
+           "tests_per_step": tests, "gen_s": gen_s,
+           "roofline": roof, "gpu_launches": launches,
+           "clocks": clk.summary(),
+           "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": statistics.mean(e2e_ms) if e2e_ms else None,
+                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
+
+    # ---- plain FP32 CUDA-core comparator of the same scan (scan kernel only)
+    if rank == 0 and not args.no_fp32:
+        ctx32 = capi.Context(local_rank, precision=capi.PREC_FP32_SIMT)
+        ctx32.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        ctx32.lmm_basis()
+        run_value_step(ctx32, Y, X)
+        s32 = ctx32.stage_ms("scan")
+        out["fp32_simt"] = {"scan_ms": s32, "tests_per_s_scan": tests / (s32 / 1e3),
+                            "tensor_speedup": s32 / scan_ms}
+        ctx32.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, rows, Y)
+    ctx.close()
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def scan_traffic(tests):
+    """DRAM bytes of the scan kernel per launch, scaled from the committed ncu
+    capture summary (profiles/tile_kernel_lmm_scan.txt: 'dram_bytes_per_test')."""
+    p = os.path.join(ROOT, "profiles", "tile_kernel_lmm_scan.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("dram_bytes_per_test:"):
+            return float(ln.split(":")[1]) * tests
+    return None
+
+
+def cpu_baseline(args, rows, Y):
+    exe = os.path.join(ROOT, "oracle", "_ref", "eqtl")
+    if not os.path.exists(exe):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "oracle/_ref not built"}
+    threads = os.cpu_count() or 1
+    tmp = tempfile.mkdtemp(prefix="eqtl_cpu_")
+    try:
+        pre, ms, gs = reference_sample(args, rows, Y, tmp)
+        tested, dt = run_reference(exe, pre, tmp, threads)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"value": tested / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"reference eqtl -t {threads}, n={args.n}, {ms} SNPs x {gs} genes, {tested} tests, "
+                      f"{dt:.1f} s wall (GRM + eigen + REML + tests)"}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=2000)
+    ap.add_argument("--m", type=int, default=500_000)
+    ap.add_argument("--genes", type=int, default=10_000)
+    ap.add_argument("--ref-snps", type=int, default=2000)
+    ap.add_argument("--ref-genes", type=int, default=1000)
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.family = (50, 10, args.n - 500) if args.n > 500 else None
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank == 0:
+            reference_arm(args)
+        return
+    b200_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -22,7 +22,10 @@ PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
 
 # every symbol include/eqtl_b200.h declares
 EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
-           "eqtl_geno_dosage", "eqtl_scan_trans_lm"]
+           "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
+           "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
+           "eqtl_stream"]
+STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
 
 class GeneResult(C.Structure):
@@ -72,6 +75,15 @@ def load() -> C.CDLL:
         lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
         lib.eqtl_scan_trans_lm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, i64, C.POINTER(i64), vp,
                                            i64, C.POINTER(i64)]
+        lib.eqtl_grm.argtypes = [vp, vp, vp, C.POINTER(i64)]
+        lib.eqtl_stage_ms.argtypes = [vp, C.c_int, C.POINTER(dp)]
+        lib.eqtl_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+        lib.eqtl_lmm_rotate.argtypes = [vp]
+        lib.eqtl_stream.argtypes = [vp, C.POINTER(vp)]
+        lib.eqtl_lmm_basis.argtypes = [vp, vp, i32, vp, vp]
+        lib.eqtl_lmm_set_basis.argtypes = [vp, vp, vp, i32]
+        lib.eqtl_scan_trans_lmm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, vp, i64, C.POINTER(i64),
+                                            vp, i64, C.POINTER(i64)]
         _lib = lib
     return _lib
 
@@ -96,6 +108,7 @@ class Context:
         if rc != EQTL_OK:
             raise EqtlError(rc, "eqtl_open failed")
         self.h = h
+        self.device = device
         if precision != PREC_SPLIT_F16:
             self._check(self.lib.eqtl_set_precision(self.h, precision))
         self.n_kept = 0
@@ -184,3 +197,52 @@ class Context:
     def scan_trans_lm(self, Y, X, pthr, perm_thr=0.0, windows=None):
         """eqtl_scan_trans_lm: Y [n, G] (gene columns), X [n, p] with intercept."""
         return self._scan(self.lib.eqtl_scan_trans_lm, Y, X, pthr, perm_thr, windows)
+
+    def stage_ms(self, stage: str) -> float:
+        """Device time of a pipeline stage in the last call that ran it."""
+        v = C.c_double()
+        self._check(self.lib.eqtl_stage_ms(self.h, STAGES[stage], C.byref(v)))
+        return v.value
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._check(self.lib.eqtl_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def stream_ptr(self) -> int:
+        v = C.c_void_p()
+        self._check(self.lib.eqtl_stream(self.h, C.byref(v)))
+        return v.value or 0
+
+    def rotate(self):
+        self._check(self.lib.eqtl_lmm_rotate(self.h))
+
+    def grm(self):
+        """eqtl_grm -> (K [n, n], N_packed [n(n+1)/2], m_used)."""
+        K = np.zeros((self.n, self.n), np.float64)
+        N = np.zeros(self.n * (self.n + 1) // 2, np.int32)
+        mu = C.c_int64()
+        self._check(self.lib.eqtl_grm(self.h, _ptr(K), _ptr(N), C.byref(mu)))
+        return K, N, mu.value
+
+    def lmm_basis(self, K=None):
+        """eqtl_lmm_basis -> (lambda [n], Q [n, n] with eigenvectors as columns)."""
+        n = self.n if K is None else K.shape[0]
+        lam = np.zeros(n, np.float64)
+        Qc = np.zeros(n * n, np.float64)
+        Kc = None if K is None else np.ascontiguousarray(K, np.float64)
+        self._check(self.lib.eqtl_lmm_basis(self.h, _ptr(Kc), n, _ptr(lam), _ptr(Qc)))
+        return lam, Qc.reshape(n, n).T
+
+    def set_basis(self, Q, lam):
+        """eqtl_lmm_set_basis with Q [n, n] (eigenvectors as columns)."""
+        Qc = np.ascontiguousarray(np.asarray(Q, np.float64).T)   # column-major
+        lam = np.ascontiguousarray(lam, np.float64)
+        self._check(self.lib.eqtl_lmm_set_basis(self.h, _ptr(Qc), _ptr(lam), lam.size))
+
+    def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None):
+        """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta)."""
+        delta = np.zeros(np.asarray(Y).shape[1], np.float64)
+        genes, pairs, cands = self._scan(self.lib.eqtl_scan_trans_lmm, Y, X, pthr, perm_thr, windows,
+                                         extra=(_ptr(delta),))
+        return genes, pairs, cands, delta

@@ -53,6 +53,20 @@ void make_map_2d(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k_p
 
 int sm_count(eqtl_ctx* ctx) { return ctx->sm_count; }
 
+void stage_begin(eqtl_ctx* ctx, int stage) {
+  StageTimer& T = ctx->timer;
+  if (!T.start[stage]) {
+    EQTL_CUDA(cudaEventCreate(&T.start[stage]));
+    EQTL_CUDA(cudaEventCreate(&T.stop[stage]));
+  }
+  EQTL_CUDA(cudaEventRecord(T.start[stage], ctx->stream));
+}
+
+void stage_end(eqtl_ctx* ctx, int stage) {
+  StageTimer& T = ctx->timer;
+  if (T.stop[stage] && cudaEventRecord(T.stop[stage], ctx->stream) == cudaSuccess) T.used[stage] = true;
+}
+
 void check_tile_status(eqtl_ctx* ctx, const char* what) {
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
   uint32_t st = 0;
@@ -168,6 +182,31 @@ void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q) 
   q.t = q.se > 0 ? q.beta / q.se : 0.0;
   q.p = t_two_sided_p(q.t, df);
   q.r2 = yty > 0 ? 1.0 - rss / yty : 0.0;
+}
+
+void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv, double rss_null,
+                    int p, double df, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (gg < 1e-12) return;
+  double aTu = 0, aTchi = 0;
+  for (int x = 0; x < p; ++x) {
+    double ux = 0;
+    for (int y = 0; y < p; ++y) ux += ainv[x * p + y] * a[y];
+    aTu += a[x] * ux;
+    aTchi += a[x] * chi0[x];
+  }
+  const double S = gg - aTu;
+  if (S <= 1e-15) return;
+  const double bg = (yg - aTchi) / S;
+  double qq = rss_null - S * bg * bg;
+  if (qq < 0) qq = 0;
+  const double sigma2 = df > 0 ? qq / df : 1.0;
+  q.beta = bg;
+  q.se = std::sqrt(std::max(sigma2 / S, 0.0));
+  q.t = q.se > 0 ? q.beta / q.se : 0.0;
+  q.p = t_two_sided_p(q.t, df);
+  q.r2 = rss_null > 1e-15 ? std::max(0.0, 1.0 - qq / rss_null) : 0.0;
 }
 
 void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
@@ -394,6 +433,10 @@ void eqtl_close(eqtl_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
   if (ctx->d_status) cudaFree(ctx->d_status);
+  for (int i = 0; i < EQTL_N_STAGES; ++i) {
+    if (ctx->timer.start[i]) cudaEventDestroy(ctx->timer.start[i]);
+    if (ctx->timer.stop[i]) cudaEventDestroy(ctx->timer.stop[i]);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -407,6 +450,38 @@ int eqtl_set_precision(eqtl_ctx* ctx, int precision) {
                EQTL_E_ARG, "unknown precision");
     EQTL_CHECK(ctx->geno.m_all == 0, EQTL_E_STATE, "set the precision before loading genotypes");
     ctx->precision = precision;
+  });
+}
+
+int eqtl_stage_ms(eqtl_ctx* ctx, int stage, double* ms) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(stage >= 0 && stage < EQTL_N_STAGES && ms, EQTL_E_ARG, "bad stage");
+    EQTL_CHECK(ctx->timer.used[stage], EQTL_E_STATE, "stage has not run");
+    EQTL_CUDA(cudaEventSynchronize(ctx->timer.stop[stage]));
+    float f = 0;
+    EQTL_CUDA(cudaEventElapsedTime(&f, ctx->timer.start[stage], ctx->timer.stop[stage]));
+    *ms = f;
+  });
+}
+
+int eqtl_launch_count(eqtl_ctx* ctx, uint64_t* count) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(count, EQTL_E_ARG, "null output");
+    *count = ctx->launches;
+  });
+}
+
+int eqtl_stream(eqtl_ctx* ctx, void** stream) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(stream, EQTL_E_ARG, "null output");
+    *stream = static_cast<void*>(ctx->stream);
+  });
+}
+
+int eqtl_lmm_rotate(eqtl_ctx* ctx) {
+  return guarded(ctx, [&] {
+    ctx->rot.m = 0;
+    eqtl::lmm_rotate(ctx);
   });
 }
 
@@ -431,6 +506,65 @@ int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
   return guarded(ctx, [&] {
     EQTL_CHECK(out || hi == lo, EQTL_E_ARG, "null output");
     eqtl::geno_dosage(ctx, lo, hi, out);
+  });
+}
+
+int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out) {
+  return guarded(ctx, [&] {
+    eqtl::DevBuf<double> K;
+    eqtl::DevBuf<int32_t> N;
+    const int64_t mu = eqtl::grm_compute(ctx, K, N);
+    const int n = ctx->geno.n;
+    if (K_out) K.download(K_out, static_cast<size_t>(n) * n, ctx->stream);
+    if (N_packed_out) N.download(N_packed_out, static_cast<size_t>(n) * (n + 1) / 2, ctx->stream);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (m_used_out) *m_used_out = mu;
+  });
+}
+
+int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out, double* Q_out) {
+  return guarded(ctx, [&] {
+    eqtl::DevBuf<double> dK;
+    if (K) {
+      EQTL_CHECK(n > 0, EQTL_E_ARG, "n must be positive");
+      dK.upload(K, static_cast<size_t>(n) * n, ctx->stream);
+    } else {
+      eqtl::DevBuf<int32_t> N;
+      eqtl::grm_compute(ctx, dK, N);
+      n = ctx->geno.n;
+    }
+    eqtl::lmm_basis_from_grm(ctx, dK.p, n);
+    if (lambda_out) std::copy(ctx->basis.lambda_h.begin(), ctx->basis.lambda_h.end(), lambda_out);
+    if (Q_out) {
+      ctx->basis.Q.download(Q_out, static_cast<size_t>(n) * n, ctx->stream);
+      EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+  });
+}
+
+int eqtl_lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int32_t n) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(Q && lambda && n > 0, EQTL_E_ARG, "null basis");
+    eqtl::lmm_set_basis(ctx, Q, lambda, n);
+  });
+}
+
+int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                        double* delta_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
+                        int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(prm && Y && X && genes, EQTL_E_ARG, "null input");
+    std::vector<eqtl_pair> pv, cv;
+    if (ctx->precision == EQTL_PREC_FP32_SIMT)
+      eqtl::scan_trans_lmm_simt(ctx, prm, Y, X, delta_out, genes, pv, cv);
+    else
+      eqtl::scan_trans_lmm(ctx, prm, Y, X, delta_out, genes, pv, cv);
+    if (n_pairs) *n_pairs = static_cast<int64_t>(pv.size());
+    if (n_cands) *n_cands = static_cast<int64_t>(cv.size());
+    EQTL_CHECK(static_cast<int64_t>(pv.size()) <= pair_cap && static_cast<int64_t>(cv.size()) <= cand_cap,
+               EQTL_E_OVERFLOW, "result buffer too small");
+    if (!pv.empty()) std::copy(pv.begin(), pv.end(), pairs);
+    if (!cv.empty()) std::copy(cv.begin(), cv.end(), cands);
   });
 }
 

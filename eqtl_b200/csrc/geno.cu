@@ -146,7 +146,9 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   g.pass.alloc(m);
   g.af.alloc(m);
   g.mu.alloc(m);
+  StageScope timer(ctx, EQTL_STAGE_DECODE);
   if (m > 0) {
+    ++ctx->launches;
     const int per_block = 8;
     bed_stats_kernel<<<static_cast<unsigned>((m + per_block - 1) / per_block), 32 * per_block, 0, st>>>(
         g.bed.p, m, bytes_per_snp, g.col.p, n, miss_hand, max_miss, maf_min, g.n_miss.p, g.s1.p, g.s2.p, g.pass.p,
@@ -172,6 +174,7 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   g.gc_lo.alloc(elems);
   if (g.m > 0) {
     dim3 grid((g.k_pad + 255) / 256, static_cast<unsigned>(g.m < 65535 ? g.m : 65535));
+    ++ctx->launches;
     if (ctx->precision == EQTL_PREC_SPLIT_BF16) {
       bed_expand_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
           g.bed.p, bytes_per_snp, g.col.p, n, g.k_pad, g.kept.p, g.m, g.mu.p, kGcScale,
@@ -191,6 +194,7 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {
   if (hi == lo) return;
   DevBuf<double> d;
   d.alloc(static_cast<size_t>(hi - lo) * g.n);
+  ++ctx->launches;
   bed_dosage_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, lo, hi,
                                                    g.mu.p, d.p);
   EQTL_CUDA(cudaGetLastError());

@@ -1,0 +1,222 @@
+// K2: GCTA-standardised GRM on the tensor cores.
+//
+// Restates compute_grm_from (src/grm.cpp:113-224) for the loaded genotypes:
+//   per SNP   mu = mean of the imputed dosages, p = mu/2, skipped unless
+//             p in [1e-8, 1-1e-8] and sd = sqrt(2p(1-p)) >= 1e-12 (:153-158);
+//             z = (g - mu) / sd, 0 at missing calls (mean-imputed) (:159);
+//   GRM       A = sum_s z_s z_s'  (tcgen05, FP16 hi/lo, split-K with FP64
+//             accumulation of the FP32 partials across K ranges);
+//   counts    J = M M' with M the 0/1 missing mask: exact in FP16 with FP32
+//             accumulation (< 2^24 SNPs); sub_miss_i = J_ii and
+//             N_ij = m - J_ii - J_jj + J_ij, N_ii = m - J_ii (:162-221);
+//   divide    K_ij = A_ij / N_ij (0 if N_ij <= 0).
+#include "internal.hpp"
+#include "scan_host.hpp"
+
+namespace eqtl {
+namespace dev {
+
+__device__ __forceinline__ int bed_code_g(const uint8_t* row, int col) {
+  const uint32_t b = __ldg(row + (col >> 2));
+  const uint32_t pair = (b >> ((col & 3) * 2)) & 3u;
+  return static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
+}
+
+// per kept SNP: GRM usability, mean and 1/sd
+__global__ void grm_snp_kernel(const int64_t* __restrict__ kept, int64_t m, int n, const double* __restrict__ mu,
+                               const int32_t* __restrict__ n_miss, const int32_t* __restrict__ s1, uint8_t* use,
+                               double* mean, double* inv_sd) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const int64_t s = kept[r];
+  const double mean_v = (static_cast<double>(s1[s]) + n_miss[s] * mu[s]) / n;
+  const double p = mean_v / 2.0;
+  bool ok = !(p < 1e-8 || p > 1.0 - 1e-8);
+  const double sd = sqrt(2.0 * p * (1.0 - p));
+  if (sd < 1e-12) ok = false;
+  use[r] = ok ? 1 : 0;
+  mean[r] = mean_v;
+  inv_sd[r] = ok ? 1.0 / sd : 0.0;
+}
+
+// Zt[i, c] for GRM column c (= used SNP c): 32 x 32 tiles through smem so
+// both the bed reads (per SNP row) and the writes (per sample row) coalesce.
+__global__ void grm_transpose_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                     int n, const int64_t* __restrict__ used_rows, int64_t m_used, int64_t m_pad,
+                                     const double* __restrict__ mean, const double* __restrict__ inv_sd, __half* zh,
+                                     __half* zl, __half* mk) {
+  __shared__ float tz[32][33];
+  __shared__ float tm[32][33];
+  const int64_t c0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const int i0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int i = i0 + tx;
+  const int ci = i < n ? __ldg(col + i) : 0;
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t c = c0 + r;
+    float z = 0.0f, mm = 0.0f;
+    if (c < m_used && i < n) {
+      const int64_t s = used_rows[c];
+      const int code = bed_code_g(bed + s * bps, ci);
+      if (code < 0) {
+        mm = 1.0f;
+      } else {
+        z = static_cast<float>((static_cast<double>(code) - mean[c]) * inv_sd[c]);
+      }
+    }
+    tz[r][tx] = z;
+    tm[r][tx] = mm;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int ii = i0 + r;
+    const int64_t c = c0 + tx;
+    if (ii < n && c < m_pad) {
+      const float z = tz[tx][r];
+      // recompute in FP64 for the split: z itself came from FP64 above, and
+      // FP32 keeps 24 bits, more than hi+lo FP16 carry
+      const __half h = __float2half_rn(z);
+      const __half l = __float2half_rn(z - __half2float(h));
+      zh[static_cast<int64_t>(ii) * m_pad + c] = h;
+      zl[static_cast<int64_t>(ii) * m_pad + c] = l;
+      mk[static_cast<int64_t>(ii) * m_pad + c] = __float2half_rn(tm[tx][r]);
+    }
+  }
+}
+
+struct GrmEpiParams {
+  int n;
+  double* A;  // [n, n] FP64 sums (atomic)
+  int* J;     // [n, n] joint-missing counts (atomic, exact integers)
+};
+
+struct GrmEpi {
+  using Params = GrmEpiParams;
+  const Params& P;
+  int row = 0;
+  int64_t col0 = 0;
+  __device__ GrmEpi(const Params& p, const TileShape&) : P(p) {}
+  __device__ void begin_tile(int r, int64_t c0) {
+    row = r;
+    col0 = c0;
+  }
+  template <int NACC>
+  __device__ void chunk(int c, const float (&v)[NACC][16]) {
+    if (row >= P.n) return;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t cc = col0 + c + j;
+      if (cc >= P.n) break;
+      const int64_t idx = static_cast<int64_t>(row) * P.n + cc;
+      atomicAdd(P.A + idx, static_cast<double>(v[0][j]));
+      if (v[1][j] != 0.0f) atomicAdd(P.J + idx, __float2int_rn(v[1][j]));
+    }
+  }
+  __device__ void end_tile() {}
+  __device__ void finish() {}
+};
+
+__global__ void grm_finalize_kernel(int n, int64_t m_used, const double* __restrict__ A, const int* __restrict__ J,
+                                    double* K, int32_t* Npk) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= static_cast<int64_t>(n) * n) return;
+  const int i = static_cast<int>(e / n), j = static_cast<int>(e - static_cast<int64_t>(i) * n);
+  const int64_t mi = static_cast<int64_t>(J[static_cast<int64_t>(i) * n + i]);
+  const int64_t mj = static_cast<int64_t>(J[static_cast<int64_t>(j) * n + j]);
+  int64_t sub;
+  if (i == j) sub = m_used - mi;
+  else sub = m_used - mi - mj + static_cast<int64_t>(J[e]);
+  K[e] = sub > 0 ? A[e] / static_cast<double>(sub) : 0.0;
+  if (j <= i) Npk[static_cast<int64_t>(i) * (i + 1) / 2 + j] = static_cast<int32_t>(sub);
+}
+
+}  // namespace dev
+
+template <>
+struct EpiOf<dev::GrmEpiParams> {
+  using type = dev::GrmEpi;
+};
+
+// Computes the GRM of the loaded genotypes. K: device [n, n] (row-major ==
+// column-major, symmetric). Returns the number of SNPs used.
+int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
+  using namespace dev;
+  Geno& g = ctx->geno;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "grm: no genotypes loaded");
+  cudaStream_t st = ctx->stream;
+  const int n = g.n;
+  const int64_t m = g.m;
+  StageScope timer(ctx, EQTL_STAGE_GRM);
+  DevBuf<uint8_t> use;
+  DevBuf<double> mean, inv_sd;
+  use.alloc(std::max<int64_t>(m, 1));
+  mean.alloc(std::max<int64_t>(m, 1));
+  inv_sd.alloc(std::max<int64_t>(m, 1));
+  if (m > 0) {
+    ++ctx->launches;
+    grm_snp_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, st>>>(g.kept.p, m, n, g.mu.p, g.n_miss.p, g.s1.p,
+                                                                           use.p, mean.p, inv_sd.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  std::vector<uint8_t> use_h(m);
+  use.download(use_h.data(), m, st);
+  std::vector<double> mean_h(m), isd_h(m);
+  mean.download(mean_h.data(), m, st);
+  inv_sd.download(isd_h.data(), m, st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  std::vector<int64_t> rows;
+  std::vector<double> mean_u, isd_u;
+  for (int64_t r = 0; r < m; ++r)
+    if (use_h[r]) {
+      rows.push_back(g.kept_h[r]);
+      mean_u.push_back(mean_h[r]);
+      isd_u.push_back(isd_h[r]);
+    }
+  const int64_t mu_n = static_cast<int64_t>(rows.size());
+  EQTL_CHECK(mu_n > 0, EQTL_E_ARG, "no SNPs for GRM");
+  const int64_t m_pad = ((mu_n + 63) / 64) * 64;
+  DevBuf<int64_t> drows;
+  DevBuf<double> dmean, disd;
+  drows.upload(rows.data(), rows.size(), st);
+  dmean.upload(mean_u.data(), mean_u.size(), st);
+  disd.upload(isd_u.data(), isd_u.size(), st);
+  DevBuf<__half> zh, zl, mk;
+  const size_t elems = static_cast<size_t>(n) * m_pad;
+  zh.alloc(elems);
+  zl.alloc(elems);
+  mk.alloc(elems);
+  {
+    dim3 grid(static_cast<unsigned>(m_pad / 32), static_cast<unsigned>((n + 31) / 32));
+    ++ctx->launches;
+    grm_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, drows.p, mu_n, m_pad,
+                                                        dmean.p, disd.p, zh.p, zl.p, mk.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  DevBuf<double> A;
+  DevBuf<int> J;
+  A.alloc(static_cast<size_t>(n) * n);
+  J.alloc(static_cast<size_t>(n) * n);
+  A.zero(st);
+  J.zero(st);
+  GrmEpiParams ep{n, A.p, J.p};
+  const __half* ah[2] = {zh.p, mk.p};
+  const __half* al[2] = {zl.p, mk.p};
+  const __half* bh[2] = {zh.p, mk.p};
+  const __half* bl[2] = {zl.p, mk.p};
+  const int bsel[2] = {0, 1}, prod[2] = {7, 1};
+  const int tiles = ((n + 127) / 128) * ((n + 255) / 256);
+  const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
+  // the GRM operands are FP16 regardless of the scan precision
+  launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, nullptr, 0,
+                        ksplit);
+  K.alloc(static_cast<size_t>(n) * n);
+  Npk.alloc(static_cast<size_t>(n) * (n + 1) / 2);
+  const int64_t tot = static_cast<int64_t>(n) * n;
+  ++ctx->launches;
+  grm_finalize_kernel<<<static_cast<unsigned>((tot + 255) / 256), 256, 0, st>>>(n, mu_n, A.p, J.p, K.p, Npk.p);
+  EQTL_CUDA(cudaGetLastError());
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  return mu_n;
+}
+
+}  // namespace eqtl

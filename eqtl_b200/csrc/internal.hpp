@@ -110,8 +110,18 @@ struct LmmBasisDev {
 
 }  // namespace eqtl
 
+// Per-stage device timing: CUDA events recorded on the context stream around
+// each stage of the last call (see eqtl_stage_ms).
+struct StageTimer {
+  cudaEvent_t start[EQTL_N_STAGES] = {};
+  cudaEvent_t stop[EQTL_N_STAGES] = {};
+  bool used[EQTL_N_STAGES] = {};
+};
+
 struct eqtl_ctx {
   int device = 0;
+  StageTimer timer;
+  uint64_t launches = 0;  // kernels launched by the library since eqtl_open
   int sm_count = 0;
   cudaStream_t stream = nullptr;
   uint32_t* d_status = nullptr;  // device status word of the last tile launch
@@ -138,6 +148,30 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
 // -- scan drivers
 void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands);
+
+void scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* delta_out,
+                    eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands);
+void scan_trans_lmm_simt(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                         double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
+                         std::vector<eqtl_pair>& cands);
+
+// -- grm.cu / lmm.cu
+template <class T>
+struct DevBuf;
+int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk);
+void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n);
+void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n);
+void lmm_rotate(eqtl_ctx* ctx);
+
+// -- stage timing (capi.cu)
+void stage_begin(eqtl_ctx* ctx, int stage);
+void stage_end(eqtl_ctx* ctx, int stage);
+struct StageScope {
+  eqtl_ctx* c;
+  int s;
+  StageScope(eqtl_ctx* ctx, int stage) : c(ctx), s(stage) { stage_begin(c, s); }
+  ~StageScope() { stage_end(c, s); }
+};
 
 // -- status check after a tile launch (capi.cu)
 void check_tile_status(eqtl_ctx* ctx, const char* what);

@@ -1,0 +1,880 @@
+// LMM path: eigenbasis, spectral rotation (K3), batched REML (K7) and the
+// trans/gw LMM scan (K5).
+//
+// Restates src/model_lmm.cpp and src/scan_trans_lmm.cpp:82-251 on the
+// shared-keep path:
+//   basis     K = Q diag(lambda) Q', lambda clipped at 0 (make_lmm_basis,
+//             src/model_lmm.cpp:106-113) - cuSOLVER syevd, or a basis the
+//             caller supplies;
+//   rotate    Gt = Q' (g - mean) for every kept SNP on the tensor cores
+//             (FP16 hi/lo x hi/lo), written once as FP16 hi/lo pairs of Gt
+//             and Gt^2 (the SNP-side operands of the scan);
+//   REML      per gene: y~ = Q'y, X~ = Q'X, delta by the reference's grid /
+//             golden-section / Newton search on reml_negll
+//             (src/model_lmm.cpp:10-86), then dinv, A00, chi0, rss_null
+//             (prep_lmm, :124-153) - one CTA per gene, FP64;
+//   scan      per (gene, SNP) the bordered-Schur Wald test
+//             (src/scan_trans_lmm.cpp:11-40) from three contractions
+//               NUM = Gt . (w o r~)      (= yg - a'chi0, r~ = y~ - X~ chi0)
+//               a_k = Gt . (w o X~_k)
+//               gg  = Gt^2 . w
+//             S = gg - a' A00^-1 a, t^2 = df r/(1-r), r = NUM^2/(S rss_null);
+//   refine    candidates and each gene's best recomputed in FP64 from raw
+//             dosages rotated by cuBLAS DGEMM.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+
+#include "internal.hpp"
+#include "scan_host.hpp"
+#include "simt_tile.cuh"
+#include "tstat.hpp"
+
+namespace eqtl {
+namespace dev {
+
+constexpr int kMaxPLmm = 16;
+
+// ----------------------------------------------------------- rotation
+struct RotEpiParams {
+  int n;          // eigen rows (valid)
+  int64_t m;      // SNPs
+  int k_pad;
+  float unscale;  // accumulator -> Gt
+  float s1, s2;   // output scales of Gt and Gt^2
+  __half *gt_hi, *gt_lo, *gt2_hi, *gt2_lo;
+};
+
+struct RotEpi {
+  using Params = RotEpiParams;
+  const Params& P;
+  int row = 0;
+  int64_t col0 = 0;
+  __device__ RotEpi(const Params& p, const TileShape&) : P(p) {}
+  __device__ void begin_tile(int r, int64_t c0) {
+    row = r;
+    col0 = c0;
+  }
+  template <int NACC>
+  __device__ void chunk(int c, const float (&v)[NACC][16]) {
+    if (row >= P.n) return;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t s = col0 + c + j;
+      if (s >= P.m) break;
+      const float g = v[0][j] * P.unscale;
+      const float a = g * P.s1;
+      const float b = g * g * P.s2;
+      const __half ah = __float2half_rn(a), bh = __float2half_rn(b);
+      const int64_t idx = s * P.k_pad + row;
+      P.gt_hi[idx] = ah;
+      P.gt_lo[idx] = __float2half_rn(a - __half2float(ah));
+      P.gt2_hi[idx] = bh;
+      P.gt2_lo[idx] = __float2half_rn(b - __half2float(bh));
+    }
+  }
+  __device__ void end_tile() {}
+  __device__ void finish() {}
+};
+
+// Qt operand: row j = eigenvector j (column j of column-major Q) * 2^10.
+__global__ void q_split_kernel(const double* __restrict__ Q, int n, int k_pad, __half* hi, __half* lo) {
+  const int j = blockIdx.y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k_pad; i += gridDim.x * blockDim.x) {
+    const double v = i < n ? Q[static_cast<int64_t>(j) * n + i] * 1024.0 : 0.0;
+    const __half h = __double2half(v);
+    hi[static_cast<int64_t>(j) * k_pad + i] = h;
+    lo[static_cast<int64_t>(j) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+  }
+}
+
+// --------------------------------------------------------------- REML
+struct RemlShared {
+  double red[2][8];
+  double res[kMaxPLmm * (kMaxPLmm + 1) / 2 + kMaxPLmm];
+  double A[kMaxPLmm * kMaxPLmm];  // thread-0 scratch: X~'DX~ and its Cholesky factor
+  double L[kMaxPLmm * kMaxPLmm];
+  double x[kMaxPLmm], e[kMaxPLmm];
+  double val;
+};
+
+// Packed upper-triangle index of (a, b), a <= b.
+__device__ __forceinline__ int tri(int a, int b, int p) { return a * p - a * (a - 1) / 2 + (b - a); }
+
+// Solves A x = b for SPD A (p x p, row-major, Cholesky); returns false if not PD.
+__device__ bool chol_solve(const double* A, const double* b, double* x, double* logdet, int p, double* L) {
+  for (int j = 0; j < p; ++j) {
+    double d = A[j * p + j];
+    for (int k = 0; k < j; ++k) d -= L[j * p + k] * L[j * p + k];
+    if (!(d > 0)) return false;
+    L[j * p + j] = sqrt(d);
+    for (int i = j + 1; i < p; ++i) {
+      double s = A[i * p + j];
+      for (int k = 0; k < j; ++k) s -= L[i * p + k] * L[j * p + k];
+      L[i * p + j] = s / L[j * p + j];
+    }
+  }
+  double ld = 0;
+  for (int j = 0; j < p; ++j) ld += 2.0 * log(L[j * p + j]);
+  *logdet = ld;
+  if (b) {
+    double y[kMaxPLmm];
+    for (int i = 0; i < p; ++i) {
+      double s = b[i];
+      for (int k = 0; k < i; ++k) s -= L[i * p + k] * y[k];
+      y[i] = s / L[i * p + i];
+    }
+    for (int i = p - 1; i >= 0; --i) {
+      double s = y[i];
+      for (int k = i + 1; k < p; ++k) s -= L[k * p + i] * x[k];
+      x[i] = s / L[i * p + i];
+    }
+  }
+  return true;
+}
+
+// Block-wide REML -loglik at delta (every thread calls; result broadcast).
+__device__ double reml_eval(double delta, const double* __restrict__ yt, const double* __restrict__ Xt,
+                            const double* __restrict__ lam, int n, int p, double* wsh, RemlShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  double ld = 0, ydy = 0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    double v = delta * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    wsh[i] = w;
+    ld += log(v);
+    ydy += w * yt[i] * yt[i];
+  }
+  for (int o = 16; o; o >>= 1) {
+    ld += __shfl_xor_sync(0xffffffffu, ld, o);
+    ydy += __shfl_xor_sync(0xffffffffu, ydy, o);
+  }
+  if (lane == 0) {
+    sh.red[0][warp] = ld;
+    sh.red[1][warp] = ydy;
+  }
+  __syncthreads();
+  const int nq = p * (p + 1) / 2;
+  for (int q = warp; q < nq + p; q += nw) {
+    double acc = 0;
+    if (q < nq) {
+      int a = 0;
+      while (tri(a, p - 1, p) < q) ++a;  // row of packed index q
+      const int b = a + (q - tri(a, a, p));
+      for (int i = lane; i < n; i += 32) acc += wsh[i] * Xt[static_cast<int64_t>(a) * n + i] * Xt[static_cast<int64_t>(b) * n + i];
+    } else {
+      const int k = q - nq;
+      for (int i = lane; i < n; i += 32) acc += wsh[i] * yt[i] * Xt[static_cast<int64_t>(k) * n + i];
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) sh.res[q] = acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double logdet_d = 0, y_dy = 0;
+    for (int w = 0; w < nw; ++w) {
+      logdet_d += sh.red[0][w];
+      y_dy += sh.red[1][w];
+    }
+    double* A = sh.A;
+    double* beta = sh.x;
+    for (int a = 0; a < p; ++a)
+      for (int b = a; b < p; ++b) A[a * p + b] = A[b * p + a] = sh.res[tri(a, b, p)];
+    const double* XtDy = sh.res + nq;
+    double logdet_x = 0;
+    double out;
+    if (!chol_solve(A, XtDy, beta, &logdet_x, p, sh.L)) {
+      out = 1e300;
+    } else {
+      double q = y_dy;
+      for (int k = 0; k < p; ++k) q -= XtDy[k] * beta[k];
+      if (q <= 0) q = 1e-12;
+      const double df = static_cast<double>(n - p);
+      out = 0.5 * (df * log(q / df) + logdet_d + logdet_x);
+    }
+    sh.val = out;
+  }
+  __syncthreads();
+  const double r = sh.val;
+  __syncthreads();
+  return r;
+}
+
+// One CTA per gene: optimize_delta (src/model_lmm.cpp:39-86) and the
+// prep_lmm caches (:124-153). Ytil [G][n], Xtil [p][n].
+__global__ void __launch_bounds__(256) reml_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
+                                                   const double* __restrict__ lam, int n, int p, int G,
+                                                   double* delta_out, double* chi0_out, double* ainv_out,
+                                                   double* rss_out) {
+  extern __shared__ double wsh[];
+  __shared__ RemlShared sh;
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  auto f = [&](double d) { return reml_eval(d, yt, Xtil, lam, n, p, wsh, sh); };
+  const int df = n - p;
+  double d = 1.0;
+  if (df > 0) {
+    double best_d = 1.0;
+    double best_ll = f(1.0);
+    for (double dd = 1e-5; dd <= 1e5; dd *= 2.0) {
+      const double v = f(dd);
+      if (v < best_ll) {
+        best_ll = v;
+        best_d = dd;
+      }
+    }
+    double lo = best_d / 4.0, hi = best_d * 4.0;
+    if (lo < 1e-8) lo = 1e-8;
+    if (hi > 1e6) hi = 1e6;
+    const double phi = (1.0 + sqrt(5.0)) / 2.0;
+    for (int it = 0; it < 40; ++it) {
+      const double m1 = hi - (hi - lo) / phi;
+      const double m2 = lo + (hi - lo) / phi;
+      const double f1 = f(m1);
+      const double f2 = f(m2);
+      if (f1 < f2) hi = m2;
+      else lo = m1;
+    }
+    d = 0.5 * (lo + hi);
+    double cur = f(d);
+    for (int it = 0; it < 8; ++it) {
+      const double h = fmax(d * 1e-4, 1e-9);
+      const double fm = f(d - h);
+      const double fp = f(d + h);
+      const double g1 = (fp - fm) / (2.0 * h);
+      const double g2 = (fp - 2.0 * cur + fm) / (h * h);
+      if (!(g2 > 1e-12)) break;
+      const double step = g1 / g2;
+      const double dn = d - step;
+      if (!(dn > 1e-8 && dn < 1e6)) break;
+      const double vn = f(dn);
+      if (!(vn < cur)) break;
+      d = dn;
+      cur = vn;
+      if (fabs(step) < d * 1e-8) break;
+    }
+  }
+  // prep_lmm caches at the chosen delta: one more weighted reduction
+  f(d);
+  if (threadIdx.x == 0) {
+    const int nq = p * (p + 1) / 2;
+    double* A = sh.A;
+    double chi0[kMaxPLmm];
+    for (int a = 0; a < p; ++a)
+      for (int b = a; b < p; ++b) A[a * p + b] = A[b * p + a] = sh.res[tri(a, b, p)];
+    const double* XtDy = sh.res + nq;
+    double y_dy = 0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) y_dy += sh.red[1][w];
+    double ld;
+    bool ok = chol_solve(A, XtDy, chi0, &ld, p, sh.L);
+    double rss = y_dy;
+    if (ok) {
+      for (int k = 0; k < p; ++k) rss -= XtDy[k] * chi0[k];
+      if (rss < 0) rss = 0;
+      // A00^-1 column by column
+      for (int c = 0; c < p; ++c) {
+        for (int i = 0; i < p; ++i) sh.e[i] = (i == c) ? 1.0 : 0.0;
+        double dummy;
+        chol_solve(A, sh.e, sh.x, &dummy, p, sh.L);
+        for (int i = 0; i < p; ++i) ainv_out[(static_cast<int64_t>(g) * p + i) * p + c] = sh.x[i];
+      }
+    } else {
+      for (int k = 0; k < p; ++k) chi0[k] = 0;
+      for (int i = 0; i < p * p; ++i) ainv_out[static_cast<int64_t>(g) * p * p + i] = 0;
+    }
+    delta_out[g] = d;
+    rss_out[g] = rss;
+    for (int k = 0; k < p; ++k) chi0_out[static_cast<int64_t>(g) * p + k] = chi0[k];
+  }
+}
+
+// Gene-side operands, one block per gene: rows (w o r~), (w o X~_k), w, each
+// FP16 hi/lo with its own power-of-two scale; unscale[] = factors that turn
+// the accumulators back into NUM, a_k, gg.
+__global__ void lmm_gene_ops_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
+                                    const double* __restrict__ lam, const double* __restrict__ delta,
+                                    const double* __restrict__ chi0, int n, int p, int G, int k_pad, float s1,
+                                    float s2, __half* const* hi, __half* const* lo, float* unscale) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const int nops = p + 2;
+  __shared__ double mx[kMaxPLmm + 2][8];
+  __shared__ double sc[kMaxPLmm + 2];
+  const double d = delta[g];
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  double c0[kMaxPLmm];
+  for (int k = 0; k < p; ++k) c0[k] = chi0[static_cast<int64_t>(g) * p + k];
+  auto value = [&](int op, int i) -> double {
+    if (i >= n) return 0.0;
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    if (op == 0) {
+      double r = yt[i];
+      for (int k = 0; k < p; ++k) r -= Xtil[static_cast<int64_t>(k) * n + i] * c0[k];
+      return w * r;
+    }
+    if (op <= p) return w * Xtil[static_cast<int64_t>(op - 1) * n + i];
+    return w;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int op = 0; op < nops; ++op) {
+    double m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(value(op, i)));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) mx[op][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < nops) {
+    double m = 0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) m = fmax(m, mx[threadIdx.x][w]);
+    int e = 0;
+    if (m > 0) e = 10 - static_cast<int>(floor(log2(m)));
+    sc[threadIdx.x] = ldexp(1.0, e);
+    const double side = threadIdx.x == nops - 1 ? s2 : s1;
+    unscale[static_cast<int64_t>(g) * nops + threadIdx.x] = static_cast<float>(1.0 / (ldexp(1.0, e) * side));
+  }
+  __syncthreads();
+  for (int op = 0; op < nops; ++op) {
+    const double s = sc[op];
+    for (int i = threadIdx.x; i < k_pad; i += blockDim.x) {
+      const double v = value(op, i) * s;
+      const __half h = __double2half(v);
+      hi[op][static_cast<int64_t>(g) * k_pad + i] = h;
+      lo[op][static_cast<int64_t>(g) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+    }
+  }
+}
+
+// ------------------------------------------------------- scan epilogue
+template <int P>
+struct LmmEpiParams {
+  int G;
+  int64_t m;
+  const float* unscale;     // [G][P+2]
+  const double* ainv;       // [G][P][P]
+  const double* rss_null;   // [G]
+  const uint8_t* snp_ok;    // [m]
+  Windows win;
+  float df;
+  float t_cand;
+  TTable tt;
+  GeneOut out;
+};
+
+template <int P>
+struct LmmEpi {
+  using Params = LmmEpiParams<P>;
+  const Params& Pr;
+  int gene = 0;
+  int64_t snp0 = 0;
+  bool gvalid = false;
+  double u[P + 2];
+  double ai[P][P];
+  double inv_rss = 0;
+  GeneAcc acc;
+  __device__ LmmEpi(const Params& p, const TileShape&) : Pr(p) {}
+  __device__ void begin_tile(int g, int64_t s0) {
+    gene = g;
+    snp0 = s0;
+    gvalid = g < Pr.G;
+    acc.reset();
+    if (gvalid) {
+#pragma unroll
+      for (int k = 0; k < P + 2; ++k) u[k] = Pr.unscale[static_cast<int64_t>(g) * (P + 2) + k];
+#pragma unroll
+      for (int a = 0; a < P; ++a)
+#pragma unroll
+        for (int b = 0; b < P; ++b) ai[a][b] = Pr.ainv[(static_cast<int64_t>(g) * P + a) * P + b];
+      const double r = Pr.rss_null[g];
+      inv_rss = r > 0 ? 1.0 / r : 0.0;
+      acc.load_window(Pr.win, g);
+    }
+  }
+  template <int NACC>
+  __device__ void chunk(int c, const float (&v)[NACC][16]) {
+    static_assert(NACC == P + 2, "accumulators");
+    if (!gvalid) return;
+#pragma unroll 2
+    for (int j = 0; j < 16; ++j) {
+      const int64_t s = snp0 + c + j;
+      if (s >= Pr.m) break;
+      if (!__ldg(Pr.snp_ok + s)) continue;
+      if (!acc.in_scope(Pr.win, s)) continue;
+      const double num = static_cast<double>(v[0][j]) * u[0];
+      const double gg = static_cast<double>(v[P + 1][j]) * u[P + 1];
+      double S = gg;
+      double a[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) a[k] = static_cast<double>(v[1 + k][j]) * u[1 + k];
+#pragma unroll
+      for (int x = 0; x < P; ++x)
+#pragma unroll
+        for (int y = 0; y < P; ++y) S -= a[x] * ai[x][y] * a[y];
+      float t = 0.0f;
+      if (!(gg < 1e-12) && S > 1e-15) {
+        const double r = num * num / S * inv_rss;
+        const double omr = 1.0 - r;
+        if (omr > 0.0) {
+          const float t2 = Pr.df * static_cast<float>(r) / static_cast<float>(omr);
+          t = copysignf(sqrtf(t2), static_cast<float>(num));
+        }
+      }
+      const TailOut o = t_tail(t, Pr.tt);
+      acc.add(o, s);
+      if (fabsf(t) >= Pr.t_cand || o.deferred) emit_candidate(Pr.out, gene, s, o.deferred);
+    }
+  }
+  __device__ void end_tile() {
+    if (gvalid) acc.flush(Pr.out, gene);
+  }
+  __device__ void finish() {}
+};
+
+// subset gate for the LMM scan (src/scan_common.cpp:133-151)
+__global__ void snp_gate_kernel(const int64_t* __restrict__ kept, int64_t m, int n, const double* __restrict__ mu,
+                                const int32_t* __restrict__ n_miss, const int32_t* __restrict__ s1,
+                                const int32_t* __restrict__ s2, uint8_t* ok) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  const int64_t s = kept[r];
+  const double mus = mu[s];
+  const int k = n_miss[s];
+  const double sum = static_cast<double>(s1[s]) + k * mus;
+  const double sum2 = static_cast<double>(s2[s]) + k * mus * mus;
+  double af = (sum / n) / 2.0;
+  af = fmin(fmax(af, 0.0), 1.0);
+  const double maf = af > 0.5 ? 1.0 - af : af;
+  const double var = sum2 / n - (sum / n) * (sum / n);
+  ok[r] = (maf < 1e-12 || var < 1e-12) ? 0 : 1;
+}
+
+// raw dosages of listed kept SNPs, column-major [n, u]
+__global__ void raw_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                  int n, const int64_t* __restrict__ kept, const double* __restrict__ mu,
+                                  const int* __restrict__ snps, int u, double* out) {
+  const int64_t tot = static_cast<int64_t>(u) * n;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < tot;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c = static_cast<int>(e / n);
+    const int i = static_cast<int>(e - static_cast<int64_t>(c) * n);
+    const int64_t s = kept[snps[c]];
+    const uint32_t b = __ldg(bed + s * bps + (col[i] >> 2));
+    const uint32_t pair = (b >> ((col[i] & 3) * 2)) & 3u;
+    const int code = static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
+    out[e] = code < 0 ? mu[s] : static_cast<double>(code);
+  }
+}
+
+// per refined pair: gg, yg, a[p] from FP64 rotated raw dosage
+__global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const int* __restrict__ pair_col,
+                                  const int2* __restrict__ pairs, int n_pairs, const double* __restrict__ Ytil,
+                                  const double* __restrict__ Xtil, int p, const double* __restrict__ lam,
+                                  const double* __restrict__ delta, double* out /* [n_pairs][p+2] */) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= n_pairs) return;
+  const int g = pairs[w].x;
+  const double* gt = Gt + static_cast<int64_t>(pair_col[w]) * n;
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  const double d = delta[g];
+  double gg = 0, yg = 0, a[kMaxPLmm];
+  for (int k = 0; k < p; ++k) a[k] = 0;
+  for (int i = lane; i < n; i += 32) {
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double dg = gt[i] / v;
+    gg += dg * gt[i];
+    yg += dg * yt[i];
+    for (int k = 0; k < p; ++k) a[k] += Xtil[static_cast<int64_t>(k) * n + i] * dg;
+  }
+  for (int o = 16; o; o >>= 1) {
+    gg += __shfl_xor_sync(0xffffffffu, gg, o);
+    yg += __shfl_xor_sync(0xffffffffu, yg, o);
+    for (int k = 0; k < p; ++k) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+  }
+  if (lane == 0) {
+    double* o = out + static_cast<int64_t>(w) * (p + 2);
+    o[0] = gg;
+    o[1] = yg;
+    for (int k = 0; k < p; ++k) o[2 + k] = a[k];
+  }
+}
+
+}  // namespace dev
+
+template <>
+struct EpiOf<dev::RotEpiParams> {
+  using type = dev::RotEpi;
+};
+template <>
+struct EpiOf<dev::LmmEpiParams<1>> {
+  using type = dev::LmmEpi<1>;
+};
+template <>
+struct EpiOf<dev::LmmEpiParams<2>> {
+  using type = dev::LmmEpi<2>;
+};
+
+using namespace dev;
+
+static cublasHandle_t blas_of(eqtl_ctx* ctx) {
+  if (!ctx->cublas) {
+    cublasHandle_t h;
+    EQTL_CHECK(cublasCreate(&h) == CUBLAS_STATUS_SUCCESS, EQTL_E_CUDA, "cublasCreate failed");
+    cublasSetStream(h, ctx->stream);
+    ctx->cublas = h;
+  }
+  return static_cast<cublasHandle_t>(ctx->cublas);
+}
+
+// ------------------------------------------------------------------ basis
+void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
+  cudaStream_t st = ctx->stream;
+  StageScope timer(ctx, EQTL_STAGE_EIGEN);
+  LmmBasisDev& B = ctx->basis;
+  B.n = n;
+  B.Q.alloc(static_cast<size_t>(n) * n);
+  B.lambda.alloc(n);
+  EQTL_CUDA(cudaMemcpyAsync(B.Q.p, K_dev, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st));
+  cusolverDnHandle_t h;
+  EQTL_CHECK(cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS, EQTL_E_CUDA, "cusolverDnCreate failed");
+  cusolverDnSetStream(h, st);
+  int lwork = 0;
+  cusolverStatus_t cs = cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, B.Q.p, n,
+                                                    B.lambda.p, &lwork);
+  DevBuf<double> work;
+  DevBuf<int> info;
+  if (cs == CUSOLVER_STATUS_SUCCESS) {
+    work.alloc(std::max(lwork, 1));
+    info.alloc(1);
+    cs = cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, B.Q.p, n, B.lambda.p, work.p, lwork,
+                          info.p);
+  }
+  int info_h = 0;
+  if (cs == CUSOLVER_STATUS_SUCCESS) {
+    info.download(&info_h, 1, st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+  }
+  cusolverDnDestroy(h);
+  EQTL_CHECK(cs == CUSOLVER_STATUS_SUCCESS && info_h == 0, EQTL_E_CUDA, "GRM eigen decomposition failed");
+  B.lambda_h.resize(n);
+  B.lambda.download(B.lambda_h.data(), n, st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  for (double& l : B.lambda_h) l = std::max(l, 0.0);  // cwiseMax(0.0)
+  B.lambda.upload(B.lambda_h.data(), n, st);
+  B.Q_h.clear();
+  ctx->have_basis = true;
+  ctx->rot.m = 0;  // rotated genotypes belong to the previous basis
+}
+
+void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n) {
+  LmmBasisDev& B = ctx->basis;
+  B.n = n;
+  B.Q.upload(Q, static_cast<size_t>(n) * n, ctx->stream);
+  B.lambda_h.assign(lambda, lambda + n);
+  for (double& l : B.lambda_h) l = std::max(l, 0.0);
+  B.lambda.upload(B.lambda_h.data(), n, ctx->stream);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->have_basis = true;
+  ctx->rot.m = 0;
+}
+
+// --------------------------------------------------------------- rotation
+static void output_scales(int n, float& s1, float& s2) {
+  // |Gt| <= |g - mean|_2 <= 2 sqrt(n); |Gt^2| <= 4 n: keep both below ~3e4
+  s1 = std::ldexp(1.0f, static_cast<int>(std::floor(std::log2(30000.0 / (2.0 * std::sqrt(static_cast<double>(n)))))));
+  s2 = std::ldexp(1.0f, static_cast<int>(std::floor(std::log2(30000.0 / (4.0 * n)))));
+}
+
+void lmm_rotate(eqtl_ctx* ctx) {
+  Geno& g = ctx->geno;
+  Rotated& R = ctx->rot;
+  EQTL_CHECK(ctx->have_basis && ctx->basis.n == g.n, EQTL_E_STATE, "rotation needs an eigenbasis of size n");
+  EQTL_CHECK(ctx->precision != EQTL_PREC_SPLIT_BF16, EQTL_E_UNSUPPORTED,
+             "the LMM path runs split-FP16 (or the FP32 CUDA-core comparator); BF16 is LM-only");
+  if (R.m == g.m && R.k_pad == g.k_pad && R.gt_hi.p) return;
+  cudaStream_t st = ctx->stream;
+  StageScope timer(ctx, EQTL_STAGE_ROTATE);
+  const int n = g.n, k_pad = g.k_pad;
+  const int64_t m = g.m;
+  DevBuf<__half> qh, ql;
+  ++ctx->launches;
+  qh.alloc(static_cast<size_t>(n) * k_pad);
+  ql.alloc(static_cast<size_t>(n) * k_pad);
+  q_split_kernel<<<dim3((k_pad + 255) / 256, n), 256, 0, st>>>(ctx->basis.Q.p, n, k_pad, qh.p, ql.p);
+  EQTL_CUDA(cudaGetLastError());
+  const size_t elems = static_cast<size_t>(m) * k_pad;
+  R.gt_hi.alloc(elems);
+  R.gt_lo.alloc(elems);
+  R.gt2_hi.alloc(elems);
+  R.gt2_lo.alloc(elems);
+  R.gt_hi.zero(st);
+  R.gt_lo.zero(st);
+  R.gt2_hi.zero(st);
+  R.gt2_lo.zero(st);
+  RotEpiParams ep{};
+  ep.n = n;
+  ep.m = m;
+  ep.k_pad = k_pad;
+  ep.unscale = 1.0f / (kGcScale * 1024.0f);
+  output_scales(n, ep.s1, ep.s2);
+  ep.gt_hi = R.gt_hi.p;
+  ep.gt_lo = R.gt_lo.p;
+  ep.gt2_hi = R.gt2_hi.p;
+  ep.gt2_lo = R.gt2_lo.p;
+  if (m > 0) {
+    const __half* ah[1] = {qh.p};
+    const __half* al[1] = {ql.p};
+    const __half* bh[1] = {g.gc_hi.p};
+    const __half* bl[1] = {g.gc_lo.p};
+    const int bsel[1] = {0}, prod[1] = {7};
+    launch_tile_n<256, 1>(ctx, false, ep, ah, al, n, bh, bl, m, k_pad, bsel, prod);
+  }
+  R.m = m;
+  R.k_pad = k_pad;
+}
+
+// ------------------------------------------------------------------- REML
+struct LmmGenePrep {
+  int G = 0, p = 0;
+  DevBuf<double> Ytil, Xtil, delta, chi0, ainv, rss;
+};
+
+void lmm_prep(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p, LmmGenePrep& gp) {
+  EQTL_CHECK(ctx->have_basis && ctx->basis.n == n, EQTL_E_STATE, "LMM prep needs an eigenbasis of size n");
+  EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED, "the device LMM handles 1 <= p <= 16 covariate columns");
+  cudaStream_t st = ctx->stream;
+  cublasHandle_t h = blas_of(ctx);
+  gp.G = G;
+  gp.p = p;
+  DevBuf<double> dY, dX;
+  dY.upload(Y, static_cast<size_t>(n) * G, st);
+  dX.upload(X, static_cast<size_t>(n) * p, st);
+  gp.Ytil.alloc(static_cast<size_t>(n) * G);
+  gp.Xtil.alloc(static_cast<size_t>(n) * p);
+  const double one = 1.0, zero = 0.0;
+  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, dY.p, n, &zero, gp.Ytil.p, n) ==
+                 CUBLAS_STATUS_SUCCESS,
+             EQTL_E_CUDA, "Q'Y failed");
+  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, p, n, &one, ctx->basis.Q.p, n, dX.p, n, &zero, gp.Xtil.p, n) ==
+                 CUBLAS_STATUS_SUCCESS,
+             EQTL_E_CUDA, "Q'X failed");
+  gp.delta.alloc(G);
+  gp.chi0.alloc(static_cast<size_t>(G) * p);
+  gp.ainv.alloc(static_cast<size_t>(G) * p * p);
+  gp.rss.alloc(G);
+  const size_t smem = sizeof(double) * n;
+  EQTL_CHECK(smem <= 200 * 1024, EQTL_E_UNSUPPORTED, "REML kernel holds n doubles in shared memory (n <= 25600)");
+  EQTL_CUDA(cudaFuncSetAttribute(reml_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  ++ctx->launches;
+  reml_kernel<<<G, 256, smem, st>>>(gp.Ytil.p, gp.Xtil.p, ctx->basis.lambda.p, n, p, G, gp.delta.p, gp.chi0.p,
+                                    gp.ainv.p, gp.rss.p);
+  EQTL_CUDA(cudaGetLastError());
+  EQTL_CUDA(cudaStreamSynchronize(st));
+}
+
+// ------------------------------------------------------------------- scan
+template <int P>
+static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah, const __half* const* al,
+                       int G, bool simt) {
+  Rotated& R = ctx->rot;
+  const __half* bh[2] = {R.gt_hi.p, R.gt2_hi.p};
+  const __half* bl[2] = {R.gt_lo.p, R.gt2_lo.p};
+  int bsel[P + 2], prod[P + 2];
+  for (int j = 0; j < P + 2; ++j) {
+    bsel[j] = j == P + 1 ? 1 : 0;
+    prod[j] = 7;
+  }
+  if (!simt) {
+    launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod);
+    return;
+  }
+  // plain FP32 CUDA-core comparator
+  cudaStream_t st = ctx->stream;
+  const __half* ptrs[2 * (P + 2) + 4];
+  for (int j = 0; j < P + 2; ++j) {
+    ptrs[j] = ah[j];
+    ptrs[P + 2 + j] = al[j];
+  }
+  ptrs[2 * (P + 2) + 0] = bh[0];
+  ptrs[2 * (P + 2) + 1] = bh[1];
+  ptrs[2 * (P + 2) + 2] = bl[0];
+  ptrs[2 * (P + 2) + 3] = bl[1];
+  DevBuf<const __half*> dptr;
+  dptr.upload(ptrs, 2 * (P + 2) + 4, st);
+  TileShape sh{};
+  const int4 bs = make_int4(bsel[0], P + 2 > 1 ? bsel[1] : 0, P + 2 > 2 ? bsel[2] : 0, P + 2 > 3 ? bsel[3] : 0);
+  dim3 grid(static_cast<unsigned>((R.m + kSimtN - 1) / kSimtN), static_cast<unsigned>((G + 127) / 128));
+  ++ctx->launches;
+  simt_tile_kernel<P + 2, LmmEpi<P>><<<grid, 128, 0, st>>>(dptr.p, dptr.p + (P + 2), G, dptr.p + 2 * (P + 2),
+                                                           dptr.p + 2 * (P + 2) + 2, R.m, R.k_pad, bs, sh, ep);
+  EQTL_CUDA(cudaGetLastError());
+  EQTL_CUDA(cudaStreamSynchronize(st));
+}
+
+static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                                double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
+                                std::vector<eqtl_pair>& cands, bool simt) {
+  Geno& g = ctx->geno;
+  const int n = prm->n, G = prm->n_genes, p = prm->p;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_trans_lmm: no genotypes loaded");
+  EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lmm: n differs from the loaded genotypes");
+  EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_trans_lmm: no genes");
+  EQTL_CHECK(p >= 1 && p <= 2, EQTL_E_UNSUPPORTED,
+             "the tensor-core LMM scan handles 1 or 2 covariate columns (p + 2 <= 4 TMEM accumulators)");
+  cudaStream_t st = ctx->stream;
+  const double df = static_cast<double>(n - p - 1);
+  lmm_rotate(ctx);
+  LmmGenePrep gp;
+  std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
+  lmm_prep(ctx, Y, X, n, G, p, gp);
+
+  // gene-side operands
+  const int k_pad = g.k_pad;
+  const int nops = p + 2;
+  float s1, s2;
+  output_scales(n, s1, s2);
+  std::vector<DevBuf<__half>> opsh(nops), opsl(nops);
+  std::vector<__half*> ph(nops), pl(nops);
+  for (int k = 0; k < nops; ++k) {
+    opsh[k].alloc(static_cast<size_t>(G) * k_pad);
+    opsl[k].alloc(static_cast<size_t>(G) * k_pad);
+    ph[k] = opsh[k].p;
+    pl[k] = opsl[k].p;
+  }
+  DevBuf<__half*> dph, dpl;
+  dph.upload(ph.data(), nops, st);
+  dpl.upload(pl.data(), nops, st);
+  DevBuf<float> unscale;
+  unscale.alloc(static_cast<size_t>(G) * nops);
+  ++ctx->launches;
+  lmm_gene_ops_kernel<<<G, 256, 0, st>>>(gp.Ytil.p, gp.Xtil.p, ctx->basis.lambda.p, gp.delta.p, gp.chi0.p, n, p, G,
+                                         k_pad, s1, s2, dph.p, dpl.p, unscale.p);
+  EQTL_CUDA(cudaGetLastError());
+
+  const int64_t m = g.m;
+  DevBuf<uint8_t> ok;
+  ok.alloc(std::max<int64_t>(m, 1));
+  if (m > 0) {
+    ++ctx->launches;
+    snp_gate_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, st>>>(g.kept.p, m, n, g.mu.p, g.n_miss.p,
+                                                                            g.s1.p, g.s2.p, ok.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  ScanWindows wins;
+  upload_windows(ctx, prm, m, wins);
+  double t_cand = t_critical(prm->pthr, df);
+  if (prm->perm_thr > 0) t_cand = std::min(t_cand, t_critical(prm->perm_thr, df));
+  DeviceTTable tt(ctx, df);
+  prep_timer.reset();
+  ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
+  if (m > 0) {
+    const __half* ah[4] = {ph[0], ph[1], ph[2], nops > 3 ? ph[3] : ph[2]};
+    const __half* al[4] = {pl[0], pl[1], pl[2], nops > 3 ? pl[3] : pl[2]};
+    auto fill = [&](auto& ep) {
+      ep.G = G;
+      ep.m = m;
+      ep.unscale = unscale.p;
+      ep.ainv = gp.ainv.p;
+      ep.rss_null = gp.rss.p;
+      ep.snp_ok = ok.p;
+      ep.win = wins.view(prm->exclude_cis ? kWinExclude : kWinNone);
+      ep.df = static_cast<float>(df);
+      ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
+      ep.tt = tt.view();
+    };
+    if (p == 1) {
+      LmmEpiParams<1> ep{};
+      fill(ep);
+      so.run([&](GeneOut out) {
+        ep.out = out;
+        lmm_launch<1>(ctx, ep, ah, al, G, simt);
+      });
+    } else {
+      LmmEpiParams<2> ep{};
+      fill(ep);
+      so.run([&](GeneOut out) {
+        ep.out = out;
+        lmm_launch<2>(ctx, ep, ah, al, G, simt);
+      });
+    }
+  }
+  scan_timer.reset();
+  std::vector<int2> todo, deferred;
+  so.collect(genes, todo, deferred);
+
+  // ---- FP64 refinement: rotate raw dosages of the SNPs involved
+  StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
+  std::vector<double> delta_h(G), rss_h(G), chi0_h(static_cast<size_t>(G) * p), ainv_h(static_cast<size_t>(G) * p * p);
+  gp.delta.download(delta_h.data(), G, st);
+  gp.rss.download(rss_h.data(), G, st);
+  gp.chi0.download(chi0_h.data(), chi0_h.size(), st);
+  gp.ainv.download(ainv_h.data(), ainv_h.size(), st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  if (delta_out) std::copy(delta_h.begin(), delta_h.end(), delta_out);
+  std::vector<eqtl_pair> refined(todo.size());
+  if (!todo.empty()) {
+    std::vector<int> snps;
+    for (const int2& q : todo) snps.push_back(q.y);
+    std::sort(snps.begin(), snps.end());
+    snps.erase(std::unique(snps.begin(), snps.end()), snps.end());
+    std::vector<int> pcol(todo.size());
+    for (size_t i = 0; i < todo.size(); ++i)
+      pcol[i] = static_cast<int>(std::lower_bound(snps.begin(), snps.end(), todo[i].y) - snps.begin());
+    const int u = static_cast<int>(snps.size());
+    DevBuf<int> dsn, dpc;
+    DevBuf<int2> dtodo;
+    dsn.upload(snps.data(), u, st);
+    dpc.upload(pcol.data(), pcol.size(), st);
+    dtodo.upload(todo.data(), todo.size(), st);
+    DevBuf<double> graw, gt, outv;
+    graw.alloc(static_cast<size_t>(n) * u);
+    gt.alloc(static_cast<size_t>(n) * u);
+    ctx->launches += 2;
+    raw_dosage_kernel<<<1184, 256, 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dsn.p, u, graw.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_T, CUBLAS_OP_N, n, u, n, &one, ctx->basis.Q.p, n, graw.p, n, &zero,
+                           gt.p, n) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "Q'g failed");
+    outv.alloc(todo.size() * (p + 2));
+    lmm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
+        gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), gp.Ytil.p, gp.Xtil.p, p, ctx->basis.lambda.p,
+        gp.delta.p, outv.p);
+    EQTL_CUDA(cudaGetLastError());
+    std::vector<double> ov(todo.size() * (p + 2));
+    outv.download(ov.data(), ov.size(), st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < todo.size(); ++i) {
+      eqtl_pair& q = refined[i];
+      q.gene = todo[i].x;
+      q.snp = todo[i].y;
+      q.reserved = 0;
+      const double* o = &ov[i * (p + 2)];
+      lmm_stats_fp64(o[0], o[1], o + 2, &chi0_h[static_cast<size_t>(q.gene) * p],
+                     &ainv_h[static_cast<size_t>(q.gene) * p * p], rss_h[q.gene], p, df, q);
+    }
+  }
+  add_deferred_acat(genes, refined, deferred);
+  finish_scan(prm, genes, refined, pairs, cands);
+}
+
+void scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* delta_out,
+                    eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands) {
+  scan_trans_lmm_impl(ctx, prm, Y, X, delta_out, genes, pairs, cands, false);
+}
+
+void scan_trans_lmm_simt(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                         double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
+                         std::vector<eqtl_pair>& cands) {
+  scan_trans_lmm_impl(ctx, prm, Y, X, delta_out, genes, pairs, cands, true);
+}
+
+}  // namespace eqtl

@@ -24,6 +24,10 @@ void gene_yty(eqtl_ctx* ctx, const double* dY, int n, int G, std::vector<double>
 
 // FP64 hit_from_gty / test_lm arithmetic (src/scan_trans_lm.cpp:21-36).
 void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q);
+// FP64 bordered-Schur Wald test from gg, yg, a (test_lmm_gtil,
+// src/scan_trans_lmm.cpp:11-40); ainv = A00^-1 row-major p x p.
+void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv, double rss_null,
+                    int p, double df, eqtl_pair& q);
 
 // Splits refined pairs into the pair list (p <= pthr, sorted by snp then
 // gene) and stage-2 candidates (p < perm_thr, sorted by gene, p, snp), and
@@ -80,6 +84,14 @@ struct ScanOutputs {
 void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                        const std::vector<int2>& deferred);
 
+// Candidate-buffer size: three times the pairs expected under the null at the
+// larger of the two thresholds, at least 2^16.
+inline int64_t expected_candidates(const eqtl_scan_params* prm, int64_t m) {
+  const double thr = std::max(prm->pthr, prm->perm_thr);
+  const double e = 3.0 * static_cast<double>(m) * prm->n_genes * std::min(1.0, thr) + 65536.0;
+  return static_cast<int64_t>(std::min(e, static_cast<double>(1 << 26)));
+}
+
 void make_map_2d(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k_pad, uint32_t box_rows, bool bf16);
 int sm_count(eqtl_ctx* ctx);
 
@@ -91,7 +103,7 @@ template <int NT, int NACC, class EpiParams>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
-                   int n_tile_list = 0);
+                   int n_tile_list = 0, int ksplit = 1);
 
 }  // namespace eqtl
 
@@ -105,7 +117,7 @@ template <int NT, int NACC, class EpiParams>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
-                   int n_tile_list) {
+                   int n_tile_list, int ksplit) {
   using Epi = typename EpiOf<EpiParams>::type;
   using C = dev::TileCfg<NT, NACC>;
   dev::TileMaps maps;
@@ -136,11 +148,15 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
   sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
   sh.tile_list = tile_list;
-  sh.n_tiles = tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b;
+  sh.ksplit = tile_list ? 1 : std::max(1, std::min(ksplit, sh.kchunks));
+  sh.kc_per_split = (sh.kchunks + sh.ksplit - 1) / sh.ksplit;
+  sh.ksplit = (sh.kchunks + sh.kc_per_split - 1) / sh.kc_per_split;  // no empty ranges
+  sh.n_tiles = tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b * sh.ksplit;
   sh.status = ctx->d_status;
   if (sh.n_tiles == 0) return;
   EQTL_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
   const int grid = std::min(sh.n_tiles, sm_count(ctx));
+  ++ctx->launches;
   if (bf16) {
     auto kern = dev::tile_kernel<NT, NACC, 1u, Epi>;
     EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 
 #include "internal.hpp"
 #include "scan_common.cuh"
@@ -261,6 +262,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   const double df = static_cast<double>(n - p - 1);
 
   // ---- covariate algebra (host, p x p) and gene prep (device DGEMMs)
+  std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
   std::vector<double> XtXinv = xtx_inverse(X, n, p);
   DevBuf<double> dX, dXtXinv, dY, dXtY;
   dX.upload(X, static_cast<size_t>(n) * p, st);
@@ -278,6 +280,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   gscale.alloc(G);
   inv_yty.alloc(G);
   const bool bf16 = ctx->precision == EQTL_PREC_SPLIT_BF16;
+  ++ctx->launches;
   if (bf16)
     gene_split_kernel<__nv_bfloat16><<<G, 256, 0, st>>>(dY.p, n, k_pad, G, reinterpret_cast<__nv_bfloat16*>(a_hi.p),
                                                         reinterpret_cast<__nv_bfloat16*>(a_lo.p), gscale.p, inv_yty.p,
@@ -295,6 +298,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   af_sub.alloc(m);
   ok.alloc(m);
   if (m > 0) {
+    ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
         g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, dX.p, p, dXtXinv.p,
         gtg.p, inv_gtg.p, ok.p, af_sub.p);
@@ -311,7 +315,9 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   const float t_cand_f = static_cast<float>(t_cand * (1.0 - 1e-3));
   DeviceTTable tt(ctx, df);
 
-  ScanOutputs so(ctx, G, m, G);
+  prep_timer.reset();
+  ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   LmEpiParams ep{};
   ep.G = G;
   ep.m = m;
@@ -336,7 +342,9 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
     });
   }
 
+  scan_timer.reset();
   // ---- refine candidates + per-gene best in FP64
+  StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
   std::vector<int2> todo, deferred;
   so.collect(genes, todo, deferred);
   std::vector<double> gtg_h(m);
@@ -350,6 +358,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
     DevBuf<double> dg;
     dt.upload(todo.data(), todo.size(), st);
     dg.alloc(todo.size());
+    ++ctx->launches;
     lm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
         g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dY.p, dt.p, static_cast<int>(todo.size()), dg.p);
     EQTL_CUDA(cudaGetLastError());

@@ -45,7 +45,9 @@ struct TileShape {
   int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi
   int tiles_a;            // ceil(rows_a / 128)
   int tiles_b;            // ceil(rows_b / NT)
-  int n_tiles;            // tile work items (tiles_a * tiles_b unless a tile list is given)
+  int n_tiles;            // work items: tiles_a * tiles_b * ksplit, or the tile-list length
+  int ksplit;             // K ranges per output tile (split-K); 1 = whole K
+  int kc_per_split;       // K chunks per range
   const int2* tile_list;  // optional explicit (tile_a, tile_b) list (banded scans); null = dense
   uint32_t* status;       // device status word (DevStatus)
 };
@@ -67,15 +69,21 @@ struct TileCfg {
   static_assert(STAGES * STAGE_BYTES + 1024 + 256 <= 232448, "smem");
 };
 
-__device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta, int& tb) {
+// Work item t -> output tile (ta, tb) and its K-chunk range [k0, k1).
+__device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta, int& tb, int& k0, int& k1) {
+  int ks = 0;
   if (sh.tile_list) {
     const int2 c = sh.tile_list[t];
     ta = c.x;
     tb = c.y;
   } else {
-    tb = t / sh.tiles_a;
-    ta = t - tb * sh.tiles_a;
+    ks = t % sh.ksplit;
+    const int r = t / sh.ksplit;
+    tb = r / sh.tiles_a;
+    ta = r - tb * sh.tiles_a;
   }
+  k0 = ks * sh.kc_per_split;
+  k1 = min(sh.kchunks, k0 + sh.kc_per_split);
 }
 
 template <int NT, int NACC, uint32_t AB_FMT, class Epi>
@@ -132,12 +140,12 @@ __global__ void __launch_bounds__(192, 1)
       bool issued[6] = {false, false, false, false, false, false};
       bool ok = true;
       for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
-        int ta, tb;
-        tile_coords(sh, t, ta, tb);
+        int ta, tb, k0, k1;
+        tile_coords(sh, t, ta, tb, k0, k1);
         const int ra = ta * kTileM, rb = tb * NT;
         for (int j = 0; j < NACC && ok; ++j) {
           const int bp = sh.bsel[j];
-          for (int kc = 0; kc < sh.kchunks; ++kc) {
+          for (int kc = k0; kc < k1; ++kc) {
             if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
               ok = false;
               break;
@@ -180,13 +188,15 @@ __global__ void __launch_bounds__(192, 1)
       uint32_t accphase = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
+        int ta, tb, k0, k1;
+        tile_coords(sh, t, ta, tb, k0, k1);
         if (!mbar_wait(&acce[buf], accphase ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) break;
         tc_fence_after();
         const uint32_t dbase = tmem_base + static_cast<uint32_t>(buf * NACC * NT);
         for (int j = 0; j < NACC && ok; ++j) {
           const uint32_t d = dbase + static_cast<uint32_t>(j * NT);
           const int pm = sh.prod[j];
-          for (int kc = 0; kc < sh.kchunks; ++kc) {
+          for (int kc = k0; kc < k1; ++kc) {
             if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
               ok = false;
               break;
@@ -198,7 +208,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
             for (int k = 0; k < kChunkK / 16; ++k) {
               const uint32_t off = static_cast<uint32_t>(k * 32);
-              uint32_t accum = (kc > 0 || k > 0) ? 1u : 0u;
+              uint32_t accum = (kc > k0 || k > 0) ? 1u : 0u;
               if (pm & 1) {
                 umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
                 accum = 1u;
@@ -245,8 +255,8 @@ __global__ void __launch_bounds__(192, 1)
     int buf = 0;
     uint32_t accphase = 0;
     for (int t = blockIdx.x; t < sh.n_tiles; t += gridDim.x) {
-      int ta, tb;
-      tile_coords(sh, t, ta, tb);
+      int ta, tb, k0, k1;
+      tile_coords(sh, t, ta, tb, k0, k1);
       if (!mbar_wait(&accf[buf], accphase, status, abort_flag, kDevTimeoutAccFull)) break;
       tc_fence_after();
       const uint32_t tbase =

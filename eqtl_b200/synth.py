@@ -254,3 +254,75 @@ def write_gff(path: str, ids, chrom, start, end, strand) -> None:
         f.write("##gff-version 3\n")
         for i, c, s, e, st in zip(ids, chrom, start, end, strand):
             f.write(f"{c}\tsynth\tgene\t{int(s)}\t{int(e)}\t.\t{st}\t.\tID={i};Name={i}\n")
+
+
+def _fast_codes(rng: np.random.Generator, mc: int, n: int, family: Optional[tuple], maf_lo: float,
+                maf_hi: float, miss_rate: float) -> np.ndarray:
+    """Vectorised float32 sampler for the large shapes: [mc, n] int8 codes."""
+    af = rng.uniform(maf_lo, maf_hi, size=mc).astype(np.float32)
+    af = np.where(rng.random(mc) < 0.5, 1.0 - af, af).astype(np.float32)[:, None]
+    codes = np.empty((mc, n), dtype=np.int8)
+    col = 0
+    if family is not None:
+        n_fam, fam_size, n_unrel = family
+        # founder haplotypes [fam, parent, hap, snp] and the haplotype each
+        # sibling inherits from each parent
+        H = rng.random((n_fam, 2, 2, mc), dtype=np.float32) < af[None, None, None, :, 0]
+        pick = rng.random((n_fam, fam_size, 2, mc), dtype=np.float32) < 0.5
+        from_p = np.where(pick[:, :, 0], H[:, None, 0, 1], H[:, None, 0, 0])
+        from_m = np.where(pick[:, :, 1], H[:, None, 1, 1], H[:, None, 1, 0])
+        sib = (from_p.astype(np.int8) + from_m.astype(np.int8)).reshape(n_fam * fam_size, mc)
+        codes[:, : n_fam * fam_size] = sib.T
+        col = n_fam * fam_size
+    if col < n:
+        k = n - col
+        codes[:, col:] = ((rng.random((mc, k), dtype=np.float32) < af).astype(np.int8) +
+                          (rng.random((mc, k), dtype=np.float32) < af).astype(np.int8))
+    if miss_rate > 0:
+        codes[rng.random((mc, n), dtype=np.float32) < miss_rate] = -1
+    return codes
+
+
+def make_bed_rows_chunked(seed: int, n: int, m: int, *, family: Optional[tuple] = None, maf_lo: float = 0.01,
+                          maf_hi: float = 0.5, miss_rate: float = 0.01, chunk: int = 32768,
+                          keep_codes_every: int = 0) -> tuple:
+    """Packed .bed rows [m, ceil(n/4)] generated in SNP chunks (bounded host
+    memory for the large benchmark shapes). With family=(n_fam, fam_size,
+    n_unrel) siblings inherit founder alleles by Mendelian transmission.
+    Also returns int8 codes of every `keep_codes_every`-th SNP (for drawing
+    polygenic phenotypes) and their indices."""
+    rng = np.random.default_rng(seed)
+    nb = (n + 3) // 4
+    rows = np.empty((m, nb), dtype=np.uint8)
+    kept_codes, kept_idx = [], []
+    for s0 in range(0, m, chunk):
+        mc = min(chunk, m - s0)
+        codes = _fast_codes(rng, mc, n, family, maf_lo, maf_hi, miss_rate)
+        rows[s0:s0 + mc] = pack_bed_rows(codes)
+        if keep_codes_every:
+            sel = np.arange((-s0) % keep_codes_every, mc, keep_codes_every)
+            kept_codes.append(codes[sel])
+            kept_idx.append(s0 + sel)
+    if keep_codes_every:
+        return rows, np.concatenate(kept_codes), np.concatenate(kept_idx)
+    return rows, None, None
+
+
+def polygenic_pheno(seed: int, codes_sub: np.ndarray, n_genes: int, h2_max: float = 0.8) -> tuple:
+    """y = sqrt(h2) u + sqrt(1-h2) e, u ~ N(0, GRM of the given SNP subset)."""
+    rng = np.random.default_rng(seed)
+    d = imputed_dosage(codes_sub)
+    mu = d.mean(1, keepdims=True)
+    p = mu / 2.0
+    sd = np.sqrt(np.maximum(2 * p * (1 - p), 1e-12))
+    Z = ((d - mu) / sd).T
+    k = Z.shape[1]
+    n = Z.shape[0]
+    h2 = rng.uniform(0.0, h2_max, size=n_genes)
+    Y = np.empty((n, n_genes))
+    for g0 in range(0, n_genes, 2048):
+        g1 = min(n_genes, g0 + 2048)
+        u = Z @ rng.standard_normal((k, g1 - g0)) / np.sqrt(k)
+        e = rng.standard_normal((n, g1 - g0))
+        Y[:, g0:g1] = np.sqrt(h2[g0:g1])[None, :] * u + np.sqrt(1 - h2[g0:g1])[None, :] * e
+    return Y, h2

@@ -45,6 +45,16 @@ extern "C" {
 #define EQTL_PREC_SPLIT_BF16 1 /* operands as BF16 hi+lo pairs, 3 products */
 #define EQTL_PREC_FP32_SIMT 2  /* plain FP32 CUDA-core kernels (comparator) */
 
+/* Pipeline stages timed with CUDA events (eqtl_stage_ms). */
+#define EQTL_STAGE_DECODE 0 /* .bed decode + FP16 expansion */
+#define EQTL_STAGE_GRM 1    /* GRM contraction + division */
+#define EQTL_STAGE_EIGEN 2  /* eigendecomposition */
+#define EQTL_STAGE_ROTATE 3 /* spectral rotation of the genotypes */
+#define EQTL_STAGE_PREP 4   /* per-gene prep (residualisation / REML) */
+#define EQTL_STAGE_SCAN 5   /* tensor-core scan kernel (all launches of the call) */
+#define EQTL_STAGE_REFINE 6 /* FP64 refinement of candidate pairs */
+#define EQTL_N_STAGES 7
+
 typedef struct eqtl_ctx eqtl_ctx;
 
 /* ---------------------------------------------------------------- context */
@@ -52,6 +62,14 @@ int eqtl_open(int device, eqtl_ctx** out);
 void eqtl_close(eqtl_ctx* ctx);
 const char* eqtl_last_error(const eqtl_ctx* ctx);
 int eqtl_set_precision(eqtl_ctx* ctx, int precision);
+/* Device time (ms, CUDA events on the context's stream) of `stage` in the
+ * most recent call that ran it; EQTL_E_STATE if it has not run. */
+int eqtl_stage_ms(eqtl_ctx* ctx, int stage, double* ms);
+/* Number of kernels the library has launched on this context. */
+int eqtl_launch_count(eqtl_ctx* ctx, uint64_t* count);
+/* The cudaStream_t all work of this context is issued on (for callers that
+ * time or order their own work against it). */
+int eqtl_stream(eqtl_ctx* ctx, void** stream);
 
 /* ---------------------------------------------------------- genotype load
  * Replaces PlinkBed::decode_row + for_each_range_pos
@@ -112,6 +130,47 @@ typedef struct {
 int eqtl_scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                        eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap, int64_t* n_pairs,
                        eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
+
+/* --------------------------------------------------------------------- GRM
+ * Replaces compute_grm (src/grm.cpp:113-224) for the loaded genotypes and
+ * the analysis samples: K_out [n, n] (row-major, symmetric, FP64) and the
+ * per-pair non-missing marker counts N_packed_out [n(n+1)/2] (row-major
+ * lower triangle incl. diagonal, the .grm.N.bin order); m_used_out = SNPs
+ * used. Either output may be NULL. */
+int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out);
+
+/* ------------------------------------------------------------- eigenbasis
+ * Replaces make_lmm_basis (src/model_lmm.cpp:106-113): eigendecomposition of
+ * the GRM K [n, n] (row-major; NULL = compute the GRM of the loaded
+ * genotypes first) on the device, eigenvalues clipped at 0. The basis stays
+ * resident for the LMM scans. lambda_out [n] ascending and Q_out [n, n]
+ * (column j = eigenvector j) are optional. */
+int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out, double* Q_out);
+
+/* Installs an eigenbasis computed elsewhere (LmmBasis, include/eqtl/models.hpp
+ * :43-46). Eigenvector signs are arbitrary; statistics do not depend on
+ * them, but LMM permutations (which shuffle residuals in eigen-coordinates,
+ * include/eqtl/scan_cis.hpp:77-87) do, so supplying the reference's own basis
+ * reproduces its permutation p-values exactly. */
+int eqtl_lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int32_t n);
+
+/* Rotates the loaded genotypes into the eigenbasis, Gt = Q'(g - mean) for
+ * every kept SNP (the per-SNP g~ = Q'g of src/scan_trans_lmm.cpp:168, done
+ * once for all SNPs); eqtl_scan_trans_lmm reuses it while the genotypes and
+ * basis are unchanged, and runs it itself when needed. */
+int eqtl_lmm_rotate(eqtl_ctx* ctx);
+
+/* ----------------------------------------------------------- trans/gw LMM
+ * Replaces scan_lmm_snp_outer (src/scan_trans_lmm.cpp:82-251) on the
+ * shared-keep path, including prep_lmm's REML delta per gene
+ * (src/model_lmm.cpp:39-86,124-153) and the bordered-Schur Wald test per
+ * (SNP, gene) (src/scan_trans_lmm.cpp:11-40). Needs an eigenbasis of size n.
+ * delta_out [n_genes] (optional) receives each gene's REML delta. Outputs as
+ * for eqtl_scan_trans_lm. The tensor-core form handles p <= 2 covariate
+ * columns; EQTL_PREC_FP32_SIMT selects the plain FP32 CUDA-core form. */
+int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                        double* delta_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
+                        int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
 
 #ifdef __cplusplus
 }

@@ -53,3 +53,19 @@ def summarize(st, use, pthr, df):
             pairs[(int(s), g)] = {k2: float(st[k2][s, g]) for k2 in ("beta", "se", "stat", "p", "r2")}
     out["stats"] = st
     return out, pairs
+
+
+def trans_lmm(G_dos, Y, X, Q, lam, pthr, excl=None):
+    """SNP-outer LMM (src/scan_trans_lmm.cpp:82-251) over kept dosages."""
+    m, n = G_dos.shape
+    Gn = Y.shape[1]
+    p = X.shape[1]
+    preps = [R.prep_lmm(Y[:, g], X, Q, lam) for g in range(Gn)]
+    af, ok = R.subset_maf(G_dos)
+    Gt = G_dos @ Q
+    cols = [R.lmm_stats_gtil(pp, Gt) for pp in preps]
+    st = {k: np.stack([c[k] for c in cols], 1) for k in cols[0]}
+    use = ok[:, None] & (np.ones((m, Gn), bool) if excl is None else ~excl)
+    out, pairs = summarize(st, use, pthr, n - p - 1)
+    out["delta"] = np.array([pp.delta for pp in preps])
+    return out, pairs

@@ -41,7 +41,9 @@ def test_decode_bit_exact(ctx, miss_hand, max_miss, maf):
     assert np.array_equal(got, dec.dosage[k])               # bit-exact incl. imputed means
 
 
-def _check_scan(res, ora, pairs_ref, pthr, df, t_err=T_ERR):
+def _check_scan(res, ora, pairs_ref, pthr, df, t_err=T_ERR, rel=1e-9):
+    """rel: relative tolerance of the FP64-refined beta / t (1e-9 for LM; the
+    LMM's REML delta comes from a different FP64 optimiser run, ~1e-8)."""
     genes, pairs, _ = res
     assert np.array_equal(genes["n_tested"], ora["n_tested"])
     ap = acat_p_from(genes)
@@ -55,9 +57,9 @@ def _check_scan(res, ora, pairs_ref, pthr, df, t_err=T_ERR):
         assert abs(np.log10(pv) - np.log10(pthr)) < 1e-6, (k, pv)
     for k in set(got) & set(pairs_ref):
         q, r = got[k], pairs_ref[k]
-        assert abs(q["beta"] - r["beta"]) <= 1e-9 * abs(r["beta"]) + 1e-12
-        assert abs(q["t"] - r["stat"]) <= 1e-8 * abs(r["stat"]) + 1e-10
-        assert log10_diff(q["p"], r["p"]) < 1e-8
+        assert abs(q["beta"] - r["beta"]) <= rel * abs(r["beta"]) + 1e-12
+        assert abs(q["t"] - r["stat"]) <= 10 * rel * abs(r["stat"]) + 1e-10
+        assert log10_diff(q["p"], r["p"]) < max(1e-8, 100 * rel)
     # best SNP per gene: identical, or a near-tie in p
     for gi in range(len(genes)):
         if ora["best_snp"][gi] < 0:

@@ -1,0 +1,92 @@
+"""GPU parity: GRM, eigenbasis, batched REML and the trans/gw LMM scan through
+the C ABI against the numpy oracle."""
+import numpy as np
+import pytest
+
+import oracle_scan
+import restate as R
+from gpu_util import T_ERRS, acat_p_from, log10_diff
+from test_gpu_lm import _check_scan
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(seed=7, n=256, m=2000, G=96, ncov=0, miss=0.02, fam=(10, 6, 196)):
+    from eqtl_b200 import synth
+    g = synth.make_genotypes(seed, n=n, m=m, n_chrom=2, chrom_len=4_000_000, miss_rate=miss, maf_lo=0.02,
+                             family=fam)
+    Y, C, _ = synth.make_pheno_lmm(seed + 1, g, G, ncov, n_trans=30, beta_sd=0.5)
+    X = np.column_stack([np.ones(n), C]) if ncov else np.ones((n, 1))
+    return g, synth.pack_bed_rows(g.codes), Y, X
+
+
+@pytest.mark.parametrize("miss_hand", [1, 0])
+def test_grm_matches_oracle(miss_hand):
+    from eqtl_b200 import capi
+    g, rows, _, _ = _case(seed=3, m=1500)
+    n = g.codes.shape[1]
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n), miss_hand, 0.8, 0.0)
+        K, N, mu = c.grm()
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute" if miss_hand else "filter", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, Nr, mr = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    assert mu == mr
+    assert np.array_equal(N, Nr)                       # integer counts bit-exact
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=2e-6 * np.abs(Kr).max())
+    np.testing.assert_allclose(np.diag(K), np.diag(Kr), rtol=2e-6)
+
+
+def test_basis_eigenvalues():
+    from eqtl_b200 import capi
+    g, rows, _, _ = _case(seed=4, m=800)
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n))
+        lam, Q = c.lmm_basis(Kr)
+    lr, Qr = np.linalg.eigh(Kr)
+    lr = np.maximum(lr, 0)                             # make_lmm_basis clips at 0
+    np.testing.assert_allclose(lam, lr, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(Q.T @ Q, np.eye(n), atol=1e-10)
+    # sign-invariant: the clipped reconstruction Q diag(lambda) Q'
+    np.testing.assert_allclose((Q * lam) @ Q.T, (Qr * lr) @ Qr.T, atol=1e-9)
+
+
+@pytest.mark.parametrize("ncov,prec", [(0, 0), (1, 0), (0, 2)])
+def test_trans_lmm_matches_oracle(ncov, prec):
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(ncov=ncov)
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    with capi.Context(0, precision=prec) as c:
+        c.load_bed(rows, n, np.arange(n))
+        c.set_basis(Q, lam)
+        res = c.scan_trans_lmm(Y, X, pthr=1e-3)
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-3)
+    np.testing.assert_allclose(res[3], ora["delta"], rtol=1e-5)
+    _check_scan(res[:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
+
+
+def test_trans_lmm_device_basis_statistics():
+    """With the device's own eigenbasis (cuSOLVER signs) every statistic still
+    matches: only permutations depend on eigenvector signs."""
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(seed=17, G=64)
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n))
+        c.lmm_basis()                         # device GRM + cuSOLVER
+        res = c.scan_trans_lmm(Y, X, pthr=1e-3)
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-3)
+    np.testing.assert_allclose(res[3], ora["delta"], rtol=1e-4)
+    _check_scan(res[:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
