@@ -24,7 +24,7 @@ PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
 EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
-           "eqtl_stream"]
+           "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail"]
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
 
@@ -80,6 +80,8 @@ def load() -> C.CDLL:
         lib.eqtl_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
         lib.eqtl_lmm_rotate.argtypes = [vp]
         lib.eqtl_stream.argtypes = [vp, C.POINTER(vp)]
+        lib.eqtl_pheno_load.argtypes = [vp, vp, vp, i32, i32, i32]
+        lib.eqtl_t_tail.argtypes = [vp, dp, vp, i64, i32, vp, vp, vp]
         lib.eqtl_lmm_basis.argtypes = [vp, vp, i32, vp, vp]
         lib.eqtl_lmm_set_basis.argtypes = [vp, vp, vp, i32]
         lib.eqtl_scan_trans_lmm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, vp, i64, C.POINTER(i64),
@@ -175,11 +177,21 @@ class Context:
             prm.exclude_cis = 1 if exclude else 0
         return prm, keep
 
+    def pheno_load(self, Y, X):
+        """eqtl_pheno_load: keep Y [n, G] and X [n, p] resident on the device."""
+        Y = np.asfortranarray(Y, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        self._check(self.lib.eqtl_pheno_load(self.h, _ptr(Y), _ptr(X), Y.shape[0], Y.shape[1], X.shape[1]))
+        self.pheno_shape = (Y.shape[0], Y.shape[1], X.shape[1])
+
     def _scan(self, fn, Y, X, pthr, perm_thr, windows, extra=()):
-        Y = np.asfortranarray(Y, dtype=np.float64)   # [n, G] column-major
-        X = np.asfortranarray(X, dtype=np.float64)   # [n, p]
-        n, G = Y.shape
-        prm, keep = self._params(n, G, X.shape[1], pthr, perm_thr, windows)
+        if Y is None:
+            n, G, p = self.pheno_shape        # resident phenotypes
+        else:
+            Y = np.asfortranarray(Y, dtype=np.float64)   # [n, G] column-major
+            X = np.asfortranarray(X, dtype=np.float64)   # [n, p]
+            (n, G), p = Y.shape, X.shape[1]
+        prm, keep = self._params(n, G, p, pthr, perm_thr, windows)
         genes = np.zeros(G, GENE_DTYPE)
         cap = 1 << 16
         while True:
@@ -209,6 +221,16 @@ class Context:
         self._check(self.lib.eqtl_launch_count(self.h, C.byref(v)))
         return v.value
 
+    def t_tail(self, df: float, t, use_smem: bool = False):
+        """Device Student-t tail -> (-log10 p, ACAT term, flags)."""
+        t = np.ascontiguousarray(t, np.float32)
+        nl = np.zeros(t.size, np.float32)
+        term = np.zeros(t.size, np.float64)
+        fl = np.zeros(t.size, np.uint8)
+        self._check(self.lib.eqtl_t_tail(self.h, df, _ptr(t), t.size, 1 if use_smem else 0, _ptr(nl), _ptr(term),
+                                         _ptr(fl)))
+        return nl, term, fl
+
     def stream_ptr(self) -> int:
         v = C.c_void_p()
         self._check(self.lib.eqtl_stream(self.h, C.byref(v)))
@@ -225,14 +247,15 @@ class Context:
         self._check(self.lib.eqtl_grm(self.h, _ptr(K), _ptr(N), C.byref(mu)))
         return K, N, mu.value
 
-    def lmm_basis(self, K=None):
-        """eqtl_lmm_basis -> (lambda [n], Q [n, n] with eigenvectors as columns)."""
+    def lmm_basis(self, K=None, outputs=True):
+        """eqtl_lmm_basis -> (lambda [n], Q [n, n] with eigenvectors as columns);
+        with outputs=False the basis only stays resident and None is returned."""
         n = self.n if K is None else K.shape[0]
-        lam = np.zeros(n, np.float64)
-        Qc = np.zeros(n * n, np.float64)
+        lam = np.zeros(n, np.float64) if outputs else None
+        Qc = np.zeros(n * n, np.float64) if outputs else None
         Kc = None if K is None else np.ascontiguousarray(K, np.float64)
         self._check(self.lib.eqtl_lmm_basis(self.h, _ptr(Kc), n, _ptr(lam), _ptr(Qc)))
-        return lam, Qc.reshape(n, n).T
+        return (lam, Qc.reshape(n, n).T) if outputs else None
 
     def set_basis(self, Q, lam):
         """eqtl_lmm_set_basis with Q [n, n] (eigenvectors as columns)."""
@@ -242,7 +265,7 @@ class Context:
 
     def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None):
         """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta)."""
-        delta = np.zeros(np.asarray(Y).shape[1], np.float64)
+        delta = np.zeros(self.pheno_shape[1] if Y is None else np.asarray(Y).shape[1], np.float64)
         genes, pairs, cands = self._scan(self.lib.eqtl_scan_trans_lmm, Y, X, pthr, perm_thr, windows,
                                          extra=(_ptr(delta),))
         return genes, pairs, cands, delta

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <map>
 #include <mutex>
 
@@ -146,68 +147,7 @@ void residualize_genes(eqtl_ctx* ctx, const double* dX, const double* dXtXinv, i
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
-namespace {
-__global__ void col_sumsq_kernel(const double* Y, int n, int G, double* out) {
-  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (g >= G) return;
-  double s = 0;
-  for (int i = lane; i < n; i += 32) {
-    const double v = Y[static_cast<int64_t>(g) * n + i];
-    s += v * v;
-  }
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) out[g] = s;
-}
-}  // namespace
 
-void gene_yty(eqtl_ctx* ctx, const double* dY, int n, int G, std::vector<double>& yty) {
-  DevBuf<double> d;
-  d.alloc(G);
-  col_sumsq_kernel<<<(G + 7) / 8, 256, 0, ctx->stream>>>(dY, n, G, d.p);
-  EQTL_CUDA(cudaGetLastError());
-  yty.resize(G);
-  d.download(yty.data(), G, ctx->stream);
-  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
-}
-
-void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q) {
-  q.beta = q.se = q.t = q.r2 = 0.0;
-  q.p = 1.0;
-  if (gtg < 1e-12 || df <= 0) return;
-  q.beta = gty / gtg;
-  const double rss = yty - q.beta * gty;
-  const double s2 = std::max(rss / df, 0.0);
-  q.se = std::sqrt(s2 / gtg);
-  q.t = q.se > 0 ? q.beta / q.se : 0.0;
-  q.p = t_two_sided_p(q.t, df);
-  q.r2 = yty > 0 ? 1.0 - rss / yty : 0.0;
-}
-
-void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv, double rss_null,
-                    int p, double df, eqtl_pair& q) {
-  q.beta = q.se = q.t = q.r2 = 0.0;
-  q.p = 1.0;
-  if (gg < 1e-12) return;
-  double aTu = 0, aTchi = 0;
-  for (int x = 0; x < p; ++x) {
-    double ux = 0;
-    for (int y = 0; y < p; ++y) ux += ainv[x * p + y] * a[y];
-    aTu += a[x] * ux;
-    aTchi += a[x] * chi0[x];
-  }
-  const double S = gg - aTu;
-  if (S <= 1e-15) return;
-  const double bg = (yg - aTchi) / S;
-  double qq = rss_null - S * bg * bg;
-  if (qq < 0) qq = 0;
-  const double sigma2 = df > 0 ? qq / df : 1.0;
-  q.beta = bg;
-  q.se = std::sqrt(std::max(sigma2 / S, 0.0));
-  q.t = q.se > 0 ? q.beta / q.se : 0.0;
-  q.p = t_two_sided_p(q.t, df);
-  q.r2 = rss_null > 1e-15 ? std::max(0.0, 1.0 - qq / rss_null) : 0.0;
-}
 
 void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                  std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands) {
@@ -248,30 +188,43 @@ void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std
 
 void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                        const std::vector<int2>& deferred) {
-  if (deferred.empty()) return;
-  std::map<std::pair<int, int64_t>, double> pv;
-  for (const eqtl_pair& q : refined) pv[{q.gene, q.snp}] = q.p;
   const long double kPiL = 3.14159265358979323846L;
   for (const int2& d : deferred) {
-    auto it = pv.find({d.x, static_cast<int64_t>(d.y)});
-    EQTL_CHECK(it != pv.end(), EQTL_E_INTERNAL, "deferred ACAT pair was not refined");
-    double p = it->second;
+    auto it = std::lower_bound(refined.begin(), refined.end(), d, [](const eqtl_pair& q, const int2& k) {
+      return q.gene != k.x ? q.gene < k.x : q.snp < static_cast<int64_t>(k.y);
+    });
+    EQTL_CHECK(it != refined.end() && it->gene == d.x && it->snp == d.y, EQTL_E_INTERNAL,
+               "deferred ACAT pair was not refined");
+    double p = it->p;
     if (!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12) continue;  // AcatAcc::add guards
     if (p <= 0.0) p = 1e-300;
     genes[d.x].acat_tan_sum += static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+    ++genes[d.x].acat_used;
   }
 }
 
-void upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, ScanWindows& w) {
-  if (!prm->gene_chrom || !prm->gene_lo || !prm->gene_hi || !prm->snp_chrom || !prm->snp_pos) return;
-  w.gc.upload(prm->gene_chrom, prm->n_genes, ctx->stream);
-  w.glo.upload(prm->gene_lo, prm->n_genes, ctx->stream);
-  w.ghi.upload(prm->gene_hi, prm->n_genes, ctx->stream);
-  w.sc.upload(prm->snp_chrom, m, ctx->stream);
-  w.sp.upload(prm->snp_pos, m, ctx->stream);
+dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int mode) {
+  dev::Windows w{};
+  w.mode = dev::kWinNone;
+  if (mode == dev::kWinNone || !prm->gene_chrom || !prm->gene_lo || !prm->gene_hi || !prm->snp_chrom ||
+      !prm->snp_pos)
+    return w;
+  Workspace& ws = ctx->ws;
+  ws.win_gc.upload(prm->gene_chrom, prm->n_genes, ctx->stream);
+  ws.win_glo.upload(prm->gene_lo, prm->n_genes, ctx->stream);
+  ws.win_ghi.upload(prm->gene_hi, prm->n_genes, ctx->stream);
+  ws.win_sc.upload(prm->snp_chrom, m, ctx->stream);
+  ws.win_sp.upload(prm->snp_pos, m, ctx->stream);
+  w.mode = mode;
+  w.gene_chrom = ws.win_gc.p;
+  w.gene_lo = ws.win_glo.p;
+  w.gene_hi = ws.win_ghi.p;
+  w.snp_chrom = ws.win_sc.p;
+  w.snp_pos = ws.win_sp.p;
+  return w;
 }
 
-DeviceTTable::DeviceTTable(eqtl_ctx* ctx, double df) {
+dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
   EQTL_CHECK(df > 0, EQTL_E_ARG, "residual degrees of freedom must be positive");
   static std::mutex mu;
   static std::map<double, TTableHost> cache;
@@ -282,28 +235,82 @@ DeviceTTable::DeviceTTable(eqtl_ctx* ctx, double df) {
     if (it == cache.end()) it = cache.emplace(df, build_ttable(df)).first;
     T = it->second;
   }
-  h.upload(T.h.data(), T.h.size(), ctx->stream);
-  L.upload(T.L.data(), T.L.size(), ctx->stream);
-  t.h = h.p;
-  t.L = L.p;
+  Workspace& ws = ctx->ws;
+  if (ws.tt_df != df) {
+    ws.tt_h.upload(T.h.data(), T.h.size(), ctx->stream);
+    ws.tt_L.upload(T.L.data(), T.L.size(), ctx->stream);
+    ws.tt_df = df;
+  }
+  dev::TTable t{};
+  t.h = ws.tt_h.p;
+  t.L = ws.tt_L.p;
   t.t0 = static_cast<float>(T.t0);
   t.du_inv = static_cast<float>(T.na / (T.t0 * T.t0));
-  t.s0 = static_cast<float>(T.s0);
-  t.ds_inv = static_cast<float>(T.nb / (T.s_end - T.s0));
-  t.s_end = static_cast<float>(T.s_end);
+  t.x0 = static_cast<float>(T.x0);
+  t.dx_inv = static_cast<float>(T.nb / (T.x_end - T.x0));
+  t.x_end = static_cast<float>(T.x_end);
   t.inv_df = static_cast<float>(1.0 / df);
+  // deferral band around t = 0: 256 ulps of df in t^2 (the reference's
+  // x = df / (df + t^2) is quantised there) widened by 4x the screening
+  // error of t for this precision
+  static const double kTErr[3] = {2e-6, 6.4e-5, 2e-6};
+  const int prec = ctx->precision >= 0 && ctx->precision < 3 ? ctx->precision : 0;
+  const double ulp = std::nextafter(df, std::numeric_limits<double>::infinity()) - df;
+  t.tiny_t = static_cast<float>(std::sqrt(256.0 * ulp) + 4.0 * kTErr[prec]);
   t.na = T.na;
   t.nb = T.nb;
+  return t;
+}
+
+const PhenoDev& resolve_pheno(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X) {
+  PhenoDev& P = ctx->pheno;
+  if (Y || X) {
+    EQTL_CHECK(Y && X, EQTL_E_ARG, "give both Y and X, or neither to use the resident phenotypes");
+    pheno_load(ctx, Y, X, prm->n, prm->n_genes, prm->p);
+  }
+  EQTL_CHECK(P.Y.p && P.n == prm->n && P.G == prm->n_genes && P.p == prm->p, EQTL_E_STATE,
+             "no resident phenotypes of this shape (call eqtl_pheno_load or pass Y and X)");
+  return P;
+}
+
+void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p) {
+  EQTL_CHECK(n > 0 && G > 0 && p > 0, EQTL_E_ARG, "pheno_load: bad sizes");
+  PhenoDev& P = ctx->pheno;
+  P.n = n;
+  P.G = G;
+  P.p = p;
+  P.Y.upload(Y, static_cast<size_t>(n) * G, ctx->stream);
+  P.X.upload(X, static_cast<size_t>(n) * p, ctx->stream);
+  P.X_h.assign(X, X + static_cast<size_t>(n) * p);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
 namespace {
+__global__ void t_tail_kernel(dev::TTable T, const float* t, int64_t n, int use_smem, float* nl, double* term,
+                              uint8_t* flags) {
+  extern __shared__ float tsm[];
+  dev::TTable tt = T;
+  if (use_smem) {
+    tt = dev::ttable_to_smem(T, tsm, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const dev::TailOut o = dev::t_tail(t[i], tt);
+  nl[i] = o.neglog10p;
+  term[i] = o.term;
+  flags[i] = static_cast<uint8_t>((o.use_acat ? 1 : 0) | (o.deferred ? 2 : 0));
+}
+
 __global__ void fill_u64(unsigned long long* p, int n, unsigned long long v) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
 }
 }  // namespace
 
-ScanOutputs::ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint) : ctx(c), G(genes) {
+ScanOutputs::ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint)
+    : ctx(c), G(genes), acat(c->ws.acat), used(c->ws.used), tested(c->ws.tested), best(c->ws.best),
+      cand(c->ws.cand), count(c->ws.count) {
   acat.alloc(G);
   used.alloc(G);
   tested.alloc(G);
@@ -315,10 +322,10 @@ ScanOutputs::ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint) : 
 }
 
 void ScanOutputs::reset() {
-  acat.zero(ctx->stream);
-  used.zero(ctx->stream);
-  tested.zero(ctx->stream);
-  count.zero(ctx->stream);
+  EQTL_CUDA(cudaMemsetAsync(acat.p, 0, sizeof(double) * G, ctx->stream));
+  EQTL_CUDA(cudaMemsetAsync(used.p, 0, sizeof(int) * G, ctx->stream));
+  EQTL_CUDA(cudaMemsetAsync(tested.p, 0, sizeof(int) * G, ctx->stream));
+  EQTL_CUDA(cudaMemsetAsync(count.p, 0, sizeof(unsigned int), ctx->stream));
   fill_u64<<<(G + 255) / 256, 256, 0, ctx->stream>>>(best.p, G, ~0ull);
   EQTL_CUDA(cudaGetLastError());
 }
@@ -432,6 +439,7 @@ void eqtl_close(eqtl_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->cublas) cublasDestroy(static_cast<cublasHandle_t>(ctx->cublas));
+  eqtl::solver_release(ctx);
   if (ctx->d_status) cudaFree(ctx->d_status);
   for (int i = 0; i < EQTL_N_STAGES; ++i) {
     if (ctx->timer.start[i]) cudaEventDestroy(ctx->timer.start[i]);
@@ -509,6 +517,37 @@ int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
   });
 }
 
+int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use_smem, float* neglog10p,
+                double* term, uint8_t* flags) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(t && neglog10p && term && flags && n >= 0, EQTL_E_ARG, "null input");
+    if (n == 0) return;
+    const eqtl::dev::TTable T = eqtl::device_ttable(ctx, df);
+    eqtl::DevBuf<float> dt, dn;
+    eqtl::DevBuf<double> dterm;
+    eqtl::DevBuf<uint8_t> dfl;
+    dt.upload(t, n, ctx->stream);
+    dn.alloc(n);
+    dterm.alloc(n);
+    dfl.alloc(n);
+    ++ctx->launches;
+    eqtl::t_tail_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, use_smem ? eqtl::dev::kTTableSmemBytes : 0,
+                          ctx->stream>>>(T, dt.p, n, use_smem, dn.p, dterm.p, dfl.p);
+    EQTL_CUDA(cudaGetLastError());
+    dn.download(neglog10p, n, ctx->stream);
+    dterm.download(term, n, ctx->stream);
+    dfl.download(flags, n, ctx->stream);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, int32_t n_genes, int32_t p) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(Y && X, EQTL_E_ARG, "null input");
+    eqtl::pheno_load(ctx, Y, X, n, n_genes, p);
+  });
+}
+
 int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out) {
   return guarded(ctx, [&] {
     eqtl::DevBuf<double> K;
@@ -553,7 +592,7 @@ int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double
                         double* delta_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
                         int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {
   return guarded(ctx, [&] {
-    EQTL_CHECK(prm && Y && X && genes, EQTL_E_ARG, "null input");
+    EQTL_CHECK(prm && genes, EQTL_E_ARG, "null input");
     std::vector<eqtl_pair> pv, cv;
     if (ctx->precision == EQTL_PREC_FP32_SIMT)
       eqtl::scan_trans_lmm_simt(ctx, prm, Y, X, delta_out, genes, pv, cv);
@@ -572,7 +611,7 @@ int eqtl_scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double*
                        eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap, int64_t* n_pairs,
                        eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {
   return guarded(ctx, [&] {
-    EQTL_CHECK(prm && Y && X && genes, EQTL_E_ARG, "null input");
+    EQTL_CHECK(prm && genes, EQTL_E_ARG, "null input");
     EQTL_CHECK(ctx->precision != EQTL_PREC_FP32_SIMT, EQTL_E_UNSUPPORTED,
                "the FP32 CUDA-core comparator is available for the LMM scan only");
     std::vector<eqtl_pair> pv, cv;

@@ -133,6 +133,7 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   EQTL_CHECK(miss_hand == EQTL_MISS_FILTER || miss_hand == EQTL_MISS_IMPUTE, EQTL_E_ARG, "geno_load: miss_hand");
   Geno& g = ctx->geno;
   cudaStream_t st = ctx->stream;
+  ctx->rot.m = 0;  // rotated genotypes belong to the previous genotypes
   g.m_all = m;
   g.n = n;
   g.n_file = n_file;

@@ -95,7 +95,9 @@ struct GrmEpi {
   const Params& P;
   int row = 0;
   int64_t col0 = 0;
-  __device__ GrmEpi(const Params& p, const TileShape&) : P(p) {}
+  static constexpr int kSmemBytes = 0;
+  __device__ GrmEpi(const Params& p, const TileShape&, uint8_t*) : P(p) {}
+  __device__ void init(int, int) {}
   __device__ void begin_tile(int r, int64_t c0) {
     row = r;
     col0 = c0;
@@ -147,8 +149,10 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   const int n = g.n;
   const int64_t m = g.m;
   StageScope timer(ctx, EQTL_STAGE_GRM);
-  DevBuf<uint8_t> use;
-  DevBuf<double> mean, inv_sd;
+  Workspace& ws = ctx->ws;
+  DevBuf<uint8_t>& use = ws.grm_use;
+  DevBuf<double>& mean = ws.grm_mean;
+  DevBuf<double>& inv_sd = ws.grm_isd;
   use.alloc(std::max<int64_t>(m, 1));
   mean.alloc(std::max<int64_t>(m, 1));
   inv_sd.alloc(std::max<int64_t>(m, 1));
@@ -175,12 +179,15 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   const int64_t mu_n = static_cast<int64_t>(rows.size());
   EQTL_CHECK(mu_n > 0, EQTL_E_ARG, "no SNPs for GRM");
   const int64_t m_pad = ((mu_n + 63) / 64) * 64;
-  DevBuf<int64_t> drows;
-  DevBuf<double> dmean, disd;
+  DevBuf<int64_t>& drows = ws.grm_rows;
+  DevBuf<double>& dmean = ws.grm_mean_u;
+  DevBuf<double>& disd = ws.grm_isd_u;
   drows.upload(rows.data(), rows.size(), st);
   dmean.upload(mean_u.data(), mean_u.size(), st);
   disd.upload(isd_u.data(), isd_u.size(), st);
-  DevBuf<__half> zh, zl, mk;
+  DevBuf<__half>& zh = ws.grm_zh;
+  DevBuf<__half>& zl = ws.grm_zl;
+  DevBuf<__half>& mk = ws.grm_mk;
   const size_t elems = static_cast<size_t>(n) * m_pad;
   zh.alloc(elems);
   zl.alloc(elems);
@@ -192,8 +199,8 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
                                                         dmean.p, disd.p, zh.p, zl.p, mk.p);
     EQTL_CUDA(cudaGetLastError());
   }
-  DevBuf<double> A;
-  DevBuf<int> J;
+  DevBuf<double>& A = ws.grm_A;
+  DevBuf<int>& J = ws.grm_J;
   A.alloc(static_cast<size_t>(n) * n);
   J.alloc(static_cast<size_t>(n) * n);
   A.zero(st);

@@ -34,10 +34,14 @@ struct Error : std::runtime_error {
     if (!(cond)) throw ::eqtl::Error((code), (msg));        \
   } while (0)
 
+// Device buffer that keeps its allocation: alloc() only reallocates when
+// the requested count exceeds the capacity, so per-call workspaces held by
+// the context cost no cudaMalloc / cudaFree after the first call.
 template <class T>
 struct DevBuf {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -45,10 +49,13 @@ struct DevBuf {
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   void alloc(size_t count) {
-    if (count == n && p) return;
+    if (count <= cap && p) {
+      n = count;
+      return;
+    }
     release();
     if (count == 0) return;
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
@@ -57,7 +64,7 @@ struct DevBuf {
       throw Error(EQTL_E_NOMEM, "device allocation of " + std::to_string(count * sizeof(T)) +
                                     " bytes failed: " + cudaGetErrorString(e));
     }
-    n = count;
+    n = cap = count;
   }
   void zero(cudaStream_t s) {
     if (p) EQTL_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
@@ -101,6 +108,45 @@ struct Rotated {
   DevBuf<__half> gt_hi, gt_lo, gt2_hi, gt2_lo;
 };
 
+// Phenotypes / covariates resident on the device (eqtl_pheno_load).
+struct PhenoDev {
+  int n = 0, G = 0, p = 0;
+  DevBuf<double> Y;   // [G][n]
+  DevBuf<double> X;   // [p][n]
+  std::vector<double> X_h;
+};
+
+// Per-call workspaces reused across calls (capacity grows, never shrinks).
+struct Workspace {
+  DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
+  DevBuf<__half> ops_hi[4], ops_lo[4];
+  DevBuf<__half*> ops_ptr;
+  DevBuf<float> unscale, gscale;
+  DevBuf<uint8_t> ok;
+  DevBuf<double> graw, gt;
+  DevBuf<eqtl_pair> refined;
+  DevBuf<__half> q_hi, q_lo;  // rotation: split eigenvector operand
+  DevBuf<int> ref_snps, ref_col;
+  DevBuf<int2> ref_pairs;
+  // per-gene scan outputs + candidates
+  DevBuf<double> acat;
+  DevBuf<int> used, tested;
+  DevBuf<unsigned long long> best;
+  DevBuf<int2> cand;
+  DevBuf<unsigned int> count;
+  // windows
+  DevBuf<int32_t> win_gc, win_sc;
+  DevBuf<int64_t> win_glo, win_ghi, win_sp;
+  DevBuf<float> tt_h, tt_L;
+  double tt_df = -1;
+  // GRM operands and accumulators, eigen-solver scratch
+  DevBuf<uint8_t> grm_use;
+  DevBuf<double> grm_mean, grm_isd, grm_mean_u, grm_isd_u, grm_A, eig_work;
+  DevBuf<int64_t> grm_rows;
+  DevBuf<__half> grm_zh, grm_zl, grm_mk;
+  DevBuf<int> grm_J, eig_info;
+};
+
 struct LmmBasisDev {
   int n = 0;
   DevBuf<double> Q;        // [n, n] column-major (column j = eigenvector j)
@@ -126,10 +172,13 @@ struct eqtl_ctx {
   cudaStream_t stream = nullptr;
   uint32_t* d_status = nullptr;  // device status word of the last tile launch
   void* cublas = nullptr;        // cublasHandle_t
+  void* cusolver = nullptr;      // cusolverDnHandle_t
   std::string last_error;
   eqtl::Geno geno;
   eqtl::Rotated rot;
   eqtl::LmmBasisDev basis;
+  eqtl::PhenoDev pheno;
+  eqtl::Workspace ws;
   bool have_basis = false;
   int precision = EQTL_PREC_SPLIT_F16;
 };
@@ -144,6 +193,7 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
                const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min);
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
+void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p);
 
 // -- scan drivers
 void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
@@ -162,6 +212,7 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk);
 void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n);
 void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n);
 void lmm_rotate(eqtl_ctx* ctx);
+void solver_release(eqtl_ctx* ctx);
 
 // -- stage timing (capi.cu)
 void stage_begin(eqtl_ctx* ctx, int stage);

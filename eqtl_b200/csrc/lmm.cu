@@ -53,7 +53,9 @@ struct RotEpi {
   const Params& P;
   int row = 0;
   int64_t col0 = 0;
-  __device__ RotEpi(const Params& p, const TileShape&) : P(p) {}
+  static constexpr int kSmemBytes = 0;
+  __device__ RotEpi(const Params& p, const TileShape&, uint8_t*) : P(p) {}
+  __device__ void init(int, int) {}
   __device__ void begin_tile(int r, int64_t c0) {
     row = r;
     col0 = c0;
@@ -370,15 +372,22 @@ struct LmmEpiParams {
 template <int P>
 struct LmmEpi {
   using Params = LmmEpiParams<P>;
+  static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
+  float* tsm;
+  TTable tt;
   int gene = 0;
   int64_t snp0 = 0;
   bool gvalid = false;
-  double u[P + 2];
-  double ai[P][P];
-  double inv_rss = 0;
+  float u[P + 2];
+  float ai[P][P];
+  float inv_rss = 0;
   GeneAcc acc;
-  __device__ LmmEpi(const Params& p, const TileShape&) : Pr(p) {}
+  __device__ LmmEpi(const Params& p, const TileShape&, uint8_t* smem)
+      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+  __device__ void init(int tid, int nthr) {
+    if (tsm) tt = ttable_to_smem(Pr.tt, tsm, tid, nthr);
+  }
   __device__ void begin_tile(int g, int64_t s0) {
     gene = g;
     snp0 = s0;
@@ -390,44 +399,44 @@ struct LmmEpi {
 #pragma unroll
       for (int a = 0; a < P; ++a)
 #pragma unroll
-        for (int b = 0; b < P; ++b) ai[a][b] = Pr.ainv[(static_cast<int64_t>(g) * P + a) * P + b];
+        for (int b = 0; b < P; ++b) ai[a][b] = static_cast<float>(Pr.ainv[(static_cast<int64_t>(g) * P + a) * P + b]);
       const double r = Pr.rss_null[g];
-      inv_rss = r > 0 ? 1.0 / r : 0.0;
+      inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
       acc.load_window(Pr.win, g);
     }
   }
+  // Screening arithmetic in FP32 (the accumulators carry ~1e-7 relative
+  // error already); printed statistics come from the FP64 refinement. The
+  // 16 pairs of a chunk share one branch-free tail evaluation, so their
+  // table lookups overlap.
   template <int NACC>
   __device__ void chunk(int c, const float (&v)[NACC][16]) {
     static_assert(NACC == P + 2, "accumulators");
-    if (!gvalid) return;
-#pragma unroll 2
-    for (int j = 0; j < 16; ++j) {
-      const int64_t s = snp0 + c + j;
-      if (s >= Pr.m) break;
-      if (!__ldg(Pr.snp_ok + s)) continue;
-      if (!acc.in_scope(Pr.win, s)) continue;
-      const double num = static_cast<double>(v[0][j]) * u[0];
-      const double gg = static_cast<double>(v[P + 1][j]) * u[P + 1];
-      double S = gg;
-      double a[P];
+    const int64_t s0 = snp0 + c;
+    if (!gvalid || s0 >= Pr.m) return;
+    uint32_t okw[4];
+    load_flags16(Pr.snp_ok + s0, okw);
 #pragma unroll
-      for (int k = 0; k < P; ++k) a[k] = static_cast<double>(v[1 + k][j]) * u[1 + k];
+    for (int j = 0; j < 16; ++j) {
+      const int64_t s = s0 + j;
+      const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
+      const float num = v[0][j] * u[0];
+      const float gg = v[P + 1][j] * u[P + 1];
+      float S = gg;
+      float a[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * u[1 + k];
 #pragma unroll
       for (int x = 0; x < P; ++x)
 #pragma unroll
-        for (int y = 0; y < P; ++y) S -= a[x] * ai[x][y] * a[y];
-      float t = 0.0f;
-      if (!(gg < 1e-12) && S > 1e-15) {
-        const double r = num * num / S * inv_rss;
-        const double omr = 1.0 - r;
-        if (omr > 0.0) {
-          const float t2 = Pr.df * static_cast<float>(r) / static_cast<float>(omr);
-          t = copysignf(sqrtf(t2), static_cast<float>(num));
-        }
-      }
-      const TailOut o = t_tail(t, Pr.tt);
-      acc.add(o, s);
-      if (fabsf(t) >= Pr.t_cand || o.deferred) emit_candidate(Pr.out, gene, s, o.deferred);
+        for (int y = 0; y < P; ++y) S = fmaf(-a[x] * ai[x][y], a[y], S);
+      const float r = num * __fdividef(num, S) * inv_rss;
+      const float omr = 1.0f - r;
+      const bool ok_stat = !(gg < 1e-12f) && S > 1e-15f && omr > 0.0f;
+      const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
+      const TailOut o = t_tail(t, tt);
+      acc.add_masked(o, s, valid);
+      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred);
     }
   }
   __device__ void end_tile() {
@@ -472,10 +481,15 @@ __global__ void raw_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
 }
 
 // per refined pair: gg, yg, a[p] from FP64 rotated raw dosage
+// One warp per (gene, snp) pair from the FP64 rotated raw dosage Gt = Q'g:
+// gg = Gt'W Gt, yg = Gt'W y~, a = X~'W Gt with W = diag(1 / (delta lambda + 1)),
+// then the pair's printed statistics (test_lmm_gtil, src/scan_trans_lmm.cpp:11-40).
 __global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const int* __restrict__ pair_col,
                                   const int2* __restrict__ pairs, int n_pairs, const double* __restrict__ Ytil,
                                   const double* __restrict__ Xtil, int p, const double* __restrict__ lam,
-                                  const double* __restrict__ delta, double* out /* [n_pairs][p+2] */) {
+                                  const double* __restrict__ delta, const double* __restrict__ chi0,
+                                  const double* __restrict__ ainv, const double* __restrict__ rss, double df,
+                                  eqtl_pair* out) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= n_pairs) return;
@@ -499,10 +513,13 @@ __global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const in
     for (int k = 0; k < p; ++k) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
   }
   if (lane == 0) {
-    double* o = out + static_cast<int64_t>(w) * (p + 2);
-    o[0] = gg;
-    o[1] = yg;
-    for (int k = 0; k < p; ++k) o[2 + k] = a[k];
+    eqtl_pair q;
+    q.snp = pairs[w].y;
+    q.gene = g;
+    q.reserved = 0;
+    lmm_stats_fp64(gg, yg, a, chi0 + static_cast<int64_t>(g) * p, ainv + static_cast<int64_t>(g) * p * p, rss[g],
+                   p, df, q);
+    out[w] = q;
   }
 }
 
@@ -542,14 +559,18 @@ void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
   B.Q.alloc(static_cast<size_t>(n) * n);
   B.lambda.alloc(n);
   EQTL_CUDA(cudaMemcpyAsync(B.Q.p, K_dev, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st));
-  cusolverDnHandle_t h;
-  EQTL_CHECK(cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS, EQTL_E_CUDA, "cusolverDnCreate failed");
+  if (!ctx->cusolver) {
+    cusolverDnHandle_t hc;
+    EQTL_CHECK(cusolverDnCreate(&hc) == CUSOLVER_STATUS_SUCCESS, EQTL_E_CUDA, "cusolverDnCreate failed");
+    ctx->cusolver = hc;
+  }
+  cusolverDnHandle_t h = static_cast<cusolverDnHandle_t>(ctx->cusolver);
   cusolverDnSetStream(h, st);
   int lwork = 0;
   cusolverStatus_t cs = cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, B.Q.p, n,
                                                     B.lambda.p, &lwork);
-  DevBuf<double> work;
-  DevBuf<int> info;
+  DevBuf<double>& work = ctx->ws.eig_work;
+  DevBuf<int>& info = ctx->ws.eig_info;
   if (cs == CUSOLVER_STATUS_SUCCESS) {
     work.alloc(std::max(lwork, 1));
     info.alloc(1);
@@ -561,7 +582,6 @@ void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
     info.download(&info_h, 1, st);
     EQTL_CUDA(cudaStreamSynchronize(st));
   }
-  cusolverDnDestroy(h);
   EQTL_CHECK(cs == CUSOLVER_STATUS_SUCCESS && info_h == 0, EQTL_E_CUDA, "GRM eigen decomposition failed");
   B.lambda_h.resize(n);
   B.lambda.download(B.lambda_h.data(), n, st);
@@ -571,6 +591,11 @@ void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
   B.Q_h.clear();
   ctx->have_basis = true;
   ctx->rot.m = 0;  // rotated genotypes belong to the previous basis
+}
+
+void solver_release(eqtl_ctx* ctx) {
+  if (ctx->cusolver) cusolverDnDestroy(static_cast<cusolverDnHandle_t>(ctx->cusolver));
+  ctx->cusolver = nullptr;
 }
 
 void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n) {
@@ -603,7 +628,8 @@ void lmm_rotate(eqtl_ctx* ctx) {
   StageScope timer(ctx, EQTL_STAGE_ROTATE);
   const int n = g.n, k_pad = g.k_pad;
   const int64_t m = g.m;
-  DevBuf<__half> qh, ql;
+  DevBuf<__half>& qh = ctx->ws.q_hi;
+  DevBuf<__half>& ql = ctx->ws.q_lo;
   ++ctx->launches;
   qh.alloc(static_cast<size_t>(n) * k_pad);
   ql.alloc(static_cast<size_t>(n) * k_pad);
@@ -641,42 +667,35 @@ void lmm_rotate(eqtl_ctx* ctx) {
 }
 
 // ------------------------------------------------------------------- REML
-struct LmmGenePrep {
-  int G = 0, p = 0;
-  DevBuf<double> Ytil, Xtil, delta, chi0, ainv, rss;
-};
-
-void lmm_prep(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p, LmmGenePrep& gp) {
+// Per-gene REML prep into the context workspace (ws.Ytil, Xtil, delta, chi0,
+// ainv, rss) from the resident phenotypes.
+void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph) {
+  const int n = ph.n, G = ph.G, p = ph.p;
   EQTL_CHECK(ctx->have_basis && ctx->basis.n == n, EQTL_E_STATE, "LMM prep needs an eigenbasis of size n");
   EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED, "the device LMM handles 1 <= p <= 16 covariate columns");
   cudaStream_t st = ctx->stream;
+  Workspace& ws = ctx->ws;
   cublasHandle_t h = blas_of(ctx);
-  gp.G = G;
-  gp.p = p;
-  DevBuf<double> dY, dX;
-  dY.upload(Y, static_cast<size_t>(n) * G, st);
-  dX.upload(X, static_cast<size_t>(n) * p, st);
-  gp.Ytil.alloc(static_cast<size_t>(n) * G);
-  gp.Xtil.alloc(static_cast<size_t>(n) * p);
+  ws.Ytil.alloc(static_cast<size_t>(n) * G);
+  ws.Xtil.alloc(static_cast<size_t>(n) * p);
   const double one = 1.0, zero = 0.0;
-  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, dY.p, n, &zero, gp.Ytil.p, n) ==
-                 CUBLAS_STATUS_SUCCESS,
+  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ph.Y.p, n, &zero, ws.Ytil.p,
+                         n) == CUBLAS_STATUS_SUCCESS,
              EQTL_E_CUDA, "Q'Y failed");
-  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, p, n, &one, ctx->basis.Q.p, n, dX.p, n, &zero, gp.Xtil.p, n) ==
-                 CUBLAS_STATUS_SUCCESS,
+  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, p, n, &one, ctx->basis.Q.p, n, ph.X.p, n, &zero, ws.Xtil.p,
+                         n) == CUBLAS_STATUS_SUCCESS,
              EQTL_E_CUDA, "Q'X failed");
-  gp.delta.alloc(G);
-  gp.chi0.alloc(static_cast<size_t>(G) * p);
-  gp.ainv.alloc(static_cast<size_t>(G) * p * p);
-  gp.rss.alloc(G);
+  ws.delta.alloc(G);
+  ws.chi0.alloc(static_cast<size_t>(G) * p);
+  ws.ainv.alloc(static_cast<size_t>(G) * p * p);
+  ws.rss.alloc(G);
   const size_t smem = sizeof(double) * n;
   EQTL_CHECK(smem <= 200 * 1024, EQTL_E_UNSUPPORTED, "REML kernel holds n doubles in shared memory (n <= 25600)");
   EQTL_CUDA(cudaFuncSetAttribute(reml_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   ++ctx->launches;
-  reml_kernel<<<G, 256, smem, st>>>(gp.Ytil.p, gp.Xtil.p, ctx->basis.lambda.p, n, p, G, gp.delta.p, gp.chi0.p,
-                                    gp.ainv.p, gp.rss.p);
+  reml_kernel<<<G, 256, smem, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, n, p, G, ws.delta.p, ws.chi0.p,
+                                    ws.ainv.p, ws.rss.p);
   EQTL_CUDA(cudaGetLastError());
-  EQTL_CUDA(cudaStreamSynchronize(st));
 }
 
 // ------------------------------------------------------------------- scan
@@ -722,6 +741,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
                                 double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
                                 std::vector<eqtl_pair>& cands, bool simt) {
   Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
   const int n = prm->n, G = prm->n_genes, p = prm->p;
   EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_trans_lmm: no genotypes loaded");
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lmm: n differs from the loaded genotypes");
@@ -730,65 +750,62 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
              "the tensor-core LMM scan handles 1 or 2 covariate columns (p + 2 <= 4 TMEM accumulators)");
   cudaStream_t st = ctx->stream;
   const double df = static_cast<double>(n - p - 1);
+  const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
   lmm_rotate(ctx);
-  LmmGenePrep gp;
   std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
-  lmm_prep(ctx, Y, X, n, G, p, gp);
+  lmm_prep(ctx, ph);
 
   // gene-side operands
   const int k_pad = g.k_pad;
   const int nops = p + 2;
   float s1, s2;
   output_scales(n, s1, s2);
-  std::vector<DevBuf<__half>> opsh(nops), opsl(nops);
-  std::vector<__half*> ph(nops), pl(nops);
+  std::vector<__half*> oph(2 * nops);
   for (int k = 0; k < nops; ++k) {
-    opsh[k].alloc(static_cast<size_t>(G) * k_pad);
-    opsl[k].alloc(static_cast<size_t>(G) * k_pad);
-    ph[k] = opsh[k].p;
-    pl[k] = opsl[k].p;
+    ws.ops_hi[k].alloc(static_cast<size_t>(G) * k_pad);
+    ws.ops_lo[k].alloc(static_cast<size_t>(G) * k_pad);
+    oph[k] = ws.ops_hi[k].p;
+    oph[nops + k] = ws.ops_lo[k].p;
   }
-  DevBuf<__half*> dph, dpl;
-  dph.upload(ph.data(), nops, st);
-  dpl.upload(pl.data(), nops, st);
-  DevBuf<float> unscale;
+  ws.ops_ptr.upload(oph.data(), oph.size(), st);
+  DevBuf<float>& unscale = ws.unscale;
   unscale.alloc(static_cast<size_t>(G) * nops);
   ++ctx->launches;
-  lmm_gene_ops_kernel<<<G, 256, 0, st>>>(gp.Ytil.p, gp.Xtil.p, ctx->basis.lambda.p, gp.delta.p, gp.chi0.p, n, p, G,
-                                         k_pad, s1, s2, dph.p, dpl.p, unscale.p);
+  lmm_gene_ops_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
+                                         k_pad, s1, s2, ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
   EQTL_CUDA(cudaGetLastError());
 
   const int64_t m = g.m;
-  DevBuf<uint8_t> ok;
-  ok.alloc(std::max<int64_t>(m, 1));
+  DevBuf<uint8_t>& ok = ws.ok;
+  ok.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));  // the epilogue reads 16 flags per chunk, up to the last tile's end
+  EQTL_CUDA(cudaMemsetAsync(ok.p, 0, ok.n, st));
   if (m > 0) {
     ++ctx->launches;
     snp_gate_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, st>>>(g.kept.p, m, n, g.mu.p, g.n_miss.p,
                                                                             g.s1.p, g.s2.p, ok.p);
     EQTL_CUDA(cudaGetLastError());
   }
-  ScanWindows wins;
-  upload_windows(ctx, prm, m, wins);
+  const Windows win = upload_windows(ctx, prm, m, prm->exclude_cis ? kWinExclude : kWinNone);
   double t_cand = t_critical(prm->pthr, df);
   if (prm->perm_thr > 0) t_cand = std::min(t_cand, t_critical(prm->perm_thr, df));
-  DeviceTTable tt(ctx, df);
+  const TTable tt = device_ttable(ctx, df);
   prep_timer.reset();
   ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
   std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   if (m > 0) {
-    const __half* ah[4] = {ph[0], ph[1], ph[2], nops > 3 ? ph[3] : ph[2]};
-    const __half* al[4] = {pl[0], pl[1], pl[2], nops > 3 ? pl[3] : pl[2]};
+    const __half* ah[4] = {oph[0], oph[1], oph[2], nops > 3 ? oph[3] : oph[2]};
+    const __half* al[4] = {oph[nops + 0], oph[nops + 1], oph[nops + 2], nops > 3 ? oph[nops + 3] : oph[nops + 2]};
     auto fill = [&](auto& ep) {
       ep.G = G;
       ep.m = m;
       ep.unscale = unscale.p;
-      ep.ainv = gp.ainv.p;
-      ep.rss_null = gp.rss.p;
+      ep.ainv = ws.ainv.p;
+      ep.rss_null = ws.rss.p;
       ep.snp_ok = ok.p;
-      ep.win = wins.view(prm->exclude_cis ? kWinExclude : kWinNone);
+      ep.win = win;
       ep.df = static_cast<float>(df);
       ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
-      ep.tt = tt.view();
+      ep.tt = tt;
     };
     if (p == 1) {
       LmmEpiParams<1> ep{};
@@ -812,16 +829,14 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
 
   // ---- FP64 refinement: rotate raw dosages of the SNPs involved
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
-  std::vector<double> delta_h(G), rss_h(G), chi0_h(static_cast<size_t>(G) * p), ainv_h(static_cast<size_t>(G) * p * p);
-  gp.delta.download(delta_h.data(), G, st);
-  gp.rss.download(rss_h.data(), G, st);
-  gp.chi0.download(chi0_h.data(), chi0_h.size(), st);
-  gp.ainv.download(ainv_h.data(), ainv_h.size(), st);
-  EQTL_CUDA(cudaStreamSynchronize(st));
-  if (delta_out) std::copy(delta_h.begin(), delta_h.end(), delta_out);
+  if (delta_out) {
+    ws.delta.download(delta_out, G, st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+  }
   std::vector<eqtl_pair> refined(todo.size());
   if (!todo.empty()) {
     std::vector<int> snps;
+    snps.reserve(todo.size());
     for (const int2& q : todo) snps.push_back(q.y);
     std::sort(snps.begin(), snps.end());
     snps.erase(std::unique(snps.begin(), snps.end()), snps.end());
@@ -829,12 +844,14 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     for (size_t i = 0; i < todo.size(); ++i)
       pcol[i] = static_cast<int>(std::lower_bound(snps.begin(), snps.end(), todo[i].y) - snps.begin());
     const int u = static_cast<int>(snps.size());
-    DevBuf<int> dsn, dpc;
-    DevBuf<int2> dtodo;
+    DevBuf<int>& dsn = ws.ref_snps;
+    DevBuf<int>& dpc = ws.ref_col;
+    DevBuf<int2>& dtodo = ws.ref_pairs;
     dsn.upload(snps.data(), u, st);
     dpc.upload(pcol.data(), pcol.size(), st);
     dtodo.upload(todo.data(), todo.size(), st);
-    DevBuf<double> graw, gt, outv;
+    DevBuf<double>& graw = ws.graw;
+    DevBuf<double>& gt = ws.gt;
     graw.alloc(static_cast<size_t>(n) * u);
     gt.alloc(static_cast<size_t>(n) * u);
     ctx->launches += 2;
@@ -844,23 +861,13 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_T, CUBLAS_OP_N, n, u, n, &one, ctx->basis.Q.p, n, graw.p, n, &zero,
                            gt.p, n) == CUBLAS_STATUS_SUCCESS,
                EQTL_E_CUDA, "Q'g failed");
-    outv.alloc(todo.size() * (p + 2));
+    ws.refined.alloc(todo.size());
     lmm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
-        gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), gp.Ytil.p, gp.Xtil.p, p, ctx->basis.lambda.p,
-        gp.delta.p, outv.p);
+        gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), ws.Ytil.p, ws.Xtil.p, p, ctx->basis.lambda.p,
+        ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p, df, ws.refined.p);
     EQTL_CUDA(cudaGetLastError());
-    std::vector<double> ov(todo.size() * (p + 2));
-    outv.download(ov.data(), ov.size(), st);
+    ws.refined.download(refined.data(), todo.size(), st);
     EQTL_CUDA(cudaStreamSynchronize(st));
-    for (size_t i = 0; i < todo.size(); ++i) {
-      eqtl_pair& q = refined[i];
-      q.gene = todo[i].x;
-      q.snp = todo[i].y;
-      q.reserved = 0;
-      const double* o = &ov[i * (p + 2)];
-      lmm_stats_fp64(o[0], o[1], o + 2, &chi0_h[static_cast<size_t>(q.gene) * p],
-                     &ainv_h[static_cast<size_t>(q.gene) * p * p], rss_h[q.gene], p, df, q);
-    }
   }
   add_deferred_acat(genes, refined, deferred);
   finish_scan(prm, genes, refined, pairs, cands);

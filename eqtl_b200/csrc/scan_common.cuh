@@ -61,6 +61,20 @@ struct GeneAcc {
                        __ldg(w.snp_pos + s) <= hi;
     return w.mode == kWinExclude ? !inwin : inwin;
   }
+  // Update for one (gene, SNP) pair; `valid` masks pairs outside the scan
+  // (SNP gate, window, padding). Kept as predicated branches: the
+  // select form `acat += u ? term : 0.0` produced zero sums on sm_100a.
+  __device__ __forceinline__ void add_masked(const TailOut& o, int64_t s, bool valid) {
+    if (valid) {
+      ++tested;
+      if (o.use_acat) {
+        acat += o.term;
+        ++used;
+      }
+      const unsigned long long k = best_key(o.neglog10p, static_cast<uint32_t>(s));
+      best = k < best ? k : best;
+    }
+  }
   __device__ __forceinline__ void add(const TailOut& o, int64_t s) {
     ++tested;
     if (o.use_acat) {
@@ -78,6 +92,20 @@ struct GeneAcc {
     atomicMin(out.best + g, best);
   }
 };
+
+__device__ __forceinline__ void named_barrier_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// 16 per-SNP flag bytes starting at a multiple of 16 (arrays padded to 16).
+__device__ __forceinline__ void load_flags16(const uint8_t* p, uint32_t (&w)[4]) {
+  const uint4 v = *reinterpret_cast<const uint4*>(p);
+  w[0] = v.x;
+  w[1] = v.y;
+  w[2] = v.z;
+  w[3] = v.w;
+}
+__device__ __forceinline__ bool flag16(const uint32_t (&w)[4], int j) { return (w[j >> 2] >> (8 * (j & 3))) & 0xFFu; }
 
 __device__ __forceinline__ void emit_candidate(const GeneOut& out, int g, int64_t s, bool deferred) {
   const unsigned int idx = atomicAdd(out.cand_count, 1u);

@@ -20,14 +20,6 @@ std::vector<double> xtx_inverse(const double* X, int n, int p);  // (X'X)^-1, ro
 // Y[n, G] <- Y - X (XtXinv X'Y), on the device (cuBLAS DGEMM). XtY: scratch [p, G].
 void residualize_genes(eqtl_ctx* ctx, const double* dX, const double* dXtXinv, int n, int p, int G, double* dY,
                        double* dXtY);
-void gene_yty(eqtl_ctx* ctx, const double* dY, int n, int G, std::vector<double>& yty);
-
-// FP64 hit_from_gty / test_lm arithmetic (src/scan_trans_lm.cpp:21-36).
-void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q);
-// FP64 bordered-Schur Wald test from gg, yg, a (test_lmm_gtil,
-// src/scan_trans_lmm.cpp:11-40); ainv = A00^-1 row-major p x p.
-void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv, double rss_null,
-                    int p, double df, eqtl_pair& q);
 
 // Splits refined pairs into the pair list (p <= pthr, sorted by snp then
 // gene) and stage-2 candidates (p < perm_thr, sorted by gene, p, snp), and
@@ -35,38 +27,27 @@ void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, c
 void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                  std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands);
 
-struct ScanWindows {
-  DevBuf<int32_t> gc, sc;
-  DevBuf<int64_t> glo, ghi, sp;
-  dev::Windows view(int mode) const {
-    dev::Windows w;
-    w.mode = (gc.p && sc.p) ? mode : dev::kWinNone;
-    w.gene_chrom = gc.p;
-    w.gene_lo = glo.p;
-    w.gene_hi = ghi.p;
-    w.snp_chrom = sc.p;
-    w.snp_pos = sp.p;
-    return w;
-  }
-};
-void upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, ScanWindows& w);
+// Uploads the scan windows into the context workspace; returns the device
+// view (mode none when the caller gave no windows).
+dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int mode);
 
-struct DeviceTTable {
-  DevBuf<float> h, L;
-  dev::TTable t{};
-  DeviceTTable(eqtl_ctx* ctx, double df);
-  dev::TTable view() const { return t; }
-};
+// Device t-tail table for `df`, cached in the context workspace.
+dev::TTable device_ttable(eqtl_ctx* ctx, double df);
 
-// Per-gene outputs of one scan launch + candidate buffer.
+// Resolves the phenotypes of a scan call: uploads (Y, X) when given,
+// otherwise checks the resident ones match the call's shape.
+const PhenoDev& resolve_pheno(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X);
+
+// Per-gene outputs of one scan launch + candidate buffer (context workspace).
 struct ScanOutputs {
   eqtl_ctx* ctx;
   int G;
-  DevBuf<double> acat;
-  DevBuf<int> used, tested;
-  DevBuf<unsigned long long> best;
-  DevBuf<int2> cand;
-  DevBuf<unsigned int> count;
+  DevBuf<double>& acat;
+  DevBuf<int>& used;
+  DevBuf<int>& tested;
+  DevBuf<unsigned long long>& best;
+  DevBuf<int2>& cand;
+  DevBuf<unsigned int>& count;
   unsigned int cap;
   unsigned int n_cand = 0;
   ScanOutputs(eqtl_ctx* c, int genes, int64_t m, int64_t cap_hint);
@@ -81,6 +62,8 @@ struct ScanOutputs {
 // Adds, for every deferred (gene, snp) pair, the reference's long-double ACAT
 // term tan((0.5L - p) pi_L) computed from the refined FP64 p
 // (src/stats_extra.cpp:16-22; p <= 0 -> 1e-300).
+// `refined` is sorted by (gene, snp), as ScanOutputs::collect orders the
+// pairs it hands to the refinement.
 void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                        const std::vector<int2>& deferred);
 
@@ -152,19 +135,27 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   sh.kc_per_split = (sh.kchunks + sh.ksplit - 1) / sh.ksplit;
   sh.ksplit = (sh.kchunks + sh.kc_per_split - 1) / sh.kc_per_split;  // no empty ranges
   sh.n_tiles = tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b * sh.ksplit;
+  // gene-side tiles per raster group: keep the group's A operands (hi+lo of
+  // every accumulator) within ~48 MB of L2
+  {
+    const double a_bytes = static_cast<double>(NACC) * 2.0 * dev::kTileM * k_pad * 2.0;
+    sh.group_a = std::max(1, std::min(sh.tiles_a, static_cast<int>(48e6 / a_bytes)));
+  }
   sh.status = ctx->d_status;
   if (sh.n_tiles == 0) return;
   EQTL_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
   const int grid = std::min(sh.n_tiles, sm_count(ctx));
   ++ctx->launches;
+  const int smem = C::SMEM_BYTES + Epi::kSmemBytes;
+  EQTL_CHECK(smem <= 232448, EQTL_E_INTERNAL, "tile kernel shared memory over the 227 KB limit");
   if (bf16) {
     auto kern = dev::tile_kernel<NT, NACC, 1u, Epi>;
-    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
-    kern<<<grid, 192, C::SMEM_BYTES, ctx->stream>>>(maps, sh, ep);
+    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<grid, dev::kTileThreads, smem, ctx->stream>>>(maps, sh, ep);
   } else {
     auto kern = dev::tile_kernel<NT, NACC, 0u, Epi>;
-    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
-    kern<<<grid, 192, C::SMEM_BYTES, ctx->stream>>>(maps, sh, ep);
+    EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<grid, dev::kTileThreads, smem, ctx->stream>>>(maps, sh, ep);
   }
   EQTL_CUDA(cudaGetLastError());
   check_tile_status(ctx, "tile kernel");

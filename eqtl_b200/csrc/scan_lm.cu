@@ -44,50 +44,54 @@ struct LmEpiParams {
 
 struct LmEpi {
   using Params = LmEpiParams;
+  static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& P;
+  float* tsm;
+  TTable tt;
   int gene = 0;
   int64_t snp0 = 0;
   bool gvalid = false;
-  double inv_yty = 0;
+  float inv_yty = 0;
   float gs = 0;
   GeneAcc acc;
 
-  __device__ LmEpi(const Params& p, const TileShape&) : P(p) {}
+  __device__ LmEpi(const Params& p, const TileShape&, uint8_t* smem)
+      : P(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+  __device__ void init(int tid, int nthr) {
+    if (tsm) tt = ttable_to_smem(P.tt, tsm, tid, nthr);
+  }
   __device__ void begin_tile(int g, int64_t s0) {
     gene = g;
     snp0 = s0;
     gvalid = g < P.G;
     acc.reset();
     if (gvalid) {
-      inv_yty = P.inv_yty[g];
+      inv_yty = static_cast<float>(P.inv_yty[g]);
       gs = P.gscale[g];
       acc.load_window(P.win, g);
     }
   }
+  // t^2 = df r / (1 - r), r = gty^2 / (gtg yty)  (hit_from_gty algebra),
+  // screened in FP32 without branches; printed statistics come from the
+  // FP64 refinement.
   template <int NACC>
   __device__ void chunk(int c, const float (&v)[NACC][16]) {
-    if (!gvalid) return;
-#pragma unroll 4
+    const int64_t s0 = snp0 + c;
+    if (!gvalid || s0 >= P.m) return;
+    uint32_t okw[4];
+    load_flags16(P.snp_ok + s0, okw);
+#pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const int64_t s = snp0 + c + j;
-      if (s >= P.m) break;
-      if (!__ldg(P.snp_ok + s)) continue;
-      if (!acc.in_scope(P.win, s)) continue;
-      const double ig = __ldg(P.inv_gtg + s);
-      float t = 0.0f;
-      if (ig > 0.0) {
-        // t^2 = df r / (1 - r), r = gty^2 / (gtg yty)  (hit_from_gty algebra)
-        const double num = static_cast<double>(v[0][j]) * gs;
-        const double r = num * num * ig * inv_yty;
-        const double omr = 1.0 - r;
-        if (omr > 0.0) {
-          const float t2 = P.df * static_cast<float>(r) / static_cast<float>(omr);
-          t = copysignf(sqrtf(t2), static_cast<float>(num));
-        }
-      }
-      const TailOut o = t_tail(t, P.tt);
-      acc.add(o, s);
-      if (fabsf(t) >= P.t_cand || o.deferred) emit_candidate(P.out, gene, s, o.deferred);
+      const int64_t s = s0 + j;
+      const bool valid = flag16(okw, j) && s < P.m && acc.in_scope(P.win, s);
+      const float ig = valid ? static_cast<float>(P.inv_gtg[s]) : 0.0f;
+      const float num = v[0][j] * gs;
+      const float r = num * num * ig * inv_yty;
+      const float omr = 1.0f - r;
+      const float t = (ig > 0.0f && omr > 0.0f) ? copysignf(sqrtf(P.df * __fdividef(r, omr)), num) : 0.0f;
+      const TailOut o = t_tail(t, tt);
+      acc.add_masked(o, s, valid);
+      if (valid && (fabsf(t) >= P.t_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred);
     }
   }
   __device__ void end_tile() {
@@ -100,7 +104,7 @@ struct LmEpi {
 // One block per gene: yty, power-of-two scale, FP16/BF16 hi/lo rows.
 template <class T>
 __global__ void gene_split_kernel(const double* __restrict__ Ys, int n, int k_pad, int G, T* hi, T* lo,
-                                  float* gscale, double* inv_yty, float snp_scale) {
+                                  float* gscale, double* yty_out, double* inv_yty, float snp_scale) {
   const int g = blockIdx.x;
   if (g >= G) return;
   const double* y = Ys + static_cast<int64_t>(g) * n;
@@ -153,6 +157,7 @@ __global__ void gene_split_kernel(const double* __restrict__ Ys, int n, int k_pa
   }
   if (threadIdx.x == 0) {
     gscale[g] = static_cast<float>(1.0 / (sc * snp_scale));
+    yty_out[g] = yty;
     inv_yty[g] = yty > 0 ? 1.0 / yty : 0.0;
   }
 }
@@ -220,10 +225,13 @@ __global__ void snp_gtg_kernel(const uint8_t* __restrict__ bed, int64_t bps, con
 }
 
 // One warp per pair: FP64 gty = sum_i (g_i - mu) y_s[i] (y_s sums to zero).
+// One warp per (gene, snp) pair: gty from the exact decoded dosage in FP64,
+// then the pair's printed statistics (hit_from_gty, src/scan_trans_lm.cpp:21-36).
 __global__ void lm_refine_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
                                  int n, const int64_t* __restrict__ kept, const double* __restrict__ mu,
-                                 const double* __restrict__ Ys, const int2* __restrict__ pairs, int n_pairs,
-                                 double* gty) {
+                                 const double* __restrict__ Ys, const double* __restrict__ gtg,
+                                 const double* __restrict__ yty, double df, const int2* __restrict__ pairs,
+                                 int n_pairs, eqtl_pair* out) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (w >= n_pairs) return;
@@ -239,7 +247,14 @@ __global__ void lm_refine_kernel(const uint8_t* __restrict__ bed, int64_t bps, c
     acc += gc * y[i];
   }
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) gty[w] = acc;
+  if (lane == 0) {
+    eqtl_pair q;
+    q.snp = pr.y;
+    q.gene = pr.x;
+    q.reserved = 0;
+    lm_stats_fp64(gtg[pr.y], acc, yty[pr.x], df, q);
+    out[w] = q;
+  }
 }
 
 }  // namespace dev
@@ -254,82 +269,77 @@ using namespace dev;
 void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands) {
   Geno& g = ctx->geno;
-  EQTL_CHECK(g.m_all > 0 || g.m == 0, EQTL_E_STATE, "scan_trans_lm: no genotypes loaded");
+  Workspace& ws = ctx->ws;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_trans_lm: no genotypes loaded");
   const int n = prm->n, G = prm->n_genes, p = prm->p;
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0 && p > 0 && p <= kMaxP, EQTL_E_ARG, "scan_trans_lm: need 1 <= p <= 32 and genes > 0");
   cudaStream_t st = ctx->stream;
   const double df = static_cast<double>(n - p - 1);
+  const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
 
   // ---- covariate algebra (host, p x p) and gene prep (device DGEMMs)
   std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
-  std::vector<double> XtXinv = xtx_inverse(X, n, p);
-  DevBuf<double> dX, dXtXinv, dY, dXtY;
-  dX.upload(X, static_cast<size_t>(n) * p, st);
-  dXtXinv.upload(XtXinv.data(), XtXinv.size(), st);
-  dY.upload(Y, static_cast<size_t>(n) * G, st);
-  dXtY.alloc(static_cast<size_t>(p) * G);
-  residualize_genes(ctx, dX.p, dXtXinv.p, n, p, G, dY.p, dXtY.p);  // dY <- Y_s
+  std::vector<double> XtXinv = xtx_inverse(ph.X_h.data(), n, p);
+  ws.XtXinv.upload(XtXinv.data(), XtXinv.size(), st);
+  ws.Ys.alloc(static_cast<size_t>(n) * G);
+  EQTL_CUDA(cudaMemcpyAsync(ws.Ys.p, ph.Y.p, sizeof(double) * n * G, cudaMemcpyDeviceToDevice, st));
+  ws.XtY.alloc(static_cast<size_t>(p) * G);
+  residualize_genes(ctx, ph.X.p, ws.XtXinv.p, n, p, G, ws.Ys.p, ws.XtY.p);  // Ys <- Y - X beta
 
   const int k_pad = g.k_pad;
-  DevBuf<__half> a_hi, a_lo;
+  DevBuf<__half>& a_hi = ws.ops_hi[0];
+  DevBuf<__half>& a_lo = ws.ops_lo[0];
   a_hi.alloc(static_cast<size_t>(G) * k_pad);
   a_lo.alloc(static_cast<size_t>(G) * k_pad);
-  DevBuf<float> gscale;
-  DevBuf<double> inv_yty;
-  gscale.alloc(G);
-  inv_yty.alloc(G);
+  ws.gscale.alloc(G);
+  ws.inv_yty.alloc(G);
+  ws.yty.alloc(G);
   const bool bf16 = ctx->precision == EQTL_PREC_SPLIT_BF16;
   ++ctx->launches;
   if (bf16)
-    gene_split_kernel<__nv_bfloat16><<<G, 256, 0, st>>>(dY.p, n, k_pad, G, reinterpret_cast<__nv_bfloat16*>(a_hi.p),
-                                                        reinterpret_cast<__nv_bfloat16*>(a_lo.p), gscale.p, inv_yty.p,
-                                                        kGcScale);
+    gene_split_kernel<__nv_bfloat16><<<G, 256, 0, st>>>(ws.Ys.p, n, k_pad, G,
+                                                        reinterpret_cast<__nv_bfloat16*>(a_hi.p),
+                                                        reinterpret_cast<__nv_bfloat16*>(a_lo.p), ws.gscale.p,
+                                                        ws.yty.p, ws.inv_yty.p, kGcScale);
   else
-    gene_split_kernel<__half><<<G, 256, 0, st>>>(dY.p, n, k_pad, G, a_hi.p, a_lo.p, gscale.p, inv_yty.p, kGcScale);
+    gene_split_kernel<__half><<<G, 256, 0, st>>>(ws.Ys.p, n, k_pad, G, a_hi.p, a_lo.p, ws.gscale.p, ws.yty.p,
+                                                 ws.inv_yty.p, kGcScale);
   EQTL_CUDA(cudaGetLastError());
 
   // ---- per-SNP FP64 residual sum of squares + subset gate
   const int64_t m = g.m;
-  DevBuf<double> gtg, inv_gtg, af_sub;
-  DevBuf<uint8_t> ok;
-  gtg.alloc(m);
-  inv_gtg.alloc(m);
-  af_sub.alloc(m);
-  ok.alloc(m);
+  ws.gtg.alloc(std::max<int64_t>(m, 1));
+  ws.inv_gtg.alloc(std::max<int64_t>(m, 1));
+  ws.af_sub.alloc(std::max<int64_t>(m, 1));
+  ws.ok.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));  // the epilogue reads 16 flags per chunk, up to the last tile's end
+  EQTL_CUDA(cudaMemsetAsync(ws.ok.p, 0, ws.ok.n, st));
   if (m > 0) {
     ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, dX.p, p, dXtXinv.p,
-        gtg.p, inv_gtg.p, ok.p, af_sub.p);
+        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
     EQTL_CUDA(cudaGetLastError());
   }
 
-  // ---- windows
-  ScanWindows wins;
-  upload_windows(ctx, prm, m, wins);
-
-  // ---- thresholds and t table
+  // ---- thresholds, windows and t table
   double t_cand = t_critical(prm->pthr, df);
   if (prm->perm_thr > 0) t_cand = std::min(t_cand, t_critical(prm->perm_thr, df));
-  const float t_cand_f = static_cast<float>(t_cand * (1.0 - 1e-3));
-  DeviceTTable tt(ctx, df);
-
-  prep_timer.reset();
-  ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
-  std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   LmEpiParams ep{};
   ep.G = G;
   ep.m = m;
-  ep.inv_yty = inv_yty.p;
-  ep.gscale = gscale.p;
-  ep.inv_gtg = inv_gtg.p;
-  ep.snp_ok = ok.p;
-  ep.win = wins.view(prm->exclude_cis ? kWinExclude : kWinNone);
+  ep.inv_yty = ws.inv_yty.p;
+  ep.gscale = ws.gscale.p;
+  ep.inv_gtg = ws.inv_gtg.p;
+  ep.snp_ok = ws.ok.p;
+  ep.win = upload_windows(ctx, prm, m, prm->exclude_cis ? kWinExclude : kWinNone);
   ep.df = static_cast<float>(df);
-  ep.t_cand = t_cand_f;
-  ep.tt = tt.view();
+  ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
+  ep.tt = device_ttable(ctx, df);
+  prep_timer.reset();
 
+  ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   if (m > 0) {
     so.run([&](GeneOut out) {
       ep.out = out;
@@ -341,37 +351,23 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
       launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, G, bh, bl, m, k_pad, bsel, prod);
     });
   }
-
   scan_timer.reset();
+
   // ---- refine candidates + per-gene best in FP64
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
   std::vector<int2> todo, deferred;
   so.collect(genes, todo, deferred);
-  std::vector<double> gtg_h(m);
-  gtg.download(gtg_h.data(), m, st);
-  std::vector<double> yty_h(G);
-  gene_yty(ctx, dY.p, n, G, yty_h);
-  EQTL_CUDA(cudaStreamSynchronize(st));
-  std::vector<double> gty(todo.size());
+  std::vector<eqtl_pair> refined(todo.size());
   if (!todo.empty()) {
-    DevBuf<int2> dt;
-    DevBuf<double> dg;
-    dt.upload(todo.data(), todo.size(), st);
-    dg.alloc(todo.size());
+    ws.ref_pairs.upload(todo.data(), todo.size(), st);
+    ws.refined.alloc(todo.size());
     ++ctx->launches;
     lm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dY.p, dt.p, static_cast<int>(todo.size()), dg.p);
+        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, ws.Ys.p, ws.gtg.p, ws.yty.p, df, ws.ref_pairs.p,
+        static_cast<int>(todo.size()), ws.refined.p);
     EQTL_CUDA(cudaGetLastError());
-    dg.download(gty.data(), todo.size(), st);
+    ws.refined.download(refined.data(), todo.size(), st);
     EQTL_CUDA(cudaStreamSynchronize(st));
-  }
-  std::vector<eqtl_pair> refined(todo.size());
-  for (size_t i = 0; i < todo.size(); ++i) {
-    eqtl_pair& q = refined[i];
-    q.gene = todo[i].x;
-    q.snp = todo[i].y;
-    q.reserved = 0;
-    lm_stats_fp64(gtg_h[q.snp], gty[i], yty_h[q.gene], df, q);
   }
   add_deferred_acat(genes, refined, deferred);
   finish_scan(prm, genes, refined, pairs, cands);

@@ -4,7 +4,7 @@
 // fused multiply-adds on the CUDA cores instead of tcgen05.mma.
 //
 // Block = 128 threads = 128 gene rows x 16 SNP columns; K is staged through
-// shared memory in chunks of 32: the gene-side rows transposed so every
+// shared memory in chunks of 16: the gene-side rows transposed so every
 // thread reads its own row conflict-free, the SNP-side rows as broadcasts.
 #pragma once
 #include "tile_gemm.cuh"
@@ -72,7 +72,8 @@ __global__ void __launch_bounds__(128) simt_tile_kernel(const __half* const* __r
     }
     __syncthreads();
   }
-  Epi epi(ep, sh);
+  Epi epi(ep, sh, nullptr);
+  epi.init(tid, 128);
   epi.begin_tile(ga + tid, sb0);
   epi.template chunk<NACC>(0, acc);
   epi.end_tile();

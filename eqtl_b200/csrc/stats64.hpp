@@ -1,0 +1,113 @@
+// FP64 per-pair statistics, compiled for host and device alike, so the
+// refinement kernels print exactly what the host formulas give:
+//   * the two-sided Student-t p through the regularised incomplete beta
+//     function (Lentz's continued fraction with the reference's constants:
+//     maxit 200, eps 3e-12, fpmin 1e-30; src/util.cpp:209-264), including
+//     its x = df / (df + t^2) arithmetic, which gives p = 1 exactly where x
+//     rounds to 1;
+//   * the LM pair statistics of hit_from_gty (src/scan_trans_lm.cpp:21-36);
+//   * the LMM bordered-Schur Wald test from gg, yg, a (test_lmm_gtil,
+//     src/scan_trans_lmm.cpp:11-40).
+#pragma once
+#include <math.h>
+
+#include "../../include/eqtl_b200.h"
+
+#if defined(__CUDACC__)
+#define EQTL_HD __host__ __device__ __forceinline__
+#else
+#define EQTL_HD inline
+#endif
+
+namespace eqtl {
+
+EQTL_HD double incbeta_cf(double a, double b, double x) {
+  const int kMaxIt = 200;
+  const double kEps = 3e-12, kTiny = 1e-30;
+  const double qab = a + b, qap = a + 1.0, qam = a - 1.0;
+  double c = 1.0;
+  double d = 1.0 - qab * x / qap;
+  if (fabs(d) < kTiny) d = kTiny;
+  d = 1.0 / d;
+  double h = d;
+  for (int m = 1; m <= kMaxIt; ++m) {
+    const int m2 = 2 * m;
+    double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
+    d = 1.0 + aa * d;
+    if (fabs(d) < kTiny) d = kTiny;
+    c = 1.0 + aa / c;
+    if (fabs(c) < kTiny) c = kTiny;
+    d = 1.0 / d;
+    h *= d * c;
+    aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
+    d = 1.0 + aa * d;
+    if (fabs(d) < kTiny) d = kTiny;
+    c = 1.0 + aa / c;
+    if (fabs(c) < kTiny) c = kTiny;
+    d = 1.0 / d;
+    const double del = d * c;
+    h *= del;
+    if (fabs(del - 1.0) < kEps) break;
+  }
+  return h;
+}
+
+// I_x(a, b)
+EQTL_HD double incbeta(double a, double b, double x) {
+  if (x < 0 || x > 1) return NAN;
+  if (x == 0 || x == 1) return x;
+  const double lbeta = lgamma(a) + lgamma(b) - lgamma(a + b);
+  const double front = exp(log(x) * a + log(1 - x) * b - lbeta) / a;
+  if (x < (a + 1) / (a + b + 2)) return front * incbeta_cf(a, b, x);
+  return 1.0 - front * incbeta_cf(b, a, 1 - x) * a / b;
+}
+
+EQTL_HD double t_two_sided_p(double t, double df) {
+  if (!isfinite(t) || df <= 0) return 1.0;
+  const double x = df / (df + t * t);
+  const double p = incbeta(0.5 * df, 0.5, x);
+  return fmin(1.0, fmax(0.0, p));
+}
+
+// LM pair from gtg = |g_s|^2, gty = g_s . y_s, yty = |y_s|^2.
+EQTL_HD void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (gtg < 1e-12 || df <= 0) return;
+  q.beta = gty / gtg;
+  const double rss = yty - q.beta * gty;
+  const double s2 = fmax(rss / df, 0.0);
+  q.se = sqrt(s2 / gtg);
+  q.t = q.se > 0 ? q.beta / q.se : 0.0;
+  q.p = t_two_sided_p(q.t, df);
+  q.r2 = yty > 0 ? 1.0 - rss / yty : 0.0;
+}
+
+// LMM pair from gg = Gt'W Gt, yg = Gt'W y~, a = X~'W Gt and the gene's null
+// fit (chi0, ainv = (X~'W X~)^-1 row-major, rss_null).
+EQTL_HD void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv,
+                            double rss_null, int p, double df, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (gg < 1e-12) return;
+  double aTu = 0, aTchi = 0;
+  for (int x = 0; x < p; ++x) {
+    double ux = 0;
+    for (int y = 0; y < p; ++y) ux += ainv[x * p + y] * a[y];
+    aTu += a[x] * ux;
+    aTchi += a[x] * chi0[x];
+  }
+  const double S = gg - aTu;
+  if (S <= 1e-15) return;
+  const double bg = (yg - aTchi) / S;
+  double qq = rss_null - S * bg * bg;
+  if (qq < 0) qq = 0;
+  const double sigma2 = df > 0 ? qq / df : 1.0;
+  q.beta = bg;
+  q.se = sqrt(fmax(sigma2 / S, 0.0));
+  q.t = q.se > 0 ? q.beta / q.se : 0.0;
+  q.p = t_two_sided_p(q.t, df);
+  q.r2 = rss_null > 1e-15 ? fmax(0.0, 1.0 - qq / rss_null) : 0.0;
+}
+
+}  // namespace eqtl

@@ -3,7 +3,11 @@
 // Every scan of one keep-set has a single residual df, so the host tabulates
 // the two-sided p once (TTableHost, tstat.hpp) and the epilogue interpolates:
 //   |t| <= t0 : 1 - p = |t| h(t^2)        (h analytic; cubic Lagrange in u = t^2)
-//   |t| >  t0 : ln p  = L(s), s = log1p(t^2/df)   (cubic Lagrange in s)
+//   |t| >  t0 : ln p  = L(x), x = sqrt(log1p(t^2/df))   (cubic Lagrange in x;
+//               ln p is analytic in x: |t| ~ sqrt(df) x at the start of the
+//               range and ln p ~ -(df/2) x^2 far out, so the cubic is exact
+//               to FP32 rounding where a grid in s would meet a sqrt(s)
+//               singularity)
 // Node k of each table sits at (k-1) steps from the region start, so the
 // four nodes around any point in range exist. The result feeds
 //   * screening: -log10 p for the per-gene best key and threshold tests;
@@ -16,11 +20,16 @@
 namespace eqtl {
 namespace dev {
 
+constexpr int kTTableNa = 512;   // central intervals (TTableHost::na)
+constexpr int kTTableNb = 4096;  // tail intervals (TTableHost::nb)
+constexpr int kTTableSmemBytes = (kTTableNa + 4 + kTTableNb + 4) * 4;
+
 struct TTable {
   const float* h;  // na + 4 nodes
   const float* L;  // nb + 4 nodes
   float du_inv;    // na / t0^2
-  float s0, ds_inv, s_end;
+  float x0, dx_inv, x_end;  // tail grid in x = sqrt(log1p(t^2/df))
+  float tiny_t;             // 0 < |t| < tiny_t: deferred (see below)
   float inv_df;
   float t0;
   int na, nb;
@@ -31,8 +40,8 @@ __device__ __forceinline__ float lagrange4(const float* y, float x, int n_int) {
   x = fminf(fmaxf(x, 0.0f), static_cast<float>(n_int) - 1e-3f);
   const int i = static_cast<int>(x);
   const float f = x - static_cast<float>(i);
-  const float* q = y + i;  // q[0] = node i-1 (stored with +1 offset)
-  const float y0 = __ldg(q), y1 = __ldg(q + 1), y2 = __ldg(q + 2), y3 = __ldg(q + 3);
+  const float* q = y + i;  // q[0] = node i-1 (stored with +1 offset); global or shared
+  const float y0 = q[0], y1 = q[1], y2 = q[2], y3 = q[3];
   const float fm1 = f - 1.0f, fm2 = f - 2.0f, fp1 = f + 1.0f;
   const float w0 = -f * fm1 * fm2 * (1.0f / 6.0f);
   const float w1 = fp1 * fm1 * fm2 * 0.5f;
@@ -44,75 +53,70 @@ __device__ __forceinline__ float lagrange4(const float* y, float x, int n_int) {
 struct TailOut {
   float neglog10p;   // -log10 p (>= 0); capped where the FP64 reference p underflows
   double term;       // tan((1/2 - p) pi)
-  bool use_acat;     // p < 1 - 1e-12
-  bool deferred;     // p < 1e-14: term left to the host (see below)
+  bool use_acat;     // p < 1 - 1e-12 and not deferred: term added on the device
+  bool deferred;     // p < 1e-14 or 0 < |t| < tiny_t: left to the host (see below)
 };
 
 // The reference evaluates tan((0.5L - p) * pi) in 80-bit long double
 // (src/stats_extra.cpp:20). For tiny p that expression is quantised by the
 // long-double spacing near 0.5 (2^-65) and, below p ~ 2.7e-20, rounds to
-// tan(0.5L * pi_L), a huge NEGATIVE value because pi_L exceeds pi. To stay a
-// drop-in, the epilogue does not add terms for p < 1e-14; it counts them
-// in `used`, emits the pair as a flagged candidate, and the host adds the
-// reference's long-double term from the pair's FP64-refined p.
+// tan(0.5L * pi_L), a huge NEGATIVE value because pi_L exceeds pi.
+// At the other end, the reference's x = df / (df + t^2) (src/util.cpp:261)
+// rounds to exactly 1 for t^2 below half an ulp of df, so p = 1 and the pair
+// leaves ACAT, while just above it 1 - p is quantised by the ulp; the term
+// there is ~ -1 / (0.8 pi |t|), so the gene's ACAT hinges on it. To stay a
+// drop-in, the epilogue adds neither kind: it emits the pair as a flagged
+// candidate, and the host refines it in FP64 with the reference's
+// arithmetic and adds the long-double term (and its `used` count) when the
+// refined p enters ACAT. tiny_t = sqrt(256 ulp(df)) plus four times the
+// screening error of t, so every pair the reference quantises is caught.
 constexpr float kDeferNegLog10P = 14.0f;
 
 constexpr float kLn10 = 2.302585092994046f;
 constexpr double kPiD = 3.141592653589793;
 
+// One branch-free path for every lane (a warp's lanes are different genes,
+// so |t| straddles t0 within a warp): the lane picks its table, interpolates
+// once, and derives m = min(p, 1-p) with full relative precision (1-p from
+// the central table, p from the tail table), so tan((1/2-p) pi) =
+// +-cot(pi m) is one sincospi and one division.
 __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
   TailOut o;
-  o.deferred = false;
   const float at = fabsf(t);
-  if (!(at == at)) {  // NaN t: p = 1 (src/util.cpp:260)
-    o.neglog10p = 0.0f;
-    o.term = 0.0;
-    o.use_acat = false;
-    return o;
-  }
-  if (at <= T.t0) {
-    const float h = lagrange4(T.h, at * at * T.du_inv, T.na + 1);
-    const float q = at * h;  // 1 - p, accurate for tiny |t|
-    o.neglog10p = -log1pf(-q) * (1.0f / kLn10);
-    o.use_acat = q > 1e-12f;
-    if (q < 0.5f) {
-      // p > 1/2: tan((1/2-p) pi) = -cot(pi q)
-      float sq, cq;
-      sincospif(q, &sq, &cq);
-      o.term = -static_cast<double>(cq) / static_cast<double>(sq);
-    } else {
-      const float p = 1.0f - q;
-      float sp, cp;
-      sincospif(p, &sp, &cp);
-      o.term = static_cast<double>(cp) / static_cast<double>(sp);
-    }
-    return o;
-  }
-  const float s = log1pf(at * at * T.inv_df);
-  if (s >= T.s_end) {
-    // beyond the table: the FP64 reference p underflows to (near) zero
-    o.neglog10p = 323.3f;
-    o.term = 0.0;
-    o.use_acat = true;
-    o.deferred = true;
-    return o;
-  }
-  const float L = lagrange4(T.L, (s - T.s0) * T.ds_inv, T.nb + 1);
-  o.neglog10p = fminf(-L * (1.0f / kLn10), 323.3f);
-  o.use_acat = true;
-  if (o.neglog10p > kDeferNegLog10P) {
-    o.term = 0.0;
-    o.deferred = true;
-  } else if (L < -6.907755f) {  // p < 1e-3: cot(pi p) = 1/(pi p) - pi p / 3 - ...
-    double pd = exp(static_cast<double>(L));
-    pd = fmax(pd, 1e-300);
-    o.term = 1.0 / (kPiD * pd) - kPiD * pd / 3.0;
-  } else {
-    const float p = __expf(L);
-    float sp, cp;
-    sincospif(p, &sp, &cp);
-    o.term = static_cast<double>(cp) / static_cast<double>(sp);
-  }
+  const bool nan_t = !(at == at);
+  const bool central = at <= T.t0;
+  const float u = at * at;
+  const float xs = sqrtf(log1pf(u * T.inv_df));
+  const bool beyond = !central && xs >= T.x_end;
+  const float x = central ? u * T.du_inv : (xs - T.x0) * T.dx_inv;
+  const float y = lagrange4(central ? T.h : T.L, x, central ? T.na + 1 : T.nb + 1);
+  // central: y = h (1-p = |t| h); tail: y = ln p
+  const float q = at * y;
+  const float lnp = central ? log1pf(-q) : y;
+  const float p = central ? 1.0f - q : __expf(y);
+  const bool p_small = !central || q >= 0.5f;        // p <= 1/2: m = p
+  const float mm = p_small ? p : q;
+  float sm, cm;
+  sincospif(mm, &sm, &cm);
+  const float cot = __fdividef(cm, sm);
+  o.neglog10p = nan_t ? 0.0f : fminf(-lnp * (1.0f / kLn10), 323.3f);
+  const bool tiny = at > 0.0f && at < T.tiny_t;
+  o.deferred = !nan_t && (beyond || tiny || o.neglog10p > kDeferNegLog10P);
+  o.use_acat = !nan_t && !o.deferred && (central ? q > 1e-12f : true);
+  o.term = (nan_t || o.deferred || !o.use_acat) ? 0.0 : static_cast<double>(p_small ? cot : -cot);
+  if (beyond) o.neglog10p = 323.3f;
+  return o;
+}
+
+// Copies the table into shared memory (cooperatively, by `nthr` threads)
+// and returns a view of it; the caller synchronises before use.
+__device__ __forceinline__ TTable ttable_to_smem(const TTable& T, float* sm, int tid, int nthr) {
+  const int nh = T.na + 4, nl = T.nb + 4;
+  for (int i = tid; i < nh; i += nthr) sm[i] = T.h[i];
+  for (int i = tid; i < nl; i += nthr) sm[nh + i] = T.L[i];
+  TTable o = T;
+  o.h = sm;
+  o.L = sm + nh;
   return o;
 }
 

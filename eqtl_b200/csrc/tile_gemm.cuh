@@ -9,14 +9,16 @@
 // rounding). Both operands are K-major in global memory (row = gene or SNP,
 // K = sample index, zero-padded to a multiple of 64).
 //
-// Roles (192 threads):
+// Roles (64 + 32 * kEpiWarps threads):
 //   warp 0      TMA producer: one elected lane streams 64-wide K chunks of
 //               (A_hi, A_lo, B_hi, B_lo) into a STAGES-deep smem ring.
 //   warp 1      TMEM owner + MMA issuer: one elected lane issues
 //               tcgen05.mma (M=128, N=NT, K=16) into TMEM accumulators and
 //               releases ring slots with tcgen05.commit.
-//   warps 2..5  epilogue: each thread owns one accumulator row (TMEM lane),
-//               reads 16-column chunks with tcgen05.ld and hands them to the
+//   warps 2..    epilogue (kEpiWarps): each thread owns one accumulator row
+//               (TMEM lane; warp w may only read lane quarter w % 4, so the
+//               warps come in groups of four that split the columns), reads
+//               16-column chunks with tcgen05.ld and hands them to the
 //               scan-specific Epi functor, which never writes the M x N
 //               matrix to HBM.
 // When NACC*NT <= 256 the accumulators are double-buffered so the epilogue of
@@ -28,6 +30,8 @@ namespace eqtl {
 namespace dev {
 
 constexpr int kMaxAcc = 4;
+constexpr int kEpiWarps = 16;
+constexpr int kTileThreads = 64 + 32 * kEpiWarps;
 constexpr int kTileM = 128;
 constexpr int kChunkK = 64;  // 16-bit elements per K chunk (one 128-byte swizzle row)
 
@@ -47,6 +51,7 @@ struct TileShape {
   int tiles_b;            // ceil(rows_b / NT)
   int n_tiles;            // work items: tiles_a * tiles_b * ksplit, or the tile-list length
   int ksplit;             // K ranges per output tile (split-K); 1 = whole K
+  int group_a;            // gene-side tiles per raster group (L2 residency of the A operands)
   int kc_per_split;       // K chunks per range
   const int2* tile_list;  // optional explicit (tile_a, tile_b) list (banded scans); null = dense
   uint32_t* status;       // device status word (DevStatus)
@@ -77,17 +82,31 @@ __device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta,
     ta = c.x;
     tb = c.y;
   } else {
+    // Raster: groups of group_a gene-side tiles sweep every SNP-side tile, so
+    // the A operands of one group stay resident in L2 while B streams.
     ks = t % sh.ksplit;
     const int r = t / sh.ksplit;
-    tb = r / sh.tiles_a;
-    ta = r - tb * sh.tiles_a;
+    const int ga = sh.group_a;
+    const int full = (sh.tiles_a / ga) * ga;
+    const int in_full = full * sh.tiles_b;
+    if (r < in_full) {
+      const int grp = r / (ga * sh.tiles_b);
+      const int q = r - grp * ga * sh.tiles_b;
+      tb = q / ga;
+      ta = grp * ga + (q - tb * ga);
+    } else {
+      const int rem = sh.tiles_a - full;
+      const int q = r - in_full;
+      tb = q / rem;
+      ta = full + (q - tb * rem);
+    }
   }
   k0 = ks * sh.kc_per_split;
   k1 = min(sh.kchunks, k0 + sh.kc_per_split);
 }
 
 template <int NT, int NACC, uint32_t AB_FMT, class Epi>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kTileThreads, 1)
     tile_kernel(const __grid_constant__ TileMaps maps, const TileShape sh,
                 const __grid_constant__ typename Epi::Params ep) {
   using C = TileCfg<NT, NACC>;
@@ -100,6 +119,7 @@ __global__ void __launch_bounds__(192, 1)
   uint64_t* drain = acce + 2;          // [1]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile uint32_t* abort_flag = tmem_slot + 1;
+  uint8_t* epi_smem = smem + C::STAGES * C::STAGE_BYTES + 256;  // Epi::kSmemBytes of epilogue scratch
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -111,7 +131,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 128);
+      mbar_init(&acce[b], 32 * kEpiWarps);
     }
     mbar_init(drain, 1);
     *abort_flag = 0u;
@@ -251,7 +271,11 @@ __global__ void __launch_bounds__(192, 1)
     // ------------------------------------------------------------ epilogue
     const int quarter = warp & 3;  // TMEM lane quarter this warp may access
     const int row = quarter * 32 + lane;
-    Epi epi(ep, sh);
+    constexpr int kSub = kEpiWarps / 4;  // warps sharing a lane quarter
+    const int sub = (warp - 2) >> 2;     // this warp's share of the columns
+    Epi epi(ep, sh, Epi::kSmemBytes ? epi_smem : nullptr);
+    epi.init(threadIdx.x - 64, 32 * kEpiWarps);
+    asm volatile("bar.sync 1, %0;" ::"r"(32 * kEpiWarps) : "memory");
     int buf = 0;
     uint32_t accphase = 0;
     for (int t = blockIdx.x; t < sh.n_tiles; t += gridDim.x) {
@@ -263,7 +287,7 @@ __global__ void __launch_bounds__(192, 1)
           tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buf * NACC * NT);
       epi.begin_tile(ta * kTileM + row, tb * NT);
 #pragma unroll 1
-      for (int c = 0; c < NT; c += 16) {
+      for (int c = 16 * sub; c < NT; c += 16 * kSub) {
         float v[NACC][16];
 #pragma unroll
         for (int j = 0; j < NACC; ++j) tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v[j]);

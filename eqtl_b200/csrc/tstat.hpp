@@ -1,8 +1,6 @@
-// FP64 statistics shared by the host side of the library and the CLI:
-// Student-t two-sided p-value through the regularised incomplete beta
-// function (Lentz's continued fraction with the same constants as the
-// reference: maxit 200, eps 3e-12, fpmin 1e-30; src/util.cpp:209-264), and
-// the construction of the interpolation tables the device epilogues use to
+// Host-side statistics shared by the library and the CLI: the beta CDF and
+// t critical values on top of the FP64 tail in stats64.hpp, and the
+// construction of the interpolation tables the device epilogues use to
 // screen t statistics (see tdist.cuh).
 #pragma once
 #include <algorithm>
@@ -10,55 +8,9 @@
 #include <limits>
 #include <vector>
 
+#include "stats64.hpp"
+
 namespace eqtl {
-
-inline double incbeta_cf(double a, double b, double x) {
-  const int kMaxIt = 200;
-  const double kEps = 3e-12, kTiny = 1e-30;
-  const double qab = a + b, qap = a + 1.0, qam = a - 1.0;
-  double c = 1.0;
-  double d = 1.0 - qab * x / qap;
-  if (std::fabs(d) < kTiny) d = kTiny;
-  d = 1.0 / d;
-  double h = d;
-  for (int m = 1; m <= kMaxIt; ++m) {
-    const int m2 = 2 * m;
-    double aa = m * (b - m) * x / ((qam + m2) * (a + m2));
-    d = 1.0 + aa * d;
-    if (std::fabs(d) < kTiny) d = kTiny;
-    c = 1.0 + aa / c;
-    if (std::fabs(c) < kTiny) c = kTiny;
-    d = 1.0 / d;
-    h *= d * c;
-    aa = -(a + m) * (qab + m) * x / ((a + m2) * (qap + m2));
-    d = 1.0 + aa * d;
-    if (std::fabs(d) < kTiny) d = kTiny;
-    c = 1.0 + aa / c;
-    if (std::fabs(c) < kTiny) c = kTiny;
-    d = 1.0 / d;
-    const double del = d * c;
-    h *= del;
-    if (std::fabs(del - 1.0) < kEps) break;
-  }
-  return h;
-}
-
-// I_x(a, b)
-inline double incbeta(double a, double b, double x) {
-  if (x < 0 || x > 1) return std::numeric_limits<double>::quiet_NaN();
-  if (x == 0 || x == 1) return x;
-  const double lbeta = std::lgamma(a) + std::lgamma(b) - std::lgamma(a + b);
-  const double front = std::exp(std::log(x) * a + std::log(1 - x) * b - lbeta) / a;
-  if (x < (a + 1) / (a + b + 2)) return front * incbeta_cf(a, b, x);
-  return 1.0 - front * incbeta_cf(b, a, 1 - x) * a / b;
-}
-
-inline double t_two_sided_p(double t, double df) {
-  if (!std::isfinite(t) || df <= 0) return 1.0;
-  const double x = df / (df + t * t);
-  const double p = incbeta(0.5 * df, 0.5, x);
-  return std::min(1.0, std::max(0.0, p));
-}
 
 inline double beta_cdf(double x, double a, double b) {
   if (a <= 0 || b <= 0) return std::numeric_limits<double>::quiet_NaN();
@@ -86,10 +38,10 @@ struct TTableHost {
   double df = 0;
   double t0 = 1.0;               // central / tail boundary in |t|
   int na = 512;                  // central intervals over u = t^2 in [0, t0^2]
-  int nb = 4096;                 // tail intervals over s = log1p(t^2/df)
-  double s0 = 0, s_end = 0;
+  int nb = 4096;                 // tail intervals over x = sqrt(log1p(t^2/df)) in [x0, x_end]
+  double x0 = 0, x_end = 0;
   std::vector<float> h;          // na + 4 nodes: h(u) = (1 - p) / |t|, node k at u = (k-1) du
-  std::vector<float> L;          // nb + 4 nodes: ln p at s = s0 + (k-1) ds
+  std::vector<float> L;          // nb + 4 nodes: ln p at x = x0 + (k-1) dx
 };
 
 inline double t_density_const(double df) {
@@ -143,29 +95,38 @@ inline TTableHost build_ttable(double df) {
   const double du = (T.t0 * T.t0) / T.na;
   T.h.resize(T.na + 4);
   for (int k = 0; k < T.na + 4; ++k) T.h[k] = static_cast<float>(central_h((k - 1) * du, df));
-  T.s0 = std::log1p(T.t0 * T.t0 / df);
-  // s where ln p falls below ln(1e-320): beyond it the reference's p underflows.
-  double s_hi = T.s0 + 1.0;
-  auto lnp = [&](double s) {
-    const double t = std::sqrt(df * std::expm1(s));
+  T.x0 = std::sqrt(std::log1p(T.t0 * T.t0 / df));
+  auto lnp = [&](double x) {
+    const double t = std::sqrt(df * std::expm1(x * x));
     const double p = t_two_sided_p(t, df);
     return p > 0 ? std::log(p) : -1e30;
   };
-  while (lnp(s_hi) > std::log(1e-320) && s_hi < 1e4) s_hi = T.s0 + 2 * (s_hi - T.s0);
-  T.s_end = s_hi;
-  const double ds = (T.s_end - T.s0) / T.nb;
+  // x_end: where ln p reaches ln(1e-320) (beyond it the reference's p
+  // underflows), capped at |t| = 1e19, past which the FP32 t^2 of the
+  // epilogue overflows (small df). Pairs beyond x_end are deferred to the
+  // FP64 refinement. Bracket by doubling, then bisect so the nodes span
+  // only the range in use.
+  const double kLnFloor = std::log(1e-320);
+  const double x_cap = std::sqrt(std::log1p(1e38 / df));
+  if (lnp(x_cap) > kLnFloor) {
+    T.x_end = x_cap;
+  } else {
+    double lo = T.x0, hi = std::min(T.x0 + 1.0, x_cap);
+    while (lnp(hi) > kLnFloor) {
+      lo = hi;
+      hi = std::min(T.x0 + 2 * (hi - T.x0), x_cap);
+    }
+    for (int it = 0; it < 80; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      (lnp(mid) > kLnFloor ? lo : hi) = mid;
+    }
+    T.x_end = hi;
+  }
+  const double dx = (T.x_end - T.x0) / T.nb;
   T.L.resize(T.nb + 4);
   for (int k = 0; k < T.nb + 4; ++k) {
-    const double s = T.s0 + (k - 1) * ds;
-    double v;
-    if (s <= T.s0 - 0.5 * ds) {
-      // below the tail's first node: extend smoothly from the exact value
-      const double t = std::sqrt(std::max(df * std::expm1(s), 0.0));
-      v = std::log(t_two_sided_p(t, df));
-    } else {
-      v = lnp(s);
-      if (v < -1e29) v = T.L[k - 1] + (T.L[k - 1] - T.L[k - 2]);  // past underflow: extrapolate
-    }
+    double v = lnp(T.x0 + (k - 1) * dx);
+    if (v < -1e29) v = 2.0 * T.L[k - 1] - T.L[k - 2];  // past underflow: extrapolate
     T.L[k] = static_cast<float>(v);
   }
   return T;

@@ -88,6 +88,25 @@ int eqtl_geno_load_bed(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t by
  * [hi - lo, n] (SnpRec.dosage after src/plink_bed.cpp:298-302). */
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);
 
+/* Evaluates the Student-t tail the scan epilogues use (K8: the device form of
+ * p_from_t, src/util.cpp:259-264, through the df-specific interpolation
+ * table) for n values of t at residual df, on the device: -log10 p, the ACAT
+ * term tan((1/2 - p) pi) and flags (bit 0: term added on the device, bit 1:
+ * pair deferred to the host's FP64 / long-double path, for p < 1e-14 and for
+ * t within a few 1e-6 of 0 where the reference's p is quantised by the
+ * ulp of df). use_smem = 1 reads the table
+ * from shared memory as the scan kernels do. For validation. */
+int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use_smem, float* neglog10p,
+                double* term, uint8_t* flags);
+
+/* ------------------------------------------------------------- phenotypes
+ * Keeps the phenotype matrix Y [n, n_genes] (after the caller's per-gene
+ * preparation: complete-case subset, optional --pheno-norm int) and the
+ * covariate matrix X [n, p] (intercept included, src/pheno.cpp:171-193)
+ * resident on the device. The scan entry points use them when called with
+ * Y == NULL and X == NULL, so repeated scans need no host transfer. */
+int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, int32_t n_genes, int32_t p);
+
 /* ------------------------------------------------------- scan result types */
 typedef struct {
   int32_t n_tested;      /* finite tests counted (GeneSummary.n_tested) */
@@ -122,7 +141,8 @@ typedef struct {
  * Replaces scan_lm_snp_outer (src/scan_trans_lm.cpp:41-163) on the shared-
  * keep path: prep_lm per gene (src/model_lm.cpp:19-30), gty = Y_s g_s and
  * hit_from_gty for every (SNP, gene) (:77-120), ACAT / n_tested / best
- * (include/eqtl/scan_trans.hpp:86-102). Y [n, n_genes], X [n, p].
+ * (include/eqtl/scan_trans.hpp:86-102). Y [n, n_genes], X [n, p], or both
+ * NULL to use the phenotypes resident from eqtl_pheno_load.
  * genes[n_genes] receives the per-gene summary; pairs (p <= pthr) come back
  * sorted by (snp, gene) like the reference's pair file; cands (p <
  * perm_thr, the stage-2 permutation candidates) sorted by (gene, p). The
