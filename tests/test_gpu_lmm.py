@@ -5,8 +5,7 @@ import pytest
 
 import oracle_scan
 import restate as R
-from gpu_util import T_ERRS, acat_p_from, log10_diff
-from test_gpu_lm import _check_scan
+from gpu_util import T_ERRS, acat_p_from, check_scan as _check_scan, log10_diff
 
 pytestmark = pytest.mark.gpu
 
