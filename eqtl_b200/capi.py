@@ -24,7 +24,8 @@ PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
 EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
-           "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail"]
+           "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc"]
+GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
 
@@ -76,6 +77,7 @@ def load() -> C.CDLL:
         lib.eqtl_scan_trans_lm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, i64, C.POINTER(i64), vp,
                                            i64, C.POINTER(i64)]
         lib.eqtl_grm.argtypes = [vp, vp, vp, C.POINTER(i64)]
+        lib.eqtl_grm_noalloc.argtypes = [vp, vp, i64, i64, vp, i32, i32, dp, dp, vp, vp, C.POINTER(i64)]
         lib.eqtl_stage_ms.argtypes = [vp, C.c_int, C.POINTER(dp)]
         lib.eqtl_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
         lib.eqtl_lmm_rotate.argtypes = [vp]
@@ -246,6 +248,17 @@ class Context:
         mu = C.c_int64()
         self._check(self.lib.eqtl_grm(self.h, _ptr(K), _ptr(N), C.byref(mu)))
         return K, N, mu.value
+
+    def grm_noalloc(self, bed_dev: int, m: int, bytes_per_snp: int, col_dev: int, n: int, K_dev: int,
+                    N_dev: int = 0, miss_hand: int = MISS_IMPUTE, max_miss: float = 0.8,
+                    maf_min: float = 0.0) -> int:
+        """eqtl_grm_noalloc on caller-owned device buffers (raw device
+        pointers); returns the number of SNPs used."""
+        mu = C.c_int64()
+        self._check(self.lib.eqtl_grm_noalloc(self.h, C.c_void_p(bed_dev), m, bytes_per_snp, C.c_void_p(col_dev), n,
+                                              miss_hand, max_miss, maf_min, C.c_void_p(K_dev),
+                                              C.c_void_p(N_dev) if N_dev else None, C.byref(mu)))
+        return mu.value
 
     def lmm_basis(self, K=None, outputs=True):
         """eqtl_lmm_basis -> (lambda [n], Q [n, n] with eigenvectors as columns);

@@ -561,6 +561,16 @@ int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_use
   });
 }
 
+int eqtl_grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed_dev, int64_t m, int64_t bytes_per_snp,
+                     const int32_t* sample_col_dev, int32_t n, int32_t miss_hand, double max_miss, double maf_min,
+                     double* K_dev, int32_t* N_packed_dev, int64_t* m_used_out) {
+  return guarded(ctx, [&] {
+    const int64_t mu = eqtl::grm_noalloc(ctx, bed_dev, m, bytes_per_snp, sample_col_dev, n, miss_hand, max_miss,
+                                         maf_min, K_dev, N_packed_dev);
+    if (m_used_out) *m_used_out = mu;
+  });
+}
+
 int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out, double* Q_out) {
   return guarded(ctx, [&] {
     eqtl::DevBuf<double> dK;

@@ -10,6 +10,10 @@
 //             accumulation (< 2^24 SNPs); sub_miss_i = J_ii and
 //             N_ij = m - J_ii - J_jj + J_ij, N_ii = m - J_ii (:162-221);
 //   divide    K_ij = A_ij / N_ij (0 if N_ij <= 0).
+#include <algorithm>
+#include <mutex>
+#include <string>
+
 #include "internal.hpp"
 #include "scan_host.hpp"
 
@@ -224,6 +228,252 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   EQTL_CUDA(cudaGetLastError());
   EQTL_CUDA(cudaStreamSynchronize(st));
   return mu_n;
+}
+
+}  // namespace eqtl
+
+// ===================================================== allocation-free GRM
+// The same GRM from caller-owned device buffers, with every piece of scratch
+// (FP16 operands of one pass, FP64/int accumulators, per-SNP statistics) in
+// one file-scope device array sized for n <= kNaMaxN samples. SNP rows go
+// through in passes of kNaChunk; each pass is one tile launch whose K extent
+// is the pass, accumulating into A and J with the split-K atomics of the
+// regular path, so the result equals the regular path's up to the FP64
+// summation order of A.
+namespace eqtl {
+namespace dev {
+
+constexpr int kNaMaxN = EQTL_GRM_NOALLOC_MAX_N;
+constexpr int kNaChunk = EQTL_GRM_NOALLOC_CHUNK;
+constexpr size_t na_align(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNaOpBytes = na_align(sizeof(__half) * kNaMaxN * kNaChunk);
+constexpr size_t kNaABytes = na_align(sizeof(double) * kNaMaxN * kNaMaxN);
+constexpr size_t kNaJBytes = na_align(sizeof(int) * kNaMaxN * kNaMaxN);
+constexpr size_t kNaSnpBytes = na_align(sizeof(double) * kNaChunk);
+constexpr size_t kNaUseBytes = na_align(kNaChunk);
+// layout: zh | zl | mk | A | J | mean | inv_sd | use | counters
+constexpr size_t kNaOffZh = 0;
+constexpr size_t kNaOffZl = kNaOffZh + kNaOpBytes;
+constexpr size_t kNaOffMk = kNaOffZl + kNaOpBytes;
+constexpr size_t kNaOffA = kNaOffMk + kNaOpBytes;
+constexpr size_t kNaOffJ = kNaOffA + kNaABytes;
+constexpr size_t kNaOffMean = kNaOffJ + kNaJBytes;
+constexpr size_t kNaOffIsd = kNaOffMean + kNaSnpBytes;
+constexpr size_t kNaOffUse = kNaOffIsd + kNaSnpBytes;
+constexpr size_t kNaOffCnt = kNaOffUse + kNaUseBytes;  // [0] SNPs used, [1] bad sample columns
+constexpr size_t kNaScratchBytes = kNaOffCnt + 256;
+static_assert(kNaScratchBytes == EQTL_GRM_NOALLOC_SCRATCH_BYTES, "header scratch size");
+
+static __device__ __align__(256) uint8_t grm_na_scratch[kNaScratchBytes];
+
+// Sample columns must address the .bed row: 0 <= col < 4 * bytes_per_snp.
+__global__ void grm_na_check_cols_kernel(const int32_t* __restrict__ col, int n, int64_t bps,
+                                         unsigned long long* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const int32_t c = col[i];
+    if (c < 0 || static_cast<int64_t>(c) >= 4 * bps) atomicAdd(bad, 1ull);
+  }
+}
+
+// One warp per SNP row of the pass: the decode filter of bed_stats_kernel
+// (geno.cu) followed by the GRM usability of grm_snp_kernel, in the same
+// FP64 expressions.
+__global__ void grm_na_stats_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                    int n, int64_t r0, int nr, int miss_hand, double max_miss, double maf_min,
+                                    uint8_t* use, double* mean, double* inv_sd, unsigned long long* m_used) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= kNaChunk) return;
+  if (r >= nr) {
+    if (lane == 0) {
+      use[r] = 0;
+      mean[r] = 0.0;
+      inv_sd[r] = 0.0;
+    }
+    return;
+  }
+  const uint8_t* row = bed + (r0 + r) * bps;
+  int nm = 0, a = 0;
+  for (int i = lane; i < n; i += 32) {
+    const int c = bed_code_g(row, __ldg(col + i));
+    if (c < 0)
+      ++nm;
+    else
+      a += c;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    nm += __shfl_xor_sync(0xffffffffu, nm, o);
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+  }
+  if (lane) return;
+  const int n_ok = n - nm;
+  bool keep = n_ok > 0;
+  const double sum = static_cast<double>(a);
+  double m_imp = 0.0, f = 0.0;
+  if (n_ok > 0) {
+    m_imp = sum / n_ok;
+    f = (sum / static_cast<double>(n_ok)) / 2.0;
+  }
+  const double miss_frac = static_cast<double>(nm) / static_cast<double>(n);
+  if (miss_frac > max_miss + 1e-15) keep = false;
+  if (miss_hand == EQTL_MISS_FILTER && nm > 0) keep = false;
+  if (f < 0) f = 0;
+  if (f > 1) f = 1;
+  if (f < 1e-12 || f > 1.0 - 1e-12) keep = false;
+  if (maf_min > 0.0 && (f < maf_min || f > 1.0 - maf_min)) keep = false;
+  const double mean_v = (static_cast<double>(a) + nm * m_imp) / n;
+  const double p = mean_v / 2.0;
+  bool ok = keep && !(p < 1e-8 || p > 1.0 - 1e-8);
+  const double sd = sqrt(2.0 * p * (1.0 - p));
+  if (sd < 1e-12) ok = false;
+  use[r] = ok ? 1 : 0;
+  mean[r] = mean_v;
+  inv_sd[r] = ok ? 1.0 / sd : 0.0;
+  if (ok) atomicAdd(m_used, 1ull);
+}
+
+// Zt[i, c] of the pass (row stride kNaChunk), zero for unused columns:
+// 32 x 32 tiles through shared memory like grm_transpose_kernel.
+__global__ void grm_na_transpose_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                        int n, int64_t r0, const uint8_t* __restrict__ use,
+                                        const double* __restrict__ mean, const double* __restrict__ inv_sd,
+                                        __half* zh, __half* zl, __half* mk) {
+  __shared__ float tz[32][33];
+  __shared__ float tm[32][33];
+  const int c0 = blockIdx.x * 32;
+  const int i0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int i = i0 + tx;
+  const int ci = i < n ? __ldg(col + i) : 0;
+  for (int r = ty; r < 32; r += 8) {
+    const int c = c0 + r;
+    float z = 0.0f, mm = 0.0f;
+    if (i < n && use[c]) {
+      const int code = bed_code_g(bed + (r0 + c) * bps, ci);
+      if (code < 0) {
+        mm = 1.0f;
+      } else {
+        z = static_cast<float>((static_cast<double>(code) - mean[c]) * inv_sd[c]);
+      }
+    }
+    tz[r][tx] = z;
+    tm[r][tx] = mm;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int ii = i0 + r;
+    const int c = c0 + tx;
+    if (ii < n) {
+      const float z = tz[tx][r];
+      const __half h = __float2half_rn(z);
+      const __half l = __float2half_rn(z - __half2float(h));
+      zh[static_cast<int64_t>(ii) * kNaChunk + c] = h;
+      zl[static_cast<int64_t>(ii) * kNaChunk + c] = l;
+      mk[static_cast<int64_t>(ii) * kNaChunk + c] = __float2half_rn(tm[tx][r]);
+    }
+  }
+}
+
+__global__ void grm_na_finalize_kernel(int n, const unsigned long long* __restrict__ m_used,
+                                       const double* __restrict__ A, const int* __restrict__ J, double* K,
+                                       int32_t* Npk) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= static_cast<int64_t>(n) * n) return;
+  const int64_t mu = static_cast<int64_t>(*m_used);
+  const int i = static_cast<int>(e / n), j = static_cast<int>(e - static_cast<int64_t>(i) * n);
+  const int64_t mi = static_cast<int64_t>(J[static_cast<int64_t>(i) * n + i]);
+  const int64_t mj = static_cast<int64_t>(J[static_cast<int64_t>(j) * n + j]);
+  int64_t sub;
+  if (i == j)
+    sub = mu - mi;
+  else
+    sub = mu - mi - mj + static_cast<int64_t>(J[e]);
+  K[e] = sub > 0 ? A[e] / static_cast<double>(sub) : 0.0;
+  if (Npk && j <= i) Npk[static_cast<int64_t>(i) * (i + 1) / 2 + j] = static_cast<int32_t>(sub);
+}
+
+}  // namespace dev
+
+namespace {
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mu;
+uint8_t* g_na_addr[kNaMaxDevices] = {};
+}  // namespace
+
+// Device address of the scratch array on the current device, resolved once
+// per device (cudaGetSymbolAddress).
+static uint8_t* grm_na_scratch_addr(int device) {
+  EQTL_CHECK(device >= 0 && device < kNaMaxDevices, EQTL_E_ARG, "eqtl_grm_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  if (!g_na_addr[device]) {
+    void* p = nullptr;
+    EQTL_CUDA(cudaGetSymbolAddress(&p, dev::grm_na_scratch));
+    g_na_addr[device] = static_cast<uint8_t*>(p);
+  }
+  return g_na_addr[device];
+}
+
+int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
+                    int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk) {
+  using namespace dev;
+  EQTL_CHECK(bed && col && K, EQTL_E_ARG, "eqtl_grm_noalloc: null input or output");
+  EQTL_CHECK(n > 0 && m > 0 && bps > 0, EQTL_E_ARG, "eqtl_grm_noalloc: bad sizes");
+  EQTL_CHECK(n <= kNaMaxN, EQTL_E_UNSUPPORTED,
+             "eqtl_grm_noalloc: n = " + std::to_string(n) + " exceeds the static scratch limit of " +
+                 std::to_string(kNaMaxN) + " samples (use eqtl_grm)");
+  EQTL_CHECK(miss_hand == EQTL_MISS_FILTER || miss_hand == EQTL_MISS_IMPUTE, EQTL_E_ARG,
+             "eqtl_grm_noalloc: miss_hand");
+  uint8_t* s = grm_na_scratch_addr(ctx->device);
+  __half* zh = reinterpret_cast<__half*>(s + kNaOffZh);
+  __half* zl = reinterpret_cast<__half*>(s + kNaOffZl);
+  __half* mk = reinterpret_cast<__half*>(s + kNaOffMk);
+  double* A = reinterpret_cast<double*>(s + kNaOffA);
+  int* J = reinterpret_cast<int*>(s + kNaOffJ);
+  double* mean = reinterpret_cast<double*>(s + kNaOffMean);
+  double* isd = reinterpret_cast<double*>(s + kNaOffIsd);
+  uint8_t* use = s + kNaOffUse;
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(s + kNaOffCnt);
+  cudaStream_t st = ctx->stream;
+  // accumulators and counters start at zero on every call
+  EQTL_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
+  EQTL_CUDA(cudaMemsetAsync(J, 0, sizeof(int) * n * n, st));
+  EQTL_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), st));
+  ++ctx->launches;
+  grm_na_check_cols_kernel<<<(n + 255) / 256, 256, 0, st>>>(col, n, bps, cnt + 1);
+  EQTL_CUDA(cudaGetLastError());
+  unsigned long long bad = 0;
+  EQTL_CUDA(cudaMemcpyAsync(&bad, cnt + 1, sizeof(bad), cudaMemcpyDeviceToHost, st));
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  EQTL_CHECK(bad == 0, EQTL_E_ARG, "eqtl_grm_noalloc: sample_col outside the .bed row");
+  GrmEpiParams ep{n, A, J};
+  const __half* ah[2] = {zh, mk};
+  const __half* al[2] = {zl, mk};
+  const int bsel[2] = {0, 1}, prod[2] = {7, 1};
+  const int tiles = ((n + 127) / 128) * ((n + 255) / 256);
+  const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
+  for (int64_t r0 = 0; r0 < m; r0 += kNaChunk) {
+    const int nr = static_cast<int>(std::min<int64_t>(kNaChunk, m - r0));
+    ctx->launches += 2;
+    grm_na_stats_kernel<<<kNaChunk / 8, 256, 0, st>>>(bed, bps, col, n, r0, nr, miss_hand, max_miss, maf_min, use,
+                                                       mean, isd, cnt);
+    EQTL_CUDA(cudaGetLastError());
+    grm_na_transpose_kernel<<<dim3(kNaChunk / 32, (n + 31) / 32), dim3(32, 8), 0, st>>>(bed, bps, col, n, r0, use,
+                                                                                        mean, isd, zh, zl, mk);
+    EQTL_CUDA(cudaGetLastError());
+    launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, ah, al, n, kNaChunk, bsel, prod, nullptr, 0, ksplit);
+  }
+  unsigned long long used = 0;
+  EQTL_CUDA(cudaMemcpyAsync(&used, cnt, sizeof(used), cudaMemcpyDeviceToHost, st));
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  EQTL_CHECK(used > 0, EQTL_E_ARG, "no SNPs for GRM");
+  const int64_t tot = static_cast<int64_t>(n) * n;
+  ++ctx->launches;
+  grm_na_finalize_kernel<<<static_cast<unsigned>((tot + 255) / 256), 256, 0, st>>>(n, cnt, A, J, K, Npk);
+  EQTL_CUDA(cudaGetLastError());
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  return static_cast<int64_t>(used);
 }
 
 }  // namespace eqtl

@@ -212,6 +212,8 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk);
 void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n);
 void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n);
 void lmm_rotate(eqtl_ctx* ctx);
+int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
+                    int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk);
 void solver_release(eqtl_ctx* ctx);
 
 // -- stage timing (capi.cu)

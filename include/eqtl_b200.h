@@ -159,6 +159,35 @@ int eqtl_scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double*
  * used. Either output may be NULL. */
 int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out);
 
+/* ---------------------------------------------------- allocation-free GRM
+ * No counterpart in the reference. The GRM of eqtl_geno_load_bed +
+ * eqtl_grm with the same arguments, computed from caller-owned DEVICE
+ * buffers without allocating device memory, for callers that cannot
+ * allocate once running (a process that reserves its device memory up
+ * front, e.g. a service sharing the GPU under a fixed budget). Inputs:
+ * bed_dev = m SNP rows of bytes_per_snp bytes (.bed payload after the
+ * 3-byte header), sample_col_dev = n analysis-sample columns. Outputs:
+ * K_dev [n, n] row-major, N_packed_dev [n(n+1)/2] (may be NULL),
+ * m_used_out (host, may be NULL). Equal to eqtl_grm up to the FP64
+ * summation order of K; N bit-exact.
+ *   - all scratch is one static device array of
+ *     EQTL_GRM_NOALLOC_SCRATCH_BYTES in the library image; n is limited to
+ *     EQTL_GRM_NOALLOC_MAX_N (larger n: EQTL_E_UNSUPPORTED), m is not (SNPs
+ *     go through in passes of EQTL_GRM_NOALLOC_CHUNK);
+ *   - the first call on a device resolves the array's address
+ *     (cudaGetSymbolAddress) with the device current; make that call before
+ *     any stream capture;
+ *   - the accumulators and counters are zeroed at the start of every call
+ *     on the context's stream;
+ *   - the scratch is shared by every context on the device: overlapping
+ *     calls (other threads, contexts or streams) race; serialise them. */
+#define EQTL_GRM_NOALLOC_MAX_N 512
+#define EQTL_GRM_NOALLOC_CHUNK 2048
+#define EQTL_GRM_NOALLOC_SCRATCH_BYTES 9472256
+int eqtl_grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed_dev, int64_t m, int64_t bytes_per_snp,
+                     const int32_t* sample_col_dev, int32_t n, int32_t miss_hand, double max_miss, double maf_min,
+                     double* K_dev, int32_t* N_packed_dev, int64_t* m_used_out);
+
 /* ------------------------------------------------------------- eigenbasis
  * Replaces make_lmm_basis (src/model_lmm.cpp:106-113): eigendecomposition of
  * the GRM K [n, n] (row-major; NULL = compute the GRM of the loaded
