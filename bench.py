@@ -328,9 +328,11 @@ def b200_arm(args, rank, world, local_rank):
 
 
 def scan_traffic(tests):
-    """DRAM bytes of the scan kernel per launch, scaled from the committed ncu
-    capture summary (profiles/tile_kernel_lmm_scan.txt: 'dram_bytes_per_test')."""
-    p = os.path.join(ROOT, "profiles", "tile_kernel_lmm_scan.txt")
+    """DRAM bytes of the scan kernel per launch, scaled by the tests of a launch
+    from the committed ncu capture of a smaller case (the SNP operand streams
+    once per fixed-size gene group, so traffic grows with the tests):
+    profiles/tile_kernel_lmm_scan_n2000_m100k_g4000.md, 'dram_bytes_per_test'."""
+    p = os.path.join(ROOT, "profiles", "tile_kernel_lmm_scan_n2000_m100k_g4000.md")
     if not os.path.exists(p):
         return None
     for ln in open(p):
