@@ -24,7 +24,8 @@ PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
 EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
-           "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc"]
+           "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
+           "eqtl_test_pairs"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -74,6 +75,8 @@ def load() -> C.CDLL:
         lib.eqtl_geno_load_bed.argtypes = [vp, vp, i64, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp,
                                            C.POINTER(i64)]
         lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
+        lib.eqtl_geno_dosage_rows.argtypes = [vp, vp, i64, vp]
+        lib.eqtl_test_pairs.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64, vp, vp]
         lib.eqtl_scan_trans_lm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, i64, C.POINTER(i64), vp,
                                            i64, C.POINTER(i64)]
         lib.eqtl_grm.argtypes = [vp, vp, vp, C.POINTER(i64)]
@@ -176,7 +179,7 @@ class Context:
             prm.gene_hi = arrs[2].ctypes.data_as(C.POINTER(C.c_int64))
             prm.snp_chrom = arrs[3].ctypes.data_as(C.POINTER(C.c_int32))
             prm.snp_pos = arrs[4].ctypes.data_as(C.POINTER(C.c_int64))
-            prm.exclude_cis = 1 if exclude else 0
+            prm.exclude_cis = int(exclude)   # 0 gw, 1 trans (skip the window), 2 cis (only the window)
         return prm, keep
 
     def pheno_load(self, Y, X):
@@ -275,6 +278,21 @@ class Context:
         Qc = np.ascontiguousarray(np.asarray(Q, np.float64).T)   # column-major
         lam = np.ascontiguousarray(lam, np.float64)
         self._check(self.lib.eqtl_lmm_set_basis(self.h, _ptr(Qc), _ptr(lam), lam.size))
+
+    def test_pairs(self, model: str, Y, X, cols, snps):
+        """eqtl_test_pairs: FP64 statistics of (column of Y, kept SNP) pairs
+        -> (pairs [k] PAIR_DTYPE, delta [G] or None)."""
+        Y = np.asfortranarray(Y, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        (n, G), p = Y.shape, X.shape[1]
+        prm, _ = self._params(n, G, p, 0.0, 0.0, None)
+        cols = np.ascontiguousarray(cols, np.int32)
+        snps = np.ascontiguousarray(snps, np.int64)
+        out = np.zeros(cols.size, PAIR_DTYPE)
+        delta = np.zeros(G, np.float64) if model == "lmm" else None
+        self._check(self.lib.eqtl_test_pairs(self.h, 0 if model == "lm" else 1, C.byref(prm), _ptr(Y), _ptr(X),
+                                             _ptr(cols), _ptr(snps), cols.size, _ptr(out), _ptr(delta)))
+        return out, delta
 
     def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None):
         """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta)."""

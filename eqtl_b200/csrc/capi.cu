@@ -517,6 +517,33 @@ int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
   });
 }
 
+int eqtl_test_pairs(eqtl_ctx* ctx, int32_t model, const eqtl_scan_params* prm, const double* Y, const double* X,
+                    const int32_t* pair_col, const int64_t* pair_snp, int64_t n_pairs, eqtl_pair* out,
+                    double* delta_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(prm && ((pair_col && pair_snp && out) || n_pairs == 0), EQTL_E_ARG, "null input");
+    EQTL_CHECK(model == EQTL_MODEL_LM || model == EQTL_MODEL_LMM, EQTL_E_ARG, "model must be EQTL_MODEL_LM or _LMM");
+    std::vector<int2> todo(static_cast<size_t>(n_pairs));
+    for (int64_t i = 0; i < n_pairs; ++i) {
+      EQTL_CHECK(pair_snp[i] >= 0 && pair_snp[i] < (int64_t(1) << 31), EQTL_E_ARG, "pair SNP index out of range");
+      todo[i] = make_int2(pair_col[i], static_cast<int>(pair_snp[i]));
+    }
+    if (model == EQTL_MODEL_LM) {
+      eqtl::test_pairs_lm(ctx, prm, Y, X, todo, out);
+    } else {
+      EQTL_CHECK(ctx->have_basis, EQTL_E_STATE, "the LMM needs an eigenbasis (eqtl_lmm_basis)");
+      eqtl::test_pairs_lmm(ctx, prm, Y, X, todo, out, delta_out);
+    }
+  });
+}
+
+int eqtl_geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK((rows && out) || k == 0, EQTL_E_ARG, "null input");
+    eqtl::geno_dosage_rows(ctx, rows, k, out);
+  });
+}
+
 int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use_smem, float* neglog10p,
                 double* term, uint8_t* flags) {
   return guarded(ctx, [&] {

@@ -122,6 +122,20 @@ __global__ void bed_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
   }
 }
 
+__global__ void bed_dosage_rows_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                       int n, const int64_t* __restrict__ kept, const int64_t* __restrict__ rows,
+                                       int64_t k, const double* __restrict__ mu, double* out) {
+  const int64_t total = k * n;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = e / n;
+    const int i = static_cast<int>(e - r * n);
+    const int64_t s = kept[rows[r]];
+    const int c = bed_code(bed + s * bps, col[i]);
+    out[e] = c < 0 ? mu[s] : static_cast<double>(c);
+  }
+}
+
 }  // namespace
 
 void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
@@ -198,6 +212,23 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {
   ++ctx->launches;
   bed_dosage_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, lo, hi,
                                                    g.mu.p, d.p);
+  EQTL_CUDA(cudaGetLastError());
+  d.download(out_host, d.n, ctx->stream);
+  EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host) {
+  Geno& g = ctx->geno;
+  for (int64_t r = 0; r < k; ++r)
+    EQTL_CHECK(rows[r] >= 0 && rows[r] < g.m, EQTL_E_ARG, "geno_dosage_rows: index outside the kept SNPs");
+  if (k == 0) return;
+  DevBuf<int64_t> d_rows;
+  DevBuf<double> d;
+  d_rows.upload(rows, k, ctx->stream);
+  d.alloc(static_cast<size_t>(k) * g.n);
+  ++ctx->launches;
+  bed_dosage_rows_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, d_rows.p,
+                                                        k, g.mu.p, d.p);
   EQTL_CUDA(cudaGetLastError());
   d.download(out_host, d.n, ctx->stream);
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));

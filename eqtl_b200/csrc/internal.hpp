@@ -193,6 +193,7 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
                const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min);
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
+void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host);
 void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p);
 
 // -- scan drivers
@@ -215,6 +216,10 @@ void lmm_rotate(eqtl_ctx* ctx);
 int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
                     int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk);
 void solver_release(eqtl_ctx* ctx);
+void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                   const std::vector<int2>& todo, eqtl_pair* out);
+void test_pairs_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                    const std::vector<int2>& todo, eqtl_pair* out, double* delta_out);
 
 // -- stage timing (capi.cu)
 void stage_begin(eqtl_ctx* ctx, int stage);

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <memory>
 
 #include "internal.hpp"
@@ -737,6 +738,68 @@ static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* c
   EQTL_CUDA(cudaStreamSynchronize(st));
 }
 
+// FP64 statistics of (gene, kept SNP) pairs against the current LMM prep
+// (ws.Ytil, Xtil, delta, chi0, ainv, rss): raw dosages of the SNPs involved,
+// Gt = Q'g by DGEMM, then one warp per pair (lmm_refine_kernel).
+static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, const std::vector<int2>& todo) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  const int n = g.n;
+  std::vector<eqtl_pair> refined(todo.size());
+  if (!todo.empty()) {
+    std::vector<int> snps;
+    snps.reserve(todo.size());
+    for (const int2& q : todo) snps.push_back(q.y);
+    std::sort(snps.begin(), snps.end());
+    snps.erase(std::unique(snps.begin(), snps.end()), snps.end());
+    std::vector<int> pcol(todo.size());
+    for (size_t i = 0; i < todo.size(); ++i)
+      pcol[i] = static_cast<int>(std::lower_bound(snps.begin(), snps.end(), todo[i].y) - snps.begin());
+    const int u = static_cast<int>(snps.size());
+    DevBuf<int>& dsn = ws.ref_snps;
+    DevBuf<int>& dpc = ws.ref_col;
+    DevBuf<int2>& dtodo = ws.ref_pairs;
+    dsn.upload(snps.data(), u, st);
+    dpc.upload(pcol.data(), pcol.size(), st);
+    dtodo.upload(todo.data(), todo.size(), st);
+    DevBuf<double>& graw = ws.graw;
+    DevBuf<double>& gt = ws.gt;
+    graw.alloc(static_cast<size_t>(n) * u);
+    gt.alloc(static_cast<size_t>(n) * u);
+    ctx->launches += 2;
+    raw_dosage_kernel<<<1184, 256, 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dsn.p, u, graw.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_T, CUBLAS_OP_N, n, u, n, &one, ctx->basis.Q.p, n, graw.p, n, &zero,
+                           gt.p, n) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "Q'g failed");
+    ws.refined.alloc(todo.size());
+    lmm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
+        gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), ws.Ytil.p, ws.Xtil.p, p, ctx->basis.lambda.p,
+        ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p, df, ws.refined.p);
+    EQTL_CUDA(cudaGetLastError());
+    ws.refined.download(refined.data(), todo.size(), st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+  }
+  return refined;
+}
+
+// Subset gate of every kept SNP on the analysis samples into ws.ok.
+static void lmm_gate(eqtl_ctx* ctx) {
+  Geno& g = ctx->geno;
+  DevBuf<uint8_t>& ok = ctx->ws.ok;
+  const int64_t m = g.m;
+  ok.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));  // the epilogue reads 16 flags per chunk, up to the last tile's end
+  EQTL_CUDA(cudaMemsetAsync(ok.p, 0, ok.n, ctx->stream));
+  if (m > 0) {
+    ++ctx->launches;
+    snp_gate_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, ctx->stream>>>(g.kept.p, m, g.n, g.mu.p,
+                                                                                     g.n_miss.p, g.s1.p, g.s2.p, ok.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+}
+
 static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                                 double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
                                 std::vector<eqtl_pair>& cands, bool simt) {
@@ -776,16 +839,9 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   EQTL_CUDA(cudaGetLastError());
 
   const int64_t m = g.m;
+  lmm_gate(ctx);
   DevBuf<uint8_t>& ok = ws.ok;
-  ok.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));  // the epilogue reads 16 flags per chunk, up to the last tile's end
-  EQTL_CUDA(cudaMemsetAsync(ok.p, 0, ok.n, st));
-  if (m > 0) {
-    ++ctx->launches;
-    snp_gate_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, st>>>(g.kept.p, m, n, g.mu.p, g.n_miss.p,
-                                                                            g.s1.p, g.s2.p, ok.p);
-    EQTL_CUDA(cudaGetLastError());
-  }
-  const Windows win = upload_windows(ctx, prm, m, prm->exclude_cis ? kWinExclude : kWinNone);
+  const Windows win = upload_windows(ctx, prm, m, prm->exclude_cis == 2 ? kWinInclude : prm->exclude_cis ? kWinExclude : kWinNone);
   double t_cand = t_critical(prm->pthr, df);
   if (prm->perm_thr > 0) t_cand = std::min(t_cand, t_critical(prm->perm_thr, df));
   const TTable tt = device_ttable(ctx, df);
@@ -833,42 +889,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     ws.delta.download(delta_out, G, st);
     EQTL_CUDA(cudaStreamSynchronize(st));
   }
-  std::vector<eqtl_pair> refined(todo.size());
-  if (!todo.empty()) {
-    std::vector<int> snps;
-    snps.reserve(todo.size());
-    for (const int2& q : todo) snps.push_back(q.y);
-    std::sort(snps.begin(), snps.end());
-    snps.erase(std::unique(snps.begin(), snps.end()), snps.end());
-    std::vector<int> pcol(todo.size());
-    for (size_t i = 0; i < todo.size(); ++i)
-      pcol[i] = static_cast<int>(std::lower_bound(snps.begin(), snps.end(), todo[i].y) - snps.begin());
-    const int u = static_cast<int>(snps.size());
-    DevBuf<int>& dsn = ws.ref_snps;
-    DevBuf<int>& dpc = ws.ref_col;
-    DevBuf<int2>& dtodo = ws.ref_pairs;
-    dsn.upload(snps.data(), u, st);
-    dpc.upload(pcol.data(), pcol.size(), st);
-    dtodo.upload(todo.data(), todo.size(), st);
-    DevBuf<double>& graw = ws.graw;
-    DevBuf<double>& gt = ws.gt;
-    graw.alloc(static_cast<size_t>(n) * u);
-    gt.alloc(static_cast<size_t>(n) * u);
-    ctx->launches += 2;
-    raw_dosage_kernel<<<1184, 256, 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dsn.p, u, graw.p);
-    EQTL_CUDA(cudaGetLastError());
-    const double one = 1.0, zero = 0.0;
-    EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_T, CUBLAS_OP_N, n, u, n, &one, ctx->basis.Q.p, n, graw.p, n, &zero,
-                           gt.p, n) == CUBLAS_STATUS_SUCCESS,
-               EQTL_E_CUDA, "Q'g failed");
-    ws.refined.alloc(todo.size());
-    lmm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
-        gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), ws.Ytil.p, ws.Xtil.p, p, ctx->basis.lambda.p,
-        ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p, df, ws.refined.p);
-    EQTL_CUDA(cudaGetLastError());
-    ws.refined.download(refined.data(), todo.size(), st);
-    EQTL_CUDA(cudaStreamSynchronize(st));
-  }
+  std::vector<eqtl_pair> refined = lmm_refine_pairs(ctx, p, df, todo);
   add_deferred_acat(genes, refined, deferred);
   finish_scan(prm, genes, refined, pairs, cands);
 }
@@ -882,6 +903,37 @@ void scan_trans_lmm_simt(eqtl_ctx* ctx, const eqtl_scan_params* prm, const doubl
                          double* delta_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
                          std::vector<eqtl_pair>& cands) {
   scan_trans_lmm_impl(ctx, prm, Y, X, delta_out, genes, pairs, cands, true);
+}
+
+// FP64 tests of explicit (column of Y, kept SNP) pairs with the resident
+// eigenbasis: the full null fit per column (Q'Y, REML delta, GLS), then the
+// refinement arithmetic of the scan; a SNP that fails the subset gate gets
+// p = NaN (it is never tested in the reference).
+void test_pairs_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                    const std::vector<int2>& todo, eqtl_pair* out, double* delta_out) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "test_pairs: no genotypes loaded");
+  const int n = prm->n, G = prm->n_genes, p = prm->p;
+  EQTL_CHECK(n == g.n, EQTL_E_ARG, "test_pairs: n differs from the loaded genotypes");
+  EQTL_CHECK(G > 0, EQTL_E_ARG, "test_pairs: no columns");
+  for (const int2& q : todo)
+    EQTL_CHECK(q.x >= 0 && q.x < G && q.y >= 0 && q.y < g.m, EQTL_E_ARG, "test_pairs: pair index out of range");
+  const double df = static_cast<double>(n - p - 1);
+  const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
+  lmm_prep(ctx, ph);
+  lmm_gate(ctx);
+  std::vector<uint8_t> ok(static_cast<size_t>(g.m));
+  ws.ok.download(ok.data(), static_cast<size_t>(g.m), ctx->stream);
+  const std::vector<eqtl_pair> refined = lmm_refine_pairs(ctx, p, df, todo);
+  for (size_t i = 0; i < todo.size(); ++i) {
+    out[i] = refined[i];
+    if (!ok[todo[i].y]) out[i].p = std::numeric_limits<double>::quiet_NaN();
+  }
+  if (delta_out) {
+    ws.delta.download(delta_out, G, ctx->stream);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
 }
 
 }  // namespace eqtl

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <memory>
 
 #include "internal.hpp"
@@ -266,6 +267,28 @@ struct EpiOf<dev::LmEpiParams> {
 
 using namespace dev;
 
+// FP64 statistics of (gene, kept SNP) pairs against the current LM prep
+// (ws.Ys, ws.yty, ws.gtg): gty from the exact decoded dosage, one warp per pair.
+static std::vector<eqtl_pair> lm_refine_pairs(eqtl_ctx* ctx, double df, const std::vector<int2>& todo) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  const int n = g.n;
+  std::vector<eqtl_pair> refined(todo.size());
+  if (!todo.empty()) {
+    ws.ref_pairs.upload(todo.data(), todo.size(), st);
+    ws.refined.alloc(todo.size());
+    ++ctx->launches;
+    lm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
+        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, ws.Ys.p, ws.gtg.p, ws.yty.p, df, ws.ref_pairs.p,
+        static_cast<int>(todo.size()), ws.refined.p);
+    EQTL_CUDA(cudaGetLastError());
+    ws.refined.download(refined.data(), todo.size(), st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+  }
+  return refined;
+}
+
 void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs, std::vector<eqtl_pair>& cands) {
   Geno& g = ctx->geno;
@@ -332,7 +355,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   ep.gscale = ws.gscale.p;
   ep.inv_gtg = ws.inv_gtg.p;
   ep.snp_ok = ws.ok.p;
-  ep.win = upload_windows(ctx, prm, m, prm->exclude_cis ? kWinExclude : kWinNone);
+  ep.win = upload_windows(ctx, prm, m, prm->exclude_cis == 2 ? kWinInclude : prm->exclude_cis ? kWinExclude : kWinNone);
   ep.df = static_cast<float>(df);
   ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
   ep.tt = device_ttable(ctx, df);
@@ -357,20 +380,63 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
   std::vector<int2> todo, deferred;
   so.collect(genes, todo, deferred);
-  std::vector<eqtl_pair> refined(todo.size());
-  if (!todo.empty()) {
-    ws.ref_pairs.upload(todo.data(), todo.size(), st);
-    ws.refined.alloc(todo.size());
-    ++ctx->launches;
-    lm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, ws.Ys.p, ws.gtg.p, ws.yty.p, df, ws.ref_pairs.p,
-        static_cast<int>(todo.size()), ws.refined.p);
-    EQTL_CUDA(cudaGetLastError());
-    ws.refined.download(refined.data(), todo.size(), st);
-    EQTL_CUDA(cudaStreamSynchronize(st));
-  }
+  std::vector<eqtl_pair> refined = lm_refine_pairs(ctx, df, todo);
   add_deferred_acat(genes, refined, deferred);
   finish_scan(prm, genes, refined, pairs, cands);
+}
+
+// FP64 tests of explicit (column of Y, kept SNP) pairs with the scan's prep:
+// Y residualised on X, gtg and the subset gate per SNP; a SNP that fails the
+// gate gets p = NaN (it is never tested in the reference).
+void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
+                   const std::vector<int2>& todo, eqtl_pair* out) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "test_pairs: no genotypes loaded");
+  const int n = prm->n, G = prm->n_genes, p = prm->p;
+  EQTL_CHECK(n == g.n, EQTL_E_ARG, "test_pairs: n differs from the loaded genotypes");
+  EQTL_CHECK(G > 0 && p > 0 && p <= kMaxP, EQTL_E_ARG, "test_pairs: need 1 <= p <= 32 and columns > 0");
+  for (const int2& q : todo)
+    EQTL_CHECK(q.x >= 0 && q.x < G && q.y >= 0 && q.y < g.m, EQTL_E_ARG, "test_pairs: pair index out of range");
+  cudaStream_t st = ctx->stream;
+  const double df = static_cast<double>(n - p - 1);
+  const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
+  std::vector<double> XtXinv = xtx_inverse(ph.X_h.data(), n, p);
+  ws.XtXinv.upload(XtXinv.data(), XtXinv.size(), st);
+  ws.Ys.alloc(static_cast<size_t>(n) * G);
+  EQTL_CUDA(cudaMemcpyAsync(ws.Ys.p, ph.Y.p, sizeof(double) * n * G, cudaMemcpyDeviceToDevice, st));
+  ws.XtY.alloc(static_cast<size_t>(p) * G);
+  residualize_genes(ctx, ph.X.p, ws.XtXinv.p, n, p, G, ws.Ys.p, ws.XtY.p);
+  const int k_pad = g.k_pad;
+  ws.ops_hi[0].alloc(static_cast<size_t>(G) * k_pad);
+  ws.ops_lo[0].alloc(static_cast<size_t>(G) * k_pad);
+  ws.gscale.alloc(G);
+  ws.inv_yty.alloc(G);
+  ws.yty.alloc(G);
+  ++ctx->launches;
+  gene_split_kernel<__half><<<G, 256, 0, st>>>(ws.Ys.p, n, k_pad, G, ws.ops_hi[0].p, ws.ops_lo[0].p, ws.gscale.p,
+                                               ws.yty.p, ws.inv_yty.p, kGcScale);
+  EQTL_CUDA(cudaGetLastError());
+  const int64_t m = g.m;
+  ws.gtg.alloc(std::max<int64_t>(m, 1));
+  ws.inv_gtg.alloc(std::max<int64_t>(m, 1));
+  ws.af_sub.alloc(std::max<int64_t>(m, 1));
+  ws.ok.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));
+  EQTL_CUDA(cudaMemsetAsync(ws.ok.p, 0, ws.ok.n, st));
+  if (m > 0) {
+    ++ctx->launches;
+    snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
+        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  std::vector<uint8_t> ok(static_cast<size_t>(m));
+  ws.ok.download(ok.data(), static_cast<size_t>(m), st);
+  const std::vector<eqtl_pair> refined = lm_refine_pairs(ctx, df, todo);
+  for (size_t i = 0; i < todo.size(); ++i) {
+    out[i] = refined[i];
+    if (!ok[todo[i].y]) out[i].p = std::numeric_limits<double>::quiet_NaN();
+  }
 }
 
 }  // namespace eqtl

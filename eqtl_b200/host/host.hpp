@@ -1,0 +1,125 @@
+// Host side of the eqtl drop-in: the command line of the reference program
+// (src/options.cpp) for PLINK input and the LM / LMM models, its input
+// readers, the scan drivers that call libeqtl_cuda through the C ABI, and the
+// pairs / top / region TSV writers (src/output.cpp:8-110). Everything here is
+// plain C++17; all association arithmetic runs on the device.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "eqtl_b200.h"
+
+namespace eqtl_host {
+
+// Fatal input or usage error; main prints "[E] <what>" and exits 1, like the
+// reference's die() (src/util.cpp:15-19, src/main.cpp:13-20).
+struct Fatal : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+[[noreturn]] void die(const std::string& msg);
+void info(const std::string& msg);
+
+// ------------------------------------------------------------------ options
+struct Options {
+  std::string bfile, pheno, out = "eqtl_out", gff, covar, grm, gff_id_key;
+  bool make_grm = false;
+  std::string mode = "all";              // cis | trans | all | gw
+  std::vector<std::string> models{"lmm"};
+  int window = 1000000;
+  double pval_cis = 1e-5, pval_trans = 1e-5;
+  bool miss_filter = false;              // --miss-hand filter
+  double max_miss = 0.8, maf = 0.0;
+  bool pheno_int = false;                // --pheno-norm int
+  int threads = 1;
+  int perm = 0;
+  double perm_trans_thr = 1e-5;
+  int perm_trans_top = 1000;
+  int seed = -1;
+  bool disable_beta_approx = false;
+};
+// Returns 0 to run, 2 after --help / --version, 1 on a usage error.
+int parse_options(int argc, char** argv, Options& opt);
+
+// ------------------------------------------------------------------- inputs
+struct Plink {
+  std::vector<std::string> fam_iid;
+  std::vector<std::string> chrom, id, a1, a2;  // .bim columns 1, 2, 5, 6
+  std::vector<int64_t> pos;                    // .bim column 4
+  int n_file = 0;
+  int64_t bytes_per_snp = 0;
+  std::vector<uint8_t> rows;                   // .bed payload, SNP-major
+};
+Plink read_plink(const std::string& prefix);
+
+struct Pheno {
+  std::vector<std::string> samples, genes;
+  std::vector<double> Y;  // [samples][genes], row-major as in the file
+};
+Pheno load_pheno(const std::string& path);
+
+// Covariates for the analysis samples, column-major [n, p], intercept first
+// unless a column is already constant 1 (src/pheno.cpp:89-196).
+std::vector<double> load_covar(const std::string& path, const std::vector<std::string>& samples, int& p);
+
+struct GeneLoc {
+  std::string chrom;
+  int64_t start = 0, end = 0, tss = 0;
+};
+std::unordered_map<std::string, GeneLoc> load_gff(const std::string& path, const std::string& id_key);
+
+// Chromosome names compare after dropping a "chr" prefix and leading zeros
+// (chrom_equal, src/util.cpp:68-87); ids are assigned per normalised name.
+std::string chrom_key(const std::string& c);
+
+struct GrmFile {
+  std::vector<std::string> ids;
+  std::vector<double> K;  // [n, n]
+};
+GrmFile load_grm(const std::string& prefix);
+std::vector<double> slice_grm(const GrmFile& g, const std::vector<std::string>& samples);
+void write_grm(const std::string& prefix, const std::vector<std::string>& ids, const std::vector<double>& K,
+               const std::vector<int32_t>& N_packed);
+
+// --------------------------------------------------------------- statistics
+double acat_p(double tan_sum, int used);                       // AcatAcc::p
+std::vector<double> bh_adjust(const std::vector<double>& p);   // src/scan_common.cpp:201-217
+void inverse_normal_transform(std::vector<double>& y);         // src/util.cpp:132-206
+uint32_t fnv1a32(const std::string& s);
+uint32_t perm_seed(int seed_opt, int b, const std::string& gene);
+double p_emp(double T_obs, const std::vector<double>& T_perm);
+struct BetaFit {
+  double p = NAN, s1 = NAN, s2 = NAN;
+};
+BetaFit beta_approx(const std::vector<double>& perm_min_p, double obs_min_p);
+
+// -------------------------------------------------------------------- output
+struct PairRow {
+  std::string gene, snp, chrom, ref, alt;
+  int64_t pos = 0;
+  double af = 0, beta = 0, se = 0, t = 0, p = 1, r2 = 0;
+  int n = 0;
+  bool has_tss = false;
+  double tss_dist = 0;
+};
+struct RegionRow {
+  std::string gene, chrom;
+  int64_t tss = 0;
+  int n_tested = 0, n_sig = 0;
+  double acat = 1.0, q = NAN, p_emp = NAN, p_beta = NAN, s1 = 0, s2 = 0;
+};
+struct ScopeFiles {
+  FILE* pairs = nullptr;
+  FILE* top = nullptr;
+  FILE* region = nullptr;
+  ScopeFiles(const std::string& prefix);
+  ~ScopeFiles();
+};
+void write_pair(FILE* f, const PairRow& r, const std::string& scope);
+void write_region(FILE* f, const RegionRow& r);
+
+}  // namespace eqtl_host

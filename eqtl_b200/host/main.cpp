@@ -1,0 +1,165 @@
+// eqtl: the reference program's command line (src/main.cpp, src/scan.cpp)
+// for PLINK input and the LM / LMM models, with every scan run on the B200
+// through libeqtl_cuda. The orchestration follows run_eqtl_geno
+// (src/scan.cpp:50-312): analysis samples = phenotype samples present in the
+// .fam, in phenotype order; one GRM (computed or -k) shared by the LMM
+// scopes; per (model, scope) the pairs / top / region files; BH over the
+// scope's genes.
+#include <algorithm>
+#include <iostream>
+#include <memory>
+#include <numeric>
+#include <unordered_set>
+
+#include "host.hpp"
+#include "scan.hpp"
+
+namespace eqtl_host {
+
+Device::Device() {
+  if (eqtl_open(0, &ctx) != EQTL_OK || !ctx) die("no usable B200 (eqtl_open failed)");
+}
+Device::~Device() {
+  if (ctx) eqtl_close(ctx);
+}
+void Device::check(int rc, const std::string& what) const {
+  if (rc != EQTL_OK) die(what + ": " + eqtl_last_error(ctx));
+}
+
+namespace {
+
+std::vector<int32_t> sample_columns(const Plink& P, const std::vector<std::string>& samples) {
+  std::unordered_map<std::string, int32_t> at;
+  for (size_t i = 0; i < P.fam_iid.size(); ++i) at.emplace(P.fam_iid[i], static_cast<int32_t>(i));
+  std::vector<int32_t> col;
+  for (const auto& s : samples) col.push_back(at.at(s));
+  return col;
+}
+
+// Phenotype samples that are in the .fam, in phenotype order (intersect_order).
+std::vector<std::string> overlap(const std::vector<std::string>& pheno, const Plink& P) {
+  std::unordered_set<std::string> fam(P.fam_iid.begin(), P.fam_iid.end());
+  std::vector<std::string> out;
+  for (const auto& s : pheno)
+    if (fam.count(s)) out.push_back(s);
+  return out;
+}
+
+int run_make_grm(const Options& opt) {
+  Plink P = read_plink(opt.bfile);
+  std::vector<std::string> samples = P.fam_iid;
+  if (!opt.pheno.empty()) {
+    samples = overlap(load_pheno(opt.pheno).samples, P);
+    if (samples.empty()) die("no overlapping samples for GRM");
+  }
+  Device dev;
+  Genotypes geno(dev, P, sample_columns(P, samples), opt);
+  const int n = static_cast<int>(samples.size());
+  std::vector<double> K(static_cast<size_t>(n) * n);
+  std::vector<int32_t> N(static_cast<size_t>(n) * (n + 1) / 2);
+  int64_t m_used = 0;
+  dev.check(eqtl_grm(dev.ctx, K.data(), N.data(), &m_used), "GRM");
+  write_grm(opt.out, samples, K, N);
+  info("wrote GRM " + opt.out + ".grm.id/.grm.bin/.grm.N.bin (" + std::to_string(m_used) + " SNPs)");
+  return 0;
+}
+
+int run_scan(const Options& opt) {
+  Plink P = read_plink(opt.bfile);
+  Pheno ph = load_pheno(opt.pheno);
+  Study st;
+  st.opt = &opt;
+  st.plink = &P;
+  st.samples = overlap(ph.samples, P);
+  if (st.samples.empty()) die("no overlapping samples between pheno and genotypes");
+  const size_t n = st.samples.size(), G = ph.genes.size();
+  {
+    std::unordered_map<std::string, size_t> row;
+    for (size_t i = 0; i < ph.samples.size(); ++i) row.emplace(ph.samples[i], i);
+    st.genes = ph.genes;
+    st.Y.resize(n * G);  // gene-major [G][n]
+    for (size_t i = 0; i < n; ++i) {
+      const double* r = &ph.Y[row.at(st.samples[i]) * G];
+      for (size_t g = 0; g < G; ++g) st.Y[g * n + i] = r[g];
+    }
+  }
+  st.X = load_covar(opt.covar, st.samples, st.p);
+  const bool have_gff = !opt.gff.empty();
+  if (have_gff) {
+    st.annot = load_gff(opt.gff, opt.gff_id_key);
+    size_t matched = 0;
+    for (const auto& g : st.genes) matched += st.annot.count(g);
+    info("pheno genes matched to GFF: " + std::to_string(matched) + "/" + std::to_string(G));
+    if (matched == 0) die("no phenotype gene IDs match the GFF annotation (check --gff-id-key and ID format)");
+  } else {
+    info("no GFF: mode ignored; genome-wide all-pairs (gw)");
+  }
+  std::vector<std::string> scopes;
+  if (!have_gff) scopes = {"gw"};
+  else if (opt.mode == "all") scopes = {"cis", "trans"};
+  else scopes = {opt.mode};
+  {
+    const std::string probe = opt.out + ".probe";
+    FILE* f = std::fopen(probe.c_str(), "w");
+    if (!f) die("cannot write to output prefix: " + opt.out);
+    std::fclose(f);
+    std::remove(probe.c_str());
+  }
+
+  Device dev;
+  Genotypes geno(dev, P, sample_columns(P, st.samples), opt);
+  st.dev = &dev;
+  st.geno = &geno;
+  if (std::find(opt.models.begin(), opt.models.end(), "lmm") != opt.models.end()) {
+    // the permutations rebuild LMM phenotypes through the basis on the host
+    if (opt.perm > 0) {
+      st.basis_Q.resize(n * n);
+      st.basis_lambda.resize(n);
+    }
+    double* lam = opt.perm > 0 ? st.basis_lambda.data() : nullptr;
+    double* Q = opt.perm > 0 ? st.basis_Q.data() : nullptr;
+    if (!opt.grm.empty()) {
+      std::vector<double> K = slice_grm(load_grm(opt.grm), st.samples);
+      dev.check(eqtl_lmm_basis(dev.ctx, K.data(), static_cast<int32_t>(n), lam, Q), "LMM basis");
+    } else {
+      info("computing GRM from genotypes (overlap samples)");
+      dev.check(eqtl_lmm_basis(dev.ctx, nullptr, static_cast<int32_t>(n), lam, Q), "LMM basis");
+    }
+  }
+  for (const auto& model : opt.models) {
+    for (const auto& scope : scopes) {
+      ScopeFiles out(opt.out + "." + model + "." + scope);
+      std::vector<RegionRow> regions;
+      if (scope == "cis") run_cis(st, model, out, regions);
+      else run_trans(st, model, scope, out, regions);
+      std::vector<double> acat;
+      for (const auto& r : regions) acat.push_back(r.acat);
+      const std::vector<double> q = bh_adjust(acat);
+      for (size_t i = 0; i < regions.size(); ++i) {
+        regions[i].q = q[i];
+        write_region(out.region, regions[i]);
+      }
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+}  // namespace eqtl_host
+
+int main(int argc, char** argv) {
+  using namespace eqtl_host;
+  try {
+    Options opt;
+    const int rc = parse_options(argc, argv, opt);
+    if (rc == 2) return 0;
+    if (rc != 0) return 1;
+    return opt.make_grm ? run_make_grm(opt) : run_scan(opt);
+  } catch (const Fatal& e) {
+    std::cerr << "[E] " << e.what() << '\n';
+    return 1;
+  } catch (const std::exception& e) {
+    std::cerr << "[E] " << e.what() << '\n';
+    return 1;
+  }
+}

@@ -1,0 +1,335 @@
+// Per-(model, scope) drivers. Both scopes run one device scan over all the
+// scope's genes:
+//   trans/gw   scan_lm_snp_outer / scan_lmm_snp_outer (src/scan_trans_lm.cpp:41-163,
+//              src/scan_trans_lmm.cpp:82-251): genes with a GFF location
+//              (trans; gw also takes genes without one), trans skipping each
+//              gene's cis window; pairs sorted by (SNP, gene).
+//   cis        the gene-outer cis scan (include/eqtl/scan_cis.hpp:15-185,
+//              src/scan_cis.cpp:18-163): only the SNPs inside each gene's
+//              window [max(start - w, 1), end + w]; pairs per gene in gene
+//              order (GFF position order when -t > 1, as the reference's
+//              per-thread scan writes them), SNPs in .bim order.
+// Per gene: n_tested, n_sig, ACAT and the best SNP (strict <, first index
+// on ties) come from the device; the printed statistics of every pair are
+// the device's FP64 refinement.
+#include <algorithm>
+#include <numeric>
+
+#include "perm.hpp"
+
+namespace eqtl_host {
+
+Genotypes::Genotypes(const Device& d, const Plink& P, const std::vector<int32_t>& sample_col, const Options& opt)
+    : dev(d), n(static_cast<int>(sample_col.size())) {
+  const int64_t m = static_cast<int64_t>(P.chrom.size());
+  std::vector<uint8_t> keep(m);
+  std::vector<double> af(m);
+  std::vector<int32_t> nm(m);
+  int64_t n_kept = 0;
+  dev.check(eqtl_geno_load_bed(dev.ctx, P.rows.data(), m, P.bytes_per_snp, P.n_file, sample_col.data(), n,
+                               opt.miss_filter ? EQTL_MISS_FILTER : EQTL_MISS_IMPUTE, opt.max_miss, opt.maf,
+                               keep.data(), af.data(), nm.data(), &n_kept),
+            "genotype decode");
+  for (int64_t s = 0; s < m; ++s)
+    if (keep[s]) kept.push_back(s);
+  info("genotypes: " + std::to_string(n_kept) + "/" + std::to_string(m) + " SNPs kept on " + std::to_string(n) +
+       " samples");
+}
+
+std::unordered_map<int64_t, double> Genotypes::af(std::vector<int64_t> idx) const {
+  std::sort(idx.begin(), idx.end());
+  idx.erase(std::unique(idx.begin(), idx.end()), idx.end());
+  std::unordered_map<int64_t, double> out;
+  const size_t chunk = 4096;
+  std::vector<double> d;
+  for (size_t a = 0; a < idx.size(); a += chunk) {
+    const size_t k = std::min(chunk, idx.size() - a);
+    d.resize(k * n);
+    dev.check(eqtl_geno_dosage_rows(dev.ctx, idx.data() + a, static_cast<int64_t>(k), d.data()), "dosage rows");
+    for (size_t r = 0; r < k; ++r) {
+      double sum = 0.0;
+      for (int i = 0; i < n; ++i) sum += d[r * n + i];
+      double f = (sum / static_cast<double>(n)) / 2.0;
+      f = std::min(std::max(f, 0.0), 1.0);
+      out.emplace(idx[a + r], f);
+    }
+  }
+  return out;
+}
+
+namespace {
+
+struct Job {
+  int gene = 0;                  // column of the phenotype matrix
+  const GeneLoc* loc = nullptr;  // null in gw scope without a location
+};
+
+// Complete-case sample set of one gene (build_gene_ready, src/scan_common.cpp:
+// 11-70): finite phenotype and covariates; fewer than 3 samples or an all-zero
+// phenotype leave the gene out. The device scans take the shared-keep case:
+// every kept gene must keep every analysis sample.
+bool gene_ready(const Study& st, const std::vector<double>& y, bool checks) {
+  const size_t n = st.samples.size();
+  size_t kept = 0;
+  double mx = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    bool ok = std::isfinite(y[i]);
+    for (int j = 0; j < st.p && ok; ++j) ok = std::isfinite(st.X[static_cast<size_t>(j) * n + i]);
+    if (ok) {
+      ++kept;
+      mx = std::max(mx, std::fabs(y[i]));
+    }
+  }
+  if (kept != n)
+    die("phenotype or covariate values missing for some samples: the device scans take the case where every "
+        "gene keeps every analysis sample");
+  if (!checks) return true;
+  return kept >= 3 && !(mx < 1e-15);
+}
+
+std::vector<double> gene_y(const Study& st, int g) {
+  const size_t n = st.samples.size();
+  std::vector<double> y(st.Y.begin() + static_cast<size_t>(g) * n, st.Y.begin() + static_cast<size_t>(g + 1) * n);
+  if (st.opt->pheno_int) inverse_normal_transform(y);
+  return y;
+}
+
+// One device scan over `jobs`; mode 0 gw, 1 trans (exclude windows), 2 cis.
+ScanResult device_scan(const Study& st, const std::string& model, const std::vector<Job>& jobs, int mode,
+                       double pthr, double perm_thr) {
+  const Options& opt = *st.opt;
+  const size_t n = st.samples.size(), J = jobs.size();
+  ScanResult R;
+  R.n = static_cast<int>(n);
+  std::vector<double> Y(J * n);
+  for (size_t j = 0; j < J; ++j) {
+    const std::vector<double> y = gene_y(st, jobs[j].gene);
+    std::copy(y.begin(), y.end(), Y.begin() + j * n);
+  }
+  // gene windows and the kept SNPs' positions, chromosomes by normalised name
+  std::unordered_map<std::string, int32_t> cid;
+  auto chrom_id = [&](const std::string& c) {
+    return cid.emplace(chrom_key(c), static_cast<int32_t>(cid.size())).first->second;
+  };
+  const auto& kept = st.geno->kept;
+  std::vector<int32_t> gchr(J, -1), schr(kept.size());
+  std::vector<int64_t> glo(J, 0), ghi(J, -1), spos(kept.size());
+  for (size_t k = 0; k < kept.size(); ++k) {
+    schr[k] = chrom_id(st.plink->chrom[kept[k]]);
+    spos[k] = st.plink->pos[kept[k]];
+  }
+  for (size_t j = 0; j < J; ++j)
+    if (jobs[j].loc) {
+      gchr[j] = chrom_id(jobs[j].loc->chrom);
+      glo[j] = std::max<int64_t>(jobs[j].loc->start - opt.window, 1);
+      ghi[j] = jobs[j].loc->end + opt.window;
+    }
+  eqtl_scan_params prm{};
+  prm.n = static_cast<int32_t>(n);
+  prm.n_genes = static_cast<int32_t>(J);
+  prm.p = st.p;
+  prm.exclude_cis = mode;
+  prm.pthr = pthr;
+  prm.perm_thr = perm_thr;
+  if (mode != 0) {
+    prm.gene_chrom = gchr.data();
+    prm.gene_lo = glo.data();
+    prm.gene_hi = ghi.data();
+    prm.snp_chrom = schr.data();
+    prm.snp_pos = spos.data();
+  }
+  R.genes.resize(J);
+  R.delta.assign(J, 0.0);
+  int64_t cap = 1 << 18, ccap = perm_thr > 0 ? (1 << 18) : 1;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    R.pairs.resize(static_cast<size_t>(cap));
+    R.cands.resize(static_cast<size_t>(ccap));
+    int64_t np = 0, nc = 0;
+    const int rc = model == "lm"
+                       ? eqtl_scan_trans_lm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.genes.data(), R.pairs.data(),
+                                            cap, &np, R.cands.data(), ccap, &nc)
+                       : eqtl_scan_trans_lmm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.delta.data(),
+                                             R.genes.data(), R.pairs.data(), cap, &np, R.cands.data(), ccap, &nc);
+    if (rc == EQTL_E_OVERFLOW) {
+      cap = std::max(cap, np);
+      ccap = std::max(ccap, nc);
+      continue;
+    }
+    st.dev->check(rc, model + " scan");
+    R.pairs.resize(static_cast<size_t>(np));
+    R.cands.resize(static_cast<size_t>(nc));
+    return R;
+  }
+  die("scan output did not fit after resizing");
+}
+
+PairRow make_row(const Study& st, const std::string& gene, const GeneLoc* loc, int64_t kept_idx, double af,
+                 double beta, double se, double t, double p, double r2, int n) {
+  const int64_t s = st.geno->kept[kept_idx];
+  const Plink& P = *st.plink;
+  PairRow r;
+  r.gene = gene;
+  r.snp = !P.id[s].empty() ? P.id[s] : P.chrom[s] + ":" + std::to_string(P.pos[s]) + ":" + P.a2[s] + ":" + P.a1[s];
+  r.chrom = P.chrom[s];
+  r.pos = P.pos[s];
+  r.ref = P.a2[s];
+  r.alt = P.a1[s];
+  r.af = af;
+  r.beta = beta;
+  r.se = se;
+  r.t = t;
+  r.p = p;
+  r.r2 = r2;
+  r.n = n;
+  if (loc) {
+    r.has_tss = true;
+    r.tss_dist = static_cast<double>(P.pos[s] - loc->tss);
+  }
+  return r;
+}
+
+// Writes pairs (in `order`), tops and region rows of one device scan.
+void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const std::string& scope, double pthr,
+          const std::vector<size_t>& pair_order, ScopeFiles& out, std::vector<RegionRow>& regions,
+          const std::vector<PermOut>* perms) {
+  std::vector<int64_t> need;
+  for (const auto& q : R.pairs) need.push_back(q.snp);
+  for (const auto& g : R.genes)
+    if (g.best_snp >= 0 && g.best_p <= pthr) need.push_back(g.best_snp);
+  const auto af = st.geno->af(need);
+  std::vector<int> n_sig(jobs.size(), 0);
+  for (size_t k : pair_order) {
+    const eqtl_pair& q = R.pairs[k];
+    const Job& jb = jobs[q.gene];
+    ++n_sig[q.gene];
+    write_pair(out.pairs, make_row(st, st.genes[jb.gene], jb.loc, q.snp, af.at(q.snp), q.beta, q.se, q.t, q.p, q.r2, R.n),
+               scope);
+  }
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const eqtl_gene_result& g = R.genes[j];
+    const Job& jb = jobs[j];
+    RegionRow rr;
+    rr.gene = st.genes[jb.gene];
+    if (jb.loc) {
+      rr.chrom = jb.loc->chrom;
+      rr.tss = jb.loc->tss;
+    }
+    rr.n_tested = g.n_tested;
+    rr.n_sig = n_sig[j];
+    rr.acat = acat_p(g.acat_tan_sum, g.acat_used);
+    if (perms && (*perms)[j].done) {
+      rr.p_emp = (*perms)[j].p_emp;
+      rr.p_beta = (*perms)[j].beta.p;
+      rr.s1 = (*perms)[j].beta.s1;
+      rr.s2 = (*perms)[j].beta.s2;
+    }
+    regions.push_back(rr);
+    if (g.best_snp >= 0 && g.best_p <= pthr && g.best_p <= 1.0)
+      write_pair(out.top,
+                 make_row(st, rr.gene, jb.loc, g.best_snp, af.at(g.best_snp), g.best_beta, g.best_se, g.best_t,
+                          g.best_p, g.best_r2, R.n),
+                 scope);
+  }
+}
+
+}  // namespace
+
+void run_trans(const Study& st, const std::string& model, const std::string& scope, ScopeFiles& out,
+               std::vector<RegionRow>& regions) {
+  const Options& opt = *st.opt;
+  const bool have_gff = !opt.gff.empty();
+  std::vector<Job> jobs;
+  for (size_t g = 0; g < st.genes.size(); ++g) {
+    Job jb;
+    jb.gene = static_cast<int>(g);
+    if (have_gff) {
+      auto it = st.annot.find(st.genes[g]);
+      if (it != st.annot.end()) jb.loc = &it->second;
+      else if (scope != "gw") continue;
+    }
+    if (scope == "trans" && !jb.loc) continue;
+    if (!gene_ready(st, gene_y(st, jb.gene), true)) continue;
+    jobs.push_back(jb);
+  }
+  info(std::string(scope) + " " + model + ": " + std::to_string(jobs.size()) + " genes");
+  if (jobs.empty()) return;
+  const double pthr = opt.pval_trans;
+  const double perm_thr = opt.perm > 0 ? opt.perm_trans_thr : 0.0;
+  ScanResult R = device_scan(st, model, jobs, scope == "trans" ? 1 : 0, pthr, perm_thr);
+  std::vector<PermOut> perms;
+  if (opt.perm > 0) {
+    std::vector<PermGene> pg(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      pg[j].name = st.genes[jobs[j].gene];
+      pg[j].y = gene_y(st, jobs[j].gene);
+      pg[j].obs_min_p = R.genes[j].best_p;
+      pg[j].active = R.genes[j].n_tested > 0 && R.genes[j].best_snp >= 0 && R.genes[j].best_p < opt.perm_trans_thr;
+    }
+    // stage-2 SNPs: each gene's top-K candidates by nominal p (p < perm_trans_thr)
+    for (const auto& q : R.cands)
+      if (pg[q.gene].active && static_cast<int>(pg[q.gene].snps.size()) < opt.perm_trans_top &&
+          std::isfinite(q.p))
+        pg[q.gene].snps.push_back(q.snp);
+    perms = run_permutations(st, model, pg, R.delta);
+  }
+  std::vector<size_t> order(R.pairs.size());
+  std::iota(order.begin(), order.end(), 0);  // already (SNP, gene)
+  emit(st, jobs, R, scope, pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
+}
+
+void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::vector<RegionRow>& regions) {
+  const Options& opt = *st.opt;
+  std::vector<Job> jobs;
+  for (size_t g = 0; g < st.genes.size(); ++g) {
+    auto it = st.annot.find(st.genes[g]);
+    if (it == st.annot.end()) continue;
+    Job jb;
+    jb.gene = static_cast<int>(g);
+    jb.loc = &it->second;
+    // the LM path applies the complete-case checks; the LMM path with the
+    // shared basis takes the gene as it is (src/scan_cis.cpp:56-63)
+    if (!gene_ready(st, gene_y(st, jb.gene), model == "lm")) continue;
+    jobs.push_back(jb);
+  }
+  if (opt.threads > 1)
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) {
+      return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
+    });
+  info("cis " + model + ": " + std::to_string(jobs.size()) + " genes");
+  if (jobs.empty()) return;
+  const double pthr = opt.pval_cis;
+  ScanResult R = device_scan(st, model, jobs, 2, pthr, 0.0);
+  std::vector<PermOut> perms;
+  if (opt.perm > 0) {
+    std::vector<PermGene> pg(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      pg[j].name = st.genes[jobs[j].gene];
+      pg[j].y = gene_y(st, jobs[j].gene);
+      pg[j].obs_min_p = R.genes[j].best_p;
+      pg[j].active = R.genes[j].n_tested > 0;
+    }
+    // every kept SNP inside the gene's window, in .bim order (the subset
+    // gate is applied where the permutations read the dosages)
+    const auto& kept = st.geno->kept;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      const GeneLoc& L = *jobs[j].loc;
+      const int64_t lo = std::max<int64_t>(L.start - opt.window, 1), hi = L.end + opt.window;
+      const std::string key = chrom_key(L.chrom);
+      for (size_t k = 0; k < kept.size(); ++k) {
+        const int64_t s = kept[k];
+        if (st.plink->pos[s] >= lo && st.plink->pos[s] <= hi && chrom_key(st.plink->chrom[s]) == key)
+          pg[j].snps.push_back(static_cast<int64_t>(k));
+      }
+    }
+    perms = run_permutations(st, model, pg, R.delta);
+  }
+  std::vector<size_t> order(R.pairs.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    const eqtl_pair &x = R.pairs[a], &y = R.pairs[b];
+    return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
+  });
+  emit(st, jobs, R, "cis", pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
+}
+
+}  // namespace eqtl_host

@@ -88,6 +88,11 @@ int eqtl_geno_load_bed(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t by
  * [hi - lo, n] (SnpRec.dosage after src/plink_bed.cpp:298-302). */
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);
 
+/* The same for k kept-SNP indices rows[0..k): out [k, n]. The host driver
+ * prints each pair's af from these (subset_maf_or_nan,
+ * src/scan_common.cpp:133-151, sums the dosages in sample order). */
+int eqtl_geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out);
+
 /* Evaluates the Student-t tail the scan epilogues use (K8: the device form of
  * p_from_t, src/util.cpp:259-264, through the df-specific interpolation
  * table) for n values of t at residual df, on the device: -log10 p, the ACAT
@@ -127,7 +132,8 @@ typedef struct {
   int32_t n;             /* samples: rows of Y and X */
   int32_t n_genes;       /* columns of Y */
   int32_t p;             /* covariate columns of X, intercept included */
-  int32_t exclude_cis;   /* 1 = trans scope: skip each gene's cis window */
+  int32_t exclude_cis;   /* scope: 0 = gw (every SNP), 1 = trans (skip each gene's
+                          * cis window), 2 = cis (only each gene's window) */
   double pthr;           /* pairs with p <= pthr are returned */
   double perm_thr;       /* candidates with p < perm_thr are returned (0 = none) */
   const int32_t* gene_chrom; /* [n_genes] chromosome id, -1 = no location */
@@ -220,6 +226,25 @@ int eqtl_lmm_rotate(eqtl_ctx* ctx);
 int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                         double* delta_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
                         int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
+
+/* -------------------------------------------------------------- pair tests
+ * FP64 tests of explicit (column of Y, kept SNP) pairs with the scans' own
+ * per-column prep: LM (EQTL_MODEL_LM) residualises each column on X
+ * (prep_lm, src/model_lm.cpp:19-30); LMM (EQTL_MODEL_LMM) runs the full null
+ * fit of each column with the resident eigenbasis, REML delta included
+ * (prep_lmm, src/model_lmm.cpp:124-153). This is test_one_p with a fresh
+ * prep_null per column, the inner loop of the gene-level permutations
+ * (include/eqtl/scan_cis.hpp:150-163, src/scan_perm.cpp:118-126): the host
+ * passes the permuted phenotypes as columns. out[i] gets beta, se, t, p, r2
+ * of pair i; p is NaN when the SNP fails the subset gate on the analysis
+ * samples (src/scan_common.cpp:133-151), which the reference never tests.
+ * delta_out [n_genes] (LMM, may be NULL) receives each column's delta. Only
+ * prm->n, n_genes and p are read. */
+#define EQTL_MODEL_LM 0
+#define EQTL_MODEL_LMM 1
+int eqtl_test_pairs(eqtl_ctx* ctx, int32_t model, const eqtl_scan_params* prm, const double* Y, const double* X,
+                    const int32_t* pair_col, const int64_t* pair_snp, int64_t n_pairs, eqtl_pair* out,
+                    double* delta_out);
 
 #ifdef __cplusplus
 }

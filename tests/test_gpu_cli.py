@@ -1,0 +1,114 @@
+"""The eqtl host program (eqtl_b200/bin/eqtl) against outputs of the reference
+program itself (tests/golden/): the same command lines, every pairs / top /
+region file and the GCTA GRM files.
+
+Tolerances: LM pairs carry the FP64 refinement (log10 p within 1e-5, beta
+within 1e-6 relative); LMM adds the REML optimiser difference (1e-4 and
+1e-5). ACAT p uses the condition-aware bound of the parity tests (1e-3 plus
+3 |dlog10 acat / dt| times the screening error of t, from the oracle).
+Permutation p_emp is exact for the LM (same seeded shuffles, FP64 tests);
+for the LMM the permuted phenotypes live in the eigenbasis, whose eigenvector
+signs differ between Eigen and cuSOLVER, so p_emp / p_beta agree in
+distribution only and are checked for presence."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import driver
+import refargs
+import tsvcmp
+from gpu_util import T_ERR
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+BIN = os.path.join(os.path.dirname(GOLD), "..", "eqtl_b200", "bin", "eqtl")
+
+
+def _runs():
+    out = []
+    for c in sorted(os.listdir(GOLD)):
+        if not os.path.isdir(os.path.join(GOLD, c)):
+            continue
+        man = json.load(open(os.path.join(GOLD, c, "manifest.json")))
+        for tag, r in man["runs"].items():
+            out.append((c, tag, r["argv"]))
+    return out
+
+
+def _run(argv, case_dir, out_prefix):
+    a = list(argv)
+    a[a.index("-o") + 1] = out_prefix
+    r = subprocess.run([os.path.abspath(BIN)] + a, cwd=case_dir, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" in r[2]])
+def test_cli_make_grm(case, tag, argv, tmp_path):
+    d = os.path.join(GOLD, case)
+    out = str(tmp_path / "out")
+    _run(argv, d, out)
+    ref = os.path.join(d, f"ref_{tag}")
+    assert open(out + ".grm.id").read() == open(ref + ".grm.id").read()
+    N, Nr = (np.fromfile(p + ".grm.N.bin", dtype=np.float32) for p in (out, ref))
+    assert np.array_equal(N, Nr)
+    K, Kr = (np.fromfile(p + ".grm.bin", dtype=np.float32) for p in (out, ref))
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=2e-6 * np.abs(Kr).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" not in r[2]])
+def test_cli_scan_matches_reference(case, tag, argv, tmp_path):
+    d = os.path.join(GOLD, case)
+    out = str(tmp_path / "out")
+    _run(argv, d, out)
+    opt = refargs.options_from_argv(argv, d)
+    ora = driver.Scanner(opt)
+    ora.run()                                    # per-gene ACAT sensitivities
+    scopes = ["gw"] if not opt.gff else {"cis": ["cis"], "trans": ["trans"], "gw": ["gw"],
+                                         "all": ["cis", "trans"]}[opt.mode]
+    errs = []
+    for model in opt.out_models:
+        tol = tsvcmp.Tol(log10p=1e-5, beta_rel=1e-6) if model == "lm" else tsvcmp.Tol(log10p=1e-4, beta_rel=1e-5)
+        for scope in scopes:
+            ref, got = os.path.join(d, f"ref_{tag}.{model}.{scope}"), f"{out}.{model}.{scope}"
+            pthr = opt.pval_cis if scope == "cis" else opt.pval_trans
+            for kind in ("pairs", "top"):
+                hr, rr = tsvcmp.read_tsv(f"{ref}.{kind}.tsv")
+                hg, gg = tsvcmp.read_tsv(f"{got}.{kind}.tsv")
+                assert hr == hg
+                errs += [f"{model}.{scope} {kind}: {e}" for e in tsvcmp.compare_pairs(rr, gg, tol, pthr)]
+            hr, rr = tsvcmp.read_tsv(f"{ref}.region.tsv")
+            hg, gg = tsvcmp.read_tsv(f"{got}.region.tsv")
+            assert hr == hg
+            exact_perm = model == "lm"
+            errs += [f"{model}.{scope} region: {e}" for e in
+                     tsvcmp.compare_region(rr, gg, tsvcmp.Tol(log10p=1e-3), check_perm=exact_perm,
+                                           acat_sens=ora.sens, t_err=T_ERR)]
+            if not exact_perm:
+                R = {r[0]: r for r in rr}
+                for g in gg:
+                    if g[0] in R and R[g[0]][7] != "NA":
+                        assert g[7] != "NA", (model, scope, g[0])
+            # the gene order of each file is the reference's
+            assert [r[0] for r in rr] == [g[0] for g in gg], (model, scope)
+    assert not errs, "\n".join(errs[:40])
+
+
+def test_cli_help_and_refusals():
+    """Host-only behaviour of the command line (no GPU needed)."""
+    exe = os.path.abspath(BIN)
+    if not os.path.exists(exe):
+        pytest.skip("eqtl_b200/bin/eqtl not built")
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--pval-cis" in r.stdout
+    r = subprocess.run([exe, "-v", "x.vcf.gz", "-e", "p.tsv"], capture_output=True, text=True)
+    assert r.returncode == 1 and "VCF" in r.stderr
+    r = subprocess.run([exe, "-b", "geno"], capture_output=True, text=True)
+    assert r.returncode == 1 and "missing -e/--pheno" in r.stderr
+    r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--model", "glm"], capture_output=True, text=True)
+    assert r.returncode == 1 and "glm" in r.stderr
+    r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--maf", "0.7"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--maf must be in [0,0.5]" in r.stderr
