@@ -95,6 +95,7 @@ struct GrmEpiParams {
 };
 
 struct GrmEpi {
+  static constexpr bool kGrouped = false;
   using Params = GrmEpiParams;
   const Params& P;
   int row = 0;

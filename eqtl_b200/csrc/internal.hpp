@@ -119,7 +119,7 @@ struct PhenoDev {
 // Per-call workspaces reused across calls (capacity grows, never shrinks).
 struct Workspace {
   DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
-  DevBuf<__half> ops_hi[4], ops_lo[4];
+  DevBuf<__half> ops_hi[20], ops_lo[20];  // gene-side operands, one per accumulator
   DevBuf<__half*> ops_ptr;
   DevBuf<float> unscale, gscale;
   DevBuf<uint8_t> ok;

@@ -50,6 +50,7 @@ struct RotEpiParams {
 };
 
 struct RotEpi {
+  static constexpr bool kGrouped = false;
   using Params = RotEpiParams;
   const Params& P;
   int row = 0;
@@ -372,6 +373,7 @@ struct LmmEpiParams {
 
 template <int P>
 struct LmmEpi {
+  static constexpr bool kGrouped = false;
   using Params = LmmEpiParams<P>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
@@ -435,6 +437,174 @@ struct LmmEpi {
       const float omr = 1.0f - r;
       const bool ok_stat = !(gg < 1e-12f) && S > 1e-15f && omr > 0.0f;
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
+      const TailOut o = t_tail(t, tt);
+      acc.add_masked(o, s, valid);
+      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred);
+    }
+  }
+  __device__ void end_tile() {
+    if (gvalid) acc.flush(Pr.out, gene);
+  }
+  __device__ void finish() {}
+};
+
+// ---------------------------------------- any number of covariates (p >= 3)
+// With A00 = X~'W X~ and U U' = A00^-1 (Cholesky of the REML kernel's ainv),
+// a' A00^-1 a = |U' a|^2 and U' a = Gt'(w o X~U): each covariate column
+// becomes one plain accumulator a~_k = Gt'(w o (X~U)_k), and
+//     S = gg - sum_k a~_k^2.
+// The p + 2 accumulators [NUM, gg, a~_0 .. a~_{p-1}] exceed what TMEM holds
+// for one tile, so the tile kernel runs them in groups of four; this
+// epilogue keeps NUM and the running S of its 16 pairs across the groups.
+__global__ void lmm_gene_ops_orth_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
+                                         const double* __restrict__ lam, const double* __restrict__ delta,
+                                         const double* __restrict__ chi0, const double* __restrict__ ainv, int n,
+                                         int p, int G, int k_pad, float s1, float s2, __half* const* hi,
+                                         __half* const* lo, float* unscale) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const int nops = p + 2;
+  __shared__ double mx[kMaxPLmm + 2][8];
+  __shared__ double sc[kMaxPLmm + 2];
+  __shared__ double U[kMaxPLmm * kMaxPLmm];  // lower Cholesky factor of ainv[g]
+  if (threadIdx.x == 0) {
+    const double* A = ainv + static_cast<int64_t>(g) * p * p;
+    for (int j = 0; j < p; ++j) {
+      double d = A[j * p + j];
+      for (int k = 0; k < j; ++k) d -= U[j * p + k] * U[j * p + k];
+      d = d > 0 ? sqrt(d) : 0.0;  // A00 is positive definite wherever REML succeeded
+      U[j * p + j] = d;
+      for (int i = j + 1; i < p; ++i) {
+        double v = A[i * p + j];
+        for (int k = 0; k < j; ++k) v -= U[i * p + k] * U[j * p + k];
+        U[i * p + j] = d > 0 ? v / d : 0.0;
+      }
+      for (int i = 0; i < j; ++i) U[i * p + j] = 0.0;
+    }
+  }
+  __syncthreads();
+  const double d = delta[g];
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  const double* c0 = chi0 + static_cast<int64_t>(g) * p;
+  auto value = [&](int op, int i) -> double {
+    if (i >= n) return 0.0;
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    if (op == 1) return w;
+    double r = 0;
+    if (op == 0) {
+      r = yt[i];
+      for (int k = 0; k < p; ++k) r -= Xtil[static_cast<int64_t>(k) * n + i] * c0[k];
+    } else {
+      const int k = op - 2;
+      for (int l = k; l < p; ++l) r += Xtil[static_cast<int64_t>(l) * n + i] * U[l * p + k];
+    }
+    return w * r;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int op = 0; op < nops; ++op) {
+    double m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(value(op, i)));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) mx[op][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < nops) {
+    double m = 0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) m = fmax(m, mx[threadIdx.x][w]);
+    int e = 0;
+    if (m > 0) e = 10 - static_cast<int>(floor(log2(m)));
+    sc[threadIdx.x] = ldexp(1.0, e);
+    const double side = threadIdx.x == 1 ? s2 : s1;  // gg pairs with Gt^2, the rest with Gt
+    unscale[static_cast<int64_t>(g) * nops + threadIdx.x] = static_cast<float>(1.0 / (ldexp(1.0, e) * side));
+  }
+  __syncthreads();
+  for (int op = 0; op < nops; ++op) {
+    const double s = sc[op];
+    for (int i = threadIdx.x; i < k_pad; i += blockDim.x) {
+      const double v = value(op, i) * s;
+      const __half h = __double2half(v);
+      hi[op][static_cast<int64_t>(g) * k_pad + i] = h;
+      lo[op][static_cast<int64_t>(g) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+    }
+  }
+}
+
+struct LmmGroupEpiParams {
+  int G;
+  int64_t m;
+  int n_acc;                // p + 2
+  const float* unscale;     // [G][n_acc]: NUM, gg, a~_0 .. a~_{p-1}
+  const double* rss_null;   // [G]
+  const uint8_t* snp_ok;    // [m]
+  Windows win;
+  float df;
+  float t_cand;
+  TTable tt;
+  GeneOut out;
+};
+
+struct LmmGroupEpi {
+  static constexpr bool kGrouped = true;
+  static constexpr int kTileN = 64;  // one 16-column chunk per epilogue thread
+  using Params = LmmGroupEpiParams;
+  static constexpr int kSmemBytes = kTTableSmemBytes;
+  const Params& Pr;
+  float* tsm;
+  TTable tt;
+  int gene = 0;
+  int64_t snp0 = 0;
+  bool gvalid = false;
+  float inv_rss = 0;
+  float num[16], S[16];
+  GeneAcc acc;
+  __device__ LmmGroupEpi(const Params& p, const TileShape&, uint8_t* smem)
+      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+  __device__ void init(int tid, int nthr) {
+    if (tsm) tt = ttable_to_smem(Pr.tt, tsm, tid, nthr);
+  }
+  __device__ void begin_tile(int g, int64_t s0) {
+    gene = g;
+    snp0 = s0;
+    gvalid = g < Pr.G;
+    acc.reset();
+    if (gvalid) {
+      const double r = Pr.rss_null[g];
+      inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
+      acc.load_window(Pr.win, g);
+    }
+  }
+  // accumulator j of this tile for the 16 columns at c
+  __device__ void acc_chunk(int j, int c, const float (&v)[16]) {
+    if (!gvalid) return;
+    const float us = Pr.unscale[static_cast<int64_t>(gene) * Pr.n_acc + j];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const float x = v[i] * us;
+      if (j == 0) {
+        num[i] = x;
+      } else if (j == 1) {
+        S[i] = x < 1e-12f ? -INFINITY : x;  // gg < 1e-12: p = 1
+      } else {
+        S[i] = fmaf(-x, x, S[i]);
+      }
+    }
+  }
+  // after the last group: the 16 pairs' t, tail and per-gene updates
+  __device__ void finish_chunk(int c) {
+    const int64_t s0 = snp0 + c;
+    if (!gvalid || s0 >= Pr.m) return;
+    uint32_t okw[4];
+    load_flags16(Pr.snp_ok + s0, okw);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t s = s0 + j;
+      const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
+      const float r = num[j] * __fdividef(num[j], S[j]) * inv_rss;
+      const float omr = 1.0f - r;
+      const bool ok_stat = S[j] > 1e-15f && omr > 0.0f;
+      const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num[j]) : 0.0f;
       const TailOut o = t_tail(t, tt);
       acc.add_masked(o, s, valid);
       if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred);
@@ -537,6 +707,10 @@ struct EpiOf<dev::LmmEpiParams<1>> {
 template <>
 struct EpiOf<dev::LmmEpiParams<2>> {
   using type = dev::LmmEpi<2>;
+};
+template <>
+struct EpiOf<dev::LmmGroupEpiParams> {
+  using type = dev::LmmGroupEpi;
 };
 
 using namespace dev;
@@ -809,8 +983,10 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_trans_lmm: no genotypes loaded");
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lmm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_trans_lmm: no genes");
-  EQTL_CHECK(p >= 1 && p <= 2, EQTL_E_UNSUPPORTED,
-             "the tensor-core LMM scan handles 1 or 2 covariate columns (p + 2 <= 4 TMEM accumulators)");
+  EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED,
+             "the LMM scan handles 1 to 16 covariate columns (intercept included)");
+  EQTL_CHECK(!(simt && p > 2), EQTL_E_UNSUPPORTED, "the FP32 CUDA-core comparator covers 1 or 2 covariate columns");
+  const bool grouped = p > 2;  // accumulators run in groups of four (LmmGroupEpi)
   cudaStream_t st = ctx->stream;
   const double df = static_cast<double>(n - p - 1);
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
@@ -834,8 +1010,13 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   DevBuf<float>& unscale = ws.unscale;
   unscale.alloc(static_cast<size_t>(G) * nops);
   ++ctx->launches;
-  lmm_gene_ops_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
-                                         k_pad, s1, s2, ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
+  if (grouped)
+    lmm_gene_ops_orth_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p,
+                                                ws.ainv.p, n, p, G, k_pad, s1, s2, ws.ops_ptr.p,
+                                                ws.ops_ptr.p + nops, unscale.p);
+  else
+    lmm_gene_ops_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
+                                           k_pad, s1, s2, ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
   EQTL_CUDA(cudaGetLastError());
 
   const int64_t m = g.m;
@@ -848,7 +1029,29 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   prep_timer.reset();
   ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
   std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
-  if (m > 0) {
+  if (m > 0 && grouped) {
+    Rotated& Rt = ctx->rot;
+    LmmGroupEpiParams ep{};
+    ep.G = G;
+    ep.m = m;
+    ep.n_acc = nops;
+    ep.unscale = unscale.p;
+    ep.rss_null = ws.rss.p;
+    ep.snp_ok = ok.p;
+    ep.win = win;
+    ep.df = static_cast<float>(df);
+    ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
+    ep.tt = tt;
+    const __half* bh[2] = {Rt.gt_hi.p, Rt.gt2_hi.p};
+    const __half* bl[2] = {Rt.gt_lo.p, Rt.gt2_lo.p};
+    std::vector<int> bsel(nops, 0), prod(nops, 7);
+    bsel[1] = 1;  // gg reads Gt^2
+    so.run([&](GeneOut out) {
+      ep.out = out;
+      launch_tile_n<LmmGroupEpi::kTileN, 4>(ctx, false, ep, oph.data(), oph.data() + nops, G, bh, bl, Rt.m, Rt.k_pad,
+                                            bsel.data(), prod.data(), nullptr, 0, 1, nops);
+    });
+  } else if (m > 0) {
     const __half* ah[4] = {oph[0], oph[1], oph[2], nops > 3 ? oph[3] : oph[2]};
     const __half* al[4] = {oph[nops + 0], oph[nops + 1], oph[nops + 2], nops > 3 ? oph[nops + 3] : oph[nops + 2]};
     auto fill = [&](auto& ep) {

@@ -86,7 +86,7 @@ template <int NT, int NACC, class EpiParams>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
-                   int n_tile_list = 0, int ksplit = 1);
+                   int n_tile_list = 0, int ksplit = 1, int n_acc = NACC);
 
 }  // namespace eqtl
 
@@ -100,17 +100,19 @@ template <int NT, int NACC, class EpiParams>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
-                   int n_tile_list, int ksplit) {
+                   int n_tile_list, int ksplit, int n_acc) {
   using Epi = typename EpiOf<EpiParams>::type;
   using C = dev::TileCfg<NT, NACC>;
   dev::TileMaps maps;
   std::memset(&maps, 0, sizeof(maps));
-  for (int j = 0; j < NACC; ++j) {
+  EQTL_CHECK(n_acc >= 1 && n_acc <= dev::kMaxAcc && (n_acc == NACC || Epi::kGrouped), EQTL_E_INTERNAL,
+             "tile kernel: accumulator count");
+  for (int j = 0; j < n_acc; ++j) {
     make_map_2d(&maps.a[2 * j], a_hi[j], rows_a, k_pad, dev::kTileM, bf16);
     make_map_2d(&maps.a[2 * j + 1], a_lo[j], rows_a, k_pad, dev::kTileM, bf16);
   }
   int npairs = 0;
-  for (int j = 0; j < NACC; ++j) npairs = std::max(npairs, bsel[j] + 1);
+  for (int j = 0; j < n_acc; ++j) npairs = std::max(npairs, bsel[j] + 1);
   for (int b = 0; b < npairs; ++b) {
     make_map_2d(&maps.b[2 * b], b_hi[b], rows_b, k_pad, NT, bf16);
     make_map_2d(&maps.b[2 * b + 1], b_lo[b], rows_b, k_pad, NT, bf16);
@@ -123,10 +125,11 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   sh.rows_a = static_cast<int>(rows_a);
   sh.rows_b = static_cast<int>(rows_b);
   sh.kchunks = k_pad / dev::kChunkK;
-  sh.n_acc = NACC;
+  sh.n_acc = n_acc;
+  sh.n_groups = (n_acc + NACC - 1) / NACC;
   for (int j = 0; j < dev::kMaxAcc; ++j) {
-    sh.bsel[j] = j < NACC ? bsel[j] : 0;
-    sh.prod[j] = j < NACC ? prod[j] : 0;
+    sh.bsel[j] = j < n_acc ? bsel[j] : 0;
+    sh.prod[j] = j < n_acc ? prod[j] : 0;
   }
   sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
   sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
@@ -138,7 +141,7 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   // gene-side tiles per raster group: keep the group's A operands (hi+lo of
   // every accumulator) within ~48 MB of L2
   {
-    const double a_bytes = static_cast<double>(NACC) * 2.0 * dev::kTileM * k_pad * 2.0;
+    const double a_bytes = static_cast<double>(n_acc) * 2.0 * dev::kTileM * k_pad * 2.0;
     sh.group_a = std::max(1, std::min(sh.tiles_a, static_cast<int>(48e6 / a_bytes)));
   }
   sh.status = ctx->d_status;

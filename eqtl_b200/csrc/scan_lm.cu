@@ -44,6 +44,7 @@ struct LmEpiParams {
 };
 
 struct LmEpi {
+  static constexpr bool kGrouped = false;
   using Params = LmEpiParams;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& P;

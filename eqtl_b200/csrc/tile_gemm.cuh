@@ -23,13 +23,17 @@
 //               matrix to HBM.
 // When NACC*NT <= 256 the accumulators are double-buffered so the epilogue of
 // tile i overlaps the MMAs of tile i+1.
+// A tile may need more accumulators than TMEM holds at once (the LMM with p
+// covariates needs p + 2): they then run in groups of NACC, one after the
+// other on the same CTA, and a grouped epilogue (Epi::kGrouped) receives each
+// accumulator of each group and keeps its per-pair state across the groups.
 #pragma once
 #include "sm100.cuh"
 
 namespace eqtl {
 namespace dev {
 
-constexpr int kMaxAcc = 4;
+constexpr int kMaxAcc = 20;  // accumulators of one tile over all its groups
 constexpr int kEpiWarps = 16;
 constexpr int kTileThreads = 64 + 32 * kEpiWarps;
 constexpr int kTileM = 128;
@@ -44,7 +48,8 @@ struct TileShape {
   int rows_a;             // valid gene-side rows
   int rows_b;             // valid SNP-side rows
   int kchunks;            // K / 64
-  int n_acc;              // == NACC
+  int n_acc;              // accumulators per tile (NACC, or more in groups of NACC)
+  int n_groups;           // ceil(n_acc / NACC): TMEM holds one group at a time
   int bsel[kMaxAcc];      // SNP-side pair used by accumulator j (0 or 1)
   int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi
   int tiles_a;            // ceil(rows_a / 128)
@@ -138,7 +143,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     fence_mbar_init();
   }
   if (warp == 0 && lane == 0) {
-    for (int j = 0; j < 2 * NACC; ++j) tma_prefetch_map(&maps.a[j]);
+    for (int j = 0; j < 2 * sh.n_acc; ++j) tma_prefetch_map(&maps.a[j]);
     for (int j = 0; j < 4; ++j) tma_prefetch_map(&maps.b[j]);
   }
   if (warp == 1) {
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         int ta, tb, k0, k1;
         tile_coords(sh, t, ta, tb, k0, k1);
         const int ra = ta * kTileM, rb = tb * NT;
-        for (int j = 0; j < NACC && ok; ++j) {
+        for (int j = 0; j < sh.n_acc && ok; ++j) {
           const int bp = sh.bsel[j];
           for (int kc = k0; kc < k1; ++kc) {
             if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
@@ -210,51 +215,57 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
         int ta, tb, k0, k1;
         tile_coords(sh, t, ta, tb, k0, k1);
-        if (!mbar_wait(&acce[buf], accphase ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) break;
-        tc_fence_after();
-        const uint32_t dbase = tmem_base + static_cast<uint32_t>(buf * NACC * NT);
-        for (int j = 0; j < NACC && ok; ++j) {
-          const uint32_t d = dbase + static_cast<uint32_t>(j * NT);
-          const int pm = sh.prod[j];
-          for (int kc = k0; kc < k1; ++kc) {
-            if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
-            const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
-            const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
+        for (int grp = 0; grp < sh.n_groups && ok; ++grp) {
+          if (!mbar_wait(&acce[buf], accphase ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t dbase = tmem_base + static_cast<uint32_t>(buf * NACC * NT);
+          const int j_end = min(sh.n_acc, (grp + 1) * NACC);
+          for (int j = grp * NACC; j < j_end && ok; ++j) {
+            const uint32_t d = dbase + static_cast<uint32_t>((j - grp * NACC) * NT);
+            const int pm = sh.prod[j];
+            for (int kc = k0; kc < k1; ++kc) {
+              if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
+              const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
+              const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
 #pragma unroll
-            for (int k = 0; k < kChunkK / 16; ++k) {
-              const uint32_t off = static_cast<uint32_t>(k * 32);
-              uint32_t accum = (kc > k0 || k > 0) ? 1u : 0u;
-              if (pm & 1) {
-                umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-                accum = 1u;
+              for (int k = 0; k < kChunkK / 16; ++k) {
+                const uint32_t off = static_cast<uint32_t>(k * 32);
+                uint32_t accum = (kc > k0 || k > 0) ? 1u : 0u;
+                if (pm & 1) {
+                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                  accum = 1u;
+                }
+                if (pm & 2) {
+                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
+                  accum = 1u;
+                }
+                if (pm & 4) {
+                  umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                }
               }
-              if (pm & 2) {
-                umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
-                accum = 1u;
+              umma_commit(&empty[stage]);
+              if (++stage == C::STAGES) {
+                stage = 0;
+                phase ^= 1u;
               }
-              if (pm & 4) {
-                umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-              }
-            }
-            umma_commit(&empty[stage]);
-            if (++stage == C::STAGES) {
-              stage = 0;
-              phase ^= 1u;
             }
           }
-        }
-        if (!ok) break;
-        umma_commit(&accf[buf]);
-        if (C::NBUF == 2) {
-          buf ^= 1;
-          if (buf == 0) accphase ^= 1u;
-        } else {
-          accphase ^= 1u;
+          if (!ok) break;
+          umma_commit(&accf[buf]);
+          if (C::NBUF == 2) {
+            buf ^= 1;
+            if (buf == 0) accphase ^= 1u;
+          } else {
+            accphase ^= 1u;
+          }
         }
       }
       // Drain: all issued MMAs complete before TMEM is released (bounded).
@@ -281,28 +292,50 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     for (int t = blockIdx.x; t < sh.n_tiles; t += gridDim.x) {
       int ta, tb, k0, k1;
       tile_coords(sh, t, ta, tb, k0, k1);
-      if (!mbar_wait(&accf[buf], accphase, status, abort_flag, kDevTimeoutAccFull)) break;
-      tc_fence_after();
-      const uint32_t tbase =
-          tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buf * NACC * NT);
       epi.begin_tile(ta * kTileM + row, tb * NT);
+      bool eok = true;
+      for (int grp = 0; grp < sh.n_groups; ++grp) {
+        if (!mbar_wait(&accf[buf], accphase, status, abort_flag, kDevTimeoutAccFull)) {
+          eok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tbase =
+            tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buf * NACC * NT);
+        if constexpr (Epi::kGrouped) {
+          const int nv = min(NACC, sh.n_acc - grp * NACC);
 #pragma unroll 1
-      for (int c = 16 * sub; c < NT; c += 16 * kSub) {
-        float v[NACC][16];
+          for (int c = 16 * sub; c < NT; c += 16 * kSub) {
+#pragma unroll 1
+            for (int j = 0; j < nv; ++j) {
+              float v[16];
+              tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v);
+              tmem_wait_ld();
+              epi.acc_chunk(grp * NACC + j, c, v);
+            }
+            if (grp == sh.n_groups - 1) epi.finish_chunk(c);
+          }
+        } else {
+#pragma unroll 1
+          for (int c = 16 * sub; c < NT; c += 16 * kSub) {
+            float v[NACC][16];
 #pragma unroll
-        for (int j = 0; j < NACC; ++j) tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v[j]);
-        tmem_wait_ld();
-        epi.template chunk<NACC>(c, v);
+            for (int j = 0; j < NACC; ++j) tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v[j]);
+            tmem_wait_ld();
+            epi.template chunk<NACC>(c, v);
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&acce[buf]);
+        if (C::NBUF == 2) {
+          buf ^= 1;
+          if (buf == 0) accphase ^= 1u;
+        } else {
+          accphase ^= 1u;
+        }
       }
-      tc_fence_before();
-      mbar_arrive(&acce[buf]);
+      if (!eok) break;
       epi.end_tile();
-      if (C::NBUF == 2) {
-        buf ^= 1;
-        if (buf == 0) accphase ^= 1u;
-      } else {
-        accphase ^= 1u;
-      }
     }
     epi.finish();
   }

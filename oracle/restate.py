@@ -557,11 +557,13 @@ class PrepLmm:
     p: int
 
 
-def prep_lmm(y, X, Q, lam) -> PrepLmm:
-    """src/model_lmm.cpp:124-153."""
+def prep_lmm(y, X, Q, lam, delta=None) -> PrepLmm:
+    """src/model_lmm.cpp:124-153. `delta` given: the null fit at that delta
+    instead of the REML optimum (for checks at another optimiser's delta)."""
     ytil = Q.T @ y
     Xtil = Q.T @ X
-    delta = optimize_delta(ytil, Xtil, lam)
+    if delta is None:
+        delta = optimize_delta(ytil, Xtil, lam)
     dinv = 1.0 / np.maximum(delta * lam + 1.0, 1e-12)
     A00 = (Xtil * dinv[:, None]).T @ Xtil
     Dy = dinv * ytil

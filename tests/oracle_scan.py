@@ -55,12 +55,14 @@ def summarize(st, use, pthr, df):
     return out, pairs
 
 
-def trans_lmm(G_dos, Y, X, Q, lam, pthr, excl=None):
-    """SNP-outer LMM (src/scan_trans_lmm.cpp:82-251) over kept dosages."""
+def trans_lmm(G_dos, Y, X, Q, lam, pthr, excl=None, deltas=None):
+    """SNP-outer LMM (src/scan_trans_lmm.cpp:82-251) over kept dosages;
+    deltas[g] (optional, NaN = optimise) fixes gene g's REML delta."""
     m, n = G_dos.shape
     Gn = Y.shape[1]
     p = X.shape[1]
-    preps = [R.prep_lmm(Y[:, g], X, Q, lam) for g in range(Gn)]
+    fix = (lambda g: None) if deltas is None else (lambda g: None if np.isnan(deltas[g]) else float(deltas[g]))
+    preps = [R.prep_lmm(Y[:, g], X, Q, lam, fix(g)) for g in range(Gn)]
     af, ok = R.subset_maf(G_dos)
     Gt = G_dos @ Q
     cols = [R.lmm_stats_gtil(pp, Gt) for pp in preps]
