@@ -203,6 +203,18 @@ void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& re
   }
 }
 
+void add_acat_terms(eqtl_gene_result* genes, const std::vector<int2>& pairs, const std::vector<double>& p_pairs) {
+  const long double kPiL = 3.14159265358979323846L;
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    double p = p_pairs[i];
+    if (!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12) continue;  // AcatAcc::add guards
+    if (p <= 0.0) p = 1e-300;
+    eqtl_gene_result& g = genes[pairs[i].x];
+    g.acat_tan_sum += static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+    ++g.acat_used;
+  }
+}
+
 dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int mode) {
   dev::Windows w{};
   w.mode = dev::kWinNone;
@@ -347,7 +359,8 @@ void ScanOutputs::run(const std::function<void(dev::GeneOut)>& launch) {
   throw Error(EQTL_E_INTERNAL, "candidate buffer did not converge");
 }
 
-void ScanOutputs::collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred) {
+void ScanOutputs::collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred,
+                          std::vector<int2>* tiny) {
   std::vector<double> a(G);
   std::vector<int> u(G), t(G);
   std::vector<unsigned long long> b(G);
@@ -360,9 +373,14 @@ void ScanOutputs::collect(eqtl_gene_result* genes, std::vector<int2>& todo, std:
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
   todo.clear();
   deferred.clear();
+  if (tiny) tiny->clear();
   for (const int2& q : c) {
     const uint32_t s = static_cast<uint32_t>(q.y);
-    const int2 clean = make_int2(q.x, static_cast<int>(s & ~dev::kCandDeferred));
+    const int2 clean = make_int2(q.x, static_cast<int>(s & ~(dev::kCandDeferred | dev::kCandTiny)));
+    if (tiny && (s & dev::kCandTiny)) {
+      tiny->push_back(clean);
+      continue;
+    }
     todo.push_back(clean);
     if (s & dev::kCandDeferred) deferred.push_back(clean);
   }

@@ -125,6 +125,7 @@ struct Workspace {
   DevBuf<uint8_t> ok;
   DevBuf<double> graw, gt;
   DevBuf<eqtl_pair> refined;
+  DevBuf<double> tiny_p;
   DevBuf<__half> q_hi, q_lo;  // rotation: split eigenvector operand
   DevBuf<int> ref_snps, ref_col;
   DevBuf<int2> ref_pairs;

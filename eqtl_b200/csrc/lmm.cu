@@ -439,7 +439,7 @@ struct LmmEpi {
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
       const TailOut o = t_tail(t, tt);
       acc.add_masked(o, s, valid);
-      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred);
+      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }
   __device__ void end_tile() {
@@ -607,7 +607,7 @@ struct LmmGroupEpi {
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num[j]) : 0.0f;
       const TailOut o = t_tail(t, tt);
       acc.add_masked(o, s, valid);
-      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred);
+      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }
   __device__ void end_tile() {
@@ -651,7 +651,6 @@ __global__ void raw_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
   }
 }
 
-// per refined pair: gg, yg, a[p] from FP64 rotated raw dosage
 // One warp per (gene, snp) pair from the FP64 rotated raw dosage Gt = Q'g:
 // gg = Gt'W Gt, yg = Gt'W y~, a = X~'W Gt with W = diag(1 / (delta lambda + 1)),
 // then the pair's printed statistics (test_lmm_gtil, src/scan_trans_lmm.cpp:11-40).
@@ -691,6 +690,87 @@ __global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const in
     lmm_stats_fp64(gg, yg, a, chi0 + static_cast<int64_t>(g) * p, ainv + static_cast<int64_t>(g) * p * p, rss[g],
                    p, df, q);
     out[w] = q;
+  }
+}
+
+// ------------------------------------------------- tiny-|t| pairs in FP64
+// Pairs screened with 0 < |t| < tiny_t need an FP64 t only to place them
+// against the reference's x = df / (df + t^2) quantisation and to form their
+// ACAT term; relative accuracy ~1e-8 is ample. So instead of rotating their
+// raw dosages (n^2 per SNP):
+//   NUM = g_raw . u,   u = Q (w o r~) for the gene (one DGEMM per scan),
+//   S   = Gt'W Gt - a'A00^-1 a from the stored FP16 hi/lo rotated genotypes
+//         (centred; S does not see the centring) accumulated in FP64.
+__global__ void lmm_wr_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
+                              const double* __restrict__ lam, const double* __restrict__ delta,
+                              const double* __restrict__ chi0, int n, int p, int G, double* wr) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const double d = delta[g];
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  const double* c0 = chi0 + static_cast<int64_t>(g) * p;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    double r = yt[i];
+    for (int k = 0; k < p; ++k) r -= Xtil[static_cast<int64_t>(k) * n + i] * c0[k];
+    wr[static_cast<int64_t>(g) * n + i] = r / v;
+  }
+}
+
+__global__ void lmm_tiny_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                int n, int k_pad, const int64_t* __restrict__ kept, const double* __restrict__ mu,
+                                const double* __restrict__ U, const __half* __restrict__ gt_hi,
+                                const __half* __restrict__ gt_lo, double inv_s1, const double* __restrict__ Xtil,
+                                int p, const double* __restrict__ lam, const double* __restrict__ delta,
+                                const double* __restrict__ ainv, const double* __restrict__ rss, double df,
+                                const int2* __restrict__ pairs, int n_pairs, double* p_out) {
+  const int lane = threadIdx.x & 31;
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= n_pairs) return;
+  const int g = pairs[w].x;
+  const int64_t r = pairs[w].y;
+  const int64_t s = kept[r];
+  const uint8_t* row = bed + s * bps;
+  const double mus = mu[s];
+  const double* u = U + static_cast<int64_t>(g) * n;
+  const __half* gh = gt_hi + r * k_pad;
+  const __half* gl = gt_lo + r * k_pad;
+  const double d = delta[g];
+  double num = 0, gg = 0, a[kMaxPLmm];
+  for (int k = 0; k < p; ++k) a[k] = 0;
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t b = __ldg(row + (col[i] >> 2));
+    const uint32_t pr = (b >> ((col[i] & 3) * 2)) & 3u;
+    const int code = static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pr * 8)) & 0xFFu));
+    num += (code < 0 ? mus : static_cast<double>(code)) * u[i];
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double gt = (static_cast<double>(__half2float(gh[i])) + static_cast<double>(__half2float(gl[i]))) * inv_s1;
+    const double dg = gt / v;
+    gg += dg * gt;
+    for (int k = 0; k < p; ++k) a[k] += Xtil[static_cast<int64_t>(k) * n + i] * dg;
+  }
+  for (int o = 16; o; o >>= 1) {
+    num += __shfl_xor_sync(0xffffffffu, num, o);
+    gg += __shfl_xor_sync(0xffffffffu, gg, o);
+    for (int k = 0; k < p; ++k) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+  }
+  if (lane == 0) {
+    eqtl_pair q;
+    double S = -1.0;
+    if (!(gg < 1e-12)) {
+      const double* A = ainv + static_cast<int64_t>(g) * p * p;
+      double aTu = 0;
+      for (int x = 0; x < p; ++x) {
+        double ux = 0;
+        for (int y = 0; y < p; ++y) ux += A[x * p + y] * a[y];
+        aTu += a[x] * ux;
+      }
+      S = gg - aTu;
+    }
+    lmm_stats_num_s(num, S, rss[g], df, q);
+    p_out[w] = q.p;
   }
 }
 
@@ -959,6 +1039,40 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
   return refined;
 }
 
+// FP64 p of tiny-|t| pairs against the current LMM prep (see lmm_tiny_kernel).
+static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std::vector<int2>& tiny) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  Rotated& R = ctx->rot;
+  cudaStream_t st = ctx->stream;
+  const int n = g.n;
+  const int G = static_cast<int>(ws.delta.n);
+  std::vector<double> out(tiny.size());
+  if (tiny.empty()) return out;
+  ws.graw.alloc(static_cast<size_t>(n) * G);  // w o r~ per gene
+  ws.gt.alloc(static_cast<size_t>(n) * G);    // u = Q (w o r~)
+  ctx->launches += 2;
+  lmm_wr_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
+                                   ws.graw.p);
+  EQTL_CUDA(cudaGetLastError());
+  const double one = 1.0, zero = 0.0;
+  EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ws.graw.p, n,
+                         &zero, ws.gt.p, n) == CUBLAS_STATUS_SUCCESS,
+             EQTL_E_CUDA, "Q (w o r) failed");
+  float s1, s2;
+  output_scales(n, s1, s2);
+  ws.ref_pairs.upload(tiny.data(), tiny.size(), st);
+  ws.tiny_p.alloc(tiny.size());
+  lmm_tiny_kernel<<<static_cast<unsigned>((tiny.size() + 7) / 8), 256, 0, st>>>(
+      g.bed.p, g.bytes_per_snp, g.col.p, n, R.k_pad, g.kept.p, g.mu.p, ws.gt.p, R.gt_hi.p, R.gt_lo.p, 1.0 / s1,
+      ws.Xtil.p, p, ctx->basis.lambda.p, ws.delta.p, ws.ainv.p, ws.rss.p, df, ws.ref_pairs.p,
+      static_cast<int>(tiny.size()), ws.tiny_p.p);
+  EQTL_CUDA(cudaGetLastError());
+  ws.tiny_p.download(out.data(), out.size(), st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  return out;
+}
+
 // Subset gate of every kept SNP on the analysis samples into ws.ok.
 static void lmm_gate(eqtl_ctx* ctx) {
   Geno& g = ctx->geno;
@@ -983,6 +1097,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_trans_lmm: no genotypes loaded");
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lmm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_trans_lmm: no genes");
+  EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_trans_lmm: more than 2^30 kept SNPs");
   EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED,
              "the LMM scan handles 1 to 16 covariate columns (intercept included)");
   EQTL_CHECK(!(simt && p > 2), EQTL_E_UNSUPPORTED, "the FP32 CUDA-core comparator covers 1 or 2 covariate columns");
@@ -1083,8 +1198,8 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     }
   }
   scan_timer.reset();
-  std::vector<int2> todo, deferred;
-  so.collect(genes, todo, deferred);
+  std::vector<int2> todo, deferred, tiny;
+  so.collect(genes, todo, deferred, &tiny);
 
   // ---- FP64 refinement: rotate raw dosages of the SNPs involved
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
@@ -1094,6 +1209,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   }
   std::vector<eqtl_pair> refined = lmm_refine_pairs(ctx, p, df, todo);
   add_deferred_acat(genes, refined, deferred);
+  add_acat_terms(genes, tiny, lmm_tiny_p(ctx, p, df, tiny));
   finish_scan(prm, genes, refined, pairs, cands);
 }
 

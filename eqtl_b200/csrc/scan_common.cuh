@@ -12,6 +12,7 @@ enum WinMode : int { kWinNone = 0, kWinExclude = 1, kWinInclude = 2 };
 
 // high bit of a candidate's SNP field: its ACAT term is added on the host
 constexpr uint32_t kCandDeferred = 0x80000000u;
+constexpr uint32_t kCandTiny = 0x40000000u;  // deferred for 0 < |t| < tiny_t (kept SNP indices < 2^30)
 
 struct GeneOut {
   double* acat_sum;            // [G] sum of tan((1/2 - p) pi)
@@ -107,10 +108,11 @@ __device__ __forceinline__ void load_flags16(const uint8_t* p, uint32_t (&w)[4])
 }
 __device__ __forceinline__ bool flag16(const uint32_t (&w)[4], int j) { return (w[j >> 2] >> (8 * (j & 3))) & 0xFFu; }
 
-__device__ __forceinline__ void emit_candidate(const GeneOut& out, int g, int64_t s, bool deferred) {
+__device__ __forceinline__ void emit_candidate(const GeneOut& out, int g, int64_t s, bool deferred, bool tiny) {
   const unsigned int idx = atomicAdd(out.cand_count, 1u);
   if (idx < out.cand_cap)
-    out.cand[idx] = make_int2(g, static_cast<int>(static_cast<uint32_t>(s) | (deferred ? kCandDeferred : 0u)));
+    out.cand[idx] = make_int2(g, static_cast<int>(static_cast<uint32_t>(s) | (deferred ? kCandDeferred : 0u) |
+                                                  (tiny ? kCandTiny : 0u)));
 }
 
 }  // namespace dev

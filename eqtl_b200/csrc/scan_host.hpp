@@ -56,7 +56,10 @@ struct ScanOutputs {
   void run(const std::function<void(dev::GeneOut)>& launch);
   // downloads per-gene sums into genes[] and returns the (gene, snp) pairs to
   // refine: all candidates plus each gene's best SNP
-  void collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred);
+  // refine: all candidates plus each gene's best SNP; with `tiny`, the pairs
+  // deferred only for 0 < |t| < tiny_t go there instead of todo / deferred
+  void collect(eqtl_gene_result* genes, std::vector<int2>& todo, std::vector<int2>& deferred,
+               std::vector<int2>* tiny = nullptr);
 };
 
 // Adds, for every deferred (gene, snp) pair, the reference's long-double ACAT
@@ -66,6 +69,10 @@ struct ScanOutputs {
 // pairs it hands to the refinement.
 void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                        const std::vector<int2>& deferred);
+
+// Adds the reference's long-double ACAT term and `used` count of each pair
+// whose FP64 p (p_pairs[i]) enters ACAT (src/stats_extra.cpp:16-22).
+void add_acat_terms(eqtl_gene_result* genes, const std::vector<int2>& pairs, const std::vector<double>& p_pairs);
 
 // Candidate-buffer size: three times the pairs expected under the null at the
 // larger of the two thresholds, at least 2^16.

@@ -93,7 +93,7 @@ struct LmEpi {
       const float t = (ig > 0.0f && omr > 0.0f) ? copysignf(sqrtf(P.df * __fdividef(r, omr)), num) : 0.0f;
       const TailOut o = t_tail(t, tt);
       acc.add_masked(o, s, valid);
-      if (valid && (fabsf(t) >= P.t_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred);
+      if (valid && (fabsf(t) >= P.t_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred, o.tiny);
     }
   }
   __device__ void end_tile() {
@@ -298,6 +298,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   const int n = prm->n, G = prm->n_genes, p = prm->p;
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0 && p > 0 && p <= kMaxP, EQTL_E_ARG, "scan_trans_lm: need 1 <= p <= 32 and genes > 0");
+  EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_trans_lm: more than 2^30 kept SNPs");
   cudaStream_t st = ctx->stream;
   const double df = static_cast<double>(n - p - 1);
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);

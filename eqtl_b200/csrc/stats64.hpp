@@ -83,6 +83,23 @@ EQTL_HD void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_p
   q.r2 = yty > 0 ? 1.0 - rss / yty : 0.0;
 }
 
+// LMM pair from its Wald numerator NUM = yg - a'chi0 and Schur denominator
+// S = gg - a'A00^-1 a (the tail of lmm_stats_fp64).
+EQTL_HD void lmm_stats_num_s(double num, double S, double rss_null, double df, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (S <= 1e-15) return;
+  const double bg = num / S;
+  double qq = rss_null - S * bg * bg;
+  if (qq < 0) qq = 0;
+  const double sigma2 = df > 0 ? qq / df : 1.0;
+  q.beta = bg;
+  q.se = sqrt(fmax(sigma2 / S, 0.0));
+  q.t = q.se > 0 ? q.beta / q.se : 0.0;
+  q.p = t_two_sided_p(q.t, df);
+  q.r2 = rss_null > 1e-15 ? fmax(0.0, 1.0 - qq / rss_null) : 0.0;
+}
+
 // LMM pair from gg = Gt'W Gt, yg = Gt'W y~, a = X~'W Gt and the gene's null
 // fit (chi0, ainv = (X~'W X~)^-1 row-major, rss_null).
 EQTL_HD void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv,

@@ -55,6 +55,7 @@ struct TailOut {
   double term;       // tan((1/2 - p) pi)
   bool use_acat;     // p < 1 - 1e-12 and not deferred: term added on the device
   bool deferred;     // p < 1e-14 or 0 < |t| < tiny_t: left to the host (see below)
+  bool tiny;         // deferred because 0 < |t| < tiny_t
 };
 
 // The reference evaluates tan((0.5L - p) * pi) in 80-bit long double
@@ -101,6 +102,7 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
   const float cot = __fdividef(cm, sm);
   o.neglog10p = nan_t ? 0.0f : fminf(-lnp * (1.0f / kLn10), 323.3f);
   const bool tiny = at > 0.0f && at < T.tiny_t;
+  o.tiny = !nan_t && tiny;
   o.deferred = !nan_t && (beyond || tiny || o.neglog10p > kDeferNegLog10P);
   o.use_acat = !nan_t && !o.deferred && (central ? q > 1e-12f : true);
   o.term = (nan_t || o.deferred || !o.use_acat) ? 0.0 : static_cast<double>(p_small ? cot : -cot);

@@ -21,8 +21,10 @@
 //               16-column chunks with tcgen05.ld and hands them to the
 //               scan-specific Epi functor, which never writes the M x N
 //               matrix to HBM.
-// When NACC*NT <= 256 the accumulators are double-buffered so the epilogue of
-// tile i overlaps the MMAs of tile i+1.
+// TMEM is used as a ring of NT-column slots: the MMAs of the next tile start
+// in whichever slots the epilogue has already read, so the epilogue of tile
+// i overlaps the MMAs of tile i+1 (fully when 2 * NACC <= slots, for its
+// first accumulators otherwise).
 // A tile may need more accumulators than TMEM holds at once (the LMM with p
 // covariates needs p + 2): they then run in groups of NACC, one after the
 // other on the same CTA, and a grouped epilogue (Epi::kGrouped) receives each
@@ -68,15 +70,18 @@ struct TileCfg {
   static constexpr int B_BYTES = NT * kChunkK * 2;
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int STAGES = (196608 / STAGE_BYTES) < 2 ? 2 : (196608 / STAGE_BYTES > 6 ? 6 : 196608 / STAGE_BYTES);
-  static constexpr int NBUF = (2 * NACC * NT <= 512) ? 2 : 1;
-  static constexpr uint32_t COLS_USED = NBUF * NACC * NT;
+  // TMEM is split into NSLOTS slots of NT columns; accumulator j of work
+  // unit u lives in slot (u * NACC + j) % NSLOTS, so the next unit's first
+  // accumulators can start in free slots while the epilogue still reads.
+  static constexpr int NSLOTS = (512 / NT) > 8 ? 8 : 512 / NT;
+  static constexpr uint32_t COLS_USED = NSLOTS * NT;
   static constexpr uint32_t TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
                                         : COLS_USED <= 256 ? 256 : 512;
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 512;
   static_assert(NACC >= 1 && NACC <= kMaxAcc, "NACC");
   static_assert(NT % 16 == 0 && NT >= 16 && NT <= 256, "NT");
-  static_assert(NACC * NT <= 512, "TMEM");
-  static_assert(STAGES * STAGE_BYTES + 1024 + 256 <= 232448, "smem");
+  static_assert(NACC <= NSLOTS, "TMEM slots");
+  static_assert(STAGES * STAGE_BYTES + 1024 + 512 <= 232448, "smem");
 };
 
 // Work item t -> output tile (ta, tb) and its K-chunk range [k0, k1).
@@ -119,12 +124,12 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
   uint64_t* empty = full + C::STAGES;
-  uint64_t* accf = empty + C::STAGES;  // [2]
-  uint64_t* acce = accf + 2;           // [2]
-  uint64_t* drain = acce + 2;          // [1]
+  uint64_t* sfull = empty + C::STAGES;    // [NSLOTS] MMA -> epilogue: a unit's accumulators are complete
+  uint64_t* sempty = sfull + C::NSLOTS;   // [NSLOTS] epilogue -> MMA: the slot has been read
+  uint64_t* drain = sempty + C::NSLOTS;   // [1]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   volatile uint32_t* abort_flag = tmem_slot + 1;
-  uint8_t* epi_smem = smem + C::STAGES * C::STAGE_BYTES + 256;  // Epi::kSmemBytes of epilogue scratch
+  uint8_t* epi_smem = smem + C::STAGES * C::STAGE_BYTES + 512;  // Epi::kSmemBytes of epilogue scratch
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -134,9 +139,9 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 32 * kEpiWarps);
+    for (int k = 0; k < C::NSLOTS; ++k) {
+      mbar_init(&sfull[k], 1);
+      mbar_init(&sempty[k], 32 * kEpiWarps);
     }
     mbar_init(drain, 1);
     *abort_flag = 0u;
@@ -209,23 +214,27 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       constexpr uint32_t idesc = idesc_f16(kTileM, NT, AB_FMT);
       int stage = 0;
       uint32_t phase = 0;
-      int buf = 0;
-      uint32_t accphase = 0;
+      uint32_t eph = 0;   // bit k: parity of slot k's next release
+      int slot0 = 0;      // ring slot of the current unit's first accumulator
       bool ok = true;
       for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
         int ta, tb, k0, k1;
         tile_coords(sh, t, ta, tb, k0, k1);
-        for (int grp = 0; grp < sh.n_groups && ok; ++grp) {
-          if (!mbar_wait(&acce[buf], accphase ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const uint32_t dbase = tmem_base + static_cast<uint32_t>(buf * NACC * NT);
-          const int j_end = min(sh.n_acc, (grp + 1) * NACC);
-          for (int j = grp * NACC; j < j_end && ok; ++j) {
-            const uint32_t d = dbase + static_cast<uint32_t>((j - grp * NACC) * NT);
-            const int pm = sh.prod[j];
+        for (int grp = 0; grp < sh.n_groups && ok; ++grp, slot0 = (slot0 + NACC) % C::NSLOTS) {
+          const int j0 = grp * NACC;
+          const int nv = min(NACC, sh.n_acc - j0);
+          int last = 0;
+          for (int jj = 0; jj < nv && ok; ++jj) {
+            const int slot = (slot0 + jj) % C::NSLOTS;
+            last = slot;
+            if (!mbar_wait(&sempty[slot], ((eph >> slot) & 1u) ^ 1u, status, abort_flag, kDevTimeoutAccEmpty)) {
+              ok = false;
+              break;
+            }
+            eph ^= 1u << slot;
+            tc_fence_after();
+            const uint32_t d = tmem_base + static_cast<uint32_t>(slot * NT);
+            const int pm = sh.prod[j0 + jj];
             for (int kc = k0; kc < k1; ++kc) {
               if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
                 ok = false;
@@ -259,13 +268,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             }
           }
           if (!ok) break;
-          umma_commit(&accf[buf]);
-          if (C::NBUF == 2) {
-            buf ^= 1;
-            if (buf == 0) accphase ^= 1u;
-          } else {
-            accphase ^= 1u;
-          }
+          umma_commit(&sfull[last]);  // completes when every MMA issued so far has
         }
       }
       // Drain: all issued MMAs complete before TMEM is released (bounded).
@@ -287,31 +290,34 @@ __global__ void __launch_bounds__(kTileThreads, 1)
     Epi epi(ep, sh, Epi::kSmemBytes ? epi_smem : nullptr);
     epi.init(threadIdx.x - 64, 32 * kEpiWarps);
     asm volatile("bar.sync 1, %0;" ::"r"(32 * kEpiWarps) : "memory");
-    int buf = 0;
-    uint32_t accphase = 0;
+    uint32_t fph = 0;   // bit k: parity of slot k's next completion
+    int slot0 = 0;      // ring slot of the current unit's first accumulator
+    const uint32_t lanes = tmem_base + (static_cast<uint32_t>(quarter * 32) << 16);
     for (int t = blockIdx.x; t < sh.n_tiles; t += gridDim.x) {
       int ta, tb, k0, k1;
       tile_coords(sh, t, ta, tb, k0, k1);
       epi.begin_tile(ta * kTileM + row, tb * NT);
       bool eok = true;
-      for (int grp = 0; grp < sh.n_groups; ++grp) {
-        if (!mbar_wait(&accf[buf], accphase, status, abort_flag, kDevTimeoutAccFull)) {
+      for (int grp = 0; grp < sh.n_groups; ++grp, slot0 = (slot0 + NACC) % C::NSLOTS) {
+        const int j0 = grp * NACC;
+        const int nv = min(NACC, sh.n_acc - j0);
+        const int last = (slot0 + nv - 1) % C::NSLOTS;
+        if (!mbar_wait(&sfull[last], (fph >> last) & 1u, status, abort_flag, kDevTimeoutAccFull)) {
           eok = false;
           break;
         }
+        fph ^= 1u << last;
         tc_fence_after();
-        const uint32_t tbase =
-            tmem_base + (static_cast<uint32_t>(quarter * 32) << 16) + static_cast<uint32_t>(buf * NACC * NT);
+        auto col = [&](int jj) { return lanes + static_cast<uint32_t>(((slot0 + jj) % C::NSLOTS) * NT); };
         if constexpr (Epi::kGrouped) {
-          const int nv = min(NACC, sh.n_acc - grp * NACC);
 #pragma unroll 1
           for (int c = 16 * sub; c < NT; c += 16 * kSub) {
 #pragma unroll 1
-            for (int j = 0; j < nv; ++j) {
+            for (int jj = 0; jj < nv; ++jj) {
               float v[16];
-              tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v);
+              tmem_ld16(col(jj) + static_cast<uint32_t>(c), v);
               tmem_wait_ld();
-              epi.acc_chunk(grp * NACC + j, c, v);
+              epi.acc_chunk(j0 + jj, c, v);
             }
             if (grp == sh.n_groups - 1) epi.finish_chunk(c);
           }
@@ -320,19 +326,13 @@ __global__ void __launch_bounds__(kTileThreads, 1)
           for (int c = 16 * sub; c < NT; c += 16 * kSub) {
             float v[NACC][16];
 #pragma unroll
-            for (int j = 0; j < NACC; ++j) tmem_ld16(tbase + static_cast<uint32_t>(j * NT + c), v[j]);
+            for (int jj = 0; jj < NACC; ++jj) tmem_ld16(col(jj) + static_cast<uint32_t>(c), v[jj]);
             tmem_wait_ld();
             epi.template chunk<NACC>(c, v);
           }
         }
         tc_fence_before();
-        mbar_arrive(&acce[buf]);
-        if (C::NBUF == 2) {
-          buf ^= 1;
-          if (buf == 0) accphase ^= 1u;
-        } else {
-          accphase ^= 1u;
-        }
+        for (int jj = 0; jj < nv; ++jj) mbar_arrive(&sempty[(slot0 + jj) % C::NSLOTS]);
       }
       if (!eok) break;
       epi.end_tile();
