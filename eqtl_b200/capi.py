@@ -226,14 +226,15 @@ class Context:
         self._check(self.lib.eqtl_launch_count(self.h, C.byref(v)))
         return v.value
 
-    def t_tail(self, df: float, t, use_smem: bool = False):
-        """Device Student-t tail -> (-log10 p, ACAT term, flags)."""
+    def t_tail(self, df: float, t, use_smem: bool = False, screen: bool = False):
+        """Device Student-t tail -> (-log10 p, ACAT term, flags); with
+        screen=True the scan epilogues' ACAT screen -> (|t|, term, flags)."""
         t = np.ascontiguousarray(t, np.float32)
         nl = np.zeros(t.size, np.float32)
         term = np.zeros(t.size, np.float64)
         fl = np.zeros(t.size, np.uint8)
-        self._check(self.lib.eqtl_t_tail(self.h, df, _ptr(t), t.size, 1 if use_smem else 0, _ptr(nl), _ptr(term),
-                                         _ptr(fl)))
+        self._check(self.lib.eqtl_t_tail(self.h, df, _ptr(t), t.size, int(use_smem) | (2 if screen else 0), _ptr(nl),
+                                         _ptr(term), _ptr(fl)))
         return nl, term, fl
 
     def stream_ptr(self) -> int:

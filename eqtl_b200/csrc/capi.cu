@@ -251,6 +251,8 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
   if (ws.tt_df != df) {
     ws.tt_h.upload(T.h.data(), T.h.size(), ctx->stream);
     ws.tt_L.upload(T.L.data(), T.L.size(), ctx->stream);
+    ws.tt_c1.upload(T.c1.data(), T.c1.size(), ctx->stream);
+    ws.tt_lt.upload(T.lt.data(), T.lt.size(), ctx->stream);
     ws.tt_df = df;
   }
   dev::TTable t{};
@@ -269,6 +271,11 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
   const int prec = ctx->precision >= 0 && ctx->precision < 3 ? ctx->precision : 0;
   const double ulp = std::nextafter(df, std::numeric_limits<double>::infinity()) - df;
   t.tiny_t = static_cast<float>(std::sqrt(256.0 * ulp) + 4.0 * kTErr[prec]);
+  t.c1 = ws.tt_c1.p;
+  t.lt = ws.tt_lt.p;
+  t.dl_inv = static_cast<float>(T.nb / (T.x_defer - T.x0));
+  // round t_defer down so that every pair with p <= 1e-14 is deferred
+  t.t_defer = static_cast<float>(T.t_defer * (1.0 - 1e-6));
   t.na = T.na;
   t.nb = T.nb;
   return t;
@@ -301,17 +308,26 @@ namespace {
 __global__ void t_tail_kernel(dev::TTable T, const float* t, int64_t n, int use_smem, float* nl, double* term,
                               uint8_t* flags) {
   extern __shared__ float tsm[];
+  const bool screen = (use_smem & 2) != 0;
   dev::TTable tt = T;
-  if (use_smem) {
-    tt = dev::ttable_to_smem(T, tsm, threadIdx.x, blockDim.x);
+  if (use_smem & 1) {
+    tt = screen ? dev::screen_to_smem(T, tsm, threadIdx.x, blockDim.x)
+                : dev::ttable_to_smem(T, tsm, threadIdx.x, blockDim.x);
     __syncthreads();
   }
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (screen) {
+    const dev::ScreenOut o = dev::acat_screen(t[i], tt);
+    nl[i] = o.key_t;
+    term[i] = o.term;
+    flags[i] = static_cast<uint8_t>((o.use_acat ? 1 : 0) | (o.deferred ? 2 : 0) | (o.tiny ? 4 : 0));
+    return;
+  }
   const dev::TailOut o = dev::t_tail(t[i], tt);
   nl[i] = o.neglog10p;
   term[i] = o.term;
-  flags[i] = static_cast<uint8_t>((o.use_acat ? 1 : 0) | (o.deferred ? 2 : 0));
+  flags[i] = static_cast<uint8_t>((o.use_acat ? 1 : 0) | (o.deferred ? 2 : 0) | (o.tiny ? 4 : 0));
 }
 
 __global__ void fill_u64(unsigned long long* p, int n, unsigned long long v) {

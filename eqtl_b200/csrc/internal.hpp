@@ -138,7 +138,7 @@ struct Workspace {
   // windows
   DevBuf<int32_t> win_gc, win_sc;
   DevBuf<int64_t> win_glo, win_ghi, win_sp;
-  DevBuf<float> tt_h, tt_L;
+  DevBuf<float> tt_h, tt_L, tt_c1, tt_lt;
   double tt_df = -1;
   // GRM operands and accumulators, eigen-solver scratch
   DevBuf<uint8_t> grm_use;

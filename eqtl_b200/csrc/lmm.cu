@@ -389,7 +389,7 @@ struct LmmEpi {
   __device__ LmmEpi(const Params& p, const TileShape&, uint8_t* smem)
       : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
   __device__ void init(int tid, int nthr) {
-    if (tsm) tt = ttable_to_smem(Pr.tt, tsm, tid, nthr);
+    if (tsm) tt = screen_to_smem(Pr.tt, tsm, tid, nthr);
   }
   __device__ void begin_tile(int g, int64_t s0) {
     gene = g;
@@ -437,8 +437,8 @@ struct LmmEpi {
       const float omr = 1.0f - r;
       const bool ok_stat = !(gg < 1e-12f) && S > 1e-15f && omr > 0.0f;
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
-      const TailOut o = t_tail(t, tt);
-      acc.add_masked(o, s, valid);
+      const ScreenOut o = acat_screen(t, tt);
+      acc.add_screen(o, s, valid);
       if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }
@@ -562,7 +562,7 @@ struct LmmGroupEpi {
   __device__ LmmGroupEpi(const Params& p, const TileShape&, uint8_t* smem)
       : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
   __device__ void init(int tid, int nthr) {
-    if (tsm) tt = ttable_to_smem(Pr.tt, tsm, tid, nthr);
+    if (tsm) tt = screen_to_smem(Pr.tt, tsm, tid, nthr);
   }
   __device__ void begin_tile(int g, int64_t s0) {
     gene = g;
@@ -605,8 +605,8 @@ struct LmmGroupEpi {
       const float omr = 1.0f - r;
       const bool ok_stat = S[j] > 1e-15f && omr > 0.0f;
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num[j]) : 0.0f;
-      const TailOut o = t_tail(t, tt);
-      acc.add_masked(o, s, valid);
+      const ScreenOut o = acat_screen(t, tt);
+      acc.add_screen(o, s, valid);
       if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }

@@ -76,6 +76,18 @@ struct GeneAcc {
       best = k < best ? k : best;
     }
   }
+  // The same for the epilogues' ACAT screen (best SNP keyed on |t|).
+  __device__ __forceinline__ void add_screen(const ScreenOut& o, int64_t s, bool valid) {
+    if (valid) {
+      ++tested;
+      if (o.use_acat) {
+        acat += o.term;
+        ++used;
+      }
+      const unsigned long long k = best_key(o.key_t, static_cast<uint32_t>(s));
+      best = k < best ? k : best;
+    }
+  }
   __device__ __forceinline__ void add(const TailOut& o, int64_t s) {
     ++tested;
     if (o.use_acat) {

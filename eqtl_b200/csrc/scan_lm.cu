@@ -60,7 +60,7 @@ struct LmEpi {
   __device__ LmEpi(const Params& p, const TileShape&, uint8_t* smem)
       : P(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
   __device__ void init(int tid, int nthr) {
-    if (tsm) tt = ttable_to_smem(P.tt, tsm, tid, nthr);
+    if (tsm) tt = screen_to_smem(P.tt, tsm, tid, nthr);
   }
   __device__ void begin_tile(int g, int64_t s0) {
     gene = g;
@@ -91,8 +91,8 @@ struct LmEpi {
       const float r = num * num * ig * inv_yty;
       const float omr = 1.0f - r;
       const float t = (ig > 0.0f && omr > 0.0f) ? copysignf(sqrtf(P.df * __fdividef(r, omr)), num) : 0.0f;
-      const TailOut o = t_tail(t, tt);
-      acc.add_masked(o, s, valid);
+      const ScreenOut o = acat_screen(t, tt);
+      acc.add_screen(o, s, valid);
       if (valid && (fabsf(t) >= P.t_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred, o.tiny);
     }
   }

@@ -33,6 +33,12 @@ struct TTable {
   float inv_df;
   float t0;
   int na, nb;
+  // ACAT screening of the scan epilogues (acat_screen): |t| tan((1/2 - p) pi)
+  // on the central u grid, ln tan((1/2 - p) pi) on x in [x0, x(t_defer)]
+  const float* c1;  // na + 4 nodes
+  const float* lt;  // nb + 4 nodes
+  float dl_inv;     // nb / (x(t_defer) - x0)
+  float t_defer;    // |t| >= t_defer (p <= 1e-14): the term is left to the host
 };
 
 __device__ __forceinline__ float lagrange4(const float* y, float x, int n_int) {
@@ -110,8 +116,53 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
   return o;
 }
 
-// Copies the table into shared memory (cooperatively, by `nthr` threads)
-// and returns a view of it; the caller synchronises before use.
+// What the scan epilogues need of each pair: the ACAT term, whether it
+// enters ACAT on the device, and whether the host takes it over. Same rules
+// as t_tail, without -log10 p: the best SNP is keyed on |t| (p falls with |t|
+// at one df) and deferral for p <= 1e-14 is |t| >= t_defer. One table lookup:
+//   central  tan((1/2 - p) pi) = c1(t^2) / |t|
+//   tail     tan((1/2 - p) pi) = exp(lt(sqrt(log1p(t^2 / df))))
+struct ScreenOut {
+  double term;    // tan((1/2 - p) pi) when use_acat, else 0
+  float key_t;    // |t| for the best-SNP key (0 for NaN)
+  bool use_acat;  // p < 1 - 1e-12 and not deferred
+  bool deferred;  // p <= 1e-14 or 0 < |t| < tiny_t
+  bool tiny;      // deferred because 0 < |t| < tiny_t
+};
+
+__device__ __forceinline__ ScreenOut acat_screen(float t, const TTable& T) {
+  ScreenOut o;
+  const float at = fabsf(t);
+  const bool nan_t = !(at == at);
+  const bool tiny = at > 0.0f && at < T.tiny_t;
+  o.tiny = !nan_t && tiny;
+  o.deferred = !nan_t && (tiny || at >= T.t_defer);
+  o.use_acat = !nan_t && !o.deferred && at > 0.0f;
+  o.key_t = nan_t ? 0.0f : at;
+  const bool central = at <= T.t0;
+  const float u = at * at;
+  const float xs = sqrtf(log1pf(u * T.inv_df));
+  const float x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
+  const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
+  const float term = central ? __fdividef(y, at) : __expf(y);
+  o.term = o.use_acat ? static_cast<double>(term) : 0.0;
+  return o;
+}
+
+// Copies the screening tables into shared memory (cooperatively, by `nthr`
+// threads) and returns a view of them; the caller synchronises before use.
+__device__ __forceinline__ TTable screen_to_smem(const TTable& T, float* sm, int tid, int nthr) {
+  const int nc = T.na + 4, nl = T.nb + 4;
+  for (int i = tid; i < nc; i += nthr) sm[i] = T.c1[i];
+  for (int i = tid; i < nl; i += nthr) sm[nc + i] = T.lt[i];
+  TTable o = T;
+  o.c1 = sm;
+  o.lt = sm + nc;
+  return o;
+}
+
+// Copies the t_tail tables into shared memory (cooperatively, by `nthr`
+// threads) and returns a view of them; the caller synchronises before use.
 __device__ __forceinline__ TTable ttable_to_smem(const TTable& T, float* sm, int tid, int nthr) {
   const int nh = T.na + 4, nl = T.nb + 4;
   for (int i = tid; i < nh; i += nthr) sm[i] = T.h[i];
@@ -123,10 +174,12 @@ __device__ __forceinline__ TTable ttable_to_smem(const TTable& T, float* sm, int
 }
 
 // Monotone 64-bit key for "smallest p, then lowest SNP index": atomicMin
-// over keys picks the reference's best (strict < keeps the first SNP).
-__device__ __forceinline__ unsigned long long best_key(float neglog10p, uint32_t snp) {
-  // larger -log10 p is better -> invert the (non-negative) float bits
-  const uint32_t b = __float_as_uint(fmaxf(neglog10p, 0.0f));
+// over keys picks the reference's best (strict < keeps the first SNP). The
+// score is any non-negative quantity that grows as p falls: -log10 p, or |t|
+// within one gene (one df).
+__device__ __forceinline__ unsigned long long best_key(float score, uint32_t snp) {
+  // larger score is better -> invert the (non-negative) float bits
+  const uint32_t b = __float_as_uint(fmaxf(score, 0.0f));
   return (static_cast<unsigned long long>(~b) << 32) | snp;
 }
 

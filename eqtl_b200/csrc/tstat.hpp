@@ -24,7 +24,7 @@ inline double t_critical(double pthr, double df) {
   if (!(pthr > 0)) return std::numeric_limits<double>::infinity();
   if (pthr >= 1) return 0.0;
   double lo = 0.0, hi = 1.0;
-  while (t_two_sided_p(hi, df) > pthr && hi < 1e8) hi *= 2;
+  while (t_two_sided_p(hi, df) > pthr && hi < 1e30) hi *= 2;  // df = 1: p = 1e-14 at |t| ~ 6e13
   for (int i = 0; i < 200; ++i) {
     const double mid = 0.5 * (lo + hi);
     if (t_two_sided_p(mid, df) > pthr) lo = mid;
@@ -40,6 +40,11 @@ struct TTableHost {
   int na = 512;                  // central intervals over u = t^2 in [0, t0^2]
   int nb = 4096;                 // tail intervals over x = sqrt(log1p(t^2/df)) in [x0, x_end]
   double x0 = 0, x_end = 0;
+  // ACAT screening tables of the scan epilogues (tdist.cuh, acat_screen):
+  std::vector<float> c1;   // na + 4 nodes on the central u grid: |t| * tan((1/2 - p) pi)
+  std::vector<float> lt;   // nb + 4 nodes on x in [x0, x_defer]: ln tan((1/2 - p) pi)
+  double x_defer = 0;      // tail grid end: x at p = 1e-14
+  double t_defer = 0;      // |t| with p = 1e-14: beyond it the term is left to the host
   std::vector<float> h;          // na + 4 nodes: h(u) = (1 - p) / |t|, node k at u = (k-1) du
   std::vector<float> L;          // nb + 4 nodes: ln p at x = x0 + (k-1) dx
 };
@@ -89,9 +94,22 @@ inline double central_h(double u, double df) {
   return 2.0 * c * acc;
 }
 
+// z cot z as a function of w = z^2 (even in z, analytic in w; y coth y for w < 0).
+inline double zcotz(double w) {
+  if (std::fabs(w) < 1e-8) return 1.0 - w / 3.0 - w * w / 45.0;
+  if (w > 0) {
+    const double z = std::sqrt(w);
+    return z * std::cos(z) / std::sin(z);
+  }
+  const double y = std::sqrt(-w);
+  return y * std::cosh(y) / std::sinh(y);
+}
+
 inline TTableHost build_ttable(double df) {
   TTableHost T;
   T.df = df;
+  // p(t0) < 1/2 keeps the tail's tan term away from 0 (df = 1 has p(1) = 1/2)
+  T.t0 = df < 1.5 ? 1.5 : 1.0;
   const double du = (T.t0 * T.t0) / T.na;
   T.h.resize(T.na + 4);
   for (int k = 0; k < T.na + 4; ++k) T.h[k] = static_cast<float>(central_h((k - 1) * du, df));
@@ -128,6 +146,26 @@ inline TTableHost build_ttable(double df) {
     double v = lnp(T.x0 + (k - 1) * dx);
     if (v < -1e29) v = 2.0 * T.L[k - 1] - T.L[k - 2];  // past underflow: extrapolate
     T.L[k] = static_cast<float>(v);
+  }
+  // ACAT screening. Central: 1 - p = |t| h(u), so |t| tan((1/2 - p) pi) =
+  // -|t| cot(pi |t| h) = -(z cot z) / (pi h) with z^2 = pi^2 u h^2, analytic
+  // in u (also at the node below 0). Tail: ln tan((1/2 - p) pi) = ln cot(pi p),
+  // smooth in x up to p = 1e-14, past which the host adds the term.
+  T.c1.resize(T.na + 4);
+  for (int k = 0; k < T.na + 4; ++k) {
+    const double u = (k - 1) * du;
+    const double h = central_h(u, df);
+    T.c1[k] = static_cast<float>(-zcotz(M_PI * M_PI * u * h * h) / (M_PI * h));
+  }
+  T.t_defer = t_critical(1e-14, df);
+  T.x_defer = std::sqrt(std::log1p(T.t_defer * T.t_defer / df));
+  const double dl = (T.x_defer - T.x0) / T.nb;
+  T.lt.resize(T.nb + 4);
+  for (int k = 0; k < T.nb + 4; ++k) {
+    const double x = T.x0 + (k - 1) * dl;
+    const double t = std::sqrt(df * std::expm1(x * x));
+    const double p = t_two_sided_p(t, df);
+    T.lt[k] = static_cast<float>(std::log(std::cos(M_PI * p) / std::sin(M_PI * p)));
   }
   return T;
 }

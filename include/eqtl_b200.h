@@ -93,15 +93,17 @@ int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);
  * src/scan_common.cpp:133-151, sums the dosages in sample order). */
 int eqtl_geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out);
 
-/* Evaluates the Student-t tail the scan epilogues use (K8: the device form of
- * p_from_t, src/util.cpp:259-264, through the df-specific interpolation
- * table) for n values of t at residual df, on the device: -log10 p, the ACAT
- * term tan((1/2 - p) pi) and flags (bit 0: term added on the device, bit 1:
- * pair deferred to the host's FP64 / long-double path, for p < 1e-14 and for
- * t within a few 1e-6 of 0 where the reference's p is quantised by the
- * ulp of df). use_smem = 1 reads the table
- * from shared memory as the scan kernels do. For validation. */
-int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use_smem, float* neglog10p,
+/* Evaluates the device Student-t tail (the device form of p_from_t,
+ * src/util.cpp:259-264, through the df-specific interpolation tables) for n
+ * values of t at residual df. mode bit 0: read the tables from shared memory
+ * as the scan kernels do. mode bit 1 clear: the full tail, giving -log10 p,
+ * the ACAT term tan((1/2 - p) pi) and flags. mode bit 1 set: the scan
+ * epilogues' ACAT screen, giving |t| in place of -log10 p, the term, and the
+ * same flags. Flag bit 0: term added on the device; bit 1: pair deferred to
+ * the host's FP64 / long-double path (p < 1e-14, and t within a few 1e-6 of
+ * 0 where the reference's p is quantised by the ulp of df); bit 2: deferred
+ * for the latter reason. For validation. */
+int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t mode, float* neglog10p,
                 double* term, uint8_t* flags);
 
 /* ------------------------------------------------------------- phenotypes

@@ -53,3 +53,34 @@ def test_t_tail_matches_p_from_t(df, smem):
     assert np.all(np.abs(m_dev - m_ref) <= rtol * m_ref + 2e-11), np.max(np.abs(m_dev - m_ref) / m_ref)
     # unused and deferred pairs contribute nothing on the device
     assert np.all(term[~q] == 0.0)
+
+
+@pytest.mark.parametrize("df", [1.0, 5.0, 30.0, 118.0, 295.0, 997.0, 1998.0])
+@pytest.mark.parametrize("smem", [False, True])
+def test_acat_screen_matches_p_from_t(df, smem):
+    """The scan epilogues' ACAT screen: the term from one table lookup,
+    deferral by |t| (p <= 1e-14, and |t| near 0), the best-SNP score |t|."""
+    from eqtl_b200 import capi
+    t = _grid()
+    with capi.Context(0) as c:
+        key, term, fl = c.t_tail(df, t, use_smem=smem, screen=True)
+    p = R.p_from_t(t.astype(np.float64), df)
+    want_nl = -np.log10(np.maximum(p, 1e-300))
+    at = np.abs(t.astype(np.float64))
+    np.testing.assert_array_equal(key, np.abs(t))
+    deferred = (fl & 2) != 0
+    used = (fl & 1) != 0
+    tiny = (at > 0) & (at < 3e-6)
+    mid = (at > 1e-3) & (want_nl < DEFER_NL * (1 - 1e-3))
+    assert np.all(deferred[(want_nl > DEFER_NL * (1 + 1e-3)) | tiny])
+    assert not np.any(deferred[mid | (at == 0)])
+    assert np.array_equal((fl & 4) != 0, deferred & (at < 1e-3))
+    np.testing.assert_array_equal(used, (p < 1 - 1e-12) & ~deferred)
+    q = used
+    m_ref = np.minimum(p[q], 1.0 - p[q])
+    tq = term[q]
+    assert np.all(((tq > 0) == (p[q] < 0.5)) | (np.abs(p[q] - 0.5) < 1e-6))
+    m_dev = np.arctan(1.0 / np.abs(tq)) / np.pi
+    rtol = 3e-6 * np.maximum(1.0, -np.log(m_ref))
+    assert np.all(np.abs(m_dev - m_ref) <= rtol * m_ref + 2e-11), np.max(np.abs(m_dev - m_ref) / m_ref)
+    assert np.all(term[~q] == 0.0)
