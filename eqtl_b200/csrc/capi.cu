@@ -236,6 +236,52 @@ dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t 
   return w;
 }
 
+// Banded tile list of a cis scan (scope 2): for every tile of 128 genes, the
+// SNP tiles of NT kept SNPs that hold some gene's window. Needs the kept
+// SNPs grouped by chromosome in position order (as in a sorted .bim); returns
+// false otherwise, and the caller runs the full grid masked to the windows.
+bool cis_tile_list(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int NT, const int2*& list, int& n_list) {
+  list = nullptr;
+  n_list = 0;
+  if (prm->exclude_cis != 2 || !prm->gene_chrom || !prm->snp_chrom || !prm->snp_pos || m == 0) return false;
+  // chromosome blocks [first, last) of the kept SNPs, positions non-decreasing
+  std::map<int32_t, std::pair<int64_t, int64_t>> block;
+  for (int64_t k = 0; k < m; ++k) {
+    const int32_t c = prm->snp_chrom[k];
+    auto it = block.find(c);
+    if (it == block.end()) {
+      block.emplace(c, std::make_pair(k, k + 1));
+      continue;
+    }
+    if (it->second.second != k || prm->snp_pos[k] < prm->snp_pos[k - 1]) return false;
+    it->second.second = k + 1;
+  }
+  const int G = prm->n_genes;
+  const int tiles_a = (G + dev::kTileM - 1) / dev::kTileM;
+  const int64_t tiles_b = (m + NT - 1) / NT;
+  std::vector<uint8_t> mark(static_cast<size_t>(tiles_a) * tiles_b, 0);
+  for (int g = 0; g < G; ++g) {
+    auto it = block.find(prm->gene_chrom[g]);
+    if (prm->gene_chrom[g] < 0 || it == block.end()) continue;
+    const int64_t* p0 = prm->snp_pos + it->second.first;
+    const int64_t* p1 = prm->snp_pos + it->second.second;
+    const int64_t k_lo = std::lower_bound(p0, p1, prm->gene_lo[g]) - prm->snp_pos;
+    const int64_t k_hi = std::upper_bound(p0, p1, prm->gene_hi[g]) - prm->snp_pos;  // exclusive
+    if (k_hi <= k_lo) continue;
+    uint8_t* row = &mark[static_cast<size_t>(g / dev::kTileM) * tiles_b];
+    for (int64_t tb = k_lo / NT; tb <= (k_hi - 1) / NT; ++tb) row[tb] = 1;
+  }
+  std::vector<int2> tl;
+  for (int ta = 0; ta < tiles_a; ++ta)
+    for (int64_t tb = 0; tb < tiles_b; ++tb)
+      if (mark[static_cast<size_t>(ta) * tiles_b + tb]) tl.push_back(make_int2(ta, static_cast<int>(tb)));
+  n_list = static_cast<int>(tl.size());
+  if (n_list == 0) tl.push_back(make_int2(0, 0));  // keeps a valid (unused) device pointer
+  ctx->ws.tile_list.upload(tl.data(), tl.size(), ctx->stream);
+  list = ctx->ws.tile_list.p;
+  return true;
+}
+
 dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
   EQTL_CHECK(df > 0, EQTL_E_ARG, "residual degrees of freedom must be positive");
   static std::mutex mu;

@@ -126,6 +126,7 @@ struct Workspace {
   DevBuf<double> graw, gt;
   DevBuf<eqtl_pair> refined;
   DevBuf<double> tiny_p;
+  DevBuf<int2> tile_list;
   DevBuf<__half> q_hi, q_lo;  // rotation: split eigenvector operand
   DevBuf<int> ref_snps, ref_col;
   DevBuf<int2> ref_pairs;

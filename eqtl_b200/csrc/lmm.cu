@@ -956,7 +956,7 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph) {
 // ------------------------------------------------------------------- scan
 template <int P>
 static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah, const __half* const* al,
-                       int G, bool simt) {
+                       int G, bool simt, const int2* tiles, int n_tiles) {
   Rotated& R = ctx->rot;
   const __half* bh[2] = {R.gt_hi.p, R.gt2_hi.p};
   const __half* bl[2] = {R.gt_lo.p, R.gt2_lo.p};
@@ -966,7 +966,7 @@ static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* c
     prod[j] = 7;
   }
   if (!simt) {
-    launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod);
+    launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod, tiles, n_tiles);
     return;
   }
   // plain FP32 CUDA-core comparator
@@ -1143,6 +1143,9 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   const TTable tt = device_ttable(ctx, df);
   prep_timer.reset();
   ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  const int2* tiles = nullptr;  // cis: banded tile list (NT of the kernel that runs)
+  int n_tiles = 0;
+  if (!simt) cis_tile_list(ctx, prm, m, grouped ? LmmGroupEpi::kTileN : 128, tiles, n_tiles);
   std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   if (m > 0 && grouped) {
     Rotated& Rt = ctx->rot;
@@ -1164,7 +1167,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     so.run([&](GeneOut out) {
       ep.out = out;
       launch_tile_n<LmmGroupEpi::kTileN, 4>(ctx, false, ep, oph.data(), oph.data() + nops, G, bh, bl, Rt.m, Rt.k_pad,
-                                            bsel.data(), prod.data(), nullptr, 0, 1, nops);
+                                            bsel.data(), prod.data(), tiles, n_tiles, 1, nops);
     });
   } else if (m > 0) {
     const __half* ah[4] = {oph[0], oph[1], oph[2], nops > 3 ? oph[3] : oph[2]};
@@ -1186,14 +1189,14 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
       fill(ep);
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<1>(ctx, ep, ah, al, G, simt);
+        lmm_launch<1>(ctx, ep, ah, al, G, simt, tiles, n_tiles);
       });
     } else {
       LmmEpiParams<2> ep{};
       fill(ep);
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<2>(ctx, ep, ah, al, G, simt);
+        lmm_launch<2>(ctx, ep, ah, al, G, simt, tiles, n_tiles);
       });
     }
   }

@@ -33,6 +33,7 @@ dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t 
 
 // Device t-tail table for `df`, cached in the context workspace.
 dev::TTable device_ttable(eqtl_ctx* ctx, double df);
+bool cis_tile_list(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int NT, const int2*& list, int& n_list);
 
 // Resolves the phenotypes of a scan call: uploads (Y, X) when given,
 // otherwise checks the resident ones match the call's shape.

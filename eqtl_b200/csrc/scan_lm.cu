@@ -364,6 +364,9 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   prep_timer.reset();
 
   ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  const int2* tiles = nullptr;  // cis: banded tile list
+  int n_tiles = 0;
+  cis_tile_list(ctx, prm, m, 256, tiles, n_tiles);
   std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
   if (m > 0) {
     so.run([&](GeneOut out) {
@@ -373,7 +376,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
       const __half* bh[1] = {g.gc_hi.p};
       const __half* bl[1] = {g.gc_lo.p};
       const int bsel[1] = {0}, prod[1] = {7};
-      launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, G, bh, bl, m, k_pad, bsel, prod);
+      launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, G, bh, bl, m, k_pad, bsel, prod, tiles, n_tiles);
     });
   }
   scan_timer.reset();

@@ -298,7 +298,30 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
   info("cis " + model + ": " + std::to_string(jobs.size()) + " genes");
   if (jobs.empty()) return;
   const double pthr = opt.pval_cis;
-  ScanResult R = device_scan(st, model, jobs, 2, pthr, 0.0);
+  // the device scan takes the genes in window order (a banded tile list);
+  // results come back to the output order
+  std::vector<size_t> dev_order(jobs.size());
+  std::iota(dev_order.begin(), dev_order.end(), 0);
+  std::vector<std::string> keys(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) keys[j] = chrom_key(jobs[j].loc->chrom);
+  std::stable_sort(dev_order.begin(), dev_order.end(), [&](size_t a, size_t b) {
+    return keys[a] != keys[b] ? keys[a] < keys[b] : jobs[a].loc->start < jobs[b].loc->start;
+  });
+  std::vector<Job> jobs_dev(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) jobs_dev[j] = jobs[dev_order[j]];
+  ScanResult R = device_scan(st, model, jobs_dev, 2, pthr, 0.0);
+  {
+    std::vector<eqtl_gene_result> genes(R.genes.size());
+    std::vector<double> delta(R.delta.size());
+    for (size_t j = 0; j < dev_order.size(); ++j) {
+      genes[dev_order[j]] = R.genes[j];
+      delta[dev_order[j]] = R.delta[j];
+    }
+    R.genes.swap(genes);
+    R.delta.swap(delta);
+    for (auto& q : R.pairs) q.gene = static_cast<int32_t>(dev_order[q.gene]);
+    for (auto& q : R.cands) q.gene = static_cast<int32_t>(dev_order[q.gene]);
+  }
   std::vector<PermOut> perms;
   if (opt.perm > 0) {
     std::vector<PermGene> pg(jobs.size());

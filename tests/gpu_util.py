@@ -52,8 +52,8 @@ def check_scan(res, ora, pairs_ref, pthr, df, t_err=T_ERR, rel=1e-9):
         assert abs(np.log10(pv) - np.log10(pthr)) < 1e-6, (k, pv)
     for k in set(got) & set(pairs_ref):
         q, r = got[k], pairs_ref[k]
-        assert abs(q["beta"] - r["beta"]) <= rel * abs(r["beta"]) + 1e-12
-        assert abs(q["t"] - r["stat"]) <= 10 * rel * abs(r["stat"]) + 1e-10
+        assert abs(q["beta"] - r["beta"]) <= rel * abs(r["beta"]) + 1e-12, (k, q["beta"], r["beta"], q["t"], r["stat"])
+        assert abs(q["t"] - r["stat"]) <= 10 * rel * abs(r["stat"]) + 1e-10, (k, q["t"], r["stat"])
         assert log10_diff(q["p"], r["p"]) < max(1e-8, 100 * rel)
     # best SNP per gene: identical, or a near-tie in p
     for gi in range(len(genes)):

@@ -75,6 +75,32 @@ def test_trans_lm_excludes_cis_windows(ctx):
     _check_scan(res, ora, pairs_ref, 1e-3, n - X.shape[1] - 1)
 
 
+@pytest.mark.parametrize("shuffle_snps", [False, True])
+def test_cis_scope_matches_oracle(ctx, shuffle_snps):
+    """Scope 2 (cis): only each gene's window. SNPs in position order take the
+    banded tile list; a shuffled SNP order takes the masked full grid."""
+    g, rows, Y, X = _case(seed=23, G=140)
+    n = g.codes.shape[1]
+    order = np.random.default_rng(4).permutation(rows.shape[0]) if shuffle_snps else np.arange(rows.shape[0])
+    rows_o = rows[order]
+    keep, _, _ = ctx.load_bed(rows_o, n, np.arange(n))
+    kidx = np.nonzero(keep)[0]
+    chrom_id = {c: i for i, c in enumerate(sorted(set(g.chrom)))}
+    schrom = np.array([chrom_id[g.chrom[order[s]]] for s in kidx], np.int32)
+    spos = g.pos[order[kidx]]
+    rng = np.random.default_rng(1)
+    G = Y.shape[1]
+    gchrom = rng.integers(-1, 3, G).astype(np.int32)
+    center = np.sort(rng.integers(1, 3_000_000, G))
+    glo, ghi = np.maximum(center - 300_000, 1), center + 300_000
+    res = ctx.scan_trans_lm(Y, X, pthr=1e-2, windows=(gchrom, glo, ghi, schrom, spos, 2))
+    inwin = oracle_scan.windows_mask(schrom, spos, gchrom, glo, ghi)
+    dos = R.decode_bed_rows(rows_o, n, np.arange(n), "impute", 0.8, 0.0).dosage[kidx]
+    ora, pairs_ref = oracle_scan.trans_lm(dos, Y, X, 1e-2, excl=~inwin)
+    assert np.array_equal(res[0]["n_tested"], ora["n_tested"])
+    _check_scan(res, ora, pairs_ref, 1e-2, n - X.shape[1] - 1)
+
+
 def test_trans_lm_stage2_candidates(ctx):
     g, rows, Y, X = _case(seed=31, G=64)
     n = g.codes.shape[1]

@@ -74,7 +74,7 @@ def test_trans_lmm_matches_oracle(ncov, prec):
     _check_scan(res[:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
 
 
-def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam):
+def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam, pthr=1e-3, excl=None):
     """REML delta: equal to the oracle's within 1e-5, or, where they differ,
     an optimum of the same objective within 1e-6 of it. That happens at the
     edge of the search (grid best 1e-5, golden section down to 2.5e-6): the
@@ -91,7 +91,41 @@ def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam):
         yt = Q.T @ Y[:, j]
         f_dev, f_ora = R.reml_negll(d_dev[j], yt, Xt, lam, df), R.reml_negll(d_ora[j], yt, Xt, lam, df)
         assert abs(f_dev - f_ora) <= 1e-6 * abs(f_ora), (j, d_dev[j], d_ora[j], f_dev, f_ora)
-    return oracle_scan.trans_lmm(G, Y, X, Q, lam, 1e-3, deltas=np.where(flat, d_dev, np.nan))
+    return oracle_scan.trans_lmm(G, Y, X, Q, lam, pthr, excl=excl, deltas=np.where(flat, d_dev, np.nan))
+
+
+@pytest.mark.parametrize("ncov", [0, 3])
+def test_cis_lmm_matches_oracle(ncov):
+    """Scope 2 (cis) on the LMM paths: one TMEM group (p = 1, banded tiles of
+    128 SNPs) and grouped accumulators (p = 4, banded tiles of 64 SNPs).
+    beta / t within 1e-5 (the north-star bar is 1e-4): genes whose REML delta
+    sits at the top of the search (~3e5) weight K's null space ~1e5 times the
+    rest, and S = gg - a'A00^-1 a then cancels enough for FP64 summation order
+    to show at 1e-6."""
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(seed=19, ncov=ncov)
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    chrom_id = {c: i for i, c in enumerate(sorted(set(g.chrom)))}
+    schrom = np.array([chrom_id[g.chrom[s]] for s in k], np.int32)
+    spos = g.pos[k]
+    rng = np.random.default_rng(2)
+    G = Y.shape[1]
+    gchrom = rng.integers(0, 2, G).astype(np.int32)
+    center = rng.integers(1, 4_000_000, G)
+    glo, ghi = np.maximum(center - 500_000, 1), center + 500_000
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n))
+        c.set_basis(Q, lam)
+        res = c.scan_trans_lmm(Y, X, pthr=1e-2, windows=(gchrom, glo, ghi, schrom, spos, 2))
+    inwin = oracle_scan.windows_mask(schrom, spos, gchrom, glo, ghi)
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-2, excl=~inwin)
+    ora, pairs_ref = _at_device_delta(res[3], ora, pairs_ref, dec.dosage[k], Y, X, Q, lam, 1e-2, ~inwin)
+    assert np.array_equal(res[0]["n_tested"], ora["n_tested"])
+    _check_scan(res[:3], ora, pairs_ref, 1e-2, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-5)
 
 
 def test_trans_lmm_device_basis_statistics():
