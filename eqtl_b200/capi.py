@@ -46,7 +46,7 @@ class ScanParams(C.Structure):
                 ("pthr", C.c_double), ("perm_thr", C.c_double),
                 ("gene_chrom", C.POINTER(C.c_int32)), ("gene_lo", C.POINTER(C.c_int64)),
                 ("gene_hi", C.POINTER(C.c_int64)), ("snp_chrom", C.POINTER(C.c_int32)),
-                ("snp_pos", C.POINTER(C.c_int64))]
+                ("snp_pos", C.POINTER(C.c_int64)), ("y_rotated", C.c_int32)]
 
 
 GENE_DTYPE = np.dtype([("n_tested", np.int32), ("acat_used", np.int32), ("acat_tan_sum", np.float64),

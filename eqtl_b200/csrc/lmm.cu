@@ -924,7 +924,7 @@ void lmm_rotate(eqtl_ctx* ctx) {
 // ------------------------------------------------------------------- REML
 // Per-gene REML prep into the context workspace (ws.Ytil, Xtil, delta, chi0,
 // ainv, rss) from the resident phenotypes.
-void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph) {
+void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
   const int n = ph.n, G = ph.G, p = ph.p;
   EQTL_CHECK(ctx->have_basis && ctx->basis.n == n, EQTL_E_STATE, "LMM prep needs an eigenbasis of size n");
   EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED, "the device LMM handles 1 <= p <= 16 covariate columns");
@@ -934,9 +934,13 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph) {
   ws.Ytil.alloc(static_cast<size_t>(n) * G);
   ws.Xtil.alloc(static_cast<size_t>(n) * p);
   const double one = 1.0, zero = 0.0;
-  EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ph.Y.p, n, &zero, ws.Ytil.p,
-                         n) == CUBLAS_STATUS_SUCCESS,
-             EQTL_E_CUDA, "Q'Y failed");
+  if (y_rotated) {
+    EQTL_CUDA(cudaMemcpyAsync(ws.Ytil.p, ph.Y.p, sizeof(double) * n * G, cudaMemcpyDeviceToDevice, st));
+  } else {
+    EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ph.Y.p, n, &zero,
+                           ws.Ytil.p, n) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "Q'Y failed");
+  }
   EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, n, p, n, &one, ctx->basis.Q.p, n, ph.X.p, n, &zero, ws.Xtil.p,
                          n) == CUBLAS_STATUS_SUCCESS,
              EQTL_E_CUDA, "Q'X failed");
@@ -1107,7 +1111,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
   lmm_rotate(ctx);
   std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
-  lmm_prep(ctx, ph);
+  lmm_prep(ctx, ph, prm->y_rotated != 0);
 
   // gene-side operands
   const int k_pad = g.k_pad;
@@ -1243,7 +1247,7 @@ void test_pairs_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y,
     EQTL_CHECK(q.x >= 0 && q.x < G && q.y >= 0 && q.y < g.m, EQTL_E_ARG, "test_pairs: pair index out of range");
   const double df = static_cast<double>(n - p - 1);
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
-  lmm_prep(ctx, ph);
+  lmm_prep(ctx, ph, prm->y_rotated != 0);
   lmm_gate(ctx);
   std::vector<uint8_t> ok(static_cast<size_t>(g.m));
   ws.ok.download(ok.data(), static_cast<size_t>(g.m), ctx->stream);

@@ -299,6 +299,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_trans_lm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0 && p > 0 && p <= kMaxP, EQTL_E_ARG, "scan_trans_lm: need 1 <= p <= 32 and genes > 0");
   EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_trans_lm: more than 2^30 kept SNPs");
+  EQTL_CHECK(prm->y_rotated == 0, EQTL_E_ARG, "y_rotated applies to the LMM only");
   cudaStream_t st = ctx->stream;
   const double df = static_cast<double>(n - p - 1);
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);

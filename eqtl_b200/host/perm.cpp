@@ -2,18 +2,21 @@
 //   LM    the permuted phenotype is the null residual y_s = y - X (X'X)^-1 X'y
 //         with its entries shuffled (include/eqtl/scan_cis.hpp:68-176).
 //   LMM   the whitened spectral residual w = (y~ - X~ b0) * sqrt(dinv) is
-//         shuffled, un-whitened and mapped back to samples:
-//         y_b = Q (X~ b0 + w_perm / sqrt(max(dinv, 1e-12)))
+//         shuffled and un-whitened, y~_b = X~ b0 + w_perm / sqrt(max(dinv, 1e-12))
 //         (src/scan_perm.cpp:48-120), with the gene's REML delta from the scan.
+//         The reference maps y~_b back to samples through Q and its null fit
+//         rotates it again; the device takes y~_b as it is (y_rotated).
 // Each permutation b of a gene draws its shuffle from std::mt19937 seeded
 // with (seed or 1) + 9973 b + fnv1a(gene) through std::shuffle, so the index
-// sequences are the reference's. Every permuted column gets a fresh null fit
-// and the FP64 tests of the gene's cached SNPs on the device
-// (eqtl_test_pairs); min p over finite p gives T_b = -log10 min p, then
-// p_emp and the beta approximation per gene.
+// sequences are the reference's; columns are built on all host threads.
+// Every permuted column gets a fresh null fit on the device. Cis: the banded
+// cis scan of all columns, each with its gene's window; min p = the column's
+// FP64-refined best SNP. Trans/gw stage 2: FP64 tests of the gene's top-K
+// SNPs (eqtl_test_pairs). Then p_emp and the beta approximation per gene.
 #include <algorithm>
 #include <numeric>
 #include <random>
+#include <thread>
 
 #include "perm.hpp"
 
@@ -80,22 +83,18 @@ PermBase lm_base(const Study& st, const std::vector<double>& y) {
   return B;
 }
 
-PermBase lmm_base(const Study& st, const std::vector<double>& y, double delta) {
+// y~ = Q'y, X~ = Q'X and the gene's GLS fit at its REML delta: the base of
+// the LMM permutations, in the eigenbasis.
+PermBase lmm_base(const Study& st, const std::vector<double>& y, double delta, const std::vector<double>& Xt) {
   const size_t n = st.samples.size();
   const int p = st.p;
   const std::vector<double>& Q = st.basis_Q;  // column-major, column j = eigenvector j
-  std::vector<double> yt(n), Xt(static_cast<size_t>(p) * n), dinv(n);
+  std::vector<double> yt(n), dinv(n);
   for (size_t j = 0; j < n; ++j) {
     const double* q = &Q[j * n];
     double s = 0;
     for (size_t i = 0; i < n; ++i) s += q[i] * y[i];
     yt[j] = s;
-    for (int a = 0; a < p; ++a) {
-      double sa = 0;
-      const double* xa = &st.X[static_cast<size_t>(a) * n];
-      for (size_t i = 0; i < n; ++i) sa += q[i] * xa[i];
-      Xt[static_cast<size_t>(a) * n + j] = sa;
-    }
     dinv[j] = 1.0 / std::max(delta * st.basis_lambda[j] + 1.0, 1e-12);
   }
   std::vector<double> A(static_cast<size_t>(p) * p), r(p);
@@ -120,7 +119,7 @@ PermBase lmm_base(const Study& st, const std::vector<double>& y, double delta) {
   return B;
 }
 
-// Phenotype column of permutation b of `gene`.
+// Column of permutation b of `gene`: LM in sample space, LMM rotated.
 void permuted_column(const Study& st, const std::string& model, const PermBase& B, const std::string& gene, int b,
                      double* col) {
   const size_t n = B.base.size();
@@ -132,15 +131,22 @@ void permuted_column(const Study& st, const std::string& model, const PermBase& 
     for (size_t i = 0; i < n; ++i) col[i] = B.base[idx[i]];
     return;
   }
-  std::vector<double> v(n);
-  for (size_t j = 0; j < n; ++j) v[j] = B.xb0[j] + B.base[idx[j]] / std::sqrt(std::max(B.dinv[j], 1e-12));
-  const std::vector<double>& Q = st.basis_Q;
-  std::fill(col, col + n, 0.0);
-  for (size_t j = 0; j < n; ++j) {
-    const double* q = &Q[j * n];
-    const double vj = v[j];
-    for (size_t i = 0; i < n; ++i) col[i] += q[i] * vj;
+  for (size_t j = 0; j < n; ++j) col[j] = B.xb0[j] + B.base[idx[j]] / std::sqrt(std::max(B.dinv[j], 1e-12));
+}
+
+template <class F>
+void parallel_for(size_t n, F&& f) {
+  const size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(n, 1));
+  if (nt <= 1) {
+    for (size_t i = 0; i < n; ++i) f(i);
+    return;
   }
+  std::vector<std::thread> th;
+  for (size_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (size_t i = t; i < n; i += nt) f(i);
+    });
+  for (auto& x : th) x.join();
 }
 
 }  // namespace
@@ -153,42 +159,67 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   std::vector<PermOut> out(genes.size());
   std::vector<size_t> active;
   for (size_t j = 0; j < genes.size(); ++j)
-    if (genes[j].active && !genes[j].snps.empty()) active.push_back(j);
+    if (genes[j].active && (genes[j].window || !genes[j].snps.empty())) active.push_back(j);
   if (active.empty() || B <= 0) return out;
-  if (model == "lmm" && st.basis_Q.size() != n * n) die("internal: LMM permutations need the eigenbasis on the host");
+  const bool lmm = model == "lmm";
+  if (lmm && st.basis_Q.size() != n * n) die("internal: LMM permutations need the eigenbasis on the host");
+  std::vector<double> Xt;  // LMM: X~ = Q'X, shared by every gene
+  if (lmm) {
+    Xt.assign(static_cast<size_t>(st.p) * n, 0.0);
+    for (int a = 0; a < st.p; ++a)
+      for (size_t j = 0; j < n; ++j) {
+        const double* q = &st.basis_Q[j * n];
+        double s = 0;
+        for (size_t i = 0; i < n; ++i) s += q[i] * st.X[static_cast<size_t>(a) * n + i];
+        Xt[a * n + j] = s;
+      }
+  }
   // genes per device batch: keep the permuted phenotype block near 2^26 doubles
   const size_t cols_budget = std::max<size_t>(static_cast<size_t>(B), (size_t(1) << 26) / std::max<size_t>(n, 1));
   const size_t genes_per_batch = std::max<size_t>(1, cols_budget / static_cast<size_t>(B));
-  eqtl_scan_params prm{};
-  prm.n = static_cast<int32_t>(n);
-  prm.p = st.p;
   for (size_t a = 0; a < active.size(); a += genes_per_batch) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
-    std::vector<double> Y(cols * n);
-    std::vector<int32_t> pc;
-    std::vector<int64_t> ps;
-    for (size_t gi = 0; gi < nb; ++gi) {
+    std::vector<PermBase> bases(nb);
+    parallel_for(nb, [&](size_t gi) {
       const PermGene& g = genes[active[a + gi]];
-      const PermBase base = model == "lm" ? lm_base(st, g.y) : lmm_base(st, g.y, delta[active[a + gi]]);
-      for (int b = 0; b < B; ++b) {
-        const size_t c = gi * B + b;
-        permuted_column(st, model, base, g.name, b, &Y[c * n]);
-        for (int64_t s : g.snps) {
+      bases[gi] = lmm ? lmm_base(st, g.y, delta[active[a + gi]], Xt) : lm_base(st, g.y);
+    });
+    std::vector<double> Y(cols * n);
+    parallel_for(cols, [&](size_t c) {
+      const size_t gi = c / B;
+      permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &Y[c * n]);
+    });
+    std::vector<double> minp(cols, 1.0);
+    if (genes[active[a]].window) {
+      // cis: one banded cis scan of every column with its gene's window
+      std::vector<const GeneLoc*> win(cols);
+      for (size_t c = 0; c < cols; ++c) win[c] = genes[active[a + c / B]].window;
+      const ScanResult R = scan_columns(st, model, Y, cols, win, 2, 0.0, 0.0, lmm);
+      for (size_t c = 0; c < cols; ++c)
+        if (R.genes[c].n_tested > 0 && R.genes[c].best_snp >= 0 && std::isfinite(R.genes[c].best_p))
+          minp[c] = std::min(1.0, R.genes[c].best_p);
+    } else {
+      // stage 2: FP64 tests of each gene's top-K SNPs
+      std::vector<int32_t> pc;
+      std::vector<int64_t> ps;
+      for (size_t c = 0; c < cols; ++c)
+        for (int64_t s : genes[active[a + c / B]].snps) {
           pc.push_back(static_cast<int32_t>(c));
           ps.push_back(s);
         }
-      }
+      eqtl_scan_params prm{};
+      prm.n = static_cast<int32_t>(n);
+      prm.p = st.p;
+      prm.n_genes = static_cast<int32_t>(cols);
+      prm.y_rotated = lmm ? 1 : 0;
+      std::vector<eqtl_pair> res(pc.size());
+      st.dev->check(eqtl_test_pairs(st.dev->ctx, lmm ? EQTL_MODEL_LMM : EQTL_MODEL_LM, &prm, Y.data(), st.X.data(),
+                                    pc.data(), ps.data(), static_cast<int64_t>(pc.size()), res.data(), nullptr),
+                    "permutation tests");
+      for (size_t i = 0; i < res.size(); ++i)
+        if (std::isfinite(res[i].p) && res[i].p < minp[pc[i]]) minp[pc[i]] = res[i].p;
     }
-    prm.n_genes = static_cast<int32_t>(cols);
-    std::vector<eqtl_pair> res(pc.size());
-    st.dev->check(eqtl_test_pairs(st.dev->ctx, model == "lm" ? EQTL_MODEL_LM : EQTL_MODEL_LMM, &prm, Y.data(),
-                                  st.X.data(), pc.data(), ps.data(), static_cast<int64_t>(pc.size()), res.data(),
-                                  nullptr),
-                  "permutation tests");
-    std::vector<double> minp(cols, 1.0);
-    for (size_t i = 0; i < res.size(); ++i)
-      if (std::isfinite(res[i].p) && res[i].p < minp[pc[i]]) minp[pc[i]] = res[i].p;
     for (size_t gi = 0; gi < nb; ++gi) {
       const PermGene& g = genes[active[a + gi]];
       PermOut& o = out[active[a + gi]];

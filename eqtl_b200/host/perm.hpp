@@ -15,10 +15,11 @@ struct ScanResult {
 
 struct PermGene {
   std::string name;
-  std::vector<double> y;        // the gene's phenotype (after --pheno-norm)
-  double obs_min_p = 1.0;       // observed min p over the gene's tested SNPs
-  bool active = false;          // gene takes part in the permutations
-  std::vector<int64_t> snps;    // kept-SNP indices the permutations test
+  std::vector<double> y;            // the gene's phenotype (after --pheno-norm)
+  double obs_min_p = 1.0;           // observed min p over the gene's tested SNPs
+  bool active = false;              // gene takes part in the permutations
+  const GeneLoc* window = nullptr;  // cis: permutations test the gene's window
+  std::vector<int64_t> snps;        // trans/gw stage 2: the top-K kept SNPs
 };
 
 struct PermOut {
@@ -26,6 +27,13 @@ struct PermOut {
   double p_emp = NAN;
   BetaFit beta;
 };
+
+// One device scan of explicit phenotype columns Y [cols][n]: scope mode 0 gw,
+// 1 trans, 2 cis with per-column windows (null = no location); LMM columns
+// may already be rotated into the eigenbasis.
+ScanResult scan_columns(const Study& st, const std::string& model, const std::vector<double>& Y, size_t cols,
+                        const std::vector<const GeneLoc*>& windows, int mode, double pthr, double perm_thr,
+                        bool rotated);
 
 std::vector<PermOut> run_permutations(const Study& st, const std::string& model, const std::vector<PermGene>& genes,
                                       const std::vector<double>& delta);

@@ -94,36 +94,37 @@ std::vector<double> gene_y(const Study& st, int g) {
   return y;
 }
 
-// One device scan over `jobs`; mode 0 gw, 1 trans (exclude windows), 2 cis.
-ScanResult device_scan(const Study& st, const std::string& model, const std::vector<Job>& jobs, int mode,
-                       double pthr, double perm_thr) {
+}  // namespace
+
+ScanResult scan_columns(const Study& st, const std::string& model, const std::vector<double>& Y, size_t cols,
+                        const std::vector<const GeneLoc*>& windows, int mode, double pthr, double perm_thr,
+                        bool rotated) {
   const Options& opt = *st.opt;
-  const size_t n = st.samples.size(), J = jobs.size();
+  const size_t n = st.samples.size(), J = cols;
   ScanResult R;
   R.n = static_cast<int>(n);
-  std::vector<double> Y(J * n);
-  for (size_t j = 0; j < J; ++j) {
-    const std::vector<double> y = gene_y(st, jobs[j].gene);
-    std::copy(y.begin(), y.end(), Y.begin() + j * n);
-  }
-  // gene windows and the kept SNPs' positions, chromosomes by normalised name
+  // windows and the kept SNPs' positions, chromosomes by normalised name
   std::unordered_map<std::string, int32_t> cid;
   auto chrom_id = [&](const std::string& c) {
     return cid.emplace(chrom_key(c), static_cast<int32_t>(cid.size())).first->second;
   };
   const auto& kept = st.geno->kept;
-  std::vector<int32_t> gchr(J, -1), schr(kept.size());
-  std::vector<int64_t> glo(J, 0), ghi(J, -1), spos(kept.size());
-  for (size_t k = 0; k < kept.size(); ++k) {
-    schr[k] = chrom_id(st.plink->chrom[kept[k]]);
-    spos[k] = st.plink->pos[kept[k]];
-  }
-  for (size_t j = 0; j < J; ++j)
-    if (jobs[j].loc) {
-      gchr[j] = chrom_id(jobs[j].loc->chrom);
-      glo[j] = std::max<int64_t>(jobs[j].loc->start - opt.window, 1);
-      ghi[j] = jobs[j].loc->end + opt.window;
+  std::vector<int32_t> gchr(J, -1), schr;
+  std::vector<int64_t> glo(J, 0), ghi(J, -1), spos;
+  if (mode != 0) {
+    schr.resize(kept.size());
+    spos.resize(kept.size());
+    for (size_t k = 0; k < kept.size(); ++k) {
+      schr[k] = chrom_id(st.plink->chrom[kept[k]]);
+      spos[k] = st.plink->pos[kept[k]];
     }
+    for (size_t j = 0; j < J; ++j)
+      if (windows[j]) {
+        gchr[j] = chrom_id(windows[j]->chrom);
+        glo[j] = std::max<int64_t>(windows[j]->start - opt.window, 1);
+        ghi[j] = windows[j]->end + opt.window;
+      }
+  }
   eqtl_scan_params prm{};
   prm.n = static_cast<int32_t>(n);
   prm.n_genes = static_cast<int32_t>(J);
@@ -131,6 +132,7 @@ ScanResult device_scan(const Study& st, const std::string& model, const std::vec
   prm.exclude_cis = mode;
   prm.pthr = pthr;
   prm.perm_thr = perm_thr;
+  prm.y_rotated = rotated ? 1 : 0;
   if (mode != 0) {
     prm.gene_chrom = gchr.data();
     prm.gene_lo = glo.data();
@@ -161,6 +163,22 @@ ScanResult device_scan(const Study& st, const std::string& model, const std::vec
     return R;
   }
   die("scan output did not fit after resizing");
+}
+
+namespace {
+
+// One device scan over `jobs`; mode 0 gw, 1 trans (exclude windows), 2 cis.
+ScanResult device_scan(const Study& st, const std::string& model, const std::vector<Job>& jobs, int mode,
+                       double pthr, double perm_thr) {
+  const size_t n = st.samples.size(), J = jobs.size();
+  std::vector<double> Y(J * n);
+  std::vector<const GeneLoc*> windows(J);
+  for (size_t j = 0; j < J; ++j) {
+    const std::vector<double> y = gene_y(st, jobs[j].gene);
+    std::copy(y.begin(), y.end(), Y.begin() + j * n);
+    windows[j] = jobs[j].loc;
+  }
+  return scan_columns(st, model, Y, J, windows, mode, pthr, perm_thr, false);
 }
 
 PairRow make_row(const Study& st, const std::string& gene, const GeneLoc* loc, int64_t kept_idx, double af,
@@ -331,19 +349,7 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
       pg[j].obs_min_p = R.genes[j].best_p;
       pg[j].active = R.genes[j].n_tested > 0;
     }
-    // every kept SNP inside the gene's window, in .bim order (the subset
-    // gate is applied where the permutations read the dosages)
-    const auto& kept = st.geno->kept;
-    for (size_t j = 0; j < jobs.size(); ++j) {
-      const GeneLoc& L = *jobs[j].loc;
-      const int64_t lo = std::max<int64_t>(L.start - opt.window, 1), hi = L.end + opt.window;
-      const std::string key = chrom_key(L.chrom);
-      for (size_t k = 0; k < kept.size(); ++k) {
-        const int64_t s = kept[k];
-        if (st.plink->pos[s] >= lo && st.plink->pos[s] <= hi && chrom_key(st.plink->chrom[s]) == key)
-          pg[j].snps.push_back(static_cast<int64_t>(k));
-      }
-    }
+    for (size_t j = 0; j < jobs.size(); ++j) pg[j].window = jobs[j].loc;  // permutations scan the window
     perms = run_permutations(st, model, pg, R.delta);
   }
   std::vector<size_t> order(R.pairs.size());

@@ -143,6 +143,8 @@ typedef struct {
   const int64_t* gene_hi;    /* [n_genes] window end (inclusive) */
   const int32_t* snp_chrom;  /* [n_kept] chromosome id of each kept SNP */
   const int64_t* snp_pos;    /* [n_kept] position of each kept SNP */
+  int32_t y_rotated;         /* LMM only: 1 = Y is already in the eigenbasis
+                              * (Q'y), as for permuted null phenotypes */
 } eqtl_scan_params;
 
 /* ------------------------------------------------------------ trans/gw LM
