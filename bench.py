@@ -304,6 +304,7 @@ def b200_arm(args, rank, world, local_rank):
            "roofline": roof, "gpu_launches": launches,
            "clocks": clk.summary(),
            "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": statistics.mean(e2e_ms) if e2e_ms else None,
+                   "ms_steps": [round(v, 1) for v in e2e_ms],
                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
 
     # ---- plain FP32 CUDA-core comparator of the same scan (scan kernel only)

@@ -13,6 +13,7 @@
 #include <map>
 #include <mutex>
 
+#include "host_par.hpp"
 #include "internal.hpp"
 #include "scan_host.hpp"
 #include "tstat.hpp"
@@ -176,9 +177,19 @@ void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std
       r.best_beta = r.best_se = r.best_t = r.best_r2 = 0.0;
     }
   }
-  std::sort(pairs.begin(), pairs.end(), [](const eqtl_pair& a, const eqtl_pair& b) {
-    return a.snp != b.snp ? a.snp < b.snp : a.gene < b.gene;
-  });
+  {
+    // (snp, gene) order through 64-bit keys: snp < 2^31, gene < 2^31
+    std::vector<uint64_t> key(pairs.size());
+    std::vector<uint32_t> idx(pairs.size());
+    for (size_t i = 0; i < pairs.size(); ++i) {
+      key[i] = (static_cast<uint64_t>(pairs[i].snp) << 32) | static_cast<uint32_t>(pairs[i].gene);
+      idx[i] = static_cast<uint32_t>(i);
+    }
+    radix_sort_u64(key, &idx);
+    std::vector<eqtl_pair> sorted(pairs.size());
+    for (size_t i = 0; i < idx.size(); ++i) sorted[i] = pairs[idx[i]];
+    pairs.swap(sorted);
+  }
   std::sort(cands.begin(), cands.end(), [](const eqtl_pair& a, const eqtl_pair& b) {
     if (a.gene != b.gene) return a.gene < b.gene;
     if (a.p != b.p) return a.p < b.p;
@@ -205,12 +216,21 @@ void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& re
 
 void add_acat_terms(eqtl_gene_result* genes, const std::vector<int2>& pairs, const std::vector<double>& p_pairs) {
   const long double kPiL = 3.14159265358979323846L;
-  for (size_t i = 0; i < pairs.size(); ++i) {
+  // terms on every host thread, then added in pair order (the sums do not
+  // depend on the thread count)
+  std::vector<double> term(pairs.size());
+  std::vector<uint8_t> use(pairs.size());
+  parallel_for(pairs.size(), [&](size_t i) {
     double p = p_pairs[i];
-    if (!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12) continue;  // AcatAcc::add guards
+    use[i] = !(!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12);  // AcatAcc::add guards
+    if (!use[i]) return;
     if (p <= 0.0) p = 1e-300;
+    term[i] = static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+  });
+  for (size_t i = 0; i < pairs.size(); ++i) {
+    if (!use[i]) continue;
     eqtl_gene_result& g = genes[pairs[i].x];
-    g.acat_tan_sum += static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+    g.acat_tan_sum += term[i];
     ++g.acat_used;
   }
 }
@@ -453,9 +473,15 @@ void ScanOutputs::collect(eqtl_gene_result* genes, std::vector<int2>& todo, std:
     genes[g].best_snp = -1;
     if (t[g] > 0 && b[g] != ~0ull) todo.push_back(make_int2(g, static_cast<int>(b[g] & 0xFFFFFFFFull)));
   }
-  std::sort(todo.begin(), todo.end(), [](int2 x, int2 y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
-  todo.erase(std::unique(todo.begin(), todo.end(), [](int2 x, int2 y) { return x.x == y.x && x.y == y.y; }),
-             todo.end());
+  // (gene, snp) order without duplicates, through 64-bit keys
+  std::vector<uint64_t> key(todo.size());
+  for (size_t i = 0; i < todo.size(); ++i)
+    key[i] = (static_cast<uint64_t>(static_cast<uint32_t>(todo[i].x)) << 32) | static_cast<uint32_t>(todo[i].y);
+  radix_sort_u64(key);
+  key.erase(std::unique(key.begin(), key.end()), key.end());
+  todo.resize(key.size());
+  for (size_t i = 0; i < key.size(); ++i)
+    todo[i] = make_int2(static_cast<int>(key[i] >> 32), static_cast<int>(key[i] & 0xFFFFFFFFull));
 }
 
 }  // namespace eqtl

@@ -7,7 +7,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -33,6 +35,25 @@ struct Error : std::runtime_error {
   do {                                                      \
     if (!(cond)) throw ::eqtl::Error((code), (msg));        \
   } while (0)
+
+// Opt-in host trace: with EQTL_TRACE set in the environment, mark() prints
+// the host time since the previous mark to stderr. Phases that end in a
+// stream synchronisation include the device time they waited for.
+struct HostTrace {
+  bool on;
+  const char* scope;
+  std::chrono::steady_clock::time_point t;
+  explicit HostTrace(const char* s) : on(std::getenv("EQTL_TRACE") != nullptr), scope(s) {
+    if (on) t = std::chrono::steady_clock::now();
+  }
+  void mark(const char* what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[eqtl trace] %s %s %.3f ms\n", scope, what,
+                 std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
 
 // Device buffer that keeps its allocation: alloc() only reallocates when
 // the requested count exceeds the capacity, so per-call workspaces held by
@@ -183,6 +204,7 @@ struct eqtl_ctx {
   eqtl::Workspace ws;
   bool have_basis = false;
   int precision = EQTL_PREC_SPLIT_F16;
+  std::vector<int> host_mark;  // per-kept-SNP scratch of the refinement's index
 };
 
 namespace eqtl {

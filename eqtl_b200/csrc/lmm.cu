@@ -144,15 +144,30 @@ __device__ bool chol_solve(const double* A, const double* b, double* x, double* 
 __device__ double reml_eval(double delta, const double* __restrict__ yt, const double* __restrict__ Xt,
                             const double* __restrict__ lam, int n, int p, double* wsh, RemlShared& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  double ld = 0, ydy = 0;
+  // sum of log v as the log of products of up to eight factors: every factor
+  // lies in [1e-12, 1e36] (larger ones take their own log), so a product
+  // stays within [1e-96, 1e288]; one FP64 log per eight samples instead of
+  // one per sample
+  double ld = 0, ydy = 0, prod = 1.0;
+  int nprod = 0;
   for (int i = tid; i < n; i += blockDim.x) {
     double v = delta * lam[i] + 1.0;
     if (v < 1e-12) v = 1e-12;
     const double w = 1.0 / v;
     wsh[i] = w;
-    ld += log(v);
+    if (v <= 1e36) {
+      prod *= v;
+      if (++nprod == 8) {
+        ld += log(prod);
+        prod = 1.0;
+        nprod = 0;
+      }
+    } else {
+      ld += log(v);
+    }
     ydy += w * yt[i] * yt[i];
   }
+  ld += log(prod);
   for (int o = 16; o; o >>= 1) {
     ld += __shfl_xor_sync(0xffffffffu, ld, o);
     ydy += __shfl_xor_sync(0xffffffffu, ydy, o);
@@ -208,8 +223,82 @@ __device__ double reml_eval(double delta, const double* __restrict__ yt, const d
   return r;
 }
 
-// One CTA per gene: optimize_delta (src/model_lmm.cpp:39-86) and the
-// prep_lmm caches (:124-153). Ytil [G][n], Xtil [p][n].
+// optimize_delta (src/model_lmm.cpp:39-86): grid 1e-5..1e5 x2 (and 1.0), 40
+// golden-section steps on [best/4, best*4] clipped to [1e-8, 1e6], then up to
+// 8 Newton steps on central differences. f(d) returns -loglik and is called
+// by every thread of the unit (warp or block) that evaluates it.
+template <class F>
+__device__ double optimize_delta_dev(F&& f, int df) {
+  double d = 1.0;
+  if (df <= 0) return d;
+  double best_d = 1.0;
+  double best_ll = f(1.0);
+  for (double dd = 1e-5; dd <= 1e5; dd *= 2.0) {
+    const double v = f(dd);
+    if (v < best_ll) {
+      best_ll = v;
+      best_d = dd;
+    }
+  }
+  double lo = best_d / 4.0, hi = best_d * 4.0;
+  if (lo < 1e-8) lo = 1e-8;
+  if (hi > 1e6) hi = 1e6;
+  const double phi = (1.0 + sqrt(5.0)) / 2.0;
+  for (int it = 0; it < 40; ++it) {
+    const double m1 = hi - (hi - lo) / phi;
+    const double m2 = lo + (hi - lo) / phi;
+    const double f1 = f(m1);
+    const double f2 = f(m2);
+    if (f1 < f2) hi = m2;
+    else lo = m1;
+  }
+  d = 0.5 * (lo + hi);
+  double cur = f(d);
+  for (int it = 0; it < 8; ++it) {
+    const double h = fmax(d * 1e-4, 1e-9);
+    const double fm = f(d - h);
+    const double fp = f(d + h);
+    const double g1 = (fp - fm) / (2.0 * h);
+    const double g2 = (fp - 2.0 * cur + fm) / (h * h);
+    if (!(g2 > 1e-12)) break;
+    const double step = g1 / g2;
+    const double dn = d - step;
+    if (!(dn > 1e-8 && dn < 1e6)) break;
+    const double vn = f(dn);
+    if (!(vn < cur)) break;
+    d = dn;
+    cur = vn;
+    if (fabs(step) < d * 1e-8) break;
+  }
+  return d;
+}
+
+// prep_lmm caches (src/model_lmm.cpp:124-153) from A = X~'DX~ (p x p,
+// row-major), b = X~'Dy~ and y~'Dy~ at the chosen delta; one thread.
+__device__ void reml_caches(double* A, const double* b, double y_dy, int p, int g, double* L, double* e,
+                            double* x, double* chi0_out, double* ainv_out, double* rss_out) {
+  double chi0[kMaxPLmm];
+  double ld;
+  const bool ok = chol_solve(A, b, chi0, &ld, p, L);
+  double rss = y_dy;
+  if (ok) {
+    for (int k = 0; k < p; ++k) rss -= b[k] * chi0[k];
+    if (rss < 0) rss = 0;
+    for (int c = 0; c < p; ++c) {  // A00^-1 column by column
+      for (int i = 0; i < p; ++i) e[i] = (i == c) ? 1.0 : 0.0;
+      double dummy;
+      chol_solve(A, e, x, &dummy, p, L);
+      for (int i = 0; i < p; ++i) ainv_out[(static_cast<int64_t>(g) * p + i) * p + c] = x[i];
+    }
+  } else {
+    for (int k = 0; k < p; ++k) chi0[k] = 0;
+    for (int i = 0; i < p * p; ++i) ainv_out[static_cast<int64_t>(g) * p * p + i] = 0;
+  }
+  rss_out[g] = rss;
+  for (int k = 0; k < p; ++k) chi0_out[static_cast<int64_t>(g) * p + k] = chi0[k];
+}
+
+// One CTA per gene, any p <= kMaxPLmm. Ytil [G][n], Xtil [p][n].
 __global__ void __launch_bounds__(256) reml_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
                                                    const double* __restrict__ lam, int n, int p, int G,
                                                    double* delta_out, double* chi0_out, double* ainv_out,
@@ -220,80 +309,127 @@ __global__ void __launch_bounds__(256) reml_kernel(const double* __restrict__ Yt
   if (g >= G) return;
   const double* yt = Ytil + static_cast<int64_t>(g) * n;
   auto f = [&](double d) { return reml_eval(d, yt, Xtil, lam, n, p, wsh, sh); };
-  const int df = n - p;
-  double d = 1.0;
-  if (df > 0) {
-    double best_d = 1.0;
-    double best_ll = f(1.0);
-    for (double dd = 1e-5; dd <= 1e5; dd *= 2.0) {
-      const double v = f(dd);
-      if (v < best_ll) {
-        best_ll = v;
-        best_d = dd;
-      }
-    }
-    double lo = best_d / 4.0, hi = best_d * 4.0;
-    if (lo < 1e-8) lo = 1e-8;
-    if (hi > 1e6) hi = 1e6;
-    const double phi = (1.0 + sqrt(5.0)) / 2.0;
-    for (int it = 0; it < 40; ++it) {
-      const double m1 = hi - (hi - lo) / phi;
-      const double m2 = lo + (hi - lo) / phi;
-      const double f1 = f(m1);
-      const double f2 = f(m2);
-      if (f1 < f2) hi = m2;
-      else lo = m1;
-    }
-    d = 0.5 * (lo + hi);
-    double cur = f(d);
-    for (int it = 0; it < 8; ++it) {
-      const double h = fmax(d * 1e-4, 1e-9);
-      const double fm = f(d - h);
-      const double fp = f(d + h);
-      const double g1 = (fp - fm) / (2.0 * h);
-      const double g2 = (fp - 2.0 * cur + fm) / (h * h);
-      if (!(g2 > 1e-12)) break;
-      const double step = g1 / g2;
-      const double dn = d - step;
-      if (!(dn > 1e-8 && dn < 1e6)) break;
-      const double vn = f(dn);
-      if (!(vn < cur)) break;
-      d = dn;
-      cur = vn;
-      if (fabs(step) < d * 1e-8) break;
-    }
-  }
-  // prep_lmm caches at the chosen delta: one more weighted reduction
-  f(d);
+  const double d = optimize_delta_dev(f, n - p);
+  f(d);  // the caches at the chosen delta: one more weighted reduction
   if (threadIdx.x == 0) {
     const int nq = p * (p + 1) / 2;
-    double* A = sh.A;
-    double chi0[kMaxPLmm];
     for (int a = 0; a < p; ++a)
-      for (int b = a; b < p; ++b) A[a * p + b] = A[b * p + a] = sh.res[tri(a, b, p)];
-    const double* XtDy = sh.res + nq;
+      for (int b = a; b < p; ++b) sh.A[a * p + b] = sh.A[b * p + a] = sh.res[tri(a, b, p)];
     double y_dy = 0;
     for (int w = 0; w < (blockDim.x >> 5); ++w) y_dy += sh.red[1][w];
-    double ld;
-    bool ok = chol_solve(A, XtDy, chi0, &ld, p, sh.L);
-    double rss = y_dy;
-    if (ok) {
-      for (int k = 0; k < p; ++k) rss -= XtDy[k] * chi0[k];
-      if (rss < 0) rss = 0;
-      // A00^-1 column by column
-      for (int c = 0; c < p; ++c) {
-        for (int i = 0; i < p; ++i) sh.e[i] = (i == c) ? 1.0 : 0.0;
-        double dummy;
-        chol_solve(A, sh.e, sh.x, &dummy, p, sh.L);
-        for (int i = 0; i < p; ++i) ainv_out[(static_cast<int64_t>(g) * p + i) * p + c] = sh.x[i];
+    delta_out[g] = d;
+    reml_caches(sh.A, sh.res + nq, y_dy, p, g, sh.L, sh.e, sh.x, chi0_out, ainv_out, rss_out);
+  }
+}
+
+// -loglik of reml_eval for P <= 3 covariate columns, evaluated by one warp:
+// each lane sums log v, w y^2, w x_a x_b and w y x_a over its samples in
+// registers, and xor-shuffle reductions give every lane the same totals
+// (IEEE addition is commutative), so there is no shared memory and no block
+// barrier. tot = [sum log v, y'Dy, X'DX packed (a <= b), X'Dy].
+template <int P>
+__device__ __forceinline__ double reml_eval_warp(double delta, const double* __restrict__ yt,
+                                                 const double* __restrict__ Xt, const double* __restrict__ lam,
+                                                 int n, double* tot) {
+  constexpr int NQ = P * (P + 1) / 2;
+  constexpr int V = 2 + NQ + P;
+  const int lane = threadIdx.x & 31;
+  double acc[V];
+#pragma unroll
+  for (int q = 0; q < V; ++q) acc[q] = 0.0;
+  double prod = 1.0;
+  int nprod = 0;
+  for (int i = lane; i < n; i += 32) {
+    double v = delta * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    if (v <= 1e36) {  // log of products of up to eight factors, as in reml_eval
+      prod *= v;
+      if (++nprod == 8) {
+        acc[0] += log(prod);
+        prod = 1.0;
+        nprod = 0;
       }
     } else {
-      for (int k = 0; k < p; ++k) chi0[k] = 0;
-      for (int i = 0; i < p * p; ++i) ainv_out[static_cast<int64_t>(g) * p * p + i] = 0;
+      acc[0] += log(v);
     }
+    const double y = yt[i];
+    acc[1] += w * y * y;
+    double x[P];
+#pragma unroll
+    for (int a = 0; a < P; ++a) x[a] = Xt[static_cast<int64_t>(a) * n + i];
+#pragma unroll
+    for (int a = 0; a < P; ++a) {
+#pragma unroll
+      for (int b = a; b < P; ++b) acc[2 + a * P - a * (a - 1) / 2 + (b - a)] += w * x[a] * x[b];
+      acc[2 + NQ + a] += w * y * x[a];
+    }
+  }
+  acc[0] += log(prod);
+#pragma unroll
+  for (int q = 0; q < V; ++q) {
+    double s = acc[q];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    tot[q] = s;
+  }
+  // Cholesky of X'DX; q = y'Dy - b'(X'DX)^-1 b as y'Dy - |z|^2 with L z = b
+  double L[P][P];
+  double logdet_x = 0.0;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    double d = tot[2 + j * P - j * (j - 1) / 2];
+#pragma unroll
+    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+    if (!(d > 0)) return 1e300;
+    L[j][j] = sqrt(d);
+    logdet_x += 2.0 * log(L[j][j]);
+#pragma unroll
+    for (int i = j + 1; i < P; ++i) {
+      double s = tot[2 + j * P - j * (j - 1) / 2 + (i - j)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+      L[i][j] = s / L[j][j];
+    }
+  }
+  double q = tot[1];
+  double z[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    double s = tot[2 + NQ + i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) s -= L[i][k] * z[k];
+    z[i] = s / L[i][i];
+    q -= z[i] * z[i];
+  }
+  if (q <= 0) q = 1e-12;
+  const double df = static_cast<double>(n - P);
+  return 0.5 * (df * log(q / df) + tot[0] + logdet_x);
+}
+
+// One warp per gene for P <= 3 (the common case: intercept and a few
+// covariates); same search and caches as reml_kernel.
+constexpr int kRemlWarpP = 3;
+template <int P>
+__global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict__ Ytil,
+                                                        const double* __restrict__ Xtil,
+                                                        const double* __restrict__ lam, int n, int G,
+                                                        double* delta_out, double* chi0_out, double* ainv_out,
+                                                        double* rss_out) {
+  constexpr int NQ = P * (P + 1) / 2;
+  const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (g >= G) return;  // whole warps only: no block barrier follows
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  double tot[2 + NQ + P];
+  auto f = [&](double d) { return reml_eval_warp<P>(d, yt, Xtil, lam, n, tot); };
+  const double d = optimize_delta_dev(f, n - P);
+  f(d);
+  if ((threadIdx.x & 31) == 0) {
+    double A[P * P], L[P * P], e[P], x[P];
+    for (int a = 0; a < P; ++a)
+      for (int b = a; b < P; ++b) A[a * P + b] = A[b * P + a] = tot[2 + a * P - a * (a - 1) / 2 + (b - a)];
     delta_out[g] = d;
-    rss_out[g] = rss;
-    for (int k = 0; k < p; ++k) chi0_out[static_cast<int64_t>(g) * p + k] = chi0[k];
+    reml_caches(A, tot + 2 + NQ, tot[1], P, g, L, e, x, chi0_out, ainv_out, rss_out);
   }
 }
 
@@ -948,10 +1084,22 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
   ws.chi0.alloc(static_cast<size_t>(G) * p);
   ws.ainv.alloc(static_cast<size_t>(G) * p * p);
   ws.rss.alloc(G);
-  const size_t smem = sizeof(double) * n;
+  ++ctx->launches;
+  if (p <= kRemlWarpP) {
+    const unsigned blocks = static_cast<unsigned>((G + 7) / 8);
+    auto args = [&](auto kern) {
+      kern<<<blocks, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, n, G, ws.delta.p, ws.chi0.p,
+                                   ws.ainv.p, ws.rss.p);
+    };
+    if (p == 1) args(reml_warp_kernel<1>);
+    else if (p == 2) args(reml_warp_kernel<2>);
+    else args(reml_warp_kernel<3>);
+    EQTL_CUDA(cudaGetLastError());
+    return;
+  }
+  const size_t smem = sizeof(double) * n;  // the n weights of the evaluation
   EQTL_CHECK(smem <= 200 * 1024, EQTL_E_UNSUPPORTED, "REML kernel holds n doubles in shared memory (n <= 25600)");
   EQTL_CUDA(cudaFuncSetAttribute(reml_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  ++ctx->launches;
   reml_kernel<<<G, 256, smem, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, n, p, G, ws.delta.p, ws.chi0.p,
                                     ws.ainv.p, ws.rss.p);
   EQTL_CUDA(cudaGetLastError());
@@ -1005,15 +1153,21 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
   cudaStream_t st = ctx->stream;
   const int n = g.n;
   std::vector<eqtl_pair> refined(todo.size());
+  HostTrace tr("lmm_refine_pairs");
   if (!todo.empty()) {
+    // distinct SNPs in index order and each pair's column among them, by a
+    // marker over the kept SNPs (O(m + pairs), no sort)
+    std::vector<int>& mark = ctx->host_mark;
+    mark.assign(static_cast<size_t>(g.m), -1);
+    for (const int2& q : todo) mark[q.y] = 0;
     std::vector<int> snps;
-    snps.reserve(todo.size());
-    for (const int2& q : todo) snps.push_back(q.y);
-    std::sort(snps.begin(), snps.end());
-    snps.erase(std::unique(snps.begin(), snps.end()), snps.end());
+    for (int64_t s = 0; s < g.m; ++s)
+      if (mark[s] == 0) {
+        mark[s] = static_cast<int>(snps.size());
+        snps.push_back(static_cast<int>(s));
+      }
     std::vector<int> pcol(todo.size());
-    for (size_t i = 0; i < todo.size(); ++i)
-      pcol[i] = static_cast<int>(std::lower_bound(snps.begin(), snps.end(), todo[i].y) - snps.begin());
+    for (size_t i = 0; i < todo.size(); ++i) pcol[i] = mark[todo[i].y];
     const int u = static_cast<int>(snps.size());
     DevBuf<int>& dsn = ws.ref_snps;
     DevBuf<int>& dpc = ws.ref_col;
@@ -1021,6 +1175,7 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
     dsn.upload(snps.data(), u, st);
     dpc.upload(pcol.data(), pcol.size(), st);
     dtodo.upload(todo.data(), todo.size(), st);
+    tr.mark("host index + upload");
     DevBuf<double>& graw = ws.graw;
     DevBuf<double>& gt = ws.gt;
     graw.alloc(static_cast<size_t>(n) * u);
@@ -1037,8 +1192,10 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
         gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), ws.Ytil.p, ws.Xtil.p, p, ctx->basis.lambda.p,
         ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p, df, ws.refined.p);
     EQTL_CUDA(cudaGetLastError());
+    tr.mark("launches");
     ws.refined.download(refined.data(), todo.size(), st);
     EQTL_CUDA(cudaStreamSynchronize(st));
+    tr.mark("device work + download");
   }
   return refined;
 }
@@ -1205,8 +1362,10 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     }
   }
   scan_timer.reset();
+  HostTrace tr("scan_trans_lmm");
   std::vector<int2> todo, deferred, tiny;
   so.collect(genes, todo, deferred, &tiny);
+  tr.mark("collect (waits for the scan)");
 
   // ---- FP64 refinement: rotate raw dosages of the SNPs involved
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
@@ -1215,9 +1374,18 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     EQTL_CUDA(cudaStreamSynchronize(st));
   }
   std::vector<eqtl_pair> refined = lmm_refine_pairs(ctx, p, df, todo);
+  tr.mark("refine pairs");
   add_deferred_acat(genes, refined, deferred);
-  add_acat_terms(genes, tiny, lmm_tiny_p(ctx, p, df, tiny));
+  tr.mark("deferred ACAT");
+  const std::vector<double> tiny_p = lmm_tiny_p(ctx, p, df, tiny);
+  tr.mark("tiny-|t| pairs");
+  add_acat_terms(genes, tiny, tiny_p);
+  tr.mark("tiny ACAT terms");
   finish_scan(prm, genes, refined, pairs, cands);
+  tr.mark("finish");
+  if (tr.on)
+    std::fprintf(stderr, "[eqtl trace] scan_trans_lmm counts: candidates %zu deferred %zu tiny %zu\n", todo.size(),
+                 deferred.size(), tiny.size());
 }
 
 void scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* delta_out,
