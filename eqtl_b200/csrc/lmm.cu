@@ -507,9 +507,17 @@ struct LmmEpiParams {
   GeneOut out;
 };
 
+// Accumulator order of the tile: [gg, a_0 .. a_{P-1}, NUM] (the gene-side
+// operands w, w o X~_k, w o r~ against Gt^2, Gt, Gt). The epilogue is
+// two-phase: S = gg - a' A00^-1 a of every pair of the warp's chunks first,
+// which frees the gg and a slots for the next tile's MMAs, then NUM and the
+// rest of the statistic.
 template <int P>
 struct LmmEpi {
   static constexpr bool kGrouped = false;
+  static constexpr bool kTwoPhase = true;
+  static constexpr int kPhase1 = P + 1;  // gg and a_k
+  static constexpr int kMaxChunks = 2;   // 16-column chunks per warp and tile
   using Params = LmmEpiParams<P>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
@@ -518,9 +526,12 @@ struct LmmEpi {
   int gene = 0;
   int64_t snp0 = 0;
   bool gvalid = false;
-  float u[P + 2];
+  float u[P + 2];  // unscale of [NUM, a_0 .. a_{P-1}, gg] (the gene-ops order)
   float ai[P][P];
   float inv_rss = 0;
+  // S per pair of the warp's two chunks (0 where gg < 1e-12); two named
+  // arrays picked by a select, so they stay in registers for a runtime ci
+  float S0[16], S1[16];
   GeneAcc acc;
   __device__ LmmEpi(const Params& p, const TileShape&, uint8_t* smem)
       : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
@@ -545,12 +556,32 @@ struct LmmEpi {
     }
   }
   // Screening arithmetic in FP32 (the accumulators carry ~1e-7 relative
-  // error already); printed statistics come from the FP64 refinement. The
-  // 16 pairs of a chunk share one branch-free tail evaluation, so their
-  // table lookups overlap.
-  template <int NACC>
-  __device__ void chunk(int c, const float (&v)[NACC][16]) {
-    static_assert(NACC == P + 2, "accumulators");
+  // error already); printed statistics come from the FP64 refinement.
+  // Phase 1: v = [gg, a_0 .. a_{P-1}] of 16 pairs.
+  template <int N>
+  __device__ void pre_chunk(int ci, int, const float (&v)[N][16]) {
+    static_assert(N == P + 1, "phase-1 accumulators");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const float gg = v[0][j] * u[P + 1];
+      float S = gg;
+      float a[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * u[1 + k];
+#pragma unroll
+      for (int x = 0; x < P; ++x)
+#pragma unroll
+        for (int y = 0; y < P; ++y) S = fmaf(-a[x] * ai[x][y], a[y], S);
+      const float Sj = gg < 1e-12f ? 0.0f : S;  // gg < 1e-12: p = 1 (S fails the S > 1e-15 test)
+      if (ci == 0) S0[j] = Sj;
+      else S1[j] = Sj;
+    }
+  }
+  // Phase 2: v = [NUM] of the same 16 pairs. The 16 pairs share one
+  // branch-free tail evaluation, so their table lookups overlap.
+  template <int N>
+  __device__ void post_chunk(int ci, int c, const float (&v)[N][16]) {
+    static_assert(N == 1, "phase-2 accumulators");
     const int64_t s0 = snp0 + c;
     if (!gvalid || s0 >= Pr.m) return;
     uint32_t okw[4];
@@ -560,23 +591,30 @@ struct LmmEpi {
       const int64_t s = s0 + j;
       const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
       const float num = v[0][j] * u[0];
-      const float gg = v[P + 1][j] * u[P + 1];
-      float S = gg;
-      float a[P];
-#pragma unroll
-      for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * u[1 + k];
-#pragma unroll
-      for (int x = 0; x < P; ++x)
-#pragma unroll
-        for (int y = 0; y < P; ++y) S = fmaf(-a[x] * ai[x][y], a[y], S);
+      const float S = ci == 0 ? S0[j] : S1[j];
       const float r = num * __fdividef(num, S) * inv_rss;
       const float omr = 1.0f - r;
-      const bool ok_stat = !(gg < 1e-12f) && S > 1e-15f && omr > 0.0f;
+      const bool ok_stat = S > 1e-15f && omr > 0.0f;
       const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
       const ScreenOut o = acat_screen(t, tt);
       acc.add_screen(o, s, valid);
       if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
+  }
+  // Both phases at once (the CUDA-core comparator): v in the tile's order.
+  template <int NACC>
+  __device__ void chunk(int c, const float (&v)[NACC][16]) {
+    static_assert(NACC == P + 2, "accumulators");
+    float v1[P + 1][16];
+#pragma unroll
+    for (int k = 0; k < P + 1; ++k)
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v1[k][j] = v[k][j];
+    pre_chunk<P + 1>(0, c, v1);
+    float v2[1][16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v2[0][j] = v[P + 1][j];
+    post_chunk<1>(0, c, v2);
   }
   __device__ void end_tile() {
     if (gvalid) acc.flush(Pr.out, gene);
@@ -1112,11 +1150,19 @@ static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* c
   Rotated& R = ctx->rot;
   const __half* bh[2] = {R.gt_hi.p, R.gt2_hi.p};
   const __half* bl[2] = {R.gt_lo.p, R.gt2_lo.p};
+  // tile order [gg, a_0 .. a_{P-1}, NUM] from the gene-ops order [NUM, a.., gg]
+  const __half* oh[P + 2];
+  const __half* ol[P + 2];
   int bsel[P + 2], prod[P + 2];
   for (int j = 0; j < P + 2; ++j) {
-    bsel[j] = j == P + 1 ? 1 : 0;
+    const int op = j == 0 ? P + 1 : (j == P + 1 ? 0 : j);
+    oh[j] = ah[op];
+    ol[j] = al[op];
+    bsel[j] = j == 0 ? 1 : 0;  // gg reads Gt^2
     prod[j] = 7;
   }
+  ah = oh;
+  al = ol;
   if (!simt) {
     launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod, tiles, n_tiles);
     return;

@@ -30,10 +30,21 @@
 // other on the same CTA, and a grouped epilogue (Epi::kGrouped) receives each
 // accumulator of each group and keeps its per-pair state across the groups.
 #pragma once
+#include <type_traits>
+
 #include "sm100.cuh"
 
 namespace eqtl {
 namespace dev {
+
+// Two-phase epilogues (Epi::kTwoPhase): the first Epi::kPhase1 accumulators
+// of a unit are read for every chunk first (pre_chunk) and their TMEM slots
+// released at once; the remaining ones follow (post_chunk). The next unit's
+// MMAs then need to wait only for the short first phase.
+template <class E, class = void>
+struct IsTwoPhase : std::false_type {};
+template <class E>
+struct IsTwoPhase<E, std::void_t<decltype(E::kTwoPhase)>> : std::bool_constant<E::kTwoPhase> {};
 
 constexpr int kMaxAcc = 20;  // accumulators of one tile over all its groups
 constexpr int kEpiWarps = 16;
@@ -321,6 +332,35 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             }
             if (grp == sh.n_groups - 1) epi.finish_chunk(c);
           }
+        } else if constexpr (IsTwoPhase<Epi>::value) {
+          constexpr int N1 = Epi::kPhase1;
+          static_assert(N1 >= 1 && N1 < NACC, "two-phase epilogue: phase sizes");
+          // every warp owns exactly NCH chunks; ci tells the epilogue which
+          constexpr int NCH = NT / (16 * kSub);
+          static_assert(NT % (16 * kSub) == 0 && NCH <= Epi::kMaxChunks, "two-phase epilogue: chunks per warp");
+#pragma unroll 1
+          for (int ci = 0; ci < NCH; ++ci) {
+            const int c = 16 * sub + 16 * kSub * ci;
+            float v[N1][16];
+#pragma unroll
+            for (int jj = 0; jj < N1; ++jj) tmem_ld16(col(jj) + static_cast<uint32_t>(c), v[jj]);
+            tmem_wait_ld();
+            epi.template pre_chunk<N1>(ci, c, v);
+          }
+          tc_fence_before();
+          for (int jj = 0; jj < N1; ++jj) mbar_arrive(&sempty[(slot0 + jj) % C::NSLOTS]);
+#pragma unroll 1
+          for (int ci = 0; ci < NCH; ++ci) {
+            const int c = 16 * sub + 16 * kSub * ci;
+            float v[NACC - N1][16];
+#pragma unroll
+            for (int jj = 0; jj < NACC - N1; ++jj) tmem_ld16(col(N1 + jj) + static_cast<uint32_t>(c), v[jj]);
+            tmem_wait_ld();
+            epi.template post_chunk<NACC - N1>(ci, c, v);
+          }
+          tc_fence_before();
+          for (int jj = N1; jj < nv; ++jj) mbar_arrive(&sempty[(slot0 + jj) % C::NSLOTS]);
+          continue;  // slots released above
         } else {
 #pragma unroll 1
           for (int c = 16 * sub; c < NT; c += 16 * kSub) {
