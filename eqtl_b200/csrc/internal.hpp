@@ -151,6 +151,10 @@ struct Workspace {
   DevBuf<__half> q_hi, q_lo;  // rotation: split eigenvector operand
   DevBuf<int> ref_snps, ref_col;
   DevBuf<int2> ref_pairs;
+  // batched REML (p > 3): covariate pair products, per-round weights and sums
+  DevBuf<double> rb_P, rb_dlt, rb_W, rb_WY, rb_A, rb_B, rb_ld, rb_ydy;
+  DevBuf<uint8_t> rb_state;
+  DevBuf<unsigned int> rb_active;
   // per-gene scan outputs + candidates
   DevBuf<double> acat;
   DevBuf<int> used, tested;

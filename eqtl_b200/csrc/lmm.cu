@@ -23,6 +23,7 @@
 //             dosages rotated by cuBLAS DGEMM.
 #include <cublas_v2.h>
 #include <cusolverDn.h>
+#include <math_constants.h>
 
 #include <algorithm>
 #include <cmath>
@@ -96,15 +97,6 @@ __global__ void q_split_kernel(const double* __restrict__ Q, int n, int k_pad, _
 }
 
 // --------------------------------------------------------------- REML
-struct RemlShared {
-  double red[2][8];
-  double res[kMaxPLmm * (kMaxPLmm + 1) / 2 + kMaxPLmm];
-  double A[kMaxPLmm * kMaxPLmm];  // thread-0 scratch: X~'DX~ and its Cholesky factor
-  double L[kMaxPLmm * kMaxPLmm];
-  double x[kMaxPLmm], e[kMaxPLmm];
-  double val;
-};
-
 // Packed upper-triangle index of (a, b), a <= b.
 __device__ __forceinline__ int tri(int a, int b, int p) { return a * p - a * (a - 1) / 2 + (b - a); }
 
@@ -138,89 +130,6 @@ __device__ bool chol_solve(const double* A, const double* b, double* x, double* 
     }
   }
   return true;
-}
-
-// Block-wide REML -loglik at delta (every thread calls; result broadcast).
-__device__ double reml_eval(double delta, const double* __restrict__ yt, const double* __restrict__ Xt,
-                            const double* __restrict__ lam, int n, int p, double* wsh, RemlShared& sh) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  // sum of log v as the log of products of up to eight factors: every factor
-  // lies in [1e-12, 1e36] (larger ones take their own log), so a product
-  // stays within [1e-96, 1e288]; one FP64 log per eight samples instead of
-  // one per sample
-  double ld = 0, ydy = 0, prod = 1.0;
-  int nprod = 0;
-  for (int i = tid; i < n; i += blockDim.x) {
-    double v = delta * lam[i] + 1.0;
-    if (v < 1e-12) v = 1e-12;
-    const double w = 1.0 / v;
-    wsh[i] = w;
-    if (v <= 1e36) {
-      prod *= v;
-      if (++nprod == 8) {
-        ld += log(prod);
-        prod = 1.0;
-        nprod = 0;
-      }
-    } else {
-      ld += log(v);
-    }
-    ydy += w * yt[i] * yt[i];
-  }
-  ld += log(prod);
-  for (int o = 16; o; o >>= 1) {
-    ld += __shfl_xor_sync(0xffffffffu, ld, o);
-    ydy += __shfl_xor_sync(0xffffffffu, ydy, o);
-  }
-  if (lane == 0) {
-    sh.red[0][warp] = ld;
-    sh.red[1][warp] = ydy;
-  }
-  __syncthreads();
-  const int nq = p * (p + 1) / 2;
-  for (int q = warp; q < nq + p; q += nw) {
-    double acc = 0;
-    if (q < nq) {
-      int a = 0;
-      while (tri(a, p - 1, p) < q) ++a;  // row of packed index q
-      const int b = a + (q - tri(a, a, p));
-      for (int i = lane; i < n; i += 32) acc += wsh[i] * Xt[static_cast<int64_t>(a) * n + i] * Xt[static_cast<int64_t>(b) * n + i];
-    } else {
-      const int k = q - nq;
-      for (int i = lane; i < n; i += 32) acc += wsh[i] * yt[i] * Xt[static_cast<int64_t>(k) * n + i];
-    }
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) sh.res[q] = acc;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    double logdet_d = 0, y_dy = 0;
-    for (int w = 0; w < nw; ++w) {
-      logdet_d += sh.red[0][w];
-      y_dy += sh.red[1][w];
-    }
-    double* A = sh.A;
-    double* beta = sh.x;
-    for (int a = 0; a < p; ++a)
-      for (int b = a; b < p; ++b) A[a * p + b] = A[b * p + a] = sh.res[tri(a, b, p)];
-    const double* XtDy = sh.res + nq;
-    double logdet_x = 0;
-    double out;
-    if (!chol_solve(A, XtDy, beta, &logdet_x, p, sh.L)) {
-      out = 1e300;
-    } else {
-      double q = y_dy;
-      for (int k = 0; k < p; ++k) q -= XtDy[k] * beta[k];
-      if (q <= 0) q = 1e-12;
-      const double df = static_cast<double>(n - p);
-      out = 0.5 * (df * log(q / df) + logdet_d + logdet_x);
-    }
-    sh.val = out;
-  }
-  __syncthreads();
-  const double r = sh.val;
-  __syncthreads();
-  return r;
 }
 
 // optimize_delta (src/model_lmm.cpp:39-86): grid 1e-5..1e5 x2 (and 1.0), 40
@@ -298,31 +207,8 @@ __device__ void reml_caches(double* A, const double* b, double y_dy, int p, int 
   for (int k = 0; k < p; ++k) chi0_out[static_cast<int64_t>(g) * p + k] = chi0[k];
 }
 
-// One CTA per gene, any p <= kMaxPLmm. Ytil [G][n], Xtil [p][n].
-__global__ void __launch_bounds__(256) reml_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
-                                                   const double* __restrict__ lam, int n, int p, int G,
-                                                   double* delta_out, double* chi0_out, double* ainv_out,
-                                                   double* rss_out) {
-  extern __shared__ double wsh[];
-  __shared__ RemlShared sh;
-  const int g = blockIdx.x;
-  if (g >= G) return;
-  const double* yt = Ytil + static_cast<int64_t>(g) * n;
-  auto f = [&](double d) { return reml_eval(d, yt, Xtil, lam, n, p, wsh, sh); };
-  const double d = optimize_delta_dev(f, n - p);
-  f(d);  // the caches at the chosen delta: one more weighted reduction
-  if (threadIdx.x == 0) {
-    const int nq = p * (p + 1) / 2;
-    for (int a = 0; a < p; ++a)
-      for (int b = a; b < p; ++b) sh.A[a * p + b] = sh.A[b * p + a] = sh.res[tri(a, b, p)];
-    double y_dy = 0;
-    for (int w = 0; w < (blockDim.x >> 5); ++w) y_dy += sh.red[1][w];
-    delta_out[g] = d;
-    reml_caches(sh.A, sh.res + nq, y_dy, p, g, sh.L, sh.e, sh.x, chi0_out, ainv_out, rss_out);
-  }
-}
-
-// -loglik of reml_eval for P <= 3 covariate columns, evaluated by one warp:
+// REML -loglik (src/model_lmm.cpp:10-37) for P <= 3 covariate columns,
+// evaluated by one warp:
 // each lane sums log v, w y^2, w x_a x_b and w y x_a over its samples in
 // registers, and xor-shuffle reductions give every lane the same totals
 // (IEEE addition is commutative), so there is no shared memory and no block
@@ -343,7 +229,10 @@ __device__ __forceinline__ double reml_eval_warp(double delta, const double* __r
     double v = delta * lam[i] + 1.0;
     if (v < 1e-12) v = 1e-12;
     const double w = 1.0 / v;
-    if (v <= 1e36) {  // log of products of up to eight factors, as in reml_eval
+    // sum of log v as the log of products of up to eight factors: every factor
+    // lies in [1e-12, 1e36] (larger ones take their own log), so a product
+    // stays within [1e-96, 1e288]
+    if (v <= 1e36) {
       prod *= v;
       if (++nprod == 8) {
         acc[0] += log(prod);
@@ -407,8 +296,8 @@ __device__ __forceinline__ double reml_eval_warp(double delta, const double* __r
   return 0.5 * (df * log(q / df) + tot[0] + logdet_x);
 }
 
-// One warp per gene for P <= 3 (the common case: intercept and a few
-// covariates); same search and caches as reml_kernel.
+// One warp per gene for P <= 3 (intercept and a few covariates):
+// optimize_delta (src/model_lmm.cpp:39-86) and the prep_lmm caches (:124-153).
 constexpr int kRemlWarpP = 3;
 template <int P>
 __global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict__ Ytil,
@@ -431,6 +320,248 @@ __global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict
     delta_out[g] = d;
     reml_caches(A, tot + 2 + NQ, tot[1], P, g, L, e, x, chi0_out, ainv_out, rss_out);
   }
+}
+
+// ------------------------------------------- batched REML (p > kRemlWarpP)
+// The same schedule and -loglik for many columns in lockstep. Each round
+// evaluates up to two deltas per column (slot s = slot * C + column); the
+// sums over the n samples run as FP64 GEMMs shared by all columns,
+//   A[q, s] = sum_i P[q, i] W[i, s]     P[q, i] = x~_ai x~_bi (q = tri(a, b))
+//   b[a, s] = sum_i x~_ai (W o Y)[i, s]
+// with W[i, s] = 1 / max(delta_s lambda_i + 1, 1e-12), and one thread per
+// column advances its search (grid, golden section, Newton) between rounds.
+enum : int { kRbGrid = 0, kRbGolden, kRbCentre, kRbNewtonPair, kRbNewtonStep, kRbFinal, kRbDone };
+constexpr int kRbGridN = 35;  // f(1.0), then 1e-5 * 2^k for k = 0..33 (the loop dd <= 1e5, dd *= 2)
+constexpr int kRbMaxRounds = (kRbGridN + 1) / 2 + 40 + 1 + 2 * 8 + 1;
+
+struct RemlBatchState {
+  int phase, k;
+  double best_d, best_ll, lo, hi, d, cur, h, step, dn;
+};
+
+// 1e-5 doubled k times is exact, so this is the reference's dd sequence
+__device__ __forceinline__ double rb_grid_delta(int j) { return j == 0 ? 1.0 : ldexp(1e-5, j - 1); }
+
+__device__ void rb_propose(const RemlBatchState& s, double& d0, double& d1) {
+  d0 = d1 = CUDART_NAN;
+  switch (s.phase) {
+    case kRbGrid:
+      d0 = rb_grid_delta(s.k);
+      if (s.k + 1 < kRbGridN) d1 = rb_grid_delta(s.k + 1);
+      break;
+    case kRbGolden: {
+      const double phi = (1.0 + sqrt(5.0)) / 2.0;
+      d0 = s.hi - (s.hi - s.lo) / phi;
+      d1 = s.lo + (s.hi - s.lo) / phi;
+      break;
+    }
+    case kRbCentre:
+    case kRbFinal:
+      d0 = s.d;
+      break;
+    case kRbNewtonPair:
+      d0 = s.d - s.h;
+      d1 = s.d + s.h;
+      break;
+    case kRbNewtonStep:
+      d0 = s.dn;
+      break;
+    default:
+      break;
+  }
+}
+
+// P[q + nq i] = x~_ai x~_bi
+__global__ void rb_pairs_kernel(const double* __restrict__ Xtil, int n, int p, double* P) {
+  const int nq = p * (p + 1) / 2;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < static_cast<int64_t>(nq) * n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(t % nq);
+    const int i = static_cast<int>(t / nq);
+    int a = 0;
+    while (tri(a, p - 1, p) < q) ++a;
+    const int b = a + (q - tri(a, a, p));
+    P[t] = Xtil[static_cast<int64_t>(a) * n + i] * Xtil[static_cast<int64_t>(b) * n + i];
+  }
+}
+
+__global__ void rb_init_kernel(int C, int df, RemlBatchState* st, double* dlt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  RemlBatchState s{};
+  s.phase = df > 0 ? kRbGrid : kRbFinal;
+  s.k = 0;
+  s.d = 1.0;
+  st[c] = s;
+  rb_propose(s, dlt[c], dlt[C + c]);
+}
+
+// One warp per slot: W, W o y, sum log v (log of eight-factor products, as in
+// reml_eval_warp) and y'Dy. Slots with no delta (NaN) are skipped.
+__global__ void __launch_bounds__(256) rb_weights_kernel(const double* __restrict__ Ytil,
+                                                         const double* __restrict__ lam, int n, int C,
+                                                         const double* __restrict__ dlt, double* W, double* WY,
+                                                         double* ld, double* ydy) {
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= 2 * C) return;
+  const double delta = dlt[s];
+  if (!(delta == delta)) return;
+  const double* y = Ytil + static_cast<int64_t>(s % C) * n;
+  double* w_out = W + static_cast<int64_t>(s) * n;
+  double* wy_out = WY + static_cast<int64_t>(s) * n;
+  double acc_ld = 0.0, acc_y = 0.0, prod = 1.0;
+  int nprod = 0;
+  for (int i = lane; i < n; i += 32) {
+    double v = delta * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    if (v <= 1e36) {
+      prod *= v;
+      if (++nprod == 8) {
+        acc_ld += log(prod);
+        prod = 1.0;
+        nprod = 0;
+      }
+    } else {
+      acc_ld += log(v);
+    }
+    const double yi = y[i];
+    w_out[i] = w;
+    wy_out[i] = w * yi;
+    acc_y += w * yi * yi;
+  }
+  acc_ld += log(prod);
+  for (int o = 16; o; o >>= 1) {
+    acc_ld += __shfl_xor_sync(0xffffffffu, acc_ld, o);
+    acc_y += __shfl_xor_sync(0xffffffffu, acc_y, o);
+  }
+  if (lane == 0) {
+    ld[s] = acc_ld;
+    ydy[s] = acc_y;
+  }
+}
+
+// -loglik of slot s from its sums; A is unpacked into Af (p x p, row-major).
+__device__ double rb_negll(const double* __restrict__ Acol, const double* __restrict__ bcol, double y_dy,
+                           double logdet_d, int p, int df, double* Af, double* L) {
+  for (int a = 0; a < p; ++a)
+    for (int b = a; b < p; ++b) Af[a * p + b] = Af[b * p + a] = Acol[tri(a, b, p)];
+  double beta[kMaxPLmm];
+  double logdet_x = 0.0;
+  if (!chol_solve(Af, bcol, beta, &logdet_x, p, L)) return 1e300;
+  double q = y_dy;
+  for (int k = 0; k < p; ++k) q -= bcol[k] * beta[k];
+  if (q <= 0) q = 1e-12;
+  const double dfd = static_cast<double>(df);
+  return 0.5 * (dfd * log(q / dfd) + logdet_d + logdet_x);
+}
+
+// One thread per column: reads the round's -loglik values, advances the
+// search exactly as optimize_delta_dev does, and proposes the next round's
+// deltas; in the final round writes delta and the prep_lmm caches.
+__global__ void rb_advance_kernel(int C, int g0, int p, int df, const double* __restrict__ A,
+                                  const double* __restrict__ B, const double* __restrict__ ld,
+                                  const double* __restrict__ ydy, RemlBatchState* st, double* dlt,
+                                  unsigned int* active, double* delta_out, double* chi0_out, double* ainv_out,
+                                  double* rss_out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  RemlBatchState s = st[c];
+  if (s.phase == kRbDone) return;
+  const int nq = p * (p + 1) / 2;
+  double Af[kMaxPLmm * kMaxPLmm], L[kMaxPLmm * kMaxPLmm];
+  auto f = [&](int slot) {
+    const int si = slot * C + c;
+    return rb_negll(A + static_cast<int64_t>(si) * nq, B + static_cast<int64_t>(si) * p, ydy[si], ld[si], p, df,
+                    Af, L);
+  };
+  switch (s.phase) {
+    case kRbGrid: {
+      for (int j = s.k; j < s.k + 2 && j < kRbGridN; ++j) {
+        const double v = f(j - s.k);
+        if (j == 0) {
+          s.best_ll = v;
+          s.best_d = 1.0;
+        } else if (v < s.best_ll) {
+          s.best_ll = v;
+          s.best_d = rb_grid_delta(j);
+        }
+      }
+      s.k += 2;
+      if (s.k >= kRbGridN) {
+        s.lo = s.best_d / 4.0;
+        s.hi = s.best_d * 4.0;
+        if (s.lo < 1e-8) s.lo = 1e-8;
+        if (s.hi > 1e6) s.hi = 1e6;
+        s.phase = kRbGolden;
+        s.k = 0;
+      }
+      break;
+    }
+    case kRbGolden: {
+      const double phi = (1.0 + sqrt(5.0)) / 2.0;
+      const double m1 = s.hi - (s.hi - s.lo) / phi;
+      const double m2 = s.lo + (s.hi - s.lo) / phi;
+      const double f1 = f(0);
+      const double f2 = f(1);
+      if (f1 < f2) s.hi = m2;
+      else s.lo = m1;
+      if (++s.k == 40) {
+        s.d = 0.5 * (s.lo + s.hi);
+        s.phase = kRbCentre;
+      }
+      break;
+    }
+    case kRbCentre:
+      s.cur = f(0);
+      s.k = 0;
+      s.h = fmax(s.d * 1e-4, 1e-9);
+      s.phase = kRbNewtonPair;
+      break;
+    case kRbNewtonPair: {
+      const double fm = f(0);
+      const double fp = f(1);
+      const double g1 = (fp - fm) / (2.0 * s.h);
+      const double g2 = (fp - 2.0 * s.cur + fm) / (s.h * s.h);
+      s.phase = kRbFinal;
+      if (g2 > 1e-12) {
+        s.step = g1 / g2;
+        s.dn = s.d - s.step;
+        if (s.dn > 1e-8 && s.dn < 1e6) s.phase = kRbNewtonStep;
+      }
+      break;
+    }
+    case kRbNewtonStep: {
+      const double vn = f(0);
+      s.phase = kRbFinal;
+      if (vn < s.cur) {
+        s.d = s.dn;
+        s.cur = vn;
+        if (!(fabs(s.step) < s.d * 1e-8) && ++s.k < 8) {
+          s.h = fmax(s.d * 1e-4, 1e-9);
+          s.phase = kRbNewtonPair;
+        }
+      }
+      break;
+    }
+    case kRbFinal: {
+      const int si = c;  // slot 0
+      const double* Acol = A + static_cast<int64_t>(si) * nq;
+      for (int a = 0; a < p; ++a)
+        for (int b = a; b < p; ++b) Af[a * p + b] = Af[b * p + a] = Acol[tri(a, b, p)];
+      double e[kMaxPLmm], x[kMaxPLmm];
+      delta_out[g0 + c] = s.d;
+      reml_caches(Af, B + static_cast<int64_t>(si) * p, ydy[si], p, g0 + c, L, e, x, chi0_out, ainv_out, rss_out);
+      s.phase = kRbDone;
+      break;
+    }
+    default:
+      break;
+  }
+  st[c] = s;
+  rb_propose(s, dlt[c], dlt[C + c]);
+  if (s.phase != kRbDone) atomicAdd(active, 1u);
 }
 
 // Gene-side operands, one block per gene: rows (w o r~), (w o X~_k), w, each
@@ -1098,6 +1229,66 @@ void lmm_rotate(eqtl_ctx* ctx) {
 // ------------------------------------------------------------------- REML
 // Per-gene REML prep into the context workspace (ws.Ytil, Xtil, delta, chi0,
 // ainv, rss) from the resident phenotypes.
+// Batched REML for p > kRemlWarpP over ws.Ytil / ws.Xtil into ws.delta,
+// chi0, ainv, rss: columns in chunks whose per-round buffers stay near 2 GB.
+static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  cublasHandle_t h = blas_of(ctx);
+  const int nq = p * (p + 1) / 2;
+  const int df = n - p;
+  ws.rb_P.alloc(static_cast<size_t>(nq) * n);
+  ++ctx->launches;
+  rb_pairs_kernel<<<1184, 256, 0, st>>>(ws.Xtil.p, n, p, ws.rb_P.p);
+  EQTL_CUDA(cudaGetLastError());
+  const int cmax = std::max(1024, static_cast<int>((int64_t(1) << 26) / std::max(n, 1)));
+  for (int g0 = 0; g0 < G; g0 += cmax) {
+    const int C = std::min(cmax, G - g0);
+    const size_t slots = 2 * static_cast<size_t>(C);
+    ws.rb_state.alloc(sizeof(RemlBatchState) * C);
+    ws.rb_dlt.alloc(slots);
+    ws.rb_W.alloc(slots * n);
+    ws.rb_WY.alloc(slots * n);
+    ws.rb_A.alloc(slots * nq);
+    ws.rb_B.alloc(slots * p);
+    ws.rb_ld.alloc(slots);
+    ws.rb_ydy.alloc(slots);
+    ws.rb_active.alloc(1);
+    RemlBatchState* state = reinterpret_cast<RemlBatchState*>(ws.rb_state.p);
+    const double* Y = ws.Ytil.p + static_cast<int64_t>(g0) * n;
+    const unsigned cblocks = static_cast<unsigned>((C + 127) / 128);
+    ++ctx->launches;
+    rb_init_kernel<<<cblocks, 128, 0, st>>>(C, df, state, ws.rb_dlt.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    for (int round = 0; round < kRbMaxRounds; ++round) {
+      ctx->launches += 2;
+      rb_weights_kernel<<<static_cast<unsigned>((slots + 7) / 8), 256, 0, st>>>(
+          Y, ctx->basis.lambda.p, n, C, ws.rb_dlt.p, ws.rb_W.p, ws.rb_WY.p, ws.rb_ld.p, ws.rb_ydy.p);
+      EQTL_CUDA(cudaGetLastError());
+      EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nq, static_cast<int>(slots), n, &one, ws.rb_P.p, nq,
+                             ws.rb_W.p, n, &zero, ws.rb_A.p, nq) == CUBLAS_STATUS_SUCCESS,
+                 EQTL_E_CUDA, "REML X'DX failed");
+      EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, p, static_cast<int>(slots), n, &one, ws.Xtil.p, n,
+                             ws.rb_WY.p, n, &zero, ws.rb_B.p, p) == CUBLAS_STATUS_SUCCESS,
+                 EQTL_E_CUDA, "REML X'Dy failed");
+      EQTL_CUDA(cudaMemsetAsync(ws.rb_active.p, 0, sizeof(unsigned int), st));
+      rb_advance_kernel<<<cblocks, 128, 0, st>>>(C, g0, p, df, ws.rb_A.p, ws.rb_B.p, ws.rb_ld.p, ws.rb_ydy.p, state,
+                                                 ws.rb_dlt.p, ws.rb_active.p, ws.delta.p, ws.chi0.p, ws.ainv.p,
+                                                 ws.rss.p);
+      EQTL_CUDA(cudaGetLastError());
+      // the grid and golden phases run the same number of rounds for every
+      // column; from the Newton phase on, stop once no column is left
+      if (round >= (kRbGridN + 1) / 2 + 40) {
+        unsigned int left = 0;
+        ws.rb_active.download(&left, 1, st);
+        EQTL_CUDA(cudaStreamSynchronize(st));
+        if (left == 0) break;
+      }
+    }
+  }
+}
+
 void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
   const int n = ph.n, G = ph.G, p = ph.p;
   EQTL_CHECK(ctx->have_basis && ctx->basis.n == n, EQTL_E_STATE, "LMM prep needs an eigenbasis of size n");
@@ -1135,12 +1326,7 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
     EQTL_CUDA(cudaGetLastError());
     return;
   }
-  const size_t smem = sizeof(double) * n;  // the n weights of the evaluation
-  EQTL_CHECK(smem <= 200 * 1024, EQTL_E_UNSUPPORTED, "REML kernel holds n doubles in shared memory (n <= 25600)");
-  EQTL_CUDA(cudaFuncSetAttribute(reml_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  reml_kernel<<<G, 256, smem, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, n, p, G, ws.delta.p, ws.chi0.p,
-                                    ws.ainv.p, ws.rss.p);
-  EQTL_CUDA(cudaGetLastError());
+  reml_batched(ctx, n, p, G);
 }
 
 // ------------------------------------------------------------------- scan

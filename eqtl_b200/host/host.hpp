@@ -4,9 +4,11 @@
 // pairs / top / region TSV writers (src/output.cpp:8-110). Everything here is
 // plain C++17; all association arithmetic runs on the device.
 #pragma once
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -23,6 +25,20 @@ struct Fatal : std::runtime_error {
 };
 [[noreturn]] void die(const std::string& msg);
 void info(const std::string& msg);
+
+// Opt-in phase timings: with EQTL_TRACE set, mark() prints the wall time
+// since the previous mark to stderr.
+struct Trace {
+  bool on = std::getenv("EQTL_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const std::string& what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[eqtl trace] %s %.1f ms\n", what.c_str(),
+                 std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
 
 // ------------------------------------------------------------------ options
 struct Options {

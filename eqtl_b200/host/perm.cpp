@@ -177,6 +177,8 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   // genes per device batch: keep the permuted phenotype block near 2^26 doubles
   const size_t cols_budget = std::max<size_t>(static_cast<size_t>(B), (size_t(1) << 26) / std::max<size_t>(n, 1));
   const size_t genes_per_batch = std::max<size_t>(1, cols_budget / static_cast<size_t>(B));
+  Trace tr;
+  tr.mark("permutations: setup");
   for (size_t a = 0; a < active.size(); a += genes_per_batch) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
@@ -190,6 +192,7 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
       const size_t gi = c / B;
       permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &Y[c * n]);
     });
+    tr.mark("permutations: " + std::to_string(cols) + " columns built on the host");
     std::vector<double> minp(cols, 1.0);
     if (genes[active[a]].window) {
       // cis: one banded cis scan of every column with its gene's window
@@ -220,6 +223,7 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
       for (size_t i = 0; i < res.size(); ++i)
         if (std::isfinite(res[i].p) && res[i].p < minp[pc[i]]) minp[pc[i]] = res[i].p;
     }
+    tr.mark("permutations: device scan of " + std::to_string(cols) + " columns");
     for (size_t gi = 0; gi < nb; ++gi) {
       const PermGene& g = genes[active[a + gi]];
       PermOut& o = out[active[a + gi]];
@@ -237,6 +241,7 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
         o.beta.s1 = o.beta.s2 = 0.0;
       }
     }
+    tr.mark("permutations: p_emp and beta fits of " + std::to_string(nb) + " genes");
   }
   return out;
 }

@@ -160,6 +160,16 @@ ScanResult scan_columns(const Study& st, const std::string& model, const std::ve
     st.dev->check(rc, model + " scan");
     R.pairs.resize(static_cast<size_t>(np));
     R.cands.resize(static_cast<size_t>(nc));
+    if (std::getenv("EQTL_TRACE")) {
+      std::string line = "[eqtl trace] device stages of " + std::to_string(J) + " columns (ms):";
+      const char* names[] = {"rotate", "prep", "scan", "refine"};
+      const int stages[] = {EQTL_STAGE_ROTATE, EQTL_STAGE_PREP, EQTL_STAGE_SCAN, EQTL_STAGE_REFINE};
+      for (int k = 0; k < 4; ++k) {
+        double ms = 0;
+        if (eqtl_stage_ms(st.dev->ctx, stages[k], &ms) == EQTL_OK) line += std::string(" ") + names[k] + " " + std::to_string(ms);
+      }
+      std::fprintf(stderr, "%s\n", line.c_str());
+    }
     return R;
   }
   die("scan output did not fit after resizing");
@@ -273,7 +283,9 @@ void run_trans(const Study& st, const std::string& model, const std::string& sco
   if (jobs.empty()) return;
   const double pthr = opt.pval_trans;
   const double perm_thr = opt.perm > 0 ? opt.perm_trans_thr : 0.0;
+  Trace tr;
   ScanResult R = device_scan(st, model, jobs, scope == "trans" ? 1 : 0, pthr, perm_thr);
+  tr.mark(scope + " " + model + ": device scan");
   std::vector<PermOut> perms;
   if (opt.perm > 0) {
     std::vector<PermGene> pg(jobs.size());
@@ -289,6 +301,7 @@ void run_trans(const Study& st, const std::string& model, const std::string& sco
           std::isfinite(q.p))
         pg[q.gene].snps.push_back(q.snp);
     perms = run_permutations(st, model, pg, R.delta);
+    tr.mark(scope + " " + model + ": stage-2 permutations");
   }
   std::vector<size_t> order(R.pairs.size());
   std::iota(order.begin(), order.end(), 0);  // already (SNP, gene)
@@ -327,7 +340,9 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
   });
   std::vector<Job> jobs_dev(jobs.size());
   for (size_t j = 0; j < jobs.size(); ++j) jobs_dev[j] = jobs[dev_order[j]];
+  Trace tr;
   ScanResult R = device_scan(st, model, jobs_dev, 2, pthr, 0.0);
+  tr.mark("cis " + model + ": device scan");
   {
     std::vector<eqtl_gene_result> genes(R.genes.size());
     std::vector<double> delta(R.delta.size());
@@ -351,6 +366,7 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
     }
     for (size_t j = 0; j < jobs.size(); ++j) pg[j].window = jobs[j].loc;  // permutations scan the window
     perms = run_permutations(st, model, pg, R.delta);
+    tr.mark("cis " + model + ": permutations");
   }
   std::vector<size_t> order(R.pairs.size());
   std::iota(order.begin(), order.end(), 0);
