@@ -153,6 +153,7 @@ struct Workspace {
   DevBuf<int2> ref_pairs;
   // batched REML (p > 3): covariate pair products, per-round weights and sums
   DevBuf<double> rb_P, rb_dlt, rb_W, rb_WY, rb_A, rb_B, rb_ld, rb_ydy;
+  DevBuf<double> rb_Wg, rb_Xw, rb_Ag, rb_Lg, rb_ldx, rb_ldD, rb_Bg, rb_Yg;  // grid phase
   DevBuf<uint8_t> rb_state;
   DevBuf<unsigned int> rb_active;
   // per-gene scan outputs + candidates

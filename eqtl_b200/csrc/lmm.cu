@@ -329,10 +329,11 @@ __global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict
 //   A[q, s] = sum_i P[q, i] W[i, s]     P[q, i] = x~_ai x~_bi (q = tri(a, b))
 //   b[a, s] = sum_i x~_ai (W o Y)[i, s]
 // with W[i, s] = 1 / max(delta_s lambda_i + 1, 1e-12), and one thread per
-// column advances its search (grid, golden section, Newton) between rounds.
-enum : int { kRbGrid = 0, kRbGolden, kRbCentre, kRbNewtonPair, kRbNewtonStep, kRbFinal, kRbDone };
+// column advances its search (golden section, Newton) between rounds; the
+// grid phase, whose deltas every column shares, runs once before them.
+enum : int { kRbGolden = 1, kRbCentre, kRbNewtonPair, kRbNewtonStep, kRbFinal, kRbDone };
 constexpr int kRbGridN = 35;  // f(1.0), then 1e-5 * 2^k for k = 0..33 (the loop dd <= 1e5, dd *= 2)
-constexpr int kRbMaxRounds = (kRbGridN + 1) / 2 + 40 + 1 + 2 * 8 + 1;
+constexpr int kRbMaxRounds = 40 + 1 + 2 * 8 + 1;  // golden, centre, Newton, final
 
 struct RemlBatchState {
   int phase, k;
@@ -345,10 +346,6 @@ __device__ __forceinline__ double rb_grid_delta(int j) { return j == 0 ? 1.0 : l
 __device__ void rb_propose(const RemlBatchState& s, double& d0, double& d1) {
   d0 = d1 = CUDART_NAN;
   switch (s.phase) {
-    case kRbGrid:
-      d0 = rb_grid_delta(s.k);
-      if (s.k + 1 < kRbGridN) d1 = rb_grid_delta(s.k + 1);
-      break;
     case kRbGolden: {
       const double phi = (1.0 + sqrt(5.0)) / 2.0;
       d0 = s.hi - (s.hi - s.lo) / phi;
@@ -385,13 +382,120 @@ __global__ void rb_pairs_kernel(const double* __restrict__ Xtil, int n, int p, d
   }
 }
 
-__global__ void rb_init_kernel(int C, int df, RemlBatchState* st, double* dlt) {
+// ---- grid phase, shared by all columns: the 35 grid deltas are the same for
+// every column, so D_k, X~'D_k X~ (and its Cholesky factor) and sum log v
+// are computed once; per column only X~'D_k y and y'D_k y remain (GEMMs).
+// Wg[i + n k] = w_k,i, Xw[i + n (k p + a)] = w_k,i x~_ai, ldD[k] = sum_i log v_k,i.
+__global__ void rb_grid_weights_kernel(const double* __restrict__ Xtil, const double* __restrict__ lam, int n,
+                                       int p, double* Wg, double* Xw, double* ldD) {
+  const int k = blockIdx.x;  // grid point
+  const double delta = rb_grid_delta(k);
+  const int lane = threadIdx.x & 31;
+  double acc = 0.0, prod = 1.0;
+  int nprod = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = delta * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    const double w = 1.0 / v;
+    Wg[i + static_cast<int64_t>(n) * k] = w;
+    for (int a = 0; a < p; ++a)
+      Xw[i + static_cast<int64_t>(n) * (k * p + a)] = w * Xtil[static_cast<int64_t>(a) * n + i];
+    if (v <= 1e36) {
+      prod *= v;
+      if (++nprod == 8) {
+        acc += log(prod);
+        prod = 1.0;
+        nprod = 0;
+      }
+    } else {
+      acc += log(v);
+    }
+  }
+  acc += log(prod);
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if (lane == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) t += red[w];
+    ldD[k] = t;
+  }
+}
+
+// Lg[k] = Cholesky factor of X~'D_k X~ (row-major, lower), ldx[k] its log
+// determinant, or ldx[k] = NaN when it is not positive definite.
+__global__ void rb_grid_chol_kernel(const double* __restrict__ Ag, int p, double* Lg, double* ldx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= kRbGridN) return;
+  const int nq = p * (p + 1) / 2;
+  double* L = Lg + static_cast<int64_t>(k) * p * p;
+  const double* Ac = Ag + static_cast<int64_t>(k) * nq;
+  double ld = 0.0;
+  for (int j = 0; j < p; ++j) {
+    double d = Ac[tri(j, j, p)];
+    for (int q = 0; q < j; ++q) d -= L[j * p + q] * L[j * p + q];
+    if (!(d > 0)) {
+      ldx[k] = CUDART_NAN;
+      return;
+    }
+    L[j * p + j] = sqrt(d);
+    ld += 2.0 * log(L[j * p + j]);
+    for (int i = j + 1; i < p; ++i) {
+      double v = Ac[tri(j, i, p)];
+      for (int q = 0; q < j; ++q) v -= L[i * p + q] * L[j * p + q];
+      L[i * p + j] = v / L[j * p + j];
+    }
+  }
+  ldx[k] = ld;
+}
+
+// Per column: the 35 grid -logliks in the reference's order (f(1.0) first,
+// strict <), then the golden-section bracket; proposes the first round.
+// Bg[(k p + a) + 35 p c] = x~_a' D_k y_c, Yg[k + 35 c] = y_c' D_k y_c.
+__global__ void rb_grid_advance_kernel(int C, int p, int df, const double* __restrict__ Lg,
+                                       const double* __restrict__ ldx, const double* __restrict__ ldD,
+                                       const double* __restrict__ Bg, const double* __restrict__ Yg,
+                                       RemlBatchState* st, double* dlt) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C) return;
   RemlBatchState s{};
-  s.phase = df > 0 ? kRbGrid : kRbFinal;
-  s.k = 0;
   s.d = 1.0;
+  if (df <= 0) {
+    s.phase = kRbFinal;
+  } else {
+    const double dfd = static_cast<double>(df);
+    for (int k = 0; k < kRbGridN; ++k) {
+      double v = 1e300;
+      const double lx = ldx[k];
+      if (lx == lx) {
+        const double* L = Lg + static_cast<int64_t>(k) * p * p;
+        const double* b = Bg + static_cast<int64_t>(kRbGridN) * p * c + static_cast<int64_t>(k) * p;
+        double z[kMaxPLmm];
+        double q = Yg[k + static_cast<int64_t>(kRbGridN) * c];
+        for (int i = 0; i < p; ++i) {
+          double t = b[i];
+          for (int j = 0; j < i; ++j) t -= L[i * p + j] * z[j];
+          z[i] = t / L[i * p + i];
+          q -= z[i] * z[i];
+        }
+        if (q <= 0) q = 1e-12;
+        v = 0.5 * (dfd * log(q / dfd) + ldD[k] + lx);
+      }
+      if (k == 0) {
+        s.best_ll = v;
+        s.best_d = 1.0;
+      } else if (v < s.best_ll) {
+        s.best_ll = v;
+        s.best_d = rb_grid_delta(k);
+      }
+    }
+    s.lo = s.best_d / 4.0;
+    s.hi = s.best_d * 4.0;
+    if (s.lo < 1e-8) s.lo = 1e-8;
+    if (s.hi > 1e6) s.hi = 1e6;
+    s.phase = kRbGolden;
+  }
   st[c] = s;
   rb_propose(s, dlt[c], dlt[C + c]);
 }
@@ -477,28 +581,6 @@ __global__ void rb_advance_kernel(int C, int g0, int p, int df, const double* __
                     Af, L);
   };
   switch (s.phase) {
-    case kRbGrid: {
-      for (int j = s.k; j < s.k + 2 && j < kRbGridN; ++j) {
-        const double v = f(j - s.k);
-        if (j == 0) {
-          s.best_ll = v;
-          s.best_d = 1.0;
-        } else if (v < s.best_ll) {
-          s.best_ll = v;
-          s.best_d = rb_grid_delta(j);
-        }
-      }
-      s.k += 2;
-      if (s.k >= kRbGridN) {
-        s.lo = s.best_d / 4.0;
-        s.hi = s.best_d * 4.0;
-        if (s.lo < 1e-8) s.lo = 1e-8;
-        if (s.hi > 1e6) s.hi = 1e6;
-        s.phase = kRbGolden;
-        s.k = 0;
-      }
-      break;
-    }
     case kRbGolden: {
       const double phi = (1.0 + sqrt(5.0)) / 2.0;
       const double m1 = s.hi - (s.hi - s.lo) / phi;
@@ -1229,6 +1311,13 @@ void lmm_rotate(eqtl_ctx* ctx) {
 // ------------------------------------------------------------------- REML
 // Per-gene REML prep into the context workspace (ws.Ytil, Xtil, delta, chi0,
 // ainv, rss) from the resident phenotypes.
+// out[i] = x[i]^2
+__global__ void square_kernel(const double* __restrict__ x, int64_t count, double* out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = x[i] * x[i];
+}
+
 // Batched REML for p > kRemlWarpP over ws.Ytil / ws.Xtil into ws.delta,
 // chi0, ainv, rss: columns in chunks whose per-round buffers stay near 2 GB.
 static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
@@ -1241,6 +1330,26 @@ static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
   ++ctx->launches;
   rb_pairs_kernel<<<1184, 256, 0, st>>>(ws.Xtil.p, n, p, ws.rb_P.p);
   EQTL_CUDA(cudaGetLastError());
+  // grid-phase quantities shared by every column
+  {
+    const int K = kRbGridN;
+    ws.rb_Wg.alloc(static_cast<size_t>(n) * K);
+    ws.rb_Xw.alloc(static_cast<size_t>(n) * K * p);
+    ws.rb_Ag.alloc(static_cast<size_t>(nq) * K);
+    ws.rb_Lg.alloc(static_cast<size_t>(K) * p * p);
+    ws.rb_ldx.alloc(K);
+    ws.rb_ldD.alloc(K);
+    ctx->launches += 2;
+    rb_grid_weights_kernel<<<K, 256, 0, st>>>(ws.Xtil.p, ctx->basis.lambda.p, n, p, ws.rb_Wg.p, ws.rb_Xw.p,
+                                             ws.rb_ldD.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nq, K, n, &one, ws.rb_P.p, nq, ws.rb_Wg.p, n, &zero,
+                           ws.rb_Ag.p, nq) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "REML grid X'DX failed");
+    rb_grid_chol_kernel<<<1, 64, 0, st>>>(ws.rb_Ag.p, p, ws.rb_Lg.p, ws.rb_ldx.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
   const int cmax = std::max(1024, static_cast<int>((int64_t(1) << 26) / std::max(n, 1)));
   for (int g0 = 0; g0 < G; g0 += cmax) {
     const int C = std::min(cmax, G - g0);
@@ -1257,10 +1366,27 @@ static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
     RemlBatchState* state = reinterpret_cast<RemlBatchState*>(ws.rb_state.p);
     const double* Y = ws.Ytil.p + static_cast<int64_t>(g0) * n;
     const unsigned cblocks = static_cast<unsigned>((C + 127) / 128);
-    ++ctx->launches;
-    rb_init_kernel<<<cblocks, 128, 0, st>>>(C, df, state, ws.rb_dlt.p);
-    EQTL_CUDA(cudaGetLastError());
     const double one = 1.0, zero = 0.0;
+    // grid phase: X~'D_k y for all columns as one GEMM over the stacked
+    // w_k o X~ (35 p rows), y'D_k y as one GEMM over y o y
+    {
+      const int K = kRbGridN;
+      ws.rb_Bg.alloc(static_cast<size_t>(K) * p * C);
+      ws.rb_Yg.alloc(static_cast<size_t>(K) * C);
+      ctx->launches += 1;
+      square_kernel<<<1184, 256, 0, st>>>(Y, static_cast<int64_t>(n) * C, ws.rb_WY.p);
+      EQTL_CUDA(cudaGetLastError());
+      EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K * p, C, n, &one, ws.rb_Xw.p, n, Y, n, &zero,
+                             ws.rb_Bg.p, K * p) == CUBLAS_STATUS_SUCCESS,
+                 EQTL_E_CUDA, "REML grid X'Dy failed");
+      EQTL_CHECK(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, K, C, n, &one, ws.rb_Wg.p, n, ws.rb_WY.p, n, &zero,
+                             ws.rb_Yg.p, K) == CUBLAS_STATUS_SUCCESS,
+                 EQTL_E_CUDA, "REML grid y'Dy failed");
+      ++ctx->launches;
+      rb_grid_advance_kernel<<<cblocks, 128, 0, st>>>(C, p, df, ws.rb_Lg.p, ws.rb_ldx.p, ws.rb_ldD.p, ws.rb_Bg.p,
+                                                       ws.rb_Yg.p, state, ws.rb_dlt.p);
+      EQTL_CUDA(cudaGetLastError());
+    }
     for (int round = 0; round < kRbMaxRounds; ++round) {
       ctx->launches += 2;
       rb_weights_kernel<<<static_cast<unsigned>((slots + 7) / 8), 256, 0, st>>>(
@@ -1277,9 +1403,9 @@ static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
                                                  ws.rb_dlt.p, ws.rb_active.p, ws.delta.p, ws.chi0.p, ws.ainv.p,
                                                  ws.rss.p);
       EQTL_CUDA(cudaGetLastError());
-      // the grid and golden phases run the same number of rounds for every
-      // column; from the Newton phase on, stop once no column is left
-      if (round >= (kRbGridN + 1) / 2 + 40) {
+      // the golden phase runs the same number of rounds for every column;
+      // from the Newton phase on, stop once no column is left
+      if (round >= 40) {
         unsigned int left = 0;
         ws.rb_active.download(&left, 1, st);
         EQTL_CUDA(cudaStreamSynchronize(st));

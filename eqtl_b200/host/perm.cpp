@@ -8,12 +8,14 @@
 //         rotates it again; the device takes y~_b as it is (y_rotated).
 // Each permutation b of a gene draws its shuffle from std::mt19937 seeded
 // with (seed or 1) + 9973 b + fnv1a(gene) through std::shuffle, so the index
-// sequences are the reference's; columns are built on all host threads.
+// sequences are the reference's; columns are built on all host threads,
+// one batch ahead of the device.
 // Every permuted column gets a fresh null fit on the device. Cis: the banded
 // cis scan of all columns, each with its gene's window; min p = the column's
 // FP64-refined best SNP. Trans/gw stage 2: FP64 tests of the gene's top-K
 // SNPs (eqtl_test_pairs). Then p_emp and the beta approximation per gene.
 #include <algorithm>
+#include <future>
 #include <numeric>
 #include <random>
 #include <thread>
@@ -179,7 +181,9 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   const size_t genes_per_batch = std::max<size_t>(1, cols_budget / static_cast<size_t>(B));
   Trace tr;
   tr.mark("permutations: setup");
-  for (size_t a = 0; a < active.size(); a += genes_per_batch) {
+  // the columns of batch k + 1 are built on the host while batch k runs on
+  // the device
+  auto build = [&](size_t a) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
     std::vector<PermBase> bases(nb);
@@ -192,7 +196,15 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
       const size_t gi = c / B;
       permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &Y[c * n]);
     });
-    tr.mark("permutations: " + std::to_string(cols) + " columns built on the host");
+    return Y;
+  };
+  std::future<std::vector<double>> next = std::async(std::launch::async, build, size_t(0));
+  for (size_t a = 0; a < active.size(); a += genes_per_batch) {
+    const size_t nb = std::min(genes_per_batch, active.size() - a);
+    const size_t cols = nb * static_cast<size_t>(B);
+    const std::vector<double> Y = next.get();
+    if (a + genes_per_batch < active.size()) next = std::async(std::launch::async, build, a + genes_per_batch);
+    tr.mark("permutations: " + std::to_string(cols) + " columns ready (host build overlapped)");
     std::vector<double> minp(cols, 1.0);
     if (genes[active[a]].window) {
       // cis: one banded cis scan of every column with its gene's window
