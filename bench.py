@@ -222,6 +222,23 @@ def config(args):
             "parallelism": f"replicas x{args.gpus}"}
 
 
+# ------------------------------------------------------- replicas (N > 1)
+def max_over_ranks(values, device):
+    """Element-wise maximum of per-rank timings over the process group (the
+    slowest replica sets the step time)."""
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def whole_job_rate(tests_per_rank, world, ms_per_step):
+    """Tests per second of the whole job: every replica tests the same
+    workload, the step lasts as long as the slowest replica."""
+    return tests_per_rank * world / (ms_per_step / 1e3)
+
+
 # ------------------------------------------------------------------ B200 arm
 def b200_arm(args, rank, world, local_rank):
     import torch
@@ -273,15 +290,11 @@ def b200_arm(args, rank, world, local_rank):
         torch.cuda.synchronize()
     launches = ctx.launch_count() - launches0
     ms_total = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms_total, max(e2e_ms) if e2e_ms else 0.0], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms_total, e2e_max = float(t[0]), float(t[1])
-    else:
-        e2e_max = max(e2e_ms) if e2e_ms else 0.0
+    e2e_mean = statistics.mean(e2e_ms) if e2e_ms else 0.0
+    ms_total, e2e_mean = max_over_ranks([ms_total, e2e_mean], "cuda") if dist else (ms_total, e2e_mean)
     ms_step = ms_total / args.steps
-    value = tests * world / (ms_step / 1e3)
-    e2e_value = tests * world / (statistics.mean(e2e_ms) / 1e3) if e2e_ms else None
+    value = whole_job_rate(tests, world, ms_step)
+    e2e_value = whole_job_rate(tests, world, e2e_mean) if e2e_ms else None
 
     # ---- roofline of the dominant kernel (the scan tile kernel)
     scan_ms = statistics.mean(stage["scan"])
@@ -303,7 +316,7 @@ def b200_arm(args, rank, world, local_rank):
            "tests_per_step": tests, "gen_s": gen_s,
            "roofline": roof, "gpu_launches": launches,
            "clocks": clk.summary(),
-           "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": statistics.mean(e2e_ms) if e2e_ms else None,
+           "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": e2e_mean if e2e_ms else None,
                    "ms_steps": [round(v, 1) for v in e2e_ms],
                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
 

@@ -1,0 +1,112 @@
+"""Throughput of the cis permutation path through the eqtl program.
+
+    python -m eqtl_b200.perm_bench [--genes G] [--perm B] [--models lmm,lm]
+
+Seeded synthetic data with the shape of the cis-LMM permutation workload:
+n = 1,000 samples (25 families of 10 siblings + 750 unrelated), 3 chromosomes
+of 10 Mb at 1,500 SNPs per Mb (about 3,000 SNPs in each gene's +-1 Mb window),
+15 N(0,1) covariates, G genes with polygenic phenotypes (h2 ~ U(0, 0.8)),
+`--mode cis -w 1000000 --perm B`. Every permuted column gets its own REML fit
+and its own banded cis scan, as in the reference. The program runs with
+EQTL_TRACE=1; the JSON line reports wall time, the device stages of the
+permutation scans (CUDA events) and permuted columns per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+from . import synth
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+
+
+def make_case(d: str, genes: int, n: int = 1000, n_chrom: int = 3, chrom_mb: int = 10, per_mb: int = 1500,
+              n_cov: int = 15) -> int:
+    m = n_chrom * chrom_mb * per_mb
+    fam = (25, 10, n - 250) if n > 250 else None
+    rows, sub, _ = synth.make_bed_rows_chunked(4242, n, m, family=fam, keep_codes_every=20)
+    rng = np.random.default_rng(7)
+    clen = chrom_mb * 1_000_000
+    chrom, pos = [], []
+    for c in range(n_chrom):
+        p = np.sort(rng.choice(np.arange(1, clen + 1), size=m // n_chrom, replace=False))
+        chrom += [str(c + 1)] * (m // n_chrom)
+        pos.append(p)
+    pos = np.concatenate(pos)
+    samples = [f"S{i + 1:05d}" for i in range(n)]
+    pre = os.path.join(d, "geno")
+    with open(pre + ".fam", "w") as f:
+        for s in samples:
+            f.write(f"{s} {s} 0 0 0 -9\n")
+    with open(pre + ".bim", "w") as f:
+        for i in range(m):
+            f.write(f"{chrom[i]}\trs{i + 1}\t0\t{int(pos[i])}\tA\tG\n")
+    with open(pre + ".bed", "wb") as f:
+        f.write(bytes([0x6C, 0x1B, 0x01]))
+        f.write(rows.tobytes())
+    Y, _ = synth.polygenic_pheno(11, sub, genes)
+    C = rng.standard_normal((n, n_cov))
+    Y += 0.5 * C.sum(1, keepdims=True)
+    ids, gc, st, en, sd, _ = synth.make_genes(5, genes, [str(c + 1) for c in range(n_chrom)], clen, body=1)
+    synth.write_pheno(os.path.join(d, "pheno.tsv"), samples, ids, Y)
+    synth.write_covar(os.path.join(d, "covar.tsv"), samples, C)
+    synth.write_gff(os.path.join(d, "genes.gff"), ids, gc, st, en, sd)
+    return m
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--genes", type=int, default=100)
+    ap.add_argument("--perm", type=int, default=1000)
+    ap.add_argument("--models", default="lmm,lm")
+    args = ap.parse_args()
+    exe = os.path.join(PKG, "bin", "eqtl")
+    with tempfile.TemporaryDirectory(prefix="eqtl_perm_") as d:
+        m = make_case(d, args.genes)
+        for model in args.models.split(","):
+            cmd = [exe, "-b", os.path.join(d, "geno"), "-e", os.path.join(d, "pheno.tsv"), "-g",
+                   os.path.join(d, "genes.gff"), "-c", os.path.join(d, "covar.tsv"), "--model", model, "--mode",
+                   "cis", "-w", "1000000", "--perm", str(args.perm), "-o", os.path.join(d, "out")]
+            t0 = time.perf_counter()
+            r = subprocess.run(cmd, capture_output=True, text=True, env={**os.environ, "EQTL_TRACE": "1"})
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                sys.exit(f"{model}: eqtl failed: {r.stderr[-2000:]}")
+            stages = {"prep": 0.0, "scan": 0.0, "refine": 0.0}
+            perm_cols = 0
+            perm_ms = 0.0
+            for ln in r.stderr.splitlines():
+                mt = re.match(r"\[eqtl trace\] device stages of (\d+) columns \(ms\):(.*)", ln)
+                if mt and int(mt.group(1)) != args.genes:  # the permutation scans
+                    kv = mt.group(2).split()
+                    for k, v in zip(kv[0::2], kv[1::2]):
+                        if k in stages:
+                            stages[k] += float(v)
+                mt = re.match(r"\[eqtl trace\] permutations: device scan of (\d+) columns ([\d.]+) ms", ln)
+                if mt:
+                    perm_cols += int(mt.group(1))
+                    perm_ms += float(mt.group(2))
+            tested = 0
+            with open(os.path.join(d, f"out.{model}.cis.region.tsv")) as f:
+                next(f)
+                for ln in f:
+                    tested += int(ln.split("\t")[3])
+            print(json.dumps({"workload": "cis permutations", "model": model, "n_samples": 1000, "n_snps": m,
+                              "genes": args.genes, "perm": args.perm, "covariates": 15,
+                              "window_snps_mean": tested / max(args.genes, 1), "wall_s": wall,
+                              "perm_columns": perm_cols, "perm_device_call_ms": perm_ms,
+                              "perm_stage_ms": stages,
+                              "perm_columns_per_s": perm_cols / (perm_ms / 1e3) if perm_ms else None}))
+
+
+if __name__ == "__main__":
+    main()
