@@ -128,12 +128,14 @@ __global__ void grm_finalize_kernel(int n, int64_t m_used, const double* __restr
   const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (e >= static_cast<int64_t>(n) * n) return;
   const int i = static_cast<int>(e / n), j = static_cast<int>(e - static_cast<int64_t>(i) * n);
+  // the sums exist for i >= j (lower triangle); K is their mirror image above
+  const int64_t lo_e = static_cast<int64_t>(i >= j ? i : j) * n + (i >= j ? j : i);
   const int64_t mi = static_cast<int64_t>(J[static_cast<int64_t>(i) * n + i]);
   const int64_t mj = static_cast<int64_t>(J[static_cast<int64_t>(j) * n + j]);
   int64_t sub;
   if (i == j) sub = m_used - mi;
-  else sub = m_used - mi - mj + static_cast<int64_t>(J[e]);
-  K[e] = sub > 0 ? A[e] / static_cast<double>(sub) : 0.0;
+  else sub = m_used - mi - mj + static_cast<int64_t>(J[lo_e]);
+  K[e] = sub > 0 ? A[lo_e] / static_cast<double>(sub) : 0.0;
   if (j <= i) Npk[static_cast<int64_t>(i) * (i + 1) / 2 + j] = static_cast<int32_t>(sub);
 }
 
@@ -216,11 +218,19 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   const __half* bh[2] = {zh.p, mk.p};
   const __half* bl[2] = {zl.p, mk.p};
   const int bsel[2] = {0, 1}, prod[2] = {7, 1};
-  const int tiles = ((n + 127) / 128) * ((n + 255) / 256);
+  // K is symmetric: only the tiles of 128 rows x 256 columns that hold some
+  // element with row >= column (the tiles wholly above the diagonal are
+  // skipped)
+  std::vector<int2> lower;
+  for (int tb = 0; tb < (n + 255) / 256; ++tb)
+    for (int ta = 0; ta < (n + 127) / 128; ++ta)
+      if (128 * ta + 127 >= 256 * tb) lower.push_back(make_int2(ta, tb));
+  ws.grm_tiles.upload(lower.data(), lower.size(), st);
+  const int tiles = static_cast<int>(lower.size());
   const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
   // the GRM operands are FP16 regardless of the scan precision
-  launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, nullptr, 0,
-                        ksplit);
+  launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, ws.grm_tiles.p,
+                        tiles, ksplit);
   K.alloc(static_cast<size_t>(n) * n);
   Npk.alloc(static_cast<size_t>(n) * (n + 1) / 2);
   const int64_t tot = static_cast<int64_t>(n) * n;

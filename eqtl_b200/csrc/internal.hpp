@@ -171,6 +171,7 @@ struct Workspace {
   DevBuf<uint8_t> grm_use;
   DevBuf<double> grm_mean, grm_isd, grm_mean_u, grm_isd_u, grm_A, eig_work;
   DevBuf<int64_t> grm_rows;
+  DevBuf<int2> grm_tiles;  // lower-triangle tile list of the GRM contraction
   DevBuf<__half> grm_zh, grm_zl, grm_mk;
   DevBuf<int> grm_J, eig_info;
 };

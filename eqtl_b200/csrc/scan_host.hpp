@@ -142,10 +142,10 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
   sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
   sh.tile_list = tile_list;
-  sh.ksplit = tile_list ? 1 : std::max(1, std::min(ksplit, sh.kchunks));
+  sh.ksplit = std::max(1, std::min(ksplit, sh.kchunks));
   sh.kc_per_split = (sh.kchunks + sh.ksplit - 1) / sh.ksplit;
   sh.ksplit = (sh.kchunks + sh.kc_per_split - 1) / sh.kc_per_split;  // no empty ranges
-  sh.n_tiles = tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b * sh.ksplit;
+  sh.n_tiles = (tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b) * sh.ksplit;
   // gene-side tiles per raster group: keep the group's A operands (hi+lo of
   // every accumulator) within ~48 MB of L2
   {

@@ -67,7 +67,7 @@ struct TileShape {
   int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi
   int tiles_a;            // ceil(rows_a / 128)
   int tiles_b;            // ceil(rows_b / NT)
-  int n_tiles;            // work items: tiles_a * tiles_b * ksplit, or the tile-list length
+  int n_tiles;            // work items: (tiles_a * tiles_b or the tile-list length) * ksplit
   int ksplit;             // K ranges per output tile (split-K); 1 = whole K
   int group_a;            // gene-side tiles per raster group (L2 residency of the A operands)
   int kc_per_split;       // K chunks per range
@@ -99,7 +99,8 @@ struct TileCfg {
 __device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta, int& tb, int& k0, int& k1) {
   int ks = 0;
   if (sh.tile_list) {
-    const int2 c = sh.tile_list[t];
+    ks = t % sh.ksplit;
+    const int2 c = sh.tile_list[t / sh.ksplit];
     ta = c.x;
     tb = c.y;
   } else {
