@@ -139,8 +139,8 @@ struct PhenoDev {
 
 // Per-call workspaces reused across calls (capacity grows, never shrinks).
 struct Workspace {
-  DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
-  DevBuf<__half> ops_hi[20], ops_lo[20];  // gene-side operands, one per accumulator
+  DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, a00L, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
+  DevBuf<__half> ops_hi[34], ops_lo[34];  // gene-side operands, one per accumulator (dev::kMaxAcc)
   DevBuf<__half*> ops_ptr;
   DevBuf<float> unscale, gscale;
   DevBuf<uint8_t> ok;

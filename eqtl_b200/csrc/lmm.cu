@@ -38,7 +38,10 @@
 namespace eqtl {
 namespace dev {
 
-constexpr int kMaxPLmm = 16;
+constexpr int kMaxPLmm = 32;
+static_assert(kMaxPLmm + 2 <= kMaxAcc, "the grouped LMM scan needs p + 2 accumulators");
+static_assert(sizeof(Workspace::ops_hi) / sizeof(Workspace::ops_hi[0]) >= static_cast<size_t>(kMaxAcc),
+              "one gene-side operand buffer per accumulator");
 
 // ----------------------------------------------------------- rotation
 struct RotEpiParams {
@@ -183,13 +186,18 @@ __device__ double optimize_delta_dev(F&& f, int df) {
 }
 
 // prep_lmm caches (src/model_lmm.cpp:124-153) from A = X~'DX~ (p x p,
-// row-major), b = X~'Dy~ and y~'Dy~ at the chosen delta; one thread.
+// row-major), b = X~'Dy~ and y~'Dy~ at the chosen delta; one thread. Besides
+// chi0, A^-1 and rss, the lower Cholesky factor of A (row-major, zeros when A
+// is not positive definite) for the FP64 pair statistics.
 __device__ void reml_caches(double* A, const double* b, double y_dy, int p, int g, double* L, double* e,
-                            double* x, double* chi0_out, double* ainv_out, double* rss_out) {
+                            double* x, double* chi0_out, double* ainv_out, double* rss_out, double* a00L_out) {
   double chi0[kMaxPLmm];
   double ld;
   const bool ok = chol_solve(A, b, chi0, &ld, p, L);
   double rss = y_dy;
+  for (int i = 0; i < p; ++i)
+    for (int j = 0; j < p; ++j)
+      a00L_out[(static_cast<int64_t>(g) * p + i) * p + j] = ok && j <= i ? L[i * p + j] : 0.0;
   if (ok) {
     for (int k = 0; k < p; ++k) rss -= b[k] * chi0[k];
     if (rss < 0) rss = 0;
@@ -304,7 +312,7 @@ __global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict
                                                         const double* __restrict__ Xtil,
                                                         const double* __restrict__ lam, int n, int G,
                                                         double* delta_out, double* chi0_out, double* ainv_out,
-                                                        double* rss_out) {
+                                                        double* rss_out, double* a00L_out) {
   constexpr int NQ = P * (P + 1) / 2;
   const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (g >= G) return;  // whole warps only: no block barrier follows
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(256) reml_warp_kernel(const double* __restrict
     for (int a = 0; a < P; ++a)
       for (int b = a; b < P; ++b) A[a * P + b] = A[b * P + a] = tot[2 + a * P - a * (a - 1) / 2 + (b - a)];
     delta_out[g] = d;
-    reml_caches(A, tot + 2 + NQ, tot[1], P, g, L, e, x, chi0_out, ainv_out, rss_out);
+    reml_caches(A, tot + 2 + NQ, tot[1], P, g, L, e, x, chi0_out, ainv_out, rss_out, a00L_out);
   }
 }
 
@@ -564,17 +572,20 @@ __device__ double rb_negll(const double* __restrict__ Acol, const double* __rest
 // One thread per column: reads the round's -loglik values, advances the
 // search exactly as optimize_delta_dev does, and proposes the next round's
 // deltas; in the final round writes delta and the prep_lmm caches.
+// PMAX bounds p for the per-thread p x p scratch (p <= 16 keeps the stack
+// frame small; 17..32 use the larger instance).
+template <int PMAX>
 __global__ void rb_advance_kernel(int C, int g0, int p, int df, const double* __restrict__ A,
                                   const double* __restrict__ B, const double* __restrict__ ld,
                                   const double* __restrict__ ydy, RemlBatchState* st, double* dlt,
                                   unsigned int* active, double* delta_out, double* chi0_out, double* ainv_out,
-                                  double* rss_out) {
+                                  double* rss_out, double* a00L_out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C) return;
   RemlBatchState s = st[c];
   if (s.phase == kRbDone) return;
   const int nq = p * (p + 1) / 2;
-  double Af[kMaxPLmm * kMaxPLmm], L[kMaxPLmm * kMaxPLmm];
+  double Af[PMAX * PMAX], L[PMAX * PMAX];
   auto f = [&](int slot) {
     const int si = slot * C + c;
     return rb_negll(A + static_cast<int64_t>(si) * nq, B + static_cast<int64_t>(si) * p, ydy[si], ld[si], p, df,
@@ -634,7 +645,8 @@ __global__ void rb_advance_kernel(int C, int g0, int p, int df, const double* __
         for (int b = a; b < p; ++b) Af[a * p + b] = Af[b * p + a] = Acol[tri(a, b, p)];
       double e[kMaxPLmm], x[kMaxPLmm];
       delta_out[g0 + c] = s.d;
-      reml_caches(Af, B + static_cast<int64_t>(si) * p, ydy[si], p, g0 + c, L, e, x, chi0_out, ainv_out, rss_out);
+      reml_caches(Af, B + static_cast<int64_t>(si) * p, ydy[si], p, g0 + c, L, e, x, chi0_out, ainv_out, rss_out,
+                  a00L_out);
       s.phase = kRbDone;
       break;
     }
@@ -1045,7 +1057,7 @@ __global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const in
                                   const int2* __restrict__ pairs, int n_pairs, const double* __restrict__ Ytil,
                                   const double* __restrict__ Xtil, int p, const double* __restrict__ lam,
                                   const double* __restrict__ delta, const double* __restrict__ chi0,
-                                  const double* __restrict__ ainv, const double* __restrict__ rss, double df,
+                                  const double* __restrict__ a00L, const double* __restrict__ rss, double df,
                                   eqtl_pair* out) {
   const int lane = threadIdx.x & 31;
   const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -1074,7 +1086,7 @@ __global__ void lmm_refine_kernel(const double* __restrict__ Gt, int n, const in
     q.snp = pairs[w].y;
     q.gene = g;
     q.reserved = 0;
-    lmm_stats_fp64(gg, yg, a, chi0 + static_cast<int64_t>(g) * p, ainv + static_cast<int64_t>(g) * p * p, rss[g],
+    lmm_stats_fp64(gg, yg, a, chi0 + static_cast<int64_t>(g) * p, a00L + static_cast<int64_t>(g) * p * p, rss[g],
                    p, df, q);
     out[w] = q;
   }
@@ -1399,9 +1411,10 @@ static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
                              ws.rb_WY.p, n, &zero, ws.rb_B.p, p) == CUBLAS_STATUS_SUCCESS,
                  EQTL_E_CUDA, "REML X'Dy failed");
       EQTL_CUDA(cudaMemsetAsync(ws.rb_active.p, 0, sizeof(unsigned int), st));
-      rb_advance_kernel<<<cblocks, 128, 0, st>>>(C, g0, p, df, ws.rb_A.p, ws.rb_B.p, ws.rb_ld.p, ws.rb_ydy.p, state,
-                                                 ws.rb_dlt.p, ws.rb_active.p, ws.delta.p, ws.chi0.p, ws.ainv.p,
-                                                 ws.rss.p);
+      auto advance = p <= 16 ? rb_advance_kernel<16> : rb_advance_kernel<kMaxPLmm>;
+      advance<<<cblocks, 128, 0, st>>>(C, g0, p, df, ws.rb_A.p, ws.rb_B.p, ws.rb_ld.p, ws.rb_ydy.p, state,
+                                       ws.rb_dlt.p, ws.rb_active.p, ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p,
+                                       ws.a00L.p);
       EQTL_CUDA(cudaGetLastError());
       // the golden phase runs the same number of rounds for every column;
       // from the Newton phase on, stop once no column is left
@@ -1418,7 +1431,7 @@ static void reml_batched(eqtl_ctx* ctx, int n, int p, int G) {
 void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
   const int n = ph.n, G = ph.G, p = ph.p;
   EQTL_CHECK(ctx->have_basis && ctx->basis.n == n, EQTL_E_STATE, "LMM prep needs an eigenbasis of size n");
-  EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED, "the device LMM handles 1 <= p <= 16 covariate columns");
+  EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED, "the device LMM handles 1 <= p <= 32 covariate columns");
   cudaStream_t st = ctx->stream;
   Workspace& ws = ctx->ws;
   cublasHandle_t h = blas_of(ctx);
@@ -1438,13 +1451,14 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
   ws.delta.alloc(G);
   ws.chi0.alloc(static_cast<size_t>(G) * p);
   ws.ainv.alloc(static_cast<size_t>(G) * p * p);
+  ws.a00L.alloc(static_cast<size_t>(G) * p * p);
   ws.rss.alloc(G);
   ++ctx->launches;
   if (p <= kRemlWarpP) {
     const unsigned blocks = static_cast<unsigned>((G + 7) / 8);
     auto args = [&](auto kern) {
       kern<<<blocks, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, n, G, ws.delta.p, ws.chi0.p,
-                                   ws.ainv.p, ws.rss.p);
+                                   ws.ainv.p, ws.rss.p, ws.a00L.p);
     };
     if (p == 1) args(reml_warp_kernel<1>);
     else if (p == 2) args(reml_warp_kernel<2>);
@@ -1548,7 +1562,7 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
     ws.refined.alloc(todo.size());
     lmm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
         gt.p, n, dpc.p, dtodo.p, static_cast<int>(todo.size()), ws.Ytil.p, ws.Xtil.p, p, ctx->basis.lambda.p,
-        ws.delta.p, ws.chi0.p, ws.ainv.p, ws.rss.p, df, ws.refined.p);
+        ws.delta.p, ws.chi0.p, ws.a00L.p, ws.rss.p, df, ws.refined.p);
     EQTL_CUDA(cudaGetLastError());
     tr.mark("launches");
     ws.refined.download(refined.data(), todo.size(), st);
@@ -1618,7 +1632,7 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_trans_lmm: no genes");
   EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_trans_lmm: more than 2^30 kept SNPs");
   EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED,
-             "the LMM scan handles 1 to 16 covariate columns (intercept included)");
+             "the LMM scan handles 1 to 32 covariate columns (intercept included)");
   EQTL_CHECK(!(simt && p > 2), EQTL_E_UNSUPPORTED, "the FP32 CUDA-core comparator covers 1 or 2 covariate columns");
   const bool grouped = p > 2;  // accumulators run in groups of four (LmmGroupEpi)
   cudaStream_t st = ctx->stream;

@@ -101,19 +101,29 @@ EQTL_HD void lmm_stats_num_s(double num, double S, double rss_null, double df, e
 }
 
 // LMM pair from gg = Gt'W Gt, yg = Gt'W y~, a = X~'W Gt and the gene's null
-// fit (chi0, ainv = (X~'W X~)^-1 row-major, rss_null).
-EQTL_HD void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* ainv,
+// fit (chi0, L = lower Cholesky factor of X~'W X~ row-major, rss_null; L = 0
+// where that matrix was not positive definite). a'A00^-1 a is |z|^2 with
+// L z = a, a solve as in the reference (src/scan_trans_lmm.cpp:26,
+// src/model_lmm.cpp:179): with a badly conditioned A00 an explicit inverse
+// loses cond(A00) eps there, the triangular solve only sqrt(cond(A00)) eps,
+// and S = gg - a'A00^-1 a can cancel by orders of magnitude.
+constexpr int kStatsMaxP = 32;
+EQTL_HD void lmm_stats_fp64(double gg, double yg, const double* a, const double* chi0, const double* L,
                             double rss_null, int p, double df, eqtl_pair& q) {
   q.beta = q.se = q.t = q.r2 = 0.0;
   q.p = 1.0;
   if (gg < 1e-12) return;
   double aTu = 0, aTchi = 0;
-  for (int x = 0; x < p; ++x) {
-    double ux = 0;
-    for (int y = 0; y < p; ++y) ux += ainv[x * p + y] * a[y];
-    aTu += a[x] * ux;
-    aTchi += a[x] * chi0[x];
+  if (p > 0 && L[0] > 0) {
+    double z[kStatsMaxP];
+    for (int x = 0; x < p; ++x) {
+      double t = a[x];
+      for (int y = 0; y < x; ++y) t -= L[x * p + y] * z[y];
+      z[x] = t / L[x * p + x];
+      aTu += z[x] * z[x];
+    }
   }
+  for (int x = 0; x < p; ++x) aTchi += a[x] * chi0[x];
   const double S = gg - aTu;
   if (S <= 1e-15) return;
   const double bg = (yg - aTchi) / S;

@@ -46,7 +46,7 @@ struct IsTwoPhase : std::false_type {};
 template <class E>
 struct IsTwoPhase<E, std::void_t<decltype(E::kTwoPhase)>> : std::bool_constant<E::kTwoPhase> {};
 
-constexpr int kMaxAcc = 20;  // accumulators of one tile over all its groups
+constexpr int kMaxAcc = 34;  // accumulators of one tile over all its groups (LMM: p + 2, p <= 32)
 constexpr int kEpiWarps = 16;
 constexpr int kTileThreads = 64 + 32 * kEpiWarps;
 constexpr int kTileM = 128;

@@ -54,10 +54,12 @@ def test_basis_eigenvalues():
     np.testing.assert_allclose((Q * lam) @ Q.T, (Qr * lr) @ Qr.T, atol=1e-9)
 
 
-@pytest.mark.parametrize("ncov,prec", [(0, 0), (1, 0), (0, 2), (2, 0), (5, 0)])
+@pytest.mark.parametrize("ncov,prec", [(0, 0), (1, 0), (0, 2), (2, 0), (5, 0), (20, 0)])
 def test_trans_lmm_matches_oracle(ncov, prec):
-    """ncov 0-1: three or four accumulators in one TMEM group; ncov 2 and 5
-    (p = 3, 6): orthonormalised covariate accumulators in groups of four."""
+    """ncov 0-1: three or four accumulators in one TMEM group; ncov 2, 5 and
+    20 (p = 3, 6, 21): orthonormalised covariate accumulators in groups of
+    four; p > 3 also takes the batched REML, and p = 21 its larger scratch
+    instance."""
     from eqtl_b200 import capi
     g, rows, Y, X = _case(ncov=ncov)
     n = g.codes.shape[1]
@@ -75,14 +77,16 @@ def test_trans_lmm_matches_oracle(ncov, prec):
 
 
 def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam, pthr=1e-3, excl=None):
-    """REML delta: equal to the oracle's within 1e-5, or, where they differ,
-    an optimum of the same objective within 1e-6 of it. That happens at the
-    edge of the search (grid best 1e-5, golden section down to 2.5e-6): the
-    Newton polish there differences with h = 1e-9, so its steps follow FP64
-    rounding on either side. The statistics are then checked at the
-    device's delta."""
+    """REML delta: wherever the device's delta differs from the oracle's, it
+    must be an optimum of the same objective (-loglik within 1e-6 of the
+    oracle's), and the statistics are then checked at the device's delta.
+    The objective is flat at its optimum, so two FP64 runs of the same
+    schedule stop at slightly different deltas (at the edge of the search,
+    grid best 1e-5, the Newton polish differences with h = 1e-9 and follows
+    FP64 rounding); with many covariates beta moves ~1e-5 across that flat
+    part."""
     d_ora = ora["delta"]
-    flat = np.abs(d_dev - d_ora) > 1e-5 * np.abs(d_ora)
+    flat = d_dev != d_ora
     if not flat.any():
         return ora, pairs_ref
     df = Y.shape[0] - X.shape[1]
