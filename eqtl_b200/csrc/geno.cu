@@ -13,6 +13,8 @@
 // contain an intercept; it removes the mean from the split).
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "internal.hpp"
 
 namespace eqtl {
@@ -108,6 +110,101 @@ __global__ void bed_expand_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
   }
 }
 
+// One warp per kept SNP row, for rows of at most kExpandMaxStage staged
+// bytes. The packed row goes to shared memory with 16-byte loads, starting at
+// the 16-byte boundary at or below the row start (the device copy of the .bed
+// carries kBedPad bytes of padding, so the last row's over-read stays inside
+// the buffer); the four values a 2-bit code can take are formed once per row
+// with bed_expand_kernel's FP64 arithmetic, so the output bits are the same;
+// each lane then writes 8 consecutive samples of hi and of lo per step with
+// 16-byte stores (512 contiguous bytes per warp store).
+constexpr int kExpandWarps = 8;
+constexpr int64_t kBedPad = 32;
+constexpr int kExpandMaxStage = 12288;
+
+__device__ __forceinline__ uint16_t bits16(__half h) { return __half_as_ushort(h); }
+__device__ __forceinline__ uint16_t bits16(__nv_bfloat16 h) { return __bfloat16_as_ushort(h); }
+
+// With the identity sample map (analysis sample k = file column k), samples
+// are decoded two at a time: a 16-entry table per row, indexed by the two
+// 2-bit codes, holds the packed hi and lo words of the pair (8 bytes; the
+// 128-byte table covers the 32 banks once, so the lookups do not conflict).
+template <class T>
+__global__ void __launch_bounds__(32 * kExpandWarps, 4)
+    bed_expand_warp_kernel(const uint8_t* __restrict__ bed, int64_t bps, int stage_bytes,
+                           const int32_t* __restrict__ col, int identity, int n, int k_pad,
+                           const int64_t* __restrict__ kept, int64_t m_kept, const double* __restrict__ mu,
+                           float scale, T* hi, T* lo) {
+  extern __shared__ __align__(16) uint8_t expand_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint2* pair_lut = reinterpret_cast<uint2*>(expand_smem) + warp * 16;
+  uint8_t* row_s = expand_smem + kExpandWarps * 16 * sizeof(uint2) + warp * stage_bytes;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kExpandWarps;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * kExpandWarps + warp; r < m_kept; r += nwarps) {
+    const int64_t s = __ldg(kept + r);
+    const int64_t off0 = s * bps;
+    const int64_t a0 = off0 & ~int64_t(15);
+    const int skew = static_cast<int>(off0 - a0);
+    const int nvec = static_cast<int>((skew + bps + 15) / 16);
+    const uint4* src = reinterpret_cast<const uint4*>(bed + a0);
+    uint4* dst = reinterpret_cast<uint4*>(row_s);
+    __syncwarp();  // the previous row's bytes are no longer read
+    for (int v = lane; v < nvec; v += 32) dst[v] = __ldg(src + v);
+    // values of the 2-bit codes 00, 01, 10, 11 (A1 count 2, missing, 1, 0)
+    uint32_t word = 0;
+    if (lane < 4) {
+      const int c = lane == 0 ? 2 : (lane == 1 ? -1 : (lane == 2 ? 1 : 0));
+      double v = c < 0 ? 0.0 : (static_cast<double>(c) - __ldg(mu + s));
+      v *= static_cast<double>(scale);
+      const T h = to16<T>(v);
+      const T l = to16<T>(v - from16(h));
+      word = static_cast<uint32_t>(bits16(h)) | (static_cast<uint32_t>(bits16(l)) << 16);
+    }
+    const uint32_t w0 = __shfl_sync(0xffffffffu, word, 0), w1 = __shfl_sync(0xffffffffu, word, 1);
+    const uint32_t w2 = __shfl_sync(0xffffffffu, word, 2), w3 = __shfl_sync(0xffffffffu, word, 3);
+    if (lane < 16) {  // entry (code of the first sample) | (code of the second) << 2
+      const int ca = lane & 3, cb = lane >> 2;
+      const uint32_t wa = ca == 0 ? w0 : (ca == 1 ? w1 : (ca == 2 ? w2 : w3));
+      const uint32_t wb = cb == 0 ? w0 : (cb == 1 ? w1 : (cb == 2 ? w2 : w3));
+      pair_lut[lane] = make_uint2((wa & 0xFFFFu) | (wb << 16), (wa >> 16) | (wb & 0xFFFF0000u));
+    }
+    __syncwarp();  // the staged row and the table are visible to every lane
+    for (int k0 = lane * 8; k0 < k_pad; k0 += 256) {
+      if (identity && k0 + 8 <= n) {  // samples k0 .. k0+7: bytes k0/4 and k0/4 + 1
+        const uint32_t b = static_cast<uint32_t>(row_s[skew + (k0 >> 2)]) |
+                           (static_cast<uint32_t>(row_s[skew + (k0 >> 2) + 1]) << 8);
+        const uint2 e0 = pair_lut[b & 15u], e1 = pair_lut[(b >> 4) & 15u];
+        const uint2 e2 = pair_lut[(b >> 8) & 15u], e3 = pair_lut[(b >> 12) & 15u];
+        const int64_t o = r * k_pad + k0;
+        *reinterpret_cast<uint4*>(hi + o) = make_uint4(e0.x, e1.x, e2.x, e3.x);
+        *reinterpret_cast<uint4*>(lo + o) = make_uint4(e0.y, e1.y, e2.y, e3.y);
+        continue;
+      }
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        uint32_t pv[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int k = k0 + j + q;
+          uint32_t v = 0;  // padding samples: +0 in hi and lo
+          if (k < n) {
+            const int c = __ldg(col + k);
+            const uint32_t code = (static_cast<uint32_t>(row_s[skew + (c >> 2)]) >> ((c & 3) * 2)) & 3u;
+            v = code == 0 ? w0 : (code == 1 ? w1 : (code == 2 ? w2 : w3));
+          }
+          pv[q] = v;
+        }
+        hw[j / 2] = (pv[0] & 0xFFFFu) | (pv[1] << 16);
+        lw[j / 2] = (pv[0] >> 16) | (pv[1] & 0xFFFF0000u);
+      }
+      const int64_t o = r * k_pad + k0;
+      *reinterpret_cast<uint4*>(hi + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(lo + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+  }
+}
+
 __global__ void bed_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
                                   int n, const int64_t* __restrict__ kept, int64_t lo, int64_t hi,
                                   const double* __restrict__ mu, double* out) {
@@ -153,7 +250,11 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   g.n_file = n_file;
   g.bytes_per_snp = bytes_per_snp;
   g.k_pad = ((n + 63) / 64) * 64;
-  g.bed.upload(rows, static_cast<size_t>(m * bytes_per_snp), st);
+  // kBedPad bytes past the last row: bed_expand_warp_kernel stages rows in
+  // 16-byte vectors from the boundary at or below each row start
+  g.bed.alloc(static_cast<size_t>(m * bytes_per_snp + kBedPad));
+  if (m > 0)
+    EQTL_CUDA(cudaMemcpyAsync(g.bed.p, rows, static_cast<size_t>(m * bytes_per_snp), cudaMemcpyHostToDevice, st));
   g.col.upload(sample_col, n, st);
   g.n_miss.alloc(m);
   g.s1.alloc(m);
@@ -187,7 +288,30 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   const size_t elems = static_cast<size_t>(g.m) * g.k_pad;
   g.gc_hi.alloc(elems);
   g.gc_lo.alloc(elems);
-  if (g.m > 0) {
+  const int stage = static_cast<int>(((bytes_per_snp + 30) / 16) * 16);
+  if (g.m > 0 && stage <= kExpandMaxStage) {
+    const int smem = stage * kExpandWarps + kExpandWarps * 16 * static_cast<int>(sizeof(uint2));
+    int identity = 1;
+    for (int i = 0; i < n; ++i) identity &= sample_col[i] == i;
+    const unsigned blocks = static_cast<unsigned>(
+        std::min<int64_t>((g.m + kExpandWarps - 1) / kExpandWarps, static_cast<int64_t>(ctx->sm_count) * 16));
+    ++ctx->launches;
+    if (ctx->precision == EQTL_PREC_SPLIT_BF16) {
+      auto kern = bed_expand_warp_kernel<__nv_bfloat16>;
+      EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      kern<<<blocks, 32 * kExpandWarps, smem, st>>>(g.bed.p, bytes_per_snp, stage, g.col.p, identity, n, g.k_pad,
+                                                    g.kept.p, g.m, g.mu.p, kGcScale,
+                                                    reinterpret_cast<__nv_bfloat16*>(g.gc_hi.p),
+                                                    reinterpret_cast<__nv_bfloat16*>(g.gc_lo.p));
+    } else {
+      auto kern = bed_expand_warp_kernel<__half>;
+      EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      kern<<<blocks, 32 * kExpandWarps, smem, st>>>(g.bed.p, bytes_per_snp, stage, g.col.p, identity, n, g.k_pad,
+                                                    g.kept.p, g.m, g.mu.p, kGcScale, g.gc_hi.p, g.gc_lo.p);
+    }
+    EQTL_CUDA(cudaGetLastError());
+  } else if (g.m > 0) {
+    // rows too long to stage (more than ~49,000 samples in the file)
     dim3 grid((g.k_pad + 255) / 256, static_cast<unsigned>(g.m < 65535 ? g.m : 65535));
     ++ctx->launches;
     if (ctx->precision == EQTL_PREC_SPLIT_BF16) {
