@@ -1,0 +1,114 @@
+"""Timings of the association-scan path at the benchmark shapes other than the
+headline trans-LMM one (bench.py), through the C ABI with the inputs resident
+on the device.
+
+    python -m eqtl_b200.config_bench [--which grm,lm] [--steps K]
+
+grm  GRM build, eigendecomposition and spectral rotation: n = 2,000 samples
+     (50 families of 10 siblings + 1,500 unrelated), m = 200,000 SNPs with
+     MAF ~ U(0.01, 0.5) and 1% missing calls.
+lm   trans/gw LM scan: n = 1,000 samples, m = 1,000,000 SNPs, 20,000 genes
+     with Y ~ N(0, 1), intercept + 10 N(0, 1) covariates, p threshold 1e-5.
+
+Seeded synthetic data of those shapes (no data set ships with the
+reference). Each JSON line gives the CUDA-event stage times (median over the
+timed steps, after one warm-up step) and the algorithmic rate of each stage's
+dominant kernel against the measured peaks (the fallback figures when
+MEASURED_PEAKS.json is absent).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+
+import numpy as np
+
+from . import capi, synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def grm_case(steps: int) -> dict:
+    n, m = 2000, 200_000
+    rows, _, _ = synth.make_bed_rows_chunked(20261202, n, m, family=(50, 10, 1500), maf_lo=0.01, maf_hi=0.5,
+                                             miss_rate=0.01)
+    pk, kind = _peaks()
+    with capi.Context(0) as c:
+        keep, _, _ = c.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        decode = c.stage_ms("decode")
+        t = {"grm": [], "eigen": [], "rotate": []}
+        for i in range(steps + 1):
+            c.lmm_basis(outputs=False)
+            c.rotate()
+            if i:
+                for k in t:
+                    t[k].append(c.stage_ms(k))
+    med = {k: statistics.median(v) for k, v in t.items()}
+    m_kept = int(np.count_nonzero(keep))
+    grm_flops = float(n) * (n + 1) * m_kept          # SYRK, symmetric half counted once
+    rot_flops = 2.0 * n * n * m_kept
+    peak = pk.get("bf16_tflops", 1590.0)
+    return {"workload": "GRM build + eigendecomposition + spectral rotation", "n_samples": n, "n_snps": m,
+            "kept_snps": m_kept, "steps": steps, "decode_ms": decode, "stage_ms": med,
+            "grm": {"algorithmic_tflops": grm_flops / (med["grm"] / 1e3) / 1e12,
+                    "frac_of_bf16_peak": grm_flops / (med["grm"] / 1e3) / 1e12 / peak,
+                    "note": "stage time: per-SNP statistics, FP16 operand transpose, tensor-core SYRK "
+                            "(lower-triangle tiles, 3 split products + missing-mask product), division"},
+            "rotation": {"algorithmic_tflops": rot_flops / (med["rotate"] / 1e3) / 1e12,
+                         "frac_of_bf16_peak": rot_flops / (med["rotate"] / 1e3) / 1e12 / peak},
+            "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
+
+
+def lm_case(steps: int) -> dict:
+    n, m, G, ncov = 1000, 1_000_000, 20_000, 10
+    rows, _, _ = synth.make_bed_rows_chunked(20261203, n, m, maf_lo=0.01, maf_hi=0.5, miss_rate=0.01)
+    rng = np.random.default_rng(20261204)
+    Y = rng.standard_normal((n, G))
+    X = np.column_stack([np.ones(n), rng.standard_normal((n, ncov))])
+    pk, kind = _peaks()
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        c.pheno_load(Y, X)
+        t = {"prep": [], "scan": [], "refine": []}
+        tests = 0
+        for i in range(steps + 1):
+            genes, pairs, _ = c.scan_trans_lm(None, None, pthr=1e-5)
+            if i:
+                tests = int(genes["n_tested"].sum())
+                for k in t:
+                    t[k].append(c.stage_ms(k))
+    med = {k: statistics.median(v) for k, v in t.items()}
+    step_ms = sum(med.values())
+    flops = 2.0 * n * tests                               # numerators G~'Y_s
+    peak = pk.get("bf16_tflops_sustained", 1400.0)
+    return {"workload": "trans/gw LM scan (--model lm --mode gw)", "n_samples": n, "n_snps": m, "n_genes": G,
+            "covariates": ncov, "pthr": 1e-5, "steps": steps, "tests_per_step": tests, "stage_ms": med,
+            "tests_per_s": tests / (step_ms / 1e3), "pairs": int(len(pairs)),
+            "scan": {"algorithmic_tflops": flops / (med["scan"] / 1e3) / 1e12,
+                     "frac_of_bf16_sustained": flops / (med["scan"] / 1e3) / 1e12 / peak,
+                     "issued_products": 3},
+            "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--which", default="grm,lm")
+    ap.add_argument("--steps", type=int, default=3)
+    args = ap.parse_args()
+    for w in args.which.split(","):
+        out = grm_case(args.steps) if w == "grm" else lm_case(args.steps)
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

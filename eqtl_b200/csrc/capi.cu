@@ -200,17 +200,29 @@ void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std
 void add_deferred_acat(eqtl_gene_result* genes, const std::vector<eqtl_pair>& refined,
                        const std::vector<int2>& deferred) {
   const long double kPiL = 3.14159265358979323846L;
-  for (const int2& d : deferred) {
+  // terms on every host thread, then added in pair order (the sums do not
+  // depend on the thread count)
+  std::vector<double> term(deferred.size());
+  std::vector<uint8_t> use(deferred.size());
+  std::vector<uint8_t> found(deferred.size());
+  parallel_for(deferred.size(), [&](size_t i) {
+    const int2 d = deferred[i];
     auto it = std::lower_bound(refined.begin(), refined.end(), d, [](const eqtl_pair& q, const int2& k) {
       return q.gene != k.x ? q.gene < k.x : q.snp < static_cast<int64_t>(k.y);
     });
-    EQTL_CHECK(it != refined.end() && it->gene == d.x && it->snp == d.y, EQTL_E_INTERNAL,
-               "deferred ACAT pair was not refined");
+    found[i] = it != refined.end() && it->gene == d.x && it->snp == d.y;
+    if (!found[i]) return;
     double p = it->p;
-    if (!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12) continue;  // AcatAcc::add guards
+    use[i] = !(!std::isfinite(p) || p < 0.0 || p >= 1.0 - 1e-12);  // AcatAcc::add guards
+    if (!use[i]) return;
     if (p <= 0.0) p = 1e-300;
-    genes[d.x].acat_tan_sum += static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
-    ++genes[d.x].acat_used;
+    term[i] = static_cast<double>(std::tan((0.5L - static_cast<long double>(p)) * kPiL));
+  });
+  for (size_t i = 0; i < deferred.size(); ++i) {
+    EQTL_CHECK(found[i], EQTL_E_INTERNAL, "deferred ACAT pair was not refined");
+    if (!use[i]) continue;
+    genes[deferred[i].x].acat_tan_sum += term[i];
+    ++genes[deferred[i].x].acat_used;
   }
 }
 

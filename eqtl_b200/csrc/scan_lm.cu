@@ -384,11 +384,19 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
 
   // ---- refine candidates + per-gene best in FP64
   StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
+  HostTrace tr("scan_trans_lm");
   std::vector<int2> todo, deferred;
   so.collect(genes, todo, deferred);
+  tr.mark("collect");
   std::vector<eqtl_pair> refined = lm_refine_pairs(ctx, df, todo);
+  tr.mark("refine pairs (device + download)");
   add_deferred_acat(genes, refined, deferred);
+  tr.mark("deferred ACAT terms");
   finish_scan(prm, genes, refined, pairs, cands);
+  tr.mark("finish");
+  if (tr.on)
+    std::fprintf(stderr, "[eqtl trace] scan_trans_lm counts: refined %zu deferred %zu\n", todo.size(),
+                 deferred.size());
 }
 
 // FP64 tests of explicit (column of Y, kept SNP) pairs with the scan's prep:
