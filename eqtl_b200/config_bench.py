@@ -69,8 +69,8 @@ def grm_case(steps: int) -> dict:
             "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
 
 
-def lm_case(steps: int) -> dict:
-    n, m, G, ncov = 1000, 1_000_000, 20_000, 10
+def lm_case(steps: int, m: int = 1_000_000, G: int = 20_000) -> dict:
+    n, ncov = 1000, 10
     rows, _, _ = synth.make_bed_rows_chunked(20261203, n, m, maf_lo=0.01, maf_hi=0.5, miss_rate=0.01)
     rng = np.random.default_rng(20261204)
     Y = rng.standard_normal((n, G))
@@ -104,9 +104,11 @@ def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--which", default="grm,lm")
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--lm-snps", type=int, default=1_000_000, help="SNPs of the lm case (smaller for profiling)")
+    ap.add_argument("--lm-genes", type=int, default=20_000, help="genes of the lm case")
     args = ap.parse_args()
     for w in args.which.split(","):
-        out = grm_case(args.steps) if w == "grm" else lm_case(args.steps)
+        out = grm_case(args.steps) if w == "grm" else lm_case(args.steps, args.lm_snps, args.lm_genes)
         print(json.dumps(out), flush=True)
 
 

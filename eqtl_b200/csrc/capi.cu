@@ -354,6 +354,9 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
   t.dl_inv = static_cast<float>(T.nb / (T.x_defer - T.x0));
   // round t_defer down so that every pair with p <= 1e-14 is deferred
   t.t_defer = static_cast<float>(T.t_defer * (1.0 - 1e-6));
+  t.u0 = static_cast<float>(T.t0 * T.t0);
+  t.u_tiny = t.tiny_t * t.tiny_t;
+  t.u_defer = static_cast<float>(T.t_defer * T.t_defer * (1.0 - 2e-6));
   t.na = T.na;
   t.nb = T.nb;
   return t;
@@ -397,7 +400,7 @@ __global__ void t_tail_kernel(dev::TTable T, const float* t, int64_t n, int use_
   if (i >= n) return;
   if (screen) {
     const dev::ScreenOut o = dev::acat_screen(t[i], tt);
-    nl[i] = o.key_t;
+    nl[i] = o.key;
     term[i] = o.term;
     flags[i] = static_cast<uint8_t>((o.use_acat ? 1 : 0) | (o.deferred ? 2 : 0) | (o.tiny ? 4 : 0));
     return;

@@ -757,9 +757,10 @@ struct LmmEpi {
   // S per pair of the warp's two chunks (0 where gg < 1e-12); two named
   // arrays picked by a select, so they stay in registers for a runtime ci
   float S0[16], S1[16];
+  float u_cand;  // t_cand^2
   GeneAcc acc;
   __device__ LmmEpi(const Params& p, const TileShape&, uint8_t* smem)
-      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt), u_cand(p.t_cand * p.t_cand) {}
   __device__ void init(int tid, int nthr) {
     if (tsm) tt = screen_to_smem(Pr.tt, tsm, tid, nthr);
   }
@@ -820,10 +821,10 @@ struct LmmEpi {
       const float r = num * __fdividef(num, S) * inv_rss;
       const float omr = 1.0f - r;
       const bool ok_stat = S > 1e-15f && omr > 0.0f;
-      const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num) : 0.0f;
-      const ScreenOut o = acat_screen(t, tt);
+      const float u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      const ScreenOut o = acat_screen_u(u, tt);
       acc.add_screen(o, s, valid);
-      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
+      if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }
   // Both phases at once (the CUDA-core comparator): v in the tile's order.
@@ -957,9 +958,10 @@ struct LmmGroupEpi {
   bool gvalid = false;
   float inv_rss = 0;
   float num[16], S[16];
+  float u_cand;  // t_cand^2
   GeneAcc acc;
   __device__ LmmGroupEpi(const Params& p, const TileShape&, uint8_t* smem)
-      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+      : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt), u_cand(p.t_cand * p.t_cand) {}
   __device__ void init(int tid, int nthr) {
     if (tsm) tt = screen_to_smem(Pr.tt, tsm, tid, nthr);
   }
@@ -1003,10 +1005,10 @@ struct LmmGroupEpi {
       const float r = num[j] * __fdividef(num[j], S[j]) * inv_rss;
       const float omr = 1.0f - r;
       const bool ok_stat = S[j] > 1e-15f && omr > 0.0f;
-      const float t = ok_stat ? copysignf(sqrtf(Pr.df * __fdividef(r, omr)), num[j]) : 0.0f;
-      const ScreenOut o = acat_screen(t, tt);
+      const float u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      const ScreenOut o = acat_screen_u(u, tt);
       acc.add_screen(o, s, valid);
-      if (valid && (fabsf(t) >= Pr.t_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
+      if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
   }
   __device__ void end_tile() {

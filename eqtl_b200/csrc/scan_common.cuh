@@ -76,7 +76,8 @@ struct GeneAcc {
       best = k < best ? k : best;
     }
   }
-  // The same for the epilogues' ACAT screen (best SNP keyed on |t|).
+  // The same for the epilogues' ACAT screen (best SNP keyed on the screen's
+  // key, t^2 in the scans).
   __device__ __forceinline__ void add_screen(const ScreenOut& o, int64_t s, bool valid) {
     if (valid) {
       ++tested;
@@ -84,7 +85,7 @@ struct GeneAcc {
         acat += o.term;
         ++used;
       }
-      const unsigned long long k = best_key(o.key_t, static_cast<uint32_t>(s));
+      const unsigned long long k = best_key(o.key, static_cast<uint32_t>(s));
       best = k < best ? k : best;
     }
   }

@@ -55,10 +55,11 @@ struct LmEpi {
   bool gvalid = false;
   float inv_yty = 0;
   float gs = 0;
+  float u_cand;  // t_cand^2
   GeneAcc acc;
 
   __device__ LmEpi(const Params& p, const TileShape&, uint8_t* smem)
-      : P(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt) {}
+      : P(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt), u_cand(p.t_cand * p.t_cand) {}
   __device__ void init(int tid, int nthr) {
     if (tsm) tt = screen_to_smem(P.tt, tsm, tid, nthr);
   }
@@ -74,8 +75,8 @@ struct LmEpi {
     }
   }
   // t^2 = df r / (1 - r), r = gty^2 / (gtg yty)  (hit_from_gty algebra),
-  // screened in FP32 without branches; printed statistics come from the
-  // FP64 refinement.
+  // screened in FP32 without branches and without t itself; printed
+  // statistics come from the FP64 refinement.
   template <int NACC>
   __device__ void chunk(int c, const float (&v)[NACC][16]) {
     const int64_t s0 = snp0 + c;
@@ -90,10 +91,10 @@ struct LmEpi {
       const float num = v[0][j] * gs;
       const float r = num * num * ig * inv_yty;
       const float omr = 1.0f - r;
-      const float t = (ig > 0.0f && omr > 0.0f) ? copysignf(sqrtf(P.df * __fdividef(r, omr)), num) : 0.0f;
-      const ScreenOut o = acat_screen(t, tt);
+      const float u = (ig > 0.0f && omr > 0.0f) ? P.df * __fdividef(r, omr) : 0.0f;  // t^2
+      const ScreenOut o = acat_screen_u(u, tt);
       acc.add_screen(o, s, valid);
-      if (valid && (fabsf(t) >= P.t_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred, o.tiny);
+      if (valid && (u >= u_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred, o.tiny);
     }
   }
   __device__ void end_tile() {

@@ -39,6 +39,10 @@ struct TTable {
   const float* lt;  // nb + 4 nodes
   float dl_inv;     // nb / (x(t_defer) - x0)
   float t_defer;    // |t| >= t_defer (p <= 1e-14): the term is left to the host
+  // the same thresholds on u = t^2 (the scan epilogues screen t^2 directly)
+  float u0;         // t0^2
+  float u_tiny;     // tiny_t^2
+  float u_defer;    // t_defer^2, rounded down
 };
 
 __device__ __forceinline__ float lagrange4(const float* y, float x, int n_int) {
@@ -118,34 +122,42 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
 
 // What the scan epilogues need of each pair: the ACAT term, whether it
 // enters ACAT on the device, and whether the host takes it over. Same rules
-// as t_tail, without -log10 p: the best SNP is keyed on |t| (p falls with |t|
-// at one df) and deferral for p <= 1e-14 is |t| >= t_defer. One table lookup:
-//   central  tan((1/2 - p) pi) = c1(t^2) / |t|
-//   tail     tan((1/2 - p) pi) = exp(lt(sqrt(log1p(t^2 / df))))
+// as t_tail, without -log10 p, and from u = t^2 alone (no square root per
+// pair): the best SNP is keyed on u (p falls as u grows at one df),
+// deferral for p <= 1e-14 is u >= u_defer, for |t| near 0 0 < u < u_tiny.
+// One table lookup:
+//   central  tan((1/2 - p) pi) = c1(u) / |t| = c1(u) rsqrt(u)
+//   tail     tan((1/2 - p) pi) = exp(lt(sqrt(log1p(u / df))))
 struct ScreenOut {
   double term;    // tan((1/2 - p) pi) when use_acat, else 0
-  float key_t;    // |t| for the best-SNP key (0 for NaN)
+  float key;      // best-SNP score: u for the scans (|t| through acat_screen); 0 for NaN
   bool use_acat;  // p < 1 - 1e-12 and not deferred
   bool deferred;  // p <= 1e-14 or 0 < |t| < tiny_t
   bool tiny;      // deferred because 0 < |t| < tiny_t
 };
 
-__device__ __forceinline__ ScreenOut acat_screen(float t, const TTable& T) {
+__device__ __forceinline__ ScreenOut acat_screen_u(float u, const TTable& T) {
   ScreenOut o;
-  const float at = fabsf(t);
-  const bool nan_t = !(at == at);
-  const bool tiny = at > 0.0f && at < T.tiny_t;
-  o.tiny = !nan_t && tiny;
-  o.deferred = !nan_t && (tiny || at >= T.t_defer);
-  o.use_acat = !nan_t && !o.deferred && at > 0.0f;
-  o.key_t = nan_t ? 0.0f : at;
-  const bool central = at <= T.t0;
-  const float u = at * at;
+  const bool nan_u = !(u == u);
+  const bool tiny = u > 0.0f && u < T.u_tiny;
+  o.tiny = !nan_u && tiny;
+  o.deferred = !nan_u && (tiny || u >= T.u_defer);
+  o.use_acat = !nan_u && !o.deferred && u > 0.0f;
+  o.key = nan_u ? 0.0f : u;
+  const bool central = u <= T.u0;
   const float xs = sqrtf(log1pf(u * T.inv_df));
   const float x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
   const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
-  const float term = central ? __fdividef(y, at) : __expf(y);
+  const float term = central ? y * rsqrtf(u) : __expf(y);
   o.term = o.use_acat ? static_cast<double>(term) : 0.0;
+  return o;
+}
+
+// The screen of one t (the t_tail ABI's screen mode): key = |t|.
+__device__ __forceinline__ ScreenOut acat_screen(float t, const TTable& T) {
+  ScreenOut o = acat_screen_u(t * t, T);
+  const float at = fabsf(t);
+  o.key = at == at ? at : 0.0f;
   return o;
 }
 
