@@ -59,7 +59,7 @@ def grm_case(steps: int) -> dict:
     rot_flops = 2.0 * n * n * m_kept
     peak = pk.get("bf16_tflops", 1590.0)
     return {"workload": "GRM build + eigendecomposition + spectral rotation", "n_samples": n, "n_snps": m,
-            "kept_snps": m_kept, "steps": steps, "decode_ms": decode, "stage_ms": med,
+            "kept_snps": m_kept, "steps": steps, "decode_ms": decode, "stage_ms": med, "stage_ms_steps": t,
             "grm": {"algorithmic_tflops": grm_flops / (med["grm"] / 1e3) / 1e12,
                     "frac_of_bf16_peak": grm_flops / (med["grm"] / 1e3) / 1e12 / peak,
                     "note": "stage time: per-SNP statistics, FP16 operand transpose, tensor-core SYRK "
@@ -93,6 +93,7 @@ def lm_case(steps: int, m: int = 1_000_000, G: int = 20_000) -> dict:
     peak = pk.get("bf16_tflops_sustained", 1400.0)
     return {"workload": "trans/gw LM scan (--model lm --mode gw)", "n_samples": n, "n_snps": m, "n_genes": G,
             "covariates": ncov, "pthr": 1e-5, "steps": steps, "tests_per_step": tests, "stage_ms": med,
+            "stage_ms_steps": t,
             "tests_per_s": tests / (step_ms / 1e3), "pairs": int(len(pairs)),
             "scan": {"algorithmic_tflops": flops / (med["scan"] / 1e3) / 1e12,
                      "frac_of_bf16_sustained": flops / (med["scan"] / 1e3) / 1e12 / peak,
