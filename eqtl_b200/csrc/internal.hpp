@@ -142,7 +142,7 @@ struct Workspace {
   DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, a00L, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
   DevBuf<__half> ops_hi[34], ops_lo[34];  // gene-side operands, one per accumulator (dev::kMaxAcc)
   DevBuf<__half*> ops_ptr;
-  DevBuf<float> unscale, gscale;
+  DevBuf<float> unscale, gscale, inv_gtg_f;
   DevBuf<uint8_t> ok;
   DevBuf<double> graw, gt;
   DevBuf<eqtl_pair> refined;

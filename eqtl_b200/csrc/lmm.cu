@@ -826,6 +826,7 @@ struct LmmEpi {
       acc.add_screen(o, s, valid);
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
+    acc.end_chunk();
   }
   // Both phases at once (the CUDA-core comparator): v in the tile's order.
   template <int NACC>
@@ -1010,6 +1011,7 @@ struct LmmGroupEpi {
       acc.add_screen(o, s, valid);
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
+    acc.end_chunk();
   }
   __device__ void end_tile() {
     if (gvalid) acc.flush(Pr.out, gene);

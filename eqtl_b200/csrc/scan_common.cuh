@@ -39,6 +39,9 @@ struct GeneAcc {
   int used = 0;
   int tested = 0;
   unsigned long long best = ~0ull;
+  // FP32 sum of the ACAT terms of the current chunk of add_screen pairs
+  // (end_chunk folds it into acat)
+  float chunk_acat = 0.0f;
   int chrom = -1;
   int64_t lo = 0, hi = -1;
 
@@ -47,6 +50,7 @@ struct GeneAcc {
     used = 0;
     tested = 0;
     best = ~0ull;
+    chunk_acat = 0.0f;
   }
   __device__ __forceinline__ void load_window(const Windows& w, int g) {
     if (w.mode != kWinNone) {
@@ -77,17 +81,23 @@ struct GeneAcc {
     }
   }
   // The same for the epilogues' ACAT screen (best SNP keyed on the screen's
-  // key, t^2 in the scans).
+  // key, t^2 in the scans). Pairs come in chunks of up to 16 SNPs; the terms
+  // of a chunk are summed in FP32 (the error is ~1e-6 of the chunk's largest
+  // term, below the screen's own) and added to the FP64 total by end_chunk.
   __device__ __forceinline__ void add_screen(const ScreenOut& o, int64_t s, bool valid) {
     if (valid) {
       ++tested;
       if (o.use_acat) {
-        acat += o.term;
+        chunk_acat += o.term;
         ++used;
       }
       const unsigned long long k = best_key(o.key, static_cast<uint32_t>(s));
       best = k < best ? k : best;
     }
+  }
+  __device__ __forceinline__ void end_chunk() {
+    acat += static_cast<double>(chunk_acat);
+    chunk_acat = 0.0f;
   }
   __device__ __forceinline__ void add(const TailOut& o, int64_t s) {
     ++tested;

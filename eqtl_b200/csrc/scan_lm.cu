@@ -34,7 +34,7 @@ struct LmEpiParams {
   int64_t m;
   const double* inv_yty;   // [G] 1 / yty (0 when yty == 0)
   const float* gscale;     // [G] accumulator -> gty factor
-  const double* inv_gtg;   // [m] 1 / gtg (0 marks gtg < 1e-12: p = 1)
+  const float* inv_gtg;    // [m, padded to 16] 1 / gtg in FP32 (0 marks gtg < 1e-12: p = 1)
   const uint8_t* snp_ok;   // [m] subset gate (src/scan_common.cpp:133-151)
   Windows win;
   float df;
@@ -83,11 +83,22 @@ struct LmEpi {
     if (!gvalid || s0 >= P.m) return;
     uint32_t okw[4];
     load_flags16(P.snp_ok + s0, okw);
+    // the 16 SNPs' 1/gtg: s0 is a multiple of 16 and the array is padded
+    float igv[16];
+    const float4* ig4 = reinterpret_cast<const float4*>(P.inv_gtg + s0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 v4 = __ldg(ig4 + q);
+      igv[4 * q] = v4.x;
+      igv[4 * q + 1] = v4.y;
+      igv[4 * q + 2] = v4.z;
+      igv[4 * q + 3] = v4.w;
+    }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int64_t s = s0 + j;
       const bool valid = flag16(okw, j) && s < P.m && acc.in_scope(P.win, s);
-      const float ig = valid ? static_cast<float>(P.inv_gtg[s]) : 0.0f;
+      const float ig = valid ? igv[j] : 0.0f;
       const float num = v[0][j] * gs;
       const float r = num * num * ig * inv_yty;
       const float omr = 1.0f - r;
@@ -96,12 +107,20 @@ struct LmEpi {
       acc.add_screen(o, s, valid);
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(P.out, gene, s, o.deferred, o.tiny);
     }
+    acc.end_chunk();
   }
   __device__ void end_tile() {
     if (gvalid) acc.flush(P.out, gene);
   }
   __device__ void finish() {}
 };
+
+// out[i] = (float) x[i]
+__global__ void to_float_kernel(const double* __restrict__ x, int64_t count, float* out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = static_cast<float>(x[i]);
+}
 
 // ---------------------------------------------------------------- prep
 // One block per gene: yty, power-of-two scale, FP16/BF16 hi/lo rows.
@@ -357,7 +376,16 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   ep.m = m;
   ep.inv_yty = ws.inv_yty.p;
   ep.gscale = ws.gscale.p;
-  ep.inv_gtg = ws.inv_gtg.p;
+  // FP32 copy of 1/gtg, padded to a multiple of 16 (+16) for vector loads
+  ws.inv_gtg_f.alloc(static_cast<size_t>(((m + 15) / 16 + 1) * 16));
+  EQTL_CUDA(cudaMemsetAsync(ws.inv_gtg_f.p, 0, ws.inv_gtg_f.n * sizeof(float), st));
+  if (m > 0) {
+    ++ctx->launches;
+    to_float_kernel<<<static_cast<unsigned>(std::min<int64_t>((m + 255) / 256, 4096)), 256, 0, st>>>(
+        ws.inv_gtg.p, m, ws.inv_gtg_f.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  ep.inv_gtg = ws.inv_gtg_f.p;
   ep.snp_ok = ws.ok.p;
   ep.win = upload_windows(ctx, prm, m, prm->exclude_cis == 2 ? kWinInclude : prm->exclude_cis ? kWinExclude : kWinNone);
   ep.df = static_cast<float>(df);

@@ -129,7 +129,7 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
 //   central  tan((1/2 - p) pi) = c1(u) / |t| = c1(u) rsqrt(u)
 //   tail     tan((1/2 - p) pi) = exp(lt(sqrt(log1p(u / df))))
 struct ScreenOut {
-  double term;    // tan((1/2 - p) pi) when use_acat, else 0
+  float term;     // tan((1/2 - p) pi) when use_acat, else 0
   float key;      // best-SNP score: u for the scans (|t| through acat_screen); 0 for NaN
   bool use_acat;  // p < 1 - 1e-12 and not deferred
   bool deferred;  // p <= 1e-14 or 0 < |t| < tiny_t
@@ -149,7 +149,7 @@ __device__ __forceinline__ ScreenOut acat_screen_u(float u, const TTable& T) {
   const float x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
   const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
   const float term = central ? y * rsqrtf(u) : __expf(y);
-  o.term = o.use_acat ? static_cast<double>(term) : 0.0;
+  o.term = o.use_acat ? term : 0.0f;
   return o;
 }
 
