@@ -77,7 +77,7 @@ def build_cli() -> str:
                                                          os.path.join(CSRC, "tstat.hpp")]
     if _newer(BIN, srcs + headers + [LIB]):
         _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, *srcs, "-o", BIN,
-              "-L" + os.path.dirname(LIB), "-leqtl_cuda", "-Wl,-rpath,$ORIGIN/../lib"])
+              "-L" + os.path.dirname(LIB), "-leqtl_cuda", "-lz", "-Wl,-rpath,$ORIGIN/../lib"])
     return BIN
 
 

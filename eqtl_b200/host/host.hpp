@@ -42,7 +42,7 @@ struct Trace {
 
 // ------------------------------------------------------------------ options
 struct Options {
-  std::string bfile, pheno, out = "eqtl_out", gff, covar, grm, gff_id_key;
+  std::string bfile, vcf, pheno, out = "eqtl_out", gff, covar, grm, gff_id_key;
   bool make_grm = false;
   std::string mode = "all";              // cis | trans | all | gw
   std::vector<std::string> models{"lmm"};
@@ -71,6 +71,19 @@ struct Plink {
   std::vector<uint8_t> rows;                   // .bed payload, SNP-major
 };
 Plink read_plink(const std::string& prefix);
+
+// VCF input (vcf.cpp): GT calls as .bed 2-bit rows (ALT counted) plus what
+// the reference's ploidy-aware filters need.
+struct VcfInfo {
+  std::vector<uint8_t> hap_chrom;               // per record: X, Y or MT (every call carries one allele)
+  std::vector<std::vector<int32_t>> hap_calls;  // per record elsewhere: file columns with a haploid call
+  int64_t n_multi = 0;                          // records skipped as not biallelic
+};
+Plink read_vcf(const std::string& path, VcfInfo& vi);
+// Keeps the records that pass the reference's VCF filters over the analysis
+// samples `cols` (file columns): calls present, missing fraction, ploidy-
+// aware allele frequency not monomorphic, --miss-hand filter, --maf.
+void vcf_filter(Plink& P, const VcfInfo& vi, const std::vector<int32_t>& cols, const Options& opt);
 
 struct Pheno {
   std::vector<std::string> samples, genes;

@@ -1,6 +1,6 @@
 // eqtl: the reference program's command line (src/main.cpp, src/scan.cpp)
-// for PLINK input and the LM / LMM models, with every scan run on the B200
-// through libeqtl_cuda. The orchestration follows run_eqtl_geno
+// for PLINK or VCF (GT) input and the LM / LMM models, with every scan run
+// on the B200 through libeqtl_cuda. The orchestration follows run_eqtl_geno
 // (src/scan.cpp:50-312): analysis samples = phenotype samples present in the
 // .fam, in phenotype order; one GRM (computed or -k) shared by the LMM
 // scopes; per (model, scope) the pairs / top / region files; BH over the
@@ -45,15 +45,33 @@ std::vector<std::string> overlap(const std::vector<std::string>& pheno, const Pl
   return out;
 }
 
+// PLINK or VCF genotypes of the run (-b / -v).
+Plink read_genotypes(const Options& opt, VcfInfo& vi) {
+  return opt.vcf.empty() ? read_plink(opt.bfile) : read_vcf(opt.vcf, vi);
+}
+
+// Options for the device decode: a VCF has been filtered on the host with
+// the reference's VCF rules (vcf_filter), so the device applies none.
+Options device_filters(const Options& opt) {
+  if (opt.vcf.empty()) return opt;
+  Options o = opt;
+  o.max_miss = 1.0;
+  o.miss_filter = false;
+  o.maf = 0.0;
+  return o;
+}
+
 int run_make_grm(const Options& opt) {
-  Plink P = read_plink(opt.bfile);
+  VcfInfo vi;
+  Plink P = read_genotypes(opt, vi);
   std::vector<std::string> samples = P.fam_iid;
   if (!opt.pheno.empty()) {
     samples = overlap(load_pheno(opt.pheno).samples, P);
     if (samples.empty()) die("no overlapping samples for GRM");
   }
+  if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, samples), opt);
   Device dev;
-  Genotypes geno(dev, P, sample_columns(P, samples), opt);
+  Genotypes geno(dev, P, sample_columns(P, samples), device_filters(opt));
   const int n = static_cast<int>(samples.size());
   std::vector<double> K(static_cast<size_t>(n) * n);
   std::vector<int32_t> N(static_cast<size_t>(n) * (n + 1) / 2);
@@ -65,7 +83,8 @@ int run_make_grm(const Options& opt) {
 }
 
 int run_scan(const Options& opt) {
-  Plink P = read_plink(opt.bfile);
+  VcfInfo vi;
+  Plink P = read_genotypes(opt, vi);
   Pheno ph = load_pheno(opt.pheno);
   Study st;
   st.opt = &opt;
@@ -106,8 +125,9 @@ int run_scan(const Options& opt) {
     std::remove(probe.c_str());
   }
 
+  if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, st.samples), opt);
   Device dev;
-  Genotypes geno(dev, P, sample_columns(P, st.samples), opt);
+  Genotypes geno(dev, P, sample_columns(P, st.samples), device_filters(opt));
   st.dev = &dev;
   st.geno = &geno;
   if (std::find(opt.models.begin(), opt.models.end(), "lmm") != opt.models.end()) {

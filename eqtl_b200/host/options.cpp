@@ -1,8 +1,9 @@
 // Command line of the reference program (src/options.cpp:145-179): the same
 // long and short flags, defaults and range checks, for PLINK input and the
-// LM / LMM models. The flags of paths outside the device scan (VCF input,
-// the GLM / GLMM models, --fast, the fission subcommand) are recognised and
-// refused with a message instead of being silently ignored.
+// LM / LMM models, with PLINK (-b) or VCF (-v, GT calls) genotypes. The
+// flags of paths outside the device scan (the GLM / GLMM models, --fast, the
+// fission subcommand) are recognised and refused with a message instead of
+// being silently ignored.
 #include <getopt.h>
 
 #include <cstdlib>
@@ -49,6 +50,7 @@ void print_help() {
                "Usage:   eqtl [options]\n"
                "\n"
                "Input options:\n"
+               "    -v, --vcf FILE         genotypes VCF (GT; plain or bgzip/gzip)\n"
                "    -b, --bfile PREFIX     PLINK bed/bim/fam prefix\n"
                "    -e, --pheno FILE       phenotype matrix (col1=sample)\n"
                "    -g, --gff FILE         GFF3 gene annotation (TSS)\n"
@@ -130,7 +132,7 @@ int parse_options(int argc, char** argv, Options& opt) {
   while ((c = getopt_long(argc, argv, "v:b:e:o:g:c:k:m:w:t:h", long_opts, &idx)) != -1) {
     const std::string a = optarg ? optarg : "";
     switch (c) {
-      case 'v': die("VCF/BCF input is outside the device scan; convert to PLINK .bed (-b)");
+      case 'v': opt.vcf = a; break;
       case 'b': opt.bfile = a; break;
       case 'e': opt.pheno = a; break;
       case 'o': opt.out = a; break;
@@ -192,8 +194,9 @@ int parse_options(int argc, char** argv, Options& opt) {
     std::cout << "eqtl 0.1.0 (eqtl_b200)\n";
     return 2;
   }
-  if (opt.bfile.empty()) {
-    std::cerr << "[E] need -b/--bfile (PLINK input)\n";
+  if (opt.vcf.empty() == opt.bfile.empty()) {
+    if (opt.vcf.empty()) std::cerr << "[E] need exactly one of -v/--vcf or -b/--bfile\n";
+    else std::cerr << "[E] use only one of -v/--vcf or -b/--bfile\n";
     return 1;
   }
   if (!opt.make_grm && opt.pheno.empty()) {

@@ -235,6 +235,29 @@ def make_genes(seed: int, n_genes: int, chroms: Sequence[str], chrom_len: int,
     return ids, gchrom, start, end, strand, tss
 
 
+def write_vcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequence[int], ids: Sequence[str],
+              ref: Sequence[str], alt: Sequence[str], dosage: np.ndarray, haploid: Optional[np.ndarray] = None,
+              phased: bool = False) -> None:
+    """VCF 4.2 with a GT field (gzip-compressed when `path` ends in .gz):
+    dosage [m, n] = ALT allele count (-1 missing); haploid [m, n] marks calls
+    written with one allele ("0", "1", ".")."""
+    import gzip
+    sep = "|" if phased else "/"
+    gt_dip = {0: f"0{sep}0", 1: f"0{sep}1", 2: f"1{sep}1", -1: f".{sep}."}
+    gt_hap = {0: "0", 1: "1", -1: "."}
+    opener = gzip.open if path.endswith(".gz") else open
+    with opener(path, "wt") as f:
+        f.write("##fileformat=VCFv4.2\n")
+        f.write('##FORMAT=<ID=GT,Number=1,Type=String,Description="Genotype">\n')
+        f.write("#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\t" + "\t".join(samples) + "\n")
+        for r in range(len(chrom)):
+            d = dosage[r]
+            h = haploid[r] if haploid is not None else np.zeros(len(d), bool)
+            calls = [gt_hap[int(v)] if hh else gt_dip[int(v)] for v, hh in zip(d, h)]
+            f.write(f"{chrom[r]}\t{int(pos[r])}\t{ids[r] or '.'}\t{ref[r]}\t{alt[r]}\t.\tPASS\t.\tGT\t" +
+                    "\t".join(calls) + "\n")
+
+
 def write_pheno(path: str, samples: Sequence[str], genes: Sequence[str], Y: np.ndarray) -> None:
     with open(path, "w") as f:
         f.write("sample\t" + "\t".join(genes) + "\n")

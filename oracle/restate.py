@@ -82,6 +82,87 @@ def decode_bed_rows(rows: np.ndarray, n_file: int, sample_col: Sequence[int], mi
     return Decoded(keep, codes, dosage, n_miss, af)
 
 
+# ---------------------------------------------------------------------------
+# VCF GT records  (src/vcf_session.cpp:148-157 haploid contigs, :160-290
+# parse_record, :294-305 for_each_snp with pass_maf)
+# ---------------------------------------------------------------------------
+def _vcf_haploid_chrom(chrom: str) -> bool:
+    k = chrom
+    if len(k) > 3 and k[:3].lower() == "chr":
+        k = k[3:]
+    return k in ("X", "x", "Y", "y", "M", "m", "MT", "mt", "Mt")
+
+
+def read_vcf_gt(path: str):
+    """Text VCF (plain or gzip): the biallelic records with a GT field as
+    (chrom, pos, id, ref, alt, dosage[int8, -1 missing], haploid_call[bool]),
+    plus the sample ids and the number of records that were not biallelic."""
+    import gzip
+    opener = gzip.open if open(path, "rb").read(2) == b"\x1f\x8b" else open
+    samples, recs, n_multi = [], [], 0
+    with opener(path, "rt") as f:
+        for line in f:
+            line = line.rstrip("\r\n")
+            if not line:
+                continue
+            if line.startswith("#CHROM"):
+                samples = line.split("\t")[9:]
+                continue
+            if line.startswith("#"):
+                continue
+            fld = line.split("\t")
+            alt = fld[4]
+            if alt == "." or "," in alt:
+                n_multi += 1
+                continue
+            keys = fld[8].split(":")
+            if "GT" not in keys:
+                continue
+            gi = keys.index("GT")
+            dos = np.empty(len(samples), np.int8)
+            hap = np.zeros(len(samples), bool)
+            for i, sf in enumerate(fld[9:9 + len(samples)]):
+                sub = sf.split(":")
+                gt = sub[gi] if gi < len(sub) else "."
+                al = gt.replace("|", "/").split("/")[:2]
+                if al[0] == "." or (len(al) > 1 and al[1] == "."):
+                    dos[i] = -1
+                    continue
+                dos[i] = sum(int(a) for a in al)
+                hap[i] = len(al) == 1
+            recs.append((fld[0], int(fld[1]), "" if fld[2] == "." else fld[2], fld[3], alt, dos, hap))
+    return samples, recs, n_multi
+
+
+def vcf_keep(recs, sample_col: Sequence[int], max_miss: float, miss_filter: bool, maf_min: float) -> np.ndarray:
+    """parse_record's filters over the analysis samples, then pass_maf on the
+    ploidy-aware allele frequency (haploid contigs and haploid calls count one
+    allele per call)."""
+    col = np.asarray(sample_col, dtype=np.int64)
+    keep = np.zeros(len(recs), bool)
+    for r, (chrom, _, _, _, _, dos, hap) in enumerate(recs):
+        d = dos[col]
+        ok = d >= 0
+        n_ok = int(ok.sum())
+        n_miss = len(col) - n_ok
+        if n_ok == 0:
+            continue
+        if n_miss / len(col) > max_miss + 1e-15:
+            continue
+        ploidy = np.where(_vcf_haploid_chrom(chrom) | hap[col], 1.0, 2.0)
+        psum = float(ploidy[ok].sum())
+        af = float(d[ok].sum()) / psum if psum > 0 else 0.0
+        af = min(max(af, 0.0), 1.0)
+        if af < 1e-12 or af > 1.0 - 1e-12:
+            continue
+        if miss_filter and n_miss > 0:
+            continue
+        if not pass_maf(af, maf_min):
+            continue
+        keep[r] = True
+    return keep
+
+
 def read_bed(prefix: str) -> Tuple[np.ndarray, int, list, list]:
     """Reads .fam/.bim/.bed like src/plink_bed.cpp:26-212 (no checks beyond the
     magic bytes). Returns (rows [m, nb], n_file, fam IIDs, bim records)."""

@@ -1,6 +1,9 @@
 """The eqtl host program (eqtl_b200/bin/eqtl) against outputs of the reference
 program itself (tests/golden/): the same command lines, every pairs / top /
-region file and the GCTA GRM files.
+region file and the GCTA GRM files. Each command line runs twice: on the
+golden PLINK files (-b) and on the same genotypes as a VCF (-v; the
+reference's own VCF reader needs htslib, absent here, so the golden outputs
+of the .bed runs are the reference for both).
 
 Tolerances: LM pairs carry the FP64 refinement (log10 p within 1e-5, beta
 within 1e-6 relative); LMM adds the REML optimiser difference (1e-4 and
@@ -18,6 +21,7 @@ import numpy as np
 import pytest
 
 import driver
+import restate as R
 import refargs
 import tsvcmp
 from gpu_util import T_ERR
@@ -37,19 +41,38 @@ def _runs():
     return out
 
 
-def _run(argv, case_dir, out_prefix):
+def bed_to_vcf(prefix: str, out_path: str) -> None:
+    """The same genotypes as a gzip-compressed VCF: ALT = A1 (the counted
+    allele), REF = A2, IDs and positions from the .bim."""
+    from eqtl_b200 import synth
+    rows, n_file, fam, bim = R.read_bed(prefix)
+    i = np.arange(n_file)
+    codes = (rows[:, i // 4] >> (2 * (i % 4))) & 3
+    dosage = np.array([2, -1, 1, 0], np.int8)[codes]
+    synth.write_vcf(out_path, fam, [b[0] for b in bim], [b[3] for b in bim], [b[1] for b in bim],
+                    [b[5] for b in bim], [b[4] for b in bim], dosage)
+
+
+def _run(argv, case_dir, out_prefix, src="bed", tmp=None):
     a = list(argv)
     a[a.index("-o") + 1] = out_prefix
+    if src == "vcf":  # the same genotypes through -v
+        vcf = os.path.join(str(tmp), "geno.vcf.gz")
+        if not os.path.exists(vcf):
+            bed_to_vcf(os.path.join(case_dir, a[a.index("-b") + 1]), vcf)
+        k = a.index("-b")
+        a[k:k + 2] = ["-v", vcf]
     r = subprocess.run([os.path.abspath(BIN)] + a, cwd=case_dir, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("src", ["bed", "vcf"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" in r[2]])
-def test_cli_make_grm(case, tag, argv, tmp_path):
+def test_cli_make_grm(case, tag, argv, src, tmp_path):
     d = os.path.join(GOLD, case)
     out = str(tmp_path / "out")
-    _run(argv, d, out)
+    _run(argv, d, out, src, tmp_path)
     ref = os.path.join(d, f"ref_{tag}")
     assert open(out + ".grm.id").read() == open(ref + ".grm.id").read()
     N, Nr = (np.fromfile(p + ".grm.N.bin", dtype=np.float32) for p in (out, ref))
@@ -59,11 +82,12 @@ def test_cli_make_grm(case, tag, argv, tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("src", ["bed", "vcf"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" not in r[2]])
-def test_cli_scan_matches_reference(case, tag, argv, tmp_path):
+def test_cli_scan_matches_reference(case, tag, argv, src, tmp_path):
     d = os.path.join(GOLD, case)
     out = str(tmp_path / "out")
-    _run(argv, d, out)
+    _run(argv, d, out, src, tmp_path)
     opt = refargs.options_from_argv(argv, d)
     ora = driver.Scanner(opt)
     ora.run()                                    # per-gene ACAT sensitivities
