@@ -256,6 +256,8 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   if (m > 0)
     EQTL_CUDA(cudaMemcpyAsync(g.bed.p, rows, static_cast<size_t>(m * bytes_per_snp), cudaMemcpyHostToDevice, st));
   g.col.upload(sample_col, n, st);
+  g.col_identity = true;
+  for (int i = 0; i < n; ++i) g.col_identity = g.col_identity && sample_col[i] == i;
   g.n_miss.alloc(m);
   g.s1.alloc(m);
   g.s2.alloc(m);
@@ -291,8 +293,7 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   const int stage = static_cast<int>(((bytes_per_snp + 30) / 16) * 16);
   if (g.m > 0 && stage <= kExpandMaxStage) {
     const int smem = stage * kExpandWarps + kExpandWarps * 16 * static_cast<int>(sizeof(uint2));
-    int identity = 1;
-    for (int i = 0; i < n; ++i) identity &= sample_col[i] == i;
+    const int identity = g.col_identity ? 1 : 0;
     const unsigned blocks = static_cast<unsigned>(
         std::min<int64_t>((g.m + kExpandWarps - 1) / kExpandWarps, static_cast<int64_t>(ctx->sm_count) * 16));
     ++ctx->launches;

@@ -43,49 +43,114 @@ __global__ void grm_snp_kernel(const int64_t* __restrict__ kept, int64_t m, int 
   inv_sd[r] = ok ? 1.0 / sd : 0.0;
 }
 
-// Zt[i, c] for GRM column c (= used SNP c): 32 x 32 tiles through smem so
-// both the bed reads (per SNP row) and the writes (per sample row) coalesce.
-__global__ void grm_transpose_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                     int n, const int64_t* __restrict__ used_rows, int64_t m_used, int64_t m_pad,
-                                     const double* __restrict__ mean, const double* __restrict__ inv_sd, __half* zh,
-                                     __half* zl, __half* mk) {
-  __shared__ float tz[32][33];
-  __shared__ float tm[32][33];
-  const int64_t c0 = static_cast<int64_t>(blockIdx.x) * 32;
-  const int i0 = blockIdx.y * 32;
-  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-  const int i = i0 + tx;
-  const int ci = i < n ? __ldg(col + i) : 0;
-  for (int r = ty; r < 32; r += 8) {
-    const int64_t c = c0 + r;
-    float z = 0.0f, mm = 0.0f;
-    if (c < m_used && i < n) {
-      const int64_t s = used_rows[c];
-      const int code = bed_code_g(bed + s * bps, ci);
-      if (code < 0) {
-        mm = 1.0f;
+// GRM operands Z[i, r] (FP16 hi/lo) and the missing mask M[i, r] for every
+// kept SNP r (rows = analysis samples, columns = SNPs, m_pad columns). SNPs
+// that the GRM does not use (use[r] = 0) and the padding columns are zero in
+// all three, so they add nothing to the sums or the missing-pair counts.
+// A block covers 64 SNPs x kTrS samples: the packed rows (the whole row, or
+// with the identity sample map just the bytes of these samples) are staged in
+// shared memory with 16-byte loads, each SNP's three code values are formed
+// once with the arithmetic of one element ((code - mean) * inv_sd in FP64,
+// rounded to FP32, split into FP16 hi + lo), and each lane writes 8 SNPs of one
+// sample per step with 16-byte stores (128 contiguous bytes per output row).
+constexpr int kTrSnps = 64;
+constexpr int kTrS = 1024;
+
+__global__ void __launch_bounds__(256)
+    grm_operands_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                        int identity, int n, const int64_t* __restrict__ kept, int64_t m, int64_t m_pad,
+                        const uint8_t* __restrict__ use, const double* __restrict__ mean,
+                        const double* __restrict__ inv_sd, int stride, __half* zh, __half* zl, __half* mk) {
+  extern __shared__ __align__(16) uint8_t tr_smem[];
+  uint64_t* lut = reinterpret_cast<uint64_t*>(tr_smem);           // [64][4]: zh | zl << 16 | mk << 32
+  int* skew = reinterpret_cast<int*>(lut + kTrSnps * 4);            // [64]
+  uint8_t* rows = tr_smem + kTrSnps * 4 * sizeof(uint64_t) + kTrSnps * sizeof(int);  // [64][stride]
+  const int64_t r0 = static_cast<int64_t>(blockIdx.x) * kTrSnps;
+  const int i0 = blockIdx.y * kTrS;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // bytes staged per row: the samples' window (identity map) or the whole row
+  const int64_t b0 = identity ? (i0 >> 2) : 0;
+  const int64_t nbytes = identity ? (bps - b0 < kTrS / 4 ? bps - b0 : kTrS / 4) : bps;
+  // per-SNP code values
+  if (threadIdx.x < kTrSnps * 4) {
+    const int rr = threadIdx.x >> 2, code = threadIdx.x & 3;
+    const int64_t r = r0 + rr;
+    uint64_t e = 0;  // unused SNPs and padding columns: z 0, no mask
+    if (r < m && use[r]) {
+      if (code == 1) {
+        e = static_cast<uint64_t>(__half_as_ushort(__float2half_rn(1.0f))) << 32;  // missing: z 0, mask 1
       } else {
-        z = static_cast<float>((static_cast<double>(code) - mean[c]) * inv_sd[c]);
+        const int c = code == 0 ? 2 : (code == 2 ? 1 : 0);
+        const float z = static_cast<float>((static_cast<double>(c) - mean[r]) * inv_sd[r]);
+        const __half h = __float2half_rn(z);
+        const __half l = __float2half_rn(z - __half2float(h));
+        e = static_cast<uint64_t>(__half_as_ushort(h)) | (static_cast<uint64_t>(__half_as_ushort(l)) << 16);
       }
     }
-    tz[r][tx] = z;
-    tm[r][tx] = mm;
+    lut[rr * 4 + code] = e;
+  }
+  // stage the packed rows: warp w takes rows w, w + 8, ...
+  for (int rr = warp; rr < kTrSnps; rr += 8) {
+    const int64_t r = r0 + rr;
+    if (r >= m) continue;
+    const int64_t off0 = __ldg(kept + r) * bps + b0;
+    const int64_t a0 = off0 & ~int64_t(15);
+    const int sk = static_cast<int>(off0 - a0);
+    const int nvec = static_cast<int>((sk + nbytes + 15) / 16);
+    const uint4* src = reinterpret_cast<const uint4*>(bed + a0);
+    // 4-byte stores: the row stride is an odd number of words, so the 8 rows
+    // a lane reads and the lanes' row groups spread over the banks
+    uint32_t* dst = reinterpret_cast<uint32_t*>(rows + rr * stride);
+    for (int v = lane; v < nvec; v += 32) {
+      const uint4 x = __ldg(src + v);
+      dst[4 * v] = x.x;
+      dst[4 * v + 1] = x.y;
+      dst[4 * v + 2] = x.z;
+      dst[4 * v + 3] = x.w;
+    }
+    if (lane == 0) skew[rr] = sk;
   }
   __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    const int ii = i0 + r;
-    const int64_t c = c0 + tx;
-    if (ii < n && c < m_pad) {
-      const float z = tz[tx][r];
-      // recompute in FP64 for the split: z itself came from FP64 above, and
-      // FP32 keeps 24 bits, more than hi+lo FP16 carry
-      const __half h = __float2half_rn(z);
-      const __half l = __float2half_rn(z - __half2float(h));
-      zh[static_cast<int64_t>(ii) * m_pad + c] = h;
-      zl[static_cast<int64_t>(ii) * m_pad + c] = l;
-      mk[static_cast<int64_t>(ii) * m_pad + c] = __float2half_rn(tm[tx][r]);
+  // lane: SNP group q = lane % 8 (8 SNPs), sample i = base + lane / 8
+  const int q = lane & 7;
+  for (int ib = i0 + warp * 4; ib < i0 + kTrS; ib += 32) {
+    const int i = ib + (lane >> 3);
+    if (i >= n) continue;
+    const int c = identity ? i : __ldg(col + i);
+    const int64_t byte = (c >> 2) - b0;
+    const int sh = (c & 3) * 2;
+    uint32_t hw[4], lw[4], mw[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      uint64_t e[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int rr = q * 8 + j + t;
+        e[t] = 0;
+        if (r0 + rr < m) {
+          const uint32_t code = (static_cast<uint32_t>(rows[rr * stride + skew[rr] + byte]) >> sh) & 3u;
+          e[t] = lut[rr * 4 + code];
+        }
+      }
+      hw[j / 2] = static_cast<uint32_t>(e[0] & 0xFFFFu) | (static_cast<uint32_t>(e[1] & 0xFFFFu) << 16);
+      lw[j / 2] = static_cast<uint32_t>((e[0] >> 16) & 0xFFFFu) | (static_cast<uint32_t>((e[1] >> 16) & 0xFFFFu) << 16);
+      mw[j / 2] = static_cast<uint32_t>((e[0] >> 32) & 0xFFFFu) | (static_cast<uint32_t>((e[1] >> 32) & 0xFFFFu) << 16);
     }
+    const int64_t o = static_cast<int64_t>(i) * m_pad + r0 + q * 8;
+    *reinterpret_cast<uint4*>(zh + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(zl + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    *reinterpret_cast<uint4*>(mk + o) = make_uint4(mw[0], mw[1], mw[2], mw[3]);
   }
+}
+
+// *m_used = number of SNPs with use[r] set
+__global__ void grm_count_kernel(const uint8_t* __restrict__ use, int64_t m, unsigned long long* m_used) {
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < m;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    c += use[r];
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(m_used, c);
 }
 
 struct GrmEpiParams {
@@ -123,10 +188,12 @@ struct GrmEpi {
   __device__ void finish() {}
 };
 
-__global__ void grm_finalize_kernel(int n, int64_t m_used, const double* __restrict__ A, const int* __restrict__ J,
-                                    double* K, int32_t* Npk) {
+__global__ void grm_finalize_kernel(int n, const unsigned long long* __restrict__ m_used_p,
+                                    const double* __restrict__ A, const int* __restrict__ J, double* K,
+                                    int32_t* Npk) {
   const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (e >= static_cast<int64_t>(n) * n) return;
+  const int64_t m_used = static_cast<int64_t>(*m_used_p);
   const int i = static_cast<int>(e / n), j = static_cast<int>(e - static_cast<int64_t>(i) * n);
   // the sums exist for i >= j (lower triangle); K is their mirror image above
   const int64_t lo_e = static_cast<int64_t>(i >= j ? i : j) * n + (i >= j ? j : i);
@@ -155,6 +222,7 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   cudaStream_t st = ctx->stream;
   const int n = g.n;
   const int64_t m = g.m;
+  EQTL_CHECK(m > 0, EQTL_E_ARG, "no SNPs for GRM");
   StageScope timer(ctx, EQTL_STAGE_GRM);
   Workspace& ws = ctx->ws;
   DevBuf<uint8_t>& use = ws.grm_use;
@@ -169,29 +237,17 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
                                                                            use.p, mean.p, inv_sd.p);
     EQTL_CUDA(cudaGetLastError());
   }
-  std::vector<uint8_t> use_h(m);
-  use.download(use_h.data(), m, st);
-  std::vector<double> mean_h(m), isd_h(m);
-  mean.download(mean_h.data(), m, st);
-  inv_sd.download(isd_h.data(), m, st);
-  EQTL_CUDA(cudaStreamSynchronize(st));
-  std::vector<int64_t> rows;
-  std::vector<double> mean_u, isd_u;
-  for (int64_t r = 0; r < m; ++r)
-    if (use_h[r]) {
-      rows.push_back(g.kept_h[r]);
-      mean_u.push_back(mean_h[r]);
-      isd_u.push_back(isd_h[r]);
-    }
-  const int64_t mu_n = static_cast<int64_t>(rows.size());
-  EQTL_CHECK(mu_n > 0, EQTL_E_ARG, "no SNPs for GRM");
-  const int64_t m_pad = ((mu_n + 63) / 64) * 64;
-  DevBuf<int64_t>& drows = ws.grm_rows;
-  DevBuf<double>& dmean = ws.grm_mean_u;
-  DevBuf<double>& disd = ws.grm_isd_u;
-  drows.upload(rows.data(), rows.size(), st);
-  dmean.upload(mean_u.data(), mean_u.size(), st);
-  disd.upload(isd_u.data(), isd_u.size(), st);
+  // every kept SNP is a column; the ones the GRM does not use are zero
+  const int64_t m_pad = ((m + 63) / 64) * 64;
+  DevBuf<unsigned long long>& cnt = ws.grm_count;
+  cnt.alloc(1);
+  cnt.zero(st);
+  if (m > 0) {
+    ++ctx->launches;
+    grm_count_kernel<<<static_cast<unsigned>(std::min<int64_t>((m + 255) / 256, 1184)), 256, 0, st>>>(use.p, m,
+                                                                                                      cnt.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
   DevBuf<__half>& zh = ws.grm_zh;
   DevBuf<__half>& zl = ws.grm_zl;
   DevBuf<__half>& mk = ws.grm_mk;
@@ -200,10 +256,19 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   zl.alloc(elems);
   mk.alloc(elems);
   {
-    dim3 grid(static_cast<unsigned>(m_pad / 32), static_cast<unsigned>((n + 31) / 32));
+    const int64_t nbytes = g.col_identity ? std::min<int64_t>(kTrS / 4, g.bytes_per_snp) : g.bytes_per_snp;
+    int stride = static_cast<int>(((nbytes + 30 + 3) / 4) * 4);
+    if ((stride / 4) % 2 == 0) stride += 4;  // an odd number of words
+    const int smem = kTrSnps * 4 * static_cast<int>(sizeof(uint64_t)) + kTrSnps * static_cast<int>(sizeof(int)) +
+                     kTrSnps * stride;
+    EQTL_CHECK(smem <= 200 * 1024, EQTL_E_UNSUPPORTED,
+               "grm: more than ~12,000 samples in the file with a non-identity sample map");
+    EQTL_CUDA(cudaFuncSetAttribute(grm_operands_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    dim3 grid(static_cast<unsigned>(m_pad / kTrSnps), static_cast<unsigned>((n + kTrS - 1) / kTrS));
     ++ctx->launches;
-    grm_transpose_kernel<<<grid, dim3(32, 8), 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, drows.p, mu_n, m_pad,
-                                                        dmean.p, disd.p, zh.p, zl.p, mk.p);
+    grm_operands_kernel<<<grid, 256, smem, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.col_identity ? 1 : 0, n,
+                                                 g.kept.p, m, m_pad, use.p, mean.p, inv_sd.p, stride, zh.p, zl.p,
+                                                 mk.p);
     EQTL_CUDA(cudaGetLastError());
   }
   DevBuf<double>& A = ws.grm_A;
@@ -235,10 +300,13 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   Npk.alloc(static_cast<size_t>(n) * (n + 1) / 2);
   const int64_t tot = static_cast<int64_t>(n) * n;
   ++ctx->launches;
-  grm_finalize_kernel<<<static_cast<unsigned>((tot + 255) / 256), 256, 0, st>>>(n, mu_n, A.p, J.p, K.p, Npk.p);
+  grm_finalize_kernel<<<static_cast<unsigned>((tot + 255) / 256), 256, 0, st>>>(n, cnt.p, A.p, J.p, K.p, Npk.p);
   EQTL_CUDA(cudaGetLastError());
+  unsigned long long mu_n = 0;
+  cnt.download(&mu_n, 1, st);
   EQTL_CUDA(cudaStreamSynchronize(st));
-  return mu_n;
+  EQTL_CHECK(mu_n > 0, EQTL_E_ARG, "no SNPs for GRM");
+  return static_cast<int64_t>(mu_n);
 }
 
 }  // namespace eqtl
@@ -346,7 +414,8 @@ __global__ void grm_na_stats_kernel(const uint8_t* __restrict__ bed, int64_t bps
 }
 
 // Zt[i, c] of the pass (row stride kNaChunk), zero for unused columns:
-// 32 x 32 tiles through shared memory like grm_transpose_kernel.
+// 32 x 32 tiles through shared memory, so that both the .bed reads and the
+// operand writes coalesce.
 __global__ void grm_na_transpose_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
                                         int n, int64_t r0, const uint8_t* __restrict__ use,
                                         const double* __restrict__ mean, const double* __restrict__ inv_sd,

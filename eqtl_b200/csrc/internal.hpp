@@ -109,6 +109,7 @@ struct Geno {
   int k_pad = 0;          // n rounded up to a multiple of 64
   DevBuf<uint8_t> bed;    // [m_all, bytes_per_snp]
   DevBuf<int32_t> col;    // [n] .fam column per analysis sample
+  bool col_identity = false;  // col[i] == i for every analysis sample
   DevBuf<int32_t> n_miss; // [m_all]
   DevBuf<int32_t> s1;     // [m_all] sum of non-missing A1 counts
   DevBuf<int32_t> s2;     // [m_all] sum of squares
@@ -169,9 +170,9 @@ struct Workspace {
   double tt_df = -1;
   // GRM operands and accumulators, eigen-solver scratch
   DevBuf<uint8_t> grm_use;
-  DevBuf<double> grm_mean, grm_isd, grm_mean_u, grm_isd_u, grm_A, eig_work;
-  DevBuf<int64_t> grm_rows;
+  DevBuf<double> grm_mean, grm_isd, grm_A, eig_work;
   DevBuf<int2> grm_tiles;  // lower-triangle tile list of the GRM contraction
+  DevBuf<unsigned long long> grm_count;  // SNPs the GRM uses
   DevBuf<__half> grm_zh, grm_zl, grm_mk;
   DevBuf<int> grm_J, eig_info;
 };
