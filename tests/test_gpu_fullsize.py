@@ -1,6 +1,7 @@
-"""Parity at the benchmark's full size (trans/gw LMM, n = 2,000, m = 500,000
-SNPs, 10,000 genes, the bench's synthetic workload), through properties that
-do not depend on size, since the oracle cannot run 5e9 tests:
+"""Parity at the benchmark shapes' full size (trans/gw LMM: n = 2,000,
+m = 500,000 SNPs, 10,000 genes, the bench's synthetic workload; trans/gw LM:
+n = 1,000, m = 1,000,000, 20,000 genes, 10 covariates), through properties
+that do not depend on size, since the oracle cannot run 5e9 or 2e10 tests:
 
 - every gene is tested on the same set of SNPs (gw scope: all SNPs that pass
   the subset gate), no more than the kept SNPs;
@@ -71,3 +72,40 @@ def test_trans_lmm_full_size_properties():
         st = R.test_lmm_many(prep, dec.dosage[k:k + 1])
         assert abs(dev["beta"][k] - st["beta"][0]) <= 1e-6 * abs(st["beta"][0]) + 1e-12, (k, dev[k], st["beta"][0])
         assert abs(np.log10(dev["p"][k]) - np.log10(st["p"][0])) <= 1e-6, (k, dev["p"][k], st["p"][0])
+
+
+@pytest.mark.gpu
+def test_trans_lm_full_size_properties():
+    """The trans/gw LM at its benchmark shape: n = 1,000, m = 1,000,000 SNPs,
+    20,000 genes with Y ~ N(0, 1), intercept + 10 covariates (2e10 tests)."""
+    from eqtl_b200 import capi, synth
+    n, m, G = 1000, 1_000_000, 20_000
+    rows, _, _ = synth.make_bed_rows_chunked(20261203, n, m, maf_lo=0.01, maf_hi=0.5, miss_rate=0.01)
+    rng = np.random.default_rng(20261204)
+    Y = rng.standard_normal((n, G))
+    X = np.column_stack([np.ones(n), rng.standard_normal((n, 10))])
+    pthr = 1e-5
+    with capi.Context(0) as c:
+        keep, _, _ = c.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        c.pheno_load(Y, X)
+        genes, pairs, _ = c.scan_trans_lm(None, None, pthr=pthr)
+        kept_rows = np.nonzero(keep)[0]
+        nt = genes["n_tested"]
+        assert np.all(nt == nt[0]) and 0 < nt[0] <= kept_rows.size
+        assert pairs.size > 0 and np.all(pairs["p"] <= pthr)
+        # about pthr of the tests under the null
+        assert 0.5 * pthr * nt.sum() < pairs.size < 1.5 * pthr * nt.sum()
+        rng = np.random.default_rng(6)
+        sel = rng.choice(pairs.size, size=min(2000, pairs.size), replace=False)
+        again, _ = c.test_pairs("lm", Y, X, pairs["gene"][sel], pairs["snp"][sel])
+        for f in ("beta", "se", "t"):
+            np.testing.assert_allclose(again[f], pairs[f][sel], rtol=1e-12, atol=0)
+        rep = pairs[rng.choice(pairs.size, size=200, replace=False)]
+        cols = np.concatenate([rep["gene"], rng.integers(0, G, 200)]).astype(np.int64)
+        snps = np.concatenate([rep["snp"], rng.integers(0, nt[0], 200)]).astype(np.int64)
+        dev, _ = c.test_pairs("lm", Y, X, cols, snps)
+    dec = R.decode_bed_rows(rows[kept_rows[snps]], n, np.arange(n), "impute", 0.8, 0.0)
+    for k in range(cols.size):
+        st = R.test_lm_many(R.prep_lm(Y[:, int(cols[k])], X), dec.dosage[k:k + 1])
+        assert abs(dev["beta"][k] - st["beta"][0]) <= 1e-9 * abs(st["beta"][0]) + 1e-13, (k, dev[k], st["beta"][0])
+        assert abs(np.log10(dev["p"][k]) - np.log10(st["p"][0])) <= 1e-8, (k, dev["p"][k], st["p"][0])
