@@ -25,7 +25,7 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
-           "eqtl_test_pairs"]
+           "eqtl_test_pairs", "eqtl_geno_load_dosage"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -74,6 +74,7 @@ def load() -> C.CDLL:
         lib.eqtl_set_precision.argtypes = [vp, C.c_int]
         lib.eqtl_geno_load_bed.argtypes = [vp, vp, i64, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp,
                                            C.POINTER(i64)]
+        lib.eqtl_geno_load_dosage.argtypes = [vp, vp, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp, vp]
         lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
         lib.eqtl_geno_dosage_rows.argtypes = [vp, vp, i64, vp]
         lib.eqtl_test_pairs.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64, vp, vp]
@@ -152,6 +153,23 @@ class Context:
         self._check(self.lib.eqtl_geno_load_bed(self.h, _ptr(rows), m, rows.shape[1] if m else (n_file + 3) // 4,
                                                 n_file, _ptr(col), col.size, miss_hand, max_miss, maf_min,
                                                 _ptr(keep), _ptr(af), _ptr(nm), C.byref(nk)))
+        self.n_kept = nk.value
+        self.n = col.size
+        return keep.astype(bool), af, nm
+
+    def load_dosage(self, ds: np.ndarray, sample_col, miss_hand: int = MISS_IMPUTE, max_miss: float = 0.8,
+                    maf_min: float = 0.0):
+        """FP32 dosage rows [m, n_file] (NaN = missing call) instead of .bed rows."""
+        ds = np.ascontiguousarray(ds, dtype=np.float32)
+        col = np.ascontiguousarray(sample_col, dtype=np.int32)
+        m, n_file = ds.shape
+        keep = np.zeros(m, np.uint8)
+        af = np.zeros(m, np.float64)
+        nm = np.zeros(m, np.int32)
+        nk = C.c_int64()
+        self._check(self.lib.eqtl_geno_load_dosage(self.h, _ptr(ds), m, n_file, _ptr(col), col.size, miss_hand,
+                                                   max_miss, maf_min, _ptr(keep), _ptr(af), _ptr(nm),
+                                                   C.byref(nk)))
         self.n_kept = nk.value
         self.n = col.size
         return keep.astype(bool), af, nm

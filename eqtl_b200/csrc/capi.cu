@@ -631,6 +631,23 @@ int eqtl_geno_load_bed(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t by
   });
 }
 
+int eqtl_geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int32_t n_file, const int32_t* sample_col,
+                          int32_t n, int32_t miss_hand, double max_miss, double maf_min, uint8_t* keep_out,
+                          double* af_out, int32_t* n_miss_out, int64_t* n_kept_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK((ds || m == 0) && sample_col, EQTL_E_ARG, "null input");
+    eqtl::geno_load_dosage(ctx, ds, m, n_file, sample_col, n, miss_hand, max_miss, maf_min);
+    const eqtl::Geno& g = ctx->geno;
+    if (keep_out) {
+      std::fill(keep_out, keep_out + m, 0);
+      for (int64_t s : g.kept_h) keep_out[s] = 1;
+    }
+    if (af_out) std::copy(g.af_h.begin(), g.af_h.end(), af_out);
+    if (n_miss_out) std::copy(g.n_miss_h.begin(), g.n_miss_h.end(), n_miss_out);
+    if (n_kept_out) *n_kept_out = g.m;
+  });
+}
+
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
   return guarded(ctx, [&] {
     EQTL_CHECK(out || hi == lo, EQTL_E_ARG, "null output");

@@ -11,6 +11,10 @@
 //     gc[s, i] = (dosage[s, i] - mu_s) * 64,   missing -> 0,
 // (centring leaves every statistic unchanged because the covariates always
 // contain an intercept; it removes the mean from the split).
+//
+// The same decode serves FP32 dosage rows (a VCF's FORMAT/DS values, or GT
+// counts, per sample; src/vcf_session.cpp:193-258): a value that is not
+// finite is a missing call, every other value is used as it is.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -20,29 +24,24 @@
 namespace eqtl {
 namespace {
 
-__device__ __forceinline__ int bed_code(const uint8_t* row, int col) {
-  const uint32_t b = __ldg(row + (col >> 2));
-  const uint32_t pair = (b >> ((col & 3) * 2)) & 3u;
-  // LUT {2, -1, 1, 0} packed as bytes
-  return static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
-}
-
-__global__ void bed_stats_kernel(const uint8_t* __restrict__ bed, int64_t m, int64_t bps,
-                                 const int32_t* __restrict__ col, int n, int miss_hand, double max_miss,
-                                 double maf_min, int32_t* n_miss, int32_t* s1, int32_t* s2, uint8_t* pass,
-                                 double* af, double* mu) {
+// Per-SNP statistics and filters, one warp per row. With 2-bit rows the sums
+// are integers (exact in FP64 in any order); with FP32 dosage rows they are
+// FP64 sums of the dosages.
+__global__ void bed_stats_kernel(GenoRows src, int64_t m, const int32_t* __restrict__ col, int n, int miss_hand,
+                                 double max_miss, double maf_min, int32_t* n_miss, double* s1, double* s2,
+                                 uint8_t* pass, double* af, double* mu) {
   const int lane = threadIdx.x & 31;
   const int64_t snp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (snp >= m) return;
-  const uint8_t* row = bed + snp * bps;
-  int nm = 0, a = 0, b = 0;
+  int nm = 0;
+  double a = 0.0, b = 0.0;
   for (int i = lane; i < n; i += 32) {
-    const int c = bed_code(row, __ldg(col + i));
-    if (c < 0) {
+    const double d = src.dosage(snp, __ldg(col + i));
+    if (isnan(d)) {
       ++nm;
     } else {
-      a += c;
-      b += c * c;
+      a += d;
+      b += d * d;
     }
   }
 #pragma unroll
@@ -54,7 +53,7 @@ __global__ void bed_stats_kernel(const uint8_t* __restrict__ bed, int64_t m, int
   if (lane) return;
   const int n_ok = n - nm;
   bool keep = n_ok > 0;
-  const double sum = static_cast<double>(a);
+  const double sum = a;
   double m_imp = 0.0, f = 0.0;
   if (n_ok > 0) {
     m_imp = sum / n_ok;
@@ -88,10 +87,12 @@ __device__ __forceinline__ __nv_bfloat16 to16<__nv_bfloat16>(double v) {
 __device__ __forceinline__ double from16(__half h) { return static_cast<double>(__half2float(h)); }
 __device__ __forceinline__ double from16(__nv_bfloat16 h) { return static_cast<double>(__bfloat162float(h)); }
 
+// One thread per (sample, kept SNP): the general expansion (FP32 dosage rows,
+// or 2-bit rows too long to stage).
 template <class T>
-__global__ void bed_expand_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                  int n, int k_pad, const int64_t* __restrict__ kept, int64_t m_kept,
-                                  const double* __restrict__ mu, float scale, T* hi, T* lo) {
+__global__ void bed_expand_kernel(GenoRows src, const int32_t* __restrict__ col, int n, int k_pad,
+                                  const int64_t* __restrict__ kept, int64_t m_kept, const double* __restrict__ mu,
+                                  float scale, T* hi, T* lo) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= k_pad) return;
   const int c_col = k < n ? __ldg(col + k) : 0;
@@ -99,8 +100,8 @@ __global__ void bed_expand_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
     const int64_t s = __ldg(kept + r);
     double v = 0.0;
     if (k < n) {
-      const int c = bed_code(bed + s * bps, c_col);
-      v = c < 0 ? 0.0 : (static_cast<double>(c) - __ldg(mu + s));
+      const double d = src.dosage(s, c_col);
+      v = isnan(d) ? 0.0 : (d - __ldg(mu + s));
     }
     v *= static_cast<double>(scale);
     const T h = to16<T>(v);
@@ -205,8 +206,8 @@ __global__ void __launch_bounds__(32 * kExpandWarps, 4)
   }
 }
 
-__global__ void bed_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                  int n, const int64_t* __restrict__ kept, int64_t lo, int64_t hi,
+__global__ void bed_dosage_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                  const int64_t* __restrict__ kept, int64_t lo, int64_t hi,
                                   const double* __restrict__ mu, double* out) {
   const int64_t total = (hi - lo) * n;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
@@ -214,13 +215,13 @@ __global__ void bed_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
     const int64_t r = e / n;
     const int i = static_cast<int>(e - r * n);
     const int64_t s = kept[lo + r];
-    const int c = bed_code(bed + s * bps, col[i]);
-    out[e] = c < 0 ? mu[s] : static_cast<double>(c);
+    const double d = src.dosage(s, col[i]);
+    out[e] = isnan(d) ? mu[s] : d;
   }
 }
 
-__global__ void bed_dosage_rows_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                       int n, const int64_t* __restrict__ kept, const int64_t* __restrict__ rows,
+__global__ void bed_dosage_rows_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                       const int64_t* __restrict__ kept, const int64_t* __restrict__ rows,
                                        int64_t k, const double* __restrict__ mu, double* out) {
   const int64_t total = k * n;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
@@ -228,33 +229,30 @@ __global__ void bed_dosage_rows_kernel(const uint8_t* __restrict__ bed, int64_t 
     const int64_t r = e / n;
     const int i = static_cast<int>(e - r * n);
     const int64_t s = kept[rows[r]];
-    const int c = bed_code(bed + s * bps, col[i]);
-    out[e] = c < 0 ? mu[s] : static_cast<double>(c);
+    const double d = src.dosage(s, col[i]);
+    out[e] = isnan(d) ? mu[s] : d;
   }
 }
 
 }  // namespace
 
-void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
-               const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min) {
-  EQTL_CHECK(m >= 0 && n > 0 && n_file > 0, EQTL_E_ARG, "geno_load: bad sizes");
-  EQTL_CHECK(bytes_per_snp == (n_file + 3) / 4, EQTL_E_ARG, "geno_load: bytes_per_snp != ceil(n_file/4)");
+namespace {
+
+void check_samples(const int32_t* sample_col, int n, int n_file, int miss_hand) {
   for (int i = 0; i < n; ++i)
     EQTL_CHECK(sample_col[i] >= 0 && sample_col[i] < n_file, EQTL_E_ARG, "geno_load: sample_col out of range");
   EQTL_CHECK(miss_hand == EQTL_MISS_FILTER || miss_hand == EQTL_MISS_IMPUTE, EQTL_E_ARG, "geno_load: miss_hand");
+}
+
+// Shared part of both loads, after the rows are on the device: per-SNP
+// statistics and filters, the kept list, and the centred FP16 hi/lo operand.
+void geno_decode(eqtl_ctx* ctx, const int32_t* sample_col, int miss_hand, double max_miss, double maf_min) {
   Geno& g = ctx->geno;
   cudaStream_t st = ctx->stream;
+  const int64_t m = g.m_all;
+  const int n = g.n;
   ctx->rot.m = 0;  // rotated genotypes belong to the previous genotypes
-  g.m_all = m;
-  g.n = n;
-  g.n_file = n_file;
-  g.bytes_per_snp = bytes_per_snp;
   g.k_pad = ((n + 63) / 64) * 64;
-  // kBedPad bytes past the last row: bed_expand_warp_kernel stages rows in
-  // 16-byte vectors from the boundary at or below each row start
-  g.bed.alloc(static_cast<size_t>(m * bytes_per_snp + kBedPad));
-  if (m > 0)
-    EQTL_CUDA(cudaMemcpyAsync(g.bed.p, rows, static_cast<size_t>(m * bytes_per_snp), cudaMemcpyHostToDevice, st));
   g.col.upload(sample_col, n, st);
   g.col_identity = true;
   for (int i = 0; i < n; ++i) g.col_identity = g.col_identity && sample_col[i] == i;
@@ -264,13 +262,13 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   g.pass.alloc(m);
   g.af.alloc(m);
   g.mu.alloc(m);
+  const GenoRows src = g.rows();
   StageScope timer(ctx, EQTL_STAGE_DECODE);
   if (m > 0) {
     ++ctx->launches;
     const int per_block = 8;
     bed_stats_kernel<<<static_cast<unsigned>((m + per_block - 1) / per_block), 32 * per_block, 0, st>>>(
-        g.bed.p, m, bytes_per_snp, g.col.p, n, miss_hand, max_miss, maf_min, g.n_miss.p, g.s1.p, g.s2.p, g.pass.p,
-        g.af.p, g.mu.p);
+        src, m, g.col.p, n, miss_hand, max_miss, maf_min, g.n_miss.p, g.s1.p, g.s2.p, g.pass.p, g.af.p, g.mu.p);
     EQTL_CUDA(cudaGetLastError());
   }
   std::vector<uint8_t> pass(m);
@@ -290,8 +288,9 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
   const size_t elems = static_cast<size_t>(g.m) * g.k_pad;
   g.gc_hi.alloc(elems);
   g.gc_lo.alloc(elems);
+  const int64_t bytes_per_snp = g.bytes_per_snp;
   const int stage = static_cast<int>(((bytes_per_snp + 30) / 16) * 16);
-  if (g.m > 0 && stage <= kExpandMaxStage) {
+  if (g.m > 0 && !g.dense && stage <= kExpandMaxStage) {
     const int smem = stage * kExpandWarps + kExpandWarps * 16 * static_cast<int>(sizeof(uint2));
     const int identity = g.col_identity ? 1 : 0;
     const unsigned blocks = static_cast<unsigned>(
@@ -312,20 +311,57 @@ void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_
     }
     EQTL_CUDA(cudaGetLastError());
   } else if (g.m > 0) {
-    // rows too long to stage (more than ~49,000 samples in the file)
+    // FP32 dosage rows, or 2-bit rows too long to stage (more than ~49,000
+    // samples in the file)
     dim3 grid((g.k_pad + 255) / 256, static_cast<unsigned>(g.m < 65535 ? g.m : 65535));
     ++ctx->launches;
     if (ctx->precision == EQTL_PREC_SPLIT_BF16) {
       bed_expand_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
-          g.bed.p, bytes_per_snp, g.col.p, n, g.k_pad, g.kept.p, g.m, g.mu.p, kGcScale,
-          reinterpret_cast<__nv_bfloat16*>(g.gc_hi.p), reinterpret_cast<__nv_bfloat16*>(g.gc_lo.p));
+          src, g.col.p, n, g.k_pad, g.kept.p, g.m, g.mu.p, kGcScale, reinterpret_cast<__nv_bfloat16*>(g.gc_hi.p),
+          reinterpret_cast<__nv_bfloat16*>(g.gc_lo.p));
     } else {
-      bed_expand_kernel<__half><<<grid, 256, 0, st>>>(g.bed.p, bytes_per_snp, g.col.p, n, g.k_pad, g.kept.p,
-                                                       g.m, g.mu.p, kGcScale, g.gc_hi.p, g.gc_lo.p);
+      bed_expand_kernel<__half><<<grid, 256, 0, st>>>(src, g.col.p, n, g.k_pad, g.kept.p, g.m, g.mu.p, kGcScale,
+                                                       g.gc_hi.p, g.gc_lo.p);
     }
     EQTL_CUDA(cudaGetLastError());
   }
   EQTL_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+
+void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
+               const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min) {
+  EQTL_CHECK(m >= 0 && n > 0 && n_file > 0, EQTL_E_ARG, "geno_load: bad sizes");
+  EQTL_CHECK(bytes_per_snp == (n_file + 3) / 4, EQTL_E_ARG, "geno_load: bytes_per_snp != ceil(n_file/4)");
+  check_samples(sample_col, n, n_file, miss_hand);
+  Geno& g = ctx->geno;
+  cudaStream_t st = ctx->stream;
+  g.m_all = m;
+  g.n = n;
+  g.n_file = n_file;
+  g.bytes_per_snp = bytes_per_snp;
+  g.dense = false;
+  // kBedPad bytes past the last row: bed_expand_warp_kernel stages rows in
+  // 16-byte vectors from the boundary at or below each row start
+  g.bed.alloc(static_cast<size_t>(m * bytes_per_snp + kBedPad));
+  if (m > 0)
+    EQTL_CUDA(cudaMemcpyAsync(g.bed.p, rows, static_cast<size_t>(m * bytes_per_snp), cudaMemcpyHostToDevice, st));
+  geno_decode(ctx, sample_col, miss_hand, max_miss, maf_min);
+}
+
+void geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int n_file, const int32_t* sample_col, int n,
+                      int miss_hand, double max_miss, double maf_min) {
+  EQTL_CHECK(m >= 0 && n > 0 && n_file > 0, EQTL_E_ARG, "geno_load_dosage: bad sizes");
+  check_samples(sample_col, n, n_file, miss_hand);
+  Geno& g = ctx->geno;
+  g.m_all = m;
+  g.n = n;
+  g.n_file = n_file;
+  g.bytes_per_snp = (n_file + 3) / 4;
+  g.dense = true;
+  g.ds.upload(ds, static_cast<size_t>(m) * n_file, ctx->stream);
+  geno_decode(ctx, sample_col, miss_hand, max_miss, maf_min);
 }
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {
@@ -335,8 +371,7 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {
   DevBuf<double> d;
   d.alloc(static_cast<size_t>(hi - lo) * g.n);
   ++ctx->launches;
-  bed_dosage_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, lo, hi,
-                                                   g.mu.p, d.p);
+  bed_dosage_kernel<<<1184, 256, 0, ctx->stream>>>(g.rows(), g.col.p, g.n, g.kept.p, lo, hi, g.mu.p, d.p);
   EQTL_CUDA(cudaGetLastError());
   d.download(out_host, d.n, ctx->stream);
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -352,8 +387,8 @@ void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out
   d_rows.upload(rows, k, ctx->stream);
   d.alloc(static_cast<size_t>(k) * g.n);
   ++ctx->launches;
-  bed_dosage_rows_kernel<<<1184, 256, 0, ctx->stream>>>(g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.kept.p, d_rows.p,
-                                                        k, g.mu.p, d.p);
+  bed_dosage_rows_kernel<<<1184, 256, 0, ctx->stream>>>(g.rows(), g.col.p, g.n, g.kept.p, d_rows.p, k, g.mu.p,
+                                                        d.p);
   EQTL_CUDA(cudaGetLastError());
   d.download(out_host, d.n, ctx->stream);
   EQTL_CUDA(cudaStreamSynchronize(ctx->stream));

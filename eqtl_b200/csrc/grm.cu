@@ -28,12 +28,12 @@ __device__ __forceinline__ int bed_code_g(const uint8_t* row, int col) {
 
 // per kept SNP: GRM usability, mean and 1/sd
 __global__ void grm_snp_kernel(const int64_t* __restrict__ kept, int64_t m, int n, const double* __restrict__ mu,
-                               const int32_t* __restrict__ n_miss, const int32_t* __restrict__ s1, uint8_t* use,
+                               const int32_t* __restrict__ n_miss, const double* __restrict__ s1, uint8_t* use,
                                double* mean, double* inv_sd) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= m) return;
   const int64_t s = kept[r];
-  const double mean_v = (static_cast<double>(s1[s]) + n_miss[s] * mu[s]) / n;
+  const double mean_v = (s1[s] + n_miss[s] * mu[s]) / n;
   const double p = mean_v / 2.0;
   bool ok = !(p < 1e-8 || p > 1.0 - 1e-8);
   const double sd = sqrt(2.0 * p * (1.0 - p));
@@ -141,6 +141,51 @@ __global__ void __launch_bounds__(256)
     *reinterpret_cast<uint4*>(zl + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     *reinterpret_cast<uint4*>(mk + o) = make_uint4(mw[0], mw[1], mw[2], mw[3]);
   }
+}
+
+// The same operands from FP32 dosage rows: z = (d - mean) * inv_sd in FP64,
+// rounded to FP32 and split into FP16 hi + lo; z 0 and mask 1 at a missing
+// call. Block: 64 SNPs x 32 samples; warp w takes SNPs r0 + 8w .. r0 + 8w + 7
+// of sample i = 32 * blockIdx.y + lane, so each dosage row is read 32
+// consecutive samples at a time, and writes them with one 16-byte store per
+// operand.
+__global__ void __launch_bounds__(256)
+    grm_operands_dense_kernel(GenoRows src, const int32_t* __restrict__ col, int n, const int64_t* __restrict__ kept,
+                              int64_t m, int64_t m_pad, const uint8_t* __restrict__ use,
+                              const double* __restrict__ mean, const double* __restrict__ inv_sd, __half* zh,
+                              __half* zl, __half* mk) {
+  const int i = blockIdx.y * 32 + (threadIdx.x & 31);
+  if (i >= n) return;
+  const int64_t rb = static_cast<int64_t>(blockIdx.x) * kTrSnps + (threadIdx.x >> 5) * 8;
+  const int c = __ldg(col + i);
+  uint32_t hw[4], lw[4], mw[4];
+#pragma unroll
+  for (int j = 0; j < 8; j += 2) {
+    uint32_t h2[2] = {0, 0}, l2[2] = {0, 0}, m2[2] = {0, 0};
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int64_t r = rb + j + t;
+      if (r < m && use[r]) {
+        const double d = src.dosage(__ldg(kept + r), c);
+        if (isnan(d)) {
+          m2[t] = __half_as_ushort(__float2half_rn(1.0f));
+        } else {
+          const float z = static_cast<float>((d - mean[r]) * inv_sd[r]);
+          const __half h = __float2half_rn(z);
+          const __half l = __float2half_rn(z - __half2float(h));
+          h2[t] = __half_as_ushort(h);
+          l2[t] = __half_as_ushort(l);
+        }
+      }
+    }
+    hw[j / 2] = h2[0] | (h2[1] << 16);
+    lw[j / 2] = l2[0] | (l2[1] << 16);
+    mw[j / 2] = m2[0] | (m2[1] << 16);
+  }
+  const int64_t o = static_cast<int64_t>(i) * m_pad + rb;
+  *reinterpret_cast<uint4*>(zh + o) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4*>(zl + o) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+  *reinterpret_cast<uint4*>(mk + o) = make_uint4(mw[0], mw[1], mw[2], mw[3]);
 }
 
 // *m_used = number of SNPs with use[r] set
@@ -255,7 +300,13 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   zh.alloc(elems);
   zl.alloc(elems);
   mk.alloc(elems);
-  {
+  if (g.dense) {
+    dim3 grid(static_cast<unsigned>(m_pad / kTrSnps), static_cast<unsigned>((n + 31) / 32));
+    ++ctx->launches;
+    grm_operands_dense_kernel<<<grid, 256, 0, st>>>(g.rows(), g.col.p, n, g.kept.p, m, m_pad, use.p, mean.p,
+                                                    inv_sd.p, zh.p, zl.p, mk.p);
+    EQTL_CUDA(cudaGetLastError());
+  } else {
     const int64_t nbytes = g.col_identity ? std::min<int64_t>(kTrS / 4, g.bytes_per_snp) : g.bytes_per_snp;
     int stride = static_cast<int>(((nbytes + 30 + 3) / 4) * 4);
     if ((stride / 4) % 2 == 0) stride += 4;  // an odd number of words

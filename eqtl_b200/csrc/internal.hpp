@@ -99,7 +99,31 @@ struct DevBuf {
   }
 };
 
-// Decoded genotypes resident on the device (one .bed load).
+// Device view of the uploaded genotype rows, in one of two forms: PLINK
+// 2-bit SNP-major rows (bed, bps bytes each; 00 -> 2 A1 alleles, 10 -> 1,
+// 11 -> 0, 01 -> missing) or FP32 dosage rows (ds, ld values each, the ALT
+// dosage of a VCF's FORMAT/DS or GT; a value that is not finite is missing).
+// dosage() is the dosage of file column c of row s, NaN when missing.
+struct GenoRows {
+  const uint8_t* bed = nullptr;
+  int64_t bps = 0;
+  const float* ds = nullptr;
+  int64_t ld = 0;
+#ifdef __CUDACC__
+  __device__ __forceinline__ double dosage(int64_t s, int c) const {
+    if (ds) {
+      const float v = __ldg(ds + s * ld + c);
+      return isfinite(v) ? static_cast<double>(v) : __longlong_as_double(0x7ff8000000000000LL);
+    }
+    const uint32_t b = __ldg(bed + s * bps + (c >> 2));
+    const uint32_t pair = (b >> ((c & 3) * 2)) & 3u;
+    return pair == 1u ? __longlong_as_double(0x7ff8000000000000LL)
+                      : static_cast<double>((0x00010002u >> (pair * 8)) & 0xFFu);
+  }
+#endif
+};
+
+// Decoded genotypes resident on the device (one .bed or dosage load).
 struct Geno {
   int64_t m_all = 0;      // SNP rows uploaded
   int64_t m = 0;          // SNPs kept by decode (rows of every SNP-side operand)
@@ -107,12 +131,14 @@ struct Geno {
   int n_file = 0;         // .fam samples
   int64_t bytes_per_snp = 0;
   int k_pad = 0;          // n rounded up to a multiple of 64
-  DevBuf<uint8_t> bed;    // [m_all, bytes_per_snp]
+  DevBuf<uint8_t> bed;    // [m_all, bytes_per_snp] (2-bit rows)
+  bool dense = false;     // rows are FP32 dosages in ds instead of bed
+  DevBuf<float> ds;       // [m_all, n_file] FP32 dosages (dense rows)
   DevBuf<int32_t> col;    // [n] .fam column per analysis sample
   bool col_identity = false;  // col[i] == i for every analysis sample
   DevBuf<int32_t> n_miss; // [m_all]
-  DevBuf<int32_t> s1;     // [m_all] sum of non-missing A1 counts
-  DevBuf<int32_t> s2;     // [m_all] sum of squares
+  DevBuf<double> s1;      // [m_all] sum of the non-missing dosages
+  DevBuf<double> s2;      // [m_all] sum of their squares
   DevBuf<uint8_t> pass;   // [m_all]
   DevBuf<double> af;      // [m_all]
   DevBuf<double> mu;      // [m_all] imputation mean
@@ -121,6 +147,17 @@ struct Geno {
   std::vector<int64_t> kept_h;
   std::vector<double> mu_h, af_h;
   std::vector<int32_t> n_miss_h;
+  GenoRows rows() const {
+    GenoRows r;
+    if (dense) {
+      r.ds = ds.p;
+      r.ld = n_file;
+    } else {
+      r.bed = bed.p;
+      r.bps = bytes_per_snp;
+    }
+    return r;
+  }
 };
 
 // Rotated genotypes for the LMM scans: Gt = Q^T (g - mean), Gt^2, hi/lo.
@@ -222,6 +259,8 @@ constexpr float kGcScale = 64.0f;
 // -- geno.cu
 void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
                const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min);
+void geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int n_file, const int32_t* sample_col, int n,
+                      int miss_hand, double max_miss, double maf_min);
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
 void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host);

@@ -1021,15 +1021,15 @@ struct LmmGroupEpi {
 
 // subset gate for the LMM scan (src/scan_common.cpp:133-151)
 __global__ void snp_gate_kernel(const int64_t* __restrict__ kept, int64_t m, int n, const double* __restrict__ mu,
-                                const int32_t* __restrict__ n_miss, const int32_t* __restrict__ s1,
-                                const int32_t* __restrict__ s2, uint8_t* ok) {
+                                const int32_t* __restrict__ n_miss, const double* __restrict__ s1,
+                                const double* __restrict__ s2, uint8_t* ok) {
   const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (r >= m) return;
   const int64_t s = kept[r];
   const double mus = mu[s];
   const int k = n_miss[s];
-  const double sum = static_cast<double>(s1[s]) + k * mus;
-  const double sum2 = static_cast<double>(s2[s]) + k * mus * mus;
+  const double sum = s1[s] + k * mus;
+  const double sum2 = s2[s] + k * mus * mus;
   double af = (sum / n) / 2.0;
   af = fmin(fmax(af, 0.0), 1.0);
   const double maf = af > 0.5 ? 1.0 - af : af;
@@ -1038,8 +1038,8 @@ __global__ void snp_gate_kernel(const int64_t* __restrict__ kept, int64_t m, int
 }
 
 // raw dosages of listed kept SNPs, column-major [n, u]
-__global__ void raw_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                  int n, const int64_t* __restrict__ kept, const double* __restrict__ mu,
+__global__ void raw_dosage_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                  const int64_t* __restrict__ kept, const double* __restrict__ mu,
                                   const int* __restrict__ snps, int u, double* out) {
   const int64_t tot = static_cast<int64_t>(u) * n;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < tot;
@@ -1047,10 +1047,8 @@ __global__ void raw_dosage_kernel(const uint8_t* __restrict__ bed, int64_t bps, 
     const int c = static_cast<int>(e / n);
     const int i = static_cast<int>(e - static_cast<int64_t>(c) * n);
     const int64_t s = kept[snps[c]];
-    const uint32_t b = __ldg(bed + s * bps + (col[i] >> 2));
-    const uint32_t pair = (b >> ((col[i] & 3) * 2)) & 3u;
-    const int code = static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
-    out[e] = code < 0 ? mu[s] : static_cast<double>(code);
+    const double d = src.dosage(s, col[i]);
+    out[e] = isnan(d) ? mu[s] : d;
   }
 }
 
@@ -1121,8 +1119,7 @@ __global__ void lmm_wr_kernel(const double* __restrict__ Ytil, const double* __r
   }
 }
 
-__global__ void lmm_tiny_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                int n, int k_pad, const int64_t* __restrict__ kept, const double* __restrict__ mu,
+__global__ void lmm_tiny_kernel(GenoRows src, const int32_t* __restrict__ col, int n, int k_pad, const int64_t* __restrict__ kept, const double* __restrict__ mu,
                                 const double* __restrict__ U, const __half* __restrict__ gt_hi,
                                 const __half* __restrict__ gt_lo, double inv_s1, const double* __restrict__ Xtil,
                                 int p, const double* __restrict__ lam, const double* __restrict__ delta,
@@ -1134,7 +1131,6 @@ __global__ void lmm_tiny_kernel(const uint8_t* __restrict__ bed, int64_t bps, co
   const int g = pairs[w].x;
   const int64_t r = pairs[w].y;
   const int64_t s = kept[r];
-  const uint8_t* row = bed + s * bps;
   const double mus = mu[s];
   const double* u = U + static_cast<int64_t>(g) * n;
   const __half* gh = gt_hi + r * k_pad;
@@ -1143,10 +1139,8 @@ __global__ void lmm_tiny_kernel(const uint8_t* __restrict__ bed, int64_t bps, co
   double num = 0, gg = 0, a[kMaxPLmm];
   for (int k = 0; k < p; ++k) a[k] = 0;
   for (int i = lane; i < n; i += 32) {
-    const uint32_t b = __ldg(row + (col[i] >> 2));
-    const uint32_t pr = (b >> ((col[i] & 3) * 2)) & 3u;
-    const int code = static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pr * 8)) & 0xFFu));
-    num += (code < 0 ? mus : static_cast<double>(code)) * u[i];
+    const double dose = src.dosage(s, col[i]);
+    num += (isnan(dose) ? mus : dose) * u[i];
     double v = d * lam[i] + 1.0;
     if (v < 1e-12) v = 1e-12;
     const double gt = (static_cast<double>(__half2float(gh[i])) + static_cast<double>(__half2float(gl[i]))) * inv_s1;
@@ -1557,7 +1551,7 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
     graw.alloc(static_cast<size_t>(n) * u);
     gt.alloc(static_cast<size_t>(n) * u);
     ctx->launches += 2;
-    raw_dosage_kernel<<<1184, 256, 0, st>>>(g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, dsn.p, u, graw.p);
+    raw_dosage_kernel<<<1184, 256, 0, st>>>(g.rows(), g.col.p, n, g.kept.p, g.mu.p, dsn.p, u, graw.p);
     EQTL_CUDA(cudaGetLastError());
     const double one = 1.0, zero = 0.0;
     EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_T, CUBLAS_OP_N, n, u, n, &one, ctx->basis.Q.p, n, graw.p, n, &zero,
@@ -1601,7 +1595,7 @@ static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std
   ws.ref_pairs.upload(tiny.data(), tiny.size(), st);
   ws.tiny_p.alloc(tiny.size());
   lmm_tiny_kernel<<<static_cast<unsigned>((tiny.size() + 7) / 8), 256, 0, st>>>(
-      g.bed.p, g.bytes_per_snp, g.col.p, n, R.k_pad, g.kept.p, g.mu.p, ws.gt.p, R.gt_hi.p, R.gt_lo.p, 1.0 / s1,
+      g.rows(), g.col.p, n, R.k_pad, g.kept.p, g.mu.p, ws.gt.p, R.gt_hi.p, R.gt_lo.p, 1.0 / s1,
       ws.Xtil.p, p, ctx->basis.lambda.p, ws.delta.p, ws.ainv.p, ws.rss.p, df, ws.ref_pairs.p,
       static_cast<int>(tiny.size()), ws.tiny_p.p);
   EQTL_CUDA(cudaGetLastError());

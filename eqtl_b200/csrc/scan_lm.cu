@@ -184,35 +184,28 @@ __global__ void gene_split_kernel(const double* __restrict__ Ys, int n, int k_pa
   }
 }
 
-__device__ __forceinline__ int bed_code_dev(const uint8_t* row, int col) {
-  const uint32_t b = __ldg(row + (col >> 2));
-  const uint32_t pair = (b >> ((col & 3) * 2)) & 3u;
-  return static_cast<int>(static_cast<int8_t>((0x0001FF02u >> (pair * 8)) & 0xFFu));
-}
-
 constexpr int kMaxP = 32;
 
 // One warp per kept SNP: FP64 |g_s|^2 with the exact decoded dosage, and the
 // subset gate on the analysis samples.
-__global__ void snp_gtg_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                               int n, const int64_t* __restrict__ kept, int64_t m, const double* __restrict__ mu,
-                               const int32_t* __restrict__ n_miss, const int32_t* __restrict__ s1,
-                               const int32_t* __restrict__ s2, const double* __restrict__ X, int p,
+__global__ void snp_gtg_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                               const int64_t* __restrict__ kept, int64_t m, const double* __restrict__ mu,
+                               const int32_t* __restrict__ n_miss, const double* __restrict__ s1,
+                               const double* __restrict__ s2, const double* __restrict__ X, int p,
                                const double* __restrict__ XtXinv, double* gtg_out, double* inv_gtg, uint8_t* ok,
                                double* af_sub) {
   const int lane = threadIdx.x & 31;
   const int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= m) return;
   const int64_t s = kept[r];
-  const uint8_t* row = bed + s * bps;
   const double mus = mu[s];
   double gg = 0;
   double v[kMaxP];
 #pragma unroll
   for (int k = 0; k < kMaxP; ++k) v[k] = 0;
   for (int i = lane; i < n; i += 32) {
-    const int c = bed_code_dev(row, __ldg(col + i));
-    const double gc = c < 0 ? 0.0 : static_cast<double>(c) - mus;
+    const double d = src.dosage(s, __ldg(col + i));
+    const double gc = isnan(d) ? 0.0 : d - mus;
     gg += gc * gc;
 #pragma unroll
     for (int k = 0; k < kMaxP; ++k)
@@ -236,8 +229,8 @@ __global__ void snp_gtg_kernel(const uint8_t* __restrict__ bed, int64_t bps, con
   inv_gtg[r] = gtg < 1e-12 ? 0.0 : 1.0 / gtg;
   // subset_maf_or_nan on the imputed vector: sum = s1 + k mu, sum2 = s2 + k mu^2
   const int k = n_miss[s];
-  const double sum = static_cast<double>(s1[s]) + k * mus;
-  const double sum2 = static_cast<double>(s2[s]) + k * mus * mus;
+  const double sum = s1[s] + k * mus;
+  const double sum2 = s2[s] + k * mus * mus;
   double af = (sum / n) / 2.0;
   af = fmin(fmax(af, 0.0), 1.0);
   const double maf = af > 0.5 ? 1.0 - af : af;
@@ -249,8 +242,8 @@ __global__ void snp_gtg_kernel(const uint8_t* __restrict__ bed, int64_t bps, con
 // One warp per pair: FP64 gty = sum_i (g_i - mu) y_s[i] (y_s sums to zero).
 // One warp per (gene, snp) pair: gty from the exact decoded dosage in FP64,
 // then the pair's printed statistics (hit_from_gty, src/scan_trans_lm.cpp:21-36).
-__global__ void lm_refine_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                 int n, const int64_t* __restrict__ kept, const double* __restrict__ mu,
+__global__ void lm_refine_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                 const int64_t* __restrict__ kept, const double* __restrict__ mu,
                                  const double* __restrict__ Ys, const double* __restrict__ gtg,
                                  const double* __restrict__ yty, double df, const int2* __restrict__ pairs,
                                  int n_pairs, eqtl_pair* out) {
@@ -259,13 +252,12 @@ __global__ void lm_refine_kernel(const uint8_t* __restrict__ bed, int64_t bps, c
   if (w >= n_pairs) return;
   const int2 pr = pairs[w];
   const int64_t s = kept[pr.y];
-  const uint8_t* row = bed + s * bps;
   const double mus = mu[s];
   const double* y = Ys + static_cast<int64_t>(pr.x) * n;
   double acc = 0;
   for (int i = lane; i < n; i += 32) {
-    const int c = bed_code_dev(row, __ldg(col + i));
-    const double gc = c < 0 ? 0.0 : static_cast<double>(c) - mus;
+    const double d = src.dosage(s, __ldg(col + i));
+    const double gc = isnan(d) ? 0.0 : d - mus;
     acc += gc * y[i];
   }
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -301,7 +293,7 @@ static std::vector<eqtl_pair> lm_refine_pairs(eqtl_ctx* ctx, double df, const st
     ws.refined.alloc(todo.size());
     ++ctx->launches;
     lm_refine_kernel<<<static_cast<unsigned>((todo.size() + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, g.mu.p, ws.Ys.p, ws.gtg.p, ws.yty.p, df, ws.ref_pairs.p,
+        g.rows(), g.col.p, n, g.kept.p, g.mu.p, ws.Ys.p, ws.gtg.p, ws.yty.p, df, ws.ref_pairs.p,
         static_cast<int>(todo.size()), ws.refined.p);
     EQTL_CUDA(cudaGetLastError());
     ws.refined.download(refined.data(), todo.size(), st);
@@ -363,7 +355,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   if (m > 0) {
     ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
         ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
     EQTL_CUDA(cudaGetLastError());
   }
@@ -469,7 +461,7 @@ void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   if (m > 0) {
     ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
         ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
     EQTL_CUDA(cudaGetLastError());
   }

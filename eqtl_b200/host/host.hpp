@@ -69,11 +69,15 @@ struct Plink {
   int n_file = 0;
   int64_t bytes_per_snp = 0;
   std::vector<uint8_t> rows;                   // .bed payload, SNP-major
+  bool dense = false;                          // dosage rows in ds instead of rows (VCF with DS)
+  std::vector<float> ds;                       // [m][n_file] ALT dosages, NaN = missing call
 };
 Plink read_plink(const std::string& prefix);
 
-// VCF input (vcf.cpp): GT calls as .bed 2-bit rows (ALT counted) plus what
-// the reference's ploidy-aware filters need.
+// VCF input (vcf.cpp): GT calls as .bed 2-bit rows (ALT counted), or, when
+// the header defines an ID "DS", FP32 dosage rows taken from FORMAT/DS where
+// a record carries it and from GT elsewhere; plus what the reference's
+// ploidy-aware filters need.
 struct VcfInfo {
   std::vector<uint8_t> hap_chrom;               // per record: X, Y or MT (every call carries one allele)
   std::vector<std::vector<int32_t>> hap_calls;  // per record elsewhere: file columns with a haploid call
@@ -84,6 +88,9 @@ Plink read_vcf(const std::string& path, VcfInfo& vi);
 // samples `cols` (file columns): calls present, missing fraction, ploidy-
 // aware allele frequency not monomorphic, --miss-hand filter, --maf.
 void vcf_filter(Plink& P, const VcfInfo& vi, const std::vector<int32_t>& cols, const Options& opt);
+// True when <path>.tbi or <path>.csi is a tabix / CSI index (its magic bytes
+// after decompression); the index content itself is not used.
+bool vcf_has_index(const std::string& path);
 
 struct Pheno {
   std::vector<std::string> samples, genes;

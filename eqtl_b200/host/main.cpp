@@ -1,5 +1,5 @@
 // eqtl: the reference program's command line (src/main.cpp, src/scan.cpp)
-// for PLINK or VCF (GT) input and the LM / LMM models, with every scan run
+// for PLINK or VCF (GT or DS) input and the LM / LMM models, with every scan run
 // on the B200 through libeqtl_cuda. The orchestration follows run_eqtl_geno
 // (src/scan.cpp:50-312): analysis samples = phenotype samples present in the
 // .fam, in phenotype order; one GRM (computed or -k) shared by the LMM
@@ -124,6 +124,11 @@ int run_scan(const Options& opt) {
     std::fclose(f);
     std::remove(probe.c_str());
   }
+  // a cis scan of a VCF needs its index, as the reference's region queries do
+  // (src/scan.cpp:92-98); the records themselves are read in file order
+  if (!opt.vcf.empty() && std::find(scopes.begin(), scopes.end(), "cis") != scopes.end() &&
+      !vcf_has_index(opt.vcf))
+    die("cis mode requires an indexed genotype file; for VCF run: tabix -p vcf <file>.vcf.gz");
 
   if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, st.samples), opt);
   Device dev;

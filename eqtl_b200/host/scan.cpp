@@ -26,10 +26,15 @@ Genotypes::Genotypes(const Device& d, const Plink& P, const std::vector<int32_t>
   std::vector<double> af(m);
   std::vector<int32_t> nm(m);
   int64_t n_kept = 0;
-  dev.check(eqtl_geno_load_bed(dev.ctx, P.rows.data(), m, P.bytes_per_snp, P.n_file, sample_col.data(), n,
-                               opt.miss_filter ? EQTL_MISS_FILTER : EQTL_MISS_IMPUTE, opt.max_miss, opt.maf,
-                               keep.data(), af.data(), nm.data(), &n_kept),
-            "genotype decode");
+  const int miss_hand = opt.miss_filter ? EQTL_MISS_FILTER : EQTL_MISS_IMPUTE;
+  if (P.dense)
+    dev.check(eqtl_geno_load_dosage(dev.ctx, P.ds.data(), m, P.n_file, sample_col.data(), n, miss_hand,
+                                    opt.max_miss, opt.maf, keep.data(), af.data(), nm.data(), &n_kept),
+              "genotype decode");
+  else
+    dev.check(eqtl_geno_load_bed(dev.ctx, P.rows.data(), m, P.bytes_per_snp, P.n_file, sample_col.data(), n,
+                                 miss_hand, opt.max_miss, opt.maf, keep.data(), af.data(), nm.data(), &n_kept),
+              "genotype decode");
   for (int64_t s = 0; s < m; ++s)
     if (keep[s]) kept.push_back(s);
   info("genotypes: " + std::to_string(n_kept) + "/" + std::to_string(m) + " SNPs kept on " + std::to_string(n) +

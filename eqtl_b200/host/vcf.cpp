@@ -16,7 +16,10 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <limits>
 
 #include "host.hpp"
 
@@ -24,6 +27,13 @@ namespace eqtl_host {
 
 namespace {
 
+// A header that defines the ID "DS" (INFO, FORMAT or FILTER) switches the
+// reader to dosage rows (src/vcf_session.cpp:66-68): a record whose FORMAT
+// carries DS, declared Type=Float, gives each sample's first DS value as its
+// dosage (".", an absent subfield or a value that is not a finite number is
+// missing; the value is used as it is, as an FP32 number); any other record
+// gives its GT counts (:193-258). Both kinds then share the FP32 rows.
+//
 // Line reader over gzread (which also reads uncompressed files as they are).
 struct GzLines {
   gzFile f = nullptr;
@@ -99,6 +109,53 @@ int parse_gt(const char* s, size_t len, bool& haploid) {
   return d;
 }
 
+// [begin, end) of the k-th ':'-separated subfield of a sample column, or
+// false when the column has fewer subfields.
+bool subfield(const char* s, size_t len, int k, size_t& p0, size_t& p1) {
+  p0 = 0;
+  for (int j = 0; j < k; ++j) {
+    const void* c = p0 < len ? std::memchr(s + p0, ':', len - p0) : nullptr;
+    if (!c) return false;
+    p0 = static_cast<const char*>(c) - s + 1;
+  }
+  p1 = p0;
+  while (p1 < len && s[p1] != ':') ++p1;
+  return true;
+}
+
+// The ID of a ##INFO / ##FORMAT / ##FILTER header line, and its Type.
+void header_id(const std::string& line, std::string& id, std::string& type) {
+  id.clear();
+  type.clear();
+  const size_t lt = line.find('<');
+  if (lt == std::string::npos) return;
+  // the key=value pairs before any quoted text (Description="...")
+  const std::string body = line.substr(lt + 1, line.find('"') == std::string::npos ? std::string::npos
+                                                                                     : line.find('"') - lt - 1);
+  size_t a = 0;
+  while (a < body.size()) {
+    size_t e = body.find_first_of(",>", a);
+    if (e == std::string::npos) e = body.size();
+    const std::string kv = body.substr(a, e - a);
+    if (kv.compare(0, 3, "ID=") == 0) id = kv.substr(3);
+    if (kv.compare(0, 5, "Type=") == 0) type = kv.substr(5);
+    a = e + 1;
+  }
+}
+
+// One DS value: the first number of the subfield, NaN when missing.
+float parse_ds(const char* s, size_t len) {
+  if (len == 0 || (len == 1 && s[0] == '.')) return std::numeric_limits<float>::quiet_NaN();
+  std::string t(s, len);
+  const size_t comma = t.find(',');
+  if (comma != std::string::npos) t.resize(comma);
+  char* end = nullptr;
+  const double v = std::strtod(t.c_str(), &end);
+  if (end == t.c_str()) return std::numeric_limits<float>::quiet_NaN();
+  const float f = static_cast<float>(v);
+  return std::isfinite(f) ? f : std::numeric_limits<float>::quiet_NaN();
+}
+
 }  // namespace
 
 Plink read_vcf(const std::string& path, VcfInfo& vi) {
@@ -112,9 +169,19 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
   std::vector<const char*> fld;
   std::vector<size_t> flen;
   int64_t n_rec = 0;
+  bool prefer_ds = false, ds_float = false, said_ds = false;
   do {
     if (line.empty()) continue;
     if (line[0] == '#') {
+      const bool fmt_line = line.compare(0, 10, "##FORMAT=<") == 0;
+      if (fmt_line || line.compare(0, 8, "##INFO=<") == 0 || line.compare(0, 10, "##FILTER=<") == 0) {
+        std::string id, type;
+        header_id(line, id, type);
+        if (id == "DS") {
+          prefer_ds = true;
+          if (fmt_line) ds_float = type == "Float";
+        }
+      }
       if (line.compare(0, 6, "#CHROM") == 0) {
         size_t a = 0;
         int col = 0;
@@ -129,6 +196,8 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
         P.n_file = static_cast<int>(P.fam_iid.size());
         P.bytes_per_snp = (P.n_file + 3) / 4;
         if (P.n_file == 0) die("VCF has no samples: " + path);
+        P.dense = prefer_ds;
+        if (prefer_ds) info("VCF: FORMAT/DS present -> use dosage field when available");
       }
       continue;
     }
@@ -150,8 +219,8 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
       ++vi.n_multi;
       continue;
     }
-    // GT's position among the FORMAT keys
-    int gt_at = -1;
+    // GT's and DS's positions among the FORMAT keys
+    int gt_at = -1, ds_at = -1;
     {
       int k = 0;
       size_t s = 0;
@@ -160,36 +229,40 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
         size_t e = fmt.find(':', s);
         if (e == std::string::npos) e = fmt.size();
         if (fmt.compare(s, e - s, "GT") == 0) gt_at = k;
+        if (fmt.compare(s, e - s, "DS") == 0) ds_at = k;
         ++k;
         s = e + 1;
       }
     }
-    if (gt_at < 0) continue;  // no genotypes in this record
+    const bool use_ds = prefer_ds && ds_float && ds_at >= 0;
+    if (!use_ds && gt_at < 0) continue;  // no genotypes in this record
+    if (use_ds && !said_ds) {
+      info("VCF: using FORMAT/DS dosages");
+      said_ds = true;
+    }
     const std::string chrom(fld[0], flen[0]);
     const bool hap = haploid_chrom(chrom);
-    std::vector<uint8_t> row(static_cast<size_t>(P.bytes_per_snp), 0);
+    std::vector<uint8_t> row(P.dense ? 0 : static_cast<size_t>(P.bytes_per_snp), 0);
+    std::vector<float> drow(P.dense ? static_cast<size_t>(P.n_file) : 0);
     std::vector<int32_t> hap_calls;
     for (int i = 0; i < P.n_file; ++i) {
       const char* s = fld[9 + i];
       const size_t len = flen[9 + i];
-      // the GT subfield of this sample (absent trailing subfields are missing)
-      size_t p0 = 0;
-      int k = 0;
-      while (k < gt_at && p0 < len) {
-        const void* c = std::memchr(s + p0, ':', len - p0);
-        if (!c) {
-          p0 = len;
-          break;
-        }
-        p0 = static_cast<const char*>(c) - s + 1;
-        ++k;
+      size_t p0 = 0, p1 = 0;
+      if (use_ds) {
+        drow[static_cast<size_t>(i)] = subfield(s, len, ds_at, p0, p1) ? parse_ds(s + p0, p1 - p0)
+                                                                         : std::numeric_limits<float>::quiet_NaN();
+        continue;
       }
-      size_t p1 = p0;
-      while (p1 < len && s[p1] != ':') ++p1;
+      // the GT subfield of this sample (absent trailing subfields are missing)
       bool haploid = false;
-      const int d = (k == gt_at && p1 > p0) ? parse_gt(s + p0, p1 - p0, haploid) : -1;
-      const uint32_t code = d < 0 ? 1u : (d == 2 ? 0u : (d == 1 ? 2u : 3u));
-      row[static_cast<size_t>(i >> 2)] |= static_cast<uint8_t>(code << ((i & 3) * 2));
+      const int d = (subfield(s, len, gt_at, p0, p1) && p1 > p0) ? parse_gt(s + p0, p1 - p0, haploid) : -1;
+      if (P.dense) {
+        drow[static_cast<size_t>(i)] = d < 0 ? std::numeric_limits<float>::quiet_NaN() : static_cast<float>(d);
+      } else {
+        const uint32_t code = d < 0 ? 1u : (d == 2 ? 0u : (d == 1 ? 2u : 3u));
+        row[static_cast<size_t>(i >> 2)] |= static_cast<uint8_t>(code << ((i & 3) * 2));
+      }
       if (d >= 0 && haploid && !hap) hap_calls.push_back(i);
     }
     P.chrom.push_back(chrom);
@@ -199,6 +272,7 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
     P.a2.push_back(std::string(fld[3], flen[3]));  // REF
     P.a1.push_back(alt);                            // ALT, the counted allele
     P.rows.insert(P.rows.end(), row.begin(), row.end());
+    P.ds.insert(P.ds.end(), drow.begin(), drow.end());
     vi.hap_chrom.push_back(hap ? 1 : 0);
     vi.hap_calls.push_back(std::move(hap_calls));
   } while (in.next(line));
@@ -210,23 +284,42 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
   return P;
 }
 
+bool vcf_has_index(const std::string& path) {
+  for (const char* ext : {".tbi", ".csi"}) {
+    gzFile f = gzopen((path + ext).c_str(), "rb");
+    if (!f) continue;
+    char magic[4] = {0, 0, 0, 0};
+    const int got = gzread(f, magic, 4);
+    gzclose(f);
+    if (got == 4 && magic[3] == 1 &&
+        ((magic[0] == 'T' && magic[1] == 'B' && magic[2] == 'I') || (magic[0] == 'C' && magic[1] == 'S' && magic[2] == 'I')))
+      return true;
+  }
+  return false;
+}
+
 void vcf_filter(Plink& P, const VcfInfo& vi, const std::vector<int32_t>& cols, const Options& opt) {
   const int64_t m = static_cast<int64_t>(P.chrom.size());
   const int n_an = static_cast<int>(cols.size());
   std::vector<uint8_t> keep(static_cast<size_t>(m), 0);
   for (int64_t s = 0; s < m; ++s) {
-    const uint8_t* row = P.rows.data() + s * P.bytes_per_snp;
     const std::vector<int32_t>& hc = vi.hap_calls[static_cast<size_t>(s)];
     int n_miss = 0, n_ok = 0;
     double sum = 0.0, ploidy = 0.0;
     for (int i = 0; i < n_an; ++i) {
       const int c = cols[i];
-      const uint32_t code = (row[c >> 2] >> ((c & 3) * 2)) & 3u;
-      if (code == 1u) {
+      double d;
+      if (P.dense) {
+        d = static_cast<double>(P.ds[static_cast<size_t>(s) * P.n_file + c]);
+      } else {
+        const uint32_t code = (P.rows[s * P.bytes_per_snp + (c >> 2)] >> ((c & 3) * 2)) & 3u;
+        d = code == 1u ? std::numeric_limits<double>::quiet_NaN() : (code == 0u ? 2.0 : (code == 2u ? 1.0 : 0.0));
+      }
+      if (std::isnan(d)) {
         ++n_miss;
         continue;
       }
-      sum += code == 0u ? 2.0 : (code == 2u ? 1.0 : 0.0);
+      sum += d;
       const bool hap = vi.hap_chrom[static_cast<size_t>(s)] || std::binary_search(hc.begin(), hc.end(), c);
       ploidy += hap ? 1.0 : 2.0;
       ++n_ok;
@@ -249,6 +342,7 @@ void vcf_filter(Plink& P, const VcfInfo& vi, const std::vector<int32_t>& cols, c
   Q.fam_iid = P.fam_iid;
   Q.n_file = P.n_file;
   Q.bytes_per_snp = P.bytes_per_snp;
+  Q.dense = P.dense;
   for (int64_t s = 0; s < m; ++s) {
     if (!keep[static_cast<size_t>(s)]) continue;
     Q.chrom.push_back(P.chrom[s]);
@@ -256,7 +350,10 @@ void vcf_filter(Plink& P, const VcfInfo& vi, const std::vector<int32_t>& cols, c
     Q.id.push_back(P.id[s]);
     Q.a1.push_back(P.a1[s]);
     Q.a2.push_back(P.a2[s]);
-    Q.rows.insert(Q.rows.end(), P.rows.begin() + s * P.bytes_per_snp, P.rows.begin() + (s + 1) * P.bytes_per_snp);
+    if (P.dense)
+      Q.ds.insert(Q.ds.end(), P.ds.begin() + s * P.n_file, P.ds.begin() + (s + 1) * P.n_file);
+    else
+      Q.rows.insert(Q.rows.end(), P.rows.begin() + s * P.bytes_per_snp, P.rows.begin() + (s + 1) * P.bytes_per_snp);
   }
   P = std::move(Q);
 }

@@ -235,27 +235,52 @@ def make_genes(seed: int, n_genes: int, chroms: Sequence[str], chrom_len: int,
     return ids, gchrom, start, end, strand, tss
 
 
+def _ds_text(v) -> str:
+    return "." if not np.isfinite(v) else np.format_float_positional(np.float32(v), unique=True, trim="-")
+
+
 def write_vcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequence[int], ids: Sequence[str],
               ref: Sequence[str], alt: Sequence[str], dosage: np.ndarray, haploid: Optional[np.ndarray] = None,
-              phased: bool = False) -> None:
+              phased: bool = False, ds: Optional[np.ndarray] = None, ds_rows: Optional[np.ndarray] = None) -> None:
     """VCF 4.2 with a GT field (gzip-compressed when `path` ends in .gz):
     dosage [m, n] = ALT allele count (-1 missing); haploid [m, n] marks calls
-    written with one allele ("0", "1", ".")."""
+    written with one allele ("0", "1", "."). With `ds` [m, n] (NaN = ".") the
+    header declares FORMAT/DS and the records where `ds_rows` is set (all by
+    default) carry GT:DS, each DS value written as the shortest text that
+    reads back as the same FP32 number."""
     import gzip
     sep = "|" if phased else "/"
     gt_dip = {0: f"0{sep}0", 1: f"0{sep}1", 2: f"1{sep}1", -1: f".{sep}."}
     gt_hap = {0: "0", 1: "1", -1: "."}
     opener = gzip.open if path.endswith(".gz") else open
+    if ds is not None and ds_rows is None:
+        ds_rows = np.ones(len(chrom), bool)
     with opener(path, "wt") as f:
         f.write("##fileformat=VCFv4.2\n")
         f.write('##FORMAT=<ID=GT,Number=1,Type=String,Description="Genotype">\n')
+        if ds is not None:
+            f.write('##FORMAT=<ID=DS,Number=A,Type=Float,Description="Estimated ALT dose, [P(0/1) + 2*P(1/1)]">\n')
         f.write("#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\t" + "\t".join(samples) + "\n")
         for r in range(len(chrom)):
             d = dosage[r]
             h = haploid[r] if haploid is not None else np.zeros(len(d), bool)
             calls = [gt_hap[int(v)] if hh else gt_dip[int(v)] for v, hh in zip(d, h)]
-            f.write(f"{chrom[r]}\t{int(pos[r])}\t{ids[r] or '.'}\t{ref[r]}\t{alt[r]}\t.\tPASS\t.\tGT\t" +
+            fmt = "GT"
+            if ds is not None and ds_rows[r]:
+                fmt = "GT:DS"
+                calls = [c + ":" + _ds_text(v) for c, v in zip(calls, ds[r])]
+            f.write(f"{chrom[r]}\t{int(pos[r])}\t{ids[r] or '.'}\t{ref[r]}\t{alt[r]}\t.\tPASS\t.\t{fmt}\t" +
                     "\t".join(calls) + "\n")
+
+
+def write_tabix_header(vcf_path: str) -> None:
+    """<vcf_path>.tbi holding a tabix index of no sequences (the magic and the
+    VCF preset): enough for a reader that only checks that an index exists;
+    a region query through it finds nothing."""
+    import gzip
+    import struct
+    with gzip.open(vcf_path + ".tbi", "wb") as f:
+        f.write(b"TBI\x01" + struct.pack("<8i", 0, 2, 1, 2, 0, ord("#"), 0, 0))
 
 
 def write_pheno(path: str, samples: Sequence[str], genes: Sequence[str], Y: np.ndarray) -> None:

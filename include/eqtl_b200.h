@@ -84,6 +84,19 @@ int eqtl_geno_load_bed(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t by
                        const int32_t* sample_col, int32_t n, int32_t miss_hand, double max_miss, double maf_min,
                        uint8_t* keep_out, double* af_out, int32_t* n_miss_out, int64_t* n_kept_out);
 
+/* The same load from dosage rows: replaces VcfSession::parse_record's
+ * FORMAT/DS and GT dosages (src/vcf_session.cpp:193-258) for a VCF read on
+ * the host. ds: m SNP-major rows of n_file FP32 ALT dosages (row s, file
+ * sample j at ds[s * n_file + j]); a value that is not finite (NaN for ".")
+ * is a missing call, every other value is used as it is. The filters and
+ * outputs are those of eqtl_geno_load_bed, with af = mean / 2 of the
+ * non-missing dosages (a caller that needs the reference's ploidy-aware VCF
+ * filters applies them itself and passes max_miss 1, maf_min 0). Every
+ * other call treats the loaded SNPs as it treats .bed SNPs. */
+int eqtl_geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int32_t n_file, const int32_t* sample_col,
+                          int32_t n, int32_t miss_hand, double max_miss, double maf_min, uint8_t* keep_out,
+                          double* af_out, int32_t* n_miss_out, int64_t* n_kept_out);
+
 /* Decoded, mean-imputed dosages of kept SNPs [lo, hi) as FP64, row-major
  * [hi - lo, n] (SnpRec.dosage after src/plink_bed.cpp:298-302). */
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);

@@ -134,15 +134,126 @@ def read_vcf_gt(path: str):
     return samples, recs, n_multi
 
 
+def _vcf_header_id(line: str):
+    body = line[line.index("<") + 1:]
+    if '"' in body:
+        body = body[:body.index('"')]
+    kv = dict(x.split("=", 1) for x in body.replace(">", ",").split(",") if "=" in x)
+    return kv.get("ID"), kv.get("Type")
+
+
+def _ds_value(text: str) -> float:
+    """One FORMAT/DS value as htslib stores it (an FP32 number); '.', an
+    unparseable or a non-finite value is missing (NaN)."""
+    if text in ("", "."):
+        return float("nan")
+    try:
+        v = float(np.float32(float(text.split(",")[0])))
+    except ValueError:
+        return float("nan")
+    return v if np.isfinite(v) else float("nan")
+
+
+def read_vcf_dosage(path: str):
+    """Text VCF (plain or gzip) as parse_record reads it
+    (src/vcf_session.cpp:66-68 DS detection, :193-258 DS / GT dosages):
+    when the header defines an ID "DS", a record whose FORMAT has DS (declared
+    Type=Float) takes each sample's DS value, other records their GT counts.
+    Returns (samples, records, n_multi) with records (chrom, pos, id, ref, alt,
+    dosage[float64, NaN missing], haploid_call[bool], used_ds)."""
+    import gzip
+    opener = gzip.open if open(path, "rb").read(2) == b"\x1f\x8b" else open
+    samples, recs, n_multi = [], [], 0
+    prefer_ds = ds_float = False
+    with opener(path, "rt") as f:
+        for line in f:
+            line = line.rstrip("\r\n")
+            if not line:
+                continue
+            if line.startswith(("##INFO=<", "##FORMAT=<", "##FILTER=<")):
+                hid, htype = _vcf_header_id(line)
+                if hid == "DS":
+                    prefer_ds = True
+                    if line.startswith("##FORMAT=<"):
+                        ds_float = htype == "Float"
+                continue
+            if line.startswith("#CHROM"):
+                samples = line.split("\t")[9:]
+                continue
+            if line.startswith("#"):
+                continue
+            fld = line.split("\t")
+            alt = fld[4]
+            if alt == "." or "," in alt:
+                n_multi += 1
+                continue
+            keys = fld[8].split(":")
+            use_ds = prefer_ds and ds_float and "DS" in keys
+            if not use_ds and "GT" not in keys:
+                continue
+            dos = np.full(len(samples), np.nan)
+            hap = np.zeros(len(samples), bool)
+            if use_ds:
+                di = keys.index("DS")
+                for i, sf in enumerate(fld[9:9 + len(samples)]):
+                    sub = sf.split(":")
+                    dos[i] = _ds_value(sub[di] if di < len(sub) else ".")
+            else:
+                gi = keys.index("GT")
+                for i, sf in enumerate(fld[9:9 + len(samples)]):
+                    sub = sf.split(":")
+                    gt = sub[gi] if gi < len(sub) else "."
+                    al = gt.replace("|", "/").split("/")[:2]
+                    if al[0] in (".", "") or (len(al) > 1 and al[1] == "."):
+                        continue
+                    dos[i] = sum(int(a) for a in al)
+                    hap[i] = len(al) == 1
+            recs.append((fld[0], int(fld[1]), "" if fld[2] == "." else fld[2], fld[3], alt, dos, hap, use_ds))
+    return samples, recs, n_multi
+
+
+def decode_dosage_rows(ds: np.ndarray, sample_col: Sequence[int], miss_hand: str, max_miss: float,
+                       maf_min: float) -> Decoded:
+    """decode_bed_rows for FP32 dosage rows [m, n_file] (a value that is not
+    finite is a missing call): the filters of src/plink_bed.cpp:292-309 with
+    af = (sum / n_ok) / 2, the sums in FP64 in sample order, and mean
+    imputation (src/vcf_session.cpp:270-279). `codes` holds -1 at missing
+    calls and 0 elsewhere."""
+    col = np.asarray(sample_col, dtype=np.int64)
+    d = np.asarray(ds, dtype=np.float32)[:, col].astype(np.float64)
+    miss = ~np.isfinite(d)
+    n = col.size
+    n_miss = miss.sum(1).astype(np.int32)
+    n_ok = n - n_miss
+    s = np.zeros(d.shape[0])
+    dz = np.where(miss, 0.0, d)
+    for i in range(n):                                               # sequential FP64 sums
+        s += dz[:, i]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        mu = s / n_ok
+        af = (s / n_ok) / 2.0
+    keep = n_ok > 0
+    keep &= ~(n_miss / float(n) > max_miss + 1e-15)
+    if miss_hand == "filter":
+        keep &= n_miss == 0
+    af = np.clip(np.nan_to_num(af, nan=0.0), 0.0, 1.0)
+    keep &= ~((af < 1e-12) | (af > 1.0 - 1e-12))
+    keep &= pass_maf(af, maf_min)
+    dosage = np.where(miss, mu[:, None] if miss_hand == "impute" else np.nan, d)
+    codes = np.where(miss, -1, 0).astype(np.int8)
+    return Decoded(keep, codes, dosage, n_miss, af)
+
+
 def vcf_keep(recs, sample_col: Sequence[int], max_miss: float, miss_filter: bool, maf_min: float) -> np.ndarray:
     """parse_record's filters over the analysis samples, then pass_maf on the
     ploidy-aware allele frequency (haploid contigs and haploid calls count one
     allele per call)."""
     col = np.asarray(sample_col, dtype=np.int64)
     keep = np.zeros(len(recs), bool)
-    for r, (chrom, _, _, _, _, dos, hap) in enumerate(recs):
+    for r, rec in enumerate(recs):
+        chrom, dos, hap = rec[0], rec[5], rec[6]
         d = dos[col]
-        ok = d >= 0
+        ok = d >= 0 if d.dtype.kind == "i" else np.isfinite(d)
         n_ok = int(ok.sum())
         n_miss = len(col) - n_ok
         if n_ok == 0:

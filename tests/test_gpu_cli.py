@@ -41,25 +41,31 @@ def _runs():
     return out
 
 
-def bed_to_vcf(prefix: str, out_path: str) -> None:
+def bed_to_vcf(prefix: str, out_path: str, ds: bool = False) -> None:
     """The same genotypes as a gzip-compressed VCF: ALT = A1 (the counted
-    allele), REF = A2, IDs and positions from the .bim."""
+    allele), REF = A2, IDs and positions from the .bim. With `ds` every record
+    also carries FORMAT/DS with the same dosages ("." where the call is
+    missing), which the program then reads instead of GT. The index next to
+    it (needed by cis scans) holds no sequences: records are read in file
+    order."""
     from eqtl_b200 import synth
     rows, n_file, fam, bim = R.read_bed(prefix)
     i = np.arange(n_file)
     codes = (rows[:, i // 4] >> (2 * (i % 4))) & 3
     dosage = np.array([2, -1, 1, 0], np.int8)[codes]
+    dsv = np.where(dosage < 0, np.nan, dosage.astype(np.float64)) if ds else None
     synth.write_vcf(out_path, fam, [b[0] for b in bim], [b[3] for b in bim], [b[1] for b in bim],
-                    [b[5] for b in bim], [b[4] for b in bim], dosage)
+                    [b[5] for b in bim], [b[4] for b in bim], dosage, ds=dsv)
+    synth.write_tabix_header(out_path)
 
 
 def _run(argv, case_dir, out_prefix, src="bed", tmp=None):
     a = list(argv)
     a[a.index("-o") + 1] = out_prefix
-    if src == "vcf":  # the same genotypes through -v
-        vcf = os.path.join(str(tmp), "geno.vcf.gz")
+    if src in ("vcf", "vcf_ds"):  # the same genotypes through -v (GT, or DS)
+        vcf = os.path.join(str(tmp), "geno.vcf.gz" if src == "vcf" else "geno_ds.vcf.gz")
         if not os.path.exists(vcf):
-            bed_to_vcf(os.path.join(case_dir, a[a.index("-b") + 1]), vcf)
+            bed_to_vcf(os.path.join(case_dir, a[a.index("-b") + 1]), vcf, ds=src == "vcf_ds")
         k = a.index("-b")
         a[k:k + 2] = ["-v", vcf]
     r = subprocess.run([os.path.abspath(BIN)] + a, cwd=case_dir, capture_output=True, text=True, timeout=600)
@@ -67,7 +73,7 @@ def _run(argv, case_dir, out_prefix, src="bed", tmp=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("src", ["bed", "vcf"])
+@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" in r[2]])
 def test_cli_make_grm(case, tag, argv, src, tmp_path):
     d = os.path.join(GOLD, case)
@@ -82,7 +88,7 @@ def test_cli_make_grm(case, tag, argv, src, tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("src", ["bed", "vcf"])
+@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" not in r[2]])
 def test_cli_scan_matches_reference(case, tag, argv, src, tmp_path):
     d = os.path.join(GOLD, case)

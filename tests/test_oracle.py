@@ -92,3 +92,46 @@ def test_shuffle_matches_reference_perm_file():
     idx = R.shuffle_indices(101, R.perm_seed(7, 3, "G00001"))
     assert sorted(idx) == list(range(101))
     assert idx != list(range(101))
+
+
+def test_dosage_decode_restates_bed_decode():
+    """decode_dosage_rows on integer dosages (NaN = missing) is the .bed
+    decode of the same calls: keep flags, af, counts and imputed dosages."""
+    from eqtl_b200 import synth
+    g = synth.make_genotypes(31, n=97, m=400, n_chrom=2, chrom_len=1_000_000, miss_rate=0.05, maf_lo=0.005)
+    rows = synth.pack_bed_rows(g.codes)
+    ds = np.where(g.codes < 0, np.nan, g.codes).astype(np.float32)
+    sel = np.random.default_rng(1).permutation(97)[:80]
+    for hand, mm, maf in (("impute", 0.8, 0.0), ("impute", 0.03, 0.05), ("filter", 0.8, 0.0)):
+        a = R.decode_bed_rows(rows, 97, sel, hand, mm, maf)
+        b = R.decode_dosage_rows(ds, sel, hand, mm, maf)
+        assert np.array_equal(a.keep, b.keep) and np.array_equal(a.n_miss, b.n_miss)
+        assert np.array_equal(a.af, b.af)
+        assert np.array_equal(a.dosage, b.dosage, equal_nan=True)
+        assert np.array_equal(a.codes < 0, b.codes < 0)
+
+
+def test_vcf_dosage_reader_restates_gt_reader(tmp_path):
+    """Without an ID "DS" in the header read_vcf_dosage gives read_vcf_gt's
+    records; with FORMAT/DS it reads the DS values as FP32 numbers."""
+    from eqtl_b200 import synth
+    rng = np.random.default_rng(2)
+    d = rng.binomial(2, 0.3, (6, 10)).astype(np.int8)
+    d[0, 3] = -1
+    p = str(tmp_path / "a.vcf")
+    synth.write_vcf(p, [f"s{i}" for i in range(10)], ["1"] * 6, list(range(1, 7)), [""] * 6, ["A"] * 6, ["C"] * 6, d)
+    s1, r1, _ = R.read_vcf_gt(p)
+    s2, r2, _ = R.read_vcf_dosage(p)
+    assert s1 == s2 and len(r1) == len(r2)
+    for a, b in zip(r1, r2):
+        assert a[:5] == b[:5] and not b[7]
+        assert np.array_equal(np.where(a[5] < 0, np.nan, a[5]), b[5], equal_nan=True)
+    ds = rng.uniform(0, 2, (6, 10))
+    ds[2, 4] = np.nan
+    q = str(tmp_path / "b.vcf")
+    synth.write_vcf(q, [f"s{i}" for i in range(10)], ["1"] * 6, list(range(1, 7)), [""] * 6, ["A"] * 6, ["C"] * 6, d,
+                    ds=ds)
+    _, r3, _ = R.read_vcf_dosage(q)
+    got = np.stack([r[5] for r in r3])
+    assert all(r[7] for r in r3)
+    assert np.array_equal(got, ds.astype(np.float32).astype(np.float64), equal_nan=True)
