@@ -222,6 +222,29 @@ def make_pheno_lmm(seed: int, g: Genotypes, n_genes: int, n_cov: int, *, h2_max:
     return Y, C, h2
 
 
+def make_pheno_counts(seed: int, g: Genotypes, n_genes: int, n_cov: int, *, n_trans: int = 0,
+                      beta_sd: float = 0.3, cov_weight: float = 0.2) -> tuple:
+    """Negative-binomial counts (NB2, log link): log mu = b0 + cov_weight *
+    sum(C) + planted SNP effects, b0 ~ U(0.5, 4), dispersion phi ~ U(0.05, 1)
+    per gene, y ~ Poisson(Gamma(1/phi, phi mu)). Returns (Y [n, G], C [n, c])."""
+    rng = np.random.default_rng(seed)
+    n = len(g.samples)
+    C = rng.standard_normal((n, n_cov))
+    eta = rng.uniform(0.5, 4.0, n_genes)[None, :] + cov_weight * C.sum(1, keepdims=True)
+    eta = np.repeat(eta, n_genes, axis=1) if eta.shape[1] == 1 else eta
+    if n_trans:
+        m = g.codes.shape[0]
+        snps = rng.integers(0, m, size=n_trans)
+        genes = rng.integers(0, n_genes, size=n_trans)
+        d = imputed_dosage(g.codes[snps])
+        for t in range(n_trans):
+            eta[:, genes[t]] += rng.normal(0.0, beta_sd) * (d[t] - d[t].mean())
+    phi = rng.uniform(0.05, 1.0, n_genes)
+    mu = np.exp(eta)
+    lam = rng.gamma(1.0 / phi[None, :], phi[None, :] * mu)
+    return rng.poisson(lam).astype(np.float64), C
+
+
 def make_genes(seed: int, n_genes: int, chroms: Sequence[str], chrom_len: int,
                body: int = 1) -> tuple:
     """Genes with uniform TSS, strand +/- 50/50, body length `body` bp."""

@@ -340,6 +340,8 @@ class Scanner:
     def run_scope(self, model, scope):
         opt = self.opt
         pthr = opt.pval_cis if scope == "cis" else opt.pval_trans
+        if model == "glm":
+            return self.run_glm(scope, pthr)
         if scope == "cis":
             return self.run_cis(model, pthr)
         jobs = []
@@ -494,6 +496,77 @@ class Scanner:
             if opt.perm > 0 and s.n_tested > 0:
                 self.perm(model, s, gene, (keep, yk, Xk, None), cached, best_p, prep,
                           lmm_basis=(Q, lam) if model == "lmm" else None)
+            if best_row is not None and best_p <= pthr and best_p <= 1.0:
+                tops.append(best_row)
+            summ.append(s)
+        return pairs, tops, self.finish(summ)
+
+    # -- NB GLM, gene-outer for every scope (src/scan.cpp:227-300 and, for cis
+    # with -t > 1, src/scan_cis.cpp:18-115; per gene include/eqtl/scan_cis.hpp:15-66)
+    def run_glm(self, scope, pthr):
+        opt = self.opt
+        if opt.perm > 0:
+            raise NotImplementedError("GLM permutations (parametric NB sampling) are not restated")
+        works = []
+        for gi, gene in enumerate(self.genes):
+            loc = self.annot.get(gene) if opt.gff else None
+            if scope == "cis" or scope == "trans":
+                if loc is None:
+                    continue
+            elif opt.gff and loc is None and scope != "gw":
+                continue
+            works.append((gi, gene, loc))
+        parallel_cis = scope == "cis" and opt.threads > 1 and bool(opt.gff)
+        if parallel_cis:
+            # the raw counts are checked before the sort (src/scan_cis.cpp:35-38)
+            works = [w for w in works if R.looks_like_counts(self.Y[:, w[0]])]
+            works.sort(key=lambda w: (w[2].chrom, w[2].tss))
+        bim_chrom = [b[0] for b in self.bim]
+        pairs, tops, summ = [], [], []
+        for gi, gene, loc in works:
+            y = self.gene_y(gi)
+            if not parallel_cis and not R.looks_like_counts(y):
+                continue                                       # "skip non-count gene"
+            ready = self.build_ready(y, need_k=False)
+            if ready is None:
+                continue
+            keep, yk, Xk, _ = ready
+            if scope == "cis":
+                lo = max(loc.start - opt.window, 1)
+                hi = loc.end + opt.window
+                snps = [s_ for s_ in self.kept
+                        if chrom_equal(bim_chrom[s_], loc.chrom) and lo <= self.bim[s_][3] <= hi]
+            elif scope == "trans":
+                snps = [s_ for s_ in self.kept if not self.in_cis(s_, loc)]
+            else:
+                snps = list(self.kept)
+            s = Summary(gene)
+            if loc is not None:
+                s.chrom, s.tss = loc.chrom, loc.tss
+            prep = R.prep_glm_nb(yk, Xk)
+            acc = R.AcatAcc()
+            best_p, best_row = 2.0, None
+            if snps:
+                G = self.dec.dosage[np.array(snps)][:, keep]
+                af_sub, ok = R.subset_maf(G)
+                st = R.test_glm_nb_many(prep, G)
+                n = len(keep)
+                for i, snp in enumerate(snps):
+                    pv = st["p"][i]
+                    if not ok[i] or not math.isfinite(pv):
+                        continue
+                    s.n_tested += 1
+                    acc.add_many([pv])
+                    acc.add_sensitivity([pv], [st["stat"][i]], None)
+                    row = pair_row(gene, self.snp_meta(snp), _hit(st, i, af_sub[i]), n, loc, scope) + (
+                        fmt(prep.phi), "1" if prep.converged else "0")
+                    if pv <= pthr:
+                        pairs.append(row)
+                        s.n_sig += 1
+                    if pv < best_p:
+                        best_p, best_row = pv, row
+            s.acat = acc.p()
+            s.acat_sens = acc.log10_sensitivity()
             if best_row is not None and best_p <= pthr and best_p <= 1.0:
                 tops.append(best_row)
             summ.append(s)

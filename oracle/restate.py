@@ -412,8 +412,11 @@ class AcatAcc:
             return
         term = np.tan((0.5 - np.where(p[use] <= 0, 1e-300, p[use])) * np.pi)
         tt = t[use]
-        logf = (math.lgamma((df + 1) / 2) - math.lgamma(df / 2) - 0.5 * math.log(df * math.pi)
-                - (df + 1) / 2 * np.log1p(tt * tt / df))
+        if df is None:                                   # normal statistic (GLM score test)
+            logf = -0.5 * math.log(2 * math.pi) - 0.5 * tt * tt
+        else:
+            logf = (math.lgamma((df + 1) / 2) - math.lgamma(df / 2) - 0.5 * math.log(df * math.pi)
+                    - (df + 1) / 2 * np.log1p(tt * tt / df))
         self.sens = getattr(self, "sens", 0.0) + float(np.sum(np.pi * (1 + term * term) * 2 * np.exp(logf)))
 
     def log10_sensitivity(self) -> float:
@@ -633,6 +636,118 @@ def test_lm_many(prep: PrepLm, G: np.ndarray):
     gtg = np.einsum("ij,ij->i", g_s, g_s)
     gty = g_s @ prep.y_s
     return lm_stats(gtg, gty, prep.yty, prep.n, prep.p)
+
+
+# ---------------------------------------------------------------------------
+# NB GLM  (src/model_glm.cpp:13-132; looks_like_counts src/model_lm.cpp:8-17;
+# pnorm_two_sided src/util.cpp:116-123)
+# ---------------------------------------------------------------------------
+def looks_like_counts(y) -> bool:
+    y = np.asarray(y, np.float64)
+    f = y[np.isfinite(y)]
+    if f.size == 0:
+        return False
+    return bool(np.all(f >= 0) and np.all(np.abs(f - np.floor(f)) <= 1e-8))
+
+
+def pnorm_two_sided(z):
+    """erfc(|z| / sqrt(2)) clipped to [0, 1]; 1 for a non-finite z."""
+    z = np.asarray(z, np.float64)
+    from scipy.special import erfc
+    p = np.where(np.isfinite(z), erfc(np.abs(z) / math.sqrt(2.0)), 1.0)
+    return np.clip(p, 0.0, 1.0)
+
+
+@dataclass
+class PrepGlm:
+    y: np.ndarray
+    X: np.ndarray
+    mu: np.ndarray
+    w: np.ndarray          # null working weights mu / (1 + phi mu)
+    r: np.ndarray          # (y - mu) / (1 + phi mu)
+    XtWX_inv: np.ndarray
+    phi: float
+    converged: bool
+    n: int
+
+
+def _nb_mom_phi(y, mu, df):
+    m = np.maximum(mu, 1e-8)
+    num = float(np.sum(((y - m) * (y - m) - m) / (m * m)))
+    return max(1e-8, num / max(1, df))
+
+
+def nb_irls(y, X, phi):
+    """nb_irls (src/model_glm.cpp:28-72) with estimate_phi: IRLS at fixed phi
+    (up to 50 rounds, until max |beta change| < 1e-6), then phi by moments,
+    until phi moves less than 1e-6 max(1, phi) (up to 10 rounds). Returns
+    (phi, beta, mu, converged); converged is False only when X'WX cannot be
+    factorised."""
+    n, p = X.shape
+    df = max(1, n - p)
+    beta = np.zeros(p)
+    mu = np.maximum(y, 0.1)
+    for _ in range(10):
+        for _ in range(50):
+            m = np.maximum(mu, 1e-8)
+            var = m + phi * m * m
+            w = (m * m) / np.maximum(var, 1e-12)
+            z = np.log(m) + (y - m) / m
+            XtWX = X.T @ (w[:, None] * X)
+            try:
+                np.linalg.cholesky(XtWX)
+            except np.linalg.LinAlgError:
+                return phi, beta, mu, False
+            beta_new = np.linalg.solve(XtWX, X.T @ (w * z))
+            mu_new = np.exp(X @ beta_new)
+            diff = float(np.max(np.abs(beta_new - beta)))
+            beta, mu = beta_new, mu_new
+            if diff < 1e-6:
+                break
+        phi_new = _nb_mom_phi(y, mu, df)
+        if abs(phi_new - phi) < 1e-6 * max(1.0, phi):
+            return phi_new, beta, mu, True
+        phi = phi_new
+    return phi, beta, mu, True
+
+
+def prep_glm_nb(y, X) -> PrepGlm:
+    """prep_glm_nb (src/model_glm.cpp:74-96): the null NB fit from phi = 1."""
+    y = np.asarray(y, np.float64)
+    if not looks_like_counts(y):
+        raise ValueError("glm (NB) requires non-negative integer counts")
+    phi, _, mu, conv = nb_irls(y, X, 1.0)
+    m = np.maximum(mu, 1e-8)
+    w = m / (1.0 + phi * m)
+    XtWX_inv = np.linalg.solve(X.T @ (w[:, None] * X), np.eye(X.shape[1]))
+    r = (y - mu) / (1.0 + phi * mu)
+    return PrepGlm(y, X, mu, w, r, XtWX_inv, phi, conv, y.size)
+
+
+def test_glm_nb_many(prep: PrepGlm, G: np.ndarray):
+    """test_glm_nb (src/model_glm.cpp:98-132) for dosage rows G [m, n]: the
+    score test at beta_g = 0 with phi fixed, U = g'r, info = g'Wg -
+    (X'Wg)' (X'WX)^-1 (X'Wg); beta = U / info, se = 1 / sqrt(info), stat =
+    U / sqrt(info), p two-sided normal. p is NaN for a null fit that did not
+    converge and 1 (the rest 0) for gvar or info below 1e-12."""
+    G = np.atleast_2d(np.asarray(G, np.float64))
+    m = G.shape[0]
+    out = {k: np.zeros(m) for k in ("beta", "se", "stat", "p", "r2")}
+    if not prep.converged:
+        out["p"][:] = np.nan
+        return out
+    out["p"][:] = 1.0
+    gvar = (G * G).mean(1) - G.mean(1) ** 2
+    U = G @ prep.r
+    XtWg = (G * prep.w[None, :]) @ prep.X
+    info = np.einsum("ij,ij->i", G * prep.w[None, :], G) - np.einsum("ij,jk,ik->i", XtWg, prep.XtWX_inv, XtWg)
+    ok = ~(gvar < 1e-12) & ~(info < 1e-12)
+    si = np.sqrt(np.where(ok, info, 1.0))
+    out["beta"] = np.where(ok, U / np.where(ok, info, 1.0), 0.0)
+    out["se"] = np.where(ok, 1.0 / si, 0.0)
+    out["stat"] = np.where(ok, U / si, 0.0)
+    out["p"] = np.where(ok, pnorm_two_sided(out["stat"]), 1.0)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -4,7 +4,7 @@ Each case is a seeded synthetic PLINK data set (eqtl_b200.synth) plus the
 outputs of the reference eqtl program itself, built from the reference's own
 sources by `make -C oracle` (oracle/_ref/eqtl). Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py [case ...]
 
 The fixtures are small (n=120 samples, 800 SNPs, 40 genes) so they commit
 cheaply; larger parity cases are generated on the fly by the GPU tests.
@@ -44,6 +44,18 @@ CASES = {
                      "1e-2", "-t", "1"]),
             ("grm", ["--make-grm"]),
         ]),
+    "counts": dict(
+        geno=dict(seed=301, n=120, m=800, n_chrom=3, chrom_len=5_000_000, family=None,
+                  miss_rate=0.01, maf_lo=0.02),
+        genes=dict(seed=302, n_genes=30, body=1000),
+        pheno=dict(kind="counts", seed=303, n_cov=2),
+        runs=[
+            ("all", ["--model", "glm", "--mode", "all", "-w", "500000", "--pval-cis", "1e-2",
+                     "--pval-trans", "1e-2", "-t", "2"]),
+            ("gw", ["--model", "glm", "--mode", "gw", "--pval-trans", "1e-2", "-t", "1"]),
+            ("mixed", ["--model", "lm,glm", "--mode", "trans", "--miss-hand", "filter", "--maf", "0.05",
+                       "--pval-trans", "5e-3", "-t", "1"]),
+        ]),
     "nogff": dict(
         geno=dict(seed=201, n=96, m=600, n_chrom=2, chrom_len=3_000_000, family=None,
                   miss_rate=0.02, maf_lo=0.01),
@@ -68,7 +80,9 @@ def build_case(name: str, spec: dict) -> None:
     ids, gc, st, en, sd, tss = synth.make_genes(gs["seed"], gs["n_genes"], chroms,
                                                 spec["geno"]["chrom_len"], body=gs["body"])
     ph = spec["pheno"]
-    if ph["kind"] == "lm":
+    if ph["kind"] == "counts":
+        Y, C = synth.make_pheno_counts(ph["seed"], g, gs["n_genes"], ph["n_cov"], n_trans=10)
+    elif ph["kind"] == "lm":
         Y, C = synth.make_pheno_lm(ph["seed"], g, gs["n_genes"], ph["n_cov"], cis_effects=True,
                                    gene_tss=tss, gene_chrom=gc, window=500_000, n_trans=10)
     else:
@@ -104,6 +118,9 @@ def build_case(name: str, spec: dict) -> None:
 if __name__ == "__main__":
     if not os.path.exists(REF):
         raise SystemExit("build the reference first: make -C oracle")
+    only = sys.argv[1:]                      # case names to (re)build; all by default
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         build_case(name, spec)
         print("built", name)

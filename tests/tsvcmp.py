@@ -76,6 +76,13 @@ def compare_pairs(ref_rows: Sequence[Sequence[str]], got_rows: Sequence[Sequence
         for i in (6, 8, 9, 11):
             if not close(_num(r[i]), _num(g[i]), tol.beta_rel, 1e-7):
                 errs.append(f"{k} {PAIR_COLS[i]} {r[i]} vs {g[i]}")
+        if len(r) != len(g):
+            errs.append(f"{k} {len(r)} vs {len(g)} columns")
+        elif len(r) == 17:                       # GLM: phi, glm_converged
+            if not close(_num(r[15]), _num(g[15]), tol.beta_rel, 1e-9):
+                errs.append(f"{k} phi {r[15]} vs {g[15]}")
+            if r[16] != g[16]:
+                errs.append(f"{k} glm_converged {r[16]} vs {g[16]}")
     return errs
 
 
