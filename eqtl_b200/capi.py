@@ -25,7 +25,7 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
-           "eqtl_test_pairs", "eqtl_geno_load_dosage"]
+           "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -92,6 +92,8 @@ def load() -> C.CDLL:
         lib.eqtl_lmm_set_basis.argtypes = [vp, vp, vp, i32]
         lib.eqtl_scan_trans_lmm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, vp, i64, C.POINTER(i64),
                                             vp, i64, C.POINTER(i64)]
+        lib.eqtl_scan_glm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, vp, vp, i64, C.POINTER(i64),
+                                      vp, i64, C.POINTER(i64)]
         _lib = lib
     return _lib
 
@@ -312,6 +314,15 @@ class Context:
         self._check(self.lib.eqtl_test_pairs(self.h, 0 if model == "lm" else 1, C.byref(prm), _ptr(Y), _ptr(X),
                                              _ptr(cols), _ptr(snps), cols.size, _ptr(out), _ptr(delta)))
         return out, delta
+
+    def scan_glm(self, Y, X, pthr, perm_thr=0.0, windows=None):
+        """eqtl_scan_glm -> (genes, pairs, cands, phi, converged); pairs' t is the score z."""
+        G = self.pheno_shape[1] if Y is None else np.asarray(Y).shape[1]
+        phi = np.zeros(G, np.float64)
+        conv = np.zeros(G, np.uint8)
+        genes, pairs, cands = self._scan(self.lib.eqtl_scan_glm, Y, X, pthr, perm_thr, windows,
+                                         extra=(_ptr(phi), _ptr(conv)))
+        return genes, pairs, cands, phi, conv.astype(bool)
 
     def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None):
         """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta)."""

@@ -314,24 +314,26 @@ bool cis_tile_list(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int NT
   return true;
 }
 
-dev::TTable device_ttable(eqtl_ctx* ctx, double df) {
-  EQTL_CHECK(df > 0, EQTL_E_ARG, "residual degrees of freedom must be positive");
+dev::TTable device_ttable(eqtl_ctx* ctx, double df, bool normal) {
+  EQTL_CHECK(normal || df > 0, EQTL_E_ARG, "residual degrees of freedom must be positive");
+  if (normal) df = kZTableD;
+  const double key = normal ? -2.0 : df;  // the normal table is cached under -2 (-1: none uploaded)
   static std::mutex mu;
   static std::map<double, TTableHost> cache;
   TTableHost T;
   {
     std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(df);
-    if (it == cache.end()) it = cache.emplace(df, build_ttable(df)).first;
+    auto it = cache.find(key);
+    if (it == cache.end()) it = cache.emplace(key, build_ttable(df, normal)).first;
     T = it->second;
   }
   Workspace& ws = ctx->ws;
-  if (ws.tt_df != df) {
+  if (ws.tt_df != key) {
     ws.tt_h.upload(T.h.data(), T.h.size(), ctx->stream);
     ws.tt_L.upload(T.L.data(), T.L.size(), ctx->stream);
     ws.tt_c1.upload(T.c1.data(), T.c1.size(), ctx->stream);
     ws.tt_lt.upload(T.lt.data(), T.lt.size(), ctx->stream);
-    ws.tt_df = df;
+    ws.tt_df = key;
   }
   dev::TTable t{};
   t.h = ws.tt_h.p;
@@ -773,6 +775,22 @@ int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double
       eqtl::scan_trans_lmm_simt(ctx, prm, Y, X, delta_out, genes, pv, cv);
     else
       eqtl::scan_trans_lmm(ctx, prm, Y, X, delta_out, genes, pv, cv);
+    if (n_pairs) *n_pairs = static_cast<int64_t>(pv.size());
+    if (n_cands) *n_cands = static_cast<int64_t>(cv.size());
+    EQTL_CHECK(static_cast<int64_t>(pv.size()) <= pair_cap && static_cast<int64_t>(cv.size()) <= cand_cap,
+               EQTL_E_OVERFLOW, "result buffer too small");
+    if (!pv.empty()) std::copy(pv.begin(), pv.end(), pairs);
+    if (!cv.empty()) std::copy(cv.begin(), cv.end(), cands);
+  });
+}
+
+int eqtl_scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* phi_out,
+                  uint8_t* converged_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
+                  int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(prm && genes, EQTL_E_ARG, "null input");
+    std::vector<eqtl_pair> pv, cv;
+    eqtl::scan_glm(ctx, prm, Y, X, phi_out, converged_out, genes, pv, cv);
     if (n_pairs) *n_pairs = static_cast<int64_t>(pv.size());
     if (n_cands) *n_cands = static_cast<int64_t>(cv.size());
     EQTL_CHECK(static_cast<int64_t>(pv.size()) <= pair_cap && static_cast<int64_t>(cv.size()) <= cand_cap,

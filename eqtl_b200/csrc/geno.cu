@@ -252,6 +252,7 @@ void geno_decode(eqtl_ctx* ctx, const int32_t* sample_col, int miss_hand, double
   const int64_t m = g.m_all;
   const int n = g.n;
   ctx->rot.m = 0;  // rotated genotypes belong to the previous genotypes
+  ctx->glm_ops.m = 0;
   g.k_pad = ((n + 63) / 64) * 64;
   g.col.upload(sample_col, n, st);
   g.col_identity = true;

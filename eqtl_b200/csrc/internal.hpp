@@ -194,6 +194,11 @@ struct Workspace {
   DevBuf<double> rb_Wg, rb_Xw, rb_Ag, rb_Lg, rb_ldx, rb_ldD, rb_Bg, rb_Yg;  // grid phase
   DevBuf<uint8_t> rb_state;
   DevBuf<unsigned int> rb_active;
+  // NB-GLM null fits: per gene and sample mu, w = mu / (1 + phi mu) and
+  // r = (y - mu) / (1 + phi mu); per gene phi, sum r and flags
+  DevBuf<double> glm_mu, glm_w, glm_r, glm_phi, glm_rsum;
+  DevBuf<float> glm_rsum_f, snp_mean;
+  DevBuf<uint8_t> glm_ok, glm_counts;
   // per-gene scan outputs + candidates
   DevBuf<double> acat;
   DevBuf<int> used, tested;
@@ -243,6 +248,7 @@ struct eqtl_ctx {
   std::string last_error;
   eqtl::Geno geno;
   eqtl::Rotated rot;
+  eqtl::Rotated glm_ops;  // NB-GLM SNP operands: centred dosages gc and gc^2 (not rotated)
   eqtl::LmmBasisDev basis;
   eqtl::PhenoDev pheno;
   eqtl::Workspace ws;
@@ -288,6 +294,11 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
 void solver_release(eqtl_ctx* ctx);
 void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    const std::vector<int2>& todo, eqtl_pair* out);
+// NB-GLM score-test scan (model_glm.cpp) of every (gene, kept SNP) pair in
+// scope; phi_out / converged_out per gene.
+void scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* phi_out,
+              uint8_t* converged_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
+              std::vector<eqtl_pair>& cands);
 void test_pairs_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                     const std::vector<int2>& todo, eqtl_pair* out, double* delta_out);
 

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <limits>
 #include <memory>
+#include <type_traits>
 
 #include "internal.hpp"
 #include "scan_host.hpp"
@@ -730,20 +731,33 @@ struct LmmEpiParams {
   float t_cand;
   TTable tt;
   GeneOut out;
+  // NB-GLM scan only (GlmEpiParams): per kept SNP the imputation mean (the
+  // SNP operand is centred), per gene sum_i r_i and the null fit's success
+  const float* snp_mean;    // [m, padded to 16 + 16]
+  const float* rsum;        // [G]
+  const uint8_t* gene_ok;   // [G]
 };
+// The same fields select the NB-GLM score-test epilogue (LmmEpi<P, true>).
+template <int P>
+struct GlmEpiParams : LmmEpiParams<P> {};
 
 // Accumulator order of the tile: [gg, a_0 .. a_{P-1}, NUM] (the gene-side
 // operands w, w o X~_k, w o r~ against Gt^2, Gt, Gt). The epilogue is
 // two-phase: S = gg - a' A00^-1 a of every pair of the warp's chunks first,
 // which frees the gg and a slots for the next tile's MMAs, then NUM and the
 // rest of the statistic.
-template <int P>
+//
+// GLM = true is the NB-GLM score test on the same accumulators (unrotated
+// centred dosages gc against w, w o x_k and r of the gene's null fit):
+// info = S, U = NUM + mean_s * sum_i r_i, and the screened statistic is
+// z^2 = U^2 / info against the normal tables.
+template <int P, bool GLM = false>
 struct LmmEpi {
   static constexpr bool kGrouped = false;
   static constexpr bool kTwoPhase = true;
   static constexpr int kPhase1 = P + 1;  // gg and a_k
   static constexpr int kMaxChunks = 2;   // 16-column chunks per warp and tile
-  using Params = LmmEpiParams<P>;
+  using Params = std::conditional_t<GLM, GlmEpiParams<P>, LmmEpiParams<P>>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
   float* tsm;
@@ -754,6 +768,7 @@ struct LmmEpi {
   float u[P + 2];  // unscale of [NUM, a_0 .. a_{P-1}, gg] (the gene-ops order)
   float ai[P][P];
   float inv_rss = 0;
+  float rs = 0;  // GLM: sum_i r_i of the gene
   // S per pair of the warp's two chunks (0 where gg < 1e-12); two named
   // arrays picked by a select, so they stay in registers for a runtime ci
   float S0[16], S1[16];
@@ -768,16 +783,20 @@ struct LmmEpi {
     gene = g;
     snp0 = s0;
     gvalid = g < Pr.G;
+    if constexpr (GLM) gvalid = gvalid && Pr.gene_ok[g];  // a failed null fit tests nothing
     acc.reset();
     if (gvalid) {
+      if constexpr (GLM) rs = Pr.rsum[g];
 #pragma unroll
       for (int k = 0; k < P + 2; ++k) u[k] = Pr.unscale[static_cast<int64_t>(g) * (P + 2) + k];
 #pragma unroll
       for (int a = 0; a < P; ++a)
 #pragma unroll
         for (int b = 0; b < P; ++b) ai[a][b] = static_cast<float>(Pr.ainv[(static_cast<int64_t>(g) * P + a) * P + b]);
-      const double r = Pr.rss_null[g];
-      inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
+      if constexpr (!GLM) {
+        const double r = Pr.rss_null[g];
+        inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
+      }
       acc.load_window(Pr.win, g);
     }
   }
@@ -818,10 +837,16 @@ struct LmmEpi {
       const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
       const float num = v[0][j] * u[0];
       const float S = ci == 0 ? S0[j] : S1[j];
-      const float r = num * __fdividef(num, S) * inv_rss;
-      const float omr = 1.0f - r;
-      const bool ok_stat = S > 1e-15f && omr > 0.0f;
-      const float u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      float u;
+      if constexpr (GLM) {
+        const float U = fmaf(__ldg(Pr.snp_mean + s), rs, num);
+        u = S > 1e-15f ? __fdividef(U * U, S) : 0.0f;  // z^2
+      } else {
+        const float r = num * __fdividef(num, S) * inv_rss;
+        const float omr = 1.0f - r;
+        const bool ok_stat = S > 1e-15f && omr > 0.0f;
+        u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      }
       const ScreenOut o = acat_screen_u(u, tt);
       acc.add_screen(o, s, valid);
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
@@ -944,12 +969,18 @@ struct LmmGroupEpiParams {
   float t_cand;
   TTable tt;
   GeneOut out;
+  const float* snp_mean;    // GLM only, as in LmmEpiParams
+  const float* rsum;
+  const uint8_t* gene_ok;
 };
+struct GlmGroupEpiParams : LmmGroupEpiParams {};
 
-struct LmmGroupEpi {
+// GLM = true: the NB-GLM score test, as in LmmEpi.
+template <bool GLM>
+struct LmmGroupEpiT {
   static constexpr bool kGrouped = true;
   static constexpr int kTileN = 64;  // one 16-column chunk per epilogue thread
-  using Params = LmmGroupEpiParams;
+  using Params = std::conditional_t<GLM, GlmGroupEpiParams, LmmGroupEpiParams>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
   float* tsm;
@@ -958,10 +989,11 @@ struct LmmGroupEpi {
   int64_t snp0 = 0;
   bool gvalid = false;
   float inv_rss = 0;
+  float rs = 0;  // GLM: sum_i r_i of the gene
   float num[16], S[16];
   float u_cand;  // t_cand^2
   GeneAcc acc;
-  __device__ LmmGroupEpi(const Params& p, const TileShape&, uint8_t* smem)
+  __device__ LmmGroupEpiT(const Params& p, const TileShape&, uint8_t* smem)
       : Pr(p), tsm(reinterpret_cast<float*>(smem)), tt(p.tt), u_cand(p.t_cand * p.t_cand) {}
   __device__ void init(int tid, int nthr) {
     if (tsm) tt = screen_to_smem(Pr.tt, tsm, tid, nthr);
@@ -970,10 +1002,15 @@ struct LmmGroupEpi {
     gene = g;
     snp0 = s0;
     gvalid = g < Pr.G;
+    if constexpr (GLM) gvalid = gvalid && Pr.gene_ok[g];
     acc.reset();
     if (gvalid) {
-      const double r = Pr.rss_null[g];
-      inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
+      if constexpr (GLM) {
+        rs = Pr.rsum[g];
+      } else {
+        const double r = Pr.rss_null[g];
+        inv_rss = r > 0 ? static_cast<float>(1.0 / r) : 0.0f;
+      }
       acc.load_window(Pr.win, g);
     }
   }
@@ -1003,10 +1040,16 @@ struct LmmGroupEpi {
     for (int j = 0; j < 16; ++j) {
       const int64_t s = s0 + j;
       const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
-      const float r = num[j] * __fdividef(num[j], S[j]) * inv_rss;
-      const float omr = 1.0f - r;
-      const bool ok_stat = S[j] > 1e-15f && omr > 0.0f;
-      const float u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      float u;
+      if constexpr (GLM) {
+        const float U = fmaf(__ldg(Pr.snp_mean + s), rs, num[j]);
+        u = S[j] > 1e-15f ? __fdividef(U * U, S[j]) : 0.0f;  // z^2
+      } else {
+        const float r = num[j] * __fdividef(num[j], S[j]) * inv_rss;
+        const float omr = 1.0f - r;
+        const bool ok_stat = S[j] > 1e-15f && omr > 0.0f;
+        u = ok_stat ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2
+      }
       const ScreenOut o = acat_screen_u(u, tt);
       acc.add_screen(o, s, valid);
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
@@ -1018,6 +1061,9 @@ struct LmmGroupEpi {
   }
   __device__ void finish() {}
 };
+
+using LmmGroupEpi = LmmGroupEpiT<false>;
+using GlmGroupEpi = LmmGroupEpiT<true>;
 
 // subset gate for the LMM scan (src/scan_common.cpp:133-151)
 __global__ void snp_gate_kernel(const int64_t* __restrict__ kept, int64_t m, int n, const double* __restrict__ mu,
@@ -1188,6 +1234,18 @@ struct EpiOf<dev::LmmEpiParams<2>> {
 template <>
 struct EpiOf<dev::LmmGroupEpiParams> {
   using type = dev::LmmGroupEpi;
+};
+template <>
+struct EpiOf<dev::GlmEpiParams<1>> {
+  using type = dev::LmmEpi<1, true>;
+};
+template <>
+struct EpiOf<dev::GlmEpiParams<2>> {
+  using type = dev::LmmEpi<2, true>;
+};
+template <>
+struct EpiOf<dev::GlmGroupEpiParams> {
+  using type = dev::GlmGroupEpi;
 };
 
 using namespace dev;
@@ -1469,9 +1527,13 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
 
 // ------------------------------------------------------------------- scan
 template <int P>
-static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah, const __half* const* al,
-                       int G, bool simt, const int2* tiles, int n_tiles) {
-  Rotated& R = ctx->rot;
+static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah,
+                            const __half* const* al, int G, const __half* const* bh, const __half* const* bl,
+                            const int* bsel, const Rotated& R);
+
+template <int P, class EP>
+static void lmm_launch(eqtl_ctx* ctx, const EP& ep, const __half* const* ah, const __half* const* al, int G,
+                       bool simt, const int2* tiles, int n_tiles, const Rotated& R) {
   const __half* bh[2] = {R.gt_hi.p, R.gt2_hi.p};
   const __half* bl[2] = {R.gt_lo.p, R.gt2_lo.p};
   // tile order [gg, a_0 .. a_{P-1}, NUM] from the gene-ops order [NUM, a.., gg]
@@ -1491,7 +1553,14 @@ static void lmm_launch(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* c
     launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod, tiles, n_tiles);
     return;
   }
-  // plain FP32 CUDA-core comparator
+  if constexpr (std::is_same_v<EP, LmmEpiParams<P>>) lmm_launch_simt<P>(ctx, ep, ah, al, G, bh, bl, bsel, R);
+}
+
+// the plain FP32 CUDA-core comparator of the LMM scan
+template <int P>
+static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah,
+                            const __half* const* al, int G, const __half* const* bh, const __half* const* bl,
+                            const int* bsel, const Rotated& R) {
   cudaStream_t st = ctx->stream;
   const __half* ptrs[2 * (P + 2) + 4];
   for (int j = 0; j < P + 2; ++j) {
@@ -1720,14 +1789,14 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
       fill(ep);
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<1>(ctx, ep, ah, al, G, simt, tiles, n_tiles);
+        lmm_launch<1>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
       });
     } else {
       LmmEpiParams<2> ep{};
       fill(ep);
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<2>(ctx, ep, ah, al, G, simt, tiles, n_tiles);
+        lmm_launch<2>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
       });
     }
   }
@@ -1798,6 +1867,552 @@ void test_pairs_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y,
     ws.delta.download(delta_out, G, ctx->stream);
     EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
   }
+}
+
+
+// ================================================================ NB GLM
+// The NB-GLM score test (src/model_glm.cpp:13-132) on the LMM scan's
+// machinery: the null fit of every gene on the device (glm_null_kernel), the
+// gene-side operands w, w o x_k (or w o (X U)_k, U U' = (X'WX)^-1, for
+// p > 2) and r against the unrotated centred dosages gc and gc^2, the
+// score-test epilogues (LmmEpi<P, true>, GlmGroupEpi), and the FP64
+// refinement of every candidate from the exact dosages (glm_refine_kernel).
+namespace dev {
+
+constexpr int kGlmThreads = 256;
+
+// Null NB2 fit of one gene per block (nb_irls + prep_glm_nb, src/model_glm.cpp:
+// 28-96): from beta = 0, mu = max(y, 0.1), phi = 1, IRLS at fixed phi (at most
+// 50 rounds, until max |beta change| < 1e-6; w = m^2 / (m + phi m^2),
+// z = log m + (y - m) / m, m = max(mu, 1e-8)), then phi by moments
+// (sum ((y - m)^2 - m) / m^2 / max(1, n - p), at least 1e-8), until phi moves
+// by less than 1e-6 max(1, phi) (at most 10 rounds). The sums of X'WX and X'Wz
+// are warp dot products over the samples (warp w takes items w, w + 8, ...);
+// thread 0 factorises and solves. Outputs per gene: W = m / (1 + phi m),
+// R = (y - mu) / (1 + phi mu), (X'WX)^-1, phi, sum R, ok (every X'WX
+// factorised) and counts (every y a non-negative integer within 1e-8).
+// MU and R double as the fit's mu and z.
+__global__ void __launch_bounds__(kGlmThreads)
+    glm_null_kernel(const double* __restrict__ Y, const double* __restrict__ X, int n, int p, int G, double* MU,
+                    double* W, double* R, double* phi_out, double* ainv_out, double* rsum_out, uint8_t* ok_out,
+                    uint8_t* counts_out) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  __shared__ double A[kMaxPLmm * kMaxPLmm];
+  __shared__ double rhs[kMaxPLmm], beta[kMaxPLmm], sol[kMaxPLmm];
+  __shared__ double red[kGlmThreads / 32];
+  __shared__ double s_phi, s_diff;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nw = kGlmThreads / 32;
+  const double* y = Y + static_cast<int64_t>(g) * n;
+  double* mu = MU + static_cast<int64_t>(g) * n;
+  double* w = W + static_cast<int64_t>(g) * n;
+  double* z = R + static_cast<int64_t>(g) * n;
+  auto block_sum = [&](double v) -> double {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();  // red[] of the previous sum has been read
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0;
+    for (int k = 0; k < nw; ++k) t += red[k];
+    return t;
+  };
+  // X'WX (lower triangle, items 0 .. p(p+1)/2 - 1) and, with rhs, X'Wz
+  const int n_tri = p * (p + 1) / 2;
+  auto weighted_sums = [&](bool with_rhs) {
+    const int items = n_tri + (with_rhs ? p : 0);
+    for (int item = warp; item < items; item += nw) {
+      int a = 0, b = 0;
+      const bool is_rhs = item >= n_tri;
+      if (is_rhs) {
+        a = item - n_tri;
+      } else {
+        while ((a + 1) * (a + 2) / 2 <= item) ++a;
+        b = item - a * (a + 1) / 2;
+      }
+      const double* xa = X + static_cast<int64_t>(a) * n;
+      const double* xb = X + static_cast<int64_t>(b) * n;
+      double acc = 0;
+      for (int i = lane; i < n; i += 32) acc += xa[i] * w[i] * (is_rhs ? z[i] : xb[i]);
+      for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) {
+        if (is_rhs) {
+          rhs[a] = acc;
+        } else {
+          A[a * p + b] = acc;
+          A[b * p + a] = acc;
+        }
+      }
+    }
+  };
+  // thread 0: lower Cholesky factor of A in place; false if A is not
+  // positive definite
+  auto cholesky = [&]() -> bool {
+    for (int j = 0; j < p; ++j) {
+      double d = A[j * p + j];
+      for (int k = 0; k < j; ++k) d -= A[j * p + k] * A[j * p + k];
+      if (!(d > 0)) return false;
+      d = sqrt(d);
+      A[j * p + j] = d;
+      for (int i = j + 1; i < p; ++i) {
+        double v = A[i * p + j];
+        for (int k = 0; k < j; ++k) v -= A[i * p + k] * A[j * p + k];
+        A[i * p + j] = v / d;
+      }
+    }
+    return true;
+  };
+  // thread 0: sol = (L L')^-1 v with the factor in A's lower triangle
+  auto solve = [&](const double* v) {
+    for (int i = 0; i < p; ++i) {
+      double t = v[i];
+      for (int k = 0; k < i; ++k) t -= A[i * p + k] * sol[k];
+      sol[i] = t / A[i * p + i];
+    }
+    for (int i = p - 1; i >= 0; --i) {
+      double t = sol[i];
+      for (int k = i + 1; k < p; ++k) t -= A[k * p + i] * sol[k];
+      sol[i] = t / A[i * p + i];
+    }
+  };
+
+  double bad = 0;
+  for (int i = tid; i < n; i += kGlmThreads) {
+    const double v = y[i];
+    if (isfinite(v) && (v < 0 || fabs(v - floor(v)) > 1e-8)) bad = 1;
+    mu[i] = fmax(v, 0.1);
+  }
+  const double n_bad = block_sum(bad);
+  if (tid < p) beta[tid] = 0.0;
+  if (tid == 0) {
+    s_phi = 1.0;
+    s_fail = 0;
+  }
+  __syncthreads();
+  const int df = n - p > 1 ? n - p : 1;
+  for (int outer = 0; outer < 10; ++outer) {
+    for (int it = 0; it < 50; ++it) {
+      const double phi = s_phi;
+      for (int i = tid; i < n; i += kGlmThreads) {
+        const double m = fmax(mu[i], 1e-8);
+        const double var = m + phi * m * m;
+        w[i] = (m * m) / fmax(var, 1e-12);
+        z[i] = log(m) + (y[i] - m) / m;
+      }
+      __syncthreads();
+      weighted_sums(true);
+      __syncthreads();
+      if (tid == 0) {
+        if (!cholesky()) {
+          s_fail = 1;
+        } else {
+          solve(rhs);
+          double diff = 0;
+          for (int k = 0; k < p; ++k) {
+            diff = fmax(diff, fabs(sol[k] - beta[k]));
+            beta[k] = sol[k];
+          }
+          s_diff = diff;
+        }
+      }
+      __syncthreads();
+      if (s_fail) break;
+      for (int i = tid; i < n; i += kGlmThreads) {
+        double e = 0;
+        for (int k = 0; k < p; ++k) e += X[static_cast<int64_t>(k) * n + i] * beta[k];
+        mu[i] = exp(e);
+      }
+      __syncthreads();
+      if (s_diff < 1e-6) break;
+    }
+    if (s_fail) break;
+    double part = 0;
+    for (int i = tid; i < n; i += kGlmThreads) {
+      const double m = fmax(mu[i], 1e-8);
+      part += ((y[i] - m) * (y[i] - m) - m) / (m * m);
+    }
+    const double phi_new = fmax(1e-8, block_sum(part) / df);
+    const double phi = s_phi;
+    __syncthreads();
+    if (tid == 0) s_phi = phi_new;
+    __syncthreads();
+    if (fabs(phi_new - phi) < 1e-6 * fmax(1.0, phi)) break;
+  }
+  // the fitted null's weights, residuals and (X'WX)^-1
+  const double phi = s_phi;
+  double rpart = 0;
+  for (int i = tid; i < n; i += kGlmThreads) {
+    const double m = fmax(mu[i], 1e-8);
+    w[i] = m / (1.0 + phi * m);
+    const double r = (y[i] - mu[i]) / (1.0 + phi * mu[i]);
+    z[i] = r;
+    rpart += r;
+  }
+  const double rs = block_sum(rpart);
+  weighted_sums(false);
+  __syncthreads();
+  if (tid == 0) {
+    const bool fact = cholesky();
+    double* ai = ainv_out + static_cast<int64_t>(g) * p * p;
+    for (int c = 0; c < p; ++c) {
+      for (int k = 0; k < p; ++k) rhs[k] = k == c ? 1.0 : 0.0;
+      if (fact) solve(rhs);
+      for (int k = 0; k < p; ++k) ai[k * p + c] = fact ? sol[k] : 0.0;
+    }
+    phi_out[g] = phi;
+    rsum_out[g] = rs;
+    ok_out[g] = (!s_fail && fact) ? 1 : 0;
+    counts_out[g] = n_bad == 0 ? 1 : 0;
+  }
+}
+
+// Gene-side operands of the GLM scan in the LMM kernels' layout (see
+// lmm_gene_ops_kernel / lmm_gene_ops_orth_kernel): order [NUM, a_0 ..
+// a_{p-1}, gg] = [r, w x_k, w] for p <= 2, [NUM, gg, a~_0 ..] = [r, w,
+// w (X U)_k] for the grouped scan, U the lower Cholesky factor of
+// (X'WX)^-1; each scaled to a power of two and split into FP16 hi + lo.
+__global__ void glm_gene_ops_kernel(const double* __restrict__ W, const double* __restrict__ Rr,
+                                    const double* __restrict__ X, const double* __restrict__ ainv, int n, int p, int G,
+                                    int k_pad, float s1, float s2, int grouped, __half* const* hi, __half* const* lo,
+                                    float* unscale) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const int nops = p + 2;
+  __shared__ double mx[kMaxPLmm + 2][8];
+  __shared__ double sc[kMaxPLmm + 2];
+  __shared__ double U[kMaxPLmm * kMaxPLmm];
+  if (grouped && threadIdx.x == 0) {
+    const double* A = ainv + static_cast<int64_t>(g) * p * p;
+    for (int j = 0; j < p; ++j) {
+      double d = A[j * p + j];
+      for (int k = 0; k < j; ++k) d -= U[j * p + k] * U[j * p + k];
+      d = d > 0 ? sqrt(d) : 0.0;
+      U[j * p + j] = d;
+      for (int i = j + 1; i < p; ++i) {
+        double v = A[i * p + j];
+        for (int k = 0; k < j; ++k) v -= U[i * p + k] * U[j * p + k];
+        U[i * p + j] = d > 0 ? v / d : 0.0;
+      }
+      for (int i = 0; i < j; ++i) U[i * p + j] = 0.0;
+    }
+  }
+  __syncthreads();
+  const double* wg = W + static_cast<int64_t>(g) * n;
+  const double* rg = Rr + static_cast<int64_t>(g) * n;
+  const int gg_op = grouped ? 1 : nops - 1;
+  auto value = [&](int op, int i) -> double {
+    if (i >= n) return 0.0;
+    if (op == 0) return rg[i];
+    if (op == gg_op) return wg[i];
+    if (!grouped) return wg[i] * X[static_cast<int64_t>(op - 1) * n + i];
+    const int k = op - 2;
+    double v = 0;
+    for (int l = k; l < p; ++l) v += X[static_cast<int64_t>(l) * n + i] * U[l * p + k];
+    return wg[i] * v;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int op = 0; op < nops; ++op) {
+    double m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(value(op, i)));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) mx[op][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < nops) {
+    double m = 0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) m = fmax(m, mx[threadIdx.x][w]);
+    int e = 0;
+    if (m > 0) e = 10 - static_cast<int>(floor(log2(m)));
+    sc[threadIdx.x] = ldexp(1.0, e);
+    const double side = static_cast<int>(threadIdx.x) == gg_op ? s2 : s1;
+    unscale[static_cast<int64_t>(g) * nops + threadIdx.x] = static_cast<float>(1.0 / (ldexp(1.0, e) * side));
+  }
+  __syncthreads();
+  for (int op = 0; op < nops; ++op) {
+    const double sv = sc[op];
+    for (int i = threadIdx.x; i < k_pad; i += blockDim.x) {
+      const double v = value(op, i) * sv;
+      const __half h = __double2half(v);
+      hi[op][static_cast<int64_t>(g) * k_pad + i] = h;
+      lo[op][static_cast<int64_t>(g) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+    }
+  }
+}
+
+// SNP-side operands of the GLM scan: gc * s1 and gc^2 * s2 from the centred
+// dosage operand (gc_hi + gc_lo = (dosage - mean) * inv_gc^-1), FP16 hi + lo.
+__global__ void glm_snp_ops_kernel(const __half* __restrict__ gc_hi, const __half* __restrict__ gc_lo, int64_t elems,
+                                   double inv_gc, float s1, float s2, __half* gh, __half* gl, __half* g2h,
+                                   __half* g2l) {
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < elems;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = (static_cast<double>(__half2float(gc_hi[e])) + static_cast<double>(__half2float(gc_lo[e]))) *
+                     inv_gc;
+    const double a = v * s1, b = v * v * s2;
+    const __half ah = __double2half(a), bh = __double2half(b);
+    gh[e] = ah;
+    gl[e] = __double2half(a - static_cast<double>(__half2float(ah)));
+    g2h[e] = bh;
+    g2l[e] = __double2half(b - static_cast<double>(__half2float(bh)));
+  }
+}
+
+// FP32 imputation mean of every kept SNP (zero past m), and FP32 sum r
+__global__ void glm_means_kernel(const int64_t* __restrict__ kept, int64_t m, const double* __restrict__ mu,
+                                 int64_t padded, float* mean_f, const double* __restrict__ rsum, int G, float* rsum_f) {
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < padded;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    mean_f[r] = r < m ? static_cast<float>(mu[kept[r]]) : 0.0f;
+    if (r < G) rsum_f[r] = static_cast<float>(rsum[r]);
+  }
+}
+
+// One warp per (gene, kept SNP) pair: the score test in FP64 from the exact
+// mean-imputed dosages g, as test_glm_nb computes it: U = g'r, g'Wg,
+// X'Wg, and the dosage variance (mean of squares - squared mean).
+__global__ void glm_refine_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                  const int64_t* __restrict__ kept, const double* __restrict__ mu_imp,
+                                  const double* __restrict__ W, const double* __restrict__ Rr,
+                                  const double* __restrict__ X, int p, const double* __restrict__ ainv,
+                                  const int2* __restrict__ pairs, int n_pairs, eqtl_pair* out) {
+  const int lane = threadIdx.x & 31;
+  const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (wid >= n_pairs) return;
+  const int g = pairs[wid].x;
+  const int64_t r = pairs[wid].y;
+  const int64_t s = kept[r];
+  const double mus = mu_imp[s];
+  const double* wg = W + static_cast<int64_t>(g) * n;
+  const double* rg = Rr + static_cast<int64_t>(g) * n;
+  double U = 0, gwg = 0, sd = 0, sd2 = 0, xw[kMaxPLmm];
+#pragma unroll
+  for (int k = 0; k < kMaxPLmm; ++k) xw[k] = 0;
+  for (int i = lane; i < n; i += 32) {
+    double d = src.dosage(s, col[i]);
+    if (isnan(d)) d = mus;
+    const double wd = wg[i] * d;
+    U += d * rg[i];
+    gwg += wd * d;
+    sd += d;
+    sd2 += d * d;
+#pragma unroll
+    for (int k = 0; k < kMaxPLmm; ++k)
+      if (k < p) xw[k] += X[static_cast<int64_t>(k) * n + i] * wd;
+  }
+  for (int o = 16; o; o >>= 1) {
+    U += __shfl_xor_sync(0xffffffffu, U, o);
+    gwg += __shfl_xor_sync(0xffffffffu, gwg, o);
+    sd += __shfl_xor_sync(0xffffffffu, sd, o);
+    sd2 += __shfl_xor_sync(0xffffffffu, sd2, o);
+#pragma unroll
+    for (int k = 0; k < kMaxPLmm; ++k)
+      if (k < p) xw[k] += __shfl_xor_sync(0xffffffffu, xw[k], o);
+  }
+  if (lane) return;
+  const double* A = ainv + static_cast<int64_t>(g) * p * p;
+  double xAx = 0;
+  for (int a = 0; a < p; ++a) {
+    double t = 0;
+    for (int b = 0; b < p; ++b) t += A[a * p + b] * xw[b];
+    xAx += xw[a] * t;
+  }
+  const double mean = sd / n;
+  eqtl_pair q;
+  q.snp = r;
+  q.gene = g;
+  q.reserved = 0;
+  glm_stats_fp64(U, gwg, xAx, sd2 / n - mean * mean, q);
+  out[wid] = q;
+}
+
+}  // namespace dev
+
+static std::vector<eqtl_pair> glm_refine_pairs(eqtl_ctx* ctx, int p, const std::vector<int2>& todo) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  std::vector<eqtl_pair> refined(todo.size());
+  if (todo.empty()) return refined;
+  ws.ref_pairs.upload(todo.data(), todo.size(), st);
+  ws.refined.alloc(todo.size());
+  const int n_pairs = static_cast<int>(todo.size());
+  ++ctx->launches;
+  glm_refine_kernel<<<static_cast<unsigned>((n_pairs + 7) / 8), 256, 0, st>>>(
+      g.rows(), g.col.p, g.n, g.kept.p, g.mu.p, ws.glm_w.p, ws.glm_r.p, ctx->pheno.X.p, p, ws.ainv.p,
+      ws.ref_pairs.p, n_pairs, ws.refined.p);
+  EQTL_CUDA(cudaGetLastError());
+  ws.refined.download(refined.data(), refined.size(), st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  // a gene whose null fit failed tests nothing (p = NaN, test_glm_nb)
+  std::vector<uint8_t> ok(ctx->pheno.G);
+  ws.glm_ok.download(ok.data(), ok.size(), st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  for (eqtl_pair& q : refined)
+    if (!ok[q.gene]) q.p = std::numeric_limits<double>::quiet_NaN();
+  return refined;
+}
+
+void scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* phi_out,
+              uint8_t* converged_out, eqtl_gene_result* genes, std::vector<eqtl_pair>& pairs,
+              std::vector<eqtl_pair>& cands) {
+  Geno& g = ctx->geno;
+  Workspace& ws = ctx->ws;
+  const int n = prm->n, G = prm->n_genes, p = prm->p;
+  EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_glm: no genotypes loaded");
+  EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_glm: n differs from the loaded genotypes");
+  EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_glm: no genes");
+  EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_glm: more than 2^30 kept SNPs");
+  EQTL_CHECK(p >= 1 && p <= kMaxPLmm, EQTL_E_UNSUPPORTED,
+             "the GLM scan handles 1 to 32 covariate columns (intercept included)");
+  EQTL_CHECK(ctx->precision == EQTL_PREC_SPLIT_F16, EQTL_E_UNSUPPORTED, "the GLM scan runs split-FP16");
+  const bool grouped = p > 2;
+  cudaStream_t st = ctx->stream;
+  const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
+  std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
+  // ---- null fits
+  const size_t gn = static_cast<size_t>(G) * n;
+  ws.glm_mu.alloc(gn);
+  ws.glm_w.alloc(gn);
+  ws.glm_r.alloc(gn);
+  ws.glm_phi.alloc(G);
+  ws.glm_rsum.alloc(G);
+  ws.glm_ok.alloc(G);
+  ws.glm_counts.alloc(G);
+  ws.ainv.alloc(static_cast<size_t>(G) * p * p);
+  ++ctx->launches;
+  glm_null_kernel<<<G, kGlmThreads, 0, st>>>(ph.Y.p, ph.X.p, n, p, G, ws.glm_mu.p, ws.glm_w.p, ws.glm_r.p,
+                                             ws.glm_phi.p, ws.ainv.p, ws.glm_rsum.p, ws.glm_ok.p, ws.glm_counts.p);
+  EQTL_CUDA(cudaGetLastError());
+  {
+    std::vector<uint8_t> counts(G), ok(G);
+    ws.glm_counts.download(counts.data(), G, st);
+    ws.glm_ok.download(ok.data(), G, st);
+    if (phi_out) ws.glm_phi.download(phi_out, G, st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+    for (int j = 0; j < G; ++j)
+      EQTL_CHECK(counts[j], EQTL_E_ARG, "glm (NB) requires non-negative integer counts (column " + std::to_string(j) + ")");
+    if (converged_out) std::copy(ok.begin(), ok.end(), converged_out);
+  }
+  // ---- SNP-side operands (unrotated), means and gene-side operands
+  Rotated& S = ctx->glm_ops;
+  const int k_pad = g.k_pad;
+  const int64_t m = g.m;
+  float s1, s2;
+  output_scales(n, s1, s2);
+  if (!(S.m == m && S.k_pad == k_pad && S.gt_hi.p)) {
+    const size_t elems = static_cast<size_t>(m) * k_pad;
+    S.gt_hi.alloc(elems);
+    S.gt_lo.alloc(elems);
+    S.gt2_hi.alloc(elems);
+    S.gt2_lo.alloc(elems);
+    if (elems) {
+      ++ctx->launches;
+      glm_snp_ops_kernel<<<static_cast<unsigned>(std::min<int64_t>((elems + 255) / 256, 148 * 64)), 256, 0, st>>>(
+          g.gc_hi.p, g.gc_lo.p, static_cast<int64_t>(elems), 1.0 / kGcScale, s1, s2, S.gt_hi.p, S.gt_lo.p,
+          S.gt2_hi.p, S.gt2_lo.p);
+      EQTL_CUDA(cudaGetLastError());
+    }
+    S.m = m;
+    S.k_pad = k_pad;
+  }
+  const int64_t padded = ((m + 255) / 256 + 1) * 256;
+  ws.snp_mean.alloc(static_cast<size_t>(std::max<int64_t>(padded, G)));
+  ws.glm_rsum_f.alloc(G);
+  ++ctx->launches;
+  glm_means_kernel<<<static_cast<unsigned>(std::min<int64_t>((std::max<int64_t>(padded, G) + 255) / 256, 4096)), 256,
+                     0, st>>>(g.kept.p, m, g.mu.p, std::max<int64_t>(padded, G), ws.snp_mean.p, ws.glm_rsum.p, G,
+                              ws.glm_rsum_f.p);
+  EQTL_CUDA(cudaGetLastError());
+  const int nops = p + 2;
+  std::vector<__half*> oph(2 * nops);
+  for (int k = 0; k < nops; ++k) {
+    ws.ops_hi[k].alloc(static_cast<size_t>(G) * k_pad);
+    ws.ops_lo[k].alloc(static_cast<size_t>(G) * k_pad);
+    oph[k] = ws.ops_hi[k].p;
+    oph[nops + k] = ws.ops_lo[k].p;
+  }
+  ws.ops_ptr.upload(oph.data(), oph.size(), st);
+  ws.unscale.alloc(static_cast<size_t>(G) * nops);
+  ++ctx->launches;
+  glm_gene_ops_kernel<<<G, 256, 0, st>>>(ws.glm_w.p, ws.glm_r.p, ph.X.p, ws.ainv.p, n, p, G, k_pad, s1, s2,
+                                         grouped ? 1 : 0, ws.ops_ptr.p, ws.ops_ptr.p + nops, ws.unscale.p);
+  EQTL_CUDA(cudaGetLastError());
+  lmm_gate(ctx);
+  const Windows win =
+      upload_windows(ctx, prm, m, prm->exclude_cis == 2 ? kWinInclude : prm->exclude_cis ? kWinExclude : kWinNone);
+  double z_cand = z_critical(prm->pthr);
+  if (prm->perm_thr > 0) z_cand = std::min(z_cand, z_critical(prm->perm_thr));
+  const TTable tt = device_ttable(ctx, 0.0, true);
+  prep_timer.reset();
+  // ---- scan
+  ScanOutputs so(ctx, G, m, expected_candidates(prm, m));
+  const int2* tiles = nullptr;
+  int n_tiles = 0;
+  cis_tile_list(ctx, prm, m, grouped ? GlmGroupEpi::kTileN : 128, tiles, n_tiles);
+  std::unique_ptr<StageScope> scan_timer(new StageScope(ctx, EQTL_STAGE_SCAN));
+  if (m > 0 && grouped) {
+    GlmGroupEpiParams ep{};
+    ep.G = G;
+    ep.m = m;
+    ep.n_acc = nops;
+    ep.unscale = ws.unscale.p;
+    ep.snp_ok = ws.ok.p;
+    ep.win = win;
+    ep.t_cand = static_cast<float>(z_cand * (1.0 - 1e-3));
+    ep.tt = tt;
+    ep.snp_mean = ws.snp_mean.p;
+    ep.rsum = ws.glm_rsum_f.p;
+    ep.gene_ok = ws.glm_ok.p;
+    const __half* bh[2] = {S.gt_hi.p, S.gt2_hi.p};
+    const __half* bl[2] = {S.gt_lo.p, S.gt2_lo.p};
+    std::vector<int> bsel(nops, 0), prod(nops, 7);
+    bsel[1] = 1;  // gg reads gc^2
+    so.run([&](GeneOut out) {
+      ep.out = out;
+      launch_tile_n<GlmGroupEpi::kTileN, 4>(ctx, false, ep, oph.data(), oph.data() + nops, G, bh, bl, S.m, S.k_pad,
+                                            bsel.data(), prod.data(), tiles, n_tiles, 1, nops);
+    });
+  } else if (m > 0) {
+    const __half* ah[4] = {oph[0], oph[1], oph[2], nops > 3 ? oph[3] : oph[2]};
+    const __half* al[4] = {oph[nops + 0], oph[nops + 1], oph[nops + 2], nops > 3 ? oph[nops + 3] : oph[nops + 2]};
+    auto fill = [&](auto& ep) {
+      ep.G = G;
+      ep.m = m;
+      ep.unscale = ws.unscale.p;
+      ep.ainv = ws.ainv.p;
+      ep.snp_ok = ws.ok.p;
+      ep.win = win;
+      ep.t_cand = static_cast<float>(z_cand * (1.0 - 1e-3));
+      ep.tt = tt;
+      ep.snp_mean = ws.snp_mean.p;
+      ep.rsum = ws.glm_rsum_f.p;
+      ep.gene_ok = ws.glm_ok.p;
+    };
+    if (p == 1) {
+      GlmEpiParams<1> ep{};
+      fill(ep);
+      so.run([&](GeneOut out) {
+        ep.out = out;
+        lmm_launch<1>(ctx, ep, ah, al, G, false, tiles, n_tiles, S);
+      });
+    } else {
+      GlmEpiParams<2> ep{};
+      fill(ep);
+      so.run([&](GeneOut out) {
+        ep.out = out;
+        lmm_launch<2>(ctx, ep, ah, al, G, false, tiles, n_tiles, S);
+      });
+    }
+  }
+  scan_timer.reset();
+  std::vector<int2> todo, deferred;
+  so.collect(genes, todo, deferred);
+  // ---- FP64 refinement of the candidates, deferred and tiny-|z| pairs
+  StageScope refine_timer(ctx, EQTL_STAGE_REFINE);
+  const std::vector<eqtl_pair> refined = glm_refine_pairs(ctx, p, todo);
+  add_deferred_acat(genes, refined, deferred);
+  finish_scan(prm, genes, refined, pairs, cands);
 }
 
 }  // namespace eqtl

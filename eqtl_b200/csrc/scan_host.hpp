@@ -32,7 +32,9 @@ void finish_scan(const eqtl_scan_params* prm, eqtl_gene_result* genes, const std
 dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int mode);
 
 // Device t-tail table for `df`, cached in the context workspace.
-dev::TTable device_ttable(eqtl_ctx* ctx, double df);
+// Device tables of the two-sided t tail with `df` residual degrees of
+// freedom, or of the normal tail (normal = true; df is then ignored).
+dev::TTable device_ttable(eqtl_ctx* ctx, double df, bool normal = false);
 bool cis_tile_list(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t m, int NT, const int2*& list, int& n_list);
 
 // Resolves the phenotypes of a scan call: uploads (Y, X) when given,

@@ -69,6 +69,31 @@ EQTL_HD double t_two_sided_p(double t, double df) {
   return fmin(1.0, fmax(0.0, p));
 }
 
+// Two-sided normal tail P(|Z| > |z|) = erfc(|z| / sqrt 2), clipped to
+// [0, 1]; 1 for a z that is not finite (pnorm_two_sided, src/util.cpp:116-123).
+EQTL_HD double z_two_sided_p(double z) {
+  if (!isfinite(z)) return 1.0;
+  const double p = erfc(fabs(z) / sqrt(2.0));
+  return fmin(1.0, fmax(0.0, p));
+}
+
+// NB-GLM score test of one pair (test_glm_nb, src/model_glm.cpp:98-132) from
+// U = g'r, gwg = g'Wg, the quadratic form xAx = (X'Wg)' (X'WX)^-1 (X'Wg) and
+// the SNP's dosage variance over the samples: beta = U / info,
+// se = 1 / sqrt(info), stat = U / sqrt(info), with info = gwg - xAx; p = 1
+// (the rest 0) for gvar or info below 1e-12.
+EQTL_HD void glm_stats_fp64(double U, double gwg, double xAx, double gvar, eqtl_pair& q) {
+  q.beta = q.se = q.t = q.r2 = 0.0;
+  q.p = 1.0;
+  if (gvar < 1e-12) return;
+  const double info = gwg - xAx;
+  if (info < 1e-12) return;
+  q.beta = U / info;
+  q.se = 1.0 / sqrt(info);
+  q.t = U / sqrt(info);
+  q.p = z_two_sided_p(q.t);
+}
+
 // LM pair from gtg = |g_s|^2, gty = g_s . y_s, yty = |y_s|^2.
 EQTL_HD void lm_stats_fp64(double gtg, double gty, double yty, double df, eqtl_pair& q) {
   q.beta = q.se = q.t = q.r2 = 0.0;

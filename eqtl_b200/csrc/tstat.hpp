@@ -33,8 +33,30 @@ inline double t_critical(double pthr, double df) {
   return hi;
 }
 
+// |z| at which the two-sided normal p equals pthr.
+inline double z_critical(double pthr) {
+  if (!(pthr > 0)) return std::numeric_limits<double>::infinity();
+  if (pthr >= 1) return 0.0;
+  double lo = 0.0, hi = 1.0;
+  while (z_two_sided_p(hi) > pthr && hi < 1e30) hi *= 2;
+  for (int i = 0; i < 200; ++i) {
+    const double mid = 0.5 * (lo + hi);
+    if (z_two_sided_p(mid) > pthr) lo = mid;
+    else hi = mid;
+  }
+  return hi;
+}
+
+// The tail variable of a normal table: x = sqrt(log1p(z^2 / kZTableD)). Any
+// scale works (ln p is analytic in x); this one spreads z in [1, 38] over x
+// in [0.01, 0.37].
+constexpr double kZTableD = 1e4;
+
 // Interpolation tables for the device t tail (layout documented in tdist.cuh).
+// A table built with normal = true holds the two-sided normal tail instead
+// (the NB-GLM score statistic), with df = kZTableD as the tail scale.
 struct TTableHost {
+  bool normal = false;
   double df = 0;
   double t0 = 1.0;               // central / tail boundary in |t|
   int na = 512;                  // central intervals over u = t^2 in [0, t0^2]
@@ -105,18 +127,38 @@ inline double zcotz(double w) {
   return y * std::cosh(y) / std::sinh(y);
 }
 
-inline TTableHost build_ttable(double df) {
+// The normal counterpart of central_h: 1 - p = |z| h(z^2) with
+// h(u) = 2 phi0 \int_0^1 exp(-x^2 u / 2) dx, phi0 = 1 / sqrt(2 pi).
+inline double central_h_normal(double u) {
+  static std::vector<double> xg, wg;
+  if (xg.empty()) gauss_legendre(24, xg, wg);
+  double acc = 0;
+  for (int seg = 0; seg < 4; ++seg) {
+    const double a = 0.25 * seg, hw = 0.125;
+    for (size_t i = 0; i < xg.size(); ++i) {
+      const double xx = a + hw + hw * xg[i];
+      acc += hw * wg[i] * std::exp(-0.5 * xx * xx * u);
+    }
+  }
+  return 2.0 * acc / std::sqrt(2.0 * M_PI);
+}
+
+inline TTableHost build_ttable(double df, bool normal = false) {
   TTableHost T;
+  T.normal = normal;
+  if (normal) df = kZTableD;
   T.df = df;
+  auto pfun = [&](double t) { return normal ? z_two_sided_p(t) : t_two_sided_p(t, df); };
+  auto hfun = [&](double u) { return normal ? central_h_normal(u) : central_h(u, df); };
   // p(t0) < 1/2 keeps the tail's tan term away from 0 (df = 1 has p(1) = 1/2)
-  T.t0 = df < 1.5 ? 1.5 : 1.0;
+  T.t0 = !normal && df < 1.5 ? 1.5 : 1.0;
   const double du = (T.t0 * T.t0) / T.na;
   T.h.resize(T.na + 4);
-  for (int k = 0; k < T.na + 4; ++k) T.h[k] = static_cast<float>(central_h((k - 1) * du, df));
+  for (int k = 0; k < T.na + 4; ++k) T.h[k] = static_cast<float>(hfun((k - 1) * du));
   T.x0 = std::sqrt(std::log1p(T.t0 * T.t0 / df));
   auto lnp = [&](double x) {
     const double t = std::sqrt(df * std::expm1(x * x));
-    const double p = t_two_sided_p(t, df);
+    const double p = pfun(t);
     return p > 0 ? std::log(p) : -1e30;
   };
   // x_end: where ln p reaches ln(1e-320) (beyond it the reference's p
@@ -154,17 +196,17 @@ inline TTableHost build_ttable(double df) {
   T.c1.resize(T.na + 4);
   for (int k = 0; k < T.na + 4; ++k) {
     const double u = (k - 1) * du;
-    const double h = central_h(u, df);
+    const double h = hfun(u);
     T.c1[k] = static_cast<float>(-zcotz(M_PI * M_PI * u * h * h) / (M_PI * h));
   }
-  T.t_defer = t_critical(1e-14, df);
+  T.t_defer = normal ? z_critical(1e-14) : t_critical(1e-14, df);
   T.x_defer = std::sqrt(std::log1p(T.t_defer * T.t_defer / df));
   const double dl = (T.x_defer - T.x0) / T.nb;
   T.lt.resize(T.nb + 4);
   for (int k = 0; k < T.nb + 4; ++k) {
     const double x = T.x0 + (k - 1) * dl;
     const double t = std::sqrt(df * std::expm1(x * x));
-    const double p = t_two_sided_p(t, df);
+    const double p = pfun(t);
     T.lt[k] = static_cast<float>(std::log(std::cos(M_PI * p) / std::sin(M_PI * p)));
   }
   return T;

@@ -25,6 +25,7 @@ struct Fatal : std::runtime_error {
 };
 [[noreturn]] void die(const std::string& msg);
 void info(const std::string& msg);
+void warn(const std::string& msg);
 
 // Opt-in phase timings: with EQTL_TRACE set, mark() prints the wall time
 // since the previous mark to stderr.
@@ -141,6 +142,9 @@ struct PairRow {
   int n = 0;
   bool has_tss = false;
   double tss_dist = 0;
+  bool glm = false;  // NB-GLM rows carry phi and glm_converged
+  double phi = 0;
+  int converged = 1;
 };
 struct RegionRow {
   std::string gene, chrom;
@@ -152,7 +156,7 @@ struct ScopeFiles {
   FILE* pairs = nullptr;
   FILE* top = nullptr;
   FILE* region = nullptr;
-  ScopeFiles(const std::string& prefix);
+  ScopeFiles(const std::string& prefix, bool glm = false);
   ~ScopeFiles();
 };
 void write_pair(FILE* f, const PairRow& r, const std::string& scope);

@@ -1,5 +1,5 @@
 // eqtl: the reference program's command line (src/main.cpp, src/scan.cpp)
-// for PLINK or VCF (GT or DS) input and the LM / LMM models, with every scan run
+// for PLINK or VCF (GT or DS) input and the LM / LMM / NB-GLM models, with every scan run
 // on the B200 through libeqtl_cuda. The orchestration follows run_eqtl_geno
 // (src/scan.cpp:50-312): analysis samples = phenotype samples present in the
 // .fam, in phenotype order; one GRM (computed or -k) shared by the LMM
@@ -153,9 +153,10 @@ int run_scan(const Options& opt) {
   }
   for (const auto& model : opt.models) {
     for (const auto& scope : scopes) {
-      ScopeFiles out(opt.out + "." + model + "." + scope);
+      ScopeFiles out(opt.out + "." + model + "." + scope, model == "glm");
       std::vector<RegionRow> regions;
-      if (scope == "cis") run_cis(st, model, out, regions);
+      if (model == "glm") run_glm(st, scope, out, regions);
+      else if (scope == "cis") run_cis(st, model, out, regions);
       else run_trans(st, model, scope, out, regions);
       std::vector<double> acat;
       for (const auto& r : regions) acat.push_back(r.acat);

@@ -1,11 +1,12 @@
 // Command line of the reference program (src/options.cpp:145-179): the same
-// long and short flags, defaults and range checks, for PLINK input and the
-// LM / LMM models, with PLINK (-b) or VCF (-v, GT calls) genotypes. The
-// flags of paths outside the device scan (the GLM / GLMM models, --fast, the
-// fission subcommand) are recognised and refused with a message instead of
-// being silently ignored.
+// long and short flags, defaults and range checks, for the LM / LMM / NB-GLM
+// models, with PLINK (-b) or VCF (-v, GT or DS) genotypes. The flags of paths
+// outside the device scan (the GLMM model, --fast, the fission subcommand,
+// permutations of the GLM) are recognised and refused with a message instead
+// of being silently ignored.
 #include <getopt.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <iostream>
 
@@ -15,6 +16,7 @@ namespace eqtl_host {
 
 [[noreturn]] void die(const std::string& msg) { throw Fatal(msg); }
 void info(const std::string& msg) { std::cerr << "[I] " << msg << '\n'; }
+void warn(const std::string& msg) { std::cerr << "[W] " << msg << '\n'; }
 
 namespace {
 
@@ -33,9 +35,8 @@ std::vector<std::string> parse_models(const std::string& s) {
     if (j == std::string::npos) j = s.size();
     const std::string t = trim(s.substr(i, j - i));
     if (!t.empty()) {
-      if (t == "glm" || t == "glmm")
-        die("--model " + t + " is outside the device scan (lm|lmm are supported)");
-      if (t != "lm" && t != "lmm") die("invalid --model value: " + t + " (lm|glm|lmm|glmm)");
+      if (t == "glmm") die("--model glmm is outside the device scan (lm|lmm|glm are supported)");
+      if (t != "lm" && t != "lmm" && t != "glm") die("invalid --model value: " + t + " (lm|glm|lmm|glmm)");
       out.push_back(t);
     }
     i = j + 1;
@@ -61,7 +62,7 @@ void print_help() {
                "Analysis options:\n"
                "        --make-grm         write relatedness matrix and exit\n"
                "    -m, --mode STR         cis|trans|all|gw  [all]\n"
-               "        --model STR        lm|lmm[,...]  [lmm]\n"
+               "        --model STR        lm|lmm|glm[,...]  [lmm]\n"
                "    -w, --window INT       cis flank around gene body (bp)  [1000000]\n"
                "        --pval-cis FLOAT   cis output p threshold  [1e-5]\n"
                "        --pval-trans FLOAT trans/gw output p threshold  [1e-5]\n"
@@ -204,6 +205,8 @@ int parse_options(int argc, char** argv, Options& opt) {
     return 1;
   }
   if (opt.window < 0) die("--window must be >= 0");
+  if (opt.perm > 0 && std::find(opt.models.begin(), opt.models.end(), "glm") != opt.models.end())
+    die("--perm with --model glm (parametric NB resampling) is outside the device scan");
   return 0;
 }
 

@@ -8,14 +8,17 @@
 
 namespace eqtl_host {
 
-ScopeFiles::ScopeFiles(const std::string& prefix) {
+ScopeFiles::ScopeFiles(const std::string& prefix, bool glm) {
   pairs = std::fopen((prefix + ".pairs.tsv").c_str(), "w");
   top = std::fopen((prefix + ".top.tsv").c_str(), "w");
   region = std::fopen((prefix + ".region.tsv").c_str(), "w");
   if (!pairs || !top || !region) die("cannot open output for " + prefix);
-  static const char kPairHeader[] = "gene\tsnp\tchrom\tpos\tref\talt\taf\tbeta\tse\tstat\tp\tr2\tn\ttss_dist\tscope\n";
-  std::fputs(kPairHeader, pairs);
-  std::fputs(kPairHeader, top);
+  // write_pairs_header (src/output.cpp:8-13): GLM files add phi, glm_converged
+  const char* header = glm ? "gene\tsnp\tchrom\tpos\tref\talt\taf\tbeta\tse\tstat\tp\tr2\tn\ttss_dist\tscope\tphi\t"
+                             "glm_converged\n"
+                           : "gene\tsnp\tchrom\tpos\tref\talt\taf\tbeta\tse\tstat\tp\tr2\tn\ttss_dist\tscope\n";
+  std::fputs(header, pairs);
+  std::fputs(header, top);
   std::fputs("gene\tchrom\ttss\tn_tested\tn_sig\tacat_p\tq_bh\tp_emp\tp_beta\tbeta_shape1\tbeta_shape2\n", region);
 }
 
@@ -30,7 +33,9 @@ void write_pair(FILE* f, const PairRow& r, const std::string& scope) {
                r.beta, r.se, r.t, r.p, r.r2, r.n);
   if (r.has_tss) std::fprintf(f, "%.10g", r.tss_dist);
   else std::fputs("NA", f);
-  std::fprintf(f, "\t%s\n", scope.c_str());
+  std::fprintf(f, "\t%s", scope.c_str());
+  if (r.glm) std::fprintf(f, "\t%.10g\t%d", r.phi, r.converged);
+  std::fputc('\n', f);
 }
 
 void write_region(FILE* f, const RegionRow& r) {

@@ -11,6 +11,8 @@ struct ScanResult {
   std::vector<eqtl_gene_result> genes;
   std::vector<eqtl_pair> pairs, cands;
   std::vector<double> delta;  // LMM: REML delta per gene
+  std::vector<double> phi;    // GLM: NB dispersion per gene
+  std::vector<uint8_t> conv;  // GLM: null fit converged
 };
 
 struct PermGene {

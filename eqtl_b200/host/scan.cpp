@@ -9,6 +9,9 @@
 //              window [max(start - w, 1), end + w]; pairs per gene in gene
 //              order (GFF position order when -t > 1, as the reference's
 //              per-thread scan writes them), SNPs in .bim order.
+//   glm        NB-GLM, gene-outer in every scope (src/scan.cpp:227-300): one
+//              device scan of the scope's count genes, pairs per gene in
+//              gene order, SNPs in .bim order, phi and glm_converged columns.
 // Per gene: n_tested, n_sig, ACAT and the best SNP (strict <, first index
 // on ties) come from the device; the printed statistics of every pair are
 // the device's FP64 refinement.
@@ -147,6 +150,10 @@ ScanResult scan_columns(const Study& st, const std::string& model, const std::ve
   }
   R.genes.resize(J);
   R.delta.assign(J, 0.0);
+  if (model == "glm") {
+    R.phi.assign(J, 0.0);
+    R.conv.assign(J, 0);
+  }
   int64_t cap = 1 << 18, ccap = perm_thr > 0 ? (1 << 18) : 1;
   for (int attempt = 0; attempt < 3; ++attempt) {
     R.pairs.resize(static_cast<size_t>(cap));
@@ -155,6 +162,9 @@ ScanResult scan_columns(const Study& st, const std::string& model, const std::ve
     const int rc = model == "lm"
                        ? eqtl_scan_trans_lm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.genes.data(), R.pairs.data(),
                                             cap, &np, R.cands.data(), ccap, &nc)
+                   : model == "glm"
+                       ? eqtl_scan_glm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.phi.data(), R.conv.data(),
+                                       R.genes.data(), R.pairs.data(), cap, &np, R.cands.data(), ccap, &nc)
                        : eqtl_scan_trans_lmm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.delta.data(),
                                              R.genes.data(), R.pairs.data(), cap, &np, R.cands.data(), ccap, &nc);
     if (rc == EQTL_E_OVERFLOW) {
@@ -231,11 +241,22 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
     if (g.best_snp >= 0 && g.best_p <= pthr) need.push_back(g.best_snp);
   const auto af = st.geno->af(need);
   std::vector<int> n_sig(jobs.size(), 0);
+  const bool glm = !R.phi.empty();
+  auto with_glm = [&](PairRow r, size_t j) {
+    if (glm) {
+      r.glm = true;
+      r.phi = R.phi[j];
+      r.converged = R.conv[j] ? 1 : 0;
+    }
+    return r;
+  };
   for (size_t k : pair_order) {
     const eqtl_pair& q = R.pairs[k];
     const Job& jb = jobs[q.gene];
     ++n_sig[q.gene];
-    write_pair(out.pairs, make_row(st, st.genes[jb.gene], jb.loc, q.snp, af.at(q.snp), q.beta, q.se, q.t, q.p, q.r2, R.n),
+    write_pair(out.pairs,
+               with_glm(make_row(st, st.genes[jb.gene], jb.loc, q.snp, af.at(q.snp), q.beta, q.se, q.t, q.p, q.r2, R.n),
+                        q.gene),
                scope);
   }
   for (size_t j = 0; j < jobs.size(); ++j) {
@@ -259,8 +280,9 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
     regions.push_back(rr);
     if (g.best_snp >= 0 && g.best_p <= pthr && g.best_p <= 1.0)
       write_pair(out.top,
-                 make_row(st, rr.gene, jb.loc, g.best_snp, af.at(g.best_snp), g.best_beta, g.best_se, g.best_t,
-                          g.best_p, g.best_r2, R.n),
+                 with_glm(make_row(st, rr.gene, jb.loc, g.best_snp, af.at(g.best_snp), g.best_beta, g.best_se,
+                                   g.best_t, g.best_p, g.best_r2, R.n),
+                          j),
                  scope);
   }
 }
@@ -380,6 +402,90 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
     return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
   });
   emit(st, jobs, R, "cis", pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
+}
+
+// Whether every finite value is a non-negative integer (within 1e-8) and one
+// is present (looks_like_counts, src/model_lm.cpp:8-17).
+static bool looks_like_counts(const std::vector<double>& y) {
+  int seen = 0;
+  for (double v : y) {
+    if (!std::isfinite(v)) continue;
+    ++seen;
+    if (v < 0 || std::fabs(v - std::floor(v)) > 1e-8) return false;
+  }
+  return seen > 0;
+}
+
+void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::vector<RegionRow>& regions) {
+  const Options& opt = *st.opt;
+  const bool have_gff = !opt.gff.empty();
+  // cis with -t > 1 runs the per-thread driver: the raw counts are checked
+  // before --pheno-norm, and the genes go in (chromosome, TSS) order
+  const bool par_cis = scope == "cis" && opt.threads > 1 && have_gff;
+  const size_t n = st.samples.size();
+  std::vector<Job> jobs;
+  for (size_t g = 0; g < st.genes.size(); ++g) {
+    Job jb;
+    jb.gene = static_cast<int>(g);
+    if (have_gff) {
+      auto it = st.annot.find(st.genes[g]);
+      if (it != st.annot.end()) jb.loc = &it->second;
+      else if (scope != "gw") continue;
+    }
+    if (scope != "gw" && !jb.loc) continue;
+    const std::vector<double> y = gene_y(st, jb.gene);
+    const std::vector<double> raw(st.Y.begin() + g * n, st.Y.begin() + (g + 1) * n);
+    if (!looks_like_counts(par_cis ? raw : y)) {
+      warn("skip non-count gene for glm: " + st.genes[g]);
+      continue;
+    }
+    if (!gene_ready(st, y, true)) continue;
+    jobs.push_back(jb);
+  }
+  if (par_cis)
+    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) {
+      return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
+    });
+  info(scope + " glm: " + std::to_string(jobs.size()) + " genes");
+  if (jobs.empty()) return;
+  const double pthr = scope == "cis" ? opt.pval_cis : opt.pval_trans;
+  const int mode = scope == "cis" ? 2 : scope == "trans" ? 1 : 0;
+  // cis: the device takes the genes in window order (a banded tile list)
+  std::vector<size_t> dev_order(jobs.size());
+  std::iota(dev_order.begin(), dev_order.end(), 0);
+  if (mode == 2) {
+    std::vector<std::string> keys(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) keys[j] = chrom_key(jobs[j].loc->chrom);
+    std::stable_sort(dev_order.begin(), dev_order.end(), [&](size_t a, size_t b) {
+      return keys[a] != keys[b] ? keys[a] < keys[b] : jobs[a].loc->start < jobs[b].loc->start;
+    });
+  }
+  std::vector<Job> jobs_dev(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) jobs_dev[j] = jobs[dev_order[j]];
+  Trace tr;
+  ScanResult R = device_scan(st, "glm", jobs_dev, mode, pthr, 0.0);
+  tr.mark(scope + " glm: device scan");
+  {
+    std::vector<eqtl_gene_result> genes(R.genes.size());
+    std::vector<double> phi(R.phi.size());
+    std::vector<uint8_t> conv(R.conv.size());
+    for (size_t j = 0; j < dev_order.size(); ++j) {
+      genes[dev_order[j]] = R.genes[j];
+      phi[dev_order[j]] = R.phi[j];
+      conv[dev_order[j]] = R.conv[j];
+    }
+    R.genes.swap(genes);
+    R.phi.swap(phi);
+    R.conv.swap(conv);
+    for (auto& q : R.pairs) q.gene = static_cast<int32_t>(dev_order[q.gene]);
+  }
+  std::vector<size_t> order(R.pairs.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    const eqtl_pair &x = R.pairs[a], &y = R.pairs[b];
+    return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
+  });
+  emit(st, jobs, R, scope, pthr, order, out, regions, nullptr);
 }
 
 }  // namespace eqtl_host

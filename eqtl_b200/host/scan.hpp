@@ -46,5 +46,9 @@ struct Study {
 void run_trans(const Study& st, const std::string& model, const std::string& scope, ScopeFiles& out,
                std::vector<RegionRow>& regions);
 void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::vector<RegionRow>& regions);
+// NB-GLM, gene-outer in every scope (src/scan.cpp:227-300; cis with -t > 1
+// src/scan_cis.cpp:18-115): genes in phenotype order (cis with -t > 1: by
+// chromosome and TSS), pairs per gene in SNP order.
+void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::vector<RegionRow>& regions);
 
 }  // namespace eqtl_host

@@ -244,6 +244,22 @@ int eqtl_scan_trans_lmm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double
                         double* delta_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
                         int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
 
+/* ---------------------------------------------------------------- NB GLM
+ * Replaces the gene-outer NB-GLM scan (src/scan.cpp:227-300, per gene
+ * include/eqtl/scan_cis.hpp:15-66) on the shared-keep path: prep_glm_nb's
+ * null fit per gene (IRLS with moment dispersion, src/model_glm.cpp:28-96)
+ * and test_glm_nb's score test per (gene, SNP) (:98-132), for every kept SNP
+ * in the gene's scope (prm->exclude_cis as for the other scans). Y holds
+ * counts (non-negative integers; other values fail with EQTL_E_ARG, as
+ * prep_glm_nb dies). Outputs as for eqtl_scan_trans_lm, with eqtl_pair.t the
+ * score statistic z and p two-sided normal; phi_out [n_genes] and
+ * converged_out [n_genes] (optional) receive each gene's dispersion and
+ * whether its null fit succeeded (a failed fit tests no SNP). Needs
+ * EQTL_PREC_SPLIT_F16 and 1 <= p <= 32. */
+int eqtl_scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X, double* phi_out,
+                  uint8_t* converged_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
+                  int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
+
 /* -------------------------------------------------------------- pair tests
  * FP64 tests of explicit (column of Y, kept SNP) pairs with the scans' own
  * per-column prep: LM (EQTL_MODEL_LM) residualises each column on X

@@ -71,3 +71,21 @@ def trans_lmm(G_dos, Y, X, Q, lam, pthr, excl=None, deltas=None):
     out, pairs = summarize(st, use, pthr, n - p - 1)
     out["delta"] = np.array([pp.delta for pp in preps])
     return out, pairs
+
+
+def glm(G_dos, Y, X, pthr, excl=None):
+    """NB-GLM score test of every (SNP, gene) pair over kept dosages
+    (prep_glm_nb / test_glm_nb, src/model_glm.cpp:74-132); a pair counts as
+    tested when the subset gate passes and p is finite (a gene whose null fit
+    failed tests nothing)."""
+    m, n = G_dos.shape
+    Gn = Y.shape[1]
+    preps = [R.prep_glm_nb(Y[:, g], X) for g in range(Gn)]
+    af, ok = R.subset_maf(G_dos)
+    cols = [R.test_glm_nb_many(pp, G_dos) for pp in preps]
+    st = {k: np.stack([c[k] for c in cols], 1) for k in cols[0]}
+    use = ok[:, None] & np.isfinite(st["p"]) & (np.ones((m, Gn), bool) if excl is None else ~excl)
+    out, pairs = summarize(st, use, pthr, None)
+    out["phi"] = np.array([pp.phi for pp in preps])
+    out["converged"] = np.array([pp.converged for pp in preps])
+    return out, pairs
