@@ -2,13 +2,16 @@
 headline trans-LMM one (bench.py), through the C ABI with the inputs resident
 on the device.
 
-    python -m eqtl_b200.config_bench [--which grm,lm] [--steps K]
+    python -m eqtl_b200.config_bench [--which grm,lm,glm] [--steps K]
 
 grm  GRM build, eigendecomposition and spectral rotation: n = 2,000 samples
      (50 families of 10 siblings + 1,500 unrelated), m = 200,000 SNPs with
      MAF ~ U(0.01, 0.5) and 1% missing calls.
 lm   trans/gw LM scan: n = 1,000 samples, m = 1,000,000 SNPs, 20,000 genes
      with Y ~ N(0, 1), intercept + 10 N(0, 1) covariates, p threshold 1e-5.
+glm  gw NB-GLM scan: n = 1,000 samples, m = 200,000 SNPs, 5,000 genes of
+     negative-binomial counts (synth.make_pheno_counts), intercept + 2
+     covariates, p threshold 1e-5.
 
 Seeded synthetic data of those shapes (no data set ships with the
 reference). Each JSON line gives the CUDA-event stage times (median over the
@@ -101,6 +104,37 @@ def lm_case(steps: int, m: int = 1_000_000, G: int = 20_000) -> dict:
             "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
 
 
+def glm_case(steps: int, m: int = 200_000, G: int = 5_000) -> dict:
+    n, ncov = 1000, 2
+    rows, _, _ = synth.make_bed_rows_chunked(20261205, n, m, maf_lo=0.01, maf_hi=0.5, miss_rate=0.01)
+    Y, C = synth.make_pheno_counts(20261206, None, G, ncov, n=n)
+    X = np.column_stack([np.ones(n), C])
+    pk, kind = _peaks()
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        c.pheno_load(Y, X)
+        t = {"prep": [], "scan": [], "refine": []}
+        tests = 0
+        for i in range(steps + 1):
+            genes, pairs, _, phi, conv = c.scan_glm(None, None, pthr=1e-5)
+            if i:
+                tests = int(genes["n_tested"].sum())
+                for k in t:
+                    t[k].append(c.stage_ms(k))
+    med = {k: statistics.median(v) for k, v in t.items()}
+    step_ms = sum(med.values())
+    flops = 2.0 * n * (X.shape[1] + 2) * tests
+    peak = pk.get("bf16_tflops_sustained", 1400.0)
+    return {"workload": "gw NB-GLM scan (--model glm --mode gw)", "n_samples": n, "n_snps": m, "n_genes": G,
+            "covariates": ncov, "pthr": 1e-5, "steps": steps, "tests_per_step": tests, "stage_ms": med,
+            "stage_ms_steps": t, "tests_per_s": tests / (step_ms / 1e3), "pairs": int(len(pairs)),
+            "converged": int(conv.sum()), "phi_median": float(np.median(phi)),
+            "scan": {"algorithmic_tflops": flops / (med["scan"] / 1e3) / 1e12,
+                     "frac_of_bf16_sustained": flops / (med["scan"] / 1e3) / 1e12 / peak,
+                     "issued_products": 3},
+            "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--which", default="grm,lm")
@@ -109,7 +143,12 @@ def main() -> None:
     ap.add_argument("--lm-genes", type=int, default=20_000, help="genes of the lm case")
     args = ap.parse_args()
     for w in args.which.split(","):
-        out = grm_case(args.steps) if w == "grm" else lm_case(args.steps, args.lm_snps, args.lm_genes)
+        if w == "grm":
+            out = grm_case(args.steps)
+        elif w == "glm":
+            out = glm_case(args.steps)
+        else:
+            out = lm_case(args.steps, args.lm_snps, args.lm_genes)
         print(json.dumps(out), flush=True)
 
 

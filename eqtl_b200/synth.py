@@ -222,17 +222,17 @@ def make_pheno_lmm(seed: int, g: Genotypes, n_genes: int, n_cov: int, *, h2_max:
     return Y, C, h2
 
 
-def make_pheno_counts(seed: int, g: Genotypes, n_genes: int, n_cov: int, *, n_trans: int = 0,
-                      beta_sd: float = 0.3, cov_weight: float = 0.2) -> tuple:
+def make_pheno_counts(seed: int, g: Optional[Genotypes], n_genes: int, n_cov: int, *, n_trans: int = 0,
+                      beta_sd: float = 0.3, cov_weight: float = 0.2, n: Optional[int] = None) -> tuple:
     """Negative-binomial counts (NB2, log link): log mu = b0 + cov_weight *
     sum(C) + planted SNP effects, b0 ~ U(0.5, 4), dispersion phi ~ U(0.05, 1)
-    per gene, y ~ Poisson(Gamma(1/phi, phi mu)). Returns (Y [n, G], C [n, c])."""
+    per gene, y ~ Poisson(Gamma(1/phi, phi mu)). Returns (Y [n, G], C [n, c]).
+    Without genotypes (g None, n given) no SNP effects are planted."""
     rng = np.random.default_rng(seed)
-    n = len(g.samples)
+    n = len(g.samples) if g is not None else n
     C = rng.standard_normal((n, n_cov))
     eta = rng.uniform(0.5, 4.0, n_genes)[None, :] + cov_weight * C.sum(1, keepdims=True)
-    eta = np.repeat(eta, n_genes, axis=1) if eta.shape[1] == 1 else eta
-    if n_trans:
+    if n_trans and g is not None:
         m = g.codes.shape[0]
         snps = rng.integers(0, m, size=n_trans)
         genes = rng.integers(0, n_genes, size=n_trans)
