@@ -715,6 +715,13 @@ int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, 
   });
 }
 
+int eqtl_pheno_int(eqtl_ctx* ctx, double* Y, int32_t n, int32_t n_cols) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(Y, EQTL_E_ARG, "null input");
+    eqtl::pheno_int(ctx, Y, n, n_cols);
+  });
+}
+
 int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out) {
   return guarded(ctx, [&] {
     eqtl::DevBuf<double> K;

@@ -269,6 +269,9 @@ void geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int n_file, con
                       int miss_hand, double max_miss, double maf_min);
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
+// Rank-based inverse normal transform of each of the G columns of Y_host
+// [G][n], in place (computed on the device).
+void pheno_int(eqtl_ctx* ctx, double* Y_host, int n, int G);
 void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host);
 void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p);
 

@@ -69,6 +69,46 @@ EQTL_HD double t_two_sided_p(double t, double df) {
   return fmin(1.0, fmax(0.0, p));
 }
 
+// Inverse of the standard normal CDF as qnorm_inv computes it
+// (src/util.cpp:132-171): Acklam's published rational approximation (central
+// region p in [0.02425, 0.97575], tails in sqrt(-2 ln p)), with the
+// coefficient digits the reference carries (they differ from the published
+// ones in the last places; the Halley step absorbs that, but parity wants the
+// same starting point), then one Halley step on Phi(v) - p. p is clamped to
+// [1e-15, 1 - 1e-15].
+EQTL_HD double normal_quantile(double p) {
+  const double a[6] = {-39.6968302866538, 220.9460984245205, -275.9285104469687,
+                       138.3577518678900, -30.6647980661472, 2.506628277459239};
+  const double b[5] = {-54.4760987982241, 161.5858368580409, -155.6989798598867, 66.8013118877197,
+                       -13.28068155278571};
+  const double c[6] = {-0.007784894002430293, -0.3223964580411364, -2.4007582771618388,
+                       -2.5497325393437340,   4.3746641414649678,  2.9381639826987831};
+  const double d[4] = {0.0077846957090414622, 0.32246712907003983, 2.4451341371429960, 3.7544086619074161};
+  p = fmin(fmax(p, 1e-15), 1.0 - 1e-15);
+  const double target = p;
+  const bool upper = p > 0.5;
+  if (upper) p = 1.0 - p;
+  double v;
+  if (p < 0.02425) {
+    const double q = sqrt(-2.0 * log(p));
+    v = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+  } else {
+    const double q = p - 0.5, r = q * q;
+    v = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+        (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+  }
+  if (upper) v = -v;
+  const double cdf = 0.5 * erfc(-v / sqrt(2.0));
+  const double phi = exp(-0.5 * v * v) / sqrt(2.0 * 3.14159265358979323846);
+  if (phi > 1e-300) {
+    const double f = cdf - target;
+    const double den = 2.0 * phi * phi + f * v * phi;
+    if (den != 0.0) v -= 2.0 * f * phi / den;
+  }
+  return v;
+}
+
 // Two-sided normal tail P(|Z| > |z|) = erfc(|z| / sqrt 2), clipped to
 // [0, 1]; 1 for a z that is not finite (pnorm_two_sided, src/util.cpp:116-123).
 EQTL_HD double z_two_sided_p(double z) {

@@ -125,7 +125,6 @@ void write_grm(const std::string& prefix, const std::vector<std::string>& ids, c
 // --------------------------------------------------------------- statistics
 double acat_p(double tan_sum, int used);                       // AcatAcc::p
 std::vector<double> bh_adjust(const std::vector<double>& p);   // src/scan_common.cpp:201-217
-void inverse_normal_transform(std::vector<double>& y);         // src/util.cpp:132-206
 uint32_t fnv1a32(const std::string& s);
 uint32_t perm_seed(int seed_opt, int b, const std::string& gene);
 double p_emp(double T_obs, const std::vector<double>& T_perm);

@@ -132,6 +132,11 @@ int run_scan(const Options& opt) {
 
   if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, st.samples), opt);
   Device dev;
+  if (opt.pheno_int) {  // every gene's rank-based inverse normal transform, on the device
+    st.Y_int = st.Y;
+    dev.check(eqtl_pheno_int(dev.ctx, st.Y_int.data(), static_cast<int32_t>(n), static_cast<int32_t>(G)),
+              "--pheno-norm int");
+  }
   Genotypes geno(dev, P, sample_columns(P, st.samples), device_filters(opt));
   st.dev = &dev;
   st.geno = &geno;

@@ -3,10 +3,6 @@
 //   ACAT p        0.5 - atan(mean tan term) / pi in long double, clamped
 //                 (AcatAcc::p, src/stats_extra.cpp:24-31)
 //   BH q          step-up over the genes of one scope (src/scan_common.cpp:201-217)
-//   INT           rank-based inverse normal transform with average ranks,
-//                 (r - 1/2) / n clamped to [1e-15, 1 - 1e-15], Acklam's
-//                 rational approximation and one Halley step
-//                 (src/util.cpp:132-206)
 //   p_emp         (1 + #{T_perm >= T_obs}) / (1 + B) (src/stats_extra.cpp:39-46)
 //   beta approx   method-of-moments start, Nelder-Mead on the beta likelihood
 //                 within s1 in [0.1, 10], s2 in [5, 1e6], then I_p(s1, s2)
@@ -45,69 +41,6 @@ std::vector<double> bh_adjust(const std::vector<double>& a) {
   return q;
 }
 
-namespace {
-
-// Inverse of the standard normal CDF: Acklam's published rational
-// approximation (central region |p - 1/2| <= 0.47575, tails by
-// sqrt(-2 ln p)), then one Halley step on Phi(v) - p.
-double normal_quantile(double p) {
-  // coefficient digits as the reference carries them (they differ from the
-  // published ones in the last places; the Halley step absorbs that, but
-  // parity wants the same starting point)
-  static const double a[6] = {-39.6968302866538, 220.9460984245205, -275.9285104469687,
-                              138.3577518678900, -30.6647980661472, 2.506628277459239};
-  static const double b[5] = {-54.4760987982241, 161.5858368580409, -155.6989798598867, 66.8013118877197,
-                              -13.28068155278571};
-  static const double c[6] = {-0.007784894002430293, -0.3223964580411364, -2.4007582771618388,
-                              -2.5497325393437340,   4.3746641414649678,  2.9381639826987831};
-  static const double d[4] = {0.0077846957090414622, 0.32246712907003983, 2.4451341371429960,
-                              3.7544086619074161};
-  p = std::min(std::max(p, 1e-15), 1.0 - 1e-15);
-  const double target = p;
-  const bool upper = p > 0.5;
-  if (upper) p = 1.0 - p;
-  double v;
-  if (p < 0.02425) {
-    const double q = std::sqrt(-2.0 * std::log(p));
-    v = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
-        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
-  } else {
-    const double q = p - 0.5, r = q * q;
-    v = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
-        (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
-  }
-  if (upper) v = -v;
-  const double cdf = 0.5 * std::erfc(-v / std::sqrt(2.0));
-  const double phi = std::exp(-0.5 * v * v) / std::sqrt(2.0 * M_PI);
-  if (phi > 1e-300) {
-    const double f = cdf - target;
-    const double den = 2.0 * phi * phi + f * v * phi;
-    if (den != 0.0) v -= 2.0 * f * phi / den;
-  }
-  return v;
-}
-
-}  // namespace
-
-void inverse_normal_transform(std::vector<double>& y) {
-  std::vector<size_t> fin;
-  for (size_t i = 0; i < y.size(); ++i)
-    if (std::isfinite(y[i])) fin.push_back(i);
-  const size_t nf = fin.size();
-  if (nf <= 1) return;
-  std::vector<size_t> order(nf);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t z) { return y[fin[x]] < y[fin[z]]; });
-  std::vector<double> rank(nf);
-  for (size_t i = 0; i < nf;) {
-    size_t j = i + 1;
-    while (j < nf && y[fin[order[j]]] == y[fin[order[i]]]) ++j;
-    const double r = 0.5 * static_cast<double>(i + 1 + j);
-    for (size_t k = i; k < j; ++k) rank[order[k]] = r;
-    i = j;
-  }
-  for (size_t k = 0; k < nf; ++k) y[fin[k]] = normal_quantile((rank[k] - 0.5) / static_cast<double>(nf));
-}
 
 uint32_t fnv1a32(const std::string& s) {
   uint64_t h = 14695981039346656037ull;

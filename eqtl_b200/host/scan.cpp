@@ -95,11 +95,12 @@ bool gene_ready(const Study& st, const std::vector<double>& y, bool checks) {
   return kept >= 3 && !(mx < 1e-15);
 }
 
+// The gene's phenotype after --pheno-norm (apply_pheno_norm,
+// src/scan_common.cpp): the transformed copy when int is on.
 std::vector<double> gene_y(const Study& st, int g) {
   const size_t n = st.samples.size();
-  std::vector<double> y(st.Y.begin() + static_cast<size_t>(g) * n, st.Y.begin() + static_cast<size_t>(g + 1) * n);
-  if (st.opt->pheno_int) inverse_normal_transform(y);
-  return y;
+  const std::vector<double>& src = st.opt->pheno_int ? st.Y_int : st.Y;
+  return std::vector<double>(src.begin() + static_cast<size_t>(g) * n, src.begin() + static_cast<size_t>(g + 1) * n);
 }
 
 }  // namespace

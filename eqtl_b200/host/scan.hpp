@@ -33,6 +33,7 @@ struct Study {
   const Plink* plink = nullptr;
   std::vector<std::string> samples, genes;
   std::vector<double> Y;  // gene-major [G][n]
+  std::vector<double> Y_int;  // --pheno-norm int: Y with every gene transformed (eqtl_pheno_int)
   std::vector<double> X;  // column-major [n, p]
   int p = 1;
   std::unordered_map<std::string, GeneLoc> annot;

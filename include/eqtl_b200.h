@@ -127,6 +127,14 @@ int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t mod
  * Y == NULL and X == NULL, so repeated scans need no host transfer. */
 int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, int32_t n_genes, int32_t p);
 
+/* --pheno-norm int on the device: replaces inverse_normal_transform
+ * (src/util.cpp:177-206, with qnorm_inv :132-171) for every column of
+ * Y [n, n_cols] (column-major, host memory), in place. Per column the finite
+ * values get average ranks (ties share them) and become
+ * qnorm_inv((rank - 1/2) / n_finite); values that are not finite are left as
+ * they are, as is a column with at most one finite value. */
+int eqtl_pheno_int(eqtl_ctx* ctx, double* Y, int32_t n, int32_t n_cols);
+
 /* ------------------------------------------------------- scan result types */
 typedef struct {
   int32_t n_tested;      /* finite tests counted (GeneSummary.n_tested) */
