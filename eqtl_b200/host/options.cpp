@@ -205,6 +205,10 @@ int parse_options(int argc, char** argv, Options& opt) {
     return 1;
   }
   if (opt.window < 0) die("--window must be >= 0");
+  // src/options.cpp:288-299: INT output is continuous, the count models need raw counts
+  if (opt.pheno_int && std::find(opt.models.begin(), opt.models.end(), "glm") != opt.models.end())
+    die("--pheno-norm int is incompatible with count model glm (apply INT only for lm/lmm; count models need raw "
+        "integer counts)");
   if (opt.perm > 0 && std::find(opt.models.begin(), opt.models.end(), "glm") != opt.models.end())
     die("--perm with --model glm (parametric NB resampling) is outside the device scan");
   return 0;

@@ -1043,3 +1043,82 @@ def shuffle_indices(n: int, seed: int) -> List[int]:
 def perm_seed(seed_opt: int, b: int, gene: str) -> int:
     base = seed_opt if seed_opt >= 0 else 1
     return (base + b * 9973 + fnv1a(gene)) & 0xFFFFFFFF
+
+
+# ---------------------------------------------------------------------------
+# PEER VB factor analysis of the fission subcommand (src/fission.cpp:104-275)
+# ---------------------------------------------------------------------------
+def std_normal_draws(seed: int, count: int) -> np.ndarray:
+    """The standard library's std::normal_distribution sequence from
+    std::mt19937(seed), read from oracle/_ref/stdnormal (built by
+    oracle/Makefile from oracle/shim/stdnormal.cpp)."""
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "stdnormal")
+    out = subprocess.run([exe, str(seed), str(count)], check=True, capture_output=True, text=True).stdout
+    return np.array([float(v) for v in out.split()], dtype=np.float64)
+
+
+def peer_start(seed: int, n: int, G: int, k: int):
+    """peer_factors' starting values (src/fission.cpp:226-236): X [n, k] then
+    W [G, k], both filled column by column from one normal sequence."""
+    z = std_normal_draws(seed, n * k + G * k)
+    X0 = z[: n * k].reshape(k, n).T.copy()
+    W0 = z[n * k:].reshape(k, G).T.copy()
+    return X0, W0
+
+
+def peer_factors(Y_raw: np.ndarray, k: int, max_iter: int, tol: float, X0: np.ndarray, W0: np.ndarray):
+    """peer_factors (src/fission.cpp:203-275) from given starting values:
+    genes centred (NaN -> 0), ARD/noise priors (0.001, 0.1) / (0.1, 10),
+    W, Alpha, X, Eps updates in that order, stop when the mean squared
+    residual moves by less than 1e-8 or `tol`. Returns (X [n, k], iterations)."""
+    Y = np.array(Y_raw, dtype=np.float64, copy=True)
+    n, G = Y.shape
+    for j in range(G):
+        fin = ~np.isnan(Y[:, j])
+        mean = Y[fin, j].mean() if fin.any() else 0.0
+        Y[:, j] = np.where(fin, Y[:, j] - mean, 0.0)
+    pa_A, pb_A, pa_E, pb_E = 0.001, 0.1, 0.1, 10.0
+    X = X0.copy()
+    W = W0.copy()
+    Eps = np.full(G, pa_E / pb_E)
+    XE2S = n * np.eye(k) + X.T @ X
+    Alpha = (pa_A + 0.5 * G) / (pb_A + 0.5 * np.zeros(k))
+    b1 = (Y * Y + 0.01).sum(0)
+    last = np.finfo(np.float64).max
+    it = 0
+    for it in range(1, max_iter + 1):
+        XtY = X.T @ Y
+        covs = np.empty((G, k, k))
+        for d in range(G):
+            M = np.diag(Alpha) + Eps[d] * XE2S
+            covs[d] = np.linalg.solve(M, np.eye(k))
+            W[d] = np.linalg.solve(M, XtY[:, d]) * Eps[d]
+        E2 = covs + W[:, :, None] * W[:, None, :]
+        W_E2S = E2.sum(0)
+        W_Xprec = (Eps[:, None, None] * E2).sum(0)
+        Alpha = (pa_A + 0.5 * G) / (pb_A + 0.5 * np.diag(W_E2S))
+        Xcov = np.linalg.solve(W_Xprec + np.eye(k), np.eye(k))
+        X = Y @ (W * Eps[:, None]) @ Xcov
+        XE2S = n * Xcov + X.T @ X
+        b2 = (XtY.T * W).sum(1)
+        b3 = np.einsum("kl,dkl->d", XE2S, E2)
+        Eps = (pa_E + 0.5 * n) / np.maximum(pb_E + 0.5 * (b1 - 2.0 * b2 + b3), 1e-10)
+        res = float(np.mean((Y - X @ W.T) ** 2))
+        if abs(last - res) < 1e-8 or abs(last - res) < tol:
+            break
+        last = res
+    return X, it
+
+
+def fission_residualize(Y1: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """src/fission.cpp:331-344: per gene, values that are not finite take
+    the gene's mean, then the least-squares fit on the covariates X (with
+    intercept) is removed."""
+    out = np.empty_like(Y1)
+    for j in range(Y1.shape[1]):
+        y = Y1[:, j].copy()
+        fin = np.isfinite(y)
+        y[~fin] = y[fin].mean() if fin.any() else 0.0
+        b = np.linalg.solve(X.T @ X, X.T @ y)
+        out[:, j] = y - X @ b
+    return out

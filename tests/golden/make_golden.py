@@ -115,6 +115,44 @@ def build_case(name: str, spec: dict) -> None:
         json.dump(manifest, f, indent=1)
 
 
+# The fission subcommand (data thinning + PEER factors) on phenotype tables
+# only: counts (binomial thinning) and continuous values with a missing entry
+# (Gaussian fission), with and without covariate residualisation.
+FISSION_RUNS = [
+    ("counts", ["-e", "counts.tsv", "--peer-factors", "4", "--epsilon", "0.4", "--seed", "7"]),
+    ("cont", ["-e", "cont.tsv", "--peer-factors", "5", "--seed", "3", "--fission-tol", "1e-9",
+              "--fission-max-iter", "300"]),
+    ("covar", ["-e", "cont.tsv", "-c", "covar.tsv", "--peer-factors", "3", "--epsilon", "0.3"]),
+]
+
+
+def build_fission_case() -> None:
+    import numpy as np
+    d = os.path.join(HERE, "fission")
+    if os.path.isdir(d):
+        shutil.rmtree(d)
+    os.makedirs(d)
+    rng = np.random.default_rng(5)
+    n, G = 60, 80
+    samples = [f"S{i:03d}" for i in range(n)]
+    genes = [f"G{j:03d}" for j in range(G)]
+    Yc, C = synth.make_pheno_counts(11, None, G, 2, n=n)
+    Yg = rng.standard_normal((n, G)) + rng.standard_normal((n, 3)) @ rng.standard_normal((3, G))
+    Yg[3, 7] = np.nan
+    synth.write_pheno(os.path.join(d, "counts.tsv"), samples, genes, Yc)
+    synth.write_pheno(os.path.join(d, "cont.tsv"), samples, genes, Yg)
+    synth.write_covar(os.path.join(d, "covar.tsv"), samples[5:], C[5:])
+    manifest = {"runs": {}}
+    for tag, argv in FISSION_RUNS:
+        cmd = [REF, "fission"] + argv + ["-o", f"ref_{tag}"]
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise SystemExit(f"fission/{tag} failed: {r.stderr}")
+        manifest["runs"][tag] = {"argv": cmd[1:]}
+    with open(os.path.join(d, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
 if __name__ == "__main__":
     if not os.path.exists(REF):
         raise SystemExit("build the reference first: make -C oracle")
@@ -124,3 +162,6 @@ if __name__ == "__main__":
             continue
         build_case(name, spec)
         print("built", name)
+    if not only or "fission" in only:
+        build_fission_case()
+        print("built fission")

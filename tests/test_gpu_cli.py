@@ -37,7 +37,8 @@ def _runs():
             continue
         man = json.load(open(os.path.join(GOLD, c, "manifest.json")))
         for tag, r in man["runs"].items():
-            out.append((c, tag, r["argv"]))
+            if r["argv"][0] != "fission":  # the fission subcommand has its own tests
+                out.append((c, tag, r["argv"]))
     return out
 
 
