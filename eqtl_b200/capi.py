@@ -25,7 +25,8 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
-           "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int"]
+           "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
+           "eqtl_peer"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -77,6 +78,7 @@ def load() -> C.CDLL:
         lib.eqtl_geno_load_dosage.argtypes = [vp, vp, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp, vp]
         lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
         lib.eqtl_pheno_int.argtypes = [vp, vp, i32, i32]
+        lib.eqtl_peer.argtypes = [vp, vp, i32, i32, i32, i32, dp, vp, vp, vp, C.POINTER(i32)]
         lib.eqtl_geno_dosage_rows.argtypes = [vp, vp, i64, vp]
         lib.eqtl_test_pairs.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64, vp, vp]
         lib.eqtl_scan_trans_lm.argtypes = [vp, C.POINTER(ScanParams), vp, vp, vp, vp, i64, C.POINTER(i64), vp,
@@ -182,6 +184,18 @@ class Context:
         out = np.array(Y, dtype=np.float64, order="F", copy=True)
         self._check(self.lib.eqtl_pheno_int(self.h, _ptr(out), out.shape[0], out.shape[1]))
         return out
+
+    def peer(self, Y: np.ndarray, k: int, max_iter: int, tol: float, X0: np.ndarray, W0: np.ndarray):
+        """eqtl_peer: PEER factors of Y [n, G] from X0 [n, k], W0 [G, k] -> (X [n, k], iterations)."""
+        Y = np.asfortranarray(Y, dtype=np.float64)
+        X0 = np.asfortranarray(X0, dtype=np.float64)
+        W0 = np.asfortranarray(W0, dtype=np.float64)
+        n, G = Y.shape
+        X = np.zeros((n, k), np.float64, order="F")
+        it = C.c_int32()
+        self._check(self.lib.eqtl_peer(self.h, _ptr(Y), n, G, k, max_iter, tol, _ptr(X0), _ptr(W0), _ptr(X),
+                                       C.byref(it)))
+        return X, it.value
 
     def dosage(self, lo: int, hi: int) -> np.ndarray:
         out = np.zeros((hi - lo, self.n), np.float64)

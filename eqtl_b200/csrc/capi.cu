@@ -715,6 +715,15 @@ int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, 
   });
 }
 
+int eqtl_peer(eqtl_ctx* ctx, const double* Y, int32_t n, int32_t n_genes, int32_t K, int32_t max_iter, double tol,
+              const double* X0, const double* W0, double* X_out, int32_t* iters_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(Y && X0 && W0 && X_out, EQTL_E_ARG, "null input");
+    const int it = eqtl::peer_factors(ctx, Y, n, n_genes, K, max_iter, tol, X0, W0, X_out);
+    if (iters_out) *iters_out = it;
+  });
+}
+
 int eqtl_pheno_int(eqtl_ctx* ctx, double* Y, int32_t n, int32_t n_cols) {
   return guarded(ctx, [&] {
     EQTL_CHECK(Y, EQTL_E_ARG, "null input");

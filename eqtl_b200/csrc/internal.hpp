@@ -272,6 +272,10 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
 // Rank-based inverse normal transform of each of the G columns of Y_host
 // [G][n], in place (computed on the device).
 void pheno_int(eqtl_ctx* ctx, double* Y_host, int n, int G);
+// PEER factors of Y_host [n, G] (column-major) from the starting X0 [n, K]
+// and W0 [G, K]; returns the iterations run.
+int peer_factors(eqtl_ctx* ctx, const double* Y_host, int n, int G, int K, int max_iter, double tol,
+                 const double* X0, const double* W0, double* X_out);
 void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host);
 void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p);
 

@@ -58,7 +58,16 @@ struct Options {
   int perm_trans_top = 1000;
   int seed = -1;
   bool disable_beta_approx = false;
+  // the fission subcommand (src/options.cpp:104-109, 237-252)
+  bool run_fission = false;
+  int peer_factors = 10;
+  double fission_epsilon = 0.5;
+  int fission_max_iter = 1000;
+  double fission_tol = 1e-3;
 };
+// eqtl fission: data thinning of the phenotype table and PEER factors of Y1
+// (src/fission.cpp:277-393).
+int run_fission(const Options& opt);
 // Returns 0 to run, 2 after --help / --version, 1 on a usage error.
 int parse_options(int argc, char** argv, Options& opt);
 

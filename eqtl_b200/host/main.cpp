@@ -185,6 +185,7 @@ int main(int argc, char** argv) {
     const int rc = parse_options(argc, argv, opt);
     if (rc == 2) return 0;
     if (rc != 0) return 1;
+    if (opt.run_fission) return run_fission(opt);
     return opt.make_grm ? run_make_grm(opt) : run_scan(opt);
   } catch (const Fatal& e) {
     std::cerr << "[E] " << e.what() << '\n';

@@ -1,9 +1,9 @@
 // Command line of the reference program (src/options.cpp:145-179): the same
 // long and short flags, defaults and range checks, for the LM / LMM / NB-GLM
 // models, with PLINK (-b) or VCF (-v, GT or DS) genotypes. The flags of paths
-// outside the device scan (the GLMM model, --fast, the fission subcommand,
-// permutations of the GLM) are recognised and refused with a message instead
-// of being silently ignored.
+// outside the device scan (the GLMM model, --fast, permutations of the GLM)
+// are recognised and refused with a message instead of being silently
+// ignored. `eqtl fission ...` selects the fission subcommand.
 #include <getopt.h>
 
 #include <algorithm>
@@ -49,9 +49,10 @@ void print_help() {
   std::cout << "Program: eqtl (expression QTL mapping, B200 device scan)\n"
                "\n"
                "Usage:   eqtl [options]\n"
+               "         eqtl fission [options]   # data fission + PEER factor estimation\n"
                "\n"
                "Input options:\n"
-               "    -v, --vcf FILE         genotypes VCF (GT; plain or bgzip/gzip)\n"
+               "    -v, --vcf FILE         genotypes VCF (GT or DS; plain or bgzip/gzip)\n"
                "    -b, --bfile PREFIX     PLINK bed/bim/fam prefix\n"
                "    -e, --pheno FILE       phenotype matrix (col1=sample)\n"
                "    -g, --gff FILE         GFF3 gene annotation (TSS)\n"
@@ -71,11 +72,18 @@ void print_help() {
                "        --maf FLOAT        min MAF on analysis samples  [0=off]\n"
                "        --pheno-norm STR   per-gene phenotype normalization none|int  [none]\n"
                "\n"
+               "Fission options (subcommand: eqtl fission ...):\n"
+               "    -c, --covar FILE       residualize known covars from Y1 before PEER\n"
+               "        --peer-factors INT number of PEER factors to estimate  [10]\n"
+               "        --epsilon FLOAT    thinning fraction (0,1)  [0.5]\n"
+               "        --fission-max-iter INT  max PEER iterations  [1000]\n"
+               "        --fission-tol FLOAT     PEER convergence tolerance  [1e-3]\n"
+               "\n"
                "Permutation options:\n"
                "        --perm INT         gene-level permutations  [0=off]\n"
                "        --perm-trans-thr FLOAT  trans/gw: stage-2 if obs min-p < thr  [1e-5]\n"
                "        --perm-trans-top INT    trans/gw: top-K SNPs for stage-2 perm  [1000]\n"
-               "        --seed INT         permutation seed\n"
+               "        --seed INT         permutation / fission seed\n"
                "        --disable-beta-approx  omit beta-approximated p\n"
                "\n"
                "Output options:\n"
@@ -92,10 +100,15 @@ int parse_options(int argc, char** argv, Options& opt) {
     print_help();
     return 2;
   }
-  if (argc >= 2 && std::string(argv[1]) == "fission") die("the fission subcommand is outside the device scan");
+  // subcommand: eqtl fission [...]
+  int start = 1;
+  if (argc >= 2 && std::string(argv[1]) == "fission") {
+    opt.run_fission = true;
+    start = 2;
+  }
   enum {
     kGffIdKey = 1001, kMakeGrm, kModel, kPvalCis, kPvalTrans, kMissHand, kFast, kPerm, kSeed, kNoBeta, kVersion,
-    kMaxMiss, kMaf, kPermThr = 1020, kPermTop, kPhenoNorm
+    kMaxMiss, kMaf, kPeerFactors, kEpsilon, kFissionMaxIter, kFissionTol, kPermThr = 1020, kPermTop, kPhenoNorm
   };
   static struct option long_opts[] = {{"vcf", required_argument, nullptr, 'v'},
                                       {"bfile", required_argument, nullptr, 'b'},
@@ -124,11 +137,15 @@ int parse_options(int argc, char** argv, Options& opt) {
                                       {"perm-trans-top", required_argument, nullptr, kPermTop},
                                       {"seed", required_argument, nullptr, kSeed},
                                       {"disable-beta-approx", no_argument, nullptr, kNoBeta},
+                                      {"peer-factors", required_argument, nullptr, kPeerFactors},
+                                      {"epsilon", required_argument, nullptr, kEpsilon},
+                                      {"fission-max-iter", required_argument, nullptr, kFissionMaxIter},
+                                      {"fission-tol", required_argument, nullptr, kFissionTol},
                                       {"help", no_argument, nullptr, 'h'},
                                       {"version", no_argument, nullptr, kVersion},
                                       {nullptr, 0, nullptr, 0}};
   bool help = false, version = false;
-  optind = 1;
+  optind = start;
   int c, idx;
   while ((c = getopt_long(argc, argv, "v:b:e:o:g:c:k:m:w:t:h", long_opts, &idx)) != -1) {
     const std::string a = optarg ? optarg : "";
@@ -179,6 +196,22 @@ int parse_options(int argc, char** argv, Options& opt) {
         opt.maf = std::atof(a.c_str());
         if (opt.maf < 0.0 || opt.maf > 0.5) die("--maf must be in [0,0.5]");
         break;
+      case kPeerFactors:
+        opt.peer_factors = std::atoi(a.c_str());
+        if (opt.peer_factors < 1) die("--peer-factors must be >= 1");
+        break;
+      case kEpsilon:
+        opt.fission_epsilon = std::atof(a.c_str());
+        if (opt.fission_epsilon <= 0.0 || opt.fission_epsilon >= 1.0) die("--epsilon must be in (0,1)");
+        break;
+      case kFissionMaxIter:
+        opt.fission_max_iter = std::atoi(a.c_str());
+        if (opt.fission_max_iter < 1) die("--fission-max-iter must be >= 1");
+        break;
+      case kFissionTol:
+        opt.fission_tol = std::atof(a.c_str());
+        if (opt.fission_tol <= 0.0) die("--fission-tol must be > 0");
+        break;
       case kPhenoNorm:
         if (a == "none" || a == "off") opt.pheno_int = false;
         else if (a == "int" || a == "rank") opt.pheno_int = true;
@@ -194,6 +227,13 @@ int parse_options(int argc, char** argv, Options& opt) {
   if (version) {
     std::cout << "eqtl 0.1.0 (eqtl_b200)\n";
     return 2;
+  }
+  if (opt.run_fission) {
+    if (opt.pheno.empty()) {
+      std::cerr << "[E] fission requires -e/--pheno\n";
+      return 1;
+    }
+    return 0;
   }
   if (opt.vcf.empty() == opt.bfile.empty()) {
     if (opt.vcf.empty()) std::cerr << "[E] need exactly one of -v/--vcf or -b/--bfile\n";

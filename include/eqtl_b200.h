@@ -135,6 +135,20 @@ int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, 
  * they are, as is a column with at most one finite value. */
 int eqtl_pheno_int(eqtl_ctx* ctx, double* Y, int32_t n, int32_t n_cols);
 
+/* ------------------------------------------------------------- fission
+ * Replaces peer_factors (src/fission.cpp:203-275): PEER variational factor
+ * analysis of Y [n, n_genes] (column-major host memory; each gene is centred
+ * over its values that are not NaN, NaN counts as 0) with K factors, from
+ * the starting factors X0 [n, K] and loadings W0 [n_genes, K] (column-major;
+ * the reference draws X0 then W0, column by column, from
+ * std::normal_distribution on std::mt19937(seed + 1)). Iterates the W,
+ * Alpha, X and Eps updates until the mean squared residual moves by less
+ * than 1e-8 or tol, at most max_iter times. X_out [n, K] receives the
+ * factors, iters_out (optional) the iterations run. 1 <= K <= 96 and
+ * K < min(n, n_genes). */
+int eqtl_peer(eqtl_ctx* ctx, const double* Y, int32_t n, int32_t n_genes, int32_t K, int32_t max_iter, double tol,
+              const double* X0, const double* W0, double* X_out, int32_t* iters_out);
+
 /* ------------------------------------------------------- scan result types */
 typedef struct {
   int32_t n_tested;      /* finite tests counted (GeneSummary.n_tested) */
