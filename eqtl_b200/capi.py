@@ -26,7 +26,7 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
            "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
-           "eqtl_peer"]
+           "eqtl_peer", "eqtl_glm_mu"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -78,6 +78,7 @@ def load() -> C.CDLL:
         lib.eqtl_geno_load_dosage.argtypes = [vp, vp, i64, i32, vp, i32, i32, dp, dp, vp, vp, vp, vp]
         lib.eqtl_geno_dosage.argtypes = [vp, i64, i64, vp]
         lib.eqtl_pheno_int.argtypes = [vp, vp, i32, i32]
+        lib.eqtl_glm_mu.argtypes = [vp, vp]
         lib.eqtl_peer.argtypes = [vp, vp, i32, i32, i32, i32, dp, vp, vp, vp, C.POINTER(i32)]
         lib.eqtl_geno_dosage_rows.argtypes = [vp, vp, i64, vp]
         lib.eqtl_test_pairs.argtypes = [vp, i32, vp, vp, vp, vp, vp, i64, vp, vp]

@@ -816,6 +816,15 @@ int eqtl_scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, c
   });
 }
 
+int eqtl_glm_mu(eqtl_ctx* ctx, double* mu_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(mu_out, EQTL_E_ARG, "null output");
+    EQTL_CHECK(ctx->ws.glm_mu.p && ctx->ws.glm_mu.n > 0, EQTL_E_STATE, "no GLM scan has run");
+    ctx->ws.glm_mu.download(mu_out, ctx->ws.glm_mu.n, ctx->stream);
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
 int eqtl_scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                        eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap, int64_t* n_pairs,
                        eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands) {

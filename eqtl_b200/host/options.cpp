@@ -1,9 +1,8 @@
 // Command line of the reference program (src/options.cpp:145-179): the same
 // long and short flags, defaults and range checks, for the LM / LMM / NB-GLM
 // models, with PLINK (-b) or VCF (-v, GT or DS) genotypes. The flags of paths
-// outside the device scan (the GLMM model, --fast, permutations of the GLM)
-// are recognised and refused with a message instead of being silently
-// ignored. `eqtl fission ...` selects the fission subcommand.
+// outside the device scan (the GLMM model, --fast) are recognised and
+// refused with a message instead of being silently ignored. `eqtl fission ...` selects the fission subcommand.
 #include <getopt.h>
 
 #include <algorithm>
@@ -249,8 +248,6 @@ int parse_options(int argc, char** argv, Options& opt) {
   if (opt.pheno_int && std::find(opt.models.begin(), opt.models.end(), "glm") != opt.models.end())
     die("--pheno-norm int is incompatible with count model glm (apply INT only for lm/lmm; count models need raw "
         "integer counts)");
-  if (opt.perm > 0 && std::find(opt.models.begin(), opt.models.end(), "glm") != opt.models.end())
-    die("--perm with --model glm (parametric NB resampling) is outside the device scan");
   return 0;
 }
 

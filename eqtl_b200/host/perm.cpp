@@ -10,6 +10,11 @@
 // with (seed or 1) + 9973 b + fnv1a(gene) through std::shuffle, so the index
 // sequences are the reference's; columns are built on all host threads,
 // one batch ahead of the device.
+//   GLM   parametric: after the same shuffle draws, y_i ~ Poisson(Gamma(1/phi,
+//         phi mu_i)) from the observed null fit (Poisson(mu_i) when phi <= 1e-9,
+//         0 when mu_i <= 1e-12), with the standard library's distributions
+//         on the same generator (include/eqtl/scan_cis.hpp:115-127); every
+//         SNP of the gene's scope is tested.
 // Every permuted column gets a fresh null fit on the device. Cis: the banded
 // cis scan of all columns, each with its gene's window; min p = the column's
 // FP64-refined best SNP. Trans/gw stage 2: FP64 tests of the gene's top-K
@@ -136,6 +141,30 @@ void permuted_column(const Study& st, const std::string& model, const PermBase& 
   for (size_t j = 0; j < n; ++j) col[j] = B.xb0[j] + B.base[idx[j]] / std::sqrt(std::max(B.dinv[j], 1e-12));
 }
 
+// Column of permutation b of a GLM gene: NB resampling of its null means.
+void glm_column(const Options& opt, const PermGene& g, int b, double* col) {
+  const size_t n = g.mu.size();
+  std::vector<int> idx(n);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::mt19937 rng(perm_seed(opt.seed, b, g.name));
+  std::shuffle(idx.begin(), idx.end(), rng);  // drawn as the reference draws it, then unused
+  for (size_t i = 0; i < n; ++i) {
+    const double mu = g.mu[i];
+    if (mu <= 1e-12) {
+      col[i] = 0.0;
+      continue;
+    }
+    if (g.phi > 1e-9) {
+      std::gamma_distribution<double> gam(1.0 / g.phi, g.phi * mu);
+      std::poisson_distribution<long> pois(gam(rng));
+      col[i] = static_cast<double>(pois(rng));
+    } else {
+      std::poisson_distribution<long> pois(mu);
+      col[i] = static_cast<double>(pois(rng));
+    }
+  }
+}
+
 template <class F>
 void parallel_for(size_t n, F&& f) {
   const size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(n, 1));
@@ -161,7 +190,8 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   std::vector<PermOut> out(genes.size());
   std::vector<size_t> active;
   for (size_t j = 0; j < genes.size(); ++j)
-    if (genes[j].active && (genes[j].window || !genes[j].snps.empty())) active.push_back(j);
+    if (genes[j].active && (genes[j].window || !genes[j].snps.empty() || genes[j].scan_mode >= 0))
+      active.push_back(j);
   if (active.empty() || B <= 0) return out;
   const bool lmm = model == "lmm";
   if (lmm && st.basis_Q.size() != n * n) die("internal: LMM permutations need the eigenbasis on the host");
@@ -186,12 +216,16 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   auto build = [&](size_t a) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
+    std::vector<double> Y(cols * n);
+    if (model == "glm") {
+      parallel_for(cols, [&](size_t c) { glm_column(opt, genes[active[a + c / B]], static_cast<int>(c % B), &Y[c * n]); });
+      return Y;
+    }
     std::vector<PermBase> bases(nb);
     parallel_for(nb, [&](size_t gi) {
       const PermGene& g = genes[active[a + gi]];
       bases[gi] = lmm ? lmm_base(st, g.y, delta[active[a + gi]], Xt) : lm_base(st, g.y);
     });
-    std::vector<double> Y(cols * n);
     parallel_for(cols, [&](size_t c) {
       const size_t gi = c / B;
       permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &Y[c * n]);
@@ -206,7 +240,15 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
     if (a + genes_per_batch < active.size()) next = std::async(std::launch::async, build, a + genes_per_batch);
     tr.mark("permutations: " + std::to_string(cols) + " columns ready (host build overlapped)");
     std::vector<double> minp(cols, 1.0);
-    if (genes[active[a]].window) {
+    if (model == "glm") {
+      // every SNP of each gene's scope, with a fresh NB null fit per column
+      std::vector<const GeneLoc*> win(cols);
+      for (size_t c = 0; c < cols; ++c) win[c] = genes[active[a + c / B]].window;
+      const ScanResult R = scan_columns(st, model, Y, cols, win, genes[active[a]].scan_mode, 0.0, 0.0, false);
+      for (size_t c = 0; c < cols; ++c)
+        if (R.genes[c].n_tested > 0 && R.genes[c].best_snp >= 0 && std::isfinite(R.genes[c].best_p))
+          minp[c] = std::min(1.0, R.genes[c].best_p);
+    } else if (genes[active[a]].window) {
       // cis: one banded cis scan of every column with its gene's window
       std::vector<const GeneLoc*> win(cols);
       for (size_t c = 0; c < cols; ++c) win[c] = genes[active[a + c / B]].window;

@@ -22,6 +22,12 @@ struct PermGene {
   bool active = false;              // gene takes part in the permutations
   const GeneLoc* window = nullptr;  // cis: permutations test the gene's window
   std::vector<int64_t> snps;        // trans/gw stage 2: the top-K kept SNPs
+  // NB-GLM: permutations resample counts from the observed null fit and
+  // test every SNP of the scope (scan_mode 0 gw, 1 trans, 2 cis; window =
+  // the gene's location for 1 and 2)
+  std::vector<double> mu;
+  double phi = 0.0;
+  int scan_mode = -1;
 };
 
 struct PermOut {

@@ -480,13 +480,38 @@ void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::ve
     R.conv.swap(conv);
     for (auto& q : R.pairs) q.gene = static_cast<int32_t>(dev_order[q.gene]);
   }
+  std::vector<PermOut> perms;
+  if (opt.perm > 0) {
+    // the observed null means, back in output order
+    std::vector<double> mu_dev(jobs.size() * n), mu(jobs.size() * n);
+    st.dev->check(eqtl_glm_mu(st.dev->ctx, mu_dev.data()), "GLM null means");
+    for (size_t j = 0; j < dev_order.size(); ++j)
+      std::copy(mu_dev.begin() + j * n, mu_dev.begin() + (j + 1) * n, mu.begin() + dev_order[j] * n);
+    std::vector<PermGene> pg(jobs.size());
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      // the reference caches every tested SNP's dosages for its permutations
+      // and stops past 25,000,000 values (include/eqtl/scan_cis.hpp:58-61)
+      if (R.genes[j].n_tested > 1 && static_cast<int64_t>(R.genes[j].n_tested - 1) * static_cast<int64_t>(n) >
+                                         25'000'000)
+        die("cis perm: too many SNPs in cis window for gene " + st.genes[jobs[j].gene] + " — reduce --window");
+      pg[j].name = st.genes[jobs[j].gene];
+      pg[j].obs_min_p = R.genes[j].best_p;
+      pg[j].active = R.genes[j].n_tested > 0;
+      pg[j].mu.assign(mu.begin() + j * n, mu.begin() + (j + 1) * n);
+      pg[j].phi = R.phi[j];
+      pg[j].scan_mode = mode;
+      pg[j].window = mode == 0 ? nullptr : jobs[j].loc;
+    }
+    perms = run_permutations(st, "glm", pg, {});
+    tr.mark(scope + " glm: permutations");
+  }
   std::vector<size_t> order(R.pairs.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
     const eqtl_pair &x = R.pairs[a], &y = R.pairs[b];
     return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
   });
-  emit(st, jobs, R, scope, pthr, order, out, regions, nullptr);
+  emit(st, jobs, R, scope, pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
 }
 
 }  // namespace eqtl_host

@@ -282,6 +282,11 @@ int eqtl_scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, c
                   uint8_t* converged_out, eqtl_gene_result* genes, eqtl_pair* pairs, int64_t pair_cap,
                   int64_t* n_pairs, eqtl_pair* cands, int64_t cand_cap, int64_t* n_cands);
 
+/* The null fits of the most recent eqtl_scan_glm call: mu_out [n, n_genes]
+ * (column-major) receives each gene's fitted means, which the reference's
+ * GLM permutations resample from (include/eqtl/scan_cis.hpp:115-127). */
+int eqtl_glm_mu(eqtl_ctx* ctx, double* mu_out);
+
 /* -------------------------------------------------------------- pair tests
  * FP64 tests of explicit (column of Y, kept SNP) pairs with the scans' own
  * per-column prep: LM (EQTL_MODEL_LM) residualises each column on X

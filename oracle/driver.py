@@ -505,8 +505,6 @@ class Scanner:
     # with -t > 1, src/scan_cis.cpp:18-115; per gene include/eqtl/scan_cis.hpp:15-66)
     def run_glm(self, scope, pthr):
         opt = self.opt
-        if opt.perm > 0:
-            raise NotImplementedError("GLM permutations (parametric NB sampling) are not restated")
         works = []
         for gi, gene in enumerate(self.genes):
             loc = self.annot.get(gene) if opt.gff else None
@@ -546,6 +544,7 @@ class Scanner:
             prep = R.prep_glm_nb(yk, Xk)
             acc = R.AcatAcc()
             best_p, best_row = 2.0, None
+            cached = []
             if snps:
                 G = self.dec.dosage[np.array(snps)][:, keep]
                 af_sub, ok = R.subset_maf(G)
@@ -565,8 +564,25 @@ class Scanner:
                         s.n_sig += 1
                     if pv < best_p:
                         best_p, best_row = pv, row
+                    cached.append(G[i])
             s.acat = acc.p()
             s.acat_sens = acc.log10_sensitivity()
+            if opt.perm > 0 and s.n_tested > 0:
+                # parametric NB resampling of the null fit (include/eqtl/scan_cis.hpp:106-127)
+                if (len(cached) - 1) * len(keep) > 25_000_000:
+                    raise ValueError("cis perm: too many SNPs in cis window for gene " + gene)
+                Ys = R.nb_resample(prep.mu, prep.phi, [R.perm_seed(opt.seed, b, gene) for b in range(opt.perm)])
+                Gc = np.array(cached)
+                T_perm, minps = [], []
+                for b in range(opt.perm):
+                    pv = R.test_glm_nb_many(R.prep_glm_nb(Ys[b], Xk), Gc)["p"]
+                    pv = pv[np.isfinite(pv)]
+                    minp = min(1.0, float(pv.min())) if pv.size else 1.0
+                    T_perm.append(-math.log10(max(minp, 1e-300)))
+                    minps.append(minp)
+                s.p_emp = R.p_emp_count(-math.log10(max(best_p, 1e-300)), T_perm)
+                if not opt.disable_beta_approx:
+                    s.p_beta, s.s1, s.s2 = R.beta_approx_p(minps, best_p)
             if best_row is not None and best_p <= pthr and best_p <= 1.0:
                 tops.append(best_row)
             summ.append(s)

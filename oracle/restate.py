@@ -1045,6 +1045,17 @@ def perm_seed(seed_opt: int, b: int, gene: str) -> int:
     return (base + b * 9973 + fnv1a(gene)) & 0xFFFFFFFF
 
 
+def nb_resample(mu: np.ndarray, phi: float, seeds: Sequence[int]) -> np.ndarray:
+    """The reference's GLM permutation phenotypes (include/eqtl/scan_cis.hpp:
+    106-127) drawn by the standard library itself (oracle/_ref/nbresample):
+    one row of counts per seed."""
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "nbresample")
+    inp = f"{len(mu)} {phi!r}\n" + " ".join(repr(float(m)) for m in mu) + f"\n{len(seeds)}\n" + \
+        " ".join(str(int(s)) for s in seeds) + "\n"
+    out = subprocess.run([exe], input=inp, check=True, capture_output=True, text=True).stdout
+    return np.array([[float(v) for v in ln.split()] for ln in out.strip().split("\n")])
+
+
 # ---------------------------------------------------------------------------
 # PEER VB factor analysis of the fission subcommand (src/fission.cpp:104-275)
 # ---------------------------------------------------------------------------

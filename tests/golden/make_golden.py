@@ -55,6 +55,8 @@ CASES = {
             ("gw", ["--model", "glm", "--mode", "gw", "--pval-trans", "1e-2", "-t", "1"]),
             ("mixed", ["--model", "lm,glm", "--mode", "trans", "--miss-hand", "filter", "--maf", "0.05",
                        "--pval-trans", "5e-3", "-t", "1"]),
+            ("perm", ["--model", "glm", "--mode", "all", "-w", "500000", "--pval-cis", "1e-2",
+                      "--pval-trans", "1e-2", "--perm", "20", "--seed", "11", "-t", "1"]),
         ]),
     "nogff": dict(
         geno=dict(seed=201, n=96, m=600, n_chrom=2, chrom_len=3_000_000, family=None,

@@ -141,8 +141,8 @@ def test_cli_help_and_refusals():
     assert r.returncode == 1 and "missing -e/--pheno" in r.stderr
     r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--model", "glmm"], capture_output=True, text=True)
     assert r.returncode == 1 and "glmm" in r.stderr
-    r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--model", "glm", "--perm", "10"], capture_output=True,
-                       text=True)
-    assert r.returncode == 1 and "--perm with --model glm" in r.stderr
+    r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--model", "lm,glm", "--pheno-norm", "int"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "--pheno-norm int is incompatible with count model glm" in r.stderr
     r = subprocess.run([exe, "-b", "geno", "-e", "p.tsv", "--maf", "0.7"], capture_output=True, text=True)
     assert r.returncode == 1 and "--maf must be in [0,0.5]" in r.stderr
