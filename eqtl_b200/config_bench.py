@@ -12,6 +12,8 @@ lm   trans/gw LM scan: n = 1,000 samples, m = 1,000,000 SNPs, 20,000 genes
 glm  gw NB-GLM scan: n = 1,000 samples, m = 200,000 SNPs, 5,000 genes of
      negative-binomial counts (synth.make_pheno_counts), intercept + 2
      covariates, p threshold 1e-5.
+fission  PEER factors (15) of a 500 x 20,000 count table, and the
+     rank-based inverse normal transform of the same table.
 
 Seeded synthetic data of those shapes (no data set ships with the
 reference). Each JSON line gives the CUDA-event stage times (median over the
@@ -135,6 +137,35 @@ def glm_case(steps: int, m: int = 200_000, G: int = 5_000) -> dict:
             "peak_tflops": peak, "peak_source": kind, "data": "synthetic"}
 
 
+def fission_case(steps: int, n: int = 500, G: int = 20_000, k: int = 15) -> dict:
+    """PEER on the device (eqtl_peer) for a thinned count table of n samples
+    x G genes with k factors and the reference's defaults (tol 1e-3, at most
+    1000 iterations), from the reference's N(0, 1) starting values."""
+    import time
+    rng = np.random.default_rng(20261207)
+    Y, _ = synth.make_pheno_counts(20261208, None, G, 0, n=n)
+    X0 = rng.standard_normal((n, k))
+    W0 = rng.standard_normal((G, k))
+    times, iters = [], 0
+    with capi.Context(0) as c:
+        for i in range(steps + 1):
+            t0 = time.perf_counter()
+            _, iters = c.peer(Y, k, 1000, 1e-3, X0, W0)
+            if i:
+                times.append(1e3 * (time.perf_counter() - t0))
+        t_int = []
+        for i in range(steps + 1):
+            t0 = time.perf_counter()
+            c.pheno_int(Y)
+            if i:
+                t_int.append(1e3 * (time.perf_counter() - t0))
+    return {"workload": "fission PEER + --pheno-norm int", "n_samples": n, "n_genes": G, "factors": k,
+            "peer_iterations": iters, "peer_ms_steps": times, "peer_ms": statistics.median(times),
+            "int_ms_steps": t_int, "int_ms": statistics.median(t_int),
+            "note": "wall time of the C-ABI calls from host buffers (upload, device work, download)",
+            "data": "synthetic"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--which", default="grm,lm")
@@ -147,6 +178,8 @@ def main() -> None:
             out = grm_case(args.steps)
         elif w == "glm":
             out = glm_case(args.steps)
+        elif w == "fission":
+            out = fission_case(args.steps)
         else:
             out = lm_case(args.steps, args.lm_snps, args.lm_genes)
         print(json.dumps(out), flush=True)

@@ -650,6 +650,19 @@ int eqtl_geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int32_t n_f
   });
 }
 
+int eqtl_vcf_parse(eqtl_ctx* ctx, const char* text, int64_t text_len, const int64_t* beg, const int64_t* end,
+                   const int32_t* gt_at, const int32_t* ds_at, int64_t n_rec, int32_t n_file, int32_t dense,
+                   uint8_t* codes_out, float* ds_out, uint8_t* hap_out, uint8_t* flag_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK((text || text_len == 0) && ((beg && end && gt_at && ds_at && hap_out && flag_out) || n_rec == 0),
+               EQTL_E_ARG, "null input");
+    EQTL_CHECK(dense ? (ds_out != nullptr || n_rec == 0) : (codes_out != nullptr || n_rec == 0), EQTL_E_ARG,
+               "null output");
+    eqtl::vcf_parse(ctx, text, text_len, beg, end, gt_at, ds_at, n_rec, n_file, dense, codes_out, ds_out, hap_out,
+                    flag_out);
+  });
+}
+
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out) {
   return guarded(ctx, [&] {
     EQTL_CHECK(out || hi == lo, EQTL_E_ARG, "null output");

@@ -272,6 +272,10 @@ void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host);
 // Rank-based inverse normal transform of each of the G columns of Y_host
 // [G][n], in place (computed on the device).
 void pheno_int(eqtl_ctx* ctx, double* Y_host, int n, int G);
+// VCF sample columns of R records parsed on the device (see vcf_parse.cu).
+void vcf_parse(eqtl_ctx* ctx, const char* text, int64_t text_len, const int64_t* beg, const int64_t* end,
+               const int32_t* gt_at, const int32_t* ds_at, int64_t R, int n_file, int dense, uint8_t* codes_out,
+               float* ds_out, uint8_t* hap_out, uint8_t* flag_out);
 // PEER factors of Y_host [n, G] (column-major) from the starting X0 [n, K]
 // and W0 [G, K]; returns the iterations run.
 int peer_factors(eqtl_ctx* ctx, const double* Y_host, int n, int G, int K, int max_iter, double tol,

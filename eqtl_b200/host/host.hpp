@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -93,7 +94,9 @@ struct VcfInfo {
   std::vector<std::vector<int32_t>> hap_calls;  // per record elsewhere: file columns with a haploid call
   int64_t n_multi = 0;                          // records skipped as not biallelic
 };
-Plink read_vcf(const std::string& path, VcfInfo& vi);
+// The calls are parsed on the device of the context that `ctx()` returns
+// (opened when first needed).
+Plink read_vcf(const std::string& path, VcfInfo& vi, const std::function<eqtl_ctx*()>& ctx);
 // Keeps the records that pass the reference's VCF filters over the analysis
 // samples `cols` (file columns): calls present, missing fraction, ploidy-
 // aware allele frequency not monomorphic, --miss-hand filter, --maf.

@@ -45,9 +45,14 @@ std::vector<std::string> overlap(const std::vector<std::string>& pheno, const Pl
   return out;
 }
 
-// PLINK or VCF genotypes of the run (-b / -v).
-Plink read_genotypes(const Options& opt, VcfInfo& vi) {
-  return opt.vcf.empty() ? read_plink(opt.bfile) : read_vcf(opt.vcf, vi);
+// PLINK or VCF genotypes of the run (-b / -v); a VCF's calls are parsed on
+// the device, which `dev` then holds.
+Plink read_genotypes(const Options& opt, VcfInfo& vi, std::unique_ptr<Device>& dev) {
+  if (opt.vcf.empty()) return read_plink(opt.bfile);
+  return read_vcf(opt.vcf, vi, [&]() {
+    if (!dev) dev = std::make_unique<Device>();
+    return dev->ctx;
+  });
 }
 
 // Options for the device decode: a VCF has been filtered on the host with
@@ -63,14 +68,16 @@ Options device_filters(const Options& opt) {
 
 int run_make_grm(const Options& opt) {
   VcfInfo vi;
-  Plink P = read_genotypes(opt, vi);
+  std::unique_ptr<Device> devp;
+  Plink P = read_genotypes(opt, vi, devp);
   std::vector<std::string> samples = P.fam_iid;
   if (!opt.pheno.empty()) {
     samples = overlap(load_pheno(opt.pheno).samples, P);
     if (samples.empty()) die("no overlapping samples for GRM");
   }
   if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, samples), opt);
-  Device dev;
+  if (!devp) devp = std::make_unique<Device>();
+  Device& dev = *devp;
   Genotypes geno(dev, P, sample_columns(P, samples), device_filters(opt));
   const int n = static_cast<int>(samples.size());
   std::vector<double> K(static_cast<size_t>(n) * n);
@@ -84,7 +91,8 @@ int run_make_grm(const Options& opt) {
 
 int run_scan(const Options& opt) {
   VcfInfo vi;
-  Plink P = read_genotypes(opt, vi);
+  std::unique_ptr<Device> devp;
+  Plink P = read_genotypes(opt, vi, devp);
   Pheno ph = load_pheno(opt.pheno);
   Study st;
   st.opt = &opt;
@@ -131,7 +139,8 @@ int run_scan(const Options& opt) {
     die("cis mode requires an indexed genotype file; for VCF run: tabix -p vcf <file>.vcf.gz");
 
   if (!opt.vcf.empty()) vcf_filter(P, vi, sample_columns(P, st.samples), opt);
-  Device dev;
+  if (!devp) devp = std::make_unique<Device>();
+  Device& dev = *devp;
   if (opt.pheno_int) {  // every gene's rank-based inverse normal transform, on the device
     st.Y_int = st.Y;
     dev.check(eqtl_pheno_int(dev.ctx, st.Y_int.data(), static_cast<int32_t>(n), static_cast<int32_t>(G)),

@@ -16,10 +16,12 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 #include "host.hpp"
 
@@ -34,43 +36,6 @@ namespace {
 // missing; the value is used as it is, as an FP32 number); any other record
 // gives its GT counts (:193-258). Both kinds then share the FP32 rows.
 //
-// Line reader over gzread (which also reads uncompressed files as they are).
-struct GzLines {
-  gzFile f = nullptr;
-  std::vector<char> buf;
-  size_t beg = 0, end = 0;
-  bool eof = false;
-  explicit GzLines(const std::string& path) : buf(1 << 20) {
-    f = gzopen(path.c_str(), "rb");
-    if (!f) die("cannot open VCF/BCF: " + path);
-    gzbuffer(f, 1 << 18);
-  }
-  ~GzLines() {
-    if (f) gzclose(f);
-  }
-  // next line without its newline; false at the end of the file
-  bool next(std::string& line) {
-    line.clear();
-    while (true) {
-      const char* s = buf.data() + beg;
-      const void* nl = beg < end ? std::memchr(s, '\n', end - beg) : nullptr;
-      if (nl) {
-        const size_t len = static_cast<const char*>(nl) - s;
-        line.append(s, len);
-        beg += len + 1;
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        return true;
-      }
-      line.append(s, end - beg);
-      beg = end = 0;
-      if (eof) return !line.empty();
-      const int got = gzread(f, buf.data(), static_cast<unsigned>(buf.size()));
-      if (got < 0) die("VCF read error");
-      if (got == 0) eof = true;
-      end = static_cast<size_t>(got);
-    }
-  }
-};
 
 // X, Y and MT, with or without a "chr" prefix (src/vcf_session.cpp:148-157)
 bool haploid_chrom(const std::string& chrom) {
@@ -158,21 +123,120 @@ float parse_ds(const char* s, size_t len) {
 
 }  // namespace
 
-Plink read_vcf(const std::string& path, VcfInfo& vi) {
-  GzLines in(path);
-  Plink P;
-  std::string line;
-  bool have_header = false;
-  if (!in.next(line)) die("empty VCF: " + path);
-  if (line.compare(0, 3, "BCF") == 0)
+namespace {
+
+// The whole file as text: a BGZF file (gzip members with the BC extra field,
+// each member at most 64 KiB of text) is inflated member by member on all
+// host threads, any other gzip stream through gzread, plain text as it is.
+std::string read_all(const std::string& path) {
+  std::string raw;
+  {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) die("cannot open VCF/BCF: " + path);
+    char buf[1 << 16];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof(buf), f)) > 0) raw.append(buf, got);
+    std::fclose(f);
+  }
+  const auto u8 = [&](size_t k) { return static_cast<uint8_t>(raw[k]); };
+  const auto le16 = [&](size_t k) { return static_cast<uint32_t>(u8(k)) | (static_cast<uint32_t>(u8(k + 1)) << 8); };
+  const auto le32 = [&](size_t k) { return le16(k) | (le16(k + 2) << 16); };
+  if (raw.size() < 2 || u8(0) != 0x1f || u8(1) != 0x8b) return raw;  // plain text
+  // BGZF members: (offset, compressed data offset, data bytes, text bytes)
+  struct Member {
+    size_t off, data, len, isize;
+  };
+  std::vector<Member> mem;
+  bool bgzf = true;
+  for (size_t off = 0; off < raw.size() && bgzf;) {
+    if (off + 18 > raw.size() || u8(off) != 0x1f || u8(off + 1) != 0x8b || u8(off + 2) != 8 || !(u8(off + 3) & 4)) {
+      bgzf = false;
+      break;
+    }
+    const size_t xlen = le16(off + 10);
+    size_t bsize = 0;
+    for (size_t x = off + 12; x + 4 <= off + 12 + xlen && x + 4 <= raw.size();) {
+      const size_t slen = le16(x + 2);
+      if (u8(x) == 'B' && u8(x + 1) == 'C' && slen == 2) bsize = le16(x + 4) + 1;
+      x += 4 + slen;
+    }
+    if (bsize == 0 || off + bsize > raw.size() || bsize < 12 + xlen + 8) {
+      bgzf = false;
+      break;
+    }
+    mem.push_back({off, off + 12 + xlen, bsize - 12 - xlen - 8, le32(off + bsize - 4)});
+    off += bsize;
+  }
+  if (!bgzf) {  // a gzip stream that is not BGZF
+    gzFile f = gzopen(path.c_str(), "rb");
+    if (!f) die("cannot open VCF/BCF: " + path);
+    std::string text;
+    std::vector<char> buf(1 << 20);
+    int got;
+    while ((got = gzread(f, buf.data(), static_cast<unsigned>(buf.size()))) > 0) text.append(buf.data(), got);
+    const bool err = got < 0;
+    gzclose(f);
+    if (err) die("VCF read error");
+    return text;
+  }
+  std::vector<size_t> at(mem.size() + 1, 0);
+  for (size_t k = 0; k < mem.size(); ++k) at[k + 1] = at[k] + mem[k].isize;
+  std::string text(at.back(), '\0');
+  std::atomic<bool> bad{false};
+  const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), mem.size()));
+  std::vector<std::thread> th;
+  for (size_t t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (size_t k = t; k < mem.size(); k += nt) {
+        if (mem[k].isize == 0) continue;
+        z_stream zs{};
+        if (inflateInit2(&zs, -15) != Z_OK) {
+          bad = true;
+          return;
+        }
+        zs.next_in = reinterpret_cast<Bytef*>(&raw[mem[k].data]);
+        zs.avail_in = static_cast<uInt>(mem[k].len);
+        zs.next_out = reinterpret_cast<Bytef*>(&text[at[k]]);
+        zs.avail_out = static_cast<uInt>(mem[k].isize);
+        const int rc = inflate(&zs, Z_FINISH);
+        if (rc != Z_STREAM_END || zs.total_out != mem[k].isize) bad = true;
+        inflateEnd(&zs);
+      }
+    });
+  for (auto& x : th) x.join();
+  if (bad) die("VCF read error (BGZF member)");
+  return text;
+}
+
+}  // namespace
+
+Plink read_vcf(const std::string& path, VcfInfo& vi, const std::function<eqtl_ctx*()>& get_ctx) {
+  Trace tr;
+  const std::string text = read_all(path);
+  tr.mark("VCF: read and inflate " + std::to_string(text.size()) + " bytes");
+  if (text.empty()) die("empty VCF: " + path);
+  if (text.compare(0, 3, "BCF") == 0)
     die("BCF input is not read by this build; convert with bcftools view -Oz to a VCF");
-  std::vector<const char*> fld;
-  std::vector<size_t> flen;
+  Plink P;
+  bool have_header = false;
   int64_t n_rec = 0;
   bool prefer_ds = false, ds_float = false, said_ds = false;
-  do {
-    if (line.empty()) continue;
-    if (line[0] == '#') {
+  // records kept: where their sample columns lie, the FORMAT positions used
+  std::vector<int64_t> beg, end;
+  std::vector<int32_t> gt_at_v, ds_at_v;
+  const char* T = text.data();
+  const size_t N = text.size();
+  for (size_t ls = 0; ls < N;) {
+    const void* nl = std::memchr(T + ls, '\n', N - ls);
+    size_t le = nl ? static_cast<const char*>(nl) - T : N;
+    const size_t next = nl ? le + 1 : N;
+    if (le > ls && T[le - 1] == '\r') --le;
+    if (le == ls) {
+      ls = next;
+      continue;
+    }
+    if (T[ls] == '#') {
+      const std::string line(T + ls, le - ls);
       const bool fmt_line = line.compare(0, 10, "##FORMAT=<") == 0;
       if (fmt_line || line.compare(0, 8, "##INFO=<") == 0 || line.compare(0, 10, "##FILTER=<") == 0) {
         std::string id, type;
@@ -199,32 +263,34 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
         P.dense = prefer_ds;
         if (prefer_ds) info("VCF: FORMAT/DS present -> use dosage field when available");
       }
+      ls = next;
       continue;
     }
     if (!have_header) die("VCF record before the #CHROM header line: " + path);
     ++n_rec;
-    fld.clear();
-    flen.clear();
-    size_t a = 0;
-    while (a <= line.size()) {
-      size_t b = line.find('\t', a);
-      if (b == std::string::npos) b = line.size();
-      fld.push_back(line.data() + a);
-      flen.push_back(b - a);
-      a = b + 1;
+    // the nine fixed columns
+    size_t f[10];
+    f[0] = ls;
+    int nf = 1;
+    for (size_t a = ls; nf < 10;) {
+      const void* tb = a < le ? std::memchr(T + a, '\t', le - a) : nullptr;
+      if (!tb) break;
+      a = static_cast<const char*>(tb) - T + 1;
+      f[nf++] = a;
     }
-    if (fld.size() < 9 + static_cast<size_t>(P.n_file)) die("VCF record with fewer sample columns than the header");
-    const std::string alt(fld[4], flen[4]);
+    if (nf < 10) die("VCF record with fewer sample columns than the header");
+    auto col = [&](int k) { return std::string(T + f[k], f[k + 1] - 1 - f[k]); };
+    const std::string alt = col(4);
     if (alt == "." || alt.find(',') != std::string::npos) {  // not biallelic (n_allele != 2)
       ++vi.n_multi;
+      ls = next;
       continue;
     }
-    // GT's and DS's positions among the FORMAT keys
     int gt_at = -1, ds_at = -1;
     {
       int k = 0;
       size_t s = 0;
-      const std::string fmt(fld[8], flen[8]);
+      const std::string fmt = col(8);
       while (s <= fmt.size()) {
         size_t e = fmt.find(':', s);
         if (e == std::string::npos) e = fmt.size();
@@ -235,48 +301,93 @@ Plink read_vcf(const std::string& path, VcfInfo& vi) {
       }
     }
     const bool use_ds = prefer_ds && ds_float && ds_at >= 0;
-    if (!use_ds && gt_at < 0) continue;  // no genotypes in this record
+    if (!use_ds && gt_at < 0) {  // no genotypes in this record
+      ls = next;
+      continue;
+    }
     if (use_ds && !said_ds) {
       info("VCF: using FORMAT/DS dosages");
       said_ds = true;
     }
-    const std::string chrom(fld[0], flen[0]);
-    const bool hap = haploid_chrom(chrom);
-    std::vector<uint8_t> row(P.dense ? 0 : static_cast<size_t>(P.bytes_per_snp), 0);
-    std::vector<float> drow(P.dense ? static_cast<size_t>(P.n_file) : 0);
-    std::vector<int32_t> hap_calls;
-    for (int i = 0; i < P.n_file; ++i) {
-      const char* s = fld[9 + i];
-      const size_t len = flen[9 + i];
-      size_t p0 = 0, p1 = 0;
-      if (use_ds) {
-        drow[static_cast<size_t>(i)] = subfield(s, len, ds_at, p0, p1) ? parse_ds(s + p0, p1 - p0)
-                                                                         : std::numeric_limits<float>::quiet_NaN();
-        continue;
-      }
-      // the GT subfield of this sample (absent trailing subfields are missing)
-      bool haploid = false;
-      const int d = (subfield(s, len, gt_at, p0, p1) && p1 > p0) ? parse_gt(s + p0, p1 - p0, haploid) : -1;
-      if (P.dense) {
-        drow[static_cast<size_t>(i)] = d < 0 ? std::numeric_limits<float>::quiet_NaN() : static_cast<float>(d);
-      } else {
-        const uint32_t code = d < 0 ? 1u : (d == 2 ? 0u : (d == 1 ? 2u : 3u));
-        row[static_cast<size_t>(i >> 2)] |= static_cast<uint8_t>(code << ((i & 3) * 2));
-      }
-      if (d >= 0 && haploid && !hap) hap_calls.push_back(i);
-    }
+    const std::string chrom = col(0);
     P.chrom.push_back(chrom);
-    P.pos.push_back(std::stoll(std::string(fld[1], flen[1])));
-    const std::string id(fld[2], flen[2]);
+    P.pos.push_back(std::stoll(col(1)));
+    const std::string id = col(2);
     P.id.push_back(id == "." ? std::string() : id);
-    P.a2.push_back(std::string(fld[3], flen[3]));  // REF
-    P.a1.push_back(alt);                            // ALT, the counted allele
-    P.rows.insert(P.rows.end(), row.begin(), row.end());
-    P.ds.insert(P.ds.end(), drow.begin(), drow.end());
-    vi.hap_chrom.push_back(hap ? 1 : 0);
-    vi.hap_calls.push_back(std::move(hap_calls));
-  } while (in.next(line));
+    P.a2.push_back(col(3));  // REF
+    P.a1.push_back(alt);     // ALT, the counted allele
+    vi.hap_chrom.push_back(haploid_chrom(chrom) ? 1 : 0);
+    beg.push_back(static_cast<int64_t>(f[9]));
+    end.push_back(static_cast<int64_t>(le));
+    gt_at_v.push_back(gt_at);
+    ds_at_v.push_back(use_ds ? ds_at : -1);
+    ls = next;
+  }
   if (!have_header) die("VCF without a #CHROM header line: " + path);
+  tr.mark("VCF: fixed columns of " + std::to_string(n_rec) + " records");
+  // the calls, on the device, in batches of at most 1 GiB of text
+  const int64_t R = static_cast<int64_t>(beg.size());
+  const int n = P.n_file;
+  const int64_t bpr = P.bytes_per_snp, hbr = (n + 7) / 8;
+  if (P.dense) P.ds.resize(static_cast<size_t>(R) * n);
+  else P.rows.assign(static_cast<size_t>(R * bpr), 0);
+  std::vector<uint8_t> hap(static_cast<size_t>(R * hbr), 0), flag(static_cast<size_t>(R), 0);
+  eqtl_ctx* ctx = R > 0 ? get_ctx() : nullptr;
+  for (int64_t r0 = 0; r0 < R;) {
+    int64_t r1 = r0 + 1;
+    while (r1 < R && end[r1] - beg[r0] <= (int64_t(1) << 30) && (r1 - r0) * n < (int64_t(1) << 27)) ++r1;
+    const int64_t base = beg[r0];
+    std::vector<int64_t> b(beg.begin() + r0, beg.begin() + r1), e(end.begin() + r0, end.begin() + r1);
+    for (auto& v : b) v -= base;
+    for (auto& v : e) v -= base;
+    const int rc = eqtl_vcf_parse(ctx, T + base, end[r1 - 1] - base, b.data(), e.data(), gt_at_v.data() + r0,
+                                  ds_at_v.data() + r0, r1 - r0, n, P.dense ? 1 : 0,
+                                  P.dense ? nullptr : P.rows.data() + r0 * bpr,
+                                  P.dense ? P.ds.data() + r0 * n : nullptr, hap.data() + r0 * hbr, flag.data() + r0);
+    if (rc != EQTL_OK) die(std::string("VCF parse on the device: ") + eqtl_last_error(ctx));
+    r0 = r1;
+  }
+  tr.mark("VCF: calls parsed on the device");
+  vi.hap_calls.assign(static_cast<size_t>(R), {});
+  for (int64_t r = 0; r < R; ++r) {
+    if (flag[r] == 1) die("VCF record with fewer sample columns than the header");
+    const bool use_ds = ds_at_v[r] >= 0;
+    if (flag[r] == 2) {
+      // a call outside the device parser's fast paths: this record on the host
+      const char* s0 = T + beg[r];
+      size_t a = 0;
+      const size_t len = static_cast<size_t>(end[r] - beg[r]);
+      uint8_t* row = P.dense ? nullptr : P.rows.data() + r * bpr;
+      if (row) std::fill(row, row + bpr, 0);
+      std::fill(hap.begin() + r * hbr, hap.begin() + (r + 1) * hbr, 0);
+      for (int i = 0; i < n; ++i) {
+        size_t b = a;
+        while (b < len && s0[b] != '\t') ++b;
+        const char* s = s0 + a;
+        const size_t sl = b - a;
+        a = b + 1;
+        size_t p0 = 0, p1 = 0;
+        if (use_ds) {
+          P.ds[static_cast<size_t>(r) * n + i] =
+              subfield(s, sl, ds_at_v[r], p0, p1) ? parse_ds(s + p0, p1 - p0) : std::numeric_limits<float>::quiet_NaN();
+          continue;
+        }
+        bool haploid = false;
+        const int d = (subfield(s, sl, gt_at_v[r], p0, p1) && p1 > p0) ? parse_gt(s + p0, p1 - p0, haploid) : -1;
+        if (P.dense) {
+          P.ds[static_cast<size_t>(r) * n + i] = d < 0 ? std::numeric_limits<float>::quiet_NaN() : static_cast<float>(d);
+        } else {
+          const uint32_t code = d < 0 ? 1u : (d == 2 ? 0u : (d == 1 ? 2u : 3u));
+          row[i >> 2] |= static_cast<uint8_t>(code << ((i & 3) * 2));
+        }
+        if (d >= 0 && haploid) hap[static_cast<size_t>(r * hbr + (i >> 3))] |= static_cast<uint8_t>(1u << (i & 7));
+      }
+    }
+    if (use_ds || vi.hap_chrom[static_cast<size_t>(r)]) continue;  // ploidy from the chromosome
+    for (int i = 0; i < n; ++i)
+      if (hap[static_cast<size_t>(r * hbr + (i >> 3))] >> (i & 7) & 1u) vi.hap_calls[static_cast<size_t>(r)].push_back(i);
+  }
+  tr.mark("VCF: host fallbacks and haploid calls");
   if (vi.n_multi > 0)
     info("VCF multi-allelic sites skipped (biallelic only): " + std::to_string(vi.n_multi));
   info("VCF: " + std::to_string(P.chrom.size()) + " biallelic records of " + std::to_string(n_rec) + " on " +

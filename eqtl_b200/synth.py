@@ -262,23 +262,45 @@ def _ds_text(v) -> str:
     return "." if not np.isfinite(v) else np.format_float_positional(np.float32(v), unique=True, trim="-")
 
 
+def write_bgzf(path: str, text: str) -> None:
+    """BGZF (blocked gzip, the SAM/VCF specifications' container): gzip
+    members of at most 65,280 text bytes, each with the BC extra field giving
+    the member's size, then the empty end-of-file member."""
+    import struct
+    import zlib
+    data = text.encode()
+    with open(path, "wb") as f:
+        for a in range(0, len(data), 65280):
+            chunk = data[a:a + 65280]
+            co = zlib.compressobj(6, zlib.DEFLATED, -15)
+            comp = co.compress(chunk) + co.flush()
+            f.write(struct.pack("<BBBBIBBHBBHH", 31, 139, 8, 4, 0, 0, 255, 6, 66, 67, 2, len(comp) + 25))
+            f.write(comp)
+            f.write(struct.pack("<II", zlib.crc32(chunk) & 0xFFFFFFFF, len(chunk)))
+        f.write(bytes.fromhex("1f8b08040000000000ff0600424302001b0003000000000000000000"))
+
+
 def write_vcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequence[int], ids: Sequence[str],
               ref: Sequence[str], alt: Sequence[str], dosage: np.ndarray, haploid: Optional[np.ndarray] = None,
-              phased: bool = False, ds: Optional[np.ndarray] = None, ds_rows: Optional[np.ndarray] = None) -> None:
+              phased: bool = False, ds: Optional[np.ndarray] = None, ds_rows: Optional[np.ndarray] = None,
+              bgzf: bool = False, ds_text=None) -> None:
     """VCF 4.2 with a GT field (gzip-compressed when `path` ends in .gz):
     dosage [m, n] = ALT allele count (-1 missing); haploid [m, n] marks calls
     written with one allele ("0", "1", "."). With `ds` [m, n] (NaN = ".") the
     header declares FORMAT/DS and the records where `ds_rows` is set (all by
     default) carry GT:DS, each DS value written as the shortest text that
-    reads back as the same FP32 number."""
+    reads back as the same FP32 number (or as `ds_text(value)` gives it).
+    bgzf: a .gz path is written as BGZF instead of one gzip member."""
     import gzip
+    import io
     sep = "|" if phased else "/"
     gt_dip = {0: f"0{sep}0", 1: f"0{sep}1", 2: f"1{sep}1", -1: f".{sep}."}
     gt_hap = {0: "0", 1: "1", -1: "."}
-    opener = gzip.open if path.endswith(".gz") else open
     if ds is not None and ds_rows is None:
         ds_rows = np.ones(len(chrom), bool)
-    with opener(path, "wt") as f:
+    fmt_ds = ds_text or _ds_text
+    f = io.StringIO()
+    if True:
         f.write("##fileformat=VCFv4.2\n")
         f.write('##FORMAT=<ID=GT,Number=1,Type=String,Description="Genotype">\n')
         if ds is not None:
@@ -291,9 +313,18 @@ def write_vcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequ
             fmt = "GT"
             if ds is not None and ds_rows[r]:
                 fmt = "GT:DS"
-                calls = [c + ":" + _ds_text(v) for c, v in zip(calls, ds[r])]
+                calls = [c + ":" + fmt_ds(v) for c, v in zip(calls, ds[r])]
             f.write(f"{chrom[r]}\t{int(pos[r])}\t{ids[r] or '.'}\t{ref[r]}\t{alt[r]}\t.\tPASS\t.\t{fmt}\t" +
                     "\t".join(calls) + "\n")
+    text = f.getvalue()
+    if path.endswith(".gz") and bgzf:
+        write_bgzf(path, text)
+    elif path.endswith(".gz"):
+        with gzip.open(path, "wt") as g:
+            g.write(text)
+    else:
+        with open(path, "w") as g:
+            g.write(text)
 
 
 def write_tabix_header(vcf_path: str) -> None:

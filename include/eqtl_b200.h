@@ -97,6 +97,21 @@ int eqtl_geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int32_t n_f
                           int32_t n, int32_t miss_hand, double max_miss, double maf_min, uint8_t* keep_out,
                           double* af_out, int32_t* n_miss_out, int64_t* n_kept_out);
 
+/* VCF sample columns parsed on the device (VcfSession::parse_record's
+ * per-call loop, src/vcf_session.cpp:193-258). text [text_len]: decompressed
+ * VCF text; per record r (n_rec of them): the sample columns lie in
+ * [beg[r], end[r]) (the 10th column to the end of the line), gt_at[r] / ds_at[r]
+ * give the FORMAT position of GT and of the DS field to use (ds_at -1: GT).
+ * dense 0: codes_out [n_rec][ceil(n_file/4)] 2-bit .bed codes of the GT
+ * calls (ALT counted); dense 1: ds_out [n_rec][n_file] FP32 dosages (DS
+ * values, or GT counts), NaN = missing. hap_out [n_rec][ceil(n_file/8)]: one
+ * bit per GT call carrying a single allele. flag_out [n_rec]: 1 = fewer
+ * sample columns than n_file, 2 = a call outside the parser's exact fast
+ * paths (the caller parses such records itself). */
+int eqtl_vcf_parse(eqtl_ctx* ctx, const char* text, int64_t text_len, const int64_t* beg, const int64_t* end,
+                   const int32_t* gt_at, const int32_t* ds_at, int64_t n_rec, int32_t n_file, int32_t dense,
+                   uint8_t* codes_out, float* ds_out, uint8_t* hap_out, uint8_t* flag_out);
+
 /* Decoded, mean-imputed dosages of kept SNPs [lo, hi) as FP64, row-major
  * [hi - lo, n] (SnpRec.dosage after src/plink_bed.cpp:298-302). */
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);
