@@ -333,6 +333,7 @@ Plink read_vcf(const std::string& path, VcfInfo& vi, const std::function<eqtl_ct
   else P.rows.assign(static_cast<size_t>(R * bpr), 0);
   std::vector<uint8_t> hap(static_cast<size_t>(R * hbr), 0), flag(static_cast<size_t>(R), 0);
   eqtl_ctx* ctx = R > 0 ? get_ctx() : nullptr;
+  tr.mark("VCF: device opened");
   for (int64_t r0 = 0; r0 < R;) {
     int64_t r1 = r0 + 1;
     while (r1 < R && end[r1] - beg[r0] <= (int64_t(1) << 30) && (r1 - r0) * n < (int64_t(1) << 27)) ++r1;
