@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -210,13 +211,311 @@ std::string read_all(const std::string& path) {
 
 }  // namespace
 
+namespace {
+
+// ------------------------------------------------------------------- BCF
+// BCF2 (the VCF specification's binary form, as htslib writes it): "BCF\2\x"
+// magic, the header text, then records of shared fields (CHROM as a contig
+// index, 0-based POS, ID, alleles, FILTER, INFO) and per-FORMAT-key sample
+// arrays of typed values. Sentinels: int8/16/32 missing 0x80.., vector end
+// 0x80..01; float missing 0x7F800001, vector end 0x7F800002. GT values are
+// (allele + 1) << 1 | phased, 0 for a missing allele.
+struct BcfReader {
+  const std::string& b;
+  size_t at;
+  explicit BcfReader(const std::string& buf, size_t off) : b(buf), at(off) {}
+  void need(size_t k) const {
+    if (at + k > b.size()) die("BCF record truncated");
+  }
+  uint32_t u32() {
+    need(4);
+    uint32_t v;
+    std::memcpy(&v, b.data() + at, 4);
+    at += 4;
+    return v;
+  }
+  uint8_t u8() {
+    need(1);
+    return static_cast<uint8_t>(b[at++]);
+  }
+  // typed descriptor: (type, count)
+  void desc(int& type, int64_t& count) {
+    const uint8_t d = u8();
+    type = d & 15;
+    count = d >> 4;
+    if (count == 15) count = int_value();
+  }
+  int64_t int_value() {
+    int t;
+    int64_t c;
+    desc(t, c);
+    if (c != 1) die("BCF typed integer with count " + std::to_string(c));
+    return scalar_int(t);
+  }
+  int64_t scalar_int(int t) {
+    if (t == 1) return static_cast<int8_t>(u8());
+    if (t == 2) {
+      need(2);
+      int16_t v;
+      std::memcpy(&v, b.data() + at, 2);
+      at += 2;
+      return v;
+    }
+    if (t == 3) return static_cast<int32_t>(u32());
+    die("BCF typed value of type " + std::to_string(t) + " where an integer is expected");
+  }
+  static size_t width(int t) { return t == 1 || t == 7 ? 1 : (t == 2 ? 2 : (t == 3 || t == 5 ? 4 : 0)); }
+  std::string string_value() {
+    int t;
+    int64_t c;
+    desc(t, c);
+    if (c > 0 && t != 7) die("BCF typed string of type " + std::to_string(t));
+    need(static_cast<size_t>(c));
+    std::string s(b.data() + at, static_cast<size_t>(c));
+    at += static_cast<size_t>(c);
+    const size_t z = s.find('\0');
+    if (z != std::string::npos) s.resize(z);
+    return s;
+  }
+  void skip_typed() {
+    int t;
+    int64_t c;
+    desc(t, c);
+    const size_t w = width(t);
+    if (c > 0 && w == 0) die("BCF typed value of unknown type " + std::to_string(t));
+    need(w * static_cast<size_t>(c));
+    at += w * static_cast<size_t>(c);
+  }
+};
+
+// one element of an integer array of type t, widened with the sentinels
+// mapped to int32's (missing INT32_MIN, vector end INT32_MIN + 1)
+int32_t widen(const char* p, int t) {
+  if (t == 1) {
+    const int8_t v = static_cast<int8_t>(*p);
+    return v == INT8_MIN ? INT32_MIN : (v == INT8_MIN + 1 ? INT32_MIN + 1 : v);
+  }
+  if (t == 2) {
+    int16_t v;
+    std::memcpy(&v, p, 2);
+    return v == INT16_MIN ? INT32_MIN : (v == INT16_MIN + 1 ? INT32_MIN + 1 : v);
+  }
+  int32_t v;
+  std::memcpy(&v, p, 4);
+  return v;
+}
+
+Plink read_bcf_records(const std::string& text, VcfInfo& vi) {
+  if (text.size() < 9 || static_cast<uint8_t>(text[3]) != 2)
+    die("BCF input of an unsupported version (BCF2 is read)");
+  uint32_t l_text;
+  std::memcpy(&l_text, text.data() + 5, 4);
+  if (9 + static_cast<size_t>(l_text) > text.size()) die("BCF header truncated");
+  std::string header(text.data() + 9, l_text);
+  const size_t z = header.find('\0');
+  if (z != std::string::npos) header.resize(z);
+  Plink P;
+  // the string dictionary (PASS first) and the contig dictionary, in header
+  // order unless an IDX attribute says otherwise
+  std::vector<std::string> dict{"PASS"}, contigs;
+  auto put = [](std::vector<std::string>& d, const std::string& id, int idx) {
+    if (idx >= 0) {
+      if (static_cast<size_t>(idx) >= d.size()) d.resize(static_cast<size_t>(idx) + 1);
+      d[static_cast<size_t>(idx)] = id;
+    } else if (std::find(d.begin(), d.end(), id) == d.end()) {
+      d.push_back(id);
+    }
+  };
+  auto attr = [](const std::string& line, const std::string& key) -> std::string {
+    const size_t lt = line.find('<');
+    if (lt == std::string::npos) return "";
+    const std::string body = line.substr(lt + 1);
+    size_t a = 0;
+    while (a < body.size()) {
+      if (body[a] == '"') {  // skip quoted text
+        const size_t q = body.find('"', a + 1);
+        a = q == std::string::npos ? body.size() : q + 1;
+        continue;
+      }
+      const size_t e = body.find_first_of(",>", a);
+      const std::string kv = body.substr(a, (e == std::string::npos ? body.size() : e) - a);
+      if (kv.compare(0, key.size() + 1, key + "=") == 0) return kv.substr(key.size() + 1);
+      if (e == std::string::npos) break;
+      a = e + 1;
+    }
+    return "";
+  };
+  bool prefer_ds = false, ds_float = false, said_ds = false;
+  size_t ls = 0;
+  while (ls < header.size()) {
+    size_t le = header.find('\n', ls);
+    if (le == std::string::npos) le = header.size();
+    std::string line = header.substr(ls, le - ls);
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    ls = le + 1;
+    const bool fmt_line = line.compare(0, 10, "##FORMAT=<") == 0;
+    if (fmt_line || line.compare(0, 8, "##INFO=<") == 0 || line.compare(0, 10, "##FILTER=<") == 0) {
+      std::string id, type;
+      header_id(line, id, type);
+      const std::string idx = attr(line, "IDX");
+      put(dict, id, idx.empty() ? -1 : std::atoi(idx.c_str()));
+      if (id == "DS") {
+        prefer_ds = true;
+        if (fmt_line) ds_float = type == "Float";
+      }
+    } else if (line.compare(0, 10, "##contig=<") == 0) {
+      const std::string idx = attr(line, "IDX");
+      put(contigs, attr(line, "ID"), idx.empty() ? -1 : std::atoi(idx.c_str()));
+    } else if (line.compare(0, 6, "#CHROM") == 0) {
+      size_t a = 0;
+      int col = 0;
+      while (a <= line.size()) {
+        size_t e = line.find('\t', a);
+        if (e == std::string::npos) e = line.size();
+        if (col >= 9) P.fam_iid.push_back(line.substr(a, e - a));
+        ++col;
+        a = e + 1;
+      }
+    }
+  }
+  P.n_file = static_cast<int>(P.fam_iid.size());
+  P.bytes_per_snp = (P.n_file + 3) / 4;
+  if (P.n_file == 0) die("BCF has no samples");
+  P.dense = prefer_ds;
+  if (prefer_ds) info("VCF: FORMAT/DS present -> use dosage field when available");
+  int gt_key = -1, ds_key = -1;
+  for (size_t k = 0; k < dict.size(); ++k) {
+    if (dict[k] == "GT") gt_key = static_cast<int>(k);
+    if (dict[k] == "DS") ds_key = static_cast<int>(k);
+  }
+  const int n = P.n_file;
+  int64_t n_rec = 0;
+  for (size_t off = 9 + l_text; off < text.size();) {
+    BcfReader r(text, off);
+    const uint32_t l_shared = r.u32(), l_indiv = r.u32();
+    const size_t shared0 = r.at, indiv0 = shared0 + l_shared;
+    off = indiv0 + l_indiv;
+    if (off > text.size()) die("BCF record truncated");
+    ++n_rec;
+    const int32_t chrom_idx = static_cast<int32_t>(r.u32());
+    const int32_t pos0 = static_cast<int32_t>(r.u32());
+    r.u32();  // rlen
+    r.u32();  // QUAL
+    const uint32_t n_allele_info = r.u32(), n_fmt_sample = r.u32();
+    const int n_allele = static_cast<int>(n_allele_info >> 16), n_info = static_cast<int>(n_allele_info & 0xFFFF);
+    const int n_fmt = static_cast<int>(n_fmt_sample >> 24), n_smp = static_cast<int>(n_fmt_sample & 0xFFFFFF);
+    std::string id = r.string_value();
+    if (n_allele != 2) {  // not biallelic
+      ++vi.n_multi;
+      continue;
+    }
+    const std::string ref = r.string_value(), alt = r.string_value();
+    r.skip_typed();  // FILTER
+    for (int k = 0; k < n_info; ++k) {
+      r.int_value();
+      r.skip_typed();
+    }
+    if (r.at != indiv0) die("BCF shared block length mismatch");
+    if (n_smp < n) die("VCF record with fewer sample columns than the header");
+    // FORMAT arrays
+    const char* gt = nullptr;
+    const char* dsv = nullptr;
+    int gt_t = 0, gt_c = 0, ds_t = 0, ds_c = 0;
+    for (int k = 0; k < n_fmt; ++k) {
+      const int64_t key = r.int_value();
+      int t;
+      int64_t c;
+      r.desc(t, c);
+      const size_t bytes = BcfReader::width(t) * static_cast<size_t>(c) * static_cast<size_t>(n_smp);
+      r.need(bytes);
+      if (key == gt_key) {
+        gt = text.data() + r.at;
+        gt_t = t;
+        gt_c = static_cast<int>(c);
+      } else if (key == ds_key) {
+        dsv = text.data() + r.at;
+        ds_t = t;
+        ds_c = static_cast<int>(c);
+      }
+      r.at += bytes;
+    }
+    const bool use_ds = prefer_ds && ds_float && dsv != nullptr && ds_t == 5 && ds_c >= 1;
+    if (!use_ds && (gt == nullptr || gt_c < 1 || BcfReader::width(gt_t) == 0 || gt_t == 5 || gt_t == 7)) continue;
+    if (use_ds && !said_ds) {
+      info("VCF: using FORMAT/DS dosages");
+      said_ds = true;
+    }
+    if (chrom_idx < 0 || static_cast<size_t>(chrom_idx) >= contigs.size()) die("BCF CHROM index outside the contigs");
+    const std::string chrom = contigs[static_cast<size_t>(chrom_idx)];
+    const bool hap = haploid_chrom(chrom);
+    std::vector<uint8_t> row(P.dense ? 0 : static_cast<size_t>(P.bytes_per_snp), 0);
+    std::vector<float> drow(P.dense ? static_cast<size_t>(n) : 0);
+    std::vector<int32_t> hap_calls;
+    for (int i = 0; i < n; ++i) {
+      if (use_ds) {
+        // the reference reads the flattened float array at the sample's column
+        uint32_t bits;
+        std::memcpy(&bits, dsv + 4 * static_cast<size_t>(i), 4);
+        float v;
+        std::memcpy(&v, &bits, 4);
+        drow[static_cast<size_t>(i)] = (bits == 0x7F800001u || bits == 0x7F800002u || !std::isfinite(v))
+                                           ? std::numeric_limits<float>::quiet_NaN()
+                                           : v;
+        continue;
+      }
+      const size_t w = BcfReader::width(gt_t);
+      const char* g = gt + w * static_cast<size_t>(gt_c) * i;
+      const int32_t a0 = widen(g, gt_t);
+      const int32_t a1 = gt_c > 1 ? widen(g + w, gt_t) : INT32_MIN + 1;
+      const auto is_missing = [](int32_t v) { return (v >> 1) == 0 || v == INT32_MIN; };
+      bool miss = is_missing(a0) || a0 == INT32_MIN + 1;
+      if (!miss && gt_c > 1 && a1 != INT32_MIN + 1 && a1 != INT32_MIN) miss = is_missing(a1);
+      int d = -1;
+      bool haploid = false;
+      if (!miss) {
+        d = (a0 >> 1) - 1;
+        int na = 1;
+        if (gt_c > 1 && a1 != INT32_MIN + 1 && a1 != INT32_MIN) {
+          d += (a1 >> 1) - 1;
+          ++na;
+        }
+        if ((a0 >> 1) - 1 > 1 || (na == 2 && (a1 >> 1) - 1 > 1))
+          die("VCF GT allele index beyond the single ALT allele");
+        haploid = na == 1;
+      }
+      if (P.dense) {
+        drow[static_cast<size_t>(i)] = d < 0 ? std::numeric_limits<float>::quiet_NaN() : static_cast<float>(d);
+      } else {
+        const uint32_t code = d < 0 ? 1u : (d == 2 ? 0u : (d == 1 ? 2u : 3u));
+        row[static_cast<size_t>(i >> 2)] |= static_cast<uint8_t>(code << ((i & 3) * 2));
+      }
+      if (d >= 0 && haploid && !hap) hap_calls.push_back(i);
+    }
+    P.chrom.push_back(chrom);
+    P.pos.push_back(static_cast<int64_t>(pos0) + 1);
+    P.id.push_back(id == "." ? std::string() : id);
+    P.a2.push_back(ref);
+    P.a1.push_back(alt);
+    P.rows.insert(P.rows.end(), row.begin(), row.end());
+    P.ds.insert(P.ds.end(), drow.begin(), drow.end());
+    vi.hap_chrom.push_back(hap ? 1 : 0);
+    vi.hap_calls.push_back(std::move(hap_calls));
+  }
+  if (vi.n_multi > 0)
+    info("VCF multi-allelic sites skipped (biallelic only): " + std::to_string(vi.n_multi));
+  info("VCF: " + std::to_string(P.chrom.size()) + " biallelic records of " + std::to_string(n_rec) + " on " +
+       std::to_string(P.n_file) + " samples");
+  return P;
+}
+
+}  // namespace
+
 Plink read_vcf(const std::string& path, VcfInfo& vi, const std::function<eqtl_ctx*()>& get_ctx) {
   Trace tr;
   const std::string text = read_all(path);
   tr.mark("VCF: read and inflate " + std::to_string(text.size()) + " bytes");
   if (text.empty()) die("empty VCF: " + path);
-  if (text.compare(0, 3, "BCF") == 0)
-    die("BCF input is not read by this build; convert with bcftools view -Oz to a VCF");
+  if (text.compare(0, 3, "BCF") == 0) return read_bcf_records(text, vi);
   Plink P;
   bool have_header = false;
   int64_t n_rec = 0;

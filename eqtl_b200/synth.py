@@ -268,7 +268,7 @@ def write_bgzf(path: str, text: str) -> None:
     the member's size, then the empty end-of-file member."""
     import struct
     import zlib
-    data = text.encode()
+    data = text.encode() if isinstance(text, str) else bytes(text)
     with open(path, "wb") as f:
         for a in range(0, len(data), 65280):
             chunk = data[a:a + 65280]
@@ -325,6 +325,61 @@ def write_vcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequ
     else:
         with open(path, "w") as g:
             g.write(text)
+
+
+def write_bcf(path: str, samples: Sequence[str], chrom: Sequence[str], pos: Sequence[int], ids: Sequence[str],
+              ref: Sequence[str], alt: Sequence[str], dosage: np.ndarray, haploid: Optional[np.ndarray] = None,
+              ds: Optional[np.ndarray] = None) -> None:
+    """The genotypes of write_vcf as BCF2 (BGZF-compressed), laid out as the
+    VCF specification's BCF2 section describes: the header text with its
+    string dictionary (PASS, GT, DS) and contig list, then per record the
+    shared fields (contig index, 0-based POS, ID, REF, ALT, FILTER PASS) and
+    the FORMAT arrays: GT as int8 pairs ((allele + 1) << 1, 0 for '.', the
+    vector-end byte 0x81 after a haploid call) and, with `ds`, DS as FP32
+    (missing 0x7F800001)."""
+    import struct
+    contigs = list(dict.fromkeys(chrom))
+    head = "##fileformat=VCFv4.2\n##FILTER=<ID=PASS,Description=\"All filters passed\">\n"
+    head += '##FORMAT=<ID=GT,Number=1,Type=String,Description="Genotype">\n'
+    if ds is not None:
+        head += '##FORMAT=<ID=DS,Number=A,Type=Float,Description="Estimated ALT dose">\n'
+    for c in contigs:
+        head += f"##contig=<ID={c}>\n"
+    head += "#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\t" + "\t".join(samples) + "\n"
+    hb = head.encode() + b"\0"
+
+    def typed_str(t: str) -> bytes:
+        e = t.encode()
+        if len(e) < 15:
+            return bytes([(len(e) << 4) | 7]) + e
+        return bytes([(15 << 4) | 7, 0x11, len(e)]) + e if len(e) < 128 else \
+            bytes([(15 << 4) | 7, 0x12]) + struct.pack("<h", len(e)) + e
+
+    n = len(samples)
+    out = bytearray(b"BCF\x02\x02" + struct.pack("<I", len(hb)) + hb)
+    pairs = {0: (0, 0), 1: (0, 1), 2: (1, 1)}
+    for r in range(len(chrom)):
+        shared = struct.pack("<iiiIII", contigs.index(chrom[r]), int(pos[r]) - 1, len(ref[r]), 0x7F800001,
+                             2 << 16, ((2 if ds is not None else 1) << 24) | n)
+        shared += typed_str(ids[r] or ".") + typed_str(ref[r]) + typed_str(alt[r]) + bytes([0x11, 0])
+        gt = bytearray()
+        for i in range(n):
+            d = int(dosage[r, i])
+            h = haploid is not None and bool(haploid[r, i])
+            if h:
+                gt += bytes([0 if d < 0 else ((d + 1) << 1), 0x81])
+            elif d < 0:
+                gt += bytes([0, 0])
+            else:
+                a0, a1 = pairs[d]
+                gt += bytes([(a0 + 1) << 1, (a1 + 1) << 1])
+        indiv = bytes([0x11, 1, (2 << 4) | 1]) + bytes(gt)
+        if ds is not None:
+            vals = b"".join(struct.pack("<I", 0x7F800001) if not np.isfinite(v) else struct.pack("<f", v)
+                            for v in ds[r])
+            indiv += bytes([0x11, 2, (1 << 4) | 5]) + vals
+        out += struct.pack("<II", len(shared), len(indiv)) + shared + indiv
+    write_bgzf(path, bytes(out))
 
 
 def write_tabix_header(vcf_path: str) -> None:

@@ -178,8 +178,8 @@ def _grm_files(prefix):
 
 @pytest.mark.parametrize("kind", ["ds_long", "gt"])
 def test_vcf_containers_and_host_fallback(kind, tmp_path):
-    """The same genotypes as plain text, one gzip member and BGZF give the
-    same GRM, equal to the oracle's from its own reading of the file. With
+    """The same genotypes as plain text, one gzip member, BGZF and BCF2 give
+    the same GRM, equal to the oracle's from its own reading of the file. With
     DS written to 17 significant digits every value misses the device's fast
     path and is parsed on the host."""
     from eqtl_b200 import synth
@@ -201,11 +201,14 @@ def test_vcf_containers_and_host_fallback(kind, tmp_path):
         for i in order:
             f.write(f"{samples[i]}\t{rng.standard_normal():.6f}\n")
     outs = []
-    for name, bgzf in (("g.vcf", False), ("g.vcf.gz", False), ("b.vcf.gz", True)):
+    for name, bgzf in (("g.vcf", False), ("g.vcf.gz", False), ("b.vcf.gz", True), ("g.bcf", True)):
         path = str(tmp_path / name)
-        synth.write_vcf(path, samples, chrom, pos, [f"rs{i}" for i in range(m)], ["A"] * m, ["G"] * m, gt, ds=ds,
-                        bgzf=bgzf, ds_text=(lambda v: "." if not np.isfinite(v) else "%.17g" % v) if ds is not None
-                        else None)
+        if name.endswith(".bcf"):
+            synth.write_bcf(path, samples, chrom, pos, [f"rs{i}" for i in range(m)], ["A"] * m, ["G"] * m, gt, ds=ds)
+        else:
+            synth.write_vcf(path, samples, chrom, pos, [f"rs{i}" for i in range(m)], ["A"] * m, ["G"] * m, gt, ds=ds,
+                            bgzf=bgzf, ds_text=(lambda v: "." if not np.isfinite(v) else "%.17g" % v)
+                            if ds is not None else None)
         out = str(tmp_path / ("o_" + name.replace(".", "_")))
         r = subprocess.run([BIN, "-v", path, "-e", ph, "--make-grm", "--maf", "0.01", "-o", out], capture_output=True,
                            text=True, timeout=300)
