@@ -26,7 +26,7 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
            "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
-           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse"]
+           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 

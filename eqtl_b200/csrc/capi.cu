@@ -768,7 +768,13 @@ int eqtl_grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed_dev, int64_t m, int64_t b
 }
 
 int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out, double* Q_out) {
+  return eqtl_lmm_basis_fast(ctx, K, n, 0.0, lambda_out, Q_out, nullptr);
+}
+
+int eqtl_lmm_basis_fast(eqtl_ctx* ctx, const double* K, int32_t n, double sparsify_thr, double* lambda_out,
+                        double* Q_out, int64_t* zeroed_out) {
   return guarded(ctx, [&] {
+    EQTL_CHECK(sparsify_thr >= 0.0, EQTL_E_ARG, "sparsify threshold must be >= 0");
     eqtl::DevBuf<double> dK;
     if (K) {
       EQTL_CHECK(n > 0, EQTL_E_ARG, "n must be positive");
@@ -778,7 +784,7 @@ int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out
       eqtl::grm_compute(ctx, dK, N);
       n = ctx->geno.n;
     }
-    eqtl::lmm_basis_from_grm(ctx, dK.p, n);
+    eqtl::lmm_basis_from_grm(ctx, dK.p, n, sparsify_thr, zeroed_out);
     if (lambda_out) std::copy(ctx->basis.lambda_h.begin(), ctx->basis.lambda_h.end(), lambda_out);
     if (Q_out) {
       ctx->basis.Q.download(Q_out, static_cast<size_t>(n) * n, ctx->stream);

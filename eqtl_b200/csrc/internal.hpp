@@ -297,7 +297,10 @@ void scan_trans_lmm_simt(eqtl_ctx* ctx, const eqtl_scan_params* prm, const doubl
 template <class T>
 struct DevBuf;
 int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk);
-void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n);
+// Eigenbasis of the device GRM K_dev; with sparsify_thr > 0 the off-diagonal
+// entries below it in magnitude are zeroed first (--fast), *zeroed = count.
+void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n, double sparsify_thr = 0.0,
+                        int64_t* zeroed = nullptr);
 void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n);
 void lmm_rotate(eqtl_ctx* ctx);
 int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,

@@ -1261,7 +1261,24 @@ static cublasHandle_t blas_of(eqtl_ctx* ctx) {
 }
 
 // ------------------------------------------------------------------ basis
-void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
+// --fast (sparsify_grm, src/model_lmm.cpp:88-104): off-diagonal entries of K
+// below `thr` in magnitude become 0; the count of zeroed entries goes to *zeroed.
+__global__ void sparsify_kernel(double* K, int n, double thr, unsigned long long* zeroed) {
+  const int64_t total = static_cast<int64_t>(n) * n;
+  unsigned long long c = 0;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = e / n, j = e - i * n;
+    if (i != j && fabs(K[e]) < thr) {
+      K[e] = 0.0;
+      ++c;
+    }
+  }
+  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(zeroed, c);
+}
+
+void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n, double sparsify_thr, int64_t* zeroed) {
   cudaStream_t st = ctx->stream;
   StageScope timer(ctx, EQTL_STAGE_EIGEN);
   LmmBasisDev& B = ctx->basis;
@@ -1269,6 +1286,20 @@ void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n) {
   B.Q.alloc(static_cast<size_t>(n) * n);
   B.lambda.alloc(n);
   EQTL_CUDA(cudaMemcpyAsync(B.Q.p, K_dev, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st));
+  if (sparsify_thr > 0) {
+    DevBuf<unsigned long long> cnt;
+    cnt.alloc(1);
+    cnt.zero(st);
+    ++ctx->launches;
+    const int64_t total = static_cast<int64_t>(n) * n;
+    sparsify_kernel<<<static_cast<unsigned>(std::min<int64_t>((total + 255) / 256, 1184)), 256, 0, st>>>(
+        B.Q.p, n, sparsify_thr, cnt.p);
+    EQTL_CUDA(cudaGetLastError());
+    unsigned long long c = 0;
+    cnt.download(&c, 1, st);
+    EQTL_CUDA(cudaStreamSynchronize(st));
+    if (zeroed) *zeroed = static_cast<int64_t>(c);
+  }
   if (!ctx->cusolver) {
     cusolverDnHandle_t hc;
     EQTL_CHECK(cusolverDnCreate(&hc) == CUSOLVER_STATUS_SUCCESS, EQTL_E_CUDA, "cusolverDnCreate failed");

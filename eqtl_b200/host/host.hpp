@@ -53,6 +53,7 @@ struct Options {
   bool miss_filter = false;              // --miss-hand filter
   double max_miss = 0.8, maf = 0.0;
   bool pheno_int = false;                // --pheno-norm int
+  bool fast = false;                     // --fast: sparse GRM before the LMM eigenbasis
   int threads = 1;
   int perm = 0;
   double perm_trans_thr = 1e-5;

@@ -157,13 +157,20 @@ int run_scan(const Options& opt) {
     }
     double* lam = opt.perm > 0 ? st.basis_lambda.data() : nullptr;
     double* Q = opt.perm > 0 ? st.basis_Q.data() : nullptr;
+    // --fast: the GRM's small off-diagonal entries are zeroed before the
+    // eigendecomposition (sparsify_grm, src/model_lmm.cpp:88-104)
+    const double thr = opt.fast ? 1e-4 : 0.0;
+    int64_t zeroed = 0;
     if (!opt.grm.empty()) {
       std::vector<double> K = slice_grm(load_grm(opt.grm), st.samples);
-      dev.check(eqtl_lmm_basis(dev.ctx, K.data(), static_cast<int32_t>(n), lam, Q), "LMM basis");
+      dev.check(eqtl_lmm_basis_fast(dev.ctx, K.data(), static_cast<int32_t>(n), thr, lam, Q, &zeroed), "LMM basis");
     } else {
       info("computing GRM from genotypes (overlap samples)");
-      dev.check(eqtl_lmm_basis(dev.ctx, nullptr, static_cast<int32_t>(n), lam, Q), "LMM basis");
+      dev.check(eqtl_lmm_basis_fast(dev.ctx, nullptr, static_cast<int32_t>(n), thr, lam, Q, &zeroed), "LMM basis");
     }
+    if (opt.fast)
+      info("fast: GRM sparse approx thr=" + std::to_string(thr) + " zeroed " + std::to_string(zeroed) +
+           " off-diagonal entries");
   }
   for (const auto& model : opt.models) {
     for (const auto& scope : scopes) {

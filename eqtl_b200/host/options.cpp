@@ -1,8 +1,8 @@
 // Command line of the reference program (src/options.cpp:145-179): the same
 // long and short flags, defaults and range checks, for the LM / LMM / NB-GLM
 // models, with PLINK (-b) or VCF (-v, GT or DS) genotypes. The flags of paths
-// outside the device scan (the GLMM model, --fast) are recognised and
-// refused with a message instead of being silently ignored. `eqtl fission ...` selects the fission subcommand.
+// outside the device scan (the GLMM model) are recognised and refused with a
+// message instead of being silently ignored. `eqtl fission ...` selects the fission subcommand.
 #include <getopt.h>
 
 #include <algorithm>
@@ -70,6 +70,7 @@ void print_help() {
                "        --max-miss FLOAT   drop SNP if missing fraction > value  [0.8]\n"
                "        --maf FLOAT        min MAF on analysis samples  [0=off]\n"
                "        --pheno-norm STR   per-gene phenotype normalization none|int  [none]\n"
+               "        --fast             sparse GRM approx (LMM); glm/glmm: fix null phi/sigma2\n"
                "\n"
                "Fission options (subcommand: eqtl fission ...):\n"
                "    -c, --covar FILE       residualize known covars from Y1 before PEER\n"
@@ -174,7 +175,7 @@ int parse_options(int argc, char** argv, Options& opt) {
         else if (a == "impute") opt.miss_filter = false;
         else die("invalid --miss-hand (filter|impute)");
         break;
-      case kFast: die("--fast (sparse GRM approximation) is outside the device scan");
+      case kFast: opt.fast = true; break;
       case kPerm: opt.perm = std::atoi(a.c_str()); break;
       case kPermThr:
         opt.perm_trans_thr = std::atof(a.c_str());

@@ -256,6 +256,14 @@ int eqtl_grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed_dev, int64_t m, int64_t b
  * (column j = eigenvector j) are optional. */
 int eqtl_lmm_basis(eqtl_ctx* ctx, const double* K, int32_t n, double* lambda_out, double* Q_out);
 
+/* The same with --fast (sparsify_grm, src/model_lmm.cpp:88-104, applied at
+ * src/scan_trans_lmm.cpp:103, src/scan_cis.cpp:60, src/scan_common.cpp:56):
+ * off-diagonal entries of K below sparsify_thr in magnitude (1e-4 in the
+ * reference) are set to 0 before the eigendecomposition; zeroed_out
+ * (optional) receives how many were. */
+int eqtl_lmm_basis_fast(eqtl_ctx* ctx, const double* K, int32_t n, double sparsify_thr, double* lambda_out,
+                        double* Q_out, int64_t* zeroed_out);
+
 /* Installs an eigenbasis computed elsewhere (LmmBasis, include/eqtl/models.hpp
  * :43-46). Eigenvector signs are arbitrary; statistics do not depend on
  * them, but LMM permutations (which shuffle residuals in eigen-coordinates,

@@ -227,6 +227,7 @@ class Options:
     disable_beta_approx: bool = False
     pheno_norm: str = "none"
     threads: int = 1
+    fast: bool = False
 
 
 def fmt(v) -> str:
@@ -380,7 +381,7 @@ class Scanner:
             degenerate = gtg < 1e-12
         else:
             K = self.grm()[np.ix_(keep0, keep0)]
-            Q, lam = R.make_lmm_basis(K)
+            Q, lam = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
             preps = [R.prep_lmm(j[2][1], j[2][2], Q, lam) for j in jobs]
             Gt = G @ Q
             cols = [R.lmm_stats_gtil(pp, Gt) for pp in preps]
@@ -447,7 +448,7 @@ class Scanner:
         if model == "lmm":
             K = self.grm()
             if K.shape[0] == len(self.samples):
-                basis = R.make_lmm_basis(K)
+                basis = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
         pairs, tops, summ = [], [], []
         bim_chrom = [b[0] for b in self.bim]
         for gi, gene, loc in works:
@@ -461,7 +462,7 @@ class Scanner:
                     continue
                 keep, yk, Xk, Kk = ready
                 if model == "lmm":
-                    Q, lam = R.make_lmm_basis(Kk)
+                    Q, lam = R.make_lmm_basis(R.sparsify_grm(Kk, 1e-4) if opt.fast else Kk)
             lo = max(loc.start - opt.window, 1)
             hi = loc.end + opt.window
             win = [s for s in self.kept

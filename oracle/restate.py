@@ -756,6 +756,16 @@ def test_glm_nb_many(prep: PrepGlm, G: np.ndarray):
 _EIGSOLVE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "eigsolve")
 
 
+def sparsify_grm(K, thr):
+    """sparsify_grm (src/model_lmm.cpp:88-104): off-diagonal entries below
+    thr in magnitude set to 0 (the --fast approximation)."""
+    K = np.array(K, dtype=np.float64, copy=True)
+    small = np.abs(K) < thr
+    np.fill_diagonal(small, False)
+    K[small] = 0.0
+    return K
+
+
 def make_lmm_basis(K):
     """src/model_lmm.cpp:106-113. Uses the reference's own eigensolver (Eigen,
     via oracle/_ref/eigsolve) when it has been built, so eigenvector signs

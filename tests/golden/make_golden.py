@@ -42,6 +42,8 @@ CASES = {
                         "--maf", "0.1", "--pval-cis", "1e-2", "--pval-trans", "1e-2", "-t", "1"]),
             ("int", ["--model", "lm,lmm", "--mode", "trans", "--pheno-norm", "int", "--pval-trans",
                      "1e-2", "-t", "1"]),
+            ("fast", ["--model", "lmm", "--mode", "all", "-w", "500000", "--pval-cis", "1e-2",
+                      "--pval-trans", "1e-2", "--fast", "-t", "2"]),
             ("grm", ["--make-grm"]),
         ]),
     "counts": dict(

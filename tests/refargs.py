@@ -54,10 +54,13 @@ def options_from_argv(argv, case_dir: str) -> driver.Options:
             o.pheno_norm = v
         elif a in ("-t", "--thread", "--threads"):
             o.threads = int(v)
+        elif a == "--fast":
+            o.fast = True
+            step = 1
         elif a == "--disable-beta-approx":
             o.disable_beta_approx = True
             step = 1
-        elif a in ("--make-grm", "--fast"):
+        elif a == "--make-grm":
             step = 1
         elif a in ("-o", "--out"):
             pass
