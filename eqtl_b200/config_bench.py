@@ -172,12 +172,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--lm-snps", type=int, default=1_000_000, help="SNPs of the lm case (smaller for profiling)")
     ap.add_argument("--lm-genes", type=int, default=20_000, help="genes of the lm case")
+    ap.add_argument("--glm-snps", type=int, default=200_000, help="SNPs of the glm case (smaller for profiling)")
+    ap.add_argument("--glm-genes", type=int, default=5_000, help="genes of the glm case")
     args = ap.parse_args()
     for w in args.which.split(","):
         if w == "grm":
             out = grm_case(args.steps)
         elif w == "glm":
-            out = glm_case(args.steps)
+            out = glm_case(args.steps, args.glm_snps, args.glm_genes)
         elif w == "fission":
             out = fission_case(args.steps)
         else:
