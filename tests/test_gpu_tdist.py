@@ -48,7 +48,7 @@ def test_t_tail_matches_p_from_t(df, smem):
     m_ref = np.minimum(p[q], 1.0 - p[q])
     tq = term[q]
     assert np.all(((tq > 0) == (p[q] < 0.5)) | (np.abs(p[q] - 0.5) < 1e-6))
-    m_dev = np.arctan(1.0 / np.abs(tq)) / np.pi
+    m_dev = np.arctan2(1.0, np.abs(tq)) / np.pi  # = atan(1/|t|); m = 1/2 at a zero term
     rtol = 3e-6 * np.maximum(1.0, -np.log(m_ref))
     assert np.all(np.abs(m_dev - m_ref) <= rtol * m_ref + 2e-11), np.max(np.abs(m_dev - m_ref) / m_ref)
     # unused and deferred pairs contribute nothing on the device
@@ -80,7 +80,7 @@ def test_acat_screen_matches_p_from_t(df, smem):
     m_ref = np.minimum(p[q], 1.0 - p[q])
     tq = term[q]
     assert np.all(((tq > 0) == (p[q] < 0.5)) | (np.abs(p[q] - 0.5) < 1e-6))
-    m_dev = np.arctan(1.0 / np.abs(tq)) / np.pi
+    m_dev = np.arctan2(1.0, np.abs(tq)) / np.pi  # = atan(1/|t|); m = 1/2 at a zero term
     rtol = 3e-6 * np.maximum(1.0, -np.log(m_ref))
     assert np.all(np.abs(m_dev - m_ref) <= rtol * m_ref + 2e-11), np.max(np.abs(m_dev - m_ref) / m_ref)
     assert np.all(term[~q] == 0.0)
