@@ -548,6 +548,9 @@ int eqtl_open(int device, eqtl_ctx** out) {
     EQTL_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     EQTL_CUDA(cudaMalloc(&ctx->d_status, sizeof(uint32_t)));
     EQTL_CUDA(cudaMemset(ctx->d_status, 0, sizeof(uint32_t)));
+    // the allocation-free GRM's static scratch and kernels are loaded here,
+    // while the caller can still allocate, not in its first call
+    eqtl::grm_noalloc_prepare(ctx);
   });
   if (rc != EQTL_OK) {
     eqtl_close(ctx);

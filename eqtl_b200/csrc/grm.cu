@@ -391,7 +391,10 @@ constexpr size_t kNaOffMean = kNaOffJ + kNaJBytes;
 constexpr size_t kNaOffIsd = kNaOffMean + kNaSnpBytes;
 constexpr size_t kNaOffUse = kNaOffIsd + kNaSnpBytes;
 constexpr size_t kNaOffCnt = kNaOffUse + kNaUseBytes;  // [0] SNPs used, [1] bad sample columns
+constexpr size_t kNaOffTiles = kNaOffCnt + 64;          // lower-triangle tile list (int2)
+constexpr int kNaMaxTiles = ((kNaMaxN + 127) / 128) * ((kNaMaxN + 255) / 256);
 constexpr size_t kNaScratchBytes = kNaOffCnt + 256;
+static_assert(64 + sizeof(int2) * kNaMaxTiles <= 256, "tile list inside the counter block");
 static_assert(kNaScratchBytes == EQTL_GRM_NOALLOC_SCRATCH_BYTES, "header scratch size");
 
 static __device__ __align__(256) uint8_t grm_na_scratch[kNaScratchBytes];
@@ -514,14 +517,17 @@ __global__ void grm_na_finalize_kernel(int n, const unsigned long long* __restri
   if (e >= static_cast<int64_t>(n) * n) return;
   const int64_t mu = static_cast<int64_t>(*m_used);
   const int i = static_cast<int>(e / n), j = static_cast<int>(e - static_cast<int64_t>(i) * n);
+  // only the tiles holding the lower triangle are summed; K above the
+  // diagonal is their mirror image, so K is exactly symmetric
+  const int64_t lo_e = static_cast<int64_t>(i >= j ? i : j) * n + (i >= j ? j : i);
   const int64_t mi = static_cast<int64_t>(J[static_cast<int64_t>(i) * n + i]);
   const int64_t mj = static_cast<int64_t>(J[static_cast<int64_t>(j) * n + j]);
   int64_t sub;
   if (i == j)
     sub = mu - mi;
   else
-    sub = mu - mi - mj + static_cast<int64_t>(J[e]);
-  K[e] = sub > 0 ? A[e] / static_cast<double>(sub) : 0.0;
+    sub = mu - mi - mj + static_cast<int64_t>(J[lo_e]);
+  K[e] = sub > 0 ? A[lo_e] / static_cast<double>(sub) : 0.0;
   if (Npk && j <= i) Npk[static_cast<int64_t>(i) * (i + 1) / 2 + j] = static_cast<int32_t>(sub);
 }
 
@@ -546,6 +552,21 @@ static uint8_t* grm_na_scratch_addr(int device) {
   return g_na_addr[device];
 }
 
+// Called by eqtl_open with the context's device current: resolves the
+// scratch array's device address and loads every kernel of the allocation-
+// free GRM, so that with lazy module loading the array and the kernel images
+// are set up while the caller can still allocate, not in its first call.
+void grm_noalloc_prepare(eqtl_ctx* ctx) {
+  using namespace dev;
+  grm_na_scratch_addr(ctx->device);
+  cudaFuncAttributes fa;
+  EQTL_CUDA(cudaFuncGetAttributes(&fa, grm_na_check_cols_kernel));
+  EQTL_CUDA(cudaFuncGetAttributes(&fa, grm_na_stats_kernel));
+  EQTL_CUDA(cudaFuncGetAttributes(&fa, grm_na_transpose_kernel));
+  EQTL_CUDA(cudaFuncGetAttributes(&fa, grm_na_finalize_kernel));
+  EQTL_CUDA(cudaFuncGetAttributes(&fa, tile_kernel<256, 2, 0u, GrmEpi>));
+}
+
 int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
                     int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk) {
   using namespace dev;
@@ -566,6 +587,7 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
   double* isd = reinterpret_cast<double*>(s + kNaOffIsd);
   uint8_t* use = s + kNaOffUse;
   unsigned long long* cnt = reinterpret_cast<unsigned long long*>(s + kNaOffCnt);
+  int2* tile_list = reinterpret_cast<int2*>(s + kNaOffTiles);
   cudaStream_t st = ctx->stream;
   // accumulators and counters start at zero on every call
   EQTL_CUDA(cudaMemsetAsync(A, 0, sizeof(double) * n * n, st));
@@ -582,7 +604,14 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
   const __half* ah[2] = {zh, mk};
   const __half* al[2] = {zl, mk};
   const int bsel[2] = {0, 1}, prod[2] = {7, 1};
-  const int tiles = ((n + 127) / 128) * ((n + 255) / 256);
+  // the tiles of 128 rows x 256 columns that hold some element with row >=
+  // column, as in grm_compute; the list lives in the scratch array
+  int2 lower[kNaMaxTiles];
+  int tiles = 0;
+  for (int tb = 0; tb < (n + 255) / 256; ++tb)
+    for (int ta = 0; ta < (n + 127) / 128; ++ta)
+      if (128 * ta + 127 >= 256 * tb) lower[tiles++] = make_int2(ta, tb);
+  EQTL_CUDA(cudaMemcpyAsync(tile_list, lower, sizeof(int2) * tiles, cudaMemcpyHostToDevice, st));
   const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
   for (int64_t r0 = 0; r0 < m; r0 += kNaChunk) {
     const int nr = static_cast<int>(std::min<int64_t>(kNaChunk, m - r0));
@@ -593,7 +622,7 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
     grm_na_transpose_kernel<<<dim3(kNaChunk / 32, (n + 31) / 32), dim3(32, 8), 0, st>>>(bed, bps, col, n, r0, use,
                                                                                         mean, isd, zh, zl, mk);
     EQTL_CUDA(cudaGetLastError());
-    launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, ah, al, n, kNaChunk, bsel, prod, nullptr, 0, ksplit);
+    launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, ah, al, n, kNaChunk, bsel, prod, tile_list, tiles, ksplit);
   }
   unsigned long long used = 0;
   EQTL_CUDA(cudaMemcpyAsync(&used, cnt, sizeof(used), cudaMemcpyDeviceToHost, st));

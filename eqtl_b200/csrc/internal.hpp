@@ -305,6 +305,7 @@ void lmm_set_basis(eqtl_ctx* ctx, const double* Q, const double* lambda, int n);
 void lmm_rotate(eqtl_ctx* ctx);
 int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
                     int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk);
+void grm_noalloc_prepare(eqtl_ctx* ctx);
 void solver_release(eqtl_ctx* ctx);
 void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    const std::vector<int2>& todo, eqtl_pair* out);

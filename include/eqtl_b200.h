@@ -234,11 +234,16 @@ int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_use
  *     EQTL_GRM_NOALLOC_SCRATCH_BYTES in the library image; n is limited to
  *     EQTL_GRM_NOALLOC_MAX_N (larger n: EQTL_E_UNSUPPORTED), m is not (SNPs
  *     go through in passes of EQTL_GRM_NOALLOC_CHUNK);
- *   - the first call on a device resolves the array's address
- *     (cudaGetSymbolAddress) with the device current; make that call before
- *     any stream capture;
+ *   - eqtl_open resolves the array's address (cudaGetSymbolAddress, with
+ *     the device current) and loads the kernels of this call, so that the
+ *     array and the kernel images are in place before the call is first
+ *     made: open the context while device memory can still be allocated,
+ *     and before any stream capture;
+ *   - the call returns once its work on the context's stream has finished
+ *     (the outputs are ready to use);
  *   - the accumulators and counters are zeroed at the start of every call
- *     on the context's stream;
+ *     on the context's stream; K is exactly symmetric (the lower triangle
+ *     is summed, the upper one mirrors it);
  *   - the scratch is shared by every context on the device: overlapping
  *     calls (other threads, contexts or streams) race; serialise them. */
 #define EQTL_GRM_NOALLOC_MAX_N 512

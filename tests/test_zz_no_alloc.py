@@ -33,18 +33,26 @@ def test_grm_noalloc_matches_grm(n_file, n, m):
         K_ref, N_ref, mu_ref = c.grm()
         bed_d = torch.from_numpy(rows).cuda()
         col_d = torch.from_numpy(cols).cuda()
-        for _ in range(2):  # two calls in a row: the scratch restarts from zero
-            K_d = torch.full((n, n), float("nan"), dtype=torch.float64, device="cuda")
-            N_d = torch.full((n * (n + 1) // 2,), -1, dtype=torch.int32, device="cuda")
+        # outputs allocated up front, as a caller that cannot allocate has them
+        outs = [(torch.full((n, n), float("nan"), dtype=torch.float64, device="cuda"),
+                 torch.full((n * (n + 1) // 2,), -1, dtype=torch.int32, device="cuda")) for _ in range(2)]
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        for K_d, N_d in outs:  # two calls in a row: the scratch restarts from zero
             mu = c.grm_noalloc(bed_d.data_ptr(), m, rows.shape[1], col_d.data_ptr(), n, K_d.data_ptr(),
                                N_d.data_ptr(), **kw)
             torch.cuda.synchronize()
+            # no device memory was taken by the call (the scratch array and the
+            # kernels were set up when the context was opened)
+            assert torch.cuda.mem_get_info()[0] == free0
             assert mu == mu_ref
             np.testing.assert_array_equal(N_d.cpu().numpy(), N_ref)
             # both paths accumulate FP32 tile partials (FP16 hi/lo operands)
             # into FP64, over different K ranges: agree to the GRM's own
             # tolerance against the FP64 oracle, twice over
-            np.testing.assert_allclose(K_d.cpu().numpy(), K_ref, rtol=0, atol=4e-6 * np.abs(K_ref).max())
+            Kh = K_d.cpu().numpy()
+            np.testing.assert_array_equal(Kh, Kh.T)
+            np.testing.assert_allclose(Kh, K_ref, rtol=0, atol=4e-6 * np.abs(K_ref).max())
 
 
 def test_grm_noalloc_rejects_oversize_n():
