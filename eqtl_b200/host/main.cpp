@@ -6,6 +6,8 @@
 // scopes; per (model, scope) the pairs / top / region files; BH over the
 // scope's genes.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <iostream>
 #include <memory>
 #include <numeric>
@@ -161,7 +163,27 @@ int run_scan(const Options& opt) {
     // eigendecomposition (sparsify_grm, src/model_lmm.cpp:88-104)
     const double thr = opt.fast ? 1e-4 : 0.0;
     int64_t zeroed = 0;
-    if (!opt.grm.empty()) {
+    if (const char* bf = std::getenv("EQTL_LMM_BASIS")) {
+      // an eigenbasis computed elsewhere (for example by the reference's own
+      // eigensolver, whose eigenvector signs its LMM permutations depend on)
+      std::vector<double> lam_in(n), Q_in(n * n);
+      FILE* fp = std::fopen(bf, "rb");
+      if (!fp) die(std::string("EQTL_LMM_BASIS: cannot open ") + bf);
+      const size_t got = std::fread(lam_in.data(), sizeof(double), n, fp) +
+                         std::fread(Q_in.data(), sizeof(double), n * n, fp);
+      const bool extra = std::fgetc(fp) != EOF;
+      std::fclose(fp);
+      if (got != n + n * n || extra)
+        die("EQTL_LMM_BASIS: expected " + std::to_string(n) + " eigenvalues and a " + std::to_string(n) + " x " +
+            std::to_string(n) + " eigenvector matrix (float64)");
+      for (double& l : lam_in) l = std::max(l, 0.0);
+      dev.check(eqtl_lmm_set_basis(dev.ctx, Q_in.data(), lam_in.data(), static_cast<int32_t>(n)), "LMM basis");
+      if (opt.perm > 0) {
+        st.basis_Q = Q_in;
+        st.basis_lambda = lam_in;
+      }
+      info(std::string("LMM eigenbasis read from ") + bf);
+    } else if (!opt.grm.empty()) {
       std::vector<double> K = slice_grm(load_grm(opt.grm), st.samples);
       dev.check(eqtl_lmm_basis_fast(dev.ctx, K.data(), static_cast<int32_t>(n), thr, lam, Q, &zeroed), "LMM basis");
     } else {

@@ -70,7 +70,25 @@ namespace {
 struct Job {
   int gene = 0;                  // column of the phenotype matrix
   const GeneLoc* loc = nullptr;  // null in gw scope without a location
+  int work = -1;                 // position in the per-thread cis driver's gene list
 };
+
+// The reference's per-thread cis driver (run_cis_parallel, src/scan_cis.cpp:
+// 29-160; cis with -t > 1) gives thread t the genes [t c, (t + 1) c) of its
+// (chromosome, TSS)-sorted list, c = ceil(genes / threads); each thread
+// writes its pairs and tops to a temporary file, and the files are appended
+// to the output in thread order with `dst << in.rdbuf()`. Appending a file
+// that holds nothing sets the output stream's failbit, after which nothing
+// more reaches that file. written[t] says whether thread t's rows appear.
+std::vector<char> threads_written(const std::vector<char>& has_rows) {
+  std::vector<char> written(has_rows.size(), 0);
+  bool ok = true;
+  for (size_t t = 0; t < has_rows.size(); ++t) {
+    written[t] = ok && has_rows[t];
+    if (!has_rows[t]) ok = false;
+  }
+  return written;
+}
 
 // Complete-case sample set of one gene (build_gene_ready, src/scan_common.cpp:
 // 11-70): finite phenotype and covariates; fewer than 3 samples or an all-zero
@@ -235,7 +253,7 @@ PairRow make_row(const Study& st, const std::string& gene, const GeneLoc* loc, i
 // Writes pairs (in `order`), tops and region rows of one device scan.
 void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const std::string& scope, double pthr,
           const std::vector<size_t>& pair_order, ScopeFiles& out, std::vector<RegionRow>& regions,
-          const std::vector<PermOut>* perms) {
+          const std::vector<PermOut>* perms, size_t n_works_par = 0) {
   std::vector<int64_t> need;
   for (const auto& q : R.pairs) need.push_back(q.snp);
   for (const auto& g : R.genes)
@@ -251,10 +269,24 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
     }
     return r;
   };
+  // per-thread driver: which thread's pairs and tops reach the files
+  const size_t T = n_works_par ? static_cast<size_t>(std::max(1, st.opt->threads)) : 0;
+  const size_t chunk = T ? (n_works_par + T - 1) / T : 1;
+  auto thread_of = [&](size_t j) { return static_cast<size_t>(jobs[j].work) / chunk; };
+  std::vector<char> pairs_ok, tops_ok;
+  if (T) {
+    std::vector<char> hp(T, 0), ht(T, 0);
+    for (const auto& q : R.pairs) hp[thread_of(q.gene)] = 1;
+    for (size_t j = 0; j < jobs.size(); ++j)
+      if (R.genes[j].best_snp >= 0 && R.genes[j].best_p <= pthr && R.genes[j].best_p <= 1.0) ht[thread_of(j)] = 1;
+    pairs_ok = threads_written(hp);
+    tops_ok = threads_written(ht);
+  }
   for (size_t k : pair_order) {
     const eqtl_pair& q = R.pairs[k];
     const Job& jb = jobs[q.gene];
     ++n_sig[q.gene];
+    if (T && !pairs_ok[thread_of(q.gene)]) continue;
     write_pair(out.pairs,
                with_glm(make_row(st, st.genes[jb.gene], jb.loc, q.snp, af.at(q.snp), q.beta, q.se, q.t, q.p, q.r2, R.n),
                         q.gene),
@@ -279,7 +311,7 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
       rr.s2 = (*perms)[j].beta.s2;
     }
     regions.push_back(rr);
-    if (g.best_snp >= 0 && g.best_p <= pthr && g.best_p <= 1.0)
+    if (g.best_snp >= 0 && g.best_p <= pthr && g.best_p <= 1.0 && !(T && !tops_ok[thread_of(j)]))
       write_pair(out.top,
                  with_glm(make_row(st, rr.gene, jb.loc, g.best_snp, af.at(g.best_snp), g.best_beta, g.best_se,
                                    g.best_t, g.best_p, g.best_r2, R.n),
@@ -338,22 +370,27 @@ void run_trans(const Study& st, const std::string& model, const std::string& sco
 
 void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::vector<RegionRow>& regions) {
   const Options& opt = *st.opt;
-  std::vector<Job> jobs;
+  std::vector<Job> works, jobs;
   for (size_t g = 0; g < st.genes.size(); ++g) {
     auto it = st.annot.find(st.genes[g]);
     if (it == st.annot.end()) continue;
     Job jb;
     jb.gene = static_cast<int>(g);
     jb.loc = &it->second;
+    works.push_back(jb);
+  }
+  if (opt.threads > 1)
+    std::stable_sort(works.begin(), works.end(), [](const Job& a, const Job& b) {
+      return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
+    });
+  for (size_t w = 0; w < works.size(); ++w) {
+    Job jb = works[w];
+    jb.work = static_cast<int>(w);
     // the LM path applies the complete-case checks; the LMM path with the
     // shared basis takes the gene as it is (src/scan_cis.cpp:56-63)
     if (!gene_ready(st, gene_y(st, jb.gene), model == "lm")) continue;
     jobs.push_back(jb);
   }
-  if (opt.threads > 1)
-    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) {
-      return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
-    });
   info("cis " + model + ": " + std::to_string(jobs.size()) + " genes");
   if (jobs.empty()) return;
   const double pthr = opt.pval_cis;
@@ -402,7 +439,8 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
     const eqtl_pair &x = R.pairs[a], &y = R.pairs[b];
     return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
   });
-  emit(st, jobs, R, "cis", pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
+  emit(st, jobs, R, "cis", pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr,
+       opt.threads > 1 ? works.size() : 0);
 }
 
 // Whether every finite value is a non-negative integer (within 1e-8) and one
@@ -424,7 +462,7 @@ void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::ve
   // before --pheno-norm, and the genes go in (chromosome, TSS) order
   const bool par_cis = scope == "cis" && opt.threads > 1 && have_gff;
   const size_t n = st.samples.size();
-  std::vector<Job> jobs;
+  std::vector<Job> works, jobs;
   for (size_t g = 0; g < st.genes.size(); ++g) {
     Job jb;
     jb.gene = static_cast<int>(g);
@@ -440,13 +478,18 @@ void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::ve
       warn("skip non-count gene for glm: " + st.genes[g]);
       continue;
     }
-    if (!gene_ready(st, y, true)) continue;
-    jobs.push_back(jb);
+    works.push_back(jb);
   }
   if (par_cis)
-    std::stable_sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) {
+    std::stable_sort(works.begin(), works.end(), [](const Job& a, const Job& b) {
       return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
     });
+  for (size_t w = 0; w < works.size(); ++w) {
+    Job jb = works[w];
+    jb.work = static_cast<int>(w);
+    if (!gene_ready(st, gene_y(st, jb.gene), true)) continue;
+    jobs.push_back(jb);
+  }
   info(scope + " glm: " + std::to_string(jobs.size()) + " genes");
   if (jobs.empty()) return;
   const double pthr = scope == "cis" ? opt.pval_cis : opt.pval_trans;
@@ -511,7 +554,8 @@ void run_glm(const Study& st, const std::string& scope, ScopeFiles& out, std::ve
     const eqtl_pair &x = R.pairs[a], &y = R.pairs[b];
     return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
   });
-  emit(st, jobs, R, scope, pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr);
+  emit(st, jobs, R, scope, pthr, order, out, regions, opt.perm > 0 ? &perms : nullptr,
+       par_cis ? works.size() : 0);
 }
 
 }  // namespace eqtl_host

@@ -250,6 +250,25 @@ class Summary:
     acat_sens: float = 0.0   # |d log10 acat_p / d t| (see AcatAcc.log10_sensitivity)
 
 
+def per_thread_written(rows, work_of_row, threads, n_works):
+    """The rows of a pairs or top file as the reference's per-thread cis
+    driver leaves them (src/scan_cis.cpp:29-160): thread t scans the works
+    [t c, (t + 1) c), c = ceil(n_works / threads), into a temporary file, and
+    the files are appended in thread order with `dst << in.rdbuf()`.
+    Appending an empty file sets the stream's failbit, so nothing of that or
+    any later thread reaches the output."""
+    T = max(1, threads)
+    c = -(-n_works // T) if n_works else 1
+    has = [False] * T
+    for w in work_of_row:
+        has[w // c] = True
+    ok, written = True, []
+    for t in range(T):
+        written.append(ok and has[t])
+        ok = ok and has[t]
+    return [r for r, w in zip(rows, work_of_row) if written[w // c]]
+
+
 def pair_row(gene, snp_meta, h, n, loc, scope):
     chrom, pos, sid, ref, alt = snp_meta
     tss = fmt(float(pos - loc.tss)) if loc is not None else "NA"
@@ -332,9 +351,15 @@ class Scanner:
 
     def run(self):
         res = {}
+        self.sens_by = {}  # "model.scope" -> gene -> |d log10 acat_p / d t|
         for model in self.opt.out_models:
             for scope in self.scopes():
+                before = dict(getattr(self, "sens", {}))
+                self.sens = {}
                 res[(model, scope)] = self.run_scope(model, scope)
+                self.sens_by[f"{model}.{scope}"] = dict(self.sens)
+                before.update(self.sens)
+                self.sens = before
         return res
 
     # -- SNP-outer trans/gw (src/scan_trans_lm.cpp:41-163, src/scan_trans_lmm.cpp:82-251) --
@@ -450,8 +475,9 @@ class Scanner:
             if K.shape[0] == len(self.samples):
                 basis = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
         pairs, tops, summ = [], [], []
+        pair_w, top_w = [], []  # position in `works` of each pair's / top's gene
         bim_chrom = [b[0] for b in self.bim]
-        for gi, gene, loc in works:
+        for wi, (gi, gene, loc) in enumerate(works):
             y = self.gene_y(gi)
             if basis is not None and np.all(np.isfinite(y)) and np.all(np.isfinite(self.X)):
                 keep, yk, Xk = np.arange(len(y)), y, self.X
@@ -487,6 +513,7 @@ class Scanner:
                     row = pair_row(gene, self.snp_meta(snp), _hit(st, i, af_sub[i]), n, loc, "cis")
                     if pv <= pthr:
                         pairs.append(row)
+                        pair_w.append(wi)
                         s.n_sig += 1
                     if pv < best_p:
                         best_p, best_row = pv, row
@@ -499,7 +526,11 @@ class Scanner:
                           lmm_basis=(Q, lam) if model == "lmm" else None)
             if best_row is not None and best_p <= pthr and best_p <= 1.0:
                 tops.append(best_row)
+                top_w.append(wi)
             summ.append(s)
+        if opt.threads > 1:
+            pairs = per_thread_written(pairs, pair_w, opt.threads, len(works))
+            tops = per_thread_written(tops, top_w, opt.threads, len(works))
         return pairs, tops, self.finish(summ)
 
     # -- NB GLM, gene-outer for every scope (src/scan.cpp:227-300 and, for cis
@@ -522,7 +553,8 @@ class Scanner:
             works.sort(key=lambda w: (w[2].chrom, w[2].tss))
         bim_chrom = [b[0] for b in self.bim]
         pairs, tops, summ = [], [], []
-        for gi, gene, loc in works:
+        pair_w, top_w = [], []  # position in `works` of each pair's / top's gene
+        for wi, (gi, gene, loc) in enumerate(works):
             y = self.gene_y(gi)
             if not parallel_cis and not R.looks_like_counts(y):
                 continue                                       # "skip non-count gene"
@@ -562,6 +594,7 @@ class Scanner:
                         fmt(prep.phi), "1" if prep.converged else "0")
                     if pv <= pthr:
                         pairs.append(row)
+                        pair_w.append(wi)
                         s.n_sig += 1
                     if pv < best_p:
                         best_p, best_row = pv, row
@@ -586,7 +619,11 @@ class Scanner:
                     s.p_beta, s.s1, s.s2 = R.beta_approx_p(minps, best_p)
             if best_row is not None and best_p <= pthr and best_p <= 1.0:
                 tops.append(best_row)
+                top_w.append(wi)
             summ.append(s)
+        if parallel_cis:
+            pairs = per_thread_written(pairs, pair_w, opt.threads, len(works))
+            tops = per_thread_written(tops, top_w, opt.threads, len(works))
         return pairs, tops, self.finish(summ)
 
     # -- permutations (include/eqtl/scan_cis.hpp:68-176, src/scan_perm.cpp:11-142) --

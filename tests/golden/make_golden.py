@@ -119,6 +119,100 @@ def build_case(name: str, spec: dict) -> None:
         json.dump(manifest, f, indent=1)
 
 
+# -k: a GRM written by the reference's --make-grm for a wider sample set
+# ("gwide": 12 more samples than the analysis fileset, in a shuffled order),
+# then sliced by sample ID to the analysis samples. The phenotype table lists
+# the samples in yet another order and holds 3 samples absent from the
+# genotypes, so the analysis order differs from both the .fam and the
+# .grm.id order.
+KGRM_RUNS = [
+    ("grmw", ["-b", "gwide", "--make-grm"]),
+    ("k", ["-b", "geno", "--model", "lm,lmm", "--mode", "all", "-k", "ref_grmw", "-w", "500000", "--pval-cis",
+           "1e-2", "--pval-trans", "1e-2", "-t", "2"]),
+    ("kperm", ["-b", "geno", "--model", "lmm", "--mode", "all", "-k", "ref_grmw", "-w", "500000", "--pval-cis",
+               "1e-2", "--pval-trans", "1e-3", "--perm", "30", "--seed", "5", "--perm-trans-thr", "1e-2",
+               "--perm-trans-top", "5", "-t", "2"]),
+]
+
+
+def build_kgrm_case() -> None:
+    import numpy as np
+    d = os.path.join(HERE, "kgrm")
+    if os.path.isdir(d):
+        shutil.rmtree(d)
+    os.makedirs(d)
+    n, n_wide = 120, 132
+    g = synth.make_genotypes(401, n=n_wide, m=800, n_chrom=3, chrom_len=5_000_000, family=(4, 5, n_wide - 20),
+                             miss_rate=0.01, maf_lo=0.02)
+    rng = np.random.default_rng(402)
+    perm = rng.permutation(n_wide)
+    wide = synth.Genotypes(g.codes[:, perm], g.chrom, g.pos, g.ids, g.a1, g.a2, [g.samples[i] for i in perm], g.af)
+    synth.write_plink(os.path.join(d, "gwide"), wide)
+    sub = synth.Genotypes(g.codes[:, :n], g.chrom, g.pos, g.ids, g.a1, g.a2, g.samples[:n], g.af)
+    synth.write_plink(os.path.join(d, "geno"), sub)
+    chroms = sorted(set(g.chrom), key=g.chrom.index)
+    ids, gc, st, en, sd, tss = synth.make_genes(403, 30, chroms, 5_000_000, body=1000)
+    Y, C = synth.make_pheno_lm(404, sub, len(ids), 2, cis_effects=True, gene_tss=tss, gene_chrom=gc,
+                               window=500_000, n_trans=8)
+    extra = 3
+    Yx = np.vstack([Y, rng.standard_normal((extra, Y.shape[1]))])
+    Cx = np.vstack([C, rng.standard_normal((extra, C.shape[1]))])
+    names = sub.samples + [f"X{i + 1:03d}" for i in range(extra)]
+    order = rng.permutation(n + extra)
+    synth.write_pheno(os.path.join(d, "pheno.tsv"), [names[i] for i in order], ids, Yx[order])
+    synth.write_covar(os.path.join(d, "covar.tsv"), names, Cx)
+    synth.write_gff(os.path.join(d, "genes.gff"), ids, gc, st, en, sd)
+    manifest = {"runs": {}}
+    for tag, argv in KGRM_RUNS:
+        cmd = [REF] + argv[:2]
+        if "--make-grm" not in argv:
+            cmd += ["-e", "pheno.tsv", "-g", "genes.gff", "-c", "covar.tsv"]
+        cmd += argv[2:] + ["-o", f"ref_{tag}"]
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise SystemExit(f"kgrm/{tag} failed: {r.stderr}")
+        manifest["runs"][tag] = {"argv": cmd[1:]}
+    for f in os.listdir(d):
+        if ".tmp." in f:
+            os.remove(os.path.join(d, f))
+    with open(os.path.join(d, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+def write_bases(case_names=None) -> None:
+    """For every golden run that has LMM permutations, the eigenbasis the
+    reference's own eigensolver gives for that run's GRM (oracle/_ref/eigsolve
+    on the oracle's FP64 GRM, or on the sliced -k file), written as
+    ref_<tag>.basis.bin: n float64 eigenvalues, then the n x n eigenvectors
+    column by column. LMM permutations shuffle residuals in eigen-
+    coordinates, so with this basis installed a run reproduces the
+    reference's permutation p-values exactly."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+    import driver
+    import refargs
+    import restate as R
+    for c in sorted(os.listdir(HERE)):
+        cd = os.path.join(HERE, c)
+        if not os.path.isdir(cd) or (case_names and c not in case_names):
+            continue
+        man = json.load(open(os.path.join(cd, "manifest.json")))
+        for tag, r in man["runs"].items():
+            argv = r["argv"]
+            if argv[0] == "fission" or "--perm" not in argv:
+                continue
+            opt = refargs.options_from_argv(argv, cd)
+            if "lmm" not in opt.out_models:
+                continue
+            K = driver.Scanner(opt).grm()
+            Q, lam = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
+            with open(os.path.join(cd, f"ref_{tag}.basis.bin"), "wb") as f:
+                f.write(np.ascontiguousarray(lam, dtype=np.float64).tobytes())
+                f.write(np.asfortranarray(Q, dtype=np.float64).tobytes(order="F"))
+            print("basis", c, tag, K.shape[0])
+
+
 # The fission subcommand (data thinning + PEER factors) on phenotype tables
 # only: counts (binomial thinning) and continuous values with a missing entry
 # (Gaussian fission), with and without covariate residualisation.
@@ -161,11 +255,18 @@ if __name__ == "__main__":
     if not os.path.exists(REF):
         raise SystemExit("build the reference first: make -C oracle")
     only = sys.argv[1:]                      # case names to (re)build; all by default
+    if only and only[0] == "--bases":        # only the LMM eigenbasis files of existing cases
+        write_bases(only[1:])
+        raise SystemExit(0)
     for name, spec in CASES.items():
         if only and name not in only:
             continue
         build_case(name, spec)
         print("built", name)
+    if not only or "kgrm" in only:
+        build_kgrm_case()
+        print("built kgrm")
     if not only or "fission" in only:
         build_fission_case()
         print("built fission")
+    write_bases(only or None)

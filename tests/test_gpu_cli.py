@@ -9,10 +9,16 @@ Tolerances: LM pairs carry the FP64 refinement (log10 p within 1e-5, beta
 within 1e-6 relative); LMM adds the REML optimiser difference (1e-4 and
 1e-5). ACAT p uses the condition-aware bound of the parity tests (1e-3 plus
 3 |dlog10 acat / dt| times the screening error of t, from the oracle).
-Permutation p_emp is exact for the LM (same seeded shuffles, FP64 tests);
-for the LMM the permuted phenotypes live in the eigenbasis, whose eigenvector
-signs differ between Eigen and cuSOLVER, so p_emp / p_beta agree in
-distribution only and are checked for presence."""
+Permutation p_emp is exact for the LM (same seeded shuffles, FP64 tests).
+LMM permutations shuffle residuals in eigen-coordinates, so they depend on
+the eigenvector signs, which differ between the reference's eigensolver
+(Eigen) and cuSOLVER: runs with LMM permutations install the reference
+eigensolver's basis of the run's GRM (ref_<tag>.basis.bin, made by
+tests/golden/make_golden.py) through EQTL_LMM_BASIS, and then p_emp is
+exact and p_beta / shapes within 5%, as for the LM.
+
+The reference's own test panel (case "refdata", tests/golden/make_refdata.py)
+runs from its converted .bed and from its original VCF."""
 import json
 import os
 import subprocess
@@ -30,16 +36,57 @@ GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 BIN = os.path.join(os.path.dirname(GOLD), "..", "eqtl_b200", "bin", "eqtl")
 
 
+def _manifest(case):
+    return json.load(open(os.path.join(GOLD, case, "manifest.json")))
+
+
 def _runs():
     out = []
     for c in sorted(os.listdir(GOLD)):
         if not os.path.isdir(os.path.join(GOLD, c)):
             continue
-        man = json.load(open(os.path.join(GOLD, c, "manifest.json")))
-        for tag, r in man["runs"].items():
+        for tag, r in _manifest(c)["runs"].items():
             if r["argv"][0] != "fission":  # the fission subcommand has its own tests
                 out.append((c, tag, r["argv"]))
     return out
+
+
+def _skip_src(case, src):
+    """Cases that carry their own VCF (the reference's test panel, "vcf" in
+    the manifest) run from it ("vcf_orig") instead of from VCFs written here."""
+    own = _manifest(case).get("vcf")
+    if src == "vcf_orig" and not own:
+        pytest.skip("no VCF of its own")
+    if src in ("vcf", "vcf_ds") and own:
+        pytest.skip("runs from the case's own VCF")
+
+
+_SENS = {}
+
+
+def _acat_sens(case, tag, argv, model, scope):
+    """gene -> |d log10 acat_p / d t| of one model and scope, from the file
+    made with the fixtures when there is one, else from the oracle."""
+    key = (case, tag)
+    if key not in _SENS:
+        f = os.path.join(GOLD, case, f"ref_{tag}.sens.json")
+        if os.path.exists(f):
+            _SENS[key] = json.load(open(f))
+        else:
+            ora = driver.Scanner(refargs.options_from_argv(argv, os.path.join(GOLD, case)))
+            ora.run()
+            _SENS[key] = ora.sens_by
+    return _SENS[key].get(f"{model}.{scope}", {})
+
+
+def _basis_env(argv, case_dir, tag):
+    """EQTL_LMM_BASIS for a run with LMM permutations (see the module text)."""
+    env = dict(os.environ)
+    env.pop("EQTL_LMM_BASIS", None)
+    f = os.path.join(case_dir, f"ref_{tag}.basis.bin")
+    if "--perm" in argv and os.path.exists(f):
+        env["EQTL_LMM_BASIS"] = f
+    return env
 
 
 def bed_to_vcf(prefix: str, out_path: str, ds: bool = False) -> None:
@@ -60,7 +107,7 @@ def bed_to_vcf(prefix: str, out_path: str, ds: bool = False) -> None:
     synth.write_tabix_header(out_path)
 
 
-def _run(argv, case_dir, out_prefix, src="bed", tmp=None):
+def _run(argv, case_dir, out_prefix, src="bed", tmp=None, env=None):
     a = list(argv)
     a[a.index("-o") + 1] = out_prefix
     if src in ("vcf", "vcf_ds"):  # the same genotypes through -v (GT, or DS)
@@ -69,14 +116,19 @@ def _run(argv, case_dir, out_prefix, src="bed", tmp=None):
             bed_to_vcf(os.path.join(case_dir, a[a.index("-b") + 1]), vcf, ds=src == "vcf_ds")
         k = a.index("-b")
         a[k:k + 2] = ["-v", vcf]
-    r = subprocess.run([os.path.abspath(BIN)] + a, cwd=case_dir, capture_output=True, text=True, timeout=600)
+    elif src == "vcf_orig":  # the VCF the case's .bed was converted from
+        k = a.index("-b")
+        a[k:k + 2] = ["-v", json.load(open(os.path.join(case_dir, "manifest.json")))["vcf"]]
+    r = subprocess.run([os.path.abspath(BIN)] + a, cwd=case_dir, capture_output=True, text=True, timeout=600,
+                       env=env)
     assert r.returncode == 0, r.stderr[-3000:]
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds"])
+@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds", "vcf_orig"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" in r[2]])
 def test_cli_make_grm(case, tag, argv, src, tmp_path):
+    _skip_src(case, src)
     d = os.path.join(GOLD, case)
     out = str(tmp_path / "out")
     _run(argv, d, out, src, tmp_path)
@@ -89,15 +141,15 @@ def test_cli_make_grm(case, tag, argv, src, tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds"])
+@pytest.mark.parametrize("src", ["bed", "vcf", "vcf_ds", "vcf_orig"])
 @pytest.mark.parametrize("case,tag,argv", [r for r in _runs() if "--make-grm" not in r[2]])
 def test_cli_scan_matches_reference(case, tag, argv, src, tmp_path):
+    _skip_src(case, src)
     d = os.path.join(GOLD, case)
     out = str(tmp_path / "out")
-    _run(argv, d, out, src, tmp_path)
+    env = _basis_env(argv, d, tag)
+    _run(argv, d, out, src, tmp_path, env)
     opt = refargs.options_from_argv(argv, d)
-    ora = driver.Scanner(opt)
-    ora.run()                                    # per-gene ACAT sensitivities
     scopes = ["gw"] if not opt.gff else {"cis": ["cis"], "trans": ["trans"], "gw": ["gw"],
                                          "all": ["cis", "trans"]}[opt.mode]
     errs = []
@@ -114,15 +166,11 @@ def test_cli_scan_matches_reference(case, tag, argv, src, tmp_path):
             hr, rr = tsvcmp.read_tsv(f"{ref}.region.tsv")
             hg, gg = tsvcmp.read_tsv(f"{got}.region.tsv")
             assert hr == hg
-            exact_perm = model == "lm"
+            if model == "lmm" and "--perm" in argv:
+                assert "EQTL_LMM_BASIS" in env, "LMM permutation run without the reference's eigenbasis"
             errs += [f"{model}.{scope} region: {e}" for e in
-                     tsvcmp.compare_region(rr, gg, tsvcmp.Tol(log10p=1e-3), check_perm=exact_perm,
-                                           acat_sens=ora.sens, t_err=T_ERR)]
-            if not exact_perm:
-                R = {r[0]: r for r in rr}
-                for g in gg:
-                    if g[0] in R and R[g[0]][7] != "NA":
-                        assert g[7] != "NA", (model, scope, g[0])
+                     tsvcmp.compare_region(rr, gg, tsvcmp.Tol(log10p=1e-3), check_perm=True,
+                                           acat_sens=_acat_sens(case, tag, argv, model, scope), t_err=T_ERR)]
             # the gene order of each file is the reference's
             assert [r[0] for r in rr] == [g[0] for g in gg], (model, scope)
     assert not errs, "\n".join(errs[:40])
