@@ -920,6 +920,38 @@ def lmm_stats_gtil(prep: PrepLmm, Gtil: np.ndarray):
     return out
 
 
+def lmm_stats_gtil_genes(preps, Gtil: np.ndarray):
+    """lmm_stats_gtil for several genes that share the eigenbasis, on the
+    same rotated dosages Gtil [m, n]: the same arithmetic
+    (src/scan_trans_lmm.cpp:11-40), with gg, a and yg of all genes formed as
+    matrix products. Returns dict of [m, len(preps)] arrays."""
+    W = np.column_stack([pr.dinv for pr in preps])             # [n, G]
+    gg = (Gtil * Gtil) @ W                                      # [m, G]
+    yg = Gtil @ (W * np.column_stack([pr.ytil for pr in preps]))
+    m, G = Gtil.shape[0], len(preps)
+    out = {k: np.zeros((m, G)) for k in ("beta", "se", "stat", "r2")}
+    out["p"] = np.ones((m, G))
+    for j, pr in enumerate(preps):
+        a = Gtil @ (pr.Xtil * pr.dinv[:, None])                 # [m, p]
+        u = np.linalg.solve(pr.A00, a.T).T
+        S = gg[:, j] - np.einsum("ij,ij->i", a, u)
+        df = pr.n - pr.p - 1
+        ok = ~(gg[:, j] < 1e-12) & ~(S <= 1e-15)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            bg = (yg[:, j] - a @ pr.chi0) / S
+            q = np.maximum(pr.rss_null - S * bg * bg, 0.0)
+            sigma2 = q / df if df > 0 else np.ones(m)
+            se = np.sqrt(np.maximum(sigma2 / S, 0.0))
+            stat = np.where(se > 0, bg / se, 0.0)
+            r2 = np.maximum(0.0, 1.0 - q / pr.rss_null) if pr.rss_null > 1e-15 else np.zeros(m)
+        out["beta"][:, j] = np.where(ok, bg, 0.0)
+        out["se"][:, j] = np.where(ok, se, 0.0)
+        out["stat"][:, j] = np.where(ok, stat, 0.0)
+        out["r2"][:, j] = np.where(ok, r2, 0.0)
+        out["p"][:, j] = np.where(ok, p_from_t(out["stat"][:, j], df), 1.0)
+    return out
+
+
 def test_lmm_many(prep: PrepLmm, G: np.ndarray):
     """test_lmm over raw dosage rows G [m, n] (rotates each row, :173)."""
     return lmm_stats_gtil(prep, G @ prep.Q)
@@ -936,19 +968,25 @@ def compute_grm(dosage: np.ndarray, miss: np.ndarray):
     use = ~((p < 1e-8) | (p > 1.0 - 1e-8))
     sd = np.sqrt(2.0 * p * (1.0 - p))
     use &= ~(sd < 1e-12)
-    Z = (dosage[use] - mu[use, None]) / sd[use, None]
-    M = miss[use].astype(np.int64)
     m = int(use.sum())
     if m == 0:
         raise ValueError("no SNPs for GRM")
-    A = Z.T @ Z
-    sub_miss = M.sum(0)
-    joint = M.T @ M
+    n = dosage.shape[1]
+    A = np.zeros((n, n))
+    joint = np.zeros((n, n))  # integer counts, exact in FP64
+    ui = np.nonzero(use)[0]
+    for c0 in range(0, ui.size, 16384):  # in SNP blocks, to bound the memory
+        u = ui[c0:c0 + 16384]
+        Z = (dosage[u] - mu[u, None]) / sd[u, None]
+        A += Z.T @ Z
+        M = miss[u].astype(np.float64)
+        joint += M.T @ M
+    sub_miss = miss[use].sum(0).astype(np.int64)
+    joint = np.rint(joint).astype(np.int64)
     subN = m - sub_miss[:, None] - sub_miss[None, :] + joint
     np.fill_diagonal(subN, m - sub_miss)
     with np.errstate(divide="ignore", invalid="ignore"):
         K = np.where(subN > 0, A / subN, 0.0)
-    n = dosage.shape[1]
     il = np.tril_indices(n)
     # row-major lower triangle incl. diagonal: (i, j<=i)
     order = np.lexsort((il[1], il[0]))

@@ -4,7 +4,7 @@ Each case is a seeded synthetic PLINK data set (eqtl_b200.synth) plus the
 outputs of the reference eqtl program itself, built from the reference's own
 sources by `make -C oracle` (oracle/_ref/eqtl). Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py [case ...]
+    make -C oracle REF=<reference tree> && python tests/golden/make_golden.py [case ...]
 
 The fixtures are small (n=120 samples, 800 SNPs, 40 genes) so they commit
 cheaply; larger parity cases are generated on the fly by the GPU tests.
@@ -253,7 +253,7 @@ def build_fission_case() -> None:
 
 if __name__ == "__main__":
     if not os.path.exists(REF):
-        raise SystemExit("build the reference first: make -C oracle")
+        raise SystemExit("build the reference first: make -C oracle REF=<reference tree>")
     only = sys.argv[1:]                      # case names to (re)build; all by default
     if only and only[0] == "--bases":        # only the LMM eigenbasis files of existing cases
         write_bases(only[1:])

@@ -11,7 +11,7 @@ reference's VcfSession::parse_record does (src/vcf_session.cpp:220-258). The
 GPU tests then run the host program on both the .bed and the original VCF
 and compare every output file with the reference's.
 
-    make -C oracle && python tests/golden/make_refdata.py [path/to/reference]
+    make -C oracle REF=<reference tree> && python tests/golden/make_refdata.py [path/to/reference]
 
 The reference tree defaults to $EQTL_REFERENCE, else /root/reference.
 """
@@ -97,7 +97,7 @@ def write_sensitivities(manifest) -> None:
 def main(ref_root: str) -> None:
     src = os.path.join(ref_root, "data", "test")
     if not os.path.exists(REF):
-        raise SystemExit("build the reference first: make -C oracle")
+        raise SystemExit("build the reference first: make -C oracle REF=<reference tree>")
     if os.path.isdir(OUT):
         shutil.rmtree(OUT)
     os.makedirs(OUT)
