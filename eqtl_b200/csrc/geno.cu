@@ -206,6 +206,70 @@ __global__ void __launch_bounds__(32 * kExpandWarps, 4)
   }
 }
 
+// The exact SNP operand of the LMM scan, one warp per kept SNP of 2-bit
+// rows. With n_ok calls present summing to S and c = n_ok / gcd(S, n_ok),
+// the imputed mean S / n_ok times c is an integer, so every value of
+// c * dosage is exact in FP16 while c <= 2048 (always when n_ok <= 2048).
+// Rows with a mean above 1 are stored as c * (2 - dosage), which keeps the
+// missing-call value M = c * mean (or c * (2 - mean)) at most c. Column n
+// (the first padding sample, n < k_pad) holds M, against which the gene-side
+// operands hold minus their own sum, so that the contraction of a gene-side
+// vector v with the row is v . (dosage - mean) / alpha, alpha = +-1 / c.
+// SNPs that are not exact are counted in *inexact.
+__global__ void raw_operand_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
+                                   int n, int k_pad, const int64_t* __restrict__ kept, int64_t m_kept,
+                                   const int32_t* __restrict__ n_miss, const double* __restrict__ s1, __half* raw,
+                                   float* alpha, unsigned long long* inexact) {
+  const int lane = threadIdx.x & 31;
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= m_kept) return;
+  const int64_t s = __ldg(kept + r);
+  const long long n_ok = n - __ldg(n_miss + s);
+  const long long S = llrint(__ldg(s1 + s));
+  long long a = S, b = n_ok;  // gcd(S, n_ok)
+  while (b) {
+    const long long t = a % b;
+    a = b;
+    b = t;
+  }
+  const long long c = a > 0 ? n_ok / a : 1;
+  const bool flip = S > n_ok;
+  if (lane == 0) {
+    alpha[r] = static_cast<float>((flip ? -1.0 : 1.0) / static_cast<double>(c));
+    if (c > 2048) atomicAdd(inexact, 1ull);
+  }
+  // values of the codes 00, 01, 10, 11 (A1 count 2, missing, 1, 0)
+  const float cv = static_cast<float>(c);
+  const uint32_t vm = __half_as_ushort(__float2half_rn(static_cast<float>(a > 0 ? (flip ? 2 * c - S / a : S / a)
+                                                                                 : 0)));
+  const uint32_t v0 = __half_as_ushort(__float2half_rn(flip ? 0.0f : 2.0f * cv));
+  const uint32_t v2 = __half_as_ushort(__float2half_rn(cv));
+  const uint32_t v3 = __half_as_ushort(__float2half_rn(flip ? 2.0f * cv : 0.0f));
+  const uint8_t* row = bed + s * bps;
+  for (int k0 = lane * 8; k0 < k_pad; k0 += 256) {
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      uint32_t h[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int k = k0 + j + t;
+        uint32_t v = 0;  // padding samples
+        if (k < n) {
+          const int cc = __ldg(col + k);
+          const uint32_t code = (static_cast<uint32_t>(__ldg(row + (cc >> 2))) >> ((cc & 3) * 2)) & 3u;
+          v = code == 0 ? v0 : (code == 1 ? vm : (code == 2 ? v2 : v3));
+        } else if (k == n) {
+          v = vm;
+        }
+        h[t] = v;
+      }
+      w[j / 2] = h[0] | (h[1] << 16);
+    }
+    *reinterpret_cast<uint4*>(raw + r * k_pad + k0) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
 __global__ void bed_dosage_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
                                   const int64_t* __restrict__ kept, int64_t lo, int64_t hi,
                                   const double* __restrict__ mu, double* out) {
@@ -252,6 +316,7 @@ void geno_decode(eqtl_ctx* ctx, const int32_t* sample_col, int miss_hand, double
   const int64_t m = g.m_all;
   const int n = g.n;
   ctx->rot.m = 0;  // rotated genotypes belong to the previous genotypes
+  ctx->rot.raw_m = -1;
   ctx->glm_ops.m = 0;
   g.k_pad = ((n + 63) / 64) * 64;
   g.col.upload(sample_col, n, st);
@@ -363,6 +428,42 @@ void geno_load_dosage(eqtl_ctx* ctx, const float* ds, int64_t m, int n_file, con
   g.dense = true;
   g.ds.upload(ds, static_cast<size_t>(m) * n_file, ctx->stream);
   geno_decode(ctx, sample_col, miss_hand, max_miss, maf_min);
+}
+
+// Builds the exact SNP operand of the LMM scan for the loaded 2-bit rows
+// (raw_operand_kernel) once per genotype load; returns whether every kept SNP
+// is exact (false for FP32 dosage rows, which it does not build, and when
+// n leaves no padding sample column).
+bool geno_raw_operand(eqtl_ctx* ctx) {
+  Geno& g = ctx->geno;
+  Rotated& R = ctx->rot;
+  if (R.raw_m == g.m && R.raw.p) return R.raw_exact;
+  R.raw_exact = false;
+  if (g.dense || g.n >= g.k_pad) return false;
+  cudaStream_t st = ctx->stream;
+  const int64_t m = g.m;
+  R.raw.alloc(std::max<size_t>(1, static_cast<size_t>(m) * g.k_pad));
+  // the scan epilogues read alpha 16 SNPs at a time, up to the end of the
+  // last tile
+  R.alpha.alloc(static_cast<size_t>(((m + 255) / 256 + 1) * 256));
+  EQTL_CUDA(cudaMemsetAsync(R.alpha.p, 0, sizeof(float) * R.alpha.n, st));
+  DevBuf<unsigned long long>& cnt = ctx->ws.raw_inexact;
+  cnt.alloc(1);
+  cnt.zero(st);
+  if (m > 0) {
+    ++ctx->launches;
+    const int per_block = 8;
+    raw_operand_kernel<<<static_cast<unsigned>((m + per_block - 1) / per_block), 32 * per_block, 0, st>>>(
+        g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.k_pad, g.kept.p, m, g.n_miss.p, g.s1.p, R.raw.p, R.alpha.p,
+        cnt.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  unsigned long long bad = 0;
+  cnt.download(&bad, 1, st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  R.raw_m = m;
+  R.raw_exact = bad == 0;
+  return R.raw_exact;
 }
 
 void geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out_host) {

@@ -165,6 +165,17 @@ struct Rotated {
   int64_t m = 0;
   int k_pad = 0;
   DevBuf<__half> gt_hi, gt_lo, gt2_hi, gt2_lo;
+  // Exact unrotated SNP operand of the LMM scan (geno_raw_operand): row r =
+  // c_r * dosage (or c_r * (2 - dosage)) in FP16, every value an integer
+  // below 4096, missing calls and padding column n at c_r times the imputed
+  // mean; a gene-side vector v holding -sum(v) at column n gives
+  // v . (dosage - mean) = alpha[r] * (v . row).
+  DevBuf<__half> raw;
+  DevBuf<float> alpha;
+  int64_t raw_m = -1;      // SNPs the operand was built for (-1: not built)
+  bool raw_exact = false;  // every kept SNP representable exactly
+  // FP32 copies of Gt and Gt^2 for the plain FP32 CUDA-core comparator
+  DevBuf<float> gt32, gt2_32;
 };
 
 // Phenotypes / covariates resident on the device (eqtl_pheno_load).
@@ -215,6 +226,10 @@ struct Workspace {
   DevBuf<double> grm_mean, grm_isd, grm_A, eig_work;
   DevBuf<int2> grm_tiles;  // lower-triangle tile list of the GRM contraction
   DevBuf<unsigned long long> grm_count;  // SNPs the GRM uses
+  DevBuf<unsigned long long> raw_inexact;  // SNPs the exact LMM operand cannot hold
+  DevBuf<double> lmm_w, lmm_uv;            // [n, G (p + 1)]: w o (r~, X~_k) and Q times them
+  DevBuf<float> ops32[4];                  // FP32 gene-side operands of the CUDA-core comparator
+  DevBuf<const float*> ops32_ptr;
   DevBuf<__half> grm_zh, grm_zl, grm_mk;
   DevBuf<int> grm_J, eig_info;
 };
@@ -306,6 +321,7 @@ void lmm_rotate(eqtl_ctx* ctx);
 int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, const int32_t* col, int n,
                     int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk);
 void grm_noalloc_prepare(eqtl_ctx* ctx);
+bool geno_raw_operand(eqtl_ctx* ctx);
 void solver_release(eqtl_ctx* ctx);
 void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    const std::vector<int2>& todo, eqtl_pair* out);

@@ -717,6 +717,105 @@ __global__ void lmm_gene_ops_kernel(const double* __restrict__ Ytil, const doubl
   }
 }
 
+// Gene-side vectors of the exact-operand scan, one block per gene, in
+// eigen-coordinates: column (p + 1) g of W is w o r~ and column
+// (p + 1) g + 1 + k is w o X~_k, with w = 1 / max(delta lambda + 1, 1e-12);
+// Q W then holds u = Q (w o r~) and v_k = Q (w o X~_k).
+__global__ void lmm_uv_w_kernel(const double* __restrict__ Ytil, const double* __restrict__ Xtil,
+                                const double* __restrict__ lam, const double* __restrict__ delta,
+                                const double* __restrict__ chi0, int n, int p, int G, double* W) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const double d = delta[g];
+  const double* yt = Ytil + static_cast<int64_t>(g) * n;
+  const double* c0 = chi0 + static_cast<int64_t>(g) * p;
+  double* out = W + static_cast<int64_t>(g) * (p + 1) * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    double r = yt[i];
+    for (int k = 0; k < p; ++k) {
+      const double x = Xtil[static_cast<int64_t>(k) * n + i];
+      r -= x * c0[k];
+      out[static_cast<int64_t>(1 + k) * n + i] = x / v;
+    }
+    out[i] = r / v;
+  }
+}
+
+// Gene-side operands of the exact-operand scan, one block per gene: rows u,
+// v_0 .. v_{p-1} (columns of UV = Q W) and w, each FP16 hi/lo with its own
+// power-of-two scale. unscale[] turns accumulators back into NUM, a_k (the
+// SNP operand carries no scale of its own) and gg (against Gt^2 at s2).
+// u and v_k are scaled to a largest entry in [8, 16), so that minus their sum
+// (at most 16 n <= 32768) fits FP16 as well: it goes to column n, where the
+// SNP operand holds its imputed mean, which centres each SNP inside the
+// contraction.
+__global__ void lmm_gene_ops_raw_kernel(const double* __restrict__ UV, const double* __restrict__ lam,
+                                        const double* __restrict__ delta, int n, int p, int G, int k_pad, float s2,
+                                        __half* const* hi, __half* const* lo, float* unscale) {
+  const int g = blockIdx.x;
+  if (g >= G) return;
+  const int nops = p + 2;
+  __shared__ double mx[kMaxPLmm + 2][8];
+  __shared__ double sc[kMaxPLmm + 2];
+  __shared__ double part[8];
+  const double d = delta[g];
+  const double* uv = UV + static_cast<int64_t>(g) * (p + 1) * n;
+  auto value = [&](int op, int i) -> double {
+    if (i >= n) return 0.0;
+    if (op <= p) return uv[static_cast<int64_t>(op) * n + i];
+    double v = d * lam[i] + 1.0;
+    if (v < 1e-12) v = 1e-12;
+    return 1.0 / v;
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int op = 0; op < nops; ++op) {
+    double m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(value(op, i)));
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) mx[op][warp] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x < nops) {
+    double m = 0;
+    for (int w = 0; w < (blockDim.x >> 5); ++w) m = fmax(m, mx[threadIdx.x][w]);
+    const bool centred = threadIdx.x < nops - 1;  // u and v_k
+    int e = 0;
+    if (m > 0) e = (centred ? 3 : 10) - static_cast<int>(floor(log2(m)));
+    sc[threadIdx.x] = ldexp(1.0, e);
+    const double side = centred ? 1.0 : s2;
+    unscale[static_cast<int64_t>(g) * nops + threadIdx.x] = static_cast<float>(1.0 / (ldexp(1.0, e) * side));
+  }
+  __syncthreads();
+  for (int op = 0; op < nops; ++op) {
+    const double s = sc[op];
+    __half* h_row = hi[op] + static_cast<int64_t>(g) * k_pad;
+    __half* l_row = lo[op] + static_cast<int64_t>(g) * k_pad;
+    double sum = 0.0;
+    for (int i = threadIdx.x; i < k_pad; i += blockDim.x) {
+      const double v = value(op, i) * s;
+      const __half h = __double2half(v);
+      const __half l = __double2half(v - static_cast<double>(__half2float(h)));
+      h_row[i] = h;
+      l_row[i] = l;
+      sum += static_cast<double>(__half2float(h)) + static_cast<double>(__half2float(l));
+    }
+    if (op > p) break;  // w is not centred
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) part[warp] = sum;
+    __syncthreads();  // every thread's writes of column n (zero) are done too
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (blockDim.x >> 5); ++w) t += part[w];
+      const __half h = __double2half(-t);
+      h_row[n] = h;
+      l_row[n] = __double2half(-t - static_cast<double>(__half2float(h)));
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------- scan epilogue
 template <int P>
 struct LmmEpiParams {
@@ -736,10 +835,16 @@ struct LmmEpiParams {
   const float* snp_mean;    // [m, padded to 16 + 16]
   const float* rsum;        // [G]
   const uint8_t* gene_ok;   // [G]
+  // exact-operand LMM scan only (LmmRawEpiParams): per kept SNP the factor
+  // alpha of the raw operand (Rotated::raw)
+  const float* snp_alpha;   // [m, padded to 256 + 256]
 };
 // The same fields select the NB-GLM score-test epilogue (LmmEpi<P, true>).
 template <int P>
 struct GlmEpiParams : LmmEpiParams<P> {};
+// ... and the LMM scan on the exact unrotated SNP operand (LmmEpi<P, false, true>).
+template <int P>
+struct LmmRawEpiParams : LmmEpiParams<P> {};
 
 // Accumulator order of the tile: [gg, a_0 .. a_{P-1}, NUM] (the gene-side
 // operands w, w o X~_k, w o r~ against Gt^2, Gt, Gt). The epilogue is
@@ -751,13 +856,20 @@ struct GlmEpiParams : LmmEpiParams<P> {};
 // centred dosages gc against w, w o x_k and r of the gene's null fit):
 // info = S, U = NUM + mean_s * sum_i r_i, and the screened statistic is
 // z^2 = U^2 / info against the normal tables.
-template <int P, bool GLM = false>
+//
+// RAW = true: NUM and a_k come from the exact unrotated SNP operand
+// (Rotated::raw) against the gene-side vectors u = Q (w o r~) and
+// v_k = Q (w o X~_k), since Gt . (w o r~) = g . Q (w o r~); the operands
+// centre each SNP themselves (padding column n), so x = alpha_s * acc.
+template <int P, bool GLM = false, bool RAW = false>
 struct LmmEpi {
+  static_assert(!(GLM && RAW), "the exact-operand form is the LMM scan's");
   static constexpr bool kGrouped = false;
   static constexpr bool kTwoPhase = true;
   static constexpr int kPhase1 = P + 1;  // gg and a_k
   static constexpr int kMaxChunks = 2;   // 16-column chunks per warp and tile
-  using Params = std::conditional_t<GLM, GlmEpiParams<P>, LmmEpiParams<P>>;
+  using Params = std::conditional_t<GLM, GlmEpiParams<P>,
+                                    std::conditional_t<RAW, LmmRawEpiParams<P>, LmmEpiParams<P>>>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
   float* tsm;
@@ -804,15 +916,17 @@ struct LmmEpi {
   // error already); printed statistics come from the FP64 refinement.
   // Phase 1: v = [gg, a_0 .. a_{P-1}] of 16 pairs.
   template <int N>
-  __device__ void pre_chunk(int ci, int, const float (&v)[N][16]) {
+  __device__ void pre_chunk(int ci, int c, const float (&v)[N][16]) {
     static_assert(N == P + 1, "phase-1 accumulators");
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const float gg = v[0][j] * u[P + 1];
       float S = gg;
       float a[P];
+      float us = 1.0f;  // RAW: alpha of the SNP
+      if constexpr (RAW) us = __ldg(Pr.snp_alpha + snp0 + c + j);
 #pragma unroll
-      for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * u[1 + k];
+      for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * (us * u[1 + k]);
 #pragma unroll
       for (int x = 0; x < P; ++x)
 #pragma unroll
@@ -835,7 +949,8 @@ struct LmmEpi {
     for (int j = 0; j < 16; ++j) {
       const int64_t s = s0 + j;
       const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
-      const float num = v[0][j] * u[0];
+      float num = v[0][j] * u[0];
+      if constexpr (RAW) num *= __ldg(Pr.snp_alpha + s);
       const float S = ci == 0 ? S0[j] : S1[j];
       float u;
       if constexpr (GLM) {
@@ -1166,7 +1281,7 @@ __global__ void lmm_wr_kernel(const double* __restrict__ Ytil, const double* __r
 }
 
 __global__ void lmm_tiny_kernel(GenoRows src, const int32_t* __restrict__ col, int n, int k_pad, const int64_t* __restrict__ kept, const double* __restrict__ mu,
-                                const double* __restrict__ U, const __half* __restrict__ gt_hi,
+                                const double* __restrict__ U, int64_t u_stride, const __half* __restrict__ gt_hi,
                                 const __half* __restrict__ gt_lo, double inv_s1, const double* __restrict__ Xtil,
                                 int p, const double* __restrict__ lam, const double* __restrict__ delta,
                                 const double* __restrict__ ainv, const double* __restrict__ rss, double df,
@@ -1178,7 +1293,7 @@ __global__ void lmm_tiny_kernel(GenoRows src, const int32_t* __restrict__ col, i
   const int64_t r = pairs[w].y;
   const int64_t s = kept[r];
   const double mus = mu[s];
-  const double* u = U + static_cast<int64_t>(g) * n;
+  const double* u = U + static_cast<int64_t>(g) * u_stride;
   const __half* gh = gt_hi + r * k_pad;
   const __half* gl = gt_lo + r * k_pad;
   const double d = delta[g];
@@ -1230,6 +1345,14 @@ struct EpiOf<dev::LmmEpiParams<1>> {
 template <>
 struct EpiOf<dev::LmmEpiParams<2>> {
   using type = dev::LmmEpi<2>;
+};
+template <>
+struct EpiOf<dev::LmmRawEpiParams<1>> {
+  using type = dev::LmmEpi<1, false, true>;
+};
+template <>
+struct EpiOf<dev::LmmRawEpiParams<2>> {
+  using type = dev::LmmEpi<2, false, true>;
 };
 template <>
 struct EpiOf<dev::LmmGroupEpiParams> {
@@ -1403,6 +1526,15 @@ void lmm_rotate(eqtl_ctx* ctx) {
     const int bsel[1] = {0}, prod[1] = {7};
     launch_tile_n<256, 1>(ctx, false, ep, ah, al, n, bh, bl, m, k_pad, bsel, prod);
   }
+  if (ctx->precision == EQTL_PREC_FP32_SIMT && m > 0) {
+    // the FP32 form keeps its SNP-side operands in FP32
+    R.gt32.alloc(elems);
+    R.gt2_32.alloc(elems);
+    ctx->launches += 2;
+    sum_split_kernel<<<1184, 256, 0, st>>>(R.gt_hi.p, R.gt_lo.p, static_cast<int64_t>(elems), R.gt32.p);
+    sum_split_kernel<<<1184, 256, 0, st>>>(R.gt2_hi.p, R.gt2_lo.p, static_cast<int64_t>(elems), R.gt2_32.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
   R.m = m;
   R.k_pad = k_pad;
 }
@@ -1565,8 +1697,11 @@ static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __ha
 template <int P, class EP>
 static void lmm_launch(eqtl_ctx* ctx, const EP& ep, const __half* const* ah, const __half* const* al, int G,
                        bool simt, const int2* tiles, int n_tiles, const Rotated& R) {
-  const __half* bh[2] = {R.gt_hi.p, R.gt2_hi.p};
-  const __half* bl[2] = {R.gt_lo.p, R.gt2_lo.p};
+  // the exact-operand form reads the raw SNP operand (one exact FP16 slice:
+  // hi*hi + lo*hi) for NUM and a_k, and Gt^2 for gg as both forms do
+  constexpr bool raw = std::is_same_v<EP, LmmRawEpiParams<P>>;
+  const __half* bh[2] = {raw ? R.raw.p : R.gt_hi.p, R.gt2_hi.p};
+  const __half* bl[2] = {raw ? R.raw.p : R.gt_lo.p, R.gt2_lo.p};
   // tile order [gg, a_0 .. a_{P-1}, NUM] from the gene-ops order [NUM, a.., gg]
   const __half* oh[P + 2];
   const __half* ol[P + 2];
@@ -1576,7 +1711,7 @@ static void lmm_launch(eqtl_ctx* ctx, const EP& ep, const __half* const* ah, con
     oh[j] = ah[op];
     ol[j] = al[op];
     bsel[j] = j == 0 ? 1 : 0;  // gg reads Gt^2
-    prod[j] = 7;
+    prod[j] = raw && j > 0 ? 5 : 7;
   }
   ah = oh;
   al = ol;
@@ -1588,28 +1723,24 @@ static void lmm_launch(eqtl_ctx* ctx, const EP& ep, const __half* const* ah, con
 }
 
 // the plain FP32 CUDA-core comparator of the LMM scan
+// The FP32 operands (ws.ops32 in tile order, Rotated::gt32 / gt2_32) are
+// formed before the scan; accumulator 0 (gg) reads Gt^2, the others Gt.
 template <int P>
-static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah,
-                            const __half* const* al, int G, const __half* const* bh, const __half* const* bl,
-                            const int* bsel, const Rotated& R) {
+static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const*, const __half* const*,
+                            int G, const __half* const*, const __half* const*, const int* bsel, const Rotated& R) {
   cudaStream_t st = ctx->stream;
-  const __half* ptrs[2 * (P + 2) + 4];
-  for (int j = 0; j < P + 2; ++j) {
-    ptrs[j] = ah[j];
-    ptrs[P + 2 + j] = al[j];
-  }
-  ptrs[2 * (P + 2) + 0] = bh[0];
-  ptrs[2 * (P + 2) + 1] = bh[1];
-  ptrs[2 * (P + 2) + 2] = bl[0];
-  ptrs[2 * (P + 2) + 3] = bl[1];
-  DevBuf<const __half*> dptr;
-  dptr.upload(ptrs, 2 * (P + 2) + 4, st);
+  EQTL_CHECK(bsel[0] == 1 && R.gt32.p && R.gt2_32.p, EQTL_E_INTERNAL, "FP32 comparator operands");
+  const float* ptrs[P + 2];
+  for (int j = 0; j < P + 2; ++j) ptrs[j] = ctx->ws.ops32[j].p;
+  DevBuf<const float*>& dptr = ctx->ws.ops32_ptr;
+  dptr.upload(ptrs, P + 2, st);
   TileShape sh{};
-  const int4 bs = make_int4(bsel[0], P + 2 > 1 ? bsel[1] : 0, P + 2 > 2 ? bsel[2] : 0, P + 2 > 3 ? bsel[3] : 0);
-  dim3 grid(static_cast<unsigned>((R.m + kSimtN - 1) / kSimtN), static_cast<unsigned>((G + 127) / 128));
+  using Cfg = SimtCfg<P + 2>;
+  auto kern = simt_tile_kernel<P + 2, LmmEpi<P>>;
+  EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM_BYTES));
+  dim3 grid(static_cast<unsigned>((R.m + kSimtBN - 1) / kSimtBN), static_cast<unsigned>((G + kSimtBM - 1) / kSimtBM));
   ++ctx->launches;
-  simt_tile_kernel<P + 2, LmmEpi<P>><<<grid, 128, 0, st>>>(dptr.p, dptr.p + (P + 2), G, dptr.p + 2 * (P + 2),
-                                                           dptr.p + 2 * (P + 2) + 2, R.m, R.k_pad, bs, sh, ep);
+  kern<<<grid, kSimtThreads, Cfg::SMEM_BYTES, st>>>(dptr.p, G, R.gt32.p, R.gt2_32.p, R.m, R.k_pad, sh, ep);
   EQTL_CUDA(cudaGetLastError());
   EQTL_CUDA(cudaStreamSynchronize(st));
 }
@@ -1671,7 +1802,10 @@ static std::vector<eqtl_pair> lmm_refine_pairs(eqtl_ctx* ctx, int p, double df, 
 }
 
 // FP64 p of tiny-|t| pairs against the current LMM prep (see lmm_tiny_kernel).
-static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std::vector<int2>& tiny) {
+// U_pre (optional): u = Q (w o r~) of gene g at U_pre + g * u_stride, as the
+// exact-operand scan has it already; otherwise it is computed here.
+static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std::vector<int2>& tiny,
+                                      const double* U_pre = nullptr, int64_t u_stride = 0) {
   Geno& g = ctx->geno;
   Workspace& ws = ctx->ws;
   Rotated& R = ctx->rot;
@@ -1680,22 +1814,28 @@ static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std
   const int G = static_cast<int>(ws.delta.n);
   std::vector<double> out(tiny.size());
   if (tiny.empty()) return out;
-  ws.graw.alloc(static_cast<size_t>(n) * G);  // w o r~ per gene
-  ws.gt.alloc(static_cast<size_t>(n) * G);    // u = Q (w o r~)
-  ctx->launches += 2;
-  lmm_wr_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
-                                   ws.graw.p);
-  EQTL_CUDA(cudaGetLastError());
-  const double one = 1.0, zero = 0.0;
-  EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ws.graw.p, n,
-                         &zero, ws.gt.p, n) == CUBLAS_STATUS_SUCCESS,
-             EQTL_E_CUDA, "Q (w o r) failed");
+  const double* U = U_pre;
+  if (!U) {
+    ws.graw.alloc(static_cast<size_t>(n) * G);  // w o r~ per gene
+    ws.gt.alloc(static_cast<size_t>(n) * G);    // u = Q (w o r~)
+    ctx->launches += 1;
+    lmm_wr_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
+                                     ws.graw.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, G, n, &one, ctx->basis.Q.p, n, ws.graw.p, n,
+                           &zero, ws.gt.p, n) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "Q (w o r) failed");
+    U = ws.gt.p;
+    u_stride = n;
+  }
+  ctx->launches += 1;
   float s1, s2;
   output_scales(n, s1, s2);
   ws.ref_pairs.upload(tiny.data(), tiny.size(), st);
   ws.tiny_p.alloc(tiny.size());
   lmm_tiny_kernel<<<static_cast<unsigned>((tiny.size() + 7) / 8), 256, 0, st>>>(
-      g.rows(), g.col.p, n, R.k_pad, g.kept.p, g.mu.p, ws.gt.p, R.gt_hi.p, R.gt_lo.p, 1.0 / s1,
+      g.rows(), g.col.p, n, R.k_pad, g.kept.p, g.mu.p, U, u_stride, R.gt_hi.p, R.gt_lo.p, 1.0 / s1,
       ws.Xtil.p, p, ctx->basis.lambda.p, ws.delta.p, ws.ainv.p, ws.rss.p, df, ws.ref_pairs.p,
       static_cast<int>(tiny.size()), ws.tiny_p.p);
   EQTL_CUDA(cudaGetLastError());
@@ -1737,6 +1877,9 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   const double df = static_cast<double>(n - p - 1);
   const PhenoDev& ph = resolve_pheno(ctx, prm, Y, X);
   lmm_rotate(ctx);
+  // p <= 2 on the tensor cores: NUM and a_k from the exact unrotated SNP
+  // operand when every kept SNP fits it (2-bit rows, FP16 operands)
+  const bool raw = !grouped && !simt && ctx->precision == EQTL_PREC_SPLIT_F16 && geno_raw_operand(ctx);
   std::unique_ptr<StageScope> prep_timer(new StageScope(ctx, EQTL_STAGE_PREP));
   lmm_prep(ctx, ph, prm->y_rotated != 0);
 
@@ -1756,14 +1899,42 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   DevBuf<float>& unscale = ws.unscale;
   unscale.alloc(static_cast<size_t>(G) * nops);
   ++ctx->launches;
-  if (grouped)
+  if (raw) {
+    // u = Q (w o r~) and v_k = Q (w o X~_k) in FP64, then their FP16 hi/lo
+    const size_t cols = static_cast<size_t>(G) * (p + 1);
+    ws.lmm_w.alloc(static_cast<size_t>(n) * cols);
+    ws.lmm_uv.alloc(static_cast<size_t>(n) * cols);
+    lmm_uv_w_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
+                                       ws.lmm_w.p);
+    EQTL_CUDA(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, static_cast<int>(cols), n, &one,
+                           ctx->basis.Q.p, n, ws.lmm_w.p, n, &zero, ws.lmm_uv.p, n) == CUBLAS_STATUS_SUCCESS,
+               EQTL_E_CUDA, "Q (w o [r~, X~]) failed");
+    ctx->launches += 1;
+    lmm_gene_ops_raw_kernel<<<G, 256, 0, st>>>(ws.lmm_uv.p, ctx->basis.lambda.p, ws.delta.p, n, p, G, k_pad, s2,
+                                               ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
+  } else if (grouped) {
     lmm_gene_ops_orth_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p,
                                                 ws.ainv.p, n, p, G, k_pad, s1, s2, ws.ops_ptr.p,
                                                 ws.ops_ptr.p + nops, unscale.p);
-  else
+  } else {
     lmm_gene_ops_kernel<<<G, 256, 0, st>>>(ws.Ytil.p, ws.Xtil.p, ctx->basis.lambda.p, ws.delta.p, ws.chi0.p, n, p, G,
                                            k_pad, s1, s2, ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
+  }
   EQTL_CUDA(cudaGetLastError());
+  if (simt) {
+    // the FP32 form's gene-side operands, in the tile's accumulator order
+    // [gg, a_0 .. a_{p-1}, NUM] (the gene-ops order is [NUM, a.., gg])
+    for (int j = 0; j < nops; ++j) {
+      const int op = j == 0 ? nops - 1 : (j == nops - 1 ? 0 : j);
+      ws.ops32[j].alloc(static_cast<size_t>(G) * k_pad);
+      ++ctx->launches;
+      sum_split_kernel<<<1184, 256, 0, st>>>(ws.ops_hi[op].p, ws.ops_lo[op].p, static_cast<int64_t>(G) * k_pad,
+                                             ws.ops32[j].p);
+    }
+    EQTL_CUDA(cudaGetLastError());
+  }
 
   const int64_t m = g.m;
   lmm_gate(ctx);
@@ -1815,21 +1986,21 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
       ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
       ep.tt = tt;
     };
-    if (p == 1) {
-      LmmEpiParams<1> ep{};
+    auto run = [&](auto ep, auto pc) {
+      constexpr int P = decltype(pc)::value;
       fill(ep);
+      ep.snp_alpha = ctx->rot.alpha.p;
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<1>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
+        lmm_launch<P>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
       });
-    } else {
-      LmmEpiParams<2> ep{};
-      fill(ep);
-      so.run([&](GeneOut out) {
-        ep.out = out;
-        lmm_launch<2>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
-      });
-    }
+    };
+    using P1 = std::integral_constant<int, 1>;
+    using P2 = std::integral_constant<int, 2>;
+    if (raw && p == 1) run(LmmRawEpiParams<1>{}, P1{});
+    else if (raw) run(LmmRawEpiParams<2>{}, P2{});
+    else if (p == 1) run(LmmEpiParams<1>{}, P1{});
+    else run(LmmEpiParams<2>{}, P2{});
   }
   scan_timer.reset();
   HostTrace tr("scan_trans_lmm");
@@ -1847,7 +2018,8 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
   tr.mark("refine pairs");
   add_deferred_acat(genes, refined, deferred);
   tr.mark("deferred ACAT");
-  const std::vector<double> tiny_p = lmm_tiny_p(ctx, p, df, tiny);
+  const std::vector<double> tiny_p =
+      raw ? lmm_tiny_p(ctx, p, df, tiny, ws.lmm_uv.p, static_cast<int64_t>(p + 1) * n) : lmm_tiny_p(ctx, p, df, tiny);
   tr.mark("tiny-|t| pairs");
   add_acat_terms(genes, tiny, tiny_p);
   tr.mark("tiny ACAT terms");

@@ -64,7 +64,7 @@ struct TileShape {
   int n_acc;              // accumulators per tile (NACC, or more in groups of NACC)
   int n_groups;           // ceil(n_acc / NACC): TMEM holds one group at a time
   int bsel[kMaxAcc];      // SNP-side pair used by accumulator j (0 or 1)
-  int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi
+  int prod[kMaxAcc];      // 1 = hi*hi, 2 = hi*lo, 4 = lo*hi (a lo part no product reads is not loaded)
   int tiles_a;            // ceil(rows_a / 128)
   int tiles_b;            // ceil(rows_b / NT)
   int n_tiles;            // work items: (tiles_a * tiles_b or the tile-list length) * ksplit
@@ -187,17 +187,22 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         const int ra = ta * kTileM, rb = tb * NT;
         for (int j = 0; j < sh.n_acc && ok; ++j) {
           const int bp = sh.bsel[j];
+          // only the lo parts some product of this accumulator reads are loaded
+          const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = (sh.prod[j] & 2) != 0;
+          const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
+                                                       (b_lo ? C::B_BYTES : 0));
           for (int kc = k0; kc < k1; ++kc) {
             if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
               ok = false;
               break;
             }
             uint8_t* sb = smem + stage * C::STAGE_BYTES;
-            mbar_arrive_expect_tx(&full[stage], C::STAGE_BYTES);
+            mbar_arrive_expect_tx(&full[stage], bytes);
             tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
-            tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
+            if (a_lo) tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
             tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[2 * bp], &full[stage], kc * kChunkK, rb);
-            tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
+            if (b_lo)
+              tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
             issued[stage] = true;
             issued_phase[stage] = phase;
             if (++stage == C::STAGES) {
