@@ -258,6 +258,10 @@ struct EpiOf<dev::GrmEpiParams> {
   using type = dev::GrmEpi;
 };
 
+// K chunks (of 64 SNPs) summed in one FP32 tensor-core accumulator before
+// the FP64 sum across ranges.
+constexpr int kGrmChunksPerRange = 8;
+
 // Computes the GRM of the loaded genotypes. K: device [n, n] (row-major ==
 // column-major, symmetric). Returns the number of SNPs used.
 int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
@@ -343,7 +347,14 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
       if (128 * ta + 127 >= 256 * tb) lower.push_back(make_int2(ta, tb));
   ws.grm_tiles.upload(lower.data(), lower.size(), st);
   const int tiles = static_cast<int>(lower.size());
-  const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
+  // The tensor cores' FP32 accumulation drifts with the number of K steps
+  // summed into one accumulator (about 2.6e-7 of the running sum per step,
+  // the same sign for the large positive sums of K's diagonal and of
+  // related pairs), so a K range holds at most kGrmChunksPerRange chunks
+  // of 64 SNPs; the ranges meet in FP64.
+  const int kchunks = static_cast<int>(m_pad / 64);
+  const int ksplit = std::max({1, (4 * sm_count(ctx) + tiles - 1) / tiles,
+                               (kchunks + kGrmChunksPerRange - 1) / kGrmChunksPerRange});
   // the GRM operands are FP16 regardless of the scan precision
   launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, ws.grm_tiles.p,
                         tiles, ksplit);
@@ -612,7 +623,8 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
     for (int ta = 0; ta < (n + 127) / 128; ++ta)
       if (128 * ta + 127 >= 256 * tb) lower[tiles++] = make_int2(ta, tb);
   EQTL_CUDA(cudaMemcpyAsync(tile_list, lower, sizeof(int2) * tiles, cudaMemcpyHostToDevice, st));
-  const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
+  const int ksplit = std::max({1, (4 * sm_count(ctx) + tiles - 1) / tiles,
+                               (kNaChunk / 64 + kGrmChunksPerRange - 1) / kGrmChunksPerRange});
   for (int64_t r0 = 0; r0 < m; r0 += kNaChunk) {
     const int nr = static_cast<int>(std::min<int64_t>(kNaChunk, m - r0));
     ctx->launches += 2;

@@ -1,6 +1,15 @@
 """Throughput of the cis permutation path through the eqtl program.
 
     python -m eqtl_b200.perm_bench [--genes G] [--perm B] [--models lmm,lm]
+    python -m eqtl_b200.perm_bench --lognormal --genes 20000 --perm 1000 --models lmm
+
+--lognormal gives the cis-LMM permutation benchmark's shape: 10 chromosomes
+of 50 Mb whose SNP density is constant within each 2 Mb segment and drawn
+lognormal across segments (median 1,500 per Mb, sd 0.9 on the log scale,
+clamped to 25 - 7,500 per Mb), so that the +-1 Mb cis windows hold a
+lognormal number of SNPs (median about 3,000, from about 50 to 15,000);
+genes have uniform TSS over the genome. The realised window sizes are
+reported (percentiles).
 
 Seeded synthetic data with the shape of the cis-LMM permutation workload:
 n = 1,000 samples (25 families of 10 siblings + 750 unrelated), 3 chromosomes
@@ -63,15 +72,60 @@ def make_case(d: str, genes: int, n: int = 1000, n_chrom: int = 3, chrom_mb: int
     return m
 
 
+def make_case_lognormal(d: str, genes: int, n: int = 1000, n_chrom: int = 10, chrom_mb: int = 50,
+                        n_cov: int = 15) -> int:
+    rng = np.random.default_rng(20261207)
+    seg_mb = 2
+    nseg = chrom_mb // seg_mb
+    dens = np.clip(np.exp(np.log(1500.0) + 0.9 * rng.standard_normal((n_chrom, nseg))), 25, 7500)
+    chrom, pos = [], []
+    for c in range(n_chrom):
+        for k in range(nseg):
+            cnt = int(round(dens[c, k] * seg_mb))
+            lo = k * seg_mb * 1_000_000 + 1
+            p = np.sort(rng.choice(np.arange(lo, lo + seg_mb * 1_000_000), size=cnt, replace=False))
+            chrom += [str(c + 1)] * cnt
+            pos.append(p)
+    pos = np.concatenate(pos)
+    m = pos.size
+    fam = (25, 10, n - 250)
+    rows, sub, _ = synth.make_bed_rows_chunked(4243, n, m, family=fam, keep_codes_every=50)
+    samples = [f"S{i + 1:05d}" for i in range(n)]
+    pre = os.path.join(d, "geno")
+    with open(pre + ".fam", "w") as f:
+        for s in samples:
+            f.write(f"{s} {s} 0 0 0 -9\n")
+    with open(pre + ".bim", "w") as f:
+        f.write("".join(f"{chrom[i]}\trs{i + 1}\t0\t{int(pos[i])}\tA\tG\n" for i in range(m)))
+    with open(pre + ".bed", "wb") as f:
+        f.write(bytes([0x6C, 0x1B, 0x01]))
+        f.write(rows.tobytes())
+    Y, _ = synth.polygenic_pheno(12, sub, genes)
+    C = rng.standard_normal((n, n_cov))
+    Y += 0.5 * C.sum(1, keepdims=True)
+    ids, gc, st, en, sd, _ = synth.make_genes(6, genes, [str(c + 1) for c in range(n_chrom)],
+                                              chrom_mb * 1_000_000, body=1)
+    with open(os.path.join(d, "pheno.tsv"), "w") as f:  # 9 significant digits: the tables stay a few hundred MB
+        f.write("sample\t" + "\t".join(ids) + "\n")
+        for i, smp in enumerate(samples):
+            f.write(smp + "\t" + "\t".join(f"{v:.9g}" for v in Y[i]) + "\n")
+    synth.write_covar(os.path.join(d, "covar.tsv"), samples, C)
+    synth.write_gff(os.path.join(d, "genes.gff"), ids, gc, st, en, sd)
+    return m
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--genes", type=int, default=100)
     ap.add_argument("--perm", type=int, default=1000)
     ap.add_argument("--models", default="lmm,lm")
+    ap.add_argument("--lognormal", action="store_true", help="lognormal cis-window sizes (see above)")
     args = ap.parse_args()
     exe = os.path.join(PKG, "bin", "eqtl")
     with tempfile.TemporaryDirectory(prefix="eqtl_perm_") as d:
-        m = make_case(d, args.genes)
+        t_gen = time.perf_counter()
+        m = make_case_lognormal(d, args.genes) if args.lognormal else make_case(d, args.genes)
+        t_gen = time.perf_counter() - t_gen
         for model in args.models.split(","):
             cmd = [exe, "-b", os.path.join(d, "geno"), "-e", os.path.join(d, "pheno.tsv"), "-g",
                    os.path.join(d, "genes.gff"), "-c", os.path.join(d, "covar.tsv"), "--model", model, "--mode",
@@ -95,14 +149,30 @@ def main() -> None:
                 if mt:
                     perm_cols += int(mt.group(1))
                     perm_ms += float(mt.group(2))
-            tested = 0
+            win = []
             with open(os.path.join(d, f"out.{model}.cis.region.tsv")) as f:
                 next(f)
                 for ln in f:
-                    tested += int(ln.split("\t")[3])
+                    win.append(int(ln.split("\t")[3]))
+            win = np.array(win)
+            # host-side phases of the permutation driver (EQTL_TRACE): time since
+            # the previous mark, summed over the batches
+            host = {}
+            kinds = (("columns ready", "wait for host-built columns"), ("device scan", "device scans"),
+                     ("p_emp", "p_emp and beta fits"), ("setup", "setup"))
+            for ln in r.stderr.splitlines():
+                mt = re.match(r"\[eqtl trace\] permutations: (.*) ([\d.]+) ms$", ln)
+                if mt:
+                    for key, name in kinds:
+                        if key in mt.group(1):
+                            host[name] = host.get(name, 0.0) + float(mt.group(2))
             print(json.dumps({"workload": "cis permutations", "model": model, "n_samples": 1000, "n_snps": m,
                               "genes": args.genes, "perm": args.perm, "covariates": 15,
-                              "window_snps_mean": tested / max(args.genes, 1), "wall_s": wall,
+                              "window_snps_mean": float(win.mean()) if win.size else 0.0,
+                              "window_snps_percentiles": {q: int(np.percentile(win, q)) for q in (0, 5, 50, 95, 100)}
+                              if win.size else {},
+                              "tests_observed": int(win.sum()), "generate_s": t_gen, "wall_s": wall,
+                              "trace_ms": host,
                               "perm_columns": perm_cols, "perm_device_call_ms": perm_ms,
                               "perm_stage_ms": stages,
                               "perm_columns_per_s": perm_cols / (perm_ms / 1e3) if perm_ms else None}))

@@ -21,7 +21,10 @@ that do not depend on size, since the oracle cannot run 5e9 or 2e10 tests:
 
 A GRM at the GRM benchmark's shape (n = 2,000 with the family structure,
 m = 200,000 SNPs) is checked against the oracle's FP64 GRM: N counts
-bit-exact, K within 2e-6 of its largest entry."""
+bit-exact, K within 5e-6 of its largest entry. K's large positive sums (its
+diagonal and related pairs) carry the drift of the tensor cores' FP32
+accumulation over one K range of 512 SNPs (about 3e-6 relative); the
+ranges meet in FP64."""
 import argparse
 import os
 import sys
@@ -215,4 +218,4 @@ def test_grm_full_size():
     Kr, Nr, mr = R.compute_grm(dec.dosage, dec.codes < 0)
     assert m_used == mr
     np.testing.assert_array_equal(N, Nr)
-    np.testing.assert_allclose(K, Kr, rtol=0, atol=2e-6 * np.abs(Kr).max())
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=5e-6 * np.abs(Kr).max())
