@@ -354,6 +354,8 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df, bool normal) {
   t.c1 = ws.tt_c1.p;
   t.lt = ws.tt_lt.p;
   t.dl_inv = static_cast<float>(T.nb / (T.x_defer - T.x0));
+  t.lt_u = T.lt_u ? 1 : 0;
+  t.dlu_inv = T.lt_u ? static_cast<float>(1.0 / T.du_t) : 0.0f;
   // round t_defer down so that every pair with p <= 1e-14 is deferred
   t.t_defer = static_cast<float>(T.t_defer * (1.0 - 1e-6));
   t.u0 = static_cast<float>(T.t0 * T.t0);

@@ -39,9 +39,11 @@ struct GeneAcc {
   int used = 0;
   int tested = 0;
   unsigned long long best = ~0ull;
-  // FP32 sum of the ACAT terms of the current chunk of add_screen pairs
-  // (end_chunk folds it into acat)
+  // FP32 sum of the ACAT terms of the current chunk of add_screen pairs, and
+  // its best key and SNP (end_chunk folds them into acat and best)
   float chunk_acat = 0.0f;
+  float chunk_key = -1.0f;
+  uint32_t chunk_snp = 0;
   int chrom = -1;
   int64_t lo = 0, hi = -1;
 
@@ -51,6 +53,7 @@ struct GeneAcc {
     tested = 0;
     best = ~0ull;
     chunk_acat = 0.0f;
+    chunk_key = -1.0f;
   }
   __device__ __forceinline__ void load_window(const Windows& w, int g) {
     if (w.mode != kWinNone) {
@@ -84,6 +87,9 @@ struct GeneAcc {
   // key, t^2 in the scans). Pairs come in chunks of up to 16 SNPs; the terms
   // of a chunk are summed in FP32 (the error is ~1e-6 of the chunk's largest
   // term, below the screen's own) and added to the FP64 total by end_chunk.
+  // A chunk's pairs come in increasing SNP order, so its best is the first
+  // pair with the largest key (strict >), and the 64-bit key that breaks ties
+  // by SNP index across chunks is formed once per chunk.
   __device__ __forceinline__ void add_screen(const ScreenOut& o, int64_t s, bool valid) {
     if (valid) {
       ++tested;
@@ -91,13 +97,20 @@ struct GeneAcc {
         chunk_acat += o.term;
         ++used;
       }
-      const unsigned long long k = best_key(o.key, static_cast<uint32_t>(s));
-      best = k < best ? k : best;
+      if (o.key > chunk_key) {
+        chunk_key = o.key;
+        chunk_snp = static_cast<uint32_t>(s);
+      }
     }
   }
   __device__ __forceinline__ void end_chunk() {
     acat += static_cast<double>(chunk_acat);
     chunk_acat = 0.0f;
+    if (chunk_key >= 0.0f) {
+      const unsigned long long k = best_key(chunk_key, chunk_snp);
+      best = k < best ? k : best;
+      chunk_key = -1.0f;
+    }
   }
   __device__ __forceinline__ void add(const TailOut& o, int64_t s) {
     ++tested;

@@ -38,6 +38,8 @@ struct TTable {
   const float* c1;  // na + 4 nodes
   const float* lt;  // nb + 4 nodes
   float dl_inv;     // nb / (x(t_defer) - x0)
+  int lt_u;         // 1: lt holds the term itself on u in [u0, u_defer] (dlu_inv = nb / that range)
+  float dlu_inv;
   float t_defer;    // |t| >= t_defer (p <= 1e-14): the term is left to the host
   // the same thresholds on u = t^2 (the scan epilogues screen t^2 directly)
   float u0;         // t0^2
@@ -127,7 +129,8 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
 // deferral for p <= 1e-14 is u >= u_defer, for |t| near 0 0 < u < u_tiny.
 // One table lookup:
 //   central  tan((1/2 - p) pi) = c1(u) / |t| = c1(u) rsqrt(u)
-//   tail     tan((1/2 - p) pi) = exp(lt(sqrt(log1p(u / df))))
+//   tail     tan((1/2 - p) pi) = lt(u)                      (T.lt_u, short tails)
+//            tan((1/2 - p) pi) = exp(lt(sqrt(log1p(u / df))))  (otherwise)
 struct ScreenOut {
   float term;     // tan((1/2 - p) pi) when use_acat, else 0
   float key;      // best-SNP score: u for the scans (|t| through acat_screen); 0 for NaN
@@ -145,10 +148,17 @@ __device__ __forceinline__ ScreenOut acat_screen_u(float u, const TTable& T) {
   o.use_acat = !nan_u && !o.deferred && u > 0.0f;
   o.key = nan_u ? 0.0f : u;
   const bool central = u <= T.u0;
-  const float xs = sqrtf(log1pf(u * T.inv_df));
-  const float x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
-  const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
-  const float term = central ? y * rsqrtf(u) : __expf(y);
+  float x, term;
+  if (T.lt_u) {  // uniform across the launch
+    x = central ? u * T.du_inv : (u - T.u0) * T.dlu_inv;
+    const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
+    term = central ? y * rsqrtf(u) : y;
+  } else {
+    const float xs = sqrtf(log1pf(u * T.inv_df));
+    x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
+    const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
+    term = central ? y * rsqrtf(u) : __expf(y);
+  }
   o.term = o.use_acat ? term : 0.0f;
   return o;
 }

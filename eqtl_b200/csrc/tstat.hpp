@@ -64,7 +64,10 @@ struct TTableHost {
   double x0 = 0, x_end = 0;
   // ACAT screening tables of the scan epilogues (tdist.cuh, acat_screen):
   std::vector<float> c1;   // na + 4 nodes on the central u grid: |t| * tan((1/2 - p) pi)
-  std::vector<float> lt;   // nb + 4 nodes on x in [x0, x_defer]: ln tan((1/2 - p) pi)
+  std::vector<float> lt;   // nb + 4 nodes on x in [x0, x_defer]: ln tan((1/2 - p) pi); with lt_u, the
+                           // term tan((1/2 - p) pi) itself on u = t^2 in [t0^2, t_defer^2]
+  bool lt_u = false;       // the tail table is linear in u (short tails: df large enough, or normal)
+  double du_t = 0;         // its u step
   double x_defer = 0;      // tail grid end: x at p = 1e-14
   double t_defer = 0;      // |t| with p = 1e-14: beyond it the term is left to the host
   std::vector<float> h;          // na + 4 nodes: h(u) = (1 - p) / |t|, node k at u = (k-1) du
@@ -201,8 +204,24 @@ inline TTableHost build_ttable(double df, bool normal = false) {
   }
   T.t_defer = normal ? z_critical(1e-14) : t_critical(1e-14, df);
   T.x_defer = std::sqrt(std::log1p(T.t_defer * T.t_defer / df));
-  const double dl = (T.x_defer - T.x0) / T.nb;
   T.lt.resize(T.nb + 4);
+  // Where the tail up to p = 1e-14 is short in u (t_defer^2 within ~200 of
+  // t0^2: df above ~30, and the normal tail), the term itself is smooth
+  // enough in u for the cubic (it grows about as exp(u / 2), 0.05 per step
+  // at most), and the epilogue's grid position is one FMA of u; longer
+  // tails keep the x grid of ln tan((1/2 - p) pi).
+  const double du_t = (T.t_defer * T.t_defer - T.t0 * T.t0) / T.nb;
+  if (du_t <= 0.05) {
+    T.lt_u = true;
+    T.du_t = du_t;
+    for (int k = 0; k < T.nb + 4; ++k) {
+      const double u = T.t0 * T.t0 + (k - 1) * du_t;
+      const double p = pfun(std::sqrt(u));
+      T.lt[k] = static_cast<float>(std::cos(M_PI * p) / std::sin(M_PI * p));
+    }
+    return T;
+  }
+  const double dl = (T.x_defer - T.x0) / T.nb;
   for (int k = 0; k < T.nb + 4; ++k) {
     const double x = T.x0 + (k - 1) * dl;
     const double t = std::sqrt(df * std::expm1(x * x));

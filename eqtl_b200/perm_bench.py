@@ -120,6 +120,10 @@ def main() -> None:
     ap.add_argument("--perm", type=int, default=1000)
     ap.add_argument("--models", default="lmm,lm")
     ap.add_argument("--lognormal", action="store_true", help="lognormal cis-window sizes (see above)")
+    ap.add_argument("--reference", type=int, nargs=2, metavar=("GENES", "PERM"),
+                    help="also time the reference program (oracle/_ref/eqtl, all host threads) on GENES genes "
+                         "of median window size with --perm PERM and extrapolate to the workload by the "
+                         "window sizes and permutation count")
     args = ap.parse_args()
     exe = os.path.join(PKG, "bin", "eqtl")
     with tempfile.TemporaryDirectory(prefix="eqtl_perm_") as d:
@@ -176,6 +180,46 @@ def main() -> None:
                               "perm_columns": perm_cols, "perm_device_call_ms": perm_ms,
                               "perm_stage_ms": stages,
                               "perm_columns_per_s": perm_cols / (perm_ms / 1e3) if perm_ms else None}))
+            if args.reference:
+                print(json.dumps(reference_estimate(d, model, win, args.reference[0], args.reference[1],
+                                                    args.perm)), flush=True)
+
+
+def reference_estimate(d: str, model: str, win: np.ndarray, k: int, perm: int, perm_full: int) -> dict:
+    """The reference program on the k genes whose windows are closest to the
+    median, with --perm perm and without permutations; the difference per
+    (window SNP, permutation) scaled by the workload's sum of window sizes
+    and its permutation count."""
+    exe = os.path.join(os.path.dirname(PKG), "oracle", "_ref", "eqtl")
+    if not os.path.exists(exe):
+        return {"reference": "oracle/_ref/eqtl not built"}
+    with open(os.path.join(d, "pheno.tsv")) as f:
+        head = f.readline().rstrip("\n").split("\t")
+        rows = [ln.rstrip("\n").split("\t") for ln in f]
+    # region rows follow the phenotype table's gene order (-t 1 below)
+    pick = np.argsort(np.abs(win - np.median(win)), kind="stable")[:k]
+    cols = [0] + [1 + int(i) for i in sorted(pick)]
+    sub = os.path.join(d, "pheno_ref.tsv")
+    with open(sub, "w") as f:
+        f.write("\t".join(head[c] for c in cols) + "\n")
+        for r in rows:
+            f.write("\t".join(r[c] for c in cols) + "\n")
+    threads = str(os.cpu_count() or 1)
+    times = {}
+    for b in (0, perm):
+        cmd = [exe, "-b", os.path.join(d, "geno"), "-e", sub, "-g", os.path.join(d, "genes.gff"), "-c",
+               os.path.join(d, "covar.tsv"), "--model", model, "--mode", "cis", "-w", "1000000", "--perm", str(b),
+               "-t", threads, "-o", os.path.join(d, "ref")]
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        times[b] = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"reference": "failed: " + r.stderr[-500:]}
+    snps = float(win[pick].sum())
+    per = (times[perm] - times[0]) / (snps * perm)
+    return {"reference": "oracle/_ref/eqtl", "model": model, "threads": int(threads), "genes": k, "perm": perm,
+            "window_snps": snps, "wall_s_no_perm": times[0], "wall_s_perm": times[perm],
+            "s_per_window_snp_perm": per, "estimate_s_full": per * float(win.sum()) * perm_full}
 
 
 if __name__ == "__main__":
