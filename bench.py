@@ -355,8 +355,15 @@ def b200_arm(args, rank, world, local_rank):
         ctx32.lmm_basis()
         run_value_step(ctx32)
         s32 = ctx32.stage_ms("scan")
+        # FP32 CUDA-core peak at the clock sampled during the timed region:
+        # 148 SMs x 128 FP32 lanes x 2 flops per FMA
+        mhz = out["clocks"].get("sm_mhz") or 1965.0
+        fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
         out["fp32_simt"] = {"scan_ms": s32, "tests_per_s_scan": tests / (s32 / 1e3),
-                            "tensor_speedup": s32 / scan_ms}
+                            "tensor_speedup": s32 / scan_ms,
+                            "algorithmic_tflops": flops / (s32 / 1e3) / 1e12,
+                            "fp32_peak_tflops_at_sampled_clock": fp32_peak,
+                            "frac_of_fp32_peak": flops / (s32 / 1e3) / 1e12 / fp32_peak}
         ctx32.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, rows, Y)
