@@ -26,7 +26,7 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
            "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
-           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast"]
+           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast", "eqtl_pheno_permute"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -91,6 +91,7 @@ def load() -> C.CDLL:
         lib.eqtl_lmm_rotate.argtypes = [vp]
         lib.eqtl_stream.argtypes = [vp, C.POINTER(vp)]
         lib.eqtl_pheno_load.argtypes = [vp, vp, vp, i32, i32, i32]
+        lib.eqtl_pheno_permute.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32, C.c_uint64, vp, i32, vp]
         lib.eqtl_t_tail.argtypes = [vp, dp, vp, i64, i32, vp, vp, vp]
         lib.eqtl_lmm_basis.argtypes = [vp, vp, i32, vp, vp]
         lib.eqtl_lmm_set_basis.argtypes = [vp, vp, vp, i32]
@@ -231,7 +232,29 @@ class Context:
         self._check(self.lib.eqtl_pheno_load(self.h, _ptr(Y), _ptr(X), Y.shape[0], Y.shape[1], X.shape[1]))
         self.pheno_shape = (Y.shape[0], Y.shape[1], X.shape[1])
 
-    def _scan(self, fn, Y, X, pthr, perm_thr, windows, extra=()):
+    def pheno_permute(self, base, X, gene_key, n_perm: int, seed: int, xb0=None, dinv=None, out: bool = False):
+        """eqtl_pheno_permute: the resident phenotypes become n_perm device-drawn
+        permutations of each gene's base vector (base, xb0, dinv [n, G]; LMM form
+        when xb0 and dinv are given); returns the columns [n, G * n_perm] when
+        out is True."""
+        base = np.asfortranarray(base, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        n, G = base.shape
+        if (xb0 is None) != (dinv is None):
+            raise ValueError("give both xb0 and dinv, or neither")
+        if xb0 is not None:
+            xb0 = np.asfortranarray(xb0, dtype=np.float64)
+            dinv = np.asfortranarray(dinv, dtype=np.float64)
+            assert xb0.shape == base.shape and dinv.shape == base.shape
+        keys = np.ascontiguousarray(gene_key, np.uint64)
+        assert keys.size == G
+        Y = np.zeros((n, G * n_perm), np.float64, order="F") if out else None
+        self._check(self.lib.eqtl_pheno_permute(self.h, _ptr(base), _ptr(xb0), _ptr(dinv), _ptr(keys), n, G, n_perm,
+                                                C.c_uint64(seed), _ptr(X), X.shape[1], _ptr(Y)))
+        self.pheno_shape = (n, G * n_perm, X.shape[1])
+        return Y
+
+    def _scan(self, fn, Y, X, pthr, perm_thr, windows, extra=(), rotated=False):
         if Y is None:
             n, G, p = self.pheno_shape        # resident phenotypes
         else:
@@ -239,6 +262,7 @@ class Context:
             X = np.asfortranarray(X, dtype=np.float64)   # [n, p]
             (n, G), p = Y.shape, X.shape[1]
         prm, keep = self._params(n, G, p, pthr, perm_thr, windows)
+        prm.y_rotated = 1 if rotated else 0
         genes = np.zeros(G, GENE_DTYPE)
         cap = 1 << 16
         while True:
@@ -346,9 +370,10 @@ class Context:
                                          extra=(_ptr(phi), _ptr(conv)))
         return genes, pairs, cands, phi, conv.astype(bool)
 
-    def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None):
-        """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta)."""
+    def scan_trans_lmm(self, Y, X, pthr, perm_thr=0.0, windows=None, rotated=False):
+        """eqtl_scan_trans_lmm -> (genes, pairs, cands, delta); rotated: the
+        columns are already in the eigenbasis (y_rotated)."""
         delta = np.zeros(self.pheno_shape[1] if Y is None else np.asarray(Y).shape[1], np.float64)
         genes, pairs, cands = self._scan(self.lib.eqtl_scan_trans_lmm, Y, X, pthr, perm_thr, windows,
-                                         extra=(_ptr(delta),))
+                                         extra=(_ptr(delta),), rotated=rotated)
         return genes, pairs, cands, delta

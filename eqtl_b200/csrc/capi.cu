@@ -333,6 +333,8 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df, bool normal) {
     ws.tt_L.upload(T.L.data(), T.L.size(), ctx->stream);
     ws.tt_c1.upload(T.c1.data(), T.c1.size(), ctx->stream);
     ws.tt_lt.upload(T.lt.data(), T.lt.size(), ctx->stream);
+    ws.tt_c1q.upload(T.c1q.data(), T.c1q.size(), ctx->stream);
+    ws.tt_ltq.upload(T.ltq.data(), T.ltq.size(), ctx->stream);
     ws.tt_df = key;
   }
   dev::TTable t{};
@@ -356,6 +358,13 @@ dev::TTable device_ttable(eqtl_ctx* ctx, double df, bool normal) {
   t.dl_inv = static_cast<float>(T.nb / (T.x_defer - T.x0));
   t.lt_u = T.lt_u ? 1 : 0;
   t.dlu_inv = T.lt_u ? static_cast<float>(1.0 / T.du_t) : 0.0f;
+  EQTL_CHECK(!T.lt_u || (T.na == dev::kTTableNa && T.nq == dev::kTTableNq), EQTL_E_INTERNAL, "screen table sizes");
+  t.c1q = T.lt_u ? reinterpret_cast<const float4*>(ws.tt_c1q.p) : nullptr;
+  t.ltq = T.lt_u ? reinterpret_cast<const float4*>(ws.tt_ltq.p) : nullptr;
+  t.nq = T.nq;
+  t.dq_inv = T.lt_u ? static_cast<float>(1.0 / T.du_q) : 0.0f;
+  t.uq0 = static_cast<float>(T.uq0);
+  t.dqc_inv = static_cast<float>(T.na / T.uq0);
   // round t_defer down so that every pair with p <= 1e-14 is deferred
   t.t_defer = static_cast<float>(T.t_defer * (1.0 - 1e-6));
   t.u0 = static_cast<float>(T.t0 * T.t0);
@@ -730,6 +739,15 @@ int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, 
   return guarded(ctx, [&] {
     EQTL_CHECK(Y && X, EQTL_E_ARG, "null input");
     eqtl::pheno_load(ctx, Y, X, n, n_genes, p);
+  });
+}
+
+int eqtl_pheno_permute(eqtl_ctx* ctx, const double* base, const double* xb0, const double* dinv,
+                       const uint64_t* gene_key, int32_t n, int32_t n_genes, int32_t n_perm, uint64_t seed,
+                       const double* X, int32_t p, double* Y_out) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(base && gene_key && X, EQTL_E_ARG, "null input");
+    eqtl::pheno_permute(ctx, base, xb0, dinv, gene_key, n, n_genes, n_perm, seed, X, p, Y_out);
   });
 }
 

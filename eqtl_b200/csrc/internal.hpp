@@ -194,6 +194,12 @@ struct Workspace {
   DevBuf<float> unscale, gscale, inv_gtg_f;
   DevBuf<uint8_t> ok;
   DevBuf<double> graw, gt;
+  // device-drawn permutations: per-gene base vectors, sort keys, offsets
+  DevBuf<double> perm_base, perm_xb0, perm_dinv;
+  DevBuf<uint64_t> perm_gkey;
+  DevBuf<unsigned long long> perm_keys, perm_sorted;
+  DevBuf<int> perm_off;
+  DevBuf<uint8_t> perm_temp;
   DevBuf<eqtl_pair> refined;
   DevBuf<double> tiny_p;
   DevBuf<int2> tile_list;
@@ -219,7 +225,7 @@ struct Workspace {
   // windows
   DevBuf<int32_t> win_gc, win_sc;
   DevBuf<int64_t> win_glo, win_ghi, win_sp;
-  DevBuf<float> tt_h, tt_L, tt_c1, tt_lt;
+  DevBuf<float> tt_h, tt_L, tt_c1, tt_lt, tt_c1q, tt_ltq;
   double tt_df = -1;
   // GRM operands and accumulators, eigen-solver scratch
   DevBuf<uint8_t> grm_use;
@@ -297,6 +303,10 @@ int peer_factors(eqtl_ctx* ctx, const double* Y_host, int n, int G, int K, int m
                  const double* X0, const double* W0, double* X_out);
 void geno_dosage_rows(eqtl_ctx* ctx, const int64_t* rows, int64_t k, double* out_host);
 void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, int p);
+// Resident phenotypes = G * B permuted columns drawn on the device (perm.cu).
+void pheno_permute(eqtl_ctx* ctx, const double* base, const double* xb0, const double* dinv,
+                   const uint64_t* gene_key, int n, int G, int B, uint64_t seed, const double* X, int p,
+                   double* Y_out);
 
 // -- scan drivers
 void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,

@@ -60,6 +60,7 @@ struct Options {
   int perm_trans_top = 1000;
   int seed = -1;
   bool disable_beta_approx = false;
+  bool perm_device = false;              // --perm-rng device: LM/LMM permutations drawn on the GPU
   // the fission subcommand (src/options.cpp:104-109, 237-252)
   bool run_fission = false;
   int peer_factors = 10;
@@ -138,6 +139,7 @@ void write_grm(const std::string& prefix, const std::vector<std::string>& ids, c
 // --------------------------------------------------------------- statistics
 double acat_p(double tan_sum, int used);                       // AcatAcc::p
 std::vector<double> bh_adjust(const std::vector<double>& p);   // src/scan_common.cpp:201-217
+uint64_t fnv1a64(const std::string& s);
 uint32_t fnv1a32(const std::string& s);
 uint32_t perm_seed(int seed_opt, int b, const std::string& gene);
 double p_emp(double T_obs, const std::vector<double>& T_perm);

@@ -85,6 +85,8 @@ void print_help() {
                "        --perm-trans-top INT    trans/gw: top-K SNPs for stage-2 perm  [1000]\n"
                "        --seed INT         permutation / fission seed\n"
                "        --disable-beta-approx  omit beta-approximated p\n"
+               "        --perm-rng STR     host: the reference's shuffles (std::mt19937, exact);\n"
+               "                           device: LM/LMM permutations drawn on the GPU (Philox)  [host]\n"
                "\n"
                "Output options:\n"
                "    -o, --out PREFIX       output prefix  [eqtl_out]\n"
@@ -108,7 +110,7 @@ int parse_options(int argc, char** argv, Options& opt) {
   }
   enum {
     kGffIdKey = 1001, kMakeGrm, kModel, kPvalCis, kPvalTrans, kMissHand, kFast, kPerm, kSeed, kNoBeta, kVersion,
-    kMaxMiss, kMaf, kPeerFactors, kEpsilon, kFissionMaxIter, kFissionTol, kPermThr = 1020, kPermTop, kPhenoNorm
+    kMaxMiss, kMaf, kPeerFactors, kEpsilon, kFissionMaxIter, kFissionTol, kPermThr = 1020, kPermTop, kPhenoNorm, kPermRng
   };
   static struct option long_opts[] = {{"vcf", required_argument, nullptr, 'v'},
                                       {"bfile", required_argument, nullptr, 'b'},
@@ -136,6 +138,7 @@ int parse_options(int argc, char** argv, Options& opt) {
                                       {"perm-trans-thr", required_argument, nullptr, kPermThr},
                                       {"perm-trans-top", required_argument, nullptr, kPermTop},
                                       {"seed", required_argument, nullptr, kSeed},
+                                      {"perm-rng", required_argument, nullptr, kPermRng},
                                       {"disable-beta-approx", no_argument, nullptr, kNoBeta},
                                       {"peer-factors", required_argument, nullptr, kPeerFactors},
                                       {"epsilon", required_argument, nullptr, kEpsilon},
@@ -186,6 +189,11 @@ int parse_options(int argc, char** argv, Options& opt) {
         if (opt.perm_trans_top < 1) die("--perm-trans-top must be >= 1");
         break;
       case kSeed: opt.seed = std::atoi(a.c_str()); break;
+      case kPermRng:
+        if (a == "host") opt.perm_device = false;
+        else if (a == "device") opt.perm_device = true;
+        else die("invalid --perm-rng (host|device)");
+        break;
       case kNoBeta: opt.disable_beta_approx = true; break;
       case kVersion: version = true; break;
       case kMaxMiss:

@@ -9,7 +9,11 @@
 // Each permutation b of a gene draws its shuffle from std::mt19937 seeded
 // with (seed or 1) + 9973 b + fnv1a(gene) through std::shuffle, so the index
 // sequences are the reference's; columns are built on all host threads,
-// one batch ahead of the device.
+// one batch ahead of the device. With --perm-rng device the LM and LMM
+// shuffles are drawn on the device instead (eqtl_pheno_permute: Philox keyed
+// by (seed or 1) and the 64-bit fnv1a of the gene): independent uniform
+// permutations, not the reference's sequences, and only the per-gene base
+// vectors cross to the device.
 //   GLM   parametric: after the same shuffle draws, y_i ~ Poisson(Gamma(1/phi,
 //         phi mu_i)) from the observed null fit (Poisson(mu_i) when phi <= 1e-9,
 //         0 when mu_i <= 1e-12), with the standard library's distributions
@@ -209,36 +213,73 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
   // genes per device batch: keep the permuted phenotype block near 2^26 doubles
   const size_t cols_budget = std::max<size_t>(static_cast<size_t>(B), (size_t(1) << 26) / std::max<size_t>(n, 1));
   const size_t genes_per_batch = std::max<size_t>(1, cols_budget / static_cast<size_t>(B));
+  // --perm-rng device (LM and LMM): the host prepares each gene's base
+  // vectors only; eqtl_pheno_permute draws and builds the columns on the
+  // device, where they stay for the scan
+  const bool on_device = opt.perm_device && model != "glm";
+  const uint64_t dev_seed = opt.seed >= 0 ? static_cast<uint64_t>(opt.seed) : 1u;
   Trace tr;
-  tr.mark("permutations: setup");
-  // the columns of batch k + 1 are built on the host while batch k runs on
-  // the device
+  tr.mark(std::string("permutations: setup (") + (on_device ? "device" : "host") + " draws)");
+  struct Batch {
+    std::vector<double> Y;                 // host draws: the columns [cols][n]
+    std::vector<double> base, xb0, dinv;   // device draws: per gene [nb][n]
+    std::vector<uint64_t> keys;
+  };
+  // batch k + 1 is prepared on the host while batch k runs on the device
   auto build = [&](size_t a) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
-    std::vector<double> Y(cols * n);
+    Batch bt;
     if (model == "glm") {
-      parallel_for(cols, [&](size_t c) { glm_column(opt, genes[active[a + c / B]], static_cast<int>(c % B), &Y[c * n]); });
-      return Y;
+      bt.Y.resize(cols * n);
+      parallel_for(cols, [&](size_t c) { glm_column(opt, genes[active[a + c / B]], static_cast<int>(c % B), &bt.Y[c * n]); });
+      return bt;
     }
     std::vector<PermBase> bases(nb);
     parallel_for(nb, [&](size_t gi) {
       const PermGene& g = genes[active[a + gi]];
       bases[gi] = lmm ? lmm_base(st, g.y, delta[active[a + gi]], Xt) : lm_base(st, g.y);
     });
+    if (on_device) {
+      bt.base.resize(nb * n);
+      if (lmm) {
+        bt.xb0.resize(nb * n);
+        bt.dinv.resize(nb * n);
+      }
+      bt.keys.resize(nb);
+      for (size_t gi = 0; gi < nb; ++gi) {
+        std::copy(bases[gi].base.begin(), bases[gi].base.end(), bt.base.begin() + gi * n);
+        if (lmm) {
+          std::copy(bases[gi].xb0.begin(), bases[gi].xb0.end(), bt.xb0.begin() + gi * n);
+          std::copy(bases[gi].dinv.begin(), bases[gi].dinv.end(), bt.dinv.begin() + gi * n);
+        }
+        bt.keys[gi] = fnv1a64(genes[active[a + gi]].name);
+      }
+      return bt;
+    }
+    bt.Y.resize(cols * n);
     parallel_for(cols, [&](size_t c) {
       const size_t gi = c / B;
-      permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &Y[c * n]);
+      permuted_column(st, model, bases[gi], genes[active[a + gi]].name, static_cast<int>(c % B), &bt.Y[c * n]);
     });
-    return Y;
+    return bt;
   };
-  std::future<std::vector<double>> next = std::async(std::launch::async, build, size_t(0));
+  std::future<Batch> next = std::async(std::launch::async, build, size_t(0));
   for (size_t a = 0; a < active.size(); a += genes_per_batch) {
     const size_t nb = std::min(genes_per_batch, active.size() - a);
     const size_t cols = nb * static_cast<size_t>(B);
-    const std::vector<double> Y = next.get();
+    const Batch bt = next.get();
+    const std::vector<double>& Y = bt.Y;  // empty with device draws: the scans read the resident columns
     if (a + genes_per_batch < active.size()) next = std::async(std::launch::async, build, a + genes_per_batch);
-    tr.mark("permutations: " + std::to_string(cols) + " columns ready (host build overlapped)");
+    if (on_device) {
+      st.dev->check(eqtl_pheno_permute(st.dev->ctx, bt.base.data(), lmm ? bt.xb0.data() : nullptr,
+                                       lmm ? bt.dinv.data() : nullptr, bt.keys.data(), static_cast<int32_t>(n),
+                                       static_cast<int32_t>(nb), B, dev_seed, st.X.data(), st.p, nullptr),
+                    "device permutation draws");
+      tr.mark("permutations: " + std::to_string(cols) + " columns drawn on the device");
+    } else {
+      tr.mark("permutations: " + std::to_string(cols) + " columns ready (host build overlapped)");
+    }
     std::vector<double> minp(cols, 1.0);
     if (model == "glm") {
       // every SNP of each gene's scope, with a fresh NB null fit per column
@@ -271,7 +312,8 @@ std::vector<PermOut> run_permutations(const Study& st, const std::string& model,
       prm.n_genes = static_cast<int32_t>(cols);
       prm.y_rotated = lmm ? 1 : 0;
       std::vector<eqtl_pair> res(pc.size());
-      st.dev->check(eqtl_test_pairs(st.dev->ctx, lmm ? EQTL_MODEL_LMM : EQTL_MODEL_LM, &prm, Y.data(), st.X.data(),
+      st.dev->check(eqtl_test_pairs(st.dev->ctx, lmm ? EQTL_MODEL_LMM : EQTL_MODEL_LM, &prm,
+                                    on_device ? nullptr : Y.data(), on_device ? nullptr : st.X.data(),
                                     pc.data(), ps.data(), static_cast<int64_t>(pc.size()), res.data(), nullptr),
                     "permutation tests");
       for (size_t i = 0; i < res.size(); ++i)

@@ -36,9 +36,10 @@ struct PermOut {
   BetaFit beta;
 };
 
-// One device scan of explicit phenotype columns Y [cols][n]: scope mode 0 gw,
-// 1 trans, 2 cis with per-column windows (null = no location); LMM columns
-// may already be rotated into the eigenbasis.
+// One device scan of explicit phenotype columns Y [cols][n] (Y empty: the
+// columns resident on the device, drawn by eqtl_pheno_permute): scope mode 0
+// gw, 1 trans, 2 cis with per-column windows (null = no location); LMM
+// columns may already be rotated into the eigenbasis.
 ScanResult scan_columns(const Study& st, const std::string& model, const std::vector<double>& Y, size_t cols,
                         const std::vector<const GeneLoc*>& windows, int mode, double pthr, double perm_thr,
                         bool rotated);

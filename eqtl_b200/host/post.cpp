@@ -42,14 +42,16 @@ std::vector<double> bh_adjust(const std::vector<double>& a) {
 }
 
 
-uint32_t fnv1a32(const std::string& s) {
+uint64_t fnv1a64(const std::string& s) {
   uint64_t h = 14695981039346656037ull;
   for (unsigned char ch : s) {
     h ^= ch;
     h *= 1099511628211ull;
   }
-  return static_cast<uint32_t>(h);
+  return h;
 }
+
+uint32_t fnv1a32(const std::string& s) { return static_cast<uint32_t>(fnv1a64(s)); }
 
 uint32_t perm_seed(int seed_opt, int b, const std::string& gene) {
   const uint64_t base = seed_opt >= 0 ? static_cast<uint64_t>(seed_opt) : 1u;

@@ -174,17 +174,20 @@ ScanResult scan_columns(const Study& st, const std::string& model, const std::ve
     R.conv.assign(J, 0);
   }
   int64_t cap = 1 << 18, ccap = perm_thr > 0 ? (1 << 18) : 1;
+  // no host columns: scan the resident ones (eqtl_pheno_permute)
+  const double* Yp = Y.empty() ? nullptr : Y.data();
+  const double* Xp = Y.empty() ? nullptr : st.X.data();
   for (int attempt = 0; attempt < 3; ++attempt) {
     R.pairs.resize(static_cast<size_t>(cap));
     R.cands.resize(static_cast<size_t>(ccap));
     int64_t np = 0, nc = 0;
     const int rc = model == "lm"
-                       ? eqtl_scan_trans_lm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.genes.data(), R.pairs.data(),
+                       ? eqtl_scan_trans_lm(st.dev->ctx, &prm, Yp, Xp, R.genes.data(), R.pairs.data(),
                                             cap, &np, R.cands.data(), ccap, &nc)
                    : model == "glm"
-                       ? eqtl_scan_glm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.phi.data(), R.conv.data(),
+                       ? eqtl_scan_glm(st.dev->ctx, &prm, Yp, Xp, R.phi.data(), R.conv.data(),
                                        R.genes.data(), R.pairs.data(), cap, &np, R.cands.data(), ccap, &nc)
-                       : eqtl_scan_trans_lmm(st.dev->ctx, &prm, Y.data(), st.X.data(), R.delta.data(),
+                       : eqtl_scan_trans_lmm(st.dev->ctx, &prm, Yp, Xp, R.delta.data(),
                                              R.genes.data(), R.pairs.data(), cap, &np, R.cands.data(), ccap, &nc);
     if (rc == EQTL_E_OVERFLOW) {
       cap = std::max(cap, np);

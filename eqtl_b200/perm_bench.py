@@ -120,6 +120,9 @@ def main() -> None:
     ap.add_argument("--perm", type=int, default=1000)
     ap.add_argument("--models", default="lmm,lm")
     ap.add_argument("--lognormal", action="store_true", help="lognormal cis-window sizes (see above)")
+    ap.add_argument("--perm-rng", choices=("host", "device"), default="host",
+                    help="host: the reference's seeded shuffles built on the host; device: permutations drawn "
+                         "on the GPU (eqtl --perm-rng device)")
     ap.add_argument("--reference", type=int, nargs=2, metavar=("GENES", "PERM"),
                     help="also time the reference program (oracle/_ref/eqtl, all host threads) on GENES genes "
                          "of median window size with --perm PERM and extrapolate to the workload by the "
@@ -133,7 +136,8 @@ def main() -> None:
         for model in args.models.split(","):
             cmd = [exe, "-b", os.path.join(d, "geno"), "-e", os.path.join(d, "pheno.tsv"), "-g",
                    os.path.join(d, "genes.gff"), "-c", os.path.join(d, "covar.tsv"), "--model", model, "--mode",
-                   "cis", "-w", "1000000", "--perm", str(args.perm), "-o", os.path.join(d, "out")]
+                   "cis", "-w", "1000000", "--perm", str(args.perm), "--perm-rng", args.perm_rng,
+                   "-o", os.path.join(d, "out")]
             t0 = time.perf_counter()
             r = subprocess.run(cmd, capture_output=True, text=True, env={**os.environ, "EQTL_TRACE": "1"})
             wall = time.perf_counter() - t0
@@ -162,7 +166,8 @@ def main() -> None:
             # host-side phases of the permutation driver (EQTL_TRACE): time since
             # the previous mark, summed over the batches
             host = {}
-            kinds = (("columns ready", "wait for host-built columns"), ("device scan", "device scans"),
+            kinds = (("columns ready", "wait for host-built columns"), ("drawn on the device", "device draws"),
+                     ("device scan", "device scans"),
                      ("p_emp", "p_emp and beta fits"), ("setup", "setup"))
             for ln in r.stderr.splitlines():
                 mt = re.match(r"\[eqtl trace\] permutations: (.*) ([\d.]+) ms$", ln)
@@ -170,7 +175,8 @@ def main() -> None:
                     for key, name in kinds:
                         if key in mt.group(1):
                             host[name] = host.get(name, 0.0) + float(mt.group(2))
-            print(json.dumps({"workload": "cis permutations", "model": model, "n_samples": 1000, "n_snps": m,
+            print(json.dumps({"workload": "cis permutations", "model": model, "perm_rng": args.perm_rng,
+                              "n_samples": 1000, "n_snps": m,
                               "genes": args.genes, "perm": args.perm, "covariates": 15,
                               "window_snps_mean": float(win.mean()) if win.size else 0.0,
                               "window_snps_percentiles": {q: int(np.percentile(win, q)) for q in (0, 5, 50, 95, 100)}

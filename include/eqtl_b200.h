@@ -142,6 +142,26 @@ int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t mod
  * Y == NULL and X == NULL, so repeated scans need no host transfer. */
 int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, int32_t n_genes, int32_t p);
 
+/* Permuted null phenotypes drawn on the device: the throughput mode of the
+ * gene-level permutations (include/eqtl/scan_cis.hpp:102-147 for cis,
+ * src/scan_perm.cpp:80-132 for trans/gw stage 2). The reference shuffles
+ * each gene's null base vector with std::mt19937 + std::shuffle on the host;
+ * here permutation b of gene g is the order of the keys
+ * Philox4x32-10(counter = (b, i / 4, gene_key[g]), key = seed) (word i % 4)
+ * of its samples i (Salmon et al., SC 2011), so the draws are independent
+ * and uniform but not the reference's sequences. The resident phenotypes
+ * (as after eqtl_pheno_load) become n_genes * n_perm columns, column
+ * g * n_perm + b:
+ *   LM  (xb0 == dinv == NULL)  base[g][perm(i)]
+ *   LMM                        xb0[g][i] + base[g][perm(i)] / sqrt(max(dinv[g][i], 1e-12))
+ * base, xb0, dinv [n_genes][n]; X [n, p] becomes the resident covariates.
+ * Scan the columns with Y == X == NULL (y_rotated = 1 for the LMM form, whose
+ * columns are in the eigenbasis). Y_out, if not NULL, receives the columns
+ * [n_genes * n_perm][n] (for validation). At most 2^31 values per call. */
+int eqtl_pheno_permute(eqtl_ctx* ctx, const double* base, const double* xb0, const double* dinv,
+                       const uint64_t* gene_key, int32_t n, int32_t n_genes, int32_t n_perm, uint64_t seed,
+                       const double* X, int32_t p, double* Y_out);
+
 /* --pheno-norm int on the device: replaces inverse_normal_transform
  * (src/util.cpp:177-206, with qnorm_inv :132-171) for every column of
  * Y [n, n_cols] (column-major, host memory), in place. Per column the finite
