@@ -33,9 +33,12 @@ struct LmEpiParams {
   int G;
   int64_t m;
   const double* inv_yty;   // [G] 1 / yty (0 when yty == 0)
-  const float* gscale;     // [G] accumulator -> gty factor
-  const float* inv_gtg;    // [m, padded to 16] 1 / gtg in FP32 (0 marks gtg < 1e-12: p = 1)
-  const uint8_t* snp_ok;   // [m] subset gate (src/scan_common.cpp:133-151)
+  const float* gscale;     // [G] gene-side factor of the accumulator -> gty
+  // [m, padded to 16] per SNP, in FP32: a^2 / gtg with a the SNP-side factor
+  // of the accumulator -> gty (0 where gtg < 1e-12: tested with p = 1; -1
+  // where the SNP is not tested: subset gate, src/scan_common.cpp:133-151,
+  // and the padding)
+  const float* igs;
   Windows win;
   float df;
   float t_cand;
@@ -53,8 +56,7 @@ struct LmEpi {
   int gene = 0;
   int64_t snp0 = 0;
   bool gvalid = false;
-  float inv_yty = 0;
-  float gs = 0;
+  float w = 0;   // gscale^2 / yty
   float u_cand;  // t_cand^2
   GeneAcc acc;
 
@@ -69,23 +71,21 @@ struct LmEpi {
     gvalid = g < P.G;
     acc.reset();
     if (gvalid) {
-      inv_yty = static_cast<float>(P.inv_yty[g]);
-      gs = P.gscale[g];
+      const float gs = P.gscale[g];
+      w = gs * gs * static_cast<float>(P.inv_yty[g]);
       acc.load_window(P.win, g);
     }
   }
-  // t^2 = df r / (1 - r), r = gty^2 / (gtg yty)  (hit_from_gty algebra),
-  // screened in FP32 without branches and without t itself; printed
-  // statistics come from the FP64 refinement.
+  // t^2 = df r / (1 - r), r = gty^2 / (gtg yty) = acc^2 (a^2 / gtg) (gscale^2 / yty)
+  // (hit_from_gty algebra), screened in FP32 without branches and without t
+  // itself; printed statistics come from the FP64 refinement.
   template <int NACC>
   __device__ void chunk(int c, const float (&v)[NACC][16]) {
     const int64_t s0 = snp0 + c;
     if (!gvalid || s0 >= P.m) return;
-    uint32_t okw[4];
-    load_flags16(P.snp_ok + s0, okw);
-    // the 16 SNPs' 1/gtg: s0 is a multiple of 16 and the array is padded
+    // the 16 SNPs' factors: s0 is a multiple of 16 and the array is padded
     float igv[16];
-    const float4* ig4 = reinterpret_cast<const float4*>(P.inv_gtg + s0);
+    const float4* ig4 = reinterpret_cast<const float4*>(P.igs + s0);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const float4 v4 = __ldg(ig4 + q);
@@ -97,10 +97,9 @@ struct LmEpi {
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int64_t s = s0 + j;
-      const bool valid = flag16(okw, j) && s < P.m && acc.in_scope(P.win, s);
-      const float ig = valid ? igv[j] : 0.0f;
-      const float num = v[0][j] * gs;
-      const float r = num * num * ig * inv_yty;
+      const bool valid = igv[j] >= 0.0f && acc.in_scope(P.win, s);
+      const float ig = valid ? igv[j] * w : 0.0f;
+      const float r = v[0][j] * v[0][j] * ig;
       const float omr = 1.0f - r;
       const float u = (ig > 0.0f && omr > 0.0f) ? P.df * __fdividef(r, omr) : 0.0f;  // t^2
       const ScreenOut o = acat_screen_u(u, tt);
@@ -115,11 +114,20 @@ struct LmEpi {
   __device__ void finish() {}
 };
 
-// out[i] = (float) x[i]
-__global__ void to_float_kernel(const double* __restrict__ x, int64_t count, float* out) {
+// The epilogue's per-SNP factor (LmEpiParams::igs) for the padded range
+// [0, count): alpha^2 / gtg (alpha null: 1) where the SNP is tested, -1
+// elsewhere.
+__global__ void lm_igs_kernel(const double* __restrict__ inv_gtg, const uint8_t* __restrict__ ok,
+                              const float* __restrict__ alpha, int64_t m, int64_t count, float* out) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    out[i] = static_cast<float>(x[i]);
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float v = -1.0f;
+    if (i < m && ok[i]) {
+      const double a = alpha ? static_cast<double>(alpha[i]) : 1.0;
+      v = static_cast<float>(a * a * inv_gtg[i]);
+    }
+    out[i] = v;
+  }
 }
 
 // ---------------------------------------------------------------- prep
@@ -334,6 +342,11 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   ws.inv_yty.alloc(G);
   ws.yty.alloc(G);
   const bool bf16 = ctx->precision == EQTL_PREC_SPLIT_BF16;
+  // FP16 scans read the exact integer-scaled dosages (one slice; the
+  // centring is implicit: the residualised y_s sum to zero, X holding the
+  // intercept), so two products per test (y hi and lo against them)
+  // instead of three against the split centred dosages
+  const bool raw = !bf16 && geno_raw_operand(ctx);
   ++ctx->launches;
   if (bf16)
     gene_split_kernel<__nv_bfloat16><<<G, 256, 0, st>>>(ws.Ys.p, n, k_pad, G,
@@ -342,7 +355,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
                                                         ws.yty.p, ws.inv_yty.p, kGcScale);
   else
     gene_split_kernel<__half><<<G, 256, 0, st>>>(ws.Ys.p, n, k_pad, G, a_hi.p, a_lo.p, ws.gscale.p, ws.yty.p,
-                                                 ws.inv_yty.p, kGcScale);
+                                                 ws.inv_yty.p, raw ? 1.0f : kGcScale);
   EQTL_CUDA(cudaGetLastError());
 
   // ---- per-SNP FP64 residual sum of squares + subset gate
@@ -368,17 +381,14 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   ep.m = m;
   ep.inv_yty = ws.inv_yty.p;
   ep.gscale = ws.gscale.p;
-  // FP32 copy of 1/gtg, padded to a multiple of 16 (+16) for vector loads
-  ws.inv_gtg_f.alloc(static_cast<size_t>(((m + 15) / 16 + 1) * 16));
-  EQTL_CUDA(cudaMemsetAsync(ws.inv_gtg_f.p, 0, ws.inv_gtg_f.n * sizeof(float), st));
-  if (m > 0) {
-    ++ctx->launches;
-    to_float_kernel<<<static_cast<unsigned>(std::min<int64_t>((m + 255) / 256, 4096)), 256, 0, st>>>(
-        ws.inv_gtg.p, m, ws.inv_gtg_f.p);
-    EQTL_CUDA(cudaGetLastError());
-  }
-  ep.inv_gtg = ws.inv_gtg_f.p;
-  ep.snp_ok = ws.ok.p;
+  // per-SNP factors, padded to the end of the last tile of 256 SNPs
+  const int64_t m_pad = ((m + 255) / 256 + 1) * 256;
+  ws.inv_gtg_f.alloc(static_cast<size_t>(m_pad));
+  ++ctx->launches;
+  lm_igs_kernel<<<static_cast<unsigned>(std::min<int64_t>((m_pad + 255) / 256, 4096)), 256, 0, st>>>(
+      ws.inv_gtg.p, ws.ok.p, raw ? ctx->rot.alpha.p : nullptr, m, m_pad, ws.inv_gtg_f.p);
+  EQTL_CUDA(cudaGetLastError());
+  ep.igs = ws.inv_gtg_f.p;
   ep.win = upload_windows(ctx, prm, m, prm->exclude_cis == 2 ? kWinInclude : prm->exclude_cis ? kWinExclude : kWinNone);
   ep.df = static_cast<float>(df);
   ep.t_cand = static_cast<float>(t_cand * (1.0 - 1e-3));
@@ -395,10 +405,18 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
       ep.out = out;
       const __half* ah[1] = {a_hi.p};
       const __half* al[1] = {a_lo.p};
-      const __half* bh[1] = {g.gc_hi.p};
-      const __half* bl[1] = {g.gc_lo.p};
-      const int bsel[1] = {0}, prod[1] = {7};
-      launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, G, bh, bl, m, k_pad, bsel, prod, tiles, n_tiles);
+      const int bsel[1] = {0};
+      if (raw) {
+        const __half* bh[1] = {ctx->rot.raw.p};
+        const int prod[1] = {5};
+        launch_tile_n<256, 1, LmEpiParams, false>(ctx, false, ep, ah, al, G, bh, bh, m, k_pad, bsel, prod, tiles,
+                                                  n_tiles);
+      } else {
+        const __half* bh[1] = {g.gc_hi.p};
+        const __half* bl[1] = {g.gc_lo.p};
+        const int prod[1] = {7};
+        launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, G, bh, bl, m, k_pad, bsel, prod, tiles, n_tiles);
+      }
     });
   }
   scan_timer.reset();

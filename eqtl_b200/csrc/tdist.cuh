@@ -22,7 +22,10 @@ namespace dev {
 
 constexpr int kTTableNa = 512;   // central intervals (TTableHost::na)
 constexpr int kTTableNb = 4096;  // tail intervals (TTableHost::nb)
-constexpr int kTTableSmemBytes = (kTTableNa + 4 + kTTableNb + 4) * 4;
+constexpr int kTTableNq = 1024;  // tail intervals of the per-interval cubics (TTableHost::nq)
+constexpr int kTTableNodeBytes = (kTTableNa + 4 + kTTableNb + 4) * 4;
+constexpr int kTTableCubicBytes = (kTTableNa + kTTableNq) * 16;
+constexpr int kTTableSmemBytes = kTTableNodeBytes > kTTableCubicBytes ? kTTableNodeBytes : kTTableCubicBytes;
 
 struct TTable {
   const float* h;  // na + 4 nodes
@@ -40,6 +43,13 @@ struct TTable {
   float dl_inv;     // nb / (x(t_defer) - x0)
   int lt_u;         // 1: lt holds the term itself on u in [u0, u_defer] (dlu_inv = nb / that range)
   float dlu_inv;
+  // with lt_u, the screen's per-interval cubics (a0, a1, a2, a3): c1q over
+  // u in [0, uq0] (na intervals, dqc_inv per unit of u), ltq over u in
+  // [uq0, u_defer] (nq intervals, dq_inv)
+  const float4* c1q;
+  const float4* ltq;
+  float uq0, dqc_inv, dq_inv;
+  int nq;
   float t_defer;    // |t| >= t_defer (p <= 1e-14): the term is left to the host
   // the same thresholds on u = t^2 (the scan epilogues screen t^2 directly)
   float u0;         // t0^2
@@ -130,6 +140,7 @@ __device__ __forceinline__ TailOut t_tail(float t, const TTable& T) {
 // One table lookup:
 //   central  tan((1/2 - p) pi) = c1(u) / |t| = c1(u) rsqrt(u)
 //   tail     tan((1/2 - p) pi) = lt(u)                      (T.lt_u, short tails)
+// (with T.lt_u both as per-interval cubics: one 16-byte load and three FMAs)
 //            tan((1/2 - p) pi) = exp(lt(sqrt(log1p(u / df))))  (otherwise)
 struct ScreenOut {
   float term;     // tan((1/2 - p) pi) when use_acat, else 0
@@ -147,13 +158,19 @@ __device__ __forceinline__ ScreenOut acat_screen_u(float u, const TTable& T) {
   o.deferred = !nan_u && (tiny || u >= T.u_defer);
   o.use_acat = !nan_u && !o.deferred && u > 0.0f;
   o.key = nan_u ? 0.0f : u;
-  const bool central = u <= T.u0;
-  float x, term;
+  float term;
   if (T.lt_u) {  // uniform across the launch
-    x = central ? u * T.du_inv : (u - T.u0) * T.dlu_inv;
-    const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
+    const bool central = u <= T.uq0;
+    float x = central ? u * T.dqc_inv : (u - T.uq0) * T.dq_inv;
+    x = fminf(fmaxf(x, 0.0f), static_cast<float>(central ? T.na : T.nq) - 1e-3f);
+    const int i = static_cast<int>(x);
+    const float f = x - static_cast<float>(i);
+    const float4 a = (central ? T.c1q : T.ltq)[i];
+    const float y = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
     term = central ? y * rsqrtf(u) : y;
   } else {
+    const bool central = u <= T.u0;
+    float x;
     const float xs = sqrtf(log1pf(u * T.inv_df));
     x = central ? u * T.du_inv : (xs - T.x0) * T.dl_inv;
     const float y = lagrange4(central ? T.c1 : T.lt, x, central ? T.na + 1 : T.nb + 1);
@@ -173,11 +190,21 @@ __device__ __forceinline__ ScreenOut acat_screen(float t, const TTable& T) {
 
 // Copies the screening tables into shared memory (cooperatively, by `nthr`
 // threads) and returns a view of them; the caller synchronises before use.
+// (With lt_u the per-interval cubics, else the node tables; `sm` 16-byte
+// aligned, kTTableSmemBytes.)
 __device__ __forceinline__ TTable screen_to_smem(const TTable& T, float* sm, int tid, int nthr) {
+  TTable o = T;
+  if (T.lt_u) {
+    float4* q = reinterpret_cast<float4*>(sm);
+    for (int i = tid; i < T.na; i += nthr) q[i] = T.c1q[i];
+    for (int i = tid; i < T.nq; i += nthr) q[T.na + i] = T.ltq[i];
+    o.c1q = q;
+    o.ltq = q + T.na;
+    return o;
+  }
   const int nc = T.na + 4, nl = T.nb + 4;
   for (int i = tid; i < nc; i += nthr) sm[i] = T.c1[i];
   for (int i = tid; i < nl; i += nthr) sm[nc + i] = T.lt[i];
-  TTable o = T;
   o.c1 = sm;
   o.lt = sm + nc;
   return o;

@@ -75,11 +75,13 @@ struct TileShape {
   uint32_t* status;       // device status word (DevStatus)
 };
 
-template <int NT, int NACC>
+// BLO = false: no product reads a SNP-side lo part (exact SNP operands), so
+// a ring stage holds A hi, A lo and B hi only and more stages fit.
+template <int NT, int NACC, bool BLO = true>
 struct TileCfg {
   static constexpr int A_BYTES = kTileM * kChunkK * 2;
   static constexpr int B_BYTES = NT * kChunkK * 2;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + (BLO ? 2 : 1) * B_BYTES;
   static constexpr int STAGES = (196608 / STAGE_BYTES) < 2 ? 2 : (196608 / STAGE_BYTES > 6 ? 6 : 196608 / STAGE_BYTES);
   // TMEM is split into NSLOTS slots of NT columns; accumulator j of work
   // unit u lives in slot (u * NACC + j) % NSLOTS, so the next unit's first
@@ -127,11 +129,11 @@ __device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta,
   k1 = min(sh.kchunks, k0 + sh.kc_per_split);
 }
 
-template <int NT, int NACC, uint32_t AB_FMT, class Epi>
+template <int NT, int NACC, uint32_t AB_FMT, class Epi, bool BLO = true>
 __global__ void __launch_bounds__(kTileThreads, 1)
     tile_kernel(const __grid_constant__ TileMaps maps, const TileShape sh,
                 const __grid_constant__ typename Epi::Params ep) {
-  using C = TileCfg<NT, NACC>;
+  using C = TileCfg<NT, NACC, BLO>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         for (int j = 0; j < sh.n_acc && ok; ++j) {
           const int bp = sh.bsel[j];
           // only the lo parts some product of this accumulator reads are loaded
-          const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = (sh.prod[j] & 2) != 0;
+          const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = BLO && (sh.prod[j] & 2) != 0;
           const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
                                                        (b_lo ? C::B_BYTES : 0));
           for (int kc = k0; kc < k1; ++kc) {
@@ -269,7 +271,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
                   umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
                   accum = 1u;
                 }
-                if (pm & 2) {
+                if (BLO && (pm & 2)) {
                   umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
                   accum = 1u;
                 }

@@ -68,6 +68,17 @@ struct TTableHost {
                            // term tan((1/2 - p) pi) itself on u = t^2 in [t0^2, t_defer^2]
   bool lt_u = false;       // the tail table is linear in u (short tails: df large enough, or normal)
   double du_t = 0;         // its u step
+  // With lt_u, the screen reads per-interval cubics instead of nodes: four
+  // coefficients (a0, a1, a2, a3) per interval, y = a0 + a1 f + a2 f^2 + a3 f^3
+  // at the fraction f of the interval (one 16-byte load per pair):
+  // (their own split at u = uq0: the term is far from exponential in u just
+  // above t0 = 1, where a cubic on the tail's coarser step would be off by
+  // up to 4e-5 at df = 30)
+  double uq0 = 4.0;
+  std::vector<float> c1q;  // na intervals on u in [0, uq0]: |t| * tan((1/2 - p) pi)
+  std::vector<float> ltq;  // nq intervals on u in [uq0, t_defer^2]: tan((1/2 - p) pi)
+  int nq = 1024;
+  double du_q = 0;
   double x_defer = 0;      // tail grid end: x at p = 1e-14
   double t_defer = 0;      // |t| with p = 1e-14: beyond it the term is left to the host
   std::vector<float> h;          // na + 4 nodes: h(u) = (1 - p) / |t|, node k at u = (k-1) du
@@ -146,6 +157,15 @@ inline double central_h_normal(double u) {
   return 2.0 * acc / std::sqrt(2.0 * M_PI);
 }
 
+// Coefficients of the cubic through (-1, y0), (0, y1), (1, y2), (2, y3) in
+// powers of f (the interval between the middle nodes is f in [0, 1]).
+inline void cubic_coeffs(double y0, double y1, double y2, double y3, float* a) {
+  a[0] = static_cast<float>(y1);
+  a[1] = static_cast<float>(-y0 / 3.0 - y1 / 2.0 + y2 - y3 / 6.0);
+  a[2] = static_cast<float>(0.5 * (y0 + y2) - y1);
+  a[3] = static_cast<float>((y3 - y0) / 6.0 + 0.5 * (y1 - y2));
+}
+
 inline TTableHost build_ttable(double df, bool normal = false) {
   TTableHost T;
   T.normal = normal;
@@ -196,12 +216,12 @@ inline TTableHost build_ttable(double df, bool normal = false) {
   // -|t| cot(pi |t| h) = -(z cot z) / (pi h) with z^2 = pi^2 u h^2, analytic
   // in u (also at the node below 0). Tail: ln tan((1/2 - p) pi) = ln cot(pi p),
   // smooth in x up to p = 1e-14, past which the host adds the term.
-  T.c1.resize(T.na + 4);
-  for (int k = 0; k < T.na + 4; ++k) {
-    const double u = (k - 1) * du;
+  auto c1fun = [&](double u) {
     const double h = hfun(u);
-    T.c1[k] = static_cast<float>(-zcotz(M_PI * M_PI * u * h * h) / (M_PI * h));
-  }
+    return -zcotz(M_PI * M_PI * u * h * h) / (M_PI * h);
+  };
+  T.c1.resize(T.na + 4);
+  for (int k = 0; k < T.na + 4; ++k) T.c1[k] = static_cast<float>(c1fun((k - 1) * du));
   T.t_defer = normal ? z_critical(1e-14) : t_critical(1e-14, df);
   T.x_defer = std::sqrt(std::log1p(T.t_defer * T.t_defer / df));
   T.lt.resize(T.nb + 4);
@@ -214,11 +234,24 @@ inline TTableHost build_ttable(double df, bool normal = false) {
   if (du_t <= 0.05) {
     T.lt_u = true;
     T.du_t = du_t;
-    for (int k = 0; k < T.nb + 4; ++k) {
-      const double u = T.t0 * T.t0 + (k - 1) * du_t;
+    auto term = [&](double u) {
       const double p = pfun(std::sqrt(u));
-      T.lt[k] = static_cast<float>(std::cos(M_PI * p) / std::sin(M_PI * p));
-    }
+      return std::cos(M_PI * p) / std::sin(M_PI * p);
+    };
+    for (int k = 0; k < T.nb + 4; ++k) T.lt[k] = static_cast<float>(term(T.t0 * T.t0 + (k - 1) * du_t));
+    // the per-interval cubics: above uq0 the term grows about as exp(u / 2)
+    // (fourth derivative ~ 1/16 of it), so at nq = 1024 intervals (u step
+    // <= 0.2) the cubic's relative error stays below 1.5e-3 step^4 ~ 3e-6
+    const double du_c = T.uq0 / T.na;
+    std::vector<double> cd(T.na + 3);
+    for (int k = 0; k < T.na + 3; ++k) cd[k] = c1fun((k - 1) * du_c);
+    T.c1q.resize(4 * static_cast<size_t>(T.na));
+    for (int i = 0; i < T.na; ++i) cubic_coeffs(cd[i], cd[i + 1], cd[i + 2], cd[i + 3], &T.c1q[4 * i]);
+    T.du_q = (T.t_defer * T.t_defer - T.uq0) / T.nq;
+    std::vector<double> ld(T.nq + 3);
+    for (int k = 0; k < T.nq + 3; ++k) ld[k] = term(T.uq0 + (k - 1) * T.du_q);
+    T.ltq.resize(4 * static_cast<size_t>(T.nq));
+    for (int i = 0; i < T.nq; ++i) cubic_coeffs(ld[i], ld[i + 1], ld[i + 2], ld[i + 3], &T.ltq[4 * i]);
     return T;
   }
   const double dl = (T.x_defer - T.x0) / T.nb;
