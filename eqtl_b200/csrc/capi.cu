@@ -399,19 +399,22 @@ void pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int n, int G, i
 }
 
 namespace {
-__global__ void t_tail_kernel(dev::TTable T, const float* t, int64_t n, int use_smem, float* nl, double* term,
-                              uint8_t* flags) {
-  extern __shared__ float tsm[];
-  const bool screen = (use_smem & 2) != 0;
+// One instantiation per mode (tables in shared memory or read from global
+// memory; the t tail or the ACAT screen), so that every table pointer the
+// kernel reads has one address space.
+template <bool SMEM, bool SCREEN>
+__global__ void t_tail_kernel(dev::TTable T, const float* t, int64_t n, float* nl, double* term, uint8_t* flags) {
+  extern __shared__ float4 tsm4[];
   dev::TTable tt = T;
-  if (use_smem & 1) {
-    tt = screen ? dev::screen_to_smem(T, tsm, threadIdx.x, blockDim.x)
-                : dev::ttable_to_smem(T, tsm, threadIdx.x, blockDim.x);
+  if constexpr (SMEM) {
+    float* tsm = reinterpret_cast<float*>(tsm4);
+    if constexpr (SCREEN) tt = dev::screen_to_smem(T, tsm, threadIdx.x, blockDim.x);
+    else tt = dev::ttable_to_smem(T, tsm, threadIdx.x, blockDim.x);
     __syncthreads();
   }
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (screen) {
+  if constexpr (SCREEN) {
     const dev::ScreenOut o = dev::acat_screen(t[i], tt);
     nl[i] = o.key;
     term[i] = o.term;
@@ -725,8 +728,14 @@ int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use
     dterm.alloc(n);
     dfl.alloc(n);
     ++ctx->launches;
-    eqtl::t_tail_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, use_smem ? eqtl::dev::kTTableSmemBytes : 0,
-                          ctx->stream>>>(T, dt.p, n, use_smem, dn.p, dterm.p, dfl.p);
+    const unsigned grid = static_cast<unsigned>((n + 255) / 256);
+    const size_t sm = eqtl::dev::kTTableSmemBytes;
+    switch (use_smem & 3) {
+      case 0: eqtl::t_tail_kernel<false, false><<<grid, 256, 0, ctx->stream>>>(T, dt.p, n, dn.p, dterm.p, dfl.p); break;
+      case 1: eqtl::t_tail_kernel<true, false><<<grid, 256, sm, ctx->stream>>>(T, dt.p, n, dn.p, dterm.p, dfl.p); break;
+      case 2: eqtl::t_tail_kernel<false, true><<<grid, 256, 0, ctx->stream>>>(T, dt.p, n, dn.p, dterm.p, dfl.p); break;
+      default: eqtl::t_tail_kernel<true, true><<<grid, 256, sm, ctx->stream>>>(T, dt.p, n, dn.p, dterm.p, dfl.p); break;
+    }
     EQTL_CUDA(cudaGetLastError());
     dn.download(neglog10p, n, ctx->stream);
     dterm.download(term, n, ctx->stream);
