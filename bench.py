@@ -365,6 +365,25 @@ def b200_arm(args, rank, world, local_rank):
                             "fp32_peak_tflops_at_sampled_clock": fp32_peak,
                             "frac_of_fp32_peak": flops / (s32 / 1e3) / 1e12 / fp32_peak}
         ctx32.close()
+    # ---- the split-BF16 form of the same scan (BF16 hi + lo on both sides,
+    # three products per accumulator: the exact dosage slice is FP16-only)
+    if rank == 0 and not args.no_bf16:
+        ctxb = capi.Context(local_rank, precision=capi.PREC_SPLIT_BF16)
+        ctxb.load_bed(rows, n, np.arange(n, dtype=np.int32))
+        ctxb.pheno_load(Y, X)
+        ctxb.lmm_basis()
+        run_value_step(ctxb)  # builds the BF16 SNP operands once
+        sb = []
+        for _ in range(3):
+            run_value_step(ctxb)
+            sb.append(ctxb.stage_ms("scan"))
+        s16 = statistics.median(sb)
+        out["bf16_split"] = {"scan_ms": s16, "tests_per_s_scan": tests / (s16 / 1e3),
+                             "algorithmic_tflops": flops / (s16 / 1e3) / 1e12,
+                             "frac": flops / (s16 / 1e3) / 1e12 / peak,
+                             "issued_flops_per_test": 2 * n * 3 * (p_cov + 2),
+                             "scan_ms_vs_f16": s16 / scan_ms}
+        ctxb.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, rows, Y)
     ctx.close()
@@ -422,6 +441,7 @@ def main():
     ap.add_argument("--ref-snps", type=int, default=4000)
     ap.add_argument("--ref-genes", type=int, default=1000)
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-bf16", action="store_true", help="skip the split-BF16 form of the scan")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.family = (50, 10, args.n - 500) if args.n > 500 else None

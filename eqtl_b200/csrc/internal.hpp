@@ -176,6 +176,10 @@ struct Rotated {
   bool raw_exact = false;  // every kept SNP representable exactly
   // FP32 copies of Gt and Gt^2 for the plain FP32 CUDA-core comparator
   DevBuf<float> gt32, gt2_32;
+  // split-BF16 scans: Gt and Gt^2 re-split into BF16 hi + lo (bits of
+  // __nv_bfloat16 in 16-bit storage), for the rotation of bf16_m SNPs
+  DevBuf<__half> bgt_hi, bgt_lo, bgt2_hi, bgt2_lo;
+  int64_t bf16_m = -1;
 };
 
 // Phenotypes / covariates resident on the device (eqtl_pheno_load).
@@ -190,6 +194,7 @@ struct PhenoDev {
 struct Workspace {
   DevBuf<double> Ytil, Xtil, Ys, XtY, XtXinv, delta, chi0, ainv, a00L, rss, gtg, inv_gtg, af_sub, inv_yty, yty;
   DevBuf<__half> ops_hi[34], ops_lo[34];  // gene-side operands, one per accumulator (dev::kMaxAcc)
+  DevBuf<__half> opsb_hi[34], opsb_lo[34];  // the same re-split into BF16 hi + lo (split-BF16 LMM scans)
   DevBuf<__half*> ops_ptr;
   DevBuf<float> unscale, gscale, inv_gtg_f;
   DevBuf<uint8_t> ok;

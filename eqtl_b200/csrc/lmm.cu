@@ -90,13 +90,22 @@ struct RotEpi {
 };
 
 // Qt operand: row j = eigenvector j (column j of column-major Q) * 2^10.
-__global__ void q_split_kernel(const double* __restrict__ Q, int n, int k_pad, __half* hi, __half* lo) {
+// Q' split into hi + lo rows of T (FP16, or BF16 for the split-BF16 form,
+// whose genotype operand is BF16 too)
+template <class T>
+__global__ void q_split_kernel(const double* __restrict__ Q, int n, int k_pad, T* hi, T* lo) {
   const int j = blockIdx.y;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k_pad; i += gridDim.x * blockDim.x) {
     const double v = i < n ? Q[static_cast<int64_t>(j) * n + i] * 1024.0 : 0.0;
-    const __half h = __double2half(v);
-    hi[static_cast<int64_t>(j) * k_pad + i] = h;
-    lo[static_cast<int64_t>(j) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+    if constexpr (std::is_same_v<T, __half>) {
+      const __half h = __double2half(v);
+      hi[static_cast<int64_t>(j) * k_pad + i] = h;
+      lo[static_cast<int64_t>(j) * k_pad + i] = __double2half(v - static_cast<double>(__half2float(h)));
+    } else {
+      const __nv_bfloat16 h = __double2bfloat16(v);
+      hi[static_cast<int64_t>(j) * k_pad + i] = h;
+      lo[static_cast<int64_t>(j) * k_pad + i] = __double2bfloat16(v - static_cast<double>(__bfloat162float(h)));
+    }
   }
 }
 
@@ -1485,9 +1494,8 @@ void lmm_rotate(eqtl_ctx* ctx) {
   Geno& g = ctx->geno;
   Rotated& R = ctx->rot;
   EQTL_CHECK(ctx->have_basis && ctx->basis.n == g.n, EQTL_E_STATE, "rotation needs an eigenbasis of size n");
-  EQTL_CHECK(ctx->precision != EQTL_PREC_SPLIT_BF16, EQTL_E_UNSUPPORTED,
-             "the LMM path runs split-FP16 (or the FP32 CUDA-core comparator); BF16 is LM-only");
   if (R.m == g.m && R.k_pad == g.k_pad && R.gt_hi.p) return;
+  R.bf16_m = -1;
   cudaStream_t st = ctx->stream;
   StageScope timer(ctx, EQTL_STAGE_ROTATE);
   const int n = g.n, k_pad = g.k_pad;
@@ -1497,7 +1505,14 @@ void lmm_rotate(eqtl_ctx* ctx) {
   ++ctx->launches;
   qh.alloc(static_cast<size_t>(n) * k_pad);
   ql.alloc(static_cast<size_t>(n) * k_pad);
-  q_split_kernel<<<dim3((k_pad + 255) / 256, n), 256, 0, st>>>(ctx->basis.Q.p, n, k_pad, qh.p, ql.p);
+  // split-BF16 contexts hold the genotype operand in BF16, so Q' is split
+  // in BF16 too and the rotation runs on BF16 pairs
+  const bool bf16 = ctx->precision == EQTL_PREC_SPLIT_BF16;
+  if (bf16)
+    q_split_kernel<__nv_bfloat16><<<dim3((k_pad + 255) / 256, n), 256, 0, st>>>(
+        ctx->basis.Q.p, n, k_pad, reinterpret_cast<__nv_bfloat16*>(qh.p), reinterpret_cast<__nv_bfloat16*>(ql.p));
+  else
+    q_split_kernel<__half><<<dim3((k_pad + 255) / 256, n), 256, 0, st>>>(ctx->basis.Q.p, n, k_pad, qh.p, ql.p);
   EQTL_CUDA(cudaGetLastError());
   const size_t elems = static_cast<size_t>(m) * k_pad;
   R.gt_hi.alloc(elems);
@@ -1524,7 +1539,7 @@ void lmm_rotate(eqtl_ctx* ctx) {
     const __half* bh[1] = {g.gc_hi.p};
     const __half* bl[1] = {g.gc_lo.p};
     const int bsel[1] = {0}, prod[1] = {7};
-    launch_tile_n<256, 1>(ctx, false, ep, ah, al, n, bh, bl, m, k_pad, bsel, prod);
+    launch_tile_n<256, 1>(ctx, bf16, ep, ah, al, n, bh, bl, m, k_pad, bsel, prod);
   }
   if (ctx->precision == EQTL_PREC_FP32_SIMT && m > 0) {
     // the FP32 form keeps its SNP-side operands in FP32
@@ -1689,6 +1704,52 @@ void lmm_prep(eqtl_ctx* ctx, const PhenoDev& ph, bool y_rotated) {
 }
 
 // ------------------------------------------------------------------- scan
+// hi + lo of an FP16 pair operand, re-split into BF16 hi + lo (the split-BF16
+// form of the scans: ~16 significant bits instead of ~22)
+__global__ void resplit_bf16_kernel(const __half* __restrict__ hi, const __half* __restrict__ lo, int64_t count,
+                                    __nv_bfloat16* bhi, __nv_bfloat16* blo) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float v = __half2float(hi[i]) + __half2float(lo[i]);
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    bhi[i] = h;
+    blo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+}
+
+static void resplit_bf16(eqtl_ctx* ctx, const __half* hi, const __half* lo, int64_t count, DevBuf<__half>& bhi,
+                         DevBuf<__half>& blo) {
+  bhi.alloc(static_cast<size_t>(std::max<int64_t>(count, 1)));
+  blo.alloc(static_cast<size_t>(std::max<int64_t>(count, 1)));
+  if (count <= 0) return;
+  ++ctx->launches;
+  resplit_bf16_kernel<<<static_cast<unsigned>(std::min<int64_t>((count + 255) / 256, int64_t(ctx->sm_count) * 32)),
+                        256, 0, ctx->stream>>>(hi, lo, count, reinterpret_cast<__nv_bfloat16*>(bhi.p),
+                                               reinterpret_cast<__nv_bfloat16*>(blo.p));
+  EQTL_CUDA(cudaGetLastError());
+}
+
+// The split-BF16 SNP-side operands of the rotation (once per rotation).
+static void rot_bf16(eqtl_ctx* ctx, Rotated& R) {
+  if (R.bf16_m == R.m && R.bgt_hi.p) return;
+  const int64_t elems = R.m * R.k_pad;
+  resplit_bf16(ctx, R.gt_hi.p, R.gt_lo.p, elems, R.bgt_hi, R.bgt_lo);
+  resplit_bf16(ctx, R.gt2_hi.p, R.gt2_lo.p, elems, R.bgt2_hi, R.bgt2_lo);
+  R.bf16_m = R.m;
+}
+
+// The split-BF16 gene-side operands: nops pairs of rows x k_pad into
+// ws.opsb_hi / opsb_lo; out[j], out[nops + j] point at pair j's hi and lo.
+static void gene_ops_bf16(eqtl_ctx* ctx, const __half* const* hi, const __half* const* lo, int nops, int64_t rows,
+                          int k_pad, const __half** out) {
+  EQTL_CHECK(nops <= dev::kMaxAcc, EQTL_E_INTERNAL, "split-BF16 gene operands");
+  for (int j = 0; j < nops; ++j) {
+    resplit_bf16(ctx, hi[j], lo[j], rows * k_pad, ctx->ws.opsb_hi[j], ctx->ws.opsb_lo[j]);
+    out[j] = ctx->ws.opsb_hi[j].p;
+    out[nops + j] = ctx->ws.opsb_lo[j].p;
+  }
+}
+
 template <int P>
 static void lmm_launch_simt(eqtl_ctx* ctx, const LmmEpiParams<P>& ep, const __half* const* ah,
                             const __half* const* al, int G, const __half* const* bh, const __half* const* bl,
@@ -1715,6 +1776,18 @@ static void lmm_launch(eqtl_ctx* ctx, const EP& ep, const __half* const* ah, con
   }
   ah = oh;
   al = ol;
+  if (!simt && !raw && ctx->precision == EQTL_PREC_SPLIT_BF16) {
+    // split-BF16: both sides re-split into BF16 hi + lo, three products each
+    const __half* b16[2 * (P + 2)];
+    gene_ops_bf16(ctx, ah, al, P + 2, G, R.k_pad, b16);
+    Rotated& Rw = const_cast<Rotated&>(R);
+    rot_bf16(ctx, Rw);
+    const __half* sbh[2] = {Rw.bgt_hi.p, Rw.bgt2_hi.p};
+    const __half* sbl[2] = {Rw.bgt_lo.p, Rw.bgt2_lo.p};
+    launch_tile_n<128, P + 2>(ctx, true, ep, b16, b16 + (P + 2), G, sbh, sbl, R.m, R.k_pad, bsel, prod, tiles,
+                              n_tiles);
+    return;
+  }
   if (!simt) {
     launch_tile_n<128, P + 2>(ctx, false, ep, ah, al, G, bh, bl, R.m, R.k_pad, bsel, prod, tiles, n_tiles);
     return;
@@ -1966,10 +2039,22 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
     const __half* bl[2] = {Rt.gt_lo.p, Rt.gt2_lo.p};
     std::vector<int> bsel(nops, 0), prod(nops, 7);
     bsel[1] = 1;  // gg reads Gt^2
+    const bool bf16 = ctx->precision == EQTL_PREC_SPLIT_BF16;
+    std::vector<const __half*> opb(2 * static_cast<size_t>(nops));
+    if (bf16) {
+      // split-BF16: both sides re-split into BF16 hi + lo
+      gene_ops_bf16(ctx, oph.data(), oph.data() + nops, nops, G, Rt.k_pad, opb.data());
+      rot_bf16(ctx, Rt);
+      bh[0] = Rt.bgt_hi.p;
+      bh[1] = Rt.bgt2_hi.p;
+      bl[0] = Rt.bgt_lo.p;
+      bl[1] = Rt.bgt2_lo.p;
+    }
+    const __half* const* ops = bf16 ? opb.data() : oph.data();
     so.run([&](GeneOut out) {
       ep.out = out;
-      launch_tile_n<LmmGroupEpi::kTileN, 4>(ctx, false, ep, oph.data(), oph.data() + nops, G, bh, bl, Rt.m, Rt.k_pad,
-                                            bsel.data(), prod.data(), tiles, n_tiles, 1, nops);
+      launch_tile_n<LmmGroupEpi::kTileN, 4>(ctx, bf16, ep, ops, ops + nops, G, bh, bl, Rt.m, Rt.k_pad, bsel.data(),
+                                            prod.data(), tiles, n_tiles, 1, nops);
     });
   } else if (m > 0) {
     const __half* ah[4] = {oph[0], oph[1], oph[2], nops > 3 ? oph[3] : oph[2]};

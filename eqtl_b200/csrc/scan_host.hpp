@@ -92,9 +92,10 @@ int sm_count(eqtl_ctx* ctx);
 // gene-side hi/lo operands of accumulator j ([rows_a, k_pad]); b_*[0..1] the
 // SNP-side pairs ([rows_b, k_pad]); bsel[j] picks the pair, prod[j] the
 // products. tiles: optional explicit tile list (device pointer) + count.
-// BLO = false: the SNP-side operands have no lo parts (exact; no product
-// may have bit 2), which lets more ring stages fit.
-template <int NT, int NACC, class EpiParams, bool BLO = true>
+// BL: where the SNP-side lo parts go (dev::kBLoStage, kBLoNone: exact
+// SNP operands, no product may have bit 2; kBLoPass: a second pass over K
+// for the accumulators whose products read them, which then need bit 1).
+template <int NT, int NACC, class EpiParams, int BL = dev::kBLoStage>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
@@ -108,13 +109,13 @@ namespace eqtl {
 template <class EpiParams>
 struct EpiOf;
 
-template <int NT, int NACC, class EpiParams, bool BLO>
+template <int NT, int NACC, class EpiParams, int BL>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
                    int n_tile_list, int ksplit, int n_acc) {
   using Epi = typename EpiOf<EpiParams>::type;
-  using C = dev::TileCfg<NT, NACC, BLO>;
+  using C = dev::TileCfg<NT, NACC, BL>;
   dev::TileMaps maps;
   std::memset(&maps, 0, sizeof(maps));
   EQTL_CHECK(n_acc >= 1 && n_acc <= dev::kMaxAcc && (n_acc == NACC || Epi::kGrouped), EQTL_E_INTERNAL,
@@ -142,7 +143,10 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   for (int j = 0; j < dev::kMaxAcc; ++j) {
     sh.bsel[j] = j < n_acc ? bsel[j] : 0;
     sh.prod[j] = j < n_acc ? prod[j] : 0;
-    EQTL_CHECK(BLO || !(sh.prod[j] & 2), EQTL_E_INTERNAL, "tile kernel: hi*lo product without SNP-side lo parts");
+    EQTL_CHECK(BL != dev::kBLoNone || !(sh.prod[j] & 2), EQTL_E_INTERNAL,
+               "tile kernel: hi*lo product without SNP-side lo parts");
+    EQTL_CHECK(BL != dev::kBLoPass || !(sh.prod[j] & 2) || (sh.prod[j] & 1), EQTL_E_INTERNAL,
+               "tile kernel: a second-pass hi*lo product needs the hi*hi product of the first pass");
   }
   sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
   sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
@@ -165,11 +169,11 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   const int smem = C::SMEM_BYTES + Epi::kSmemBytes;
   EQTL_CHECK(smem <= 232448, EQTL_E_INTERNAL, "tile kernel shared memory over the 227 KB limit");
   if (bf16) {
-    auto kern = dev::tile_kernel<NT, NACC, 1u, Epi, BLO>;
+    auto kern = dev::tile_kernel<NT, NACC, 1u, Epi, BL>;
     EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     kern<<<grid, dev::kTileThreads, smem, ctx->stream>>>(maps, sh, ep);
   } else {
-    auto kern = dev::tile_kernel<NT, NACC, 0u, Epi, BLO>;
+    auto kern = dev::tile_kernel<NT, NACC, 0u, Epi, BL>;
     EQTL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     kern<<<grid, dev::kTileThreads, smem, ctx->stream>>>(maps, sh, ep);
   }

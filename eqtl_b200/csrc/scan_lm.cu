@@ -409,8 +409,8 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
       if (raw) {
         const __half* bh[1] = {ctx->rot.raw.p};
         const int prod[1] = {5};
-        launch_tile_n<256, 1, LmEpiParams, false>(ctx, false, ep, ah, al, G, bh, bh, m, k_pad, bsel, prod, tiles,
-                                                  n_tiles);
+        launch_tile_n<256, 1, LmEpiParams, dev::kBLoNone>(ctx, false, ep, ah, al, G, bh, bh, m, k_pad, bsel, prod,
+                                                          tiles, n_tiles);
       } else {
         const __half* bh[1] = {g.gc_hi.p};
         const __half* bl[1] = {g.gc_lo.p};

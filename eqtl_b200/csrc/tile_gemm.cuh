@@ -75,13 +75,20 @@ struct TileShape {
   uint32_t* status;       // device status word (DevStatus)
 };
 
-// BLO = false: no product reads a SNP-side lo part (exact SNP operands), so
-// a ring stage holds A hi, A lo and B hi only and more stages fit.
-template <int NT, int NACC, bool BLO = true>
+// Where a SNP-side lo part goes (BL):
+//   kBLoStage  in the same ring stage as A hi, A lo and B hi (four parts);
+//   kBLoNone   nowhere: no product reads one (exact SNP operands);
+//   kBLoPass   in a second pass over K for the accumulators whose products
+//              read it (hi*lo from A hi and B lo; hi*hi and lo*hi in the
+//              first pass).
+// With kBLoNone and kBLoPass a stage holds three parts, so more stages fit.
+constexpr int kBLoStage = 0, kBLoNone = 1, kBLoPass = 2;
+
+template <int NT, int NACC, int BL = kBLoStage>
 struct TileCfg {
   static constexpr int A_BYTES = kTileM * kChunkK * 2;
   static constexpr int B_BYTES = NT * kChunkK * 2;
-  static constexpr int STAGE_BYTES = 2 * A_BYTES + (BLO ? 2 : 1) * B_BYTES;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + (BL == kBLoStage ? 2 : 1) * B_BYTES;
   static constexpr int STAGES = (196608 / STAGE_BYTES) < 2 ? 2 : (196608 / STAGE_BYTES > 6 ? 6 : 196608 / STAGE_BYTES);
   // TMEM is split into NSLOTS slots of NT columns; accumulator j of work
   // unit u lives in slot (u * NACC + j) % NSLOTS, so the next unit's first
@@ -129,11 +136,11 @@ __device__ __forceinline__ void tile_coords(const TileShape& sh, int t, int& ta,
   k1 = min(sh.kchunks, k0 + sh.kc_per_split);
 }
 
-template <int NT, int NACC, uint32_t AB_FMT, class Epi, bool BLO = true>
+template <int NT, int NACC, uint32_t AB_FMT, class Epi, int BL = kBLoStage>
 __global__ void __launch_bounds__(kTileThreads, 1)
     tile_kernel(const __grid_constant__ TileMaps maps, const TileShape sh,
                 const __grid_constant__ typename Epi::Params ep) {
-  using C = TileCfg<NT, NACC, BLO>;
+  using C = TileCfg<NT, NACC, BL>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + C::STAGES * C::STAGE_BYTES);
@@ -189,27 +196,34 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         const int ra = ta * kTileM, rb = tb * NT;
         for (int j = 0; j < sh.n_acc && ok; ++j) {
           const int bp = sh.bsel[j];
-          // only the lo parts some product of this accumulator reads are loaded
-          const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = BLO && (sh.prod[j] & 2) != 0;
-          const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
-                                                       (b_lo ? C::B_BYTES : 0));
-          for (int kc = k0; kc < k1; ++kc) {
-            if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
-              ok = false;
-              break;
-            }
-            uint8_t* sb = smem + stage * C::STAGE_BYTES;
-            mbar_arrive_expect_tx(&full[stage], bytes);
-            tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
-            if (a_lo) tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
-            tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[2 * bp], &full[stage], kc * kChunkK, rb);
-            if (b_lo)
-              tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
-            issued[stage] = true;
-            issued_phase[stage] = phase;
-            if (++stage == C::STAGES) {
-              stage = 0;
-              phase ^= 1u;
+          const int pm = sh.prod[j];
+          const int npass = (BL == kBLoPass && (pm & 2)) ? 2 : 1;
+          for (int pass = 0; pass < npass && ok; ++pass) {
+            // only the parts some product of this pass reads are loaded;
+            // the second pass puts B lo in the B slot
+            const bool a_lo = pass == 0 && (pm & 4) != 0;
+            const bool b_lo_same = BL == kBLoStage && (pm & 2) != 0;
+            const int b_map = 2 * bp + (pass == 0 ? 0 : 1);
+            const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
+                                                         (b_lo_same ? C::B_BYTES : 0));
+            for (int kc = k0; kc < k1; ++kc) {
+              if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
+                ok = false;
+                break;
+              }
+              uint8_t* sb = smem + stage * C::STAGE_BYTES;
+              mbar_arrive_expect_tx(&full[stage], bytes);
+              tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
+              if (a_lo) tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
+              tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[b_map], &full[stage], kc * kChunkK, rb);
+              if (b_lo_same)
+                tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
+              issued[stage] = true;
+              issued_phase[stage] = phase;
+              if (++stage == C::STAGES) {
+                stage = 0;
+                phase ^= 1u;
+              }
             }
           }
         }
@@ -254,35 +268,44 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             tc_fence_after();
             const uint32_t d = tmem_base + static_cast<uint32_t>(slot * NT);
             const int pm = sh.prod[j0 + jj];
-            for (int kc = k0; kc < k1; ++kc) {
-              if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
-                ok = false;
-                break;
-              }
-              tc_fence_after();
-              const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
-              const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
-              const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
+            const int npass = (BL == kBLoPass && (pm & 2)) ? 2 : 1;
+            for (int pass = 0; pass < npass && ok; ++pass) {
+              for (int kc = k0; kc < k1; ++kc) {
+                if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
+                  ok = false;
+                  break;
+                }
+                tc_fence_after();
+                const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
+                const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
+                const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
 #pragma unroll
-              for (int k = 0; k < kChunkK / 16; ++k) {
-                const uint32_t off = static_cast<uint32_t>(k * 32);
-                uint32_t accum = (kc > k0 || k > 0) ? 1u : 0u;
-                if (pm & 1) {
-                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-                  accum = 1u;
+                for (int k = 0; k < kChunkK / 16; ++k) {
+                  const uint32_t off = static_cast<uint32_t>(k * 32);
+                  // the first product of the accumulator's first pass over
+                  // its K range starts it; every later one adds
+                  uint32_t accum = (pass > 0 || kc > k0 || k > 0) ? 1u : 0u;
+                  if (pass > 0) {  // hi*lo: A hi against B lo (in the B slot)
+                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, 1u);
+                    continue;
+                  }
+                  if (pm & 1) {
+                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                    accum = 1u;
+                  }
+                  if (BL == kBLoStage && (pm & 2)) {
+                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
+                    accum = 1u;
+                  }
+                  if (pm & 4) {
+                    umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                  }
                 }
-                if (BLO && (pm & 2)) {
-                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
-                  accum = 1u;
+                umma_commit(&empty[stage]);
+                if (++stage == C::STAGES) {
+                  stage = 0;
+                  phase ^= 1u;
                 }
-                if (pm & 4) {
-                  umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-                }
-              }
-              umma_commit(&empty[stage]);
-              if (++stage == C::STAGES) {
-                stage = 0;
-                phase ^= 1u;
               }
             }
           }
