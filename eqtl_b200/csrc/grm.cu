@@ -233,6 +233,63 @@ struct GrmEpi {
   __device__ void finish() {}
 };
 
+// The same sums over a work item made of K sub-ranges: each sub-range's
+// FP32 tensor-core sums (256 SNPs, so the accumulation's drift stays near
+// 1e-6) are added into per-thread FP32 registers (round to nearest, so
+// across sub-ranges the error is a random walk), and the work item's total
+// goes to the FP64 sums with one atomic per element. The joint-missing
+// counts are exact integers in every sub-range and are added where
+// non-zero. Tiles of 128 x 128: two 16-column chunks per thread.
+struct GrmSubEpi {
+  static constexpr bool kGrouped = false;
+  static constexpr bool kChunkIdx = true;
+  static constexpr int kMaxChunks = 2;
+  static constexpr int kSmemBytes = 0;
+  using Params = GrmEpiParams;
+  const Params& P;
+  int row = 0;
+  int64_t col0 = 0;
+  int cbase[kMaxChunks];
+  float acc[kMaxChunks][16];
+  __device__ GrmSubEpi(const Params& p, const TileShape&, uint8_t*) : P(p) {}
+  __device__ void init(int, int) {}
+  __device__ void begin_tile(int r, int64_t c0) {
+    row = r;
+    col0 = c0;
+#pragma unroll
+    for (int ci = 0; ci < kMaxChunks; ++ci) {
+      cbase[ci] = -1;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc[ci][j] = 0.0f;
+    }
+  }
+  template <int NACC>
+  __device__ void chunk_at(int ci, int c, const float (&v)[NACC][16]) {
+    cbase[ci] = c;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc[ci][j] += v[0][j];
+    if (row >= P.n) return;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t cc = col0 + c + j;
+      if (cc < P.n && v[1][j] != 0.0f) atomicAdd(P.J + static_cast<int64_t>(row) * P.n + cc, __float2int_rn(v[1][j]));
+    }
+  }
+  __device__ void end_tile() {
+    if (row >= P.n) return;
+#pragma unroll
+    for (int ci = 0; ci < kMaxChunks; ++ci) {
+      if (cbase[ci] < 0) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int64_t cc = col0 + cbase[ci] + j;
+        if (cc < P.n) atomicAdd(P.A + static_cast<int64_t>(row) * P.n + cc, static_cast<double>(acc[ci][j]));
+      }
+    }
+  }
+  __device__ void finish() {}
+};
+
 __global__ void grm_finalize_kernel(int n, const unsigned long long* __restrict__ m_used_p,
                                     const double* __restrict__ A, const int* __restrict__ J, double* K,
                                     int32_t* Npk) {
@@ -257,10 +314,18 @@ template <>
 struct EpiOf<dev::GrmEpiParams> {
   using type = dev::GrmEpi;
 };
+// the sub-range form of the same sums (its own parameter type, so that the
+// launcher picks its epilogue)
+struct GrmSubParams : dev::GrmEpiParams {};
+template <>
+struct EpiOf<GrmSubParams> {
+  using type = dev::GrmSubEpi;
+};
 
 // K chunks (of 64 SNPs) summed in one FP32 tensor-core accumulator before
 // the FP64 sum across ranges.
 constexpr int kGrmChunksPerRange = 8;
+constexpr int kGrmChunksPerSub = 4;
 
 // Computes the GRM of the loaded genotypes. K: device [n, n] (row-major ==
 // column-major, symmetric). Returns the number of SNPs used.
@@ -332,32 +397,31 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   J.alloc(static_cast<size_t>(n) * n);
   A.zero(st);
   J.zero(st);
-  GrmEpiParams ep{n, A.p, J.p};
+  GrmSubParams ep{};
+  ep.n = n;
+  ep.A = A.p;
+  ep.J = J.p;
   const __half* ah[2] = {zh.p, mk.p};
   const __half* al[2] = {zl.p, mk.p};
   const __half* bh[2] = {zh.p, mk.p};
   const __half* bl[2] = {zl.p, mk.p};
   const int bsel[2] = {0, 1}, prod[2] = {7, 1};
-  // K is symmetric: only the tiles of 128 rows x 256 columns that hold some
-  // element with row >= column (the tiles wholly above the diagonal are
-  // skipped)
+  // K is symmetric: only the tiles of 128 x 128 on or below the diagonal
   std::vector<int2> lower;
-  for (int tb = 0; tb < (n + 255) / 256; ++tb)
-    for (int ta = 0; ta < (n + 127) / 128; ++ta)
-      if (128 * ta + 127 >= 256 * tb) lower.push_back(make_int2(ta, tb));
+  for (int tb = 0; tb < (n + 127) / 128; ++tb)
+    for (int ta = tb; ta < (n + 127) / 128; ++ta) lower.push_back(make_int2(ta, tb));
   ws.grm_tiles.upload(lower.data(), lower.size(), st);
   const int tiles = static_cast<int>(lower.size());
   // The tensor cores' FP32 accumulation drifts with the number of K steps
   // summed into one accumulator (about 2.6e-7 of the running sum per step,
   // the same sign for the large positive sums of K's diagonal and of
-  // related pairs), so a K range holds at most kGrmChunksPerRange chunks
-  // of 64 SNPs; the ranges meet in FP64.
-  const int kchunks = static_cast<int>(m_pad / 64);
-  const int ksplit = std::max({1, (4 * sm_count(ctx) + tiles - 1) / tiles,
-                               (kchunks + kGrmChunksPerRange - 1) / kGrmChunksPerRange});
+  // related pairs), so the accumulators restart every kGrmChunksPerSub
+  // chunks of 64 SNPs and the epilogue sums the sub-ranges (GrmSubEpi);
+  // the K ranges of a tile (enough of them for every SM) meet in FP64.
+  const int ksplit = std::max(1, (4 * sm_count(ctx) + tiles - 1) / tiles);
   // the GRM operands are FP16 regardless of the scan precision
-  launch_tile_n<256, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, ws.grm_tiles.p,
-                        tiles, ksplit);
+  launch_tile_n<128, 2>(ctx, false, ep, ah, al, n, bh, bl, n, static_cast<int>(m_pad), bsel, prod, ws.grm_tiles.p,
+                        tiles, ksplit, 2, kGrmChunksPerSub);
   K.alloc(static_cast<size_t>(n) * n);
   Npk.alloc(static_cast<size_t>(n) * (n + 1) / 2);
   const int64_t tot = static_cast<int64_t>(n) * n;

@@ -92,14 +92,14 @@ int sm_count(eqtl_ctx* ctx);
 // gene-side hi/lo operands of accumulator j ([rows_a, k_pad]); b_*[0..1] the
 // SNP-side pairs ([rows_b, k_pad]); bsel[j] picks the pair, prod[j] the
 // products. tiles: optional explicit tile list (device pointer) + count.
-// BL: where the SNP-side lo parts go (dev::kBLoStage, kBLoNone: exact
-// SNP operands, no product may have bit 2; kBLoPass: a second pass over K
-// for the accumulators whose products read them, which then need bit 1).
+// BL: where the SNP-side lo parts go (dev::kBLoStage; kBLoNone: exact SNP
+// operands, no product may have bit 2, and more ring stages fit). kc_sub:
+// K chunks per sub-range (0: none; single-group epilogues only).
 template <int NT, int NACC, class EpiParams, int BL = dev::kBLoStage>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
-                   int n_tile_list = 0, int ksplit = 1, int n_acc = NACC);
+                   int n_tile_list = 0, int ksplit = 1, int n_acc = NACC, int kc_sub = 0);
 
 }  // namespace eqtl
 
@@ -113,7 +113,7 @@ template <int NT, int NACC, class EpiParams, int BL>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
-                   int n_tile_list, int ksplit, int n_acc) {
+                   int n_tile_list, int ksplit, int n_acc, int kc_sub) {
   using Epi = typename EpiOf<EpiParams>::type;
   using C = dev::TileCfg<NT, NACC, BL>;
   dev::TileMaps maps;
@@ -145,8 +145,6 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
     sh.prod[j] = j < n_acc ? prod[j] : 0;
     EQTL_CHECK(BL != dev::kBLoNone || !(sh.prod[j] & 2), EQTL_E_INTERNAL,
                "tile kernel: hi*lo product without SNP-side lo parts");
-    EQTL_CHECK(BL != dev::kBLoPass || !(sh.prod[j] & 2) || (sh.prod[j] & 1), EQTL_E_INTERNAL,
-               "tile kernel: a second-pass hi*lo product needs the hi*hi product of the first pass");
   }
   sh.tiles_a = static_cast<int>((rows_a + dev::kTileM - 1) / dev::kTileM);
   sh.tiles_b = static_cast<int>((rows_b + NT - 1) / NT);
@@ -155,6 +153,9 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   sh.kc_per_split = (sh.kchunks + sh.ksplit - 1) / sh.ksplit;
   sh.ksplit = (sh.kchunks + sh.kc_per_split - 1) / sh.kc_per_split;  // no empty ranges
   sh.n_tiles = (tile_list ? n_tile_list : sh.tiles_a * sh.tiles_b) * sh.ksplit;
+  EQTL_CHECK(kc_sub >= 0 && (kc_sub == 0 || (!Epi::kGrouped && !dev::IsTwoPhase<Epi>::value)), EQTL_E_INTERNAL,
+             "tile kernel: K sub-ranges need a single-group epilogue");
+  sh.kc_sub = kc_sub;
   // gene-side tiles per raster group: keep the group's A operands (hi+lo of
   // every accumulator) within ~48 MB of L2
   {

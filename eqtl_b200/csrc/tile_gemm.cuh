@@ -45,6 +45,13 @@ template <class E, class = void>
 struct IsTwoPhase : std::false_type {};
 template <class E>
 struct IsTwoPhase<E, std::void_t<decltype(E::kTwoPhase)>> : std::bool_constant<E::kTwoPhase> {};
+// Epilogues that keep per-chunk state in registers (E::kChunkIdx): their
+// chunks come from a fully unrolled loop with the chunk index known at
+// compile time (chunk_at).
+template <class E, class = void>
+struct HasChunkIdx : std::false_type {};
+template <class E>
+struct HasChunkIdx<E, std::void_t<decltype(E::kChunkIdx)>> : std::bool_constant<E::kChunkIdx> {};
 
 constexpr int kMaxAcc = 34;  // accumulators of one tile over all its groups (LMM: p + 2, p <= 32)
 constexpr int kEpiWarps = 16;
@@ -71,18 +78,18 @@ struct TileShape {
   int ksplit;             // K ranges per output tile (split-K); 1 = whole K
   int group_a;            // gene-side tiles per raster group (L2 residency of the A operands)
   int kc_per_split;       // K chunks per range
+  int kc_sub;             // K chunks per sub-range (0: the whole range). Each sub-range starts its
+                          // accumulators afresh and goes through the epilogue on its own, which
+                          // sums the sub-ranges of a work item itself (single-group epilogues)
   const int2* tile_list;  // optional explicit (tile_a, tile_b) list (banded scans); null = dense
   uint32_t* status;       // device status word (DevStatus)
 };
 
 // Where a SNP-side lo part goes (BL):
 //   kBLoStage  in the same ring stage as A hi, A lo and B hi (four parts);
-//   kBLoNone   nowhere: no product reads one (exact SNP operands);
-//   kBLoPass   in a second pass over K for the accumulators whose products
-//              read it (hi*lo from A hi and B lo; hi*hi and lo*hi in the
-//              first pass).
-// With kBLoNone and kBLoPass a stage holds three parts, so more stages fit.
-constexpr int kBLoStage = 0, kBLoNone = 1, kBLoPass = 2;
+//   kBLoNone   nowhere: no product reads one (exact SNP operands), so a
+//              stage holds three parts and more stages fit.
+constexpr int kBLoStage = 0, kBLoNone = 1;
 
 template <int NT, int NACC, int BL = kBLoStage>
 struct TileCfg {
@@ -194,36 +201,32 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         int ta, tb, k0, k1;
         tile_coords(sh, t, ta, tb, k0, k1);
         const int ra = ta * kTileM, rb = tb * NT;
+        const int ksub = sh.kc_sub > 0 ? sh.kc_sub : k1 - k0;
+        for (int q0 = k0; q0 < k1 && ok; q0 += ksub)
         for (int j = 0; j < sh.n_acc && ok; ++j) {
+          const int q1 = min(k1, q0 + ksub);
           const int bp = sh.bsel[j];
-          const int pm = sh.prod[j];
-          const int npass = (BL == kBLoPass && (pm & 2)) ? 2 : 1;
-          for (int pass = 0; pass < npass && ok; ++pass) {
-            // only the parts some product of this pass reads are loaded;
-            // the second pass puts B lo in the B slot
-            const bool a_lo = pass == 0 && (pm & 4) != 0;
-            const bool b_lo_same = BL == kBLoStage && (pm & 2) != 0;
-            const int b_map = 2 * bp + (pass == 0 ? 0 : 1);
-            const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
-                                                         (b_lo_same ? C::B_BYTES : 0));
-            for (int kc = k0; kc < k1; ++kc) {
-              if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
-                ok = false;
-                break;
-              }
-              uint8_t* sb = smem + stage * C::STAGE_BYTES;
-              mbar_arrive_expect_tx(&full[stage], bytes);
-              tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
-              if (a_lo) tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
-              tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[b_map], &full[stage], kc * kChunkK, rb);
-              if (b_lo_same)
-                tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
-              issued[stage] = true;
-              issued_phase[stage] = phase;
-              if (++stage == C::STAGES) {
-                stage = 0;
-                phase ^= 1u;
-              }
+          // only the lo parts some product of this accumulator reads are loaded
+          const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = BL == kBLoStage && (sh.prod[j] & 2) != 0;
+          const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
+                                                       (b_lo ? C::B_BYTES : 0));
+          for (int kc = q0; kc < q1; ++kc) {
+            if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
+              ok = false;
+              break;
+            }
+            uint8_t* sb = smem + stage * C::STAGE_BYTES;
+            mbar_arrive_expect_tx(&full[stage], bytes);
+            tma_load_2d(sb, &maps.a[2 * j], &full[stage], kc * kChunkK, ra);
+            if (a_lo) tma_load_2d(sb + C::A_BYTES, &maps.a[2 * j + 1], &full[stage], kc * kChunkK, ra);
+            tma_load_2d(sb + 2 * C::A_BYTES, &maps.b[2 * bp], &full[stage], kc * kChunkK, rb);
+            if (b_lo)
+              tma_load_2d(sb + 2 * C::A_BYTES + C::B_BYTES, &maps.b[2 * bp + 1], &full[stage], kc * kChunkK, rb);
+            issued[stage] = true;
+            issued_phase[stage] = phase;
+            if (++stage == C::STAGES) {
+              stage = 0;
+              phase ^= 1u;
             }
           }
         }
@@ -253,7 +256,10 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       for (int t = blockIdx.x; t < sh.n_tiles && ok; t += gridDim.x) {
         int ta, tb, k0, k1;
         tile_coords(sh, t, ta, tb, k0, k1);
+        const int ksub = sh.kc_sub > 0 ? sh.kc_sub : k1 - k0;
+        for (int q0 = k0; q0 < k1 && ok; q0 += ksub)
         for (int grp = 0; grp < sh.n_groups && ok; ++grp, slot0 = (slot0 + NACC) % C::NSLOTS) {
+          const int q1 = min(k1, q0 + ksub);
           const int j0 = grp * NACC;
           const int nv = min(NACC, sh.n_acc - j0);
           int last = 0;
@@ -268,44 +274,37 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             tc_fence_after();
             const uint32_t d = tmem_base + static_cast<uint32_t>(slot * NT);
             const int pm = sh.prod[j0 + jj];
-            const int npass = (BL == kBLoPass && (pm & 2)) ? 2 : 1;
-            for (int pass = 0; pass < npass && ok; ++pass) {
-              for (int kc = k0; kc < k1; ++kc) {
-                if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
-                  ok = false;
-                  break;
-                }
-                tc_fence_after();
-                const uint32_t s0 = smem_u32(smem + stage * C::STAGE_BYTES);
-                const uint32_t sa0 = s0, sa1 = s0 + C::A_BYTES;
-                const uint32_t sb0 = s0 + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
+            for (int kc = q0; kc < q1; ++kc) {
+              if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              const uint32_t sbase = smem_u32(smem + stage * C::STAGE_BYTES);
+              const uint32_t sa0 = sbase, sa1 = sbase + C::A_BYTES;
+              const uint32_t sb0 = sbase + 2 * C::A_BYTES, sb1 = sb0 + C::B_BYTES;
 #pragma unroll
-                for (int k = 0; k < kChunkK / 16; ++k) {
-                  const uint32_t off = static_cast<uint32_t>(k * 32);
-                  // the first product of the accumulator's first pass over
-                  // its K range starts it; every later one adds
-                  uint32_t accum = (pass > 0 || kc > k0 || k > 0) ? 1u : 0u;
-                  if (pass > 0) {  // hi*lo: A hi against B lo (in the B slot)
-                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, 1u);
-                    continue;
-                  }
-                  if (pm & 1) {
-                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-                    accum = 1u;
-                  }
-                  if (BL == kBLoStage && (pm & 2)) {
-                    umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
-                    accum = 1u;
-                  }
-                  if (pm & 4) {
-                    umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
-                  }
+              for (int k = 0; k < kChunkK / 16; ++k) {
+                const uint32_t off = static_cast<uint32_t>(k * 32);
+                // the first product of a (sub-)range starts the accumulator;
+                // every later one adds
+                uint32_t accum = (kc > q0 || k > 0) ? 1u : 0u;
+                if (pm & 1) {
+                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                  accum = 1u;
                 }
-                umma_commit(&empty[stage]);
-                if (++stage == C::STAGES) {
-                  stage = 0;
-                  phase ^= 1u;
+                if (BL == kBLoStage && (pm & 2)) {
+                  umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb1 + off), idesc, accum);
+                  accum = 1u;
                 }
+                if (pm & 4) {
+                  umma_f16(d, smem_desc_sw128(sa1 + off), smem_desc_sw128(sb0 + off), idesc, accum);
+                }
+              }
+              umma_commit(&empty[stage]);
+              if (++stage == C::STAGES) {
+                stage = 0;
+                phase ^= 1u;
               }
             }
           }
@@ -340,6 +339,8 @@ __global__ void __launch_bounds__(kTileThreads, 1)
       tile_coords(sh, t, ta, tb, k0, k1);
       epi.begin_tile(ta * kTileM + row, tb * NT);
       bool eok = true;
+      const int ksub = sh.kc_sub > 0 ? sh.kc_sub : k1 - k0;
+      for (int q0 = k0; q0 < k1 && eok; q0 += ksub)
       for (int grp = 0; grp < sh.n_groups; ++grp, slot0 = (slot0 + NACC) % C::NSLOTS) {
         const int j0 = grp * NACC;
         const int nv = min(NACC, sh.n_acc - j0);
@@ -392,6 +393,18 @@ __global__ void __launch_bounds__(kTileThreads, 1)
           tc_fence_before();
           for (int jj = N1; jj < nv; ++jj) mbar_arrive(&sempty[(slot0 + jj) % C::NSLOTS]);
           continue;  // slots released above
+        } else if constexpr (HasChunkIdx<Epi>::value) {
+          constexpr int NCH = NT / (16 * kSub);
+          static_assert(NT % (16 * kSub) == 0 && NCH <= Epi::kMaxChunks, "indexed epilogue: chunks per warp");
+#pragma unroll
+          for (int ci = 0; ci < NCH; ++ci) {
+            const int c = 16 * sub + 16 * kSub * ci;
+            float v[NACC][16];
+#pragma unroll
+            for (int jj = 0; jj < NACC; ++jj) tmem_ld16(col(jj) + static_cast<uint32_t>(c), v[jj]);
+            tmem_wait_ld();
+            epi.template chunk_at<NACC>(ci, c, v);
+          }
         } else {
 #pragma unroll 1
           for (int c = 16 * sub; c < NT; c += 16 * kSub) {
