@@ -927,13 +927,15 @@ struct LmmEpi {
   template <int N>
   __device__ void pre_chunk(int ci, int c, const float (&v)[N][16]) {
     static_assert(N == P + 1, "phase-1 accumulators");
+    float al[16];  // RAW: alpha of each SNP (the array is padded past the last tile)
+    if constexpr (RAW) load16(Pr.snp_alpha + snp0 + c, al);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const float gg = v[0][j] * u[P + 1];
       float S = gg;
       float a[P];
-      float us = 1.0f;  // RAW: alpha of the SNP
-      if constexpr (RAW) us = __ldg(Pr.snp_alpha + snp0 + c + j);
+      float us = 1.0f;
+      if constexpr (RAW) us = al[j];
 #pragma unroll
       for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * (us * u[1 + k]);
 #pragma unroll
@@ -954,12 +956,32 @@ struct LmmEpi {
     if (!gvalid || s0 >= Pr.m) return;
     uint32_t okw[4];
     load_flags16(Pr.snp_ok + s0, okw);
+    float al[16];
+    if constexpr (RAW) load16(Pr.snp_alpha + s0, al);
+    if (!GLM && tt.lt_u) {  // uniform across the launch
+      float uu[16];
+      bool valid[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int64_t s = s0 + j;
+        valid[j] = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
+        float num = v[0][j] * u[0];
+        if constexpr (RAW) num *= al[j];
+        const float S = ci == 0 ? S0[j] : S1[j];
+        const float r = num * __fdividef(num, S) * inv_rss;
+        const float omr = 1.0f - r;
+        uu[j] = S > 1e-15f && omr > 0.0f ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2, never NaN
+        if (!valid[j]) uu[j] = 0.0f;
+      }
+      screen16_cubic(tt, uu, valid, u_cand, Pr.out, gene, s0, acc);
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int64_t s = s0 + j;
       const bool valid = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
       float num = v[0][j] * u[0];
-      if constexpr (RAW) num *= __ldg(Pr.snp_alpha + s);
+      if constexpr (RAW) num *= al[j];
       const float S = ci == 0 ? S0[j] : S1[j];
       float u;
       if constexpr (GLM) {

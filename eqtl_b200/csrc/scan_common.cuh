@@ -144,11 +144,70 @@ __device__ __forceinline__ void load_flags16(const uint8_t* p, uint32_t (&w)[4])
 }
 __device__ __forceinline__ bool flag16(const uint32_t (&w)[4], int j) { return (w[j >> 2] >> (8 * (j & 3))) & 0xFFu; }
 
+// 16 floats starting at a multiple of 16 of an array padded past its last
+// tile (four 16-byte loads).
+__device__ __forceinline__ void load16(const float* p, float (&v)[16]) {
+  const float4* p4 = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float4 x = __ldg(p4 + q);
+    v[4 * q] = x.x;
+    v[4 * q + 1] = x.y;
+    v[4 * q + 2] = x.z;
+    v[4 * q + 3] = x.w;
+  }
+}
+
 __device__ __forceinline__ void emit_candidate(const GeneOut& out, int g, int64_t s, bool deferred, bool tiny) {
   const unsigned int idx = atomicAdd(out.cand_count, 1u);
   if (idx < out.cand_cap)
     out.cand[idx] = make_int2(g, static_cast<int>(static_cast<uint32_t>(s) | (deferred ? kCandDeferred : 0u) |
                                                   (tiny ? kCandTiny : 0u)));
+}
+
+// The ACAT screen of one gene's 16 pairs s0 .. s0 + 15 with the per-interval
+// cubics (acat_screen_u's lt_u branch, T.lt_u set), for epilogues whose u =
+// t^2 is never NaN (a pair outside the scan, or with p = 1, has u = 0). With
+// u_tiny > 0:
+//   tiny      0 < u < u_tiny         deferred   tiny or u >= u_defer
+//   ACAT      u_tiny <= u < u_defer  candidate  u >= min(u_cand, u_defer) or tiny
+// The counts, the FP32 term sum and the chunk's best go into acc without
+// per-pair flag structs; candidates are emitted as they are found.
+__device__ __forceinline__ void screen16_cubic(const TTable& tt, const float (&u)[16], const bool (&valid)[16],
+                                               float u_cand, const GeneOut& out, int gene, int64_t s0,
+                                               GeneAcc& acc) {
+  const float uc = fminf(u_cand, tt.u_defer);
+  const float cmax = static_cast<float>(tt.na) - 1e-3f, tmax = static_cast<float>(tt.nq) - 1e-3f;
+  float sum = 0.0f, bkey = -1.0f;
+  int ntest = 0, nused = 0, bj = 0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float uj = u[j];
+    const bool central = uj <= tt.uq0;
+    const float x = fminf(central ? uj * tt.dqc_inv : (uj - tt.uq0) * tt.dq_inv, central ? cmax : tmax);
+    const int i = static_cast<int>(x);
+    const float f = x - static_cast<float>(i);
+    const float4 a = (central ? tt.c1q : tt.ltq)[i];
+    const float y = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
+    const float term = central ? y * rsqrtf(uj) : y;
+    const bool lo = uj < tt.u_tiny;
+    const bool use = !lo && uj < tt.u_defer;
+    sum += use ? term : 0.0f;
+    nused += use ? 1 : 0;
+    ntest += valid[j] ? 1 : 0;
+    const float key = valid[j] ? uj : -1.0f;
+    bj = key > bkey ? j : bj;
+    bkey = fmaxf(key, bkey);
+    if (uj >= uc || (lo && uj > 0.0f)) emit_candidate(out, gene, s0 + j, lo || uj >= tt.u_defer, lo);
+  }
+  acc.tested += ntest;
+  acc.used += nused;
+  acc.chunk_acat += sum;
+  if (bkey >= 0.0f && bkey > acc.chunk_key) {
+    acc.chunk_key = bkey;
+    acc.chunk_snp = static_cast<uint32_t>(s0 + bj);
+  }
+  acc.end_chunk();
 }
 
 }  // namespace dev

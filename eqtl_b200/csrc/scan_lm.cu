@@ -112,50 +112,20 @@ struct LmEpi {
     }
     acc.end_chunk();
   }
-  // The same screen with the per-interval cubics (acat_screen_u's lt_u
-  // branch), written out for the LM's pairs: u is never NaN here (a pair
-  // outside the scan or with p = 1 has u = 0), so with u_tiny > 0
-  //   tiny      0 < u < u_tiny         deferred   tiny or u >= u_defer
-  //   ACAT      u_tiny <= u < u_defer  candidate  u >= min(u_cand, u_defer) or tiny
-  // and the counts, the FP32 term sum and the chunk's best stay in
-  // registers without per-pair flags.
+  // The same screen with the per-interval cubics (screen16_cubic): u is
+  // never NaN here (a pair outside the scan or with p = 1 has u = 0).
   __device__ void chunk_cubic(int64_t s0, const float (&v)[16], const float (&igv)[16]) {
-    const float uc = fminf(u_cand, tt.u_defer);
-    const float cmax = static_cast<float>(tt.na) - 1e-3f, tmax = static_cast<float>(tt.nq) - 1e-3f;
-    float sum = 0.0f, bkey = -1.0f;
-    int ntest = 0, nused = 0, bj = 0;
+    float u[16];
+    bool valid[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const bool valid = igv[j] >= 0.0f && acc.in_scope(P.win, s0 + j);
-      const float ig = valid ? igv[j] * w : 0.0f;
+      valid[j] = igv[j] >= 0.0f && acc.in_scope(P.win, s0 + j);
+      const float ig = valid[j] ? igv[j] * w : 0.0f;
       const float r = v[j] * v[j] * ig;
       const float omr = 1.0f - r;
-      const float u = (ig > 0.0f && omr > 0.0f) ? P.df * __fdividef(r, omr) : 0.0f;  // t^2
-      const bool central = u <= tt.uq0;
-      const float x = fminf(central ? u * tt.dqc_inv : (u - tt.uq0) * tt.dq_inv, central ? cmax : tmax);
-      const int i = static_cast<int>(x);
-      const float f = x - static_cast<float>(i);
-      const float4 a = (central ? tt.c1q : tt.ltq)[i];
-      const float y = fmaf(fmaf(fmaf(a.w, f, a.z), f, a.y), f, a.x);
-      const float term = central ? y * rsqrtf(u) : y;
-      const bool lo = u < tt.u_tiny;
-      const bool use = !lo && u < tt.u_defer;
-      sum += use ? term : 0.0f;
-      nused += use ? 1 : 0;
-      ntest += valid ? 1 : 0;
-      const float key = valid ? u : -1.0f;
-      bj = key > bkey ? j : bj;
-      bkey = fmaxf(key, bkey);
-      if (u >= uc || (lo && u > 0.0f)) emit_candidate(P.out, gene, s0 + j, lo || u >= tt.u_defer, lo);
+      u[j] = (ig > 0.0f && omr > 0.0f) ? P.df * __fdividef(r, omr) : 0.0f;  // t^2
     }
-    acc.tested += ntest;
-    acc.used += nused;
-    acc.chunk_acat += sum;
-    if (bkey >= 0.0f && bkey > acc.chunk_key) {
-      acc.chunk_key = bkey;
-      acc.chunk_snp = static_cast<uint32_t>(s0 + bj);
-    }
-    acc.end_chunk();
+    screen16_cubic(tt, u, valid, u_cand, P.out, gene, s0, acc);
   }
   __device__ void end_tile() {
     if (gvalid) acc.flush(P.out, gene);
