@@ -95,7 +95,9 @@ struct LmEpi {
       igv[4 * q + 3] = v4.w;
     }
     if (tt.lt_u) {  // uniform across the launch
-      chunk_cubic(s0, v[0], igv);
+      // a gw scan (no windows) skips the per-pair window test altogether
+      if (P.win.mode == kWinNone) chunk_cubic<false>(s0, v[0], igv);
+      else chunk_cubic<true>(s0, v[0], igv);
       return;
     }
 #pragma unroll
@@ -114,12 +116,13 @@ struct LmEpi {
   }
   // The same screen with the per-interval cubics (screen16_cubic): u is
   // never NaN here (a pair outside the scan or with p = 1 has u = 0).
+  template <bool WIN>
   __device__ void chunk_cubic(int64_t s0, const float (&v)[16], const float (&igv)[16]) {
     float u[16];
     bool valid[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      valid[j] = igv[j] >= 0.0f && acc.in_scope(P.win, s0 + j);
+      valid[j] = igv[j] >= 0.0f && (!WIN || acc.in_scope(P.win, s0 + j));
       const float ig = valid[j] ? igv[j] * w : 0.0f;
       const float r = v[j] * v[j] * ig;
       const float omr = 1.0f - r;
