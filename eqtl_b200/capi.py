@@ -26,7 +26,8 @@ EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "
            "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
            "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
-           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast", "eqtl_pheno_permute"]
+           "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast", "eqtl_pheno_permute",
+           "eqtl_geno_subset"]
 GRM_NOALLOC_MAX_N = 512
 STAGES = {"decode": 0, "grm": 1, "eigen": 2, "rotate": 3, "prep": 4, "scan": 5, "refine": 6}
 
@@ -91,6 +92,7 @@ def load() -> C.CDLL:
         lib.eqtl_lmm_rotate.argtypes = [vp]
         lib.eqtl_stream.argtypes = [vp, C.POINTER(vp)]
         lib.eqtl_pheno_load.argtypes = [vp, vp, vp, i32, i32, i32]
+        lib.eqtl_geno_subset.argtypes = [vp, vp, i32]
         lib.eqtl_pheno_permute.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32, C.c_uint64, vp, i32, vp]
         lib.eqtl_t_tail.argtypes = [vp, dp, vp, i64, i32, vp, vp, vp]
         lib.eqtl_lmm_basis.argtypes = [vp, vp, i32, vp, vp]
@@ -161,7 +163,7 @@ class Context:
                                                 n_file, _ptr(col), col.size, miss_hand, max_miss, maf_min,
                                                 _ptr(keep), _ptr(af), _ptr(nm), C.byref(nk)))
         self.n_kept = nk.value
-        self.n = col.size
+        self.n = self.n_full = col.size
         return keep.astype(bool), af, nm
 
     def load_dosage(self, ds: np.ndarray, sample_col, miss_hand: int = MISS_IMPUTE, max_miss: float = 0.8,
@@ -178,7 +180,7 @@ class Context:
                                                    max_miss, maf_min, _ptr(keep), _ptr(af), _ptr(nm),
                                                    C.byref(nk)))
         self.n_kept = nk.value
-        self.n = col.size
+        self.n = self.n_full = col.size
         return keep.astype(bool), af, nm
 
     def pheno_int(self, Y: np.ndarray) -> np.ndarray:
@@ -198,6 +200,17 @@ class Context:
         self._check(self.lib.eqtl_peer(self.h, _ptr(Y), n, G, k, max_iter, tol, _ptr(X0), _ptr(W0), _ptr(X),
                                        C.byref(it)))
         return X, it.value
+
+    def geno_subset(self, idx=None):
+        """eqtl_geno_subset: restrict the loaded genotypes to the analysis
+        samples idx (increasing positions); None restores them all."""
+        if idx is None:
+            self._check(self.lib.eqtl_geno_subset(self.h, None, 0))
+            self.n = self.n_full
+            return
+        idx = np.ascontiguousarray(idx, np.int32)
+        self._check(self.lib.eqtl_geno_subset(self.h, _ptr(idx), idx.size))
+        self.n = idx.size
 
     def dosage(self, lo: int, hi: int) -> np.ndarray:
         out = np.zeros((hi - lo, self.n), np.float64)

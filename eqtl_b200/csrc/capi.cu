@@ -744,6 +744,10 @@ int eqtl_t_tail(eqtl_ctx* ctx, double df, const float* t, int64_t n, int32_t use
   });
 }
 
+int eqtl_geno_subset(eqtl_ctx* ctx, const int32_t* idx, int32_t n_sub) {
+  return guarded(ctx, [&] { eqtl::geno_subset(ctx, idx, n_sub); });
+}
+
 int eqtl_pheno_load(eqtl_ctx* ctx, const double* Y, const double* X, int32_t n, int32_t n_genes, int32_t p) {
   return guarded(ctx, [&] {
     EQTL_CHECK(Y && X, EQTL_E_ARG, "null input");

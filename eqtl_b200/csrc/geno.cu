@@ -217,14 +217,16 @@ __global__ void __launch_bounds__(32 * kExpandWarps, 4)
 // vector v with the row is v . (dosage - mean) / alpha, alpha = +-1 / c.
 // SNPs that are not exact are counted in *inexact.
 __global__ void raw_operand_kernel(const uint8_t* __restrict__ bed, int64_t bps, const int32_t* __restrict__ col,
-                                   int n, int k_pad, const int64_t* __restrict__ kept, int64_t m_kept,
-                                   const int32_t* __restrict__ n_miss, const double* __restrict__ s1, __half* raw,
-                                   float* alpha, unsigned long long* inexact) {
+                                   int n, int n_full, int k_pad, const int64_t* __restrict__ kept,
+                                   int64_t m_kept, const int32_t* __restrict__ n_miss, const double* __restrict__ s1,
+                                   __half* raw, float* alpha, unsigned long long* inexact) {
   const int lane = threadIdx.x & 31;
   const int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (r >= m_kept) return;
   const int64_t s = __ldg(kept + r);
-  const long long n_ok = n - __ldg(n_miss + s);
+  // the imputation mean S / n_ok is over every analysis sample (n_full), also
+  // when the view (n samples) is a subset of them
+  const long long n_ok = n_full - __ldg(n_miss + s);
   const long long S = llrint(__ldg(s1 + s));
   long long a = S, b = n_ok;  // gcd(S, n_ok)
   while (b) {
@@ -351,6 +353,21 @@ void geno_decode(eqtl_ctx* ctx, const int32_t* sample_col, int miss_hand, double
     if (pass[s]) g.kept_h.push_back(s);
   g.m = static_cast<int64_t>(g.kept_h.size());
   g.kept.upload(g.kept_h.data(), g.kept_h.size(), st);
+  g.n_full = n;
+  g.col_full_h.assign(sample_col, sample_col + n);
+  g.subset = false;
+  geno_expand(ctx);
+}
+
+}  // namespace
+
+// The centred FP16 (or BF16) hi/lo operand of the kept SNPs over the current
+// sample view (g.col, g.n), missing calls at the imputation mean.
+void geno_expand(eqtl_ctx* ctx) {
+  Geno& g = ctx->geno;
+  cudaStream_t st = ctx->stream;
+  const int n = g.n;
+  const GenoRows src = g.rows();
   const size_t elems = static_cast<size_t>(g.m) * g.k_pad;
   g.gc_hi.alloc(elems);
   g.gc_lo.alloc(elems);
@@ -394,7 +411,75 @@ void geno_decode(eqtl_ctx* ctx, const int32_t* sample_col, int miss_hand, double
   EQTL_CUDA(cudaStreamSynchronize(st));
 }
 
+namespace {
+// Per kept SNP, one warp: sums of the imputed dosage and of its square over
+// the view's samples (the gate of a per-gene sample subset).
+__global__ void view_sums_kernel(GenoRows src, const int32_t* __restrict__ col, int n,
+                                 const int64_t* __restrict__ kept, int64_t m, const double* __restrict__ mu,
+                                 double* vs1, double* vs2) {
+  const int lane = threadIdx.x & 31;
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= m) return;
+  const int64_t s = kept[r];
+  const double mus = mu[s];
+  double a = 0.0, b = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double d0 = src.dosage(s, __ldg(col + i));
+    const double d = isnan(d0) ? mus : d0;
+    a += d;
+    b += d * d;
+  }
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    vs1[s] = a;
+    vs2[s] = b;
+  }
+}
 }  // namespace
+
+void geno_subset(eqtl_ctx* ctx, const int32_t* idx, int n_sub) {
+  Geno& g = ctx->geno;
+  EQTL_CHECK(g.m_all > 0 && g.n_full > 0, EQTL_E_STATE, "geno_subset: no genotypes loaded");
+  cudaStream_t st = ctx->stream;
+  std::vector<int32_t> col;
+  if (idx) {
+    EQTL_CHECK(n_sub >= 1 && n_sub <= g.n_full, EQTL_E_ARG, "geno_subset: bad subset size");
+    col.resize(n_sub);
+    for (int i = 0; i < n_sub; ++i) {
+      EQTL_CHECK(idx[i] >= 0 && idx[i] < g.n_full && (i == 0 || idx[i] > idx[i - 1]), EQTL_E_ARG,
+                 "geno_subset: indices must be increasing analysis-sample positions");
+      col[i] = g.col_full_h[idx[i]];
+    }
+  } else {
+    col = g.col_full_h;
+  }
+  const int n = static_cast<int>(col.size());
+  ctx->rot.m = 0;  // operands of the previous view
+  ctx->rot.raw_m = -1;
+  ctx->glm_ops.m = 0;
+  g.n = n;
+  g.k_pad = ((n + 63) / 64) * 64;
+  g.col.upload(col.data(), col.size(), st);
+  g.col_identity = true;
+  for (int i = 0; i < n; ++i) g.col_identity = g.col_identity && col[i] == i;
+  g.subset = idx != nullptr;
+  if (g.subset) {
+    g.vs1.alloc(static_cast<size_t>(g.m_all));
+    g.vs2.alloc(static_cast<size_t>(g.m_all));
+    g.vzero.alloc(static_cast<size_t>(g.m_all));
+    g.vzero.zero(st);
+    if (g.m > 0) {
+      ++ctx->launches;
+      view_sums_kernel<<<static_cast<unsigned>((g.m + 7) / 8), 256, 0, st>>>(g.rows(), g.col.p, n, g.kept.p, g.m,
+                                                                           g.mu.p, g.vs1.p, g.vs2.p);
+      EQTL_CUDA(cudaGetLastError());
+    }
+  }
+  geno_expand(ctx);
+}
 
 void geno_load(eqtl_ctx* ctx, const uint8_t* rows, int64_t m, int64_t bytes_per_snp, int n_file,
                const int32_t* sample_col, int n, int miss_hand, double max_miss, double maf_min) {
@@ -454,8 +539,8 @@ bool geno_raw_operand(eqtl_ctx* ctx) {
     ++ctx->launches;
     const int per_block = 8;
     raw_operand_kernel<<<static_cast<unsigned>((m + per_block - 1) / per_block), 32 * per_block, 0, st>>>(
-        g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.k_pad, g.kept.p, m, g.n_miss.p, g.s1.p, R.raw.p, R.alpha.p,
-        cnt.p);
+        g.bed.p, g.bytes_per_snp, g.col.p, g.n, g.n_full, g.k_pad, g.kept.p, m, g.n_miss.p, g.s1.p, R.raw.p,
+        R.alpha.p, cnt.p);
     EQTL_CUDA(cudaGetLastError());
   }
   unsigned long long bad = 0;

@@ -333,6 +333,7 @@ int64_t grm_compute(eqtl_ctx* ctx, DevBuf<double>& K, DevBuf<int32_t>& Npk) {
   using namespace dev;
   Geno& g = ctx->geno;
   EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "grm: no genotypes loaded");
+  EQTL_CHECK(!g.subset, EQTL_E_STATE, "grm: the GRM covers every analysis sample; restore the full sample view first");
   cudaStream_t st = ctx->stream;
   const int n = g.n;
   const int64_t m = g.m;

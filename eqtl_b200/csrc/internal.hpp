@@ -144,6 +144,19 @@ struct Geno {
   DevBuf<double> mu;      // [m_all] imputation mean
   DevBuf<int64_t> kept;   // [m] row index of kept SNP
   DevBuf<__half> gc_hi, gc_lo;  // [m, k_pad] (dosage - mean) * kGcScale, hi/lo FP16
+  // Sample view (eqtl_geno_subset): n, col and the operands above cover
+  // either every analysis sample of the load (n_full, col_full_h) or a
+  // subset of them; the kept SNPs and imputation means stay the load's.
+  int n_full = 0;
+  std::vector<int32_t> col_full_h;
+  bool subset = false;
+  // per-SNP sums of the imputed dosage and its square over a subset view
+  // ([m_all]), with zero missing counts, for the per-gene SNP gate
+  DevBuf<double> vs1, vs2;
+  DevBuf<int32_t> vzero;
+  const double* gate_s1() const { return subset ? vs1.p : s1.p; }
+  const double* gate_s2() const { return subset ? vs2.p : s2.p; }
+  const int32_t* gate_nmiss() const { return subset ? vzero.p : n_miss.p; }
   std::vector<int64_t> kept_h;
   std::vector<double> mu_h, af_h;
   std::vector<int32_t> n_miss_h;
@@ -337,6 +350,10 @@ int64_t grm_noalloc(eqtl_ctx* ctx, const uint8_t* bed, int64_t m, int64_t bps, c
                     int miss_hand, double max_miss, double maf_min, double* K, int32_t* Npk);
 void grm_noalloc_prepare(eqtl_ctx* ctx);
 bool geno_raw_operand(eqtl_ctx* ctx);
+void geno_expand(eqtl_ctx* ctx);
+// Restricts the genotype view to the analysis samples idx[0..n_sub) (null:
+// every analysis sample again).
+void geno_subset(eqtl_ctx* ctx, const int32_t* idx, int n_sub);
 void solver_release(eqtl_ctx* ctx);
 void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const double* X,
                    const std::vector<int2>& todo, eqtl_pair* out);

@@ -1949,7 +1949,7 @@ static void lmm_gate(eqtl_ctx* ctx) {
   if (m > 0) {
     ++ctx->launches;
     snp_gate_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, ctx->stream>>>(g.kept.p, m, g.n, g.mu.p,
-                                                                                     g.n_miss.p, g.s1.p, g.s2.p, ok.p);
+                                                                                     g.gate_nmiss(), g.gate_s1(), g.gate_s2(), ok.p);
     EQTL_CUDA(cudaGetLastError());
   }
 }
@@ -2570,6 +2570,7 @@ void scan_glm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, const
   Workspace& ws = ctx->ws;
   const int n = prm->n, G = prm->n_genes, p = prm->p;
   EQTL_CHECK(g.m_all > 0, EQTL_E_STATE, "scan_glm: no genotypes loaded");
+  EQTL_CHECK(!g.subset, EQTL_E_UNSUPPORTED, "scan_glm: the NB-GLM scan takes every analysis sample");
   EQTL_CHECK(n == g.n, EQTL_E_ARG, "scan_glm: n differs from the loaded genotypes");
   EQTL_CHECK(G > 0, EQTL_E_ARG, "scan_glm: no genes");
   EQTL_CHECK(g.m < (int64_t(1) << 30), EQTL_E_UNSUPPORTED, "scan_glm: more than 2^30 kept SNPs");

@@ -390,7 +390,7 @@ void scan_trans_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   if (m > 0) {
     ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
-        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.gate_nmiss(), g.gate_s1(), g.gate_s2(), ph.X.p, p,
         ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
     EQTL_CUDA(cudaGetLastError());
   }
@@ -501,7 +501,7 @@ void test_pairs_lm(eqtl_ctx* ctx, const eqtl_scan_params* prm, const double* Y, 
   if (m > 0) {
     ++ctx->launches;
     snp_gtg_kernel<<<static_cast<unsigned>((m + 7) / 8), 256, 0, st>>>(
-        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.n_miss.p, g.s1.p, g.s2.p, ph.X.p, p,
+        g.rows(), g.col.p, n, g.kept.p, m, g.mu.p, g.gate_nmiss(), g.gate_s1(), g.gate_s2(), ph.X.p, p,
         ws.XtXinv.p, ws.gtg.p, ws.inv_gtg.p, ws.ok.p, ws.af_sub.p);
     EQTL_CUDA(cudaGetLastError());
   }

@@ -152,13 +152,20 @@ int run_scan(const Options& opt) {
   st.dev = &dev;
   st.geno = &geno;
   if (std::find(opt.models.begin(), opt.models.end(), "lmm") != opt.models.end()) {
+    // genes that miss some samples get the basis of their own slice of the
+    // GRM (build_gene_ready, src/scan_common.cpp:41-63), and the scans of the
+    // other genes the shared basis back: both on the host
+    bool missing = false;
+    for (double v : st.Y) missing = missing || !std::isfinite(v);
+    for (double v : st.X) missing = missing || !std::isfinite(v);
     // the permutations rebuild LMM phenotypes through the basis on the host
-    if (opt.perm > 0) {
+    const bool host_basis = opt.perm > 0 || missing;
+    if (host_basis) {
       st.basis_Q.resize(n * n);
       st.basis_lambda.resize(n);
     }
-    double* lam = opt.perm > 0 ? st.basis_lambda.data() : nullptr;
-    double* Q = opt.perm > 0 ? st.basis_Q.data() : nullptr;
+    double* lam = host_basis ? st.basis_lambda.data() : nullptr;
+    double* Q = host_basis ? st.basis_Q.data() : nullptr;
     // --fast: the GRM's small off-diagonal entries are zeroed before the
     // eigendecomposition (sparsify_grm, src/model_lmm.cpp:88-104)
     const double thr = opt.fast ? 1e-4 : 0.0;
@@ -178,7 +185,7 @@ int run_scan(const Options& opt) {
             std::to_string(n) + " eigenvector matrix (float64)");
       for (double& l : lam_in) l = std::max(l, 0.0);
       dev.check(eqtl_lmm_set_basis(dev.ctx, Q_in.data(), lam_in.data(), static_cast<int32_t>(n)), "LMM basis");
-      if (opt.perm > 0) {
+      if (host_basis) {
         st.basis_Q = Q_in;
         st.basis_lambda = lam_in;
       }
@@ -186,6 +193,7 @@ int run_scan(const Options& opt) {
     } else if (!opt.grm.empty()) {
       std::vector<double> K = slice_grm(load_grm(opt.grm), st.samples);
       dev.check(eqtl_lmm_basis_fast(dev.ctx, K.data(), static_cast<int32_t>(n), thr, lam, Q, &zeroed), "LMM basis");
+      if (missing) st.K_full = std::move(K);
     } else {
       info("computing GRM from genotypes (overlap samples)");
       dev.check(eqtl_lmm_basis_fast(dev.ctx, nullptr, static_cast<int32_t>(n), thr, lam, Q, &zeroed), "LMM basis");
@@ -193,6 +201,12 @@ int run_scan(const Options& opt) {
     if (opt.fast)
       info("fast: GRM sparse approx thr=" + std::to_string(thr) + " zeroed " + std::to_string(zeroed) +
            " off-diagonal entries");
+    if (missing && st.K_full.empty()) {
+      st.K_full.resize(n * n);
+      std::vector<int32_t> N(n * (n + 1) / 2);
+      int64_t m_used = 0;
+      dev.check(eqtl_grm(dev.ctx, st.K_full.data(), N.data(), &m_used), "GRM");
+    }
   }
   for (const auto& model : opt.models) {
     for (const auto& scope : scopes) {

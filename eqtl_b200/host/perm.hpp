@@ -39,10 +39,12 @@ struct PermOut {
 // One device scan of explicit phenotype columns Y [cols][n] (Y empty: the
 // columns resident on the device, drawn by eqtl_pheno_permute): scope mode 0
 // gw, 1 trans, 2 cis with per-column windows (null = no location); LMM
-// columns may already be rotated into the eigenbasis.
+// columns may already be rotated into the eigenbasis. X_view: the covariates
+// of the current sample view (eqtl_geno_subset), column-major [n_view, p];
+// null = every analysis sample.
 ScanResult scan_columns(const Study& st, const std::string& model, const std::vector<double>& Y, size_t cols,
                         const std::vector<const GeneLoc*>& windows, int mode, double pthr, double perm_thr,
-                        bool rotated);
+                        bool rotated, const std::vector<double>* X_view = nullptr);
 
 std::vector<PermOut> run_permutations(const Study& st, const std::string& model, const std::vector<PermGene>& genes,
                                       const std::vector<double>& delta);

@@ -16,6 +16,7 @@
 // on ties) come from the device; the printed statistics of every pair are
 // the device's FP64 refinement.
 #include <algorithm>
+#include <map>
 #include <numeric>
 
 #include "perm.hpp"
@@ -44,7 +45,8 @@ Genotypes::Genotypes(const Device& d, const Plink& P, const std::vector<int32_t>
        " samples");
 }
 
-std::unordered_map<int64_t, double> Genotypes::af(std::vector<int64_t> idx) const {
+std::unordered_map<int64_t, double> Genotypes::af(std::vector<int64_t> idx, int n_view) const {
+  const int n = n_view > 0 ? n_view : this->n;
   std::sort(idx.begin(), idx.end());
   idx.erase(std::unique(idx.begin(), idx.end()), idx.end());
   std::unordered_map<int64_t, double> out;
@@ -66,6 +68,8 @@ std::unordered_map<int64_t, double> Genotypes::af(std::vector<int64_t> idx) cons
 }
 
 namespace {
+
+using AfMap = std::unordered_map<int64_t, double>;
 
 struct Job {
   int gene = 0;                  // column of the phenotype matrix
@@ -92,23 +96,28 @@ std::vector<char> threads_written(const std::vector<char>& has_rows) {
 
 // Complete-case sample set of one gene (build_gene_ready, src/scan_common.cpp:
 // 11-70): finite phenotype and covariates; fewer than 3 samples or an all-zero
-// phenotype leave the gene out. The device scans take the shared-keep case:
-// every kept gene must keep every analysis sample.
-bool gene_ready(const Study& st, const std::vector<double>& y, bool checks) {
+// phenotype leave the gene out. keep (if given) receives the kept analysis
+// samples; without it, a gene that does not keep every analysis sample stops
+// the run (the scopes and models that take only the shared-keep case).
+bool gene_ready(const Study& st, const std::vector<double>& y, bool checks,
+                std::vector<int32_t>* keep = nullptr) {
   const size_t n = st.samples.size();
   size_t kept = 0;
   double mx = 0.0;
+  if (keep) keep->clear();
   for (size_t i = 0; i < n; ++i) {
     bool ok = std::isfinite(y[i]);
     for (int j = 0; j < st.p && ok; ++j) ok = std::isfinite(st.X[static_cast<size_t>(j) * n + i]);
     if (ok) {
       ++kept;
       mx = std::max(mx, std::fabs(y[i]));
+      if (keep) keep->push_back(static_cast<int32_t>(i));
     }
   }
-  if (kept != n)
-    die("phenotype or covariate values missing for some samples: the device scans take the case where every "
-        "gene keeps every analysis sample");
+  if (kept != n && !keep)
+    die("phenotype or covariate values missing for some samples: the device scans take per-gene sample sets in "
+        "the trans and gw scopes of the LM and LMM without permutations; here every gene must keep every "
+        "analysis sample");
   if (!checks) return true;
   return kept >= 3 && !(mx < 1e-15);
 }
@@ -125,9 +134,10 @@ std::vector<double> gene_y(const Study& st, int g) {
 
 ScanResult scan_columns(const Study& st, const std::string& model, const std::vector<double>& Y, size_t cols,
                         const std::vector<const GeneLoc*>& windows, int mode, double pthr, double perm_thr,
-                        bool rotated) {
+                        bool rotated, const std::vector<double>* X_view) {
   const Options& opt = *st.opt;
-  const size_t n = st.samples.size(), J = cols;
+  const std::vector<double>& Xs = X_view ? *X_view : st.X;
+  const size_t n = Xs.size() / static_cast<size_t>(st.p), J = cols;
   ScanResult R;
   R.n = static_cast<int>(n);
   // windows and the kept SNPs' positions, chromosomes by normalised name
@@ -176,7 +186,7 @@ ScanResult scan_columns(const Study& st, const std::string& model, const std::ve
   int64_t cap = 1 << 18, ccap = perm_thr > 0 ? (1 << 18) : 1;
   // no host columns: scan the resident ones (eqtl_pheno_permute)
   const double* Yp = Y.empty() ? nullptr : Y.data();
-  const double* Xp = Y.empty() ? nullptr : st.X.data();
+  const double* Xp = Y.empty() ? nullptr : Xs.data();
   for (int attempt = 0; attempt < 3; ++attempt) {
     R.pairs.resize(static_cast<size_t>(cap));
     R.cands.resize(static_cast<size_t>(ccap));
@@ -256,12 +266,20 @@ PairRow make_row(const Study& st, const std::string& gene, const GeneLoc* loc, i
 // Writes pairs (in `order`), tops and region rows of one device scan.
 void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const std::string& scope, double pthr,
           const std::vector<size_t>& pair_order, ScopeFiles& out, std::vector<RegionRow>& regions,
-          const std::vector<PermOut>* perms, size_t n_works_par = 0) {
-  std::vector<int64_t> need;
-  for (const auto& q : R.pairs) need.push_back(q.snp);
-  for (const auto& g : R.genes)
-    if (g.best_snp >= 0 && g.best_p <= pthr) need.push_back(g.best_snp);
-  const auto af = st.geno->af(need);
+          const std::vector<PermOut>* perms, size_t n_works_par = 0, const std::vector<int>* n_job = nullptr,
+          const std::vector<const AfMap*>* af_job = nullptr) {
+  AfMap af;
+  if (!af_job) {
+    std::vector<int64_t> need;
+    for (const auto& q : R.pairs) need.push_back(q.snp);
+    for (const auto& g : R.genes)
+      if (g.best_snp >= 0 && g.best_p <= pthr) need.push_back(g.best_snp);
+    af = st.geno->af(need);
+  }
+  // allele frequency and sample count of gene j's rows (its own sample set
+  // when the genes keep different samples)
+  auto af_of = [&](size_t j, int64_t snp) { return (af_job ? *(*af_job)[j] : af).at(snp); };
+  auto n_of = [&](size_t j) { return n_job ? (*n_job)[j] : R.n; };
   std::vector<int> n_sig(jobs.size(), 0);
   const bool glm = !R.phi.empty();
   auto with_glm = [&](PairRow r, size_t j) {
@@ -291,7 +309,8 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
     ++n_sig[q.gene];
     if (T && !pairs_ok[thread_of(q.gene)]) continue;
     write_pair(out.pairs,
-               with_glm(make_row(st, st.genes[jb.gene], jb.loc, q.snp, af.at(q.snp), q.beta, q.se, q.t, q.p, q.r2, R.n),
+               with_glm(make_row(st, st.genes[jb.gene], jb.loc, q.snp, af_of(q.gene, q.snp), q.beta, q.se, q.t, q.p,
+                                 q.r2, n_of(q.gene)),
                         q.gene),
                scope);
   }
@@ -316,11 +335,115 @@ void emit(const Study& st, const std::vector<Job>& jobs, ScanResult& R, const st
     regions.push_back(rr);
     if (g.best_snp >= 0 && g.best_p <= pthr && g.best_p <= 1.0 && !(T && !tops_ok[thread_of(j)]))
       write_pair(out.top,
-                 with_glm(make_row(st, rr.gene, jb.loc, g.best_snp, af.at(g.best_snp), g.best_beta, g.best_se,
-                                   g.best_t, g.best_p, g.best_r2, R.n),
+                 with_glm(make_row(st, rr.gene, jb.loc, g.best_snp, af_of(j, g.best_snp), g.best_beta, g.best_se,
+                                   g.best_t, g.best_p, g.best_r2, n_of(j)),
                           j),
                  scope);
   }
+}
+
+// Trans/gw scans of genes whose sample sets differ (the reference's per-job
+// paths for mixed keep sets, src/scan_trans_lm.cpp:121-151 and
+// src/scan_trans_lmm.cpp:192-228): the genes are grouped by keep set, and
+// each group is scanned over its own sample view (eqtl_geno_subset: the SNPs
+// imputed and filtered over every analysis sample, then subset, as the
+// reference's for_each_snp and g_buf do); the LMM takes the eigenbasis of the
+// GRM sliced to the group's samples, as build_gene_ready slices it. The
+// results come back in job order, pairs by (SNP, gene).
+struct KeepScan {
+  ScanResult R;
+  std::vector<int> n_job;
+  std::vector<AfMap> af_grp;
+  std::vector<const AfMap*> af_job;
+};
+
+KeepScan scan_by_keep(const Study& st, const std::string& model, const std::vector<Job>& jobs,
+                      const std::vector<std::vector<int32_t>>& keeps, int mode, double pthr) {
+  const Device& dev = *st.dev;
+  const size_t n = st.samples.size(), J = jobs.size();
+  const size_t p = static_cast<size_t>(st.p);
+  std::vector<std::vector<size_t>> groups;
+  std::map<std::vector<int32_t>, size_t> gid;
+  for (size_t j = 0; j < J; ++j) {
+    auto it = gid.find(keeps[j]);
+    if (it == gid.end()) {
+      it = gid.emplace(keeps[j], groups.size()).first;
+      groups.emplace_back();
+    }
+    groups[it->second].push_back(j);
+  }
+  const bool lmm = model == "lmm";
+  if (lmm && (st.K_full.size() != n * n || st.basis_Q.size() != n * n))
+    die("internal: per-gene sample sets of the LMM need the GRM and the eigenbasis on the host");
+  KeepScan K;
+  K.R.n = static_cast<int>(n);
+  K.R.genes.resize(J);
+  K.R.delta.assign(J, 0.0);
+  K.n_job.assign(J, static_cast<int>(n));
+  K.af_grp.resize(groups.size());
+  K.af_job.assign(J, nullptr);
+  Trace tr;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const std::vector<size_t>& grp = groups[gi];
+    const std::vector<int32_t>& keep = keeps[grp[0]];
+    const size_t ns = keep.size();
+    const bool full = ns == n;
+    dev.check(eqtl_geno_subset(dev.ctx, full ? nullptr : keep.data(), full ? 0 : static_cast<int32_t>(ns)),
+              "sample view");
+    if (lmm) {
+      if (full) {
+        dev.check(eqtl_lmm_set_basis(dev.ctx, st.basis_Q.data(), st.basis_lambda.data(), static_cast<int32_t>(n)),
+                  "LMM basis");
+      } else {
+        std::vector<double> Ks(ns * ns);
+        for (size_t b = 0; b < ns; ++b)
+          for (size_t a = 0; a < ns; ++a) Ks[b * ns + a] = st.K_full[static_cast<size_t>(keep[b]) * n + keep[a]];
+        int64_t zeroed = 0;
+        dev.check(eqtl_lmm_basis_fast(dev.ctx, Ks.data(), static_cast<int32_t>(ns), st.opt->fast ? 1e-4 : 0.0, nullptr,
+                                      nullptr, &zeroed),
+                  "LMM basis of a gene sample set");
+      }
+    }
+    const size_t Jg = grp.size();
+    std::vector<double> Yg(Jg * ns), Xg(ns * p);
+    std::vector<const GeneLoc*> win(Jg);
+    for (size_t a = 0; a < p; ++a)
+      for (size_t i = 0; i < ns; ++i) Xg[a * ns + i] = st.X[a * n + keep[i]];
+    for (size_t k = 0; k < Jg; ++k) {
+      const std::vector<double> y = gene_y(st, jobs[grp[k]].gene);
+      for (size_t i = 0; i < ns; ++i) Yg[k * ns + i] = y[keep[i]];
+      win[k] = jobs[grp[k]].loc;
+    }
+    ScanResult R = scan_columns(st, model, Yg, Jg, win, mode, pthr, 0.0, false, &Xg);
+    // allele frequencies over the view, while it is active
+    std::vector<int64_t> need;
+    for (const auto& q : R.pairs) need.push_back(q.snp);
+    for (const auto& g : R.genes)
+      if (g.best_snp >= 0 && g.best_p <= pthr) need.push_back(g.best_snp);
+    K.af_grp[gi] = st.geno->af(need, static_cast<int>(ns));
+    for (size_t k = 0; k < Jg; ++k) {
+      const size_t j = grp[k];
+      K.R.genes[j] = R.genes[k];
+      if (!R.delta.empty()) K.R.delta[j] = R.delta[k];
+      K.n_job[j] = static_cast<int>(ns);
+      K.af_job[j] = &K.af_grp[gi];
+    }
+    for (eqtl_pair q : R.pairs) {
+      q.gene = static_cast<int32_t>(grp[q.gene]);
+      K.R.pairs.push_back(q);
+    }
+    tr.mark("sample set " + std::to_string(gi + 1) + "/" + std::to_string(groups.size()) + ": " +
+            std::to_string(Jg) + " genes on " + std::to_string(ns) + " samples");
+  }
+  // every analysis sample again, and the shared basis, for the scans after
+  dev.check(eqtl_geno_subset(dev.ctx, nullptr, 0), "sample view");
+  if (lmm)
+    dev.check(eqtl_lmm_set_basis(dev.ctx, st.basis_Q.data(), st.basis_lambda.data(), static_cast<int32_t>(n)),
+              "LMM basis");
+  std::stable_sort(K.R.pairs.begin(), K.R.pairs.end(), [](const eqtl_pair& a, const eqtl_pair& b) {
+    return a.snp != b.snp ? a.snp < b.snp : a.gene < b.gene;
+  });
+  return K;
 }
 
 }  // namespace
@@ -330,6 +453,8 @@ void run_trans(const Study& st, const std::string& model, const std::string& sco
   const Options& opt = *st.opt;
   const bool have_gff = !opt.gff.empty();
   std::vector<Job> jobs;
+  std::vector<std::vector<int32_t>> keeps;
+  bool mixed = false;
   for (size_t g = 0; g < st.genes.size(); ++g) {
     Job jb;
     jb.gene = static_cast<int>(g);
@@ -339,14 +464,28 @@ void run_trans(const Study& st, const std::string& model, const std::string& sco
       else if (scope != "gw") continue;
     }
     if (scope == "trans" && !jb.loc) continue;
-    if (!gene_ready(st, gene_y(st, jb.gene), true)) continue;
+    std::vector<int32_t> keep;
+    if (!gene_ready(st, gene_y(st, jb.gene), true, &keep)) continue;
+    mixed = mixed || keep.size() != st.samples.size();
     jobs.push_back(jb);
+    keeps.push_back(std::move(keep));
   }
   info(std::string(scope) + " " + model + ": " + std::to_string(jobs.size()) + " genes");
   if (jobs.empty()) return;
   const double pthr = opt.pval_trans;
   const double perm_thr = opt.perm > 0 ? opt.perm_trans_thr : 0.0;
   Trace tr;
+  if (mixed) {
+    if (opt.perm > 0)
+      die("phenotype or covariate values missing for some samples: gene-level permutations take the case where "
+          "every gene keeps every analysis sample");
+    KeepScan K = scan_by_keep(st, model, jobs, keeps, scope == "trans" ? 1 : 0, pthr);
+    tr.mark(scope + " " + model + ": device scans of the gene sample sets");
+    std::vector<size_t> order(K.R.pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    emit(st, jobs, K.R, scope, pthr, order, out, regions, nullptr, 0, &K.n_job, &K.af_job);
+    return;
+  }
   ScanResult R = device_scan(st, model, jobs, scope == "trans" ? 1 : 0, pthr, perm_thr);
   tr.mark(scope + " " + model + ": device scan");
   std::vector<PermOut> perms;

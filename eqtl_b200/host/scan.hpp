@@ -25,7 +25,9 @@ struct Genotypes {
   // Reference allele frequency of each listed kept SNP over the analysis
   // samples: (sum of imputed dosages in sample order / n) / 2, clamped to
   // [0, 1] (subset_maf_or_nan, src/scan_common.cpp:133-151).
-  std::unordered_map<int64_t, double> af(std::vector<int64_t> kept_idx) const;
+  // n_view: the samples of the current device view (eqtl_geno_subset); 0 =
+  // every analysis sample.
+  std::unordered_map<int64_t, double> af(std::vector<int64_t> kept_idx, int n_view = 0) const;
 };
 
 struct Study {
@@ -42,6 +44,9 @@ struct Study {
   // LMM permutations: the device eigenbasis on the host (Q column-major,
   // column j = eigenvector j; lambda clipped at 0)
   std::vector<double> basis_Q, basis_lambda;
+  // genes whose phenotype or covariates miss some samples (per-gene keep
+  // sets): the full GRM on the host, sliced to each keep set for its basis
+  std::vector<double> K_full;
 };
 
 void run_trans(const Study& st, const std::string& model, const std::string& scope, ScopeFiles& out,

@@ -116,6 +116,21 @@ int eqtl_vcf_parse(eqtl_ctx* ctx, const char* text, int64_t text_len, const int6
  * [hi - lo, n] (SnpRec.dosage after src/plink_bed.cpp:298-302). */
 int eqtl_geno_dosage(eqtl_ctx* ctx, int64_t lo, int64_t hi, double* out);
 
+/* Per-gene sample subsets (the reference's per-gene keep sets,
+ * build_gene_ready, src/scan_common.cpp:11-65, and the trans/gw paths for
+ * genes whose keep sets differ, src/scan_trans_lm.cpp:121-151,
+ * src/scan_trans_lmm.cpp:192-228). Restricts the loaded genotypes to the
+ * analysis samples idx[0..n_sub) (positions in the sample order of the
+ * load, increasing); idx == NULL restores every analysis sample. The kept
+ * SNPs, their imputation means and the load's filters stay those of the
+ * whole sample set, as the reference imputes each SNP before it subsets it;
+ * the per-SNP gate (subset_maf_or_nan) and every scan, refinement and
+ * dosage call that follows use the subset (n = n_sub). The rotated LMM
+ * operands are dropped: install the subset's basis (eqtl_lmm_basis with the
+ * GRM sliced to the subset) before an LMM scan. eqtl_grm refuses a subset
+ * view; the NB-GLM scan too. */
+int eqtl_geno_subset(eqtl_ctx* ctx, const int32_t* idx, int32_t n_sub);
+
 /* The same for k kept-SNP indices rows[0..k): out [k, n]. The host driver
  * prints each pair's af from these (subset_maf_or_nan,
  * src/scan_common.cpp:133-151, sums the dosages in sample order). */

@@ -384,74 +384,87 @@ class Scanner:
         pairs, tops, summ = [], [], []
         if not jobs:
             return pairs, tops, []
-        keep0 = jobs[0][2][0]
-        if any(not np.array_equal(j[2][0], keep0) for j in jobs):
-            raise NotImplementedError("mixed keep sets are not restated")
-        X = jobs[0][2][2]
-        n, p = X.shape
-        G = self.dec.dosage[self.kept][:, keep0]
-        af_sub, ok = R.subset_maf(G)
-        snps = self.kept[ok]
-        G = G[ok]
-        af_sub = af_sub[ok]
-        ng = len(jobs)
-        if model == "lm":
-            preps = [R.prep_lm(j[2][1], j[2][2]) for j in jobs]
-            Xt_g = G @ X
-            g_s = G - (Xt_g @ preps[0].XtX_inv.T) @ X.T
-            gtg = np.einsum("ij,ij->i", g_s, g_s)
-            Ys = np.stack([pp.y_s for pp in preps], 1)
-            gty = g_s @ Ys                                  # [m, G]
-            st = R.lm_stats(gtg[:, None], gty, np.array([pp.yty for pp in preps])[None, :], n, p)
-            degenerate = gtg < 1e-12
-        else:
-            K = self.grm()[np.ix_(keep0, keep0)]
-            Q, lam = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
-            preps = [R.prep_lmm(j[2][1], j[2][2], Q, lam) for j in jobs]
-            Gt = G @ Q
-            cols = [R.lmm_stats_gtil(pp, Gt) for pp in preps]
-            st = {k: np.stack([c[k] for c in cols], 1) for k in cols[0]}
-            degenerate = np.zeros(G.shape[0], dtype=bool)
-        excl = np.zeros((len(snps), ng), dtype=bool)
-        if scope == "trans":
-            for j, (gene, loc, _) in enumerate(jobs):
-                excl[:, j] = [self.in_cis(s, loc) for s in snps]
-        topk = opt.perm_trans_top if opt.perm > 0 else 0
-        for j, (gene, loc, ready) in enumerate(jobs):
-            s = Summary(gene)
-            if loc is not None:
-                s.chrom, s.tss = loc.chrom, loc.tss
-            acc = R.AcatAcc()
-            best_p, best = 2.0, None
-            pv = st["p"][:, j]
-            use = ~excl[:, j]
-            s.n_tested = int(use.sum())
-            acc.add_many(pv[use])
-            acc.add_sensitivity(pv[use], st["stat"][:, j][use], n - p - 1)
-            sig = use & (pv <= pthr)
-            s.n_sig = int(sig.sum())
-            for i in np.nonzero(sig)[0]:
-                pairs.append((int(snps[i]), j, pair_row(gene, self.snp_meta(snps[i]),
-                                                         _hit(st, i, af_sub[i], j) if not degenerate[i]
-                                                         else _p1(af_sub[i]), n, loc, scope)))
-            cand = np.nonzero(use)[0]
-            if cand.size:
-                k = cand[np.argmin(pv[cand])]   # first index on ties (strict <)
-                best_p, best = pv[k], k
-            s.acat = acc.p()
-            s.acat_sens = acc.log10_sensitivity()
-            if best is not None and best_p <= pthr and best_p <= 1.0:
-                tops.append(pair_row(gene, self.snp_meta(snps[best]),
-                                     _hit(st, best, af_sub[best], j) if not degenerate[best]
-                                     else _p1(af_sub[best]), n, loc, scope))
-            if topk > 0 and best is not None and best_p < opt.perm_trans_thr and s.n_tested > 0:
-                cidx = np.nonzero(use & np.isfinite(pv) & (pv < opt.perm_trans_thr) & ~degenerate)[0]
-                cidx = cidx[np.argsort(pv[cidx], kind="stable")][:topk]
-                cached = [G[i] for i in cidx]
-                if cached:
-                    self.perm(model, s, gene, ready, cached, best_p, preps[j], lmm_basis=(
-                        (Q, lam) if model == "lmm" else None))
-            summ.append(s)
+        # genes whose keep sets differ run per keep set (the reference's
+        # per-job paths, src/scan_trans_lm.cpp:121-151,
+        # src/scan_trans_lmm.cpp:192-228): the SNP gate, residualisation and
+        # (LMM) basis of each set's samples; pairs keep their (SNP, gene) order
+        groups = {}
+        for jg, job in enumerate(jobs):
+            groups.setdefault(tuple(int(i) for i in job[2][0]), []).append(jg)
+        summ = [None] * len(jobs)
+        tops_by = [[] for _ in jobs]
+        for keep_t, idxs in groups.items():
+            keep0 = np.array(keep_t, dtype=np.int64)
+            gjobs = [jobs[jg] for jg in idxs]
+            X = gjobs[0][2][2]
+            n, p = X.shape
+            G = self.dec.dosage[self.kept][:, keep0]
+            af_sub, ok = R.subset_maf(G)
+            snps = self.kept[ok]
+            G = G[ok]
+            af_sub = af_sub[ok]
+            ng = len(gjobs)
+            if model == "lm":
+                preps = [R.prep_lm(j[2][1], j[2][2]) for j in gjobs]
+                Xt_g = G @ X
+                g_s = G - (Xt_g @ preps[0].XtX_inv.T) @ X.T
+                gtg = np.einsum("ij,ij->i", g_s, g_s)
+                Ys = np.stack([pp.y_s for pp in preps], 1)
+                gty = g_s @ Ys                                  # [m, G]
+                st = R.lm_stats(gtg[:, None], gty, np.array([pp.yty for pp in preps])[None, :], n, p)
+                degenerate = gtg < 1e-12
+            else:
+                K = self.grm()[np.ix_(keep0, keep0)]
+                Q, lam = R.make_lmm_basis(R.sparsify_grm(K, 1e-4) if opt.fast else K)
+                preps = [R.prep_lmm(j[2][1], j[2][2], Q, lam) for j in gjobs]
+                Gt = G @ Q
+                cols = [R.lmm_stats_gtil(pp, Gt) for pp in preps]
+                st = {k: np.stack([c[k] for c in cols], 1) for k in cols[0]}
+                degenerate = np.zeros(G.shape[0], dtype=bool)
+            excl = np.zeros((len(snps), ng), dtype=bool)
+            if scope == "trans":
+                for j, (gene, loc, _) in enumerate(gjobs):
+                    excl[:, j] = [self.in_cis(s, loc) for s in snps]
+            topk = opt.perm_trans_top if opt.perm > 0 else 0
+            for j, (gene, loc, ready) in enumerate(gjobs):
+                s = Summary(gene)
+                gtops = []
+                if loc is not None:
+                    s.chrom, s.tss = loc.chrom, loc.tss
+                acc = R.AcatAcc()
+                best_p, best = 2.0, None
+                pv = st["p"][:, j]
+                use = ~excl[:, j]
+                s.n_tested = int(use.sum())
+                acc.add_many(pv[use])
+                acc.add_sensitivity(pv[use], st["stat"][:, j][use], n - p - 1)
+                sig = use & (pv <= pthr)
+                s.n_sig = int(sig.sum())
+                for i in np.nonzero(sig)[0]:
+                    pairs.append((int(snps[i]), idxs[j], pair_row(gene, self.snp_meta(snps[i]),
+                                                             _hit(st, i, af_sub[i], j) if not degenerate[i]
+                                                             else _p1(af_sub[i]), n, loc, scope)))
+                cand = np.nonzero(use)[0]
+                if cand.size:
+                    k = cand[np.argmin(pv[cand])]   # first index on ties (strict <)
+                    best_p, best = pv[k], k
+                s.acat = acc.p()
+                s.acat_sens = acc.log10_sensitivity()
+                if best is not None and best_p <= pthr and best_p <= 1.0:
+                    gtops.append(pair_row(gene, self.snp_meta(snps[best]),
+                                         _hit(st, best, af_sub[best], j) if not degenerate[best]
+                                         else _p1(af_sub[best]), n, loc, scope))
+                if topk > 0 and best is not None and best_p < opt.perm_trans_thr and s.n_tested > 0:
+                    cidx = np.nonzero(use & np.isfinite(pv) & (pv < opt.perm_trans_thr) & ~degenerate)[0]
+                    cidx = cidx[np.argsort(pv[cidx], kind="stable")][:topk]
+                    cached = [G[i] for i in cidx]
+                    if cached:
+                        self.perm(model, s, gene, ready, cached, best_p, preps[j], lmm_basis=(
+                            (Q, lam) if model == "lmm" else None))
+                summ[idxs[j]] = s
+                tops_by[idxs[j]] = gtops
+        for t in tops_by:
+            tops.extend(t)
         pairs.sort(key=lambda t: (t[0], t[1]))
         return [p_[2] for p_ in pairs], tops, self.finish(summ)
 

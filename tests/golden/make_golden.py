@@ -69,7 +69,41 @@ CASES = {
             ("gw", ["--model", "lm,lmm", "--pval-trans", "5e-2", "--max-miss", "0.05", "-t", "1"]),
             ("grm", ["--make-grm", "--max-miss", "0.05"]),
         ]),
+    # per-gene sample sets: some genes miss phenotype values (two of them at
+    # the same samples, one with only 2 values left, so it drops out), and in
+    # the *_cna runs one sample misses a covariate value, so no gene keeps
+    # every analysis sample
+    "nakeep": dict(
+        geno=dict(seed=501, n=110, m=700, n_chrom=3, chrom_len=5_000_000, family=(4, 5, 90),
+                  miss_rate=0.01, maf_lo=0.02),
+        genes=dict(seed=502, n_genes=30, body=1000),
+        pheno=dict(kind="lm", seed=503, n_cov=2),
+        na=dict(seed=504, genes=9, most=6, shared=(3, 4), sparse=11),
+        cov_na=(17, 1),
+        runs=[
+            ("trans", ["--model", "lm,lmm", "--mode", "trans", "--pval-trans", "1e-2", "-t", "1"]),
+            ("gw", ["--model", "lm,lmm", "--mode", "gw", "--pval-trans", "1e-2", "-t", "1"]),
+            ("trans_cna", ["--model", "lm,lmm", "--mode", "trans", "--pval-trans", "1e-2", "-t", "1"]),
+        ]),
 }
+
+
+def plant_na(Y, na: dict):
+    """NaN phenotype values: na["genes"] genes (from gene 1 on) miss 1 to
+    na["most"] samples each; gene na["shared"][1] misses the same samples as
+    gene na["shared"][0]; gene na["sparse"] keeps only 2 samples."""
+    import numpy as np
+    rng = np.random.default_rng(na["seed"])
+    n, G = Y.shape
+    Y = Y.copy()
+    a, b = na["shared"]
+    for g in range(1, 1 + na["genes"]):
+        if g == b:
+            continue
+        Y[rng.choice(n, int(rng.integers(1, na["most"] + 1)), replace=False), g] = np.nan
+    Y[:, b] = np.where(np.isnan(Y[:, a]), np.nan, Y[:, b])
+    Y[2:, na["sparse"]] = np.nan
+    return Y
 
 
 def build_case(name: str, spec: dict) -> None:
@@ -91,10 +125,16 @@ def build_case(name: str, spec: dict) -> None:
                                    gene_tss=tss, gene_chrom=gc, window=500_000, n_trans=10)
     else:
         Y, C, _ = synth.make_pheno_lmm(ph["seed"], g, gs["n_genes"], ph["n_cov"], n_trans=10)
+    if "na" in spec:
+        Y = plant_na(Y, spec["na"])
     synth.write_pheno(os.path.join(d, "pheno.tsv"), g.samples, ids, Y)
     have_cov = C.shape[1] > 0
     if have_cov:
         synth.write_covar(os.path.join(d, "covar.tsv"), g.samples, C)
+    if "cov_na" in spec:
+        Cn = C.copy()
+        Cn[spec["cov_na"]] = float("nan")
+        synth.write_covar(os.path.join(d, "covar_na.tsv"), g.samples, Cn)
     have_gff = name != "nogff"
     if have_gff:
         synth.write_gff(os.path.join(d, "genes.gff"), ids, gc, st, en, sd)
@@ -106,7 +146,7 @@ def build_case(name: str, spec: dict) -> None:
             if have_gff:
                 cmd += ["-g", "genes.gff"]
             if have_cov:
-                cmd += ["-c", "covar.tsv"]
+                cmd += ["-c", "covar_na.tsv" if tag.endswith("_cna") else "covar.tsv"]
         cmd += argv + ["-o", f"ref_{tag}"]
         r = subprocess.run(cmd, cwd=d, capture_output=True, text=True)
         if r.returncode != 0:
