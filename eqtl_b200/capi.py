@@ -23,7 +23,7 @@ PREC_SPLIT_F16, PREC_SPLIT_BF16, PREC_FP32_SIMT = 0, 1, 2
 # every symbol include/eqtl_b200.h declares
 EXPORTS = ["eqtl_open", "eqtl_close", "eqtl_last_error", "eqtl_set_precision", "eqtl_geno_load_bed",
            "eqtl_geno_dosage", "eqtl_scan_trans_lm", "eqtl_grm", "eqtl_lmm_basis", "eqtl_lmm_set_basis",
-           "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_rotate",
+           "eqtl_scan_trans_lmm", "eqtl_stage_ms", "eqtl_launch_count", "eqtl_lmm_form", "eqtl_lmm_rotate",
            "eqtl_stream", "eqtl_pheno_load", "eqtl_t_tail", "eqtl_grm_noalloc", "eqtl_geno_dosage_rows",
            "eqtl_test_pairs", "eqtl_geno_load_dosage", "eqtl_scan_glm", "eqtl_pheno_int",
            "eqtl_peer", "eqtl_glm_mu", "eqtl_vcf_parse", "eqtl_lmm_basis_fast", "eqtl_pheno_permute",
@@ -89,6 +89,7 @@ def load() -> C.CDLL:
         lib.eqtl_grm_noalloc.argtypes = [vp, vp, i64, i64, vp, i32, i32, dp, dp, vp, vp, C.POINTER(i64)]
         lib.eqtl_stage_ms.argtypes = [vp, C.c_int, C.POINTER(dp)]
         lib.eqtl_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+        lib.eqtl_lmm_form.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         lib.eqtl_lmm_rotate.argtypes = [vp]
         lib.eqtl_stream.argtypes = [vp, C.POINTER(vp)]
         lib.eqtl_pheno_load.argtypes = [vp, vp, vp, i32, i32, i32]
@@ -304,6 +305,13 @@ class Context:
         v = C.c_uint64()
         self._check(self.lib.eqtl_launch_count(self.h, C.byref(v)))
         return v.value
+
+    def lmm_form(self):
+        """(node deltas, K columns per accumulator) of the most recent LMM
+        scan's interpolated gg and a_k; (0, 0) for the direct form."""
+        a, b = C.c_int32(), C.c_int32()
+        self._check(self.lib.eqtl_lmm_form(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def t_tail(self, df: float, t, use_smem: bool = False, screen: bool = False):
         """Device Student-t tail -> (-log10 p, ACAT term, flags); with

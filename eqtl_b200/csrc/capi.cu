@@ -619,6 +619,14 @@ int eqtl_launch_count(eqtl_ctx* ctx, uint64_t* count) {
   });
 }
 
+int eqtl_lmm_form(eqtl_ctx* ctx, int32_t* nodes, int32_t* node_cols) {
+  return guarded(ctx, [&] {
+    EQTL_CHECK(nodes && node_cols, EQTL_E_ARG, "null output");
+    *nodes = ctx->ws.lr_nodes;
+    *node_cols = ctx->ws.lr_nodes > 0 ? ctx->ws.lr_kn : 0;
+  });
+}
+
 int eqtl_stream(eqtl_ctx* ctx, void** stream) {
   return guarded(ctx, [&] {
     EQTL_CHECK(stream, EQTL_E_ARG, "null output");

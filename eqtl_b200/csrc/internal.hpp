@@ -252,6 +252,17 @@ struct Workspace {
   DevBuf<unsigned long long> grm_count;  // SNPs the GRM uses
   DevBuf<unsigned long long> raw_inexact;  // SNPs the exact LMM operand cannot hold
   DevBuf<double> lmm_w, lmm_uv;            // [n, G (p + 1)]: w o (r~, X~_k) and Q times them
+  // interpolated LMM scan (lmm_lr_prepare): node log-deltas and deltas, the
+  // node pass's gene-side operands, its FP32 table [m][lr_kb] with the column
+  // maxima and scales, the split SNP-side table and the genes' coefficients
+  DevBuf<double> lr_a, lr_delta, lr_zero, lr_w, lr_uv;
+  DevBuf<__half> lr_ops_hi[4], lr_ops_lo[4];
+  DevBuf<__half*> lr_ops_ptr;
+  DevBuf<float> lr_unscale, lr_val, lr_sigma;
+  DevBuf<unsigned int> lr_colmax;
+  DevBuf<__half> lr_phi, lr_plo, lr_chi, lr_clo;
+  int lr_kn = 0, lr_kb = 0;
+  int lr_nodes = 0;  // node deltas of the most recent LMM scan (0: direct form)
   DevBuf<float> ops32[4];                  // FP32 gene-side operands of the CUDA-core comparator
   DevBuf<const float*> ops32_ptr;
   DevBuf<__half> grm_zh, grm_zl, grm_mk;

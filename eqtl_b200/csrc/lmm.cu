@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <limits>
 #include <memory>
 #include <type_traits>
@@ -854,6 +855,10 @@ struct GlmEpiParams : LmmEpiParams<P> {};
 // ... and the LMM scan on the exact unrotated SNP operand (LmmEpi<P, false, true>).
 template <int P>
 struct LmmRawEpiParams : LmmEpiParams<P> {};
+// ... and the same with gg and a_k interpolated between node deltas
+// (LmmEpi<P, false, true, true>): a_k then carries no SNP factor alpha.
+template <int P>
+struct LmmLrEpiParams : LmmEpiParams<P> {};
 
 // Accumulator order of the tile: [gg, a_0 .. a_{P-1}, NUM] (the gene-side
 // operands w, w o X~_k, w o r~ against Gt^2, Gt, Gt). The epilogue is
@@ -870,15 +875,20 @@ struct LmmRawEpiParams : LmmEpiParams<P> {};
 // (Rotated::raw) against the gene-side vectors u = Q (w o r~) and
 // v_k = Q (w o X~_k), since Gt . (w o r~) = g . Q (w o r~); the operands
 // centre each SNP themselves (padding column n), so x = alpha_s * acc.
-template <int P, bool GLM = false, bool RAW = false>
+//
+// LR = true (with RAW): gg and a_k come from the node-interpolated operands
+// (lmm_lr_scan), which hold each SNP's factor alpha already; NUM as RAW.
+template <int P, bool GLM = false, bool RAW = false, bool LR = false>
 struct LmmEpi {
   static_assert(!(GLM && RAW), "the exact-operand form is the LMM scan's");
+  static_assert(!LR || RAW, "the interpolated form reads NUM from the exact operand");
   static constexpr bool kGrouped = false;
   static constexpr bool kTwoPhase = true;
   static constexpr int kPhase1 = P + 1;  // gg and a_k
   static constexpr int kMaxChunks = 2;   // 16-column chunks per warp and tile
-  using Params = std::conditional_t<GLM, GlmEpiParams<P>,
-                                    std::conditional_t<RAW, LmmRawEpiParams<P>, LmmEpiParams<P>>>;
+  using Params = std::conditional_t<
+      GLM, GlmEpiParams<P>,
+      std::conditional_t<LR, LmmLrEpiParams<P>, std::conditional_t<RAW, LmmRawEpiParams<P>, LmmEpiParams<P>>>>;
   static constexpr int kSmemBytes = kTTableSmemBytes;
   const Params& Pr;
   float* tsm;
@@ -928,14 +938,14 @@ struct LmmEpi {
   __device__ void pre_chunk(int ci, int c, const float (&v)[N][16]) {
     static_assert(N == P + 1, "phase-1 accumulators");
     float al[16];  // RAW: alpha of each SNP (the array is padded past the last tile)
-    if constexpr (RAW) load16(Pr.snp_alpha + snp0 + c, al);
+    if constexpr (RAW && !LR) load16(Pr.snp_alpha + snp0 + c, al);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const float gg = v[0][j] * u[P + 1];
       float S = gg;
       float a[P];
       float us = 1.0f;
-      if constexpr (RAW) us = al[j];
+      if constexpr (RAW && !LR) us = al[j];
 #pragma unroll
       for (int k = 0; k < P; ++k) a[k] = v[1 + k][j] * (us * u[1 + k]);
 #pragma unroll
@@ -1019,6 +1029,186 @@ struct LmmEpi {
   }
   __device__ void finish() {}
 };
+
+// ------------------------------------- node-interpolated gg and a_k (p <= 2)
+// The weights w_i = 1 / (1 + delta lambda_i) of a gene enter gg and a_k only
+// through delta, and as functions of a = ln(delta) they are analytic in a
+// strip of half-width pi around the real axis. So on an interval of a of
+// length <= 3, the Lagrange interpolant through 12 Chebyshev-Lobatto nodes
+// reproduces every w_i to 1.1e-7 relative at worst (where delta lambda_i is
+// near 8), below the 2^-22 to which the FP16 hi/lo pair holds w itself, and
+// far closer on shorter intervals; with it
+//     gg(s, g) = sum_j l_j(a_g) gg(s, node j),   a_k likewise,
+// where gg(s, node j) is the contraction for a "node gene" of delta_j. The
+// node pass computes those for the <= 128 nodes that cover the scan's genes
+// (one gene-side tile), and the scan then forms gg and a_k with K = the node
+// count instead of n. The Lebesgue constants keep |l_j| sums below ~5, so the
+// interpolation adds at most a few FP32 roundings.
+
+// Node pass epilogue: rows = nodes, accumulators [gg, a_0 .. a_{P-1}] of
+// every kept SNP in FP32 (gg as the scan forms it, a_k with the SNP's alpha)
+// into val[s][kind * kn + node] (kind 0 = gg, 1 + k = a_k), and per column
+// the largest magnitude (colmax, FP32 bits; non-negative floats order as
+// unsigned integers).
+template <int P>
+struct LmmNodeEpiParams {
+  int n_nodes;
+  int64_t m;
+  int kn, kb;               // node columns per kind (64 or 128); kb = (P + 1) kn
+  const float* unscale;     // [nodes][P + 2] in the gene-ops order [NUM, a_0 .., gg]
+  const float* snp_alpha;   // [m, padded to 256 + 256]
+  float* val;               // [m][kb]
+  unsigned int* colmax;     // [kb]
+};
+
+template <int P>
+struct LmmNodeEpi {
+  static constexpr bool kGrouped = false;
+  static constexpr int kSmemBytes = 0;
+  using Params = LmmNodeEpiParams<P>;
+  const Params& Pr;
+  int node = 0;
+  int64_t snp0 = 0;
+  bool valid = false;
+  float u[P + 1];   // unscale of [gg, a_0 ..]
+  float mx[P + 1];  // largest magnitude of each kind over the tile
+  __device__ LmmNodeEpi(const Params& p, const TileShape&, uint8_t*) : Pr(p) {}
+  __device__ void init(int, int) {}
+  __device__ void begin_tile(int g, int64_t s0) {
+    node = g;
+    snp0 = s0;
+    valid = g < Pr.n_nodes;
+#pragma unroll
+    for (int k = 0; k <= P; ++k) mx[k] = 0.0f;
+    if (valid) {
+      u[0] = Pr.unscale[static_cast<int64_t>(g) * (P + 2) + P + 1];
+#pragma unroll
+      for (int k = 0; k < P; ++k) u[1 + k] = Pr.unscale[static_cast<int64_t>(g) * (P + 2) + 1 + k];
+    }
+  }
+  template <int N>
+  __device__ void chunk(int c, const float (&v)[N][16]) {
+    static_assert(N == P + 1, "node pass accumulators");
+    const int64_t s0 = snp0 + c;
+    if (!valid || s0 >= Pr.m) return;
+    float al[16];
+    load16(Pr.snp_alpha + s0, al);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t s = s0 + j;
+      if (s < Pr.m) {
+        float* row = Pr.val + s * Pr.kb + node;
+        const float gg = v[0][j] * u[0];
+        row[0] = gg;
+        mx[0] = fmaxf(mx[0], fabsf(gg));
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+          const float a = v[1 + k][j] * (u[1 + k] * al[j]);
+          row[static_cast<int64_t>(1 + k) * Pr.kn] = a;
+          mx[1 + k] = fmaxf(mx[1 + k], fabsf(a));
+        }
+      }
+    }
+  }
+  __device__ void end_tile() {
+    if (!valid) return;
+#pragma unroll
+    for (int k = 0; k <= P; ++k)
+      if (mx[k] > 0.0f) atomicMax(Pr.colmax + k * Pr.kn + node, __float_as_uint(mx[k]));
+  }
+  __device__ void finish() {}
+};
+
+// Scale of each node column: a power of two that takes its largest value
+// into [2^14, 2^15) (0 for a column that is zero throughout, and for the
+// padding columns).
+__global__ void lr_sigma_kernel(const unsigned int* __restrict__ colmax, int kb, float* sigma) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kb) return;
+  const float mx = __uint_as_float(colmax[i]);
+  sigma[i] = mx > 0.0f ? ldexpf(1.0f, min(14 - ilogbf(mx), 100)) : 0.0f;
+}
+
+// The SNP-side operand of the interpolated accumulators: val * sigma of its
+// column as FP16 hi + lo, four values per thread (kb is a multiple of 64).
+// Columns of scale 0 are written as 0 without reading val (padding columns
+// are never written by the node pass).
+__global__ void lr_split_kernel(const float* __restrict__ val, int64_t total, int kb,
+                                const float* __restrict__ sigma, __half* hi, __half* lo) {
+  const int64_t n4 = total / 4;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n4;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int c0 = static_cast<int>((4 * i) % kb);
+    float x[4];
+    const float4 sg = *reinterpret_cast<const float4*>(sigma + c0);
+    const float sv[4] = {sg.x, sg.y, sg.z, sg.w};
+    const bool any = sv[0] != 0.0f || sv[1] != 0.0f || sv[2] != 0.0f || sv[3] != 0.0f;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (any) v = reinterpret_cast<const float4*>(val)[i];
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    uint32_t hw[2], lw[2];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) x[t] = sv[t] != 0.0f ? vv[t] * sv[t] : 0.0f;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const __half h0 = __float2half_rn(x[2 * t]), h1 = __float2half_rn(x[2 * t + 1]);
+      const __half l0 = __float2half_rn(x[2 * t] - __half2float(h0));
+      const __half l1 = __float2half_rn(x[2 * t + 1] - __half2float(h1));
+      hw[t] = static_cast<uint32_t>(__half_as_ushort(h0)) | (static_cast<uint32_t>(__half_as_ushort(h1)) << 16);
+      lw[t] = static_cast<uint32_t>(__half_as_ushort(l0)) | (static_cast<uint32_t>(__half_as_ushort(l1)) << 16);
+    }
+    reinterpret_cast<uint2*>(hi)[i] = make_uint2(hw[0], hw[1]);
+    reinterpret_cast<uint2*>(lo)[i] = make_uint2(lw[0], lw[1]);
+  }
+}
+
+constexpr int kLrNodes = 12;     // Chebyshev-Lobatto nodes per interval of ln(delta)
+constexpr double kLrSpan = 3.0;  // longest interval of ln(delta)
+
+// Gene-side operands of the interpolated accumulators, one thread per gene:
+// the Lagrange weights l_j(a) of the gene's interval (a = ln delta, nodes
+// node_a[base .. base + kLrNodes), base = q (kLrNodes - 1)) over each kind's
+// column scale, times a power of two per gene and kind, as FP16 hi + lo at
+// [g][kind * kn + base + j] (rows zeroed beforehand), and that power's
+// inverse as the unscale of gg (kind 0) and a_k (kind 1 + k).
+__global__ void lr_coef_kernel(const double* __restrict__ delta, int G, const double* __restrict__ node_a,
+                               double a0, double h, int nint, const float* __restrict__ sigma, int kn, int kb,
+                               int P, __half* hi, __half* lo, float* unscale) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  double a = log(fmax(delta[g], 1e-300));
+  if (!(a == a)) a = a0;
+  int q = static_cast<int>(floor((a - a0) / h));
+  q = q < 0 ? 0 : (q >= nint ? nint - 1 : q);
+  const int base = q * (kLrNodes - 1);
+  double l[kLrNodes];
+#pragma unroll
+  for (int j = 0; j < kLrNodes; ++j) {
+    double t = 1.0;
+#pragma unroll
+    for (int i = 0; i < kLrNodes; ++i)
+      if (i != j) t *= (a - node_a[base + i]) / (node_a[base + j] - node_a[base + i]);
+    l[j] = t;
+  }
+  for (int kind = 0; kind <= P; ++kind) {
+    const float* sg = sigma + kind * kn + base;
+    double mx = 0.0;
+#pragma unroll
+    for (int j = 0; j < kLrNodes; ++j)
+      if (sg[j] != 0.0f) mx = fmax(mx, fabs(l[j] / static_cast<double>(sg[j])));
+    const double sc = mx > 0.0 ? ldexp(1.0, 10 - ilogb(mx)) : 1.0;
+    __half* hr = hi + static_cast<int64_t>(g) * kb + kind * kn + base;
+    __half* lr = lo + static_cast<int64_t>(g) * kb + kind * kn + base;
+#pragma unroll
+    for (int j = 0; j < kLrNodes; ++j) {
+      const double y = sg[j] != 0.0f ? l[j] / static_cast<double>(sg[j]) * sc : 0.0;
+      const __half hv = __double2half(y);
+      hr[j] = hv;
+      lr[j] = __double2half(y - static_cast<double>(__half2float(hv)));
+    }
+    unscale[static_cast<int64_t>(g) * (P + 2) + (kind == 0 ? P + 1 : kind)] = static_cast<float>(1.0 / sc);
+  }
+}
 
 // ---------------------------------------- any number of covariates (p >= 3)
 // With A00 = X~'W X~ and U U' = A00^-1 (Cholesky of the REML kernel's ainv),
@@ -1380,6 +1570,22 @@ struct EpiOf<dev::LmmEpiParams<2>> {
 template <>
 struct EpiOf<dev::LmmRawEpiParams<1>> {
   using type = dev::LmmEpi<1, false, true>;
+};
+template <>
+struct EpiOf<dev::LmmLrEpiParams<1>> {
+  using type = dev::LmmEpi<1, false, true, true>;
+};
+template <>
+struct EpiOf<dev::LmmLrEpiParams<2>> {
+  using type = dev::LmmEpi<2, false, true, true>;
+};
+template <>
+struct EpiOf<dev::LmmNodeEpiParams<1>> {
+  using type = dev::LmmNodeEpi<1>;
+};
+template <>
+struct EpiOf<dev::LmmNodeEpiParams<2>> {
+  using type = dev::LmmNodeEpi<2>;
 };
 template <>
 struct EpiOf<dev::LmmRawEpiParams<2>> {
@@ -1939,6 +2145,186 @@ static std::vector<double> lmm_tiny_p(eqtl_ctx* ctx, int p, double df, const std
   return out;
 }
 
+// Which form of the exact-operand scan (p <= 2, dense) forms gg and a_k:
+// interpolated between node deltas (lmm_lr_prepare) from 256 genes on, where
+// the node pass costs less than it saves, otherwise directly. EQTL_LMM_FORM
+// = "direct" or "lr" fixes the form for every gene count.
+static bool lmm_lr_wanted(int G) {
+  const char* f = std::getenv("EQTL_LMM_FORM");
+  if (f && std::strcmp(f, "direct") == 0) return false;
+  if (f && std::strcmp(f, "lr") == 0) return true;
+  return G >= 256;
+}
+
+// Interpolated gg and a_k: Chebyshev-Lobatto nodes over the genes' range of
+// ln(delta) (5 or 11 equal intervals, whichever first keeps them within
+// kLrSpan, kLrNodes nodes each, neighbours sharing their end node), the node genes' operands (w and Q (w o X~_k) at
+// each node delta, as lmm_gene_ops_raw_kernel forms a gene's), the node pass
+// over every kept SNP, then both sides of the scan's gg and a_k accumulators
+// (ws.lr_phi / lr_plo: SNP side [m][kb]; ws.lr_chi / lr_clo: gene side
+// [G][kb]; ws.unscale of gg and a_k). Returns false, leaving the direct form,
+// when the nodes would not fit one gene-side tile.
+template <int P>
+static bool lmm_lr_prepare(eqtl_ctx* ctx, int n, int G, float s2) {
+  Workspace& ws = ctx->ws;
+  const Geno& g = ctx->geno;
+  const Rotated& R = ctx->rot;
+  cudaStream_t st = ctx->stream;
+  constexpr int nops = P + 2;
+  const int k_pad = g.k_pad;
+  const int64_t m = g.m;
+  std::vector<double> d(static_cast<size_t>(G));
+  ws.delta.download(d.data(), d.size(), st);
+  EQTL_CUDA(cudaStreamSynchronize(st));
+  double lo = INFINITY, hi = -INFINITY;
+  for (double x : d) {
+    const double a = std::log(std::max(x, 1e-300));
+    if (std::isfinite(a)) {
+      lo = std::min(lo, a);
+      hi = std::max(hi, a);
+    }
+  }
+  if (!(lo <= hi)) lo = hi = 0.0;
+  if (hi - lo < 1e-6) {
+    lo -= 0.5;
+    hi += 0.5;
+  }
+  // as many intervals as one or two 64-column chunks of nodes hold (5 or 11)
+  const int nint = static_cast<int>(std::ceil((hi - lo) / kLrSpan)) <= 5 ? 5 : 11;
+  const double h = (hi - lo) / nint;
+  const int nn = nint * (kLrNodes - 1) + 1;
+  if (nn > kTileM) return false;
+  std::vector<double> na(static_cast<size_t>(nn)), nd(static_cast<size_t>(nn));
+  for (int q = 0; q < nint; ++q)
+    for (int i = 0; i < kLrNodes; ++i)
+      na[static_cast<size_t>(q * (kLrNodes - 1) + i)] =
+          lo + h * (q + 0.5 * (1.0 - std::cos(M_PI * i / (kLrNodes - 1))));
+  for (int j = 0; j < nn; ++j) nd[static_cast<size_t>(j)] = std::exp(na[static_cast<size_t>(j)]);
+  const int kn = nn <= 64 ? 64 : 128, kb = (P + 1) * kn;
+  ws.lr_kn = kn;
+  ws.lr_kb = kb;
+  ws.lr_nodes = nn;
+  ws.lr_a.upload(na.data(), na.size(), st);
+  ws.lr_delta.upload(nd.data(), nd.size(), st);
+
+  // node genes' operands: a zero residual (u = 0), w o X~_k, Q times them
+  const size_t cols = static_cast<size_t>(nn) * (P + 1);
+  ws.lr_zero.alloc(static_cast<size_t>(nn) * (n + P));
+  ws.lr_zero.zero(st);
+  ws.lr_w.alloc(static_cast<size_t>(n) * cols);
+  ws.lr_uv.alloc(static_cast<size_t>(n) * cols);
+  ++ctx->launches;
+  lmm_uv_w_kernel<<<nn, 256, 0, st>>>(ws.lr_zero.p, ws.Xtil.p, ctx->basis.lambda.p, ws.lr_delta.p,
+                                      ws.lr_zero.p + static_cast<size_t>(nn) * n, n, P, nn, ws.lr_w.p);
+  EQTL_CUDA(cudaGetLastError());
+  const double one = 1.0, zero = 0.0;
+  EQTL_CHECK(cublasDgemm(blas_of(ctx), CUBLAS_OP_N, CUBLAS_OP_N, n, static_cast<int>(cols), n, &one,
+                         ctx->basis.Q.p, n, ws.lr_w.p, n, &zero, ws.lr_uv.p, n) == CUBLAS_STATUS_SUCCESS,
+             EQTL_E_CUDA, "Q (w o X~) at the node deltas failed");
+  ctx->launches += 1;
+  __half* nptr[2 * nops];
+  for (int k = 0; k < nops; ++k) {
+    ws.lr_ops_hi[k].alloc(static_cast<size_t>(nn) * k_pad);
+    ws.lr_ops_lo[k].alloc(static_cast<size_t>(nn) * k_pad);
+    nptr[k] = ws.lr_ops_hi[k].p;
+    nptr[nops + k] = ws.lr_ops_lo[k].p;
+  }
+  ws.lr_ops_ptr.upload(nptr, 2 * nops, st);
+  ws.lr_unscale.alloc(static_cast<size_t>(nn) * nops);
+  ++ctx->launches;
+  lmm_gene_ops_raw_kernel<<<nn, 256, 0, st>>>(ws.lr_uv.p, ctx->basis.lambda.p, ws.lr_delta.p, n, P, nn, k_pad, s2,
+                                              ws.lr_ops_ptr.p, ws.lr_ops_ptr.p + nops, ws.lr_unscale.p);
+  EQTL_CUDA(cudaGetLastError());
+
+  // node pass: accumulators [gg, a_0 ..] against Gt^2 and the raw operand
+  ws.lr_val.alloc(static_cast<size_t>(m) * kb);
+  ws.lr_colmax.alloc(static_cast<size_t>(kb));
+  ws.lr_colmax.zero(st);
+  if (m > 0) {
+    LmmNodeEpiParams<P> ep{};
+    ep.n_nodes = nn;
+    ep.m = m;
+    ep.kn = kn;
+    ep.kb = kb;
+    ep.unscale = ws.lr_unscale.p;
+    ep.snp_alpha = R.alpha.p;
+    ep.val = ws.lr_val.p;
+    ep.colmax = ws.lr_colmax.p;
+    const __half* ah[P + 1];
+    const __half* al[P + 1];
+    int bsel[P + 1], prod[P + 1];
+    ah[0] = ws.lr_ops_hi[P + 1].p;
+    al[0] = ws.lr_ops_lo[P + 1].p;
+    bsel[0] = 1;
+    prod[0] = 7;
+    for (int k = 0; k < P; ++k) {
+      ah[1 + k] = ws.lr_ops_hi[1 + k].p;
+      al[1 + k] = ws.lr_ops_lo[1 + k].p;
+      bsel[1 + k] = 0;
+      prod[1 + k] = 5;
+    }
+    const __half* bh[2] = {R.raw.p, R.gt2_hi.p};
+    const __half* bl[2] = {R.raw.p, R.gt2_lo.p};
+    launch_tile_n<128, P + 1>(ctx, false, ep, ah, al, nn, bh, bl, m, k_pad, bsel, prod);
+  }
+  ws.lr_sigma.alloc(static_cast<size_t>(kb));
+  ++ctx->launches;
+  lr_sigma_kernel<<<(kb + 255) / 256, 256, 0, st>>>(ws.lr_colmax.p, kb, ws.lr_sigma.p);
+  EQTL_CUDA(cudaGetLastError());
+  ws.lr_phi.alloc(std::max<size_t>(1, static_cast<size_t>(m) * kb));
+  ws.lr_plo.alloc(std::max<size_t>(1, static_cast<size_t>(m) * kb));
+  if (m > 0) {
+    ++ctx->launches;
+    lr_split_kernel<<<4 * sm_count(ctx), 256, 0, st>>>(ws.lr_val.p, m * kb, kb, ws.lr_sigma.p, ws.lr_phi.p,
+                                                       ws.lr_plo.p);
+    EQTL_CUDA(cudaGetLastError());
+  }
+  // genes' coefficients (rows zero outside each gene's nodes)
+  ws.lr_chi.alloc(static_cast<size_t>(G) * kb);
+  ws.lr_clo.alloc(static_cast<size_t>(G) * kb);
+  ws.lr_chi.zero(st);
+  ws.lr_clo.zero(st);
+  ++ctx->launches;
+  lr_coef_kernel<<<(G + 127) / 128, 128, 0, st>>>(ws.delta.p, G, ws.lr_a.p, lo, h, nint, ws.lr_sigma.p, kn, kb, P,
+                                                  ws.lr_chi.p, ws.lr_clo.p, ws.unscale.p);
+  EQTL_CUDA(cudaGetLastError());
+  return true;
+}
+
+// The scan with interpolated gg and a_k: tile order [gg, a_0 .., NUM]; gg
+// and a_k read their kind's node columns of both interpolated operands
+// (K chunks [kind c, (kind + 1) c), c = kn / 64), NUM reads u hi + lo
+// against the exact raw operand over all of K. ah / al: the gene-ops order
+// [NUM, a_0 .., gg] (only NUM's u is read).
+template <int P>
+static void lmm_launch_lr(eqtl_ctx* ctx, const LmmLrEpiParams<P>& ep, const __half* const* ah,
+                          const __half* const* al, int G, const Rotated& R) {
+  Workspace& ws = ctx->ws;
+  const int kb = ws.lr_kb, c = ws.lr_kn / kChunkK;
+  const __half* oh[P + 2];
+  const __half* ol[P + 2];
+  int bsel[P + 2], prod[P + 2];
+  TileK tk;
+  for (int j = 0; j <= P; ++j) {
+    oh[j] = ws.lr_chi.p;
+    ol[j] = ws.lr_clo.p;
+    bsel[j] = 1;
+    prod[j] = 7;
+    tk.beg[j] = j * c;
+    tk.end[j] = (j + 1) * c;
+    tk.k_a[j] = kb;
+  }
+  oh[P + 1] = ah[0];
+  ol[P + 1] = al[0];
+  bsel[P + 1] = 0;
+  prod[P + 1] = 5;
+  tk.k_b[1] = kb;
+  const __half* bh[2] = {R.raw.p, ws.lr_phi.p};
+  const __half* bl[2] = {R.raw.p, ws.lr_plo.p};
+  launch_tile_n<128, P + 2>(ctx, false, ep, oh, ol, G, bh, bl, R.m, R.k_pad, bsel, prod, nullptr, 0, 1, P + 2, 0,
+                            &tk);
+}
+
 // Subset gate of every kept SNP on the analysis samples into ws.ok.
 static void lmm_gate(eqtl_ctx* ctx) {
   Geno& g = ctx->geno;
@@ -2018,6 +2404,12 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
                                            k_pad, s1, s2, ws.ops_ptr.p, ws.ops_ptr.p + nops, unscale.p);
   }
   EQTL_CUDA(cudaGetLastError());
+  // dense scans with the exact operand: gg and a_k interpolated between node
+  // deltas when that pays (lmm_lr_wanted)
+  bool lr = false;
+  ws.lr_nodes = 0;
+  if (raw && prm->exclude_cis != 2 && lmm_lr_wanted(G))
+    lr = p == 1 ? lmm_lr_prepare<1>(ctx, n, G, s2) : lmm_lr_prepare<2>(ctx, n, G, s2);
   if (simt) {
     // the FP32 form's gene-side operands, in the tile's accumulator order
     // [gg, a_0 .. a_{p-1}, NUM] (the gene-ops order is [NUM, a.., gg])
@@ -2099,12 +2491,15 @@ static void scan_trans_lmm_impl(eqtl_ctx* ctx, const eqtl_scan_params* prm, cons
       ep.snp_alpha = ctx->rot.alpha.p;
       so.run([&](GeneOut out) {
         ep.out = out;
-        lmm_launch<P>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
+        if constexpr (std::is_same_v<std::decay_t<decltype(ep)>, LmmLrEpiParams<P>>) lmm_launch_lr<P>(ctx, ep, ah, al, G, ctx->rot);
+        else lmm_launch<P>(ctx, ep, ah, al, G, simt, tiles, n_tiles, ctx->rot);
       });
     };
     using P1 = std::integral_constant<int, 1>;
     using P2 = std::integral_constant<int, 2>;
-    if (raw && p == 1) run(LmmRawEpiParams<1>{}, P1{});
+    if (lr && p == 1) run(LmmLrEpiParams<1>{}, P1{});
+    else if (lr) run(LmmLrEpiParams<2>{}, P2{});
+    else if (raw && p == 1) run(LmmRawEpiParams<1>{}, P1{});
     else if (raw) run(LmmRawEpiParams<2>{}, P2{});
     else if (p == 1) run(LmmEpiParams<1>{}, P1{});
     else run(LmmEpiParams<2>{}, P2{});

@@ -88,18 +88,30 @@ inline int64_t expected_candidates(const eqtl_scan_params* prm, int64_t m) {
 void make_map_2d(CUtensorMap* map, const void* base, uint64_t rows, uint64_t k_pad, uint32_t box_rows, bool bf16);
 int sm_count(eqtl_ctx* ctx);
 
+// Per-accumulator K ranges and operand K extents of one tile launch: an
+// accumulator j with end[j] > 0 runs over the K chunks [beg[j], end[j]) of
+// its own operands instead of the whole K (ksplit 1, no sub-ranges).
+struct TileK {
+  int beg[dev::kMaxAcc] = {};
+  int end[dev::kMaxAcc] = {};
+  int k_a[dev::kMaxAcc] = {};  // K extent of accumulator j's gene-side operand (0: k_pad)
+  int k_b[2] = {};             // K extent of SNP-side pair b (0: k_pad)
+};
+
 // Launches the persistent tile kernel for NACC accumulators. a_*[j] are the
 // gene-side hi/lo operands of accumulator j ([rows_a, k_pad]); b_*[0..1] the
 // SNP-side pairs ([rows_b, k_pad]); bsel[j] picks the pair, prod[j] the
 // products. tiles: optional explicit tile list (device pointer) + count.
 // BL: where the SNP-side lo parts go (dev::kBLoStage; kBLoNone: exact SNP
 // operands, no product may have bit 2, and more ring stages fit). kc_sub:
-// K chunks per sub-range (0: none; single-group epilogues only).
+// K chunks per sub-range (0: none; single-group epilogues only). tk:
+// per-accumulator K ranges (TileK; null: every accumulator over all of K).
 template <int NT, int NACC, class EpiParams, int BL = dev::kBLoStage>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list = nullptr,
-                   int n_tile_list = 0, int ksplit = 1, int n_acc = NACC, int kc_sub = 0);
+                   int n_tile_list = 0, int ksplit = 1, int n_acc = NACC, int kc_sub = 0,
+                   const TileK* tk = nullptr);
 
 }  // namespace eqtl
 
@@ -113,7 +125,7 @@ template <int NT, int NACC, class EpiParams, int BL>
 void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* const* a_hi,
                    const __half* const* a_lo, int64_t rows_a, const __half* const* b_hi, const __half* const* b_lo,
                    int64_t rows_b, int k_pad, const int* bsel, const int* prod, const int2* tile_list,
-                   int n_tile_list, int ksplit, int n_acc, int kc_sub) {
+                   int n_tile_list, int ksplit, int n_acc, int kc_sub, const TileK* tk) {
   using Epi = typename EpiOf<EpiParams>::type;
   using C = dev::TileCfg<NT, NACC, BL>;
   dev::TileMaps maps;
@@ -121,14 +133,16 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   EQTL_CHECK(n_acc >= 1 && n_acc <= dev::kMaxAcc && (n_acc == NACC || Epi::kGrouped), EQTL_E_INTERNAL,
              "tile kernel: accumulator count");
   for (int j = 0; j < n_acc; ++j) {
-    make_map_2d(&maps.a[2 * j], a_hi[j], rows_a, k_pad, dev::kTileM, bf16);
-    make_map_2d(&maps.a[2 * j + 1], a_lo[j], rows_a, k_pad, dev::kTileM, bf16);
+    const int ka = tk && tk->k_a[j] > 0 ? tk->k_a[j] : k_pad;
+    make_map_2d(&maps.a[2 * j], a_hi[j], rows_a, ka, dev::kTileM, bf16);
+    make_map_2d(&maps.a[2 * j + 1], a_lo[j], rows_a, ka, dev::kTileM, bf16);
   }
   int npairs = 0;
   for (int j = 0; j < n_acc; ++j) npairs = std::max(npairs, bsel[j] + 1);
   for (int b = 0; b < npairs; ++b) {
-    make_map_2d(&maps.b[2 * b], b_hi[b], rows_b, k_pad, NT, bf16);
-    make_map_2d(&maps.b[2 * b + 1], b_lo[b], rows_b, k_pad, NT, bf16);
+    const int kb = tk && tk->k_b[b] > 0 ? tk->k_b[b] : k_pad;
+    make_map_2d(&maps.b[2 * b], b_hi[b], rows_b, kb, NT, bf16);
+    make_map_2d(&maps.b[2 * b + 1], b_lo[b], rows_b, kb, NT, bf16);
   }
   for (int b = npairs; b < 2; ++b) {
     maps.b[2 * b] = maps.b[0];
@@ -143,6 +157,19 @@ void launch_tile_n(eqtl_ctx* ctx, bool bf16, const EpiParams& ep, const __half* 
   for (int j = 0; j < dev::kMaxAcc; ++j) {
     sh.bsel[j] = j < n_acc ? bsel[j] : 0;
     sh.prod[j] = j < n_acc ? prod[j] : 0;
+    if (tk && j < n_acc && tk->end[j] > 0) {
+      // the range lies inside both operands' K extents and is not empty
+      const int ka = tk->k_a[j] > 0 ? tk->k_a[j] : k_pad, kb = tk->k_b[sh.bsel[j]] > 0 ? tk->k_b[sh.bsel[j]] : k_pad;
+      EQTL_CHECK(tk->beg[j] >= 0 && tk->beg[j] < tk->end[j] && tk->end[j] * dev::kChunkK <= std::min(ka, kb) &&
+                     ksplit == 1 && kc_sub == 0,
+                 EQTL_E_INTERNAL, "tile kernel: accumulator K range");
+      sh.kc_beg[j] = tk->beg[j];
+      sh.kc_end[j] = tk->end[j];
+    } else {
+      EQTL_CHECK(!tk || j >= n_acc || ((tk->k_a[j] <= 0 || tk->k_a[j] == k_pad) &&
+                                       (tk->k_b[sh.bsel[j]] <= 0 || tk->k_b[sh.bsel[j]] == k_pad)),
+                 EQTL_E_INTERNAL, "tile kernel: an accumulator over all of K needs operands of K extent k_pad");
+    }
     EQTL_CHECK(BL != dev::kBLoNone || !(sh.prod[j] & 2), EQTL_E_INTERNAL,
                "tile kernel: hi*lo product without SNP-side lo parts");
   }

@@ -81,6 +81,8 @@ struct TileShape {
   int kc_sub;             // K chunks per sub-range (0: the whole range). Each sub-range starts its
                           // accumulators afresh and goes through the epilogue on its own, which
                           // sums the sub-ranges of a work item itself (single-group epilogues)
+  int kc_beg[kMaxAcc];    // K-chunk range [kc_beg, kc_end) of accumulator j; kc_end 0: the work item's
+  int kc_end[kMaxAcc];    // range (an accumulator with its own range needs ksplit 1, no sub-ranges)
   const int2* tile_list;  // optional explicit (tile_a, tile_b) list (banded scans); null = dense
   uint32_t* status;       // device status word (DevStatus)
 };
@@ -204,13 +206,14 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         const int ksub = sh.kc_sub > 0 ? sh.kc_sub : k1 - k0;
         for (int q0 = k0; q0 < k1 && ok; q0 += ksub)
         for (int j = 0; j < sh.n_acc && ok; ++j) {
-          const int q1 = min(k1, q0 + ksub);
+          const bool own = sh.kc_end[j] > 0;
+          const int qa = own ? sh.kc_beg[j] : q0, qb = own ? sh.kc_end[j] : min(k1, q0 + ksub);
           const int bp = sh.bsel[j];
           // only the lo parts some product of this accumulator reads are loaded
           const bool a_lo = (sh.prod[j] & 4) != 0, b_lo = BL == kBLoStage && (sh.prod[j] & 2) != 0;
           const uint32_t bytes = static_cast<uint32_t>(C::A_BYTES + C::B_BYTES + (a_lo ? C::A_BYTES : 0) +
                                                        (b_lo ? C::B_BYTES : 0));
-          for (int kc = q0; kc < q1; ++kc) {
+          for (int kc = qa; kc < qb; ++kc) {
             if (!mbar_wait(&empty[stage], phase ^ 1u, status, abort_flag, kDevTimeoutEmpty)) {
               ok = false;
               break;
@@ -259,7 +262,6 @@ __global__ void __launch_bounds__(kTileThreads, 1)
         const int ksub = sh.kc_sub > 0 ? sh.kc_sub : k1 - k0;
         for (int q0 = k0; q0 < k1 && ok; q0 += ksub)
         for (int grp = 0; grp < sh.n_groups && ok; ++grp, slot0 = (slot0 + NACC) % C::NSLOTS) {
-          const int q1 = min(k1, q0 + ksub);
           const int j0 = grp * NACC;
           const int nv = min(NACC, sh.n_acc - j0);
           int last = 0;
@@ -274,7 +276,9 @@ __global__ void __launch_bounds__(kTileThreads, 1)
             tc_fence_after();
             const uint32_t d = tmem_base + static_cast<uint32_t>(slot * NT);
             const int pm = sh.prod[j0 + jj];
-            for (int kc = q0; kc < q1; ++kc) {
+            const bool own = sh.kc_end[j0 + jj] > 0;
+            const int qa = own ? sh.kc_beg[j0 + jj] : q0, qb = own ? sh.kc_end[j0 + jj] : min(k1, q0 + ksub);
+            for (int kc = qa; kc < qb; ++kc) {
               if (!mbar_wait(&full[stage], phase, status, abort_flag, kDevTimeoutFull)) {
                 ok = false;
                 break;
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(kTileThreads, 1)
                 const uint32_t off = static_cast<uint32_t>(k * 32);
                 // the first product of a (sub-)range starts the accumulator;
                 // every later one adds
-                uint32_t accum = (kc > q0 || k > 0) ? 1u : 0u;
+                uint32_t accum = (kc > qa || k > 0) ? 1u : 0u;
                 if (pm & 1) {
                   umma_f16(d, smem_desc_sw128(sa0 + off), smem_desc_sw128(sb0 + off), idesc, accum);
                   accum = 1u;

@@ -67,6 +67,12 @@ int eqtl_set_precision(eqtl_ctx* ctx, int precision);
 int eqtl_stage_ms(eqtl_ctx* ctx, int stage, double* ms);
 /* Number of kernels the library has launched on this context. */
 int eqtl_launch_count(eqtl_ctx* ctx, uint64_t* count);
+/* How the most recent LMM scan (p <= 2, split FP16) formed gg and a_k:
+ * *nodes = 0 directly (K = n); otherwise interpolated between *nodes node
+ * deltas, K = *node_cols per accumulator. EQTL_LMM_FORM=direct|lr in the
+ * environment fixes the form (default: interpolated from 256 genes on, in
+ * dense scans). */
+int eqtl_lmm_form(eqtl_ctx* ctx, int32_t* nodes, int32_t* node_cols);
 /* The cudaStream_t all work of this context is issued on (for callers that
  * time or order their own work against it). */
 int eqtl_stream(eqtl_ctx* ctx, void** stream);

@@ -78,6 +78,39 @@ def test_trans_lmm_matches_oracle(ncov, prec):
     _check_scan(res[:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[1 if prec == 1 else 0], rel=1e-6)
 
 
+@pytest.mark.parametrize("ncov", [0, 1])
+def test_trans_lmm_interpolated_matches_oracle(ncov, monkeypatch):
+    """gg and a_k interpolated between node deltas (EQTL_LMM_FORM=lr; the
+    default from 256 genes on) on genes whose REML deltas span the search
+    range: pure noise (delta at its lower end), mostly polygenic, and the
+    rest. The direct form of the same scan agrees with the oracle too."""
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(ncov=ncov, G=96)
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    rng = np.random.default_rng(11)
+    Y = Y.copy()
+    Y[:, :8] = rng.standard_normal((n, 8))
+    Y[:, 8:16] = (Q * np.sqrt(lam)) @ rng.standard_normal((n, 8)) + 1e-3 * rng.standard_normal((n, 8))
+    res = {}
+    for form in ("lr", "direct"):
+        monkeypatch.setenv("EQTL_LMM_FORM", form)
+        with capi.Context(0) as c:
+            c.load_bed(rows, n, np.arange(n))
+            c.set_basis(Q, lam)
+            res[form] = c.scan_trans_lmm(Y, X, pthr=1e-3)
+    d = res["lr"][3]
+    assert np.array_equal(d, res["direct"][3])            # REML does not depend on the form
+    assert d.min() < 1e-4 and d.max() > 1e2, (d.min(), d.max())
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-3)
+    ora, pairs_ref = _at_device_delta(d, ora, pairs_ref, dec.dosage[k], Y, X, Q, lam)
+    for form in ("lr", "direct"):
+        _check_scan(res[form][:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
+
+
 def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam, pthr=1e-3, excl=None):
     """REML delta: wherever the device's delta differs from the oracle's, it
     must be an optimum of the same objective (-loglik within 1e-6 of the
