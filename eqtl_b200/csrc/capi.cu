@@ -140,7 +140,7 @@ void residualize_genes(eqtl_ctx* ctx, const double* dX, const double* dXtXinv, i
   // XtY = X' Y  [p, G]
   EQTL_BLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, p, G, n, &one, dX, n, dY, n, &zero, dXtY, p));
   // C = XtXinv XtY (XtXinv symmetric; row-major == column-major)
-  DevBuf<double> C;
+  DevBuf<double>& C = ctx->ws.resid_C;
   C.alloc(static_cast<size_t>(p) * G);
   EQTL_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, p, G, p, &one, dXtXinv, p, dXtY, p, &zero, C.p, p));
   // Y <- Y - X C
@@ -790,8 +790,8 @@ int eqtl_pheno_int(eqtl_ctx* ctx, double* Y, int32_t n, int32_t n_cols) {
 
 int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_used_out) {
   return guarded(ctx, [&] {
-    eqtl::DevBuf<double> K;
-    eqtl::DevBuf<int32_t> N;
+    eqtl::DevBuf<double>& K = ctx->ws.basis_K;
+    eqtl::DevBuf<int32_t>& N = ctx->ws.basis_N;
     const int64_t mu = eqtl::grm_compute(ctx, K, N);
     const int n = ctx->geno.n;
     if (K_out) K.download(K_out, static_cast<size_t>(n) * n, ctx->stream);
@@ -819,13 +819,12 @@ int eqtl_lmm_basis_fast(eqtl_ctx* ctx, const double* K, int32_t n, double sparsi
                         double* Q_out, int64_t* zeroed_out) {
   return guarded(ctx, [&] {
     EQTL_CHECK(sparsify_thr >= 0.0, EQTL_E_ARG, "sparsify threshold must be >= 0");
-    eqtl::DevBuf<double> dK;
+    eqtl::DevBuf<double>& dK = ctx->ws.basis_K;
     if (K) {
       EQTL_CHECK(n > 0, EQTL_E_ARG, "n must be positive");
       dK.upload(K, static_cast<size_t>(n) * n, ctx->stream);
     } else {
-      eqtl::DevBuf<int32_t> N;
-      eqtl::grm_compute(ctx, dK, N);
+      eqtl::grm_compute(ctx, dK, ctx->ws.basis_N);
       n = ctx->geno.n;
     }
     eqtl::lmm_basis_from_grm(ctx, dK.p, n, sparsify_thr, zeroed_out);

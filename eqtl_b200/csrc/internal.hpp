@@ -252,6 +252,12 @@ struct Workspace {
   DevBuf<unsigned long long> grm_count;  // SNPs the GRM uses
   DevBuf<unsigned long long> raw_inexact;  // SNPs the exact LMM operand cannot hold
   DevBuf<double> lmm_w, lmm_uv;            // [n, G (p + 1)]: w o (r~, X~_k) and Q times them
+  // per-call scratch kept with the context, so warm calls allocate nothing:
+  // the GRM and its joint-missing counts of eqtl_grm / eqtl_lmm_basis, the
+  // --fast sparsification count, the covariate coefficients of the LM prep
+  DevBuf<double> basis_K, resid_C;
+  DevBuf<int32_t> basis_N;
+  DevBuf<unsigned long long> sparsify_cnt;
   // interpolated LMM scan (lmm_lr_prepare): node log-deltas and deltas, the
   // node pass's gene-side operands, its FP32 table [m][lr_kb] with the column
   // maxima and scales, the split SNP-side table and the genes' coefficients

@@ -1647,7 +1647,7 @@ void lmm_basis_from_grm(eqtl_ctx* ctx, const double* K_dev, int n, double sparsi
   B.lambda.alloc(n);
   EQTL_CUDA(cudaMemcpyAsync(B.Q.p, K_dev, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st));
   if (sparsify_thr > 0) {
-    DevBuf<unsigned long long> cnt;
+    DevBuf<unsigned long long>& cnt = ctx->ws.sparsify_cnt;
     cnt.alloc(1);
     cnt.zero(st);
     ++ctx->launches;
