@@ -969,21 +969,9 @@ struct LmmEpi {
     float al[16];
     if constexpr (RAW) load16(Pr.snp_alpha + s0, al);
     if (!GLM && tt.lt_u) {  // uniform across the launch
-      float uu[16];
-      bool valid[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int64_t s = s0 + j;
-        valid[j] = flag16(okw, j) && s < Pr.m && acc.in_scope(Pr.win, s);
-        float num = v[0][j] * u[0];
-        if constexpr (RAW) num *= al[j];
-        const float S = ci == 0 ? S0[j] : S1[j];
-        const float r = num * __fdividef(num, S) * inv_rss;
-        const float omr = 1.0f - r;
-        uu[j] = S > 1e-15f && omr > 0.0f ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2, never NaN
-        if (!valid[j]) uu[j] = 0.0f;
-      }
-      screen16_cubic(tt, uu, valid, u_cand, Pr.out, gene, s0, acc);
+      // a gw scan (no windows) skips the per-pair window test altogether
+      if (Pr.win.mode == kWinNone) post_cubic<false>(ci, s0, v[0], okw, al);
+      else post_cubic<true>(ci, s0, v[0], okw, al);
       return;
     }
 #pragma unroll
@@ -1008,6 +996,26 @@ struct LmmEpi {
       if (valid && (u >= u_cand || o.deferred)) emit_candidate(Pr.out, gene, s, o.deferred, o.tiny);
     }
     acc.end_chunk();
+  }
+  // Phase 2 with the per-interval cubics (screen16_cubic). The SNP flags are
+  // zero past the last kept SNP, so they also mask the padding.
+  template <bool WIN>
+  __device__ void post_cubic(int ci, int64_t s0, const float (&v)[16], const uint32_t (&okw)[4],
+                             const float (&al)[16]) {
+    float uu[16];
+    bool valid[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      valid[j] = flag16(okw, j) && (!WIN || acc.in_scope(Pr.win, s0 + j));
+      float num = v[j] * u[0];
+      if constexpr (RAW) num *= al[j];
+      const float S = ci == 0 ? S0[j] : S1[j];
+      const float r = num * __fdividef(num, S) * inv_rss;
+      const float omr = 1.0f - r;
+      uu[j] = S > 1e-15f && omr > 0.0f ? Pr.df * __fdividef(r, omr) : 0.0f;  // t^2, never NaN
+      if (!valid[j]) uu[j] = 0.0f;
+    }
+    screen16_cubic(tt, uu, valid, u_cand, Pr.out, gene, s0, acc);
   }
   // Both phases at once (the CUDA-core comparator): v in the tile's order.
   template <int NACC>
