@@ -265,6 +265,29 @@ dev::Windows upload_windows(eqtl_ctx* ctx, const eqtl_scan_params* prm, int64_t 
   w.gene_hi = ws.win_ghi.p;
   w.snp_chrom = ws.win_sc.p;
   w.snp_pos = ws.win_sp.p;
+  // 16-SNP block bounds, up to one 256-SNP tile past the last padded tile
+  const int64_t nb = ((m + 255) / 256 + 1) * 16;
+  std::vector<int32_t> bc(static_cast<size_t>(nb), -1);
+  std::vector<int64_t> blo(static_cast<size_t>(nb), 0), bhi(static_cast<size_t>(nb), -1);
+  for (int64_t b = 0; b * 16 < m; ++b) {
+    const int64_t s1 = std::min<int64_t>(m, b * 16 + 16);
+    int32_t c = prm->snp_chrom[b * 16];
+    int64_t lo = prm->snp_pos[b * 16], hi = lo;
+    for (int64_t s = b * 16 + 1; s < s1; ++s) {
+      if (prm->snp_chrom[s] != c) c = -1;
+      lo = std::min<int64_t>(lo, prm->snp_pos[s]);
+      hi = std::max<int64_t>(hi, prm->snp_pos[s]);
+    }
+    bc[static_cast<size_t>(b)] = c;
+    blo[static_cast<size_t>(b)] = lo;
+    bhi[static_cast<size_t>(b)] = hi;
+  }
+  ws.win_bc.upload(bc.data(), bc.size(), ctx->stream);
+  ws.win_blo.upload(blo.data(), blo.size(), ctx->stream);
+  ws.win_bhi.upload(bhi.data(), bhi.size(), ctx->stream);
+  w.blk_chrom = ws.win_bc.p;
+  w.blk_lo = ws.win_blo.p;
+  w.blk_hi = ws.win_bhi.p;
   return w;
 }
 

@@ -243,6 +243,8 @@ struct Workspace {
   // windows
   DevBuf<int32_t> win_gc, win_sc;
   DevBuf<int64_t> win_glo, win_ghi, win_sp;
+  DevBuf<int32_t> win_bc;            // Windows::blk_chrom
+  DevBuf<int64_t> win_blo, win_bhi;  // Windows::blk_lo / blk_hi
   DevBuf<float> tt_h, tt_L, tt_c1, tt_lt, tt_c1q, tt_ltq;
   double tt_df = -1;
   // GRM operands and accumulators, eigen-solver scratch

@@ -31,6 +31,12 @@ struct Windows {
   const int64_t* gene_hi;
   const int32_t* snp_chrom;
   const int64_t* snp_pos;
+  // per block of 16 kept SNPs (b = s / 16, covering the padded tiles): the
+  // block's chromosome (-1 where it mixes chromosomes or lies past the last
+  // SNP) and its smallest and largest position
+  const int32_t* blk_chrom;
+  const int64_t* blk_lo;
+  const int64_t* blk_hi;
 };
 
 // Per-thread (= per gene row) running state inside one tile.
@@ -61,6 +67,15 @@ struct GeneAcc {
       lo = w.gene_lo[g];
       hi = w.gene_hi[g];
     }
+  }
+  // true if no SNP of the 16-SNP block starting at s0 (a multiple of 16) can
+  // lie in this gene's window: a gene without one, or a block on another
+  // chromosome or wholly before or after it
+  __device__ __forceinline__ bool chunk_clear(const Windows& w, int64_t s0) const {
+    if (chrom < 0) return true;
+    const int64_t b = s0 >> 4;
+    const int32_t c = __ldg(w.blk_chrom + b);
+    return c >= 0 && (c != chrom || __ldg(w.blk_hi + b) < lo || __ldg(w.blk_lo + b) > hi);
   }
   // true if the (gene, snp) pair is part of this scope
   __device__ __forceinline__ bool in_scope(const Windows& w, int64_t s) const {

@@ -95,9 +95,12 @@ struct LmEpi {
       igv[4 * q + 3] = v4.w;
     }
     if (tt.lt_u) {  // uniform across the launch
-      // a gw scan (no windows) skips the per-pair window test altogether
-      if (P.win.mode == kWinNone) chunk_cubic<false>(s0, v[0], igv);
-      else chunk_cubic<true>(s0, v[0], igv);
+      // a gw scan (no windows), and a trans scan on a chunk clear of the
+      // gene's window, skip the per-pair window test
+      if (P.win.mode == kWinNone || (P.win.mode == kWinExclude && acc.chunk_clear(P.win, s0)))
+        chunk_cubic<false>(s0, v[0], igv);
+      else
+        chunk_cubic<true>(s0, v[0], igv);
       return;
     }
 #pragma unroll

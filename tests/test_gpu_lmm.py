@@ -85,7 +85,8 @@ def test_trans_lmm_interpolated_matches_oracle(ncov, monkeypatch):
     range: pure noise (delta at its lower end), mostly polygenic, and the
     rest. The direct form of the same scan agrees with the oracle too."""
     from eqtl_b200 import capi
-    g, rows, Y, X = _case(ncov=ncov, G=96)
+    # n = 250 < k_pad = 256 leaves the padding column the exact operand needs
+    g, rows, Y, X = _case(ncov=ncov, G=96, n=250, fam=(10, 6, 190))
     n = g.codes.shape[1]
     dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
     k = np.nonzero(dec.keep)[0]
@@ -102,6 +103,7 @@ def test_trans_lmm_interpolated_matches_oracle(ncov, monkeypatch):
             c.load_bed(rows, n, np.arange(n))
             c.set_basis(Q, lam)
             res[form] = c.scan_trans_lmm(Y, X, pthr=1e-3)
+            assert (c.lmm_form()[0] > 0) == (form == "lr")
     d = res["lr"][3]
     assert np.array_equal(d, res["direct"][3])            # REML does not depend on the form
     assert d.min() < 1e-4 and d.max() > 1e2, (d.min(), d.max())
@@ -109,6 +111,39 @@ def test_trans_lmm_interpolated_matches_oracle(ncov, monkeypatch):
     ora, pairs_ref = _at_device_delta(d, ora, pairs_ref, dec.dosage[k], Y, X, Q, lam)
     for form in ("lr", "direct"):
         _check_scan(res[form][:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
+
+
+@pytest.mark.parametrize("form", ["lr", "direct"])
+def test_trans_lmm_excludes_cis_windows(form, monkeypatch):
+    """The trans scope: each gene's cis window excluded (genes without a
+    location test every SNP). Windows of 0.8 Mb on 4 Mb chromosomes leave
+    16-SNP chunks clear of a gene's window (the chunk-level shortcut) and
+    chunks that straddle it (the per-pair test), in both forms of gg and a_k."""
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(seed=23, ncov=1, G=96, n=250, fam=(10, 6, 190))
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    chrom_id = {c: i for i, c in enumerate(sorted(set(g.chrom)))}
+    schrom = np.array([chrom_id[g.chrom[s]] for s in k], np.int32)
+    spos = g.pos[k]
+    rng = np.random.default_rng(2)
+    G = Y.shape[1]
+    gchrom = rng.integers(-1, 2, G).astype(np.int32)        # -1 = gene without location
+    center = rng.integers(1, 4_000_000, G)
+    glo, ghi = np.maximum(center - 400_000, 1), center + 400_000
+    monkeypatch.setenv("EQTL_LMM_FORM", form)
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n))
+        c.set_basis(Q, lam)
+        res = c.scan_trans_lmm(Y, X, pthr=1e-3, windows=(gchrom, glo, ghi, schrom, spos, True))
+        assert (c.lmm_form()[0] > 0) == (form == "lr")
+    excl = oracle_scan.windows_mask(schrom, spos, gchrom, glo, ghi)
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-3, excl=excl)
+    ora, pairs_ref = _at_device_delta(res[3], ora, pairs_ref, dec.dosage[k], Y, X, Q, lam, excl=excl)
+    _check_scan(res[:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
 
 
 def _at_device_delta(d_dev, ora, pairs_ref, G, Y, X, Q, lam, pthr=1e-3, excl=None):
