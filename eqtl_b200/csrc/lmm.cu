@@ -969,9 +969,12 @@ struct LmmEpi {
     float al[16];
     if constexpr (RAW) load16(Pr.snp_alpha + s0, al);
     if (!GLM && tt.lt_u) {  // uniform across the launch
-      // a gw scan (no windows), and a trans scan on a chunk clear of the
-      // gene's window, skip the per-pair window test
-      if (Pr.win.mode == kWinNone || (Pr.win.mode == kWinExclude && acc.chunk_clear(Pr.win, s0)))
+      // a gw scan (no windows), and a trans scan on a chunk clear of every
+      // lane's gene window, skip the per-pair window test; the vote keeps
+      // the warp on one path
+      if (Pr.win.mode == kWinNone)
+        post_cubic<false>(ci, s0, v[0], okw, al);
+      else if (Pr.win.mode == kWinExclude && __all_sync(__activemask(), acc.chunk_clear(Pr.win, s0)))
         post_cubic<false>(ci, s0, v[0], okw, al);
       else
         post_cubic<true>(ci, s0, v[0], okw, al);

@@ -95,9 +95,12 @@ struct LmEpi {
       igv[4 * q + 3] = v4.w;
     }
     if (tt.lt_u) {  // uniform across the launch
-      // a gw scan (no windows), and a trans scan on a chunk clear of the
-      // gene's window, skip the per-pair window test
-      if (P.win.mode == kWinNone || (P.win.mode == kWinExclude && acc.chunk_clear(P.win, s0)))
+      // a gw scan (no windows), and a trans scan on a chunk clear of every
+      // lane's gene window, skip the per-pair window test; the vote keeps
+      // the warp on one path
+      if (P.win.mode == kWinNone)
+        chunk_cubic<false>(s0, v[0], igv);
+      else if (P.win.mode == kWinExclude && __all_sync(__activemask(), acc.chunk_clear(P.win, s0)))
         chunk_cubic<false>(s0, v[0], igv);
       else
         chunk_cubic<true>(s0, v[0], igv);
