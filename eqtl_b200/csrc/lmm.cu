@@ -2207,7 +2207,9 @@ static bool lmm_lr_prepare(eqtl_ctx* ctx, int n, int G, float s2) {
   const int nint = static_cast<int>(std::ceil((hi - lo) / kLrSpan)) <= 5 ? 5 : 11;
   const double h = (hi - lo) / nint;
   const int nn = nint * (kLrNodes - 1) + 1;
-  if (nn > kTileM) return false;
+  // intervals longer than kLrSpan (a delta range beyond REML's 1e-8 .. 1e6)
+  // would lose the interpolation's accuracy: the direct form then
+  if (nn > kTileM || h > kLrSpan * (1.0 + 1e-12)) return false;
   std::vector<double> na(static_cast<size_t>(nn)), nd(static_cast<size_t>(nn));
   for (int q = 0; q < nint; ++q)
     for (int i = 0; i < kLrNodes; ++i)
