@@ -2179,7 +2179,7 @@ static bool lmm_lr_wanted(int G) {
 // [G][kb]; ws.unscale of gg and a_k). Returns false, leaving the direct form,
 // when the nodes would not fit one gene-side tile.
 template <int P>
-static bool lmm_lr_prepare(eqtl_ctx* ctx, int n, int G, float s2) {
+static bool lmm_lr_build(eqtl_ctx* ctx, int n, int G, float s2) {
   Workspace& ws = ctx->ws;
   const Geno& g = ctx->geno;
   const Rotated& R = ctx->rot;
@@ -2305,6 +2305,27 @@ static bool lmm_lr_prepare(eqtl_ctx* ctx, int n, int G, float s2) {
                                                   ws.lr_chi.p, ws.lr_clo.p, ws.unscale.p);
   EQTL_CUDA(cudaGetLastError());
   return true;
+}
+
+// lmm_lr_build, or the direct form when its tables do not fit in device
+// memory beside the scan's operands (their large buffers are given back).
+template <int P>
+static bool lmm_lr_prepare(eqtl_ctx* ctx, int n, int G, float s2) {
+  try {
+    return lmm_lr_build<P>(ctx, n, G, s2);
+  } catch (const Error& e) {
+    if (e.code != EQTL_E_NOMEM) throw;
+    EQTL_CUDA(cudaStreamSynchronize(ctx->stream));
+    (void)cudaGetLastError();  // the failed allocation's error, so later launch checks do not see it
+    Workspace& ws = ctx->ws;
+    ws.lr_val.release();
+    ws.lr_phi.release();
+    ws.lr_plo.release();
+    ws.lr_chi.release();
+    ws.lr_clo.release();
+    ws.lr_nodes = 0;
+    return false;
+  }
 }
 
 // The scan with interpolated gg and a_k: tile order [gg, a_0 .., NUM]; gg
