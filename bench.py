@@ -368,7 +368,8 @@ def b200_arm(args, rank, world, local_rank):
                             "tensor_speedup": s32 / scan_ms,
                             "algorithmic_tflops": flops / (s32 / 1e3) / 1e12,
                             "fp32_peak_tflops_at_sampled_clock": fp32_peak,
-                            "frac_of_fp32_peak": flops / (s32 / 1e3) / 1e12 / fp32_peak}
+                            "frac_of_fp32_peak": flops / (s32 / 1e3) / 1e12 / fp32_peak,
+                            "form": "direct (gg and a_k over K = n)"}
         ctx32.close()
     # ---- the split-BF16 form of the same scan (BF16 hi + lo on both sides,
     # three products per accumulator: the exact dosage slice is FP16-only)
