@@ -116,7 +116,7 @@ bool gene_ready(const Study& st, const std::vector<double>& y, bool checks,
   }
   if (kept != n && !keep)
     die("phenotype or covariate values missing for some samples: the device scans take per-gene sample sets in "
-        "the trans and gw scopes of the LM and LMM without permutations; here every gene must keep every "
+        "the cis, trans and gw scopes of the LM and LMM without permutations; here every gene must keep every "
         "analysis sample");
   if (!checks) return true;
   return kept >= 3 && !(mx < 1e-15);
@@ -525,17 +525,45 @@ void run_cis(const Study& st, const std::string& model, ScopeFiles& out, std::ve
     std::stable_sort(works.begin(), works.end(), [](const Job& a, const Job& b) {
       return a.loc->chrom != b.loc->chrom ? a.loc->chrom < b.loc->chrom : a.loc->tss < b.loc->tss;
     });
+  std::vector<std::vector<int32_t>> keeps;
+  bool mixed = false;
   for (size_t w = 0; w < works.size(); ++w) {
     Job jb = works[w];
     jb.work = static_cast<int>(w);
-    // the LM path applies the complete-case checks; the LMM path with the
-    // shared basis takes the gene as it is (src/scan_cis.cpp:56-63)
-    if (!gene_ready(st, gene_y(st, jb.gene), model == "lm")) continue;
+    // the LM takes every gene through the complete-case checks; the LMM with
+    // the shared basis takes a gene that keeps every sample as it is, and one
+    // with missing values through the checks on its own sample set
+    // (src/scan_cis.cpp:111-120, src/scan.cpp:259-269)
+    std::vector<int32_t> keep;
+    const bool ok = gene_ready(st, gene_y(st, jb.gene), true, &keep);
+    const bool full = keep.size() == st.samples.size();
+    if (!ok && !(model == "lmm" && full)) continue;
+    mixed = mixed || !full;
     jobs.push_back(jb);
+    keeps.push_back(std::move(keep));
   }
   info("cis " + model + ": " + std::to_string(jobs.size()) + " genes");
   if (jobs.empty()) return;
   const double pthr = opt.pval_cis;
+  if (mixed) {
+    // per-gene sample sets: the genes of each set scan on its sample view
+    // (scan_by_keep), results in job order; pairs by gene, then SNP
+    if (opt.perm > 0)
+      die("phenotype or covariate values missing for some samples: gene-level permutations take the case where "
+          "every gene keeps every analysis sample");
+    Trace tr;
+    KeepScan K = scan_by_keep(st, model, jobs, keeps, 2, pthr);
+    tr.mark("cis " + model + ": device scans of the gene sample sets");
+    std::vector<size_t> order(K.R.pairs.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      const eqtl_pair &x = K.R.pairs[a], &y = K.R.pairs[b];
+      return x.gene != y.gene ? x.gene < y.gene : x.snp < y.snp;
+    });
+    emit(st, jobs, K.R, "cis", pthr, order, out, regions, nullptr, opt.threads > 1 ? works.size() : 0, &K.n_job,
+         &K.af_job);
+    return;
+  }
   // the device scan takes the genes in window order (a banded tile list);
   // results come back to the output order
   std::vector<size_t> dev_order(jobs.size());

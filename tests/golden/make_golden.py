@@ -72,7 +72,8 @@ CASES = {
     # per-gene sample sets: some genes miss phenotype values (two of them at
     # the same samples, one with only 2 values left, so it drops out), and in
     # the *_cna runs one sample misses a covariate value, so no gene keeps
-    # every analysis sample
+    # every analysis sample; cis_cna also takes the reference's per-thread
+    # cis path (-t 2)
     "nakeep": dict(
         geno=dict(seed=501, n=110, m=700, n_chrom=3, chrom_len=5_000_000, family=(4, 5, 90),
                   miss_rate=0.01, maf_lo=0.02),
@@ -84,6 +85,8 @@ CASES = {
             ("trans", ["--model", "lm,lmm", "--mode", "trans", "--pval-trans", "1e-2", "-t", "1"]),
             ("gw", ["--model", "lm,lmm", "--mode", "gw", "--pval-trans", "1e-2", "-t", "1"]),
             ("trans_cna", ["--model", "lm,lmm", "--mode", "trans", "--pval-trans", "1e-2", "-t", "1"]),
+            ("cis", ["--model", "lm,lmm", "--mode", "cis", "-w", "500000", "--pval-cis", "1e-2", "-t", "1"]),
+            ("cis_cna", ["--model", "lm,lmm", "--mode", "cis", "-w", "500000", "--pval-cis", "1e-2", "-t", "2"]),
         ]),
 }
 
