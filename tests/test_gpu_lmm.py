@@ -113,6 +113,33 @@ def test_trans_lmm_interpolated_matches_oracle(ncov, monkeypatch):
         _check_scan(res[form][:3], ora, pairs_ref, 1e-3, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
 
 
+@pytest.mark.parametrize("G", [1, 2])
+def test_trans_lmm_interpolated_narrow_delta_range(G, monkeypatch):
+    """A narrow range of deltas takes the smaller node layout: 5 intervals,
+    56 nodes, K = 64 columns per accumulator (one gene: the degenerate range,
+    widened by 1/2 on each side)."""
+    from eqtl_b200 import capi
+    g, rows, Y, X = _case(seed=29, ncov=1, G=4, n=250, fam=(10, 6, 190))
+    Y = Y[:, :G].copy()
+    n = g.codes.shape[1]
+    dec = R.decode_bed_rows(rows, n, np.arange(n), "impute", 0.8, 0.0)
+    k = np.nonzero(dec.keep)[0]
+    Kr, _, _ = R.compute_grm(dec.dosage[k], dec.codes[k] < 0)
+    Q, lam = R.make_lmm_basis(Kr)
+    monkeypatch.setenv("EQTL_LMM_FORM", "lr")
+    with capi.Context(0) as c:
+        c.load_bed(rows, n, np.arange(n))
+        c.set_basis(Q, lam)
+        res = c.scan_trans_lmm(Y, X, pthr=1e-2)
+        nodes, cols = c.lmm_form()
+    assert nodes > 0 and cols == (64 if nodes <= 64 else 128)
+    if G == 1:
+        assert (nodes, cols) == (56, 64)
+    ora, pairs_ref = oracle_scan.trans_lmm(dec.dosage[k], Y, X, Q, lam, 1e-2)
+    ora, pairs_ref = _at_device_delta(res[3], ora, pairs_ref, dec.dosage[k], Y, X, Q, lam, pthr=1e-2)
+    _check_scan(res[:3], ora, pairs_ref, 1e-2, n - X.shape[1] - 1, t_err=T_ERRS[0], rel=1e-6)
+
+
 @pytest.mark.parametrize("form", ["lr", "direct"])
 def test_trans_lmm_excludes_cis_windows(form, monkeypatch):
     """The trans scope: each gene's cis window excluded (genes without a
