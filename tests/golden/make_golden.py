@@ -87,6 +87,8 @@ CASES = {
             ("trans_cna", ["--model", "lm,lmm", "--mode", "trans", "--pval-trans", "1e-2", "-t", "1"]),
             ("cis", ["--model", "lm,lmm", "--mode", "cis", "-w", "500000", "--pval-cis", "1e-2", "-t", "1"]),
             ("cis_cna", ["--model", "lm,lmm", "--mode", "cis", "-w", "500000", "--pval-cis", "1e-2", "-t", "2"]),
+            ("int", ["--model", "lm,lmm", "--mode", "trans", "--pheno-norm", "int", "--pval-trans", "1e-2",
+                     "-t", "1"]),
         ]),
 }
 
