@@ -2171,13 +2171,14 @@ static bool lmm_lr_wanted(int G) {
 }
 
 // Interpolated gg and a_k: Chebyshev-Lobatto nodes over the genes' range of
-// ln(delta) (5 or 11 equal intervals, whichever first keeps them within
-// kLrSpan, kLrNodes nodes each, neighbours sharing their end node), the node genes' operands (w and Q (w o X~_k) at
-// each node delta, as lmm_gene_ops_raw_kernel forms a gene's), the node pass
-// over every kept SNP, then both sides of the scan's gg and a_k accumulators
-// (ws.lr_phi / lr_plo: SNP side [m][kb]; ws.lr_chi / lr_clo: gene side
-// [G][kb]; ws.unscale of gg and a_k). Returns false, leaving the direct form,
-// when the nodes would not fit one gene-side tile.
+// ln(delta) (5 equal intervals if that keeps each within kLrSpan, else 11;
+// kLrNodes nodes each, neighbours sharing their end node: 56 or 122 nodes),
+// the node genes' operands (w and Q (w o X~_k) at each node delta, as
+// lmm_gene_ops_raw_kernel forms a gene's), the node pass over every kept
+// SNP, then both sides of the scan's gg and a_k accumulators (ws.lr_phi /
+// lr_plo: SNP side [m][kb]; ws.lr_chi / lr_clo: gene side [G][kb];
+// ws.unscale of gg and a_k). Returns false, leaving the direct form, when
+// the intervals would be longer than kLrSpan.
 template <int P>
 static bool lmm_lr_build(eqtl_ctx* ctx, int n, int G, float s2) {
   Workspace& ws = ctx->ws;
