@@ -281,7 +281,8 @@ int eqtl_grm(eqtl_ctx* ctx, double* K_out, int32_t* N_packed_out, int64_t* m_use
  *     made: open the context while device memory can still be allocated,
  *     and before any stream capture;
  *   - the call returns once its work on the context's stream has finished
- *     (the outputs are ready to use);
+ *     (the outputs are ready to use): it synchronises the stream, so it
+ *     cannot itself be recorded in a stream capture;
  *   - the accumulators and counters are zeroed at the start of every call
  *     on the context's stream; K is exactly symmetric (the lower triangle
  *     is summed, the upper one mirrors it);
